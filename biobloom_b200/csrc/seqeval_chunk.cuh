@@ -1,0 +1,379 @@
+/*
+ * seqeval_chunk.cuh -- SeqEval::evalSimple (Common/SeqEval.h:37-114) and
+ * SeqEval::evalMinMatchLen (Common/SeqEval.h:295-332) restated over 32-frame
+ * chunks of hit bits.
+ *
+ * A warp probes the filter for 32 consecutive frames at once (one frame per
+ * lane) and ballots the results.  The functions here then advance the
+ * reference's sequential state machine over those 32 frames using mask
+ * arithmetic (popcounts over prefixes), so the decision, and the frame at
+ * which it is taken, are exactly those of the sequential loop.  All inputs are
+ * warp-uniform, so every lane runs the same scalar code; the functions are
+ * also compiled for the host, where tests drive them against the CPU oracle.
+ *
+ * Frame model.  Frame p is the k-mer starting at base p of the read,
+ * p in [0, len-k].  It is "valid" when the k-mer holds only ACGT: those are the
+ * positions ntHashIterator visits.  The reference's gap handling
+ * (SeqEval.h:71-77) adds, at the next valid frame, one to antiScore for each
+ * skipped invalid frame; that is counted here one frame at a time.  The only
+ * observable difference is where a rejection is taken, and a rejection is
+ * final either way, so decisions are unchanged.  Leading invalid frames are not
+ * counted (the first frame has no gap check, SeqEval.h:52-67).  After a miss
+ * that ends a streak of at least streakThreshold hits, the reference walks the
+ * visited positions below pos+k adding one per position without probing
+ * (SeqEval.h:99-110); invalid frames inside that window before its last valid
+ * frame are therefore not counted, and those after it are counted by the next
+ * gap check.
+ */
+#ifndef BBT_SEQEVAL_CHUNK_CUH
+#define BBT_SEQEVAL_CHUNK_CUH
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define BBT_HD __host__ __device__ __forceinline__
+#else
+#define BBT_HD inline
+#endif
+
+namespace bbt {
+
+BBT_HD int popc32(uint32_t x)
+{
+#if defined(__CUDA_ARCH__)
+	return __popc(x);
+#else
+	return __builtin_popcount(x);
+#endif
+}
+
+/* index of the lowest set bit (x != 0) */
+BBT_HD int lowbit32(uint32_t x)
+{
+#if defined(__CUDA_ARCH__)
+	return __ffs(x) - 1;
+#else
+	return __builtin_ctz(x);
+#endif
+}
+
+/* index of the highest set bit (x != 0) */
+BBT_HD int highbit32(uint32_t x)
+{
+#if defined(__CUDA_ARCH__)
+	return 31 - __clz(x);
+#else
+	return 31 - __builtin_clz(x);
+#endif
+}
+
+/* bits [0, n) set, n in [0, 32] */
+BBT_HD uint32_t low_mask(int n)
+{
+	return n >= 32 ? 0xffffffffu : (n <= 0 ? 0u : ((1u << n) - 1u));
+}
+
+/* bits [lo, hi) set */
+BBT_HD uint32_t range_mask(int lo, int hi)
+{
+	return low_mask(hi) & ~low_mask(lo);
+}
+
+/* position of the n-th (1-based) set bit of x, which has at least n set bits */
+BBT_HD int nth_bit(uint32_t x, int n)
+{
+	for (int i = 1; i < n; ++i)
+		x &= x - 1;
+	return lowbit32(x);
+}
+
+enum { EVAL_OPEN = 0, EVAL_ACCEPT = 1, EVAL_REJECT = 2 };
+
+/*
+ * State of one (read, filter) evaluation under SIMPLE scoring.
+ * score2 is twice the reference's double score (a multiple of 0.5), so
+ * "thres <= score" is "score2 >= thres2" with thres2 = ceil(2*thres); anti
+ * is antiScore and "antiThres <= antiScore" is "anti >= anti_thres".
+ */
+struct SimpleState {
+	int64_t score2;
+	int64_t anti;
+	int64_t thres2;
+	int64_t anti_thres;
+	int32_t streak;       /* hits in the current streak (saturates at 64) */
+	int32_t started;      /* a valid frame has been visited */
+	int64_t skip_until;   /* frames below this belong to a skip window */
+	int32_t in_window;    /* a skip window is open (frames < skip_until) */
+	int32_t pending;      /* invalid window frames after its last valid one */
+	int32_t decided;      /* EVAL_* */
+};
+
+/*
+ * Thresholds exactly as SeqEval.h:41-45 computes them:
+ *   thres     = threshold * (len - k + 1)
+ *   antiThres = floor((1 - threshold) * (len - k + 1))
+ * with one IEEE double multiply each (one_minus = 1.0 - threshold is
+ * computed once by the caller, as the reference's argument is).
+ */
+BBT_HD void simple_init(SimpleState &s, double threshold, double one_minus,
+		uint64_t frames)
+{
+	double fr = (double)frames;
+	double thres = threshold * fr;
+	double anti = one_minus * fr;
+#if defined(__CUDA_ARCH__)
+	thres = __dmul_rn(threshold, fr);
+	anti = __dmul_rn(one_minus, fr);
+#endif
+	double t2 = thres * 2.0; /* exact */
+	double c = t2 <= 0.0 ? 0.0 : (double)(int64_t)t2;
+	if (c < t2)
+		c += 1.0;
+	double a = anti;
+	double fa = (double)(int64_t)a;
+	if (fa > a)
+		fa -= 1.0; /* floor for negative values */
+	s.score2 = 0;
+	s.anti = 0;
+	s.thres2 = (int64_t)c;
+	s.anti_thres = (int64_t)fa;
+	s.streak = 0;
+	s.started = 0;
+	s.skip_until = 0;
+	s.in_window = 0;
+	s.pending = 0;
+	s.decided = EVAL_OPEN;
+}
+
+/*
+ * Advance over one chunk of 32 frames starting at frame `base`.
+ *   V:  valid frames (bit j = frame base+j), already limited to the read
+ *   H:  hits among V (only bits the caller probed matter; see below)
+ *   nf: frames of the read that exist in this chunk (bits >= nf are past the
+ *       end of the read)
+ * Frames below s.skip_until are inside a skip window: their H bits are never
+ * read, so the caller need not probe them.  Returns s.decided.
+ */
+BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int64_t base,
+		int nf, int k, int streak_thr)
+{
+	if (s.decided)
+		return s.decided;
+	const uint32_t inread = low_mask(nf);
+	V &= inread;
+	H &= V;
+	int j = 0;
+	while (j < nf) {
+		/* ---- skip-window frames ---- */
+		if (s.in_window) {
+			int64_t we = s.skip_until - base;
+			int e = we >= nf ? nf : (int)we;
+			if (e > j) {
+				uint32_t r = range_mask(j, e);
+				uint32_t vw = V & r;
+				s.anti += popc32(vw);
+				if (vw) {
+					int last = highbit32(vw);
+					s.pending = popc32(~V & range_mask(last + 1, e));
+				} else {
+					s.pending += popc32(~V & r);
+				}
+				if (s.anti >= s.anti_thres) {
+					s.decided = EVAL_REJECT;
+					return s.decided;
+				}
+				j = e;
+			}
+			if (s.skip_until - base <= nf) {
+				/* window closed inside the read: its trailing invalid
+				 * frames count as the next gap does */
+				s.anti += s.pending;
+				s.pending = 0;
+				s.in_window = 0;
+				s.streak = 0;
+				if (s.anti >= s.anti_thres) {
+					s.decided = EVAL_REJECT;
+					return s.decided;
+				}
+			}
+			continue;
+		}
+		/* ---- ordinary frames [j, nf) ---- */
+		const uint32_t rng = range_mask(j, nf);
+		const uint32_t Hr = H & rng;
+		const uint32_t Mr = V & ~H & rng;
+		uint32_t Cr = ~V & rng; /* invalid frames */
+		if (!s.started) {
+			uint32_t vr = V & rng;
+			/* leading invalid frames are not counted */
+			Cr = vr ? (Cr & ~low_mask(lowbit32(vr))) : 0u;
+		}
+		/* ext: bit 32+i is "frame base+i was a hit"; bits below 32 hold the
+		 * carried streak ending at frame base+j-1 */
+		uint64_t carry = 0;
+		{
+			int st = s.streak;
+			if (st > 0) {
+				/* streak frames end at frame j-1 */
+				uint64_t ones = st >= 64 ? ~0ull : ((1ull << st) - 1ull);
+				carry = ones << (32 + j - (st > 32 + j ? 32 + j : st));
+				if (st > 32 + j)
+					carry = (1ull << (32 + j)) - 1ull;
+			}
+		}
+		const uint64_t ext = ((uint64_t)Hr << 32) | carry;
+		/* hits whose previous frame is a hit of the same streak: these add
+		 * 1.0 to the score, the others 0.5 */
+		const uint32_t prevhit = (uint32_t)((ext << 1) >> 32) & Hr;
+		/* skip triggers: a miss after at least streak_thr consecutive hits */
+		uint32_t trig;
+		if (streak_thr <= 0) {
+			trig = Mr;
+		} else if (streak_thr <= 32) {
+			uint64_t t = ~0ull;
+			for (int q = 1; q <= streak_thr; ++q)
+				t &= ext << q;
+			trig = Mr & (uint32_t)(t >> 32);
+		} else {
+			trig = 0; /* resolved frame by frame below */
+			if (s.streak + popc32(Hr) >= streak_thr) {
+				int run = s.streak;
+				for (int q = j; q < nf; ++q) {
+					uint32_t b = 1u << q;
+					if (Hr & b) {
+						++run;
+					} else if (Mr & b) {
+						if (run >= streak_thr) {
+							trig = b;
+							break;
+						}
+						run = 0;
+					} else {
+						run = 0;
+					}
+				}
+			}
+		}
+		/* the first visited frame never opens a window (SeqEval.h:52-67
+		 * has no skip branch), which matters when streak_thr is 0 */
+		if (!s.started && (V & rng))
+			trig &= ~(1u << lowbit32(V & rng));
+		const int t = trig ? lowbit32(trig) : nf;
+		const uint32_t pre = range_mask(j, t);
+		const uint32_t hp = Hr & pre;
+		const uint32_t hp2 = prevhit & pre;
+		const uint32_t ap = (Mr | Cr) & pre;
+		const int64_t dS = popc32(hp) + popc32(hp2);
+		const int64_t dA = popc32(ap);
+		int acc_pos = 32, rej_pos = 32;
+		if (s.score2 + dS >= s.thres2) {
+			int64_t sc = s.score2;
+			uint32_t x = hp;
+			while (x) {
+				int q = lowbit32(x);
+				x &= x - 1;
+				sc += ((hp2 >> q) & 1u) ? 2 : 1;
+				if (sc >= s.thres2) {
+					acc_pos = q;
+					break;
+				}
+			}
+		}
+		if (s.anti + dA >= s.anti_thres) {
+			int64_t need = s.anti_thres - s.anti;
+			rej_pos = need <= 0 ? (ap ? lowbit32(ap) : 32)
+			                    : nth_bit(ap, (int)need);
+		}
+		if (acc_pos < rej_pos) {
+			s.decided = EVAL_ACCEPT;
+			return s.decided;
+		}
+		if (rej_pos < 32) {
+			s.decided = EVAL_REJECT;
+			return s.decided;
+		}
+		s.score2 += dS;
+		s.anti += dA;
+		if (V & pre)
+			s.started = 1;
+		/* streak at frame t (or at the end of the chunk) */
+		{
+			uint32_t nonhit = ~hp & pre;
+			if (nonhit) {
+				int lastbreak = highbit32(nonhit);
+				s.streak = popc32(hp & ~low_mask(lastbreak + 1));
+			} else {
+				int add = popc32(hp);
+				s.streak = s.streak + add > 64 ? 64 : s.streak + add;
+			}
+		}
+		if (t >= nf)
+			break;
+		/* open the skip window at the trigger frame: the trigger frame itself
+		 * is its first visited position */
+		s.started = 1;
+		s.in_window = 1;
+		s.pending = 0;
+		s.skip_until = base + t + k;
+		j = t;
+	}
+	return s.decided;
+}
+
+/*
+ * State of one (read, filter) evaluation under LENGTH scoring
+ * (evalMinMatchLen): the length of the current run of matching bases.
+ */
+struct LengthState {
+	int64_t match;
+	int64_t prev;     /* last visited frame, -1 before the first */
+	int64_t min_len;
+	int64_t len;      /* read length in bases */
+	int32_t k;
+	int32_t decided;
+};
+
+BBT_HD void length_init(LengthState &s, unsigned min_len, uint64_t len, int k)
+{
+	s.match = 0;
+	s.prev = 0; /* the reference starts prevPos at 0 */
+	s.min_len = min_len;
+	s.len = (int64_t)len;
+	s.k = k;
+	s.decided = EVAL_OPEN;
+}
+
+/* Advance over one chunk; every valid frame must have been probed. */
+BBT_HD int length_chunk(LengthState &s, uint32_t V, uint32_t H, int64_t base,
+		int nf)
+{
+	if (s.decided)
+		return s.decided;
+	V &= low_mask(nf);
+	uint32_t x = V;
+	while (x) {
+		int q = lowbit32(x);
+		x &= x - 1;
+		int64_t pos = base + q;
+		if (s.len - pos + s.match < s.min_len) {
+			s.decided = EVAL_REJECT;
+			return s.decided;
+		}
+		if (pos != s.prev + 1)
+			s.match = 0;
+		if ((H >> q) & 1u)
+			s.match = s.match == 0 ? s.k : s.match + 1;
+		else
+			s.match = 0;
+		if (s.match >= s.min_len) {
+			s.decided = EVAL_ACCEPT;
+			return s.decided;
+		}
+		s.prev = pos;
+	}
+	return s.decided;
+}
+
+} // namespace bbt
+
+#endif

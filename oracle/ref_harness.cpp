@@ -1,0 +1,183 @@
+/*
+ * ref_harness.cpp -- drives the reference's own classification code
+ * (compiled from the reference sources by oracle/Makefile into oracle/_ref).
+ * TEST INFRASTRUCTURE ONLY.
+ *
+ *   ref_harness hits  SCORE STREAK FILTER.bf[,FILTER.bf...] READS [READS2]
+ *       For every read (pair), prints one line "<name>\t<hits>" where hits is
+ *       the comma-separated list of filter indices whose
+ *       SeqEval::evalRead (Common/SeqEval.h:493-524) accepted the read
+ *       (for pairs: "<hits1>|<hits2>").  Then prints "#SUMMARY" and the
+ *       ResultsManager summary text (ResultsManager.hpp:191-237), computed
+ *       by the reference's own ResultsManager.
+ *   ref_harness time  SCORE STREAK THREADS INCLUSIVE PREFIX FILTERS READS [READS2]
+ *       Builds a BioBloomClassifier (BioBloomClassifier.cpp:21-28; filter
+ *       load not timed), then times filter()/filterPair() and prints one JSON
+ *       line with the wall time, reads and cores used.
+ *
+ * A score > 1 selects LENGTH scoring, as BioBloomCategorizer.cpp:423-430 does.
+ */
+#include "BioBloomClassifier.h"
+#include "ResultsManager.hpp"
+#include "Common/Options.h"
+#include "Common/SeqEval.h"
+#include <omp.h>
+#include <cstdio>
+#include <cstdlib>
+#include <sstream>
+#include <string>
+#include <vector>
+
+using namespace std;
+
+static vector<string> split_commas(const string &s)
+{
+	vector<string> out;
+	string cur;
+	stringstream in(s);
+	while (getline(in, cur, ','))
+		if (!cur.empty())
+			out.push_back(cur);
+	return out;
+}
+
+static void set_score(double score)
+{
+	opt::score = score;
+	unsigned matchLen = (unsigned)score;
+	if (matchLen > 1) {
+		opt::score = (unsigned)matchLen;
+		opt::scoringMethod = opt::LENGTH;
+	}
+}
+
+static string join(const vector<unsigned> &v)
+{
+	string s;
+	for (size_t i = 0; i < v.size(); ++i) {
+		if (i)
+			s += ",";
+		s += to_string(v[i]);
+	}
+	return s;
+}
+
+static int mode_hits(int argc, char **argv)
+{
+	if (argc < 6) {
+		fprintf(stderr, "usage: ref_harness hits SCORE STREAK FILTERS READS [READS2]\n");
+		return 2;
+	}
+	set_score(atof(argv[2]));
+	opt::streakThreshold = (unsigned)atoi(argv[3]);
+	vector<string> paths = split_commas(argv[4]);
+	vector<BloomFilter *> filters;
+	vector<string> ids;
+	for (size_t i = 0; i < paths.size(); ++i) {
+		filters.push_back(new BloomFilter(paths[i]));
+		BloomFilterInfo info(paths[i].substr(0, paths[i].size() - 2) + "txt");
+		ids.push_back(info.getFilterID());
+	}
+	bool paired = argc > 6;
+	ResultsManager<unsigned> res(ids, false);
+	gzFile fp1 = gzopen(argv[5], "r");
+	gzFile fp2 = paired ? gzopen(argv[6], "r") : Z_NULL;
+	if (fp1 == Z_NULL || (paired && fp2 == Z_NULL)) {
+		fprintf(stderr, "cannot open reads\n");
+		return 1;
+	}
+	kseq_t *k1 = kseq_init(fp1);
+	kseq_t *k2 = paired ? kseq_init(fp2) : NULL;
+	size_t total = 0;
+	for (;;) {
+		int l1 = kseq_read(k1);
+		int l2 = paired ? kseq_read(k2) : 0;
+		if (l1 < 0 || l2 < 0)
+			break;
+		string s1(k1->seq.s, l1);
+		vector<unsigned> h1, h2;
+		for (unsigned f = 0; f < filters.size(); ++f)
+			if (SeqEval::evalRead(s1, *filters[f], opt::score))
+				h1.push_back(f);
+		++total;
+		if (paired) {
+			string s2(k2->seq.s, l2);
+			for (unsigned f = 0; f < filters.size(); ++f)
+				if (SeqEval::evalRead(s2, *filters[f], opt::score))
+					h2.push_back(f);
+			res.updateSummaryData(h1, h2);
+			printf("%s\t%s|%s\n", k1->name.s, join(h1).c_str(), join(h2).c_str());
+		} else {
+			res.updateSummaryData(h1);
+			printf("%s\t%s\n", k1->name.s, join(h1).c_str());
+		}
+	}
+	printf("#SUMMARY\n%s", res.getResultsSummary(total).c_str());
+	kseq_destroy(k1);
+	gzclose(fp1);
+	if (paired) {
+		kseq_destroy(k2);
+		gzclose(fp2);
+	}
+	return 0;
+}
+
+static size_t count_records(const char *path)
+{
+	gzFile fp = gzopen(path, "r");
+	if (fp == Z_NULL)
+		return 0;
+	kseq_t *k = kseq_init(fp);
+	size_t n = 0;
+	while (kseq_read(k) >= 0)
+		++n;
+	kseq_destroy(k);
+	gzclose(fp);
+	return n;
+}
+
+static int mode_time(int argc, char **argv)
+{
+	if (argc < 9) {
+		fprintf(stderr, "usage: ref_harness time SCORE STREAK THREADS INCLUSIVE PREFIX FILTERS READS [READS2]\n");
+		return 2;
+	}
+	set_score(atof(argv[2]));
+	opt::streakThreshold = (unsigned)atoi(argv[3]);
+	int threads = atoi(argv[4]);
+	if (threads > 0)
+		omp_set_num_threads(threads);
+	opt::threads = (unsigned)(threads > 0 ? threads : omp_get_max_threads());
+	bool inclusive = atoi(argv[5]) != 0;
+	opt::outputPrefix = argv[6];
+	vector<string> paths = split_commas(argv[7]);
+	bool paired = argc > 9;
+	size_t reads = count_records(argv[8]);
+	BioBloomClassifier bbc(paths, opt::score, opt::outputPrefix, opt::filePostfix);
+	if (inclusive)
+		bbc.setInclusive();
+	double t0 = omp_get_wtime();
+	if (paired)
+		bbc.filterPair(argv[8], argv[9]);
+	else
+		bbc.filter(vector<string>(1, argv[8]));
+	double t1 = omp_get_wtime();
+	printf("{\"seconds\": %.6f, \"records\": %zu, \"paired\": %d, \"threads\": %u}\n",
+			t1 - t0, reads, paired ? 1 : 0, opt::threads);
+	return 0;
+}
+
+int main(int argc, char **argv)
+{
+	if (argc < 2) {
+		fprintf(stderr, "usage: ref_harness hits|time ...\n");
+		return 2;
+	}
+	string mode = argv[1];
+	if (mode == "hits")
+		return mode_hits(argc, argv);
+	if (mode == "time")
+		return mode_time(argc, argv);
+	fprintf(stderr, "unknown mode %s\n", argv[1]);
+	return 2;
+}

@@ -1,0 +1,57 @@
+/*
+ * chunk_model.cpp -- host build of the product's chunked SeqEval state
+ * machine (biobloom_b200/csrc/seqeval_chunk.cuh), fed with per-frame hit bits
+ * from the CPU oracle.  Used by tests/test_chunk_model.py to check the
+ * chunked decision against the oracle's sequential evalSimple /
+ * evalMinMatchLen on random reads, without a GPU.
+ */
+#include "seqeval_chunk.cuh"
+#include "bbt_oracle.h"
+#include <vector>
+
+extern "C" int model_eval(const char *seq, uint64_t len, const oracle_bf *bf,
+		double threshold, unsigned streak_thr, int scoring,
+		uint64_t *probed_frames)
+{
+	const unsigned k = bf->k;
+	if (len < k)
+		return 0;
+	const uint64_t frames = len - k + 1;
+	std::vector<uint8_t> valid(frames), hit(frames);
+	/* validity and hit bit of every frame, from the oracle's iterator */
+	oracle_ntitr it;
+	for (oracle_ntitr_init(&it, seq, len, bf->h, k); !oracle_ntitr_end(&it);
+			oracle_ntitr_next(&it)) {
+		valid[it.pos] = 1;
+		hit[it.pos] = (uint8_t)oracle_bf_contains(bf, it.hv, 0);
+	}
+	bbt::SimpleState ss;
+	bbt::LengthState ls;
+	if (scoring == ORACLE_LENGTH)
+		bbt::length_init(ls, (unsigned)(threshold + 0.5), len, (int)k);
+	else
+		bbt::simple_init(ss, threshold, 1.0 - threshold, frames);
+	for (uint64_t base = 0; base < frames; base += 32) {
+		int nf = frames - base >= 32 ? 32 : (int)(frames - base);
+		uint32_t V = 0, H = 0;
+		for (int j = 0; j < nf; ++j) {
+			uint64_t p = base + j;
+			if (!valid[p])
+				continue;
+			V |= 1u << j;
+			bool probe = scoring == ORACLE_LENGTH || (int64_t)p >= ss.skip_until;
+			if (probe) {
+				if (probed_frames)
+					++*probed_frames;
+				if (hit[p])
+					H |= 1u << j;
+			}
+		}
+		int d = scoring == ORACLE_LENGTH
+				? bbt::length_chunk(ls, V, H, (int64_t)base, nf)
+				: bbt::simple_chunk(ss, V, H, (int64_t)base, nf, (int)k, (int)streak_thr);
+		if (d)
+			return d == bbt::EVAL_ACCEPT;
+	}
+	return 0;
+}

@@ -1,0 +1,219 @@
+"""ctypes access to the CPU oracle (oracle/_build/liboracle.so).
+
+Test infrastructure only: tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg use this module as the checker; the product path never does.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+
+SIMPLE = 0
+LENGTH = 1
+
+
+class _BF(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_uint64), ("h", ctypes.c_uint), ("k", ctypes.c_uint),
+                ("dfpr", ctypes.c_double), ("n_entry", ctypes.c_uint64),
+                ("t_entry", ctypes.c_uint64), ("bits", ctypes.POINTER(ctypes.c_uint8))]
+
+
+class _Itr(ctypes.Structure):
+    _fields_ = [("seq", ctypes.c_char_p), ("len", ctypes.c_size_t), ("k", ctypes.c_uint),
+                ("h", ctypes.c_uint), ("pos", ctypes.c_size_t), ("fh", ctypes.c_uint64),
+                ("rh", ctypes.c_uint64), ("hv", ctypes.c_uint64 * 64)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle")], check=True,
+                           capture_output=True)
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        u64, u32, dbl, sz = ctypes.c_uint64, ctypes.c_uint, ctypes.c_double, ctypes.c_size_t
+        L.oracle_nt_forward.restype = u64
+        L.oracle_nt_forward.argtypes = [ctypes.c_char_p, u32]
+        L.oracle_nt_reverse.restype = u64
+        L.oracle_nt_reverse.argtypes = [ctypes.c_char_p, u32]
+        L.oracle_nt_extra.restype = u64
+        L.oracle_nt_extra.argtypes = [u64, u32, u32]
+        L.oracle_ntitr_init.argtypes = [P(_Itr), ctypes.c_char_p, sz, u32, u32]
+        L.oracle_ntitr_next.argtypes = [P(_Itr)]
+        L.oracle_bf_create.argtypes = [P(_BF), u64, u32, u32]
+        L.oracle_bf_free.argtypes = [P(_BF)]
+        L.oracle_bf_contains.argtypes = [P(_BF), P(u64), P(u64)]
+        L.oracle_bf_insert.argtypes = [P(_BF), P(u64)]
+        L.oracle_bf_store.argtypes = [P(_BF), ctypes.c_char_p]
+        L.oracle_bf_load.argtypes = [P(_BF), ctypes.c_char_p]
+        L.oracle_calc_optimal_size.restype = u64
+        L.oracle_calc_optimal_size.argtypes = [u64, dbl, u32]
+        L.oracle_calc_optimal_hash_num.restype = u32
+        L.oracle_calc_optimal_hash_num.argtypes = [dbl]
+        L.oracle_make_filter.argtypes = [P(_BF), P(ctypes.c_char_p), P(u64), sz, u32, dbl,
+                                         u32, P(u64), P(u64)]
+        L.oracle_write_info.argtypes = [ctypes.c_char_p, ctypes.c_char_p, u32, dbl, u32, u64,
+                                        ctypes.c_char_p, u64, u64, dbl, u64, dbl]
+        L.oracle_eval_simple.argtypes = [ctypes.c_char_p, sz, P(_BF), dbl, u32, P(u64)]
+        L.oracle_eval_min_match_len.argtypes = [ctypes.c_char_p, sz, P(_BF), u32, P(u64)]
+        L.oracle_classify.argtypes = [ctypes.c_char_p, P(u64), sz, P(P(_BF)), u32, dbl, u32,
+                                      ctypes.c_int, P(u64), P(u64)]
+        L.oracle_update_summary.restype = u32
+        L.oracle_update_summary.argtypes = [P(u64), u32, P(u64)]
+        L.oracle_update_summary_pair.restype = u32
+        L.oracle_update_summary_pair.argtypes = [P(u64), u32, P(u64), P(u64), ctypes.c_int]
+        L.oracle_summary_tsv.restype = sz
+        L.oracle_summary_tsv.argtypes = [P(u64), u32, P(ctypes.c_char_p), u64, ctypes.c_char_p,
+                                         sz]
+        _lib = L
+    return _lib
+
+
+def _u64p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+class Filter:
+    """A Bloom filter held by the oracle."""
+
+    def __init__(self):
+        self.bf = _BF()
+        self._owned = False
+
+    @classmethod
+    def create(cls, m, h, k):
+        f = cls()
+        if lib().oracle_bf_create(ctypes.byref(f.bf), m, h, k):
+            raise MemoryError
+        f._owned = True
+        return f
+
+    @classmethod
+    def load(cls, path):
+        f = cls()
+        rc = lib().oracle_bf_load(ctypes.byref(f.bf), path.encode())
+        if rc:
+            raise IOError(f"oracle_bf_load({path}) = {rc}")
+        f._owned = True
+        return f
+
+    @classmethod
+    def make(cls, seqs, k=25, fpr=0.075, h=0):
+        f = cls()
+        arr = (ctypes.c_char_p * len(seqs))(*seqs)
+        lens = np.array([len(s) for s in seqs], dtype=np.uint64)
+        exp = ctypes.c_uint64()
+        red = ctypes.c_uint64()
+        if lib().oracle_make_filter(ctypes.byref(f.bf), arr, _u64p(lens), len(seqs), k, fpr, h,
+                                    ctypes.byref(exp), ctypes.byref(red)):
+            raise MemoryError
+        f._owned = True
+        f.expected_entries = exp.value
+        f.redundant = red.value
+        return f
+
+    def __del__(self):
+        if getattr(self, "_owned", False) and _lib is not None:
+            _lib.oracle_bf_free(ctypes.byref(self.bf))
+
+    @property
+    def m(self):
+        return self.bf.m
+
+    @property
+    def h(self):
+        return self.bf.h
+
+    @property
+    def k(self):
+        return self.bf.k
+
+    def bits(self):
+        return np.ctypeslib.as_array(self.bf.bits, shape=(self.bf.m // 8,)).copy()
+
+    def store(self, path):
+        if lib().oracle_bf_store(ctypes.byref(self.bf), path.encode()):
+            raise IOError(path)
+
+    def insert_sequence(self, seq):
+        for _, hv in kmers(seq, self.h, self.k):
+            arr = (ctypes.c_uint64 * 64)(*hv)
+            lib().oracle_bf_insert(ctypes.byref(self.bf), arr)
+
+    def contains_kmer(self, kmer):
+        for _, hv in kmers(kmer, self.h, self.k):
+            arr = (ctypes.c_uint64 * 64)(*hv)
+            return bool(lib().oracle_bf_contains(ctypes.byref(self.bf), arr, None))
+        return False
+
+
+def write_info(path, fid, k, fpr, h, expected, sources, size, num_entries, approx_fpr,
+               redundant, redundant_fpr):
+    lib().oracle_write_info(path.encode(), fid.encode(), k, fpr, h, expected, sources.encode(),
+                            size, num_entries, approx_fpr, redundant, redundant_fpr)
+
+
+def kmers(seq, h, k):
+    """(pos, hashes) of every valid k-mer, via the oracle's iterator."""
+    it = _Itr()
+    buf = ctypes.create_string_buffer(seq, len(seq))
+    lib().oracle_ntitr_init(ctypes.byref(it), buf, len(seq), h, k)
+    out = []
+    while it.pos != 2**64 - 1:
+        out.append((it.pos, list(it.hv[:max(h, 1)])))
+        lib().oracle_ntitr_next(ctypes.byref(it))
+    return out
+
+
+def pack_reads(seqs):
+    """Concatenate byte strings; returns (bytes, uint64 offsets)."""
+    off = np.zeros(len(seqs) + 1, dtype=np.uint64)
+    off[1:] = np.cumsum([len(s) for s in seqs])
+    return b"".join(seqs), off
+
+
+def classify(seq_bytes, offsets, filters, threshold=0.15, streak=3, scoring=SIMPLE,
+             count_probes=False):
+    """Per-read hit bitmasks (n x words uint64) and the algorithmic probe count."""
+    n = len(offsets) - 1
+    nf = len(filters)
+    words = (nf + 63) // 64
+    hits = np.zeros((n, words), dtype=np.uint64)
+    arr = (ctypes.POINTER(_BF) * nf)(*[ctypes.pointer(f.bf) for f in filters])
+    probes = ctypes.c_uint64(0)
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    lib().oracle_classify(seq_bytes, _u64p(off), n, arr, nf, threshold, streak, scoring,
+                          _u64p(hits), ctypes.byref(probes) if count_probes else None)
+    return hits, probes.value
+
+
+def summary_counts(hits, nf, hits2=None, inclusive=False):
+    counts = np.zeros(2 * (nf + 2) + 2, dtype=np.uint64)
+    cats = np.zeros(len(hits), dtype=np.uint32)
+    for i in range(len(hits)):
+        row = np.ascontiguousarray(hits[i])
+        if hits2 is None:
+            cats[i] = lib().oracle_update_summary(_u64p(counts), nf, _u64p(row))
+        else:
+            row2 = np.ascontiguousarray(hits2[i])
+            cats[i] = lib().oracle_update_summary_pair(_u64p(counts), nf, _u64p(row), _u64p(row2),
+                                                       int(inclusive))
+    return counts, cats
+
+
+def summary_tsv(counts, ids, read_count):
+    nf = len(ids)
+    arr = (ctypes.c_char_p * nf)(*[i.encode() for i in ids])
+    cap = 1 << 20
+    buf = ctypes.create_string_buffer(cap)
+    n = lib().oracle_summary_tsv(_u64p(np.ascontiguousarray(counts, dtype=np.uint64)), nf, arr,
+                                 read_count, buf, cap)
+    return buf.raw[:n].decode()
