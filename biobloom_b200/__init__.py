@@ -1,0 +1,11 @@
+"""biobloom_b200: BioBloom Tools' read-classification path on B200 GPUs.
+
+The product is libbbt.so (CUDA kernels for sm_100a behind the C ABI in
+include/bbt.h) and the biobloomcategorizer CLI over it; this package holds the
+Python mirror of the reference's BioBloomClassifier interface and the workload
+generators used by tests and the benchmark.
+"""
+from ._lib import BBTError, LibraryMissing, lib  # noqa: F401
+from .classifier import BioBloomClassifier, pack  # noqa: F401
+
+__all__ = ["BioBloomClassifier", "BBTError", "LibraryMissing", "lib", "pack"]

@@ -1,0 +1,117 @@
+"""ctypes binding of libbbt.so (the C ABI declared in include/bbt.h).
+
+The library is built in-tree by biobloom_b200.build_native; importing this
+module never falls back to anything else: if the library is missing or cannot
+be loaded, LibraryMissing is raised.
+"""
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libbbt.so")
+
+BBT_OK = 0
+BBT_ERR = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "CUDA", -5: "NOMEM", -6: "UNSUPPORTED",
+           -7: "TIMEOUT", -8: "NODEVICE"}
+SCORE_SIMPLE, SCORE_LENGTH = 0, 1
+HOST, DEVICE = 0, 1
+PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT = 0, 1, 2
+
+
+class LibraryMissing(RuntimeError):
+    pass
+
+
+class BBTError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"bbt error {code} ({BBT_ERR.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class Params(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_double), ("streak_threshold", ctypes.c_uint),
+                ("scoring", ctypes.c_int), ("inclusive", ctypes.c_int), ("device", ctypes.c_int),
+                ("path", ctypes.c_int), ("warps_per_block", ctypes.c_uint32),
+                ("frames_per_lane", ctypes.c_uint32), ("max_batch_bases", ctypes.c_uint64),
+                ("max_batch_reads", ctypes.c_uint64)]
+
+
+class Batch(ctypes.Structure):
+    _fields_ = [("seq", ctypes.c_void_p), ("offsets", ctypes.c_void_p), ("seq2", ctypes.c_void_p),
+                ("offsets2", ctypes.c_void_p), ("n_reads", ctypes.c_uint64),
+                ("location", ctypes.c_int)]
+
+
+class Result(ctypes.Structure):
+    _fields_ = [("hits", ctypes.c_void_p), ("hits2", ctypes.c_void_p),
+                ("category", ctypes.c_void_p), ("location", ctypes.c_int)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("reads", ctypes.c_uint64), ("frames", ctypes.c_uint64),
+                ("probes_issued", ctypes.c_uint64), ("kernel_ms", ctypes.c_double)]
+
+
+class SynthReadParams(ctypes.Structure):
+    _fields_ = [("len_min", ctypes.c_uint32), ("len_max", ctypes.c_uint32),
+                ("long_frac", ctypes.c_double), ("long_min", ctypes.c_uint32),
+                ("long_max", ctypes.c_uint32), ("sub_rate", ctypes.c_double),
+                ("n_rate", ctypes.c_double), ("frag_min", ctypes.c_uint32),
+                ("frag_max", ctypes.c_uint32)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libbbt.so (raises LibraryMissing if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise LibraryMissing(f"{LIB_PATH} is not built; run biobloom_b200.build_native.build()")
+    try:
+        L = ctypes.CDLL(LIB_PATH)
+    except OSError as e:
+        raise LibraryMissing(f"cannot load {LIB_PATH}: {e}") from e
+    P = ctypes.POINTER
+    vp, u64, i32, u32, dbl, cp = (ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint,
+                                  ctypes.c_double, ctypes.c_char_p)
+    sig = {
+        "bbt_default_params": (None, [P(Params)]),
+        "bbt_open": (i32, [P(cp), i32, P(Params), P(vp)]),
+        "bbt_close": (i32, [vp]),
+        "bbt_last_error": (cp, [vp]),
+        "bbt_num_filters": (i32, [vp]),
+        "bbt_filter_id": (cp, [vp, i32]),
+        "bbt_classify_batch": (i32, [vp, P(Batch), P(Result), vp]),
+        "bbt_sync": (i32, [vp]),
+        "bbt_summary": (i32, [vp, P(u64), P(u64)]),
+        "bbt_reset_summary": (i32, [vp]),
+        "bbt_summary_tsv": (i32, [vp, ctypes.c_char_p, ctypes.c_size_t, P(ctypes.c_size_t)]),
+        "bbt_filter_files": (i32, [vp, P(cp), i32, cp, cp]),
+        "bbt_filter_pair_files": (i32, [vp, cp, cp, cp, cp]),
+        "bbt_last_stats": (i32, [vp, P(Stats)]),
+        "bbt_set_counting": (i32, [vp, i32]),
+        "bbt_set_launch": (i32, [vp, i32, i32, i32]),
+        "bbt_set_inclusive": (i32, [vp, i32]),
+        "bbt_make_filter": (i32, [vp, P(u64), u64, u32, dbl, u32, u64, cp, cp, cp, i32]),
+        "bbt_synth_genome": (i32, [u64, u64, dbl, dbl, ctypes.c_uint32, ctypes.c_uint32, dbl, dbl,
+                                   vp]),
+        "bbt_synth_read_lengths": (i32, [u64, P(SynthReadParams), u64, vp]),
+        "bbt_synth_reads": (i32, [u64, vp, vp, ctypes.c_uint32, vp, P(SynthReadParams), u64, vp,
+                                  vp, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def check(rc, ctx=None):
+    if rc != BBT_OK:
+        msg = lib().bbt_last_error(ctx)
+        raise BBTError(rc, msg.decode() if msg else "")
+    return rc

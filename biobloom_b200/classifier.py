@@ -1,0 +1,192 @@
+"""Python mirror of BioBloomClassifier (BioBloomCategorizer/BioBloomClassifier.h:47-98)
+over the C ABI of libbbt.so.
+
+    bbc = BioBloomClassifier(["a.bf", "b.bf"], 0.15, "out")
+    bbc.filter(["reads.fq"])                 # writes out_summary.tsv
+    bbc.filterPair("r1.fq", "r2.fq")         # paired (intersection of mates)
+    hits, cats = bbc.classify([b"ACGT...", ...])  # in-memory batch
+
+Every call goes through the CUDA path; there is no CPU fallback.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def pack(seqs):
+    """Concatenate byte strings into (uint8 array, uint64 offsets)."""
+    off = np.zeros(len(seqs) + 1, dtype=np.uint64)
+    if seqs:
+        off[1:] = np.cumsum([len(s) for s in seqs])
+    buf = np.frombuffer(b"".join(seqs) or b"\0", dtype=np.uint8)
+    return buf, off
+
+
+class BioBloomClassifier:
+    def __init__(self, filter_paths, score_threshold=0.15, prefix="", postfix="", *,
+                 streak_threshold=3, device=0, path=L.PATH_AUTO, warps_per_block=0,
+                 frames_per_lane=0, max_batch_reads=0, max_batch_bases=0):
+        lib = L.lib()
+        p = L.Params()
+        lib.bbt_default_params(ctypes.byref(p))
+        p.score = float(score_threshold)
+        p.streak_threshold = int(streak_threshold)
+        p.device = int(device)
+        p.path = int(path)
+        p.warps_per_block = int(warps_per_block)
+        p.frames_per_lane = int(frames_per_lane)
+        p.max_batch_reads = int(max_batch_reads)
+        p.max_batch_bases = int(max_batch_bases)
+        # BioBloomCategorizer.cpp:423-430: an integer score > 1 is a minimum
+        # match length (LENGTH scoring)
+        if int(score_threshold) > 1:
+            p.score = float(int(score_threshold))
+            p.scoring = L.SCORE_LENGTH
+        paths = [str(x).encode() for x in filter_paths]
+        arr = (ctypes.c_char_p * len(paths))(*paths)
+        ctx = ctypes.c_void_p()
+        L.check(lib.bbt_open(arr, len(paths), ctypes.byref(p), ctypes.byref(ctx)))
+        self._ctx = ctx
+        self.params = p
+        self.prefix = prefix
+        self.postfix = postfix
+        self.n_filters = lib.bbt_num_filters(ctx)
+        self.words = (self.n_filters + 63) // 64
+        self.filter_ids = [lib.bbt_filter_id(ctx, i).decode() for i in range(self.n_filters)]
+        self._inclusive = False
+
+    # -- reference-style configuration -------------------------------------
+    def setInclusive(self):
+        """-i: a pair counts for a filter when either mate hits (union);
+        BioBloomClassifier::setInclusive (BioBloomClassifier.h:77-79)."""
+        L.check(L.lib().bbt_set_inclusive(self._ctx, 1), self._ctx)
+        self._inclusive = True
+
+    def setOrderedFilter(self):
+        raise L.BBTError(-6, "ordered filtering (-c) is not implemented on the GPU path")
+
+    def set_launch(self, path=0, warps_per_block=0, frames_per_lane=0):
+        L.check(L.lib().bbt_set_launch(self._ctx, path, warps_per_block, frames_per_lane),
+                self._ctx)
+
+    def set_counting(self, on=True):
+        L.check(L.lib().bbt_set_counting(self._ctx, int(on)), self._ctx)
+
+    # -- file pipeline (BioBloomClassifier::filter / filterPair) -----------
+    def filter(self, input_files, read_status=None):
+        files = [str(f).encode() for f in input_files]
+        arr = (ctypes.c_char_p * len(files))(*files)
+        L.check(L.lib().bbt_filter_files(self._ctx, arr, len(files), self.prefix.encode(),
+                                          read_status.encode() if read_status else None),
+                self._ctx)
+
+    def filterPair(self, file1, file2, read_status=None):
+        L.check(L.lib().bbt_filter_pair_files(self._ctx, str(file1).encode(), str(file2).encode(),
+                                              self.prefix.encode(),
+                                              read_status.encode() if read_status else None),
+                self._ctx)
+
+    # -- in-memory batches ---------------------------------------------------
+    def classify(self, reads, reads2=None):
+        """Classify host reads (list of bytes or (uint8 array, uint64 offsets)).
+        Returns (hits, hits2, category) as numpy arrays; hits2 is None for
+        single-end input."""
+        seq, off = pack(reads) if isinstance(reads, list) else reads
+        seq = np.ascontiguousarray(seq, dtype=np.uint8)
+        off = np.ascontiguousarray(off, dtype=np.uint64)
+        n = len(off) - 1
+        b = L.Batch()
+        b.seq, b.offsets, b.n_reads, b.location = _ptr(seq), _ptr(off), n, L.HOST
+        hits = np.zeros((n, self.words), dtype=np.uint64)
+        cat = np.zeros(n, dtype=np.uint32)
+        r = L.Result()
+        r.hits, r.category, r.location = _ptr(hits), _ptr(cat), L.HOST
+        hits2 = None
+        if reads2 is not None:
+            seq2, off2 = pack(reads2) if isinstance(reads2, list) else reads2
+            seq2 = np.ascontiguousarray(seq2, dtype=np.uint8)
+            off2 = np.ascontiguousarray(off2, dtype=np.uint64)
+            if len(off2) - 1 != n:
+                raise ValueError("mate arrays differ in length")
+            b.seq2, b.offsets2 = _ptr(seq2), _ptr(off2)
+            hits2 = np.zeros((n, self.words), dtype=np.uint64)
+            r.hits2 = _ptr(hits2)
+        L.check(L.lib().bbt_classify_batch(self._ctx, ctypes.byref(b), ctypes.byref(r), None),
+                self._ctx)
+        return hits, hits2, cat
+
+    def classify_device(self, seq, off, seq2=None, off2=None, hits=None, hits2=None,
+                        category=None, stream=None):
+        """Classify reads resident on the GPU (torch uint8 / int64 tensors).
+        Enqueued on `stream` (a torch.cuda.Stream, default: the current
+        stream); returns (hits, hits2, category) tensors."""
+        import torch
+        n = off.numel() - 1
+        dev = seq.device
+        if hits is None:
+            hits = torch.empty((n, self.words), dtype=torch.int64, device=dev)
+        if category is None:
+            category = torch.empty(n, dtype=torch.int32, device=dev)
+        b = L.Batch()
+        b.seq, b.offsets, b.n_reads, b.location = seq.data_ptr(), off.data_ptr(), n, L.DEVICE
+        r = L.Result()
+        r.hits, r.category, r.location = hits.data_ptr(), category.data_ptr(), L.DEVICE
+        if seq2 is not None:
+            if hits2 is None:
+                hits2 = torch.empty((n, self.words), dtype=torch.int64, device=dev)
+            b.seq2, b.offsets2 = seq2.data_ptr(), off2.data_ptr()
+            r.hits2 = hits2.data_ptr()
+        s = stream if stream is not None else torch.cuda.current_stream(dev)
+        L.check(L.lib().bbt_classify_batch(self._ctx, ctypes.byref(b), ctypes.byref(r),
+                                           ctypes.c_void_p(s.cuda_stream)), self._ctx)
+        return hits, hits2, category
+
+    def last_stats(self):
+        st = L.Stats()
+        L.check(L.lib().bbt_last_stats(self._ctx, ctypes.byref(st)), self._ctx)
+        return {"reads": st.reads, "frames": st.frames, "probes_issued": st.probes_issued,
+                "kernel_ms": st.kernel_ms}
+
+    # -- summary (ResultsManager) ---------------------------------------------
+    def summary(self):
+        counts = np.zeros(2 * (self.n_filters + 2) + 2, dtype=np.uint64)
+        reads = ctypes.c_uint64()
+        L.check(L.lib().bbt_summary(self._ctx, counts.ctypes.data_as(
+            ctypes.POINTER(ctypes.c_uint64)), ctypes.byref(reads)), self._ctx)
+        return counts, reads.value
+
+    def summary_tsv(self):
+        n = ctypes.c_size_t()
+        L.check(L.lib().bbt_summary_tsv(self._ctx, None, 0, ctypes.byref(n)), self._ctx)
+        buf = ctypes.create_string_buffer(n.value + 1)
+        L.check(L.lib().bbt_summary_tsv(self._ctx, buf, n.value + 1, ctypes.byref(n)), self._ctx)
+        return buf.value.decode()
+
+    def reset_summary(self):
+        L.check(L.lib().bbt_reset_summary(self._ctx), self._ctx)
+
+    def sync(self):
+        L.check(L.lib().bbt_sync(self._ctx), self._ctx)
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            L.lib().bbt_close(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

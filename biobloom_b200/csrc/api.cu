@@ -1,0 +1,682 @@
+/*
+ * api.cu -- the C ABI of libbbt.so (declared in include/bbt.h): contexts,
+ * filter upload, batch classification with host staging, summary counters.
+ */
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "bbt.h"
+#include "classify.cuh"
+#include "ctx.hpp"
+#include "formats.hpp"
+
+namespace bbt {
+
+static std::mutex g_err_mu;
+static std::string g_err;
+
+void set_global_error(const std::string &msg)
+{
+	std::lock_guard<std::mutex> lk(g_err_mu);
+	g_err = msg;
+}
+
+int fail(bbt_ctx *ctx, int code, const std::string &msg)
+{
+	if (ctx)
+		ctx->err = msg;
+	else
+		set_global_error(msg);
+	return code;
+}
+
+int cuda_fail(bbt_ctx *ctx, cudaError_t e, const char *what)
+{
+	std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+	return fail(ctx, e == cudaErrorMemoryAllocation ? BBT_ERR_NOMEM : BBT_ERR_CUDA, m);
+}
+
+/* ResultsManager::getResultsSummary (ResultsManager.hpp:191-237): the same
+ * rows and the default ostream number format. */
+std::string summary_text(const bbt_ctx *ctx, const std::vector<uint64_t> &c, uint64_t reads)
+{
+	const uint32_t nf = ctx->nf;
+	const uint64_t *above = c.data();
+	const uint64_t *unique = c.data() + (nf + 2);
+	const uint64_t multi = c[2 * (nf + 2)];
+	const uint64_t nomatch = c[2 * (nf + 2) + 1];
+	const double rc = (double)reads;
+	std::ostringstream o;
+	o << "filter_id\thits\tmisses\tshared\trate_hit\trate_miss\trate_shared\n";
+	for (uint32_t i = 0; i < nf; ++i) {
+		o << ctx->ids[i] << "\t" << above[i] << "\t" << reads - above[i] << "\t"
+		  << (above[i] - unique[i]) << "\t" << double(above[i]) / rc << "\t"
+		  << double(reads - above[i]) / rc << "\t" << double(above[i] - unique[i]) / rc << "\n";
+	}
+	o << "multiMatch\t" << multi << "\t" << reads - multi << "\t" << 0 << "\t"
+	  << double(multi) / rc << "\t" << double(reads - multi) / rc << "\t" << 0.0 << "\n";
+	o << "noMatch\t" << nomatch << "\t" << reads - nomatch << "\t" << 0 << "\t"
+	  << double(nomatch) / rc << "\t" << double(reads - nomatch) / rc << "\t" << 0.0 << "\n";
+	return o.str();
+}
+
+} // namespace bbt
+
+using namespace bbt;
+
+#define CUDA_TRY(ctx, call)                                                                \
+	do {                                                                                   \
+		cudaError_t e_ = (call);                                                           \
+		if (e_ != cudaSuccess)                                                             \
+			return cuda_fail((ctx), e_, #call);                                            \
+	} while (0)
+
+extern "C" void bbt_default_params(bbt_params *p)
+{
+	if (!p)
+		return;
+	memset(p, 0, sizeof(*p));
+	p->score = 0.15;           /* BioBloomCategorizer/Options.cpp:15 */
+	p->streak_threshold = 3;   /* Common/Options.cpp:9 */
+	p->scoring = BBT_SCORE_SIMPLE;
+	p->path = BBT_PATH_AUTO;
+}
+
+extern "C" const char *bbt_last_error(const bbt_ctx *ctx)
+{
+	if (ctx)
+		return ctx->err.c_str();
+	static thread_local std::string copy;
+	std::lock_guard<std::mutex> lk(g_err_mu);
+	copy = g_err;
+	return copy.c_str();
+}
+
+static void free_slot(Slot &s)
+{
+	for (int m = 0; m < 2; ++m) {
+		cudaFree(s.d_seq[m]);
+		cudaFree(s.d_off[m]);
+		cudaFree(s.d_hits[m]);
+		s.d_seq[m] = nullptr;
+		s.d_off[m] = nullptr;
+		s.d_hits[m] = nullptr;
+	}
+	cudaFree(s.d_cat);
+	s.d_cat = nullptr;
+}
+
+extern "C" int bbt_close(bbt_ctx *ctx)
+{
+	if (!ctx)
+		return BBT_OK;
+	cudaSetDevice(ctx->dev);
+	if (ctx->stream)
+		cudaStreamSynchronize(ctx->stream);
+	if (ctx->h2d)
+		cudaStreamSynchronize(ctx->h2d);
+	if (ctx->d2h)
+		cudaStreamSynchronize(ctx->d2h);
+	for (uint32_t *w : ctx->d_words)
+		cudaFree(w);
+	cudaFree(ctx->d_filters);
+	cudaFree(ctx->d_counts);
+	cudaFree(ctx->d_work);
+	cudaFree(ctx->d_stat);
+	cudaFree(ctx->d_tmp_hits[0]);
+	cudaFree(ctx->d_tmp_hits[1]);
+	for (Slot &s : ctx->slot) {
+		free_slot(s);
+		if (s.copied)
+			cudaEventDestroy(s.copied);
+		if (s.computed)
+			cudaEventDestroy(s.computed);
+		if (s.done)
+			cudaEventDestroy(s.done);
+	}
+	if (ctx->ev_start)
+		cudaEventDestroy(ctx->ev_start);
+	if (ctx->ev_stop)
+		cudaEventDestroy(ctx->ev_stop);
+	if (ctx->stream)
+		cudaStreamDestroy(ctx->stream);
+	if (ctx->h2d)
+		cudaStreamDestroy(ctx->h2d);
+	if (ctx->d2h)
+		cudaStreamDestroy(ctx->d2h);
+	delete ctx;
+	return BBT_OK;
+}
+
+/* Read one .bf payload and copy it to the device in pinned chunks. */
+static int upload_filter(bbt_ctx *ctx, const std::string &path, BfHeader &hd, uint32_t **d_out)
+{
+	FILE *f = fopen(path.c_str(), "rb");
+	if (!f)
+		return fail(ctx, BBT_ERR_IO, "file " + path + " cannot be opened");
+	const char *msg = read_bf_header(f, hd);
+	if (msg) {
+		fclose(f);
+		return fail(ctx, BBT_ERR_FORMAT, path + ": " + msg);
+	}
+	const uint64_t bytes = hd.m / 8;
+	uint32_t *d = nullptr;
+	cudaError_t e = cudaMalloc(&d, bytes);
+	if (e != cudaSuccess) {
+		fclose(f);
+		return cuda_fail(ctx, e, "cudaMalloc(filter)");
+	}
+	const size_t chunk = 64ull << 20;
+	void *pinned = nullptr;
+	e = cudaMallocHost(&pinned, std::min<uint64_t>(chunk, bytes) * 2);
+	if (e != cudaSuccess) {
+		fclose(f);
+		cudaFree(d);
+		return cuda_fail(ctx, e, "cudaMallocHost(filter staging)");
+	}
+	uint64_t done = 0;
+	int which = 0;
+	cudaEvent_t ev[2];
+	cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming);
+	cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming);
+	bool ev_used[2] = {false, false};
+	int rc = BBT_OK;
+	while (done < bytes) {
+		size_t n = (size_t)std::min<uint64_t>(chunk, bytes - done);
+		char *buf = (char *)pinned + which * std::min<uint64_t>(chunk, bytes);
+		if (ev_used[which])
+			cudaEventSynchronize(ev[which]);
+		if (fread(buf, 1, n, f) != n) {
+			rc = fail(ctx, BBT_ERR_FORMAT, path + ": filter payload is shorter than its header says");
+			break;
+		}
+		e = cudaMemcpyAsync((char *)d + done, buf, n, cudaMemcpyHostToDevice, ctx->h2d);
+		if (e != cudaSuccess) {
+			rc = cuda_fail(ctx, e, "cudaMemcpyAsync(filter)");
+			break;
+		}
+		cudaEventRecord(ev[which], ctx->h2d);
+		ev_used[which] = true;
+		done += n;
+		which ^= 1;
+	}
+	cudaStreamSynchronize(ctx->h2d);
+	cudaEventDestroy(ev[0]);
+	cudaEventDestroy(ev[1]);
+	cudaFreeHost(pinned);
+	fclose(f);
+	if (rc != BBT_OK) {
+		cudaFree(d);
+		return rc;
+	}
+	*d_out = d;
+	return BBT_OK;
+}
+
+static int alloc_slot(bbt_ctx *ctx, Slot &s, uint64_t bases, uint64_t reads)
+{
+	free_slot(s);
+	for (int m = 0; m < 2; ++m) {
+		CUDA_TRY(ctx, cudaMalloc(&s.d_seq[m], std::max<uint64_t>(bases, 16)));
+		CUDA_TRY(ctx, cudaMalloc(&s.d_off[m], (reads + 1) * sizeof(uint64_t)));
+		CUDA_TRY(ctx, cudaMalloc(&s.d_hits[m], reads * ctx->words * sizeof(uint64_t)));
+	}
+	CUDA_TRY(ctx, cudaMalloc(&s.d_cat, reads * sizeof(uint32_t)));
+	return BBT_OK;
+}
+
+static LaunchConfig pick_config(const bbt_ctx *ctx)
+{
+	LaunchConfig lc;
+	lc.path = ctx->p.path == BBT_PATH_PLAIN ? BBT_PATH_PLAIN : BBT_PATH_PERSISTENT;
+	lc.warps_per_block = ctx->p.warps_per_block ? (int)ctx->p.warps_per_block : 8;
+	lc.seg = ctx->p.frames_per_lane == 8 ? 8 : 4;
+	lc.num_sms = ctx->num_sms;
+	lc.count = 0;
+	return lc;
+}
+
+extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_params *params,
+		bbt_ctx **out)
+{
+	if (!out || !bf_paths || n_filters <= 0)
+		return fail(nullptr, BBT_ERR_ARG, "bbt_open: need at least one filter path and an out pointer");
+	*out = nullptr;
+	bbt_ctx *ctx = new bbt_ctx();
+	if (params)
+		ctx->p = *params;
+	else
+		bbt_default_params(&ctx->p);
+	if (ctx->p.score > 1 && ctx->p.scoring == BBT_SCORE_SIMPLE &&
+			(unsigned)ctx->p.score > 1) {
+		/* BioBloomCategorizer.cpp:423-430: an integer score > 1 is a
+		 * minimum match length */
+		ctx->p.score = (double)(unsigned)ctx->p.score;
+		ctx->p.scoring = BBT_SCORE_LENGTH;
+	}
+	if (ctx->p.scoring == BBT_SCORE_SIMPLE && (ctx->p.score < 0 || ctx->p.score > 1)) {
+		std::string m = "score must be in [0, 1] or an integer > 1";
+		bbt_close(ctx);
+		return fail(nullptr, BBT_ERR_ARG, m);
+	}
+	int ndev = 0;
+	cudaError_t e = cudaGetDeviceCount(&ndev);
+	if (e != cudaSuccess || ndev == 0) {
+		bbt_close(ctx);
+		return fail(nullptr, BBT_ERR_NODEVICE,
+				std::string("no CUDA device: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "0 devices"));
+	}
+	if (ctx->p.device < 0 || ctx->p.device >= ndev) {
+		bbt_close(ctx);
+		return fail(nullptr, BBT_ERR_ARG, "device ordinal out of range");
+	}
+	ctx->dev = ctx->p.device;
+	int rc = BBT_OK;
+#define OPEN_TRY(call)                                              \
+	do {                                                            \
+		cudaError_t e_ = (call);                                    \
+		if (e_ != cudaSuccess) {                                    \
+			rc = cuda_fail(ctx, e_, #call);                         \
+			goto fail_out;                                          \
+		}                                                           \
+	} while (0)
+	OPEN_TRY(cudaSetDevice(ctx->dev));
+	OPEN_TRY(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->dev));
+	OPEN_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+	OPEN_TRY(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
+	OPEN_TRY(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
+	OPEN_TRY(cudaEventCreate(&ctx->ev_start));
+	OPEN_TRY(cudaEventCreate(&ctx->ev_stop));
+	for (Slot &s : ctx->slot) {
+		OPEN_TRY(cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming));
+		OPEN_TRY(cudaEventCreateWithFlags(&s.computed, cudaEventDisableTiming));
+		OPEN_TRY(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+	}
+	for (int i = 0; i < n_filters; ++i) {
+		if (!bf_paths[i]) {
+			rc = fail(ctx, BBT_ERR_ARG, "null filter path");
+			goto fail_out;
+		}
+		std::string path = bf_paths[i];
+		std::map<std::string, std::string> kv;
+		std::string info = info_path_for(path);
+		if (!read_ini(info, kv)) {
+			rc = fail(ctx, BBT_ERR_IO, "file " + info + " cannot be opened");
+			goto fail_out;
+		}
+		auto it = kv.find("user_input_options.filter_id");
+		if (it == kv.end()) {
+			rc = fail(ctx, BBT_ERR_FORMAT, info + ": no user_input_options.filter_id");
+			goto fail_out;
+		}
+		ctx->ids.push_back(it->second);
+		BfHeader hd;
+		uint32_t *d = nullptr;
+		rc = upload_filter(ctx, path, hd, &d);
+		if (rc != BBT_OK)
+			goto fail_out;
+		ctx->d_words.push_back(d);
+		FilterDev fd;
+		fd.words = d;
+		fd.m = hd.m;
+		fd.minv = ~0ull / hd.m;
+		fd.h = hd.h;
+		fd.k = hd.k;
+		ctx->hf.push_back(fd);
+		ctx->kmax = std::max(ctx->kmax, hd.k);
+	}
+	ctx->nf = (uint32_t)n_filters;
+	ctx->words = (ctx->nf + 63) / 64;
+	OPEN_TRY(cudaMalloc(&ctx->d_filters, sizeof(FilterDev) * ctx->nf));
+	OPEN_TRY(cudaMemcpy(ctx->d_filters, ctx->hf.data(), sizeof(FilterDev) * ctx->nf,
+			cudaMemcpyHostToDevice));
+	OPEN_TRY(cudaMalloc(&ctx->d_counts, sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
+	OPEN_TRY(cudaMemset(ctx->d_counts, 0, sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
+	OPEN_TRY(cudaMalloc(&ctx->d_work, sizeof(unsigned long long)));
+	OPEN_TRY(cudaMalloc(&ctx->d_stat, 2 * sizeof(unsigned long long)));
+	ctx->cap_reads = ctx->p.max_batch_reads ? ctx->p.max_batch_reads : (1ull << 20);
+	ctx->cap_bases = ctx->p.max_batch_bases ? ctx->p.max_batch_bases : (256ull << 20);
+	for (Slot &s : ctx->slot) {
+		rc = alloc_slot(ctx, s, ctx->cap_bases, ctx->cap_reads);
+		if (rc != BBT_OK)
+			goto fail_out;
+	}
+	ctx->lc = pick_config(ctx);
+	*out = ctx;
+	return BBT_OK;
+fail_out : {
+	std::string m = ctx->err;
+	bbt_close(ctx);
+	return fail(nullptr, rc, m);
+}
+#undef OPEN_TRY
+}
+
+extern "C" int bbt_num_filters(const bbt_ctx *ctx)
+{
+	return ctx ? (int)ctx->nf : BBT_ERR_ARG;
+}
+
+extern "C" const char *bbt_filter_id(const bbt_ctx *ctx, int i)
+{
+	if (!ctx || i < 0 || (uint32_t)i >= ctx->nf)
+		return nullptr;
+	return ctx->ids[i].c_str();
+}
+
+static ClassifyArgs base_args(const bbt_ctx *ctx)
+{
+	ClassifyArgs a;
+	memset(&a, 0, sizeof a);
+	a.filters = ctx->d_filters;
+	a.nf = ctx->nf;
+	a.words = ctx->words;
+	a.score = ctx->p.score;
+	a.one_minus = 1.0 - ctx->p.score;
+	a.streak_thr = ctx->p.streak_threshold;
+	a.scoring = ctx->p.scoring;
+	a.min_len = (unsigned)std::round(ctx->p.score);
+	a.kmax = ctx->kmax;
+	a.work = ctx->d_work;
+	if (ctx->lc.count) {
+		a.probes = ctx->d_stat;
+		a.frames = ctx->d_stat + 1;
+	}
+	return a;
+}
+
+/* classify + summarize one staged or device-resident batch on stream s */
+static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStream_t s)
+{
+	if (ctx->lc.path == BBT_PATH_PERSISTENT)
+		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), s));
+	CUDA_TRY(ctx, launch_classify(a, ctx->lc, s));
+	CUDA_TRY(ctx, launch_summarize(a.hits[0], a.mates == 2 ? a.hits[1] : nullptr, a.n, ctx->nf,
+			ctx->words, ctx->p.inclusive, d_cat, ctx->d_counts, ctx->num_sms, s));
+	return BBT_OK;
+}
+
+static int ensure_tmp_hits(bbt_ctx *ctx, uint64_t n)
+{
+	if (n <= ctx->tmp_hits_cap)
+		return BBT_OK;
+	cudaFree(ctx->d_tmp_hits[0]);
+	cudaFree(ctx->d_tmp_hits[1]);
+	ctx->d_tmp_hits[0] = ctx->d_tmp_hits[1] = nullptr;
+	ctx->tmp_hits_cap = 0;
+	CUDA_TRY(ctx, cudaMalloc(&ctx->d_tmp_hits[0], n * ctx->words * sizeof(uint64_t)));
+	CUDA_TRY(ctx, cudaMalloc(&ctx->d_tmp_hits[1], n * ctx->words * sizeof(uint64_t)));
+	ctx->tmp_hits_cap = n;
+	return BBT_OK;
+}
+
+static int classify_device(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r, cudaStream_t s)
+{
+	const bool paired = b->seq2 != nullptr;
+	ClassifyArgs a = base_args(ctx);
+	a.seq[0] = (const uint8_t *)b->seq;
+	a.off[0] = b->offsets;
+	a.seq[1] = (const uint8_t *)(paired ? b->seq2 : b->seq);
+	a.off[1] = paired ? b->offsets2 : b->offsets;
+	a.n = b->n_reads;
+	a.mates = paired ? 2 : 1;
+	if (!r->hits || (paired && !r->hits2)) {
+		int rc = ensure_tmp_hits(ctx, b->n_reads);
+		if (rc)
+			return rc;
+	}
+	a.hits[0] = r->hits ? r->hits : ctx->d_tmp_hits[0];
+	a.hits[1] = paired ? (r->hits2 ? r->hits2 : ctx->d_tmp_hits[1]) : nullptr;
+	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, s));
+	int rc = run_kernels(ctx, a, r->category, s);
+	if (rc)
+		return rc;
+	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, s));
+	ctx->reads_seen += b->n_reads;
+	ctx->last.reads = b->n_reads * a.mates;
+	return BBT_OK;
+}
+
+/* Host batches: split into sub-batches that fit the staging slots; copies in
+ * (h2d stream), kernels (ctx->stream) and copies out (d2h stream) of
+ * consecutive sub-batches overlap, two slots deep. */
+static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r)
+{
+	const bool paired = b->seq2 != nullptr;
+	const uint64_t n = b->n_reads;
+	uint64_t i0 = 0;
+	int which = 0;
+	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
+	while (i0 < n) {
+		/* largest i1 with bases and reads inside the slot capacity */
+		uint64_t i1 = std::min(n, i0 + ctx->cap_reads);
+		auto bases = [&](uint64_t lo, uint64_t hi) {
+			uint64_t x = b->offsets[hi] - b->offsets[lo];
+			if (paired)
+				x = std::max(x, b->offsets2[hi] - b->offsets2[lo]);
+			return x;
+		};
+		if (bases(i0, i1) > ctx->cap_bases) {
+			uint64_t lo = i0 + 1, hi = i1;
+			while (lo < hi) {
+				uint64_t mid = (lo + hi + 1) / 2;
+				if (bases(i0, mid) <= ctx->cap_bases)
+					lo = mid;
+				else
+					hi = mid - 1;
+			}
+			i1 = lo;
+			if (bases(i0, i1) > ctx->cap_bases) {
+				/* one read longer than the staging area: grow both slots */
+				for (Slot &s : ctx->slot) {
+					if (s.used)
+						CUDA_TRY(ctx, cudaEventSynchronize(s.done));
+					s.used = false;
+				}
+				uint64_t need = bases(i0, i1);
+				for (Slot &s : ctx->slot) {
+					int rc = alloc_slot(ctx, s, need, ctx->cap_reads);
+					if (rc)
+						return rc;
+				}
+				ctx->cap_bases = need;
+			}
+		}
+		Slot &s = ctx->slot[which];
+		if (s.used)
+			CUDA_TRY(ctx, cudaEventSynchronize(s.done));
+		const uint64_t cnt = i1 - i0;
+		ClassifyArgs a = base_args(ctx);
+		a.n = cnt;
+		a.mates = paired ? 2 : 1;
+		for (int m = 0; m < (paired ? 2 : 1); ++m) {
+			const char *seq = m ? b->seq2 : b->seq;
+			const uint64_t *off = m ? b->offsets2 : b->offsets;
+			const uint64_t lo = off[i0], hi = off[i1];
+			if (hi > lo)
+				CUDA_TRY(ctx, cudaMemcpyAsync(s.d_seq[m], seq + lo, hi - lo,
+						cudaMemcpyHostToDevice, ctx->h2d));
+			CUDA_TRY(ctx, cudaMemcpyAsync(s.d_off[m], off + i0, (cnt + 1) * sizeof(uint64_t),
+					cudaMemcpyHostToDevice, ctx->h2d));
+			a.seq[m] = s.d_seq[m];
+			a.off[m] = s.d_off[m];
+			a.off_base[m] = lo;
+			a.hits[m] = s.d_hits[m];
+		}
+		if (!paired) {
+			a.seq[1] = a.seq[0];
+			a.off[1] = a.off[0];
+			a.off_base[1] = a.off_base[0];
+			a.hits[1] = nullptr;
+		}
+		CUDA_TRY(ctx, cudaEventRecord(s.copied, ctx->h2d));
+		CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, s.copied, 0));
+		int rc = run_kernels(ctx, a, s.d_cat, ctx->stream);
+		if (rc)
+			return rc;
+		CUDA_TRY(ctx, cudaEventRecord(s.computed, ctx->stream));
+		CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->d2h, s.computed, 0));
+		const size_t hb = cnt * ctx->words * sizeof(uint64_t);
+		if (r->hits)
+			CUDA_TRY(ctx, cudaMemcpyAsync(r->hits + i0 * ctx->words, s.d_hits[0], hb,
+					cudaMemcpyDeviceToHost, ctx->d2h));
+		if (paired && r->hits2)
+			CUDA_TRY(ctx, cudaMemcpyAsync(r->hits2 + i0 * ctx->words, s.d_hits[1], hb,
+					cudaMemcpyDeviceToHost, ctx->d2h));
+		if (r->category)
+			CUDA_TRY(ctx, cudaMemcpyAsync(r->category + i0, s.d_cat, cnt * sizeof(uint32_t),
+					cudaMemcpyDeviceToHost, ctx->d2h));
+		CUDA_TRY(ctx, cudaEventRecord(s.done, ctx->d2h));
+		s.used = true;
+		which ^= 1;
+		i0 = i1;
+	}
+	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
+	CUDA_TRY(ctx, cudaStreamSynchronize(ctx->d2h));
+	CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+	for (Slot &s : ctx->slot)
+		s.used = false;
+	ctx->reads_seen += n;
+	ctx->last.reads = n * (paired ? 2 : 1);
+	return BBT_OK;
+}
+
+extern "C" int bbt_classify_batch(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *result,
+		void *stream)
+{
+	if (!ctx || !batch || !result)
+		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch: null argument");
+	if (batch->n_reads == 0)
+		return BBT_OK;
+	if (!batch->seq || !batch->offsets || (batch->seq2 && !batch->offsets2))
+		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch: missing sequence or offsets");
+	if (batch->location != result->location)
+		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch: batch and result must both be host or both device");
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	if (batch->location == BBT_DEVICE) {
+		cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+		return classify_device(ctx, batch, result, s);
+	}
+	if (batch->location != BBT_HOST)
+		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch: location must be BBT_HOST or BBT_DEVICE");
+	return classify_host(ctx, batch, result);
+}
+
+extern "C" int bbt_sync(bbt_ctx *ctx)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	CUDA_TRY(ctx, cudaDeviceSynchronize());
+	return BBT_OK;
+}
+
+extern "C" int bbt_summary(bbt_ctx *ctx, uint64_t *counts, uint64_t *reads)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	CUDA_TRY(ctx, cudaDeviceSynchronize());
+	if (counts)
+		CUDA_TRY(ctx, cudaMemcpy(counts, ctx->d_counts,
+				sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2), cudaMemcpyDeviceToHost));
+	if (reads)
+		*reads = ctx->reads_seen;
+	return BBT_OK;
+}
+
+extern "C" int bbt_reset_summary(bbt_ctx *ctx)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	CUDA_TRY(ctx, cudaDeviceSynchronize());
+	CUDA_TRY(ctx, cudaMemset(ctx->d_counts, 0,
+			sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
+	ctx->reads_seen = 0;
+	return BBT_OK;
+}
+
+extern "C" int bbt_summary_tsv(bbt_ctx *ctx, char *buf, size_t cap, size_t *len)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	std::vector<uint64_t> c(2 * (ctx->nf + 2) + 2);
+	uint64_t reads = 0;
+	int rc = bbt_summary(ctx, c.data(), &reads);
+	if (rc)
+		return rc;
+	std::string t = summary_text(ctx, c, reads);
+	if (len)
+		*len = t.size();
+	if (buf && cap) {
+		size_t n = std::min(cap - 1, t.size());
+		memcpy(buf, t.data(), n);
+		buf[n] = 0;
+	}
+	return BBT_OK;
+}
+
+extern "C" int bbt_last_stats(bbt_ctx *ctx, bbt_stats *out)
+{
+	if (!ctx || !out)
+		return BBT_ERR_ARG;
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	CUDA_TRY(ctx, cudaEventSynchronize(ctx->ev_stop));
+	float ms = 0;
+	CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+	ctx->last.kernel_ms = ms;
+	if (ctx->lc.count) {
+		unsigned long long st[2];
+		CUDA_TRY(ctx, cudaMemcpy(st, ctx->d_stat, sizeof st, cudaMemcpyDeviceToHost));
+		ctx->last.probes_issued = st[0];
+		ctx->last.frames = st[1];
+	}
+	*out = ctx->last;
+	return BBT_OK;
+}
+
+extern "C" int bbt_set_inclusive(bbt_ctx *ctx, int inclusive)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	ctx->p.inclusive = inclusive ? 1 : 0;
+	return BBT_OK;
+}
+
+/* Turn on probe/frame counting (diagnostics; adds atomics). */
+extern "C" int bbt_set_counting(bbt_ctx *ctx, int on)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	ctx->lc.count = on ? 1 : 0;
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	CUDA_TRY(ctx, cudaMemset(ctx->d_stat, 0, 2 * sizeof(unsigned long long)));
+	return BBT_OK;
+}
+
+/* Change kernel path / launch shape after open (autotuner, bench). */
+extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int seg)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	if (path != 0)
+		ctx->p.path = path;
+	if (warps_per_block)
+		ctx->p.warps_per_block = (uint32_t)warps_per_block;
+	if (seg)
+		ctx->p.frames_per_lane = (uint32_t)seg;
+	int cnt = ctx->lc.count;
+	ctx->lc = pick_config(ctx);
+	ctx->lc.count = cnt;
+	return BBT_OK;
+}

@@ -1,0 +1,128 @@
+/*
+ * bbt_device.cuh -- device building blocks of the classification path:
+ * ntHash over ASCII bases, the derived extra hashes, hash -> bit reduction and
+ * the Bloom bit probe.
+ *
+ * ntHash follows the published method (Mohamadi et al., Bioinformatics 2016),
+ * which the reference uses through the btl_bloomfilter submodule
+ * (Common/SeqEval.h:50): each base has a 64-bit seed, the forward hash of
+ * s[0..k) is XOR_i rol(seed(s_i), k-1-i), the reverse-complement hash is
+ * XOR_i rol(seed(comp(s_i)), i), the canonical hash is the smaller of the two,
+ * and extra hash i (i >= 1) is canon * (i ^ (k * M)) followed by x ^= x >> 27.
+ * Both strand hashes are built here in Horner form (one rotate-by-one per base)
+ * and then rolled one base at a time.
+ *
+ * Filter layout in device memory: bit j of a filter is bit (j % 32) of 32-bit
+ * word j / 32 (little-endian, so byte j / 8 bit j % 8 of the .bf payload).
+ * A hash value v maps to bit v mod m.
+ */
+#ifndef BBT_DEVICE_CUH
+#define BBT_DEVICE_CUH
+
+#include <stdint.h>
+
+namespace bbt {
+
+constexpr uint64_t kSeedA = 0x3c8bfbb395c60474ULL;
+constexpr uint64_t kSeedC = 0x3193c18562a02b4cULL;
+constexpr uint64_t kSeedG = 0x20323ed082572324ULL;
+constexpr uint64_t kSeedT = 0x295549f54be24456ULL;
+constexpr uint64_t kMultiSeed = 0x90b45d39fb6da1faULL;
+constexpr unsigned kMultiShift = 27;
+
+/* One filter as the kernels see it. */
+struct FilterDev {
+	const uint32_t *words; /* m / 32 words */
+	uint64_t m;            /* bits (a multiple of 64) */
+	uint64_t minv;         /* floor((2^64 - 1) / m), for the reduction */
+	uint32_t h;            /* hash functions */
+	uint32_t k;            /* k-mer size */
+};
+
+#if defined(__CUDACC__)
+
+__device__ __forceinline__ uint64_t rol1(uint64_t v)
+{
+	return (v << 1) | (v >> 63);
+}
+
+__device__ __forceinline__ uint64_t ror1(uint64_t v)
+{
+	return (v >> 1) | (v << 63);
+}
+
+__device__ __forceinline__ uint64_t rolk(uint64_t v, unsigned s)
+{
+	s &= 63u;
+	return s ? (v << s) | (v >> (64u - s)) : v;
+}
+
+/* Forward seed of an ASCII base, 0 for a base that is not ACGT/acgt. */
+__device__ __forceinline__ uint64_t seed_fw(uint8_t c)
+{
+	uint8_t u = c & 0xDF; /* upper case */
+	return u == 'A' ? kSeedA : u == 'C' ? kSeedC : u == 'G' ? kSeedG
+	     : u == 'T' ? kSeedT : 0ull;
+}
+
+/* Seed of the complementary base. */
+__device__ __forceinline__ uint64_t seed_rc(uint8_t c)
+{
+	uint8_t u = c & 0xDF;
+	return u == 'A' ? kSeedT : u == 'C' ? kSeedG : u == 'G' ? kSeedC
+	     : u == 'T' ? kSeedA : 0ull;
+}
+
+__device__ __forceinline__ bool base_ok(uint8_t c)
+{
+	uint8_t u = c & 0xDF;
+	return u == 'A' || u == 'C' || u == 'G' || u == 'T';
+}
+
+__device__ __forceinline__ uint64_t extra_hash(uint64_t canon, unsigned k, unsigned i)
+{
+	uint64_t t = canon * ((uint64_t)i ^ ((uint64_t)k * kMultiSeed));
+	return t ^ (t >> kMultiShift);
+}
+
+/* v mod m by Barrett reduction with minv = floor((2^64-1)/m): the estimate is
+ * at most two below the true quotient. */
+__device__ __forceinline__ uint64_t reduce(uint64_t v, uint64_t m, uint64_t minv)
+{
+	uint64_t q = __umul64hi(v, minv);
+	uint64_t r = v - q * m;
+	if (r >= m)
+		r -= m;
+	if (r >= m)
+		r -= m;
+	return r;
+}
+
+__device__ __forceinline__ bool test_bit(const uint32_t *__restrict__ words, uint64_t b)
+{
+	uint32_t w = __ldg(words + (b >> 5));
+	return (w >> (b & 31u)) & 1u;
+}
+
+/* BloomFilter::contains: all h bits set, reading them in order and stopping at
+ * the first clear one.  *reads counts the words read. */
+__device__ __forceinline__ bool contains(const FilterDev &f, uint64_t canon, unsigned &reads)
+{
+	if (!test_bit(f.words, reduce(canon, f.m, f.minv))) {
+		++reads;
+		return false;
+	}
+	++reads;
+	for (unsigned i = 1; i < f.h; ++i) {
+		++reads;
+		if (!test_bit(f.words, reduce(extra_hash(canon, f.k, i), f.m, f.minv)))
+			return false;
+	}
+	return true;
+}
+
+#endif /* __CUDACC__ */
+
+} // namespace bbt
+
+#endif

@@ -1,0 +1,335 @@
+/*
+ * classify.cu -- the read-classification kernels.
+ *
+ * One warp classifies one read at a time against every filter, replacing the
+ * per-read body of BioBloomClassifier::filter (BioBloomClassifier.cpp:59-89):
+ * evaluateReadStd (BioBloomClassifier.cpp:1182-1189) calls SeqEval::evalRead
+ * (Common/SeqEval.h:493-524) once per filter, which walks the read's k-mers
+ * with ntHashIterator and probes the filter (BloomFilter::contains).
+ *
+ * Per read the warp
+ *   1. stages a window of up to 32*SEG frames: the bases go to shared memory
+ *      and each lane hashes SEG consecutive frames (one Horner pass over k
+ *      bases, then rolling), writing the canonical hash and a validity flag
+ *      per frame to shared memory; windows are cached across filters with the
+ *      same k;
+ *   2. for each filter, walks the window 32 frames at a time: each lane probes
+ *      one frame (h bit tests, stopping at the first clear bit, exactly as
+ *      BloomFilter::contains), the warp ballots the hit bits and runs the
+ *      SeqEval state machine over the chunk (seqeval_chunk.cuh); the filter is
+ *      done when the state machine accepts or rejects.
+ * Frames inside a skip window are not probed; frames after an accept/reject
+ * inside the last chunk are probed speculatively (they change the bytes read,
+ * never the result).
+ *
+ * Two launch shapes: PLAIN gives each warp one read (one launch per batch);
+ * PERSISTENT keeps one resident grid whose warps take reads from a global
+ * counter until the batch is done, which balances reads of very different
+ * lengths.
+ */
+#include "classify.cuh"
+#include "seqeval_chunk.cuh"
+
+#include "bbt.h"
+
+namespace bbt {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+/* Per-warp shared-memory window. */
+template <int SEG>
+struct Window {
+	static constexpr int W = 32 * SEG;
+	uint64_t *roll;   /* [8]: rol(seed_fw(A,C,G,T), k), rol(seed_rc(A,C,G,T), k-1) */
+	uint64_t *h0;     /* canonical hash of frame q (window-relative) */
+	uint8_t *vld;     /* 1 if frame q holds only ACGT */
+	uint8_t *bases;   /* bases [w0, w0 + wn + k - 1) */
+};
+
+template <int SEG>
+__device__ __forceinline__ size_t window_stride(uint32_t kmax)
+{
+	size_t b = 64 + (size_t)Window<SEG>::W * 9 + Window<SEG>::W + kmax;
+	return (b + 15) & ~(size_t)15;
+}
+
+/* Per-k constants of the rolling update (lanes 0-7 write one each). */
+template <int SEG>
+__device__ __forceinline__ void set_roll(const Window<SEG> &win, unsigned k, int lane)
+{
+	if (lane < 8) {
+		const uint64_t seeds[4] = {kSeedA, kSeedC, kSeedG, kSeedT};
+		win.roll[lane] = lane < 4 ? rolk(seeds[lane], k) : rolk(seeds[7 - lane], k - 1);
+	}
+	__syncwarp();
+}
+
+__device__ __forceinline__ int base_code(uint8_t c)
+{
+	uint8_t u = c & 0xDF;
+	return u == 'A' ? 0 : u == 'C' ? 1 : u == 'G' ? 2 : u == 'T' ? 3 : -1;
+}
+
+/* Hash frames [w0, w0 + wn) of the read at s (len bases) into the window. */
+template <int SEG>
+__device__ void hash_window(const uint8_t *__restrict__ s, uint64_t w0, int wn, unsigned k,
+		const Window<SEG> &win, int lane)
+{
+	const int nb = wn + (int)k - 1;
+	for (int b = lane; b < nb; b += 32)
+		win.bases[b] = s[w0 + b];
+	__syncwarp();
+	const int S = (wn + 31) >> 5; /* frames per lane in this window */
+	const int q0 = lane * S;
+	if (q0 < wn) {
+		const uint8_t *bb = win.bases + q0;
+		uint64_t fh = 0, rh = 0;
+		int lb = -1; /* last invalid base, window-relative */
+		for (unsigned i = 0; i < k; ++i) {
+			uint8_t c = bb[i];
+			fh = rol1(fh) ^ seed_fw(c);
+			if (!base_ok(c))
+				lb = q0 + (int)i;
+		}
+		for (int i = (int)k - 1; i >= 0; --i)
+			rh = rol1(rh) ^ seed_rc(bb[i]);
+		win.h0[q0] = fh < rh ? fh : rh;
+		win.vld[q0] = lb < q0;
+		const int qe = min(q0 + S, wn);
+		for (int q = q0 + 1; q < qe; ++q) {
+			uint8_t out = win.bases[q - 1], in = win.bases[q + k - 1];
+			const int co = base_code(out), ci = base_code(in);
+			fh = rol1(fh) ^ (co >= 0 ? win.roll[co] : 0ull) ^ seed_fw(in);
+			rh = ror1(rh) ^ ror1(seed_rc(out)) ^ (ci >= 0 ? win.roll[4 + ci] : 0ull);
+			if (!base_ok(in))
+				lb = q + (int)k - 1;
+			win.h0[q] = fh < rh ? fh : rh;
+			win.vld[q] = lb < q;
+		}
+	}
+	__syncwarp();
+}
+
+template <int SEG, bool COUNT, bool LENGTH_MODE>
+__device__ void classify_read(const ClassifyArgs &a, uint64_t r, const Window<SEG> &win,
+		int lane, unsigned long long &probe_acc, unsigned long long &frame_acc)
+{
+	constexpr int W = Window<SEG>::W;
+	const uint32_t mate = r >= a.n ? 1u : 0u;
+	const uint64_t i = r - (mate ? a.n : 0);
+	const uint64_t *off = a.off[mate];
+	const uint64_t start = off[i] - a.off_base[mate];
+	const uint64_t len = off[i + 1] - off[i];
+	const uint8_t *s = a.seq[mate] + start;
+	uint64_t myword = 0;
+	unsigned cached_k = 0;
+	int64_t cached_w0 = -1;
+	unsigned reads = 0;
+	for (uint32_t f = 0; f < a.nf; ++f) {
+		const FilterDev F = a.filters[f];
+		const unsigned k = F.k;
+		if (len < k)
+			continue;
+		const uint64_t frames = len - k + 1;
+		SimpleState st;
+		LengthState ls;
+		constexpr bool length_mode = LENGTH_MODE;
+		if (length_mode)
+			length_init(ls, a.min_len, len, (int)k);
+		else
+			simple_init(st, a.score, a.one_minus, frames);
+		int decided = EVAL_OPEN;
+		for (uint64_t w0 = 0; w0 < frames && !decided; w0 += W) {
+			const int wn = (int)min((uint64_t)W, frames - w0);
+			if (cached_k != k || cached_w0 != (int64_t)w0) {
+				if (cached_k != k)
+					set_roll<SEG>(win, k, lane);
+				hash_window<SEG>(s, w0, wn, k, win, lane);
+				cached_k = k;
+				cached_w0 = (int64_t)w0;
+				if (COUNT)
+					frame_acc += (lane == 0) ? (unsigned long long)wn : 0ull;
+			}
+			for (int c = 0; c < wn; c += 32) {
+				const int q = c + lane;
+				const int64_t p = (int64_t)w0 + q;
+				const bool v = q < wn && win.vld[q];
+				const bool probe = v && (length_mode || p >= st.skip_until);
+				const bool hit = probe && contains(F, win.h0[q], reads);
+				const uint32_t V = __ballot_sync(kFull, v);
+				const uint32_t H = __ballot_sync(kFull, hit);
+				const int nfc = min(32, wn - c);
+				decided = length_mode
+						? length_chunk(ls, V, H, (int64_t)w0 + c, nfc)
+						: simple_chunk(st, V, H, (int32_t)w0 + c, nfc, (int)k, (int)a.streak_thr);
+				if (decided)
+					break;
+			}
+		}
+		if (decided == EVAL_ACCEPT && lane == (int)(f >> 6))
+			myword |= 1ull << (f & 63);
+	}
+	if (lane < (int)a.words)
+		a.hits[mate][i * a.words + lane] = myword;
+	if (COUNT)
+		probe_acc += reads;
+}
+
+template <int SEG, bool PERSISTENT, bool COUNT, bool LENGTH_MODE>
+__global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
+{
+	extern __shared__ __align__(16) unsigned char smem[];
+	const int lane = threadIdx.x & 31;
+	const int warp = threadIdx.x >> 5;
+	const size_t stride = window_stride<SEG>(a.kmax);
+	Window<SEG> win;
+	win.roll = reinterpret_cast<uint64_t *>(smem + warp * stride);
+	win.h0 = win.roll + 8;
+	win.vld = reinterpret_cast<uint8_t *>(win.h0 + Window<SEG>::W);
+	win.bases = win.vld + Window<SEG>::W;
+	const uint64_t total = a.n * a.mates;
+	unsigned long long probe_acc = 0, frame_acc = 0;
+	if (PERSISTENT) {
+		for (;;) {
+			unsigned long long r = 0;
+			if (lane == 0)
+				r = atomicAdd(a.work, 1ull);
+			r = __shfl_sync(kFull, r, 0);
+			if (r >= total)
+				break;
+			classify_read<SEG, COUNT, LENGTH_MODE>(a, r, win, lane, probe_acc, frame_acc);
+		}
+	} else {
+		const uint64_t r = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp;
+		if (r < total)
+			classify_read<SEG, COUNT, LENGTH_MODE>(a, r, win, lane, probe_acc, frame_acc);
+	}
+	if (COUNT) {
+		for (int o = 16; o; o >>= 1) {
+			probe_acc += __shfl_xor_sync(kFull, probe_acc, o);
+			frame_acc += __shfl_xor_sync(kFull, frame_acc, o);
+		}
+		if (lane == 0) {
+			if (a.probes)
+				atomicAdd(a.probes, probe_acc);
+			if (a.frames)
+				atomicAdd(a.frames, frame_acc);
+		}
+	}
+}
+
+/* ResultsManager::updateSummaryData (ResultsManager.hpp:66-189) over a batch:
+ * the category of each read (pair) and block-aggregated counter updates. */
+__global__ void summarize_kernel(const uint64_t *__restrict__ h1, const uint64_t *__restrict__ h2,
+		uint64_t n, uint32_t nf, uint32_t words, int inclusive, uint32_t *category,
+		unsigned long long *counts)
+{
+	extern __shared__ unsigned long long sc[];
+	const uint32_t ncount = 2 * (nf + 2) + 2;
+	for (uint32_t j = threadIdx.x; j < ncount; j += blockDim.x)
+		sc[j] = 0;
+	__syncthreads();
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+			i += (uint64_t)gridDim.x * blockDim.x) {
+		uint32_t idx = nf;
+		for (uint32_t w = 0; w < words; ++w) {
+			uint64_t x = h1[i * words + w];
+			if (h2)
+				x = inclusive ? (x | h2[i * words + w]) : (x & h2[i * words + w]);
+			while (x) {
+				uint32_t f = w * 64 + (uint32_t)(__ffsll((long long)x) - 1);
+				x &= x - 1;
+				atomicAdd(&sc[f], 1ull);
+				idx = idx == nf ? f : nf + 1;
+			}
+		}
+		if (idx == nf)
+			atomicAdd(&sc[2 * (nf + 2) + 1], 1ull);
+		else if (idx == nf + 1)
+			atomicAdd(&sc[2 * (nf + 2)], 1ull);
+		else
+			atomicAdd(&sc[(nf + 2) + idx], 1ull);
+		if (category)
+			category[i] = idx;
+	}
+	__syncthreads();
+	for (uint32_t j = threadIdx.x; j < ncount; j += blockDim.x)
+		if (sc[j])
+			atomicAdd(&counts[j], sc[j]);
+}
+
+template <int SEG, bool P, bool C>
+cudaError_t launch_one(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
+{
+	const int threads = lc.warps_per_block * 32;
+	const size_t smem = classify_smem_bytes(lc, a.kmax);
+	auto kern = a.scoring == BBT_SCORE_LENGTH ? classify_kernel<SEG, P, C, true>
+	                                          : classify_kernel<SEG, P, C, false>;
+	cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)smem);
+	if (e != cudaSuccess)
+		return e;
+	uint64_t total = a.n * a.mates;
+	unsigned blocks;
+	if (P) {
+		int per_sm = 0;
+		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+		if (e != cudaSuccess)
+			return e;
+		if (per_sm < 1)
+			per_sm = 1;
+		uint64_t need = (total + lc.warps_per_block - 1) / lc.warps_per_block;
+		uint64_t full = (uint64_t)per_sm * lc.num_sms;
+		blocks = (unsigned)(need < full ? need : full);
+	} else {
+		blocks = (unsigned)((total + lc.warps_per_block - 1) / lc.warps_per_block);
+	}
+	if (blocks == 0)
+		return cudaSuccess;
+	kern<<<blocks, threads, smem, s>>>(a);
+	return cudaGetLastError();
+}
+
+} // namespace
+
+size_t classify_smem_bytes(const LaunchConfig &lc, uint32_t kmax)
+{
+	size_t W = 32 * (size_t)lc.seg;
+	size_t b = 64 + W * 9 + W + kmax;
+	b = (b + 15) & ~(size_t)15;
+	return b * (size_t)lc.warps_per_block;
+}
+
+cudaError_t launch_classify(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
+{
+	const bool P = lc.path == BBT_PATH_PERSISTENT;
+	const bool C = lc.count != 0;
+	if (lc.seg == 8) {
+		if (P)
+			return C ? launch_one<8, true, true>(a, lc, s) : launch_one<8, true, false>(a, lc, s);
+		return C ? launch_one<8, false, true>(a, lc, s) : launch_one<8, false, false>(a, lc, s);
+	}
+	if (P)
+		return C ? launch_one<4, true, true>(a, lc, s) : launch_one<4, true, false>(a, lc, s);
+	return C ? launch_one<4, false, true>(a, lc, s) : launch_one<4, false, false>(a, lc, s);
+}
+
+cudaError_t launch_summarize(const uint64_t *h1, const uint64_t *h2, uint64_t n, uint32_t nf,
+		uint32_t words, int inclusive, uint32_t *category, unsigned long long *counts,
+		int num_sms, cudaStream_t s)
+{
+	if (n == 0)
+		return cudaSuccess;
+	const int threads = 256;
+	uint64_t need = (n + threads - 1) / threads;
+	uint64_t cap = (uint64_t)num_sms * 4;
+	unsigned blocks = (unsigned)(need < cap ? need : cap);
+	size_t smem = sizeof(unsigned long long) * (2 * (nf + 2) + 2);
+	summarize_kernel<<<blocks, threads, smem, s>>>(h1, h2, n, nf, words, inclusive, category,
+			counts);
+	return cudaGetLastError();
+}
+
+} // namespace bbt

@@ -1,0 +1,58 @@
+/*
+ * classify.cuh -- launch interface of the classification kernels
+ * (classify.cu), used by the C ABI layer (api.cu).
+ */
+#ifndef BBT_CLASSIFY_CUH
+#define BBT_CLASSIFY_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "bbt_device.cuh"
+
+namespace bbt {
+
+/* Everything one classify launch needs.  Reads r in [0, n * mates): r < n is
+ * read r of mate array 0, otherwise read r - n of mate array 1. */
+struct ClassifyArgs {
+	const uint8_t *seq[2];
+	const uint64_t *off[2];
+	uint64_t off_base[2];      /* subtracted from offsets (staged batches) */
+	uint64_t n;                /* reads per mate array */
+	uint32_t mates;            /* 1 or 2 */
+	const FilterDev *filters;  /* device array of nf filters */
+	uint32_t nf;
+	uint32_t words;            /* (nf + 63) / 64 */
+	double score;              /* SIMPLE threshold */
+	double one_minus;          /* 1.0 - score, computed on the host */
+	uint32_t streak_thr;
+	int scoring;               /* BBT_SCORE_* */
+	uint32_t min_len;          /* LENGTH: (unsigned) round(score) */
+	uint32_t kmax;             /* largest k among the filters */
+	uint64_t *hits[2];         /* n x words per mate array */
+	unsigned long long *work;  /* persistent: next read to take (zeroed) */
+	unsigned long long *probes;/* optional: filter words read */
+	unsigned long long *frames;/* optional: frames hashed */
+};
+
+struct LaunchConfig {
+	int path;             /* BBT_PATH_PLAIN or BBT_PATH_PERSISTENT */
+	int warps_per_block;  /* 4 or 8 */
+	int seg;              /* frames per lane when hashing: 4 or 8 */
+	int num_sms;
+	int count;            /* gather probe / frame counters */
+};
+
+/* Dynamic shared memory one block needs. */
+size_t classify_smem_bytes(const LaunchConfig &lc, uint32_t kmax);
+cudaError_t launch_classify(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s);
+
+/* Categories and summary counters for n reads (or pairs when h2 != NULL):
+ * counts = aboveThreshold[nf+2], unique[nf+2], multiMatch, noMatch. */
+cudaError_t launch_summarize(const uint64_t *h1, const uint64_t *h2, uint64_t n, uint32_t nf,
+		uint32_t words, int inclusive, uint32_t *category, unsigned long long *counts,
+		int num_sms, cudaStream_t s);
+
+} // namespace bbt
+
+#endif

@@ -1,0 +1,236 @@
+/*
+ * cli_categorizer.cpp -- biobloomcategorizer on the B200 path.
+ *
+ * Same flags as the reference CLI (BioBloomCategorizer/BioBloomCategorizer.cpp:
+ * 171-205); the score conversion (integer > 1 selects LENGTH scoring,
+ * :416-441), the filter existence check (:444-452) and the mode dispatch
+ * (:458-532) follow it.  Output: "<prefix>_summary.tsv" and, with
+ * --read_status FILE, one "<read>\t<category>" line per read (pair).
+ * Options whose outputs this build does not produce yet (--fa/--fq, -d, -n,
+ * -b, -w, -c, -S, -D, -l, single-file paired input) are refused with a message
+ * instead of being ignored.
+ */
+#include <getopt.h>
+#include <sys/stat.h>
+
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "bbt.h"
+
+using namespace std;
+
+static void usage_exit(int code)
+{
+	cerr << "Usage: biobloomcategorizer [OPTION]... -f \"[FILTER1]...\" [FILE]...\n"
+	        "biobloomcategorizer [OPTION]... -e -f \"[FILTER1]...\" [FILE1.fq] [FILE2.fq]\n"
+	        "Categorize Sequences. The input format may be FASTA, FASTQ, and compressed gz.\n"
+	        "\n"
+	        "  -p, --prefix=N         Output prefix to use. Otherwise will output to current\n"
+	        "                         directory.\n"
+	        "  -f, --filter_files=N   List of filter files to use. Required option.\n"
+	        "  -e, --paired_mode      Uses paired-end information.\n"
+	        "  -i, --inclusive        If one paired read matches, both reads will be included\n"
+	        "                         in the filter.\n"
+	        "  -s, --score=N          Score threshold for matching: a floating point score\n"
+	        "                         between 0 and 1, or a positive integer minimum match\n"
+	        "                         length in bases. [0.15]\n"
+	        "  -t, --threads=N        Accepted for compatibility (work runs on the GPU).\n"
+	        "  -r, --streak=N         Hits tiling in second pass needed to jump several tiles\n"
+	        "                         upon a miss. [3]\n"
+	        "  -I, --interval         Accepted for compatibility.\n"
+	        "      --read_status=F    Write one '<read>\\t<category>' line per read to F.\n"
+	        "      --device=N         CUDA device ordinal. [0]\n"
+	        "  -v, --version          Display version information.\n"
+	        "  -h, --help             Display this dialog.\n";
+	exit(code);
+}
+
+static vector<string> split_ws(const string &s)
+{
+	vector<string> out;
+	stringstream in(s);
+	string t;
+	while (in >> t)
+		out.push_back(t);
+	return out;
+}
+
+static bool fexists(const string &p)
+{
+	ifstream f(p.c_str());
+	return f.good();
+}
+
+int main(int argc, char **argv)
+{
+	bbt_params p;
+	bbt_default_params(&p);
+	string filters, prefix, read_status;
+	bool paired = false, die = false;
+	int fastq = 0, fasta = 0, verbose = 0;
+	int device = 0;
+	string unsupported;
+	enum { OPT_READ_STATUS = 1000, OPT_DEVICE };
+	static struct option long_options[] = {
+		{"prefix", required_argument, NULL, 'p'},
+		{"filter_files", required_argument, NULL, 'f'},
+		{"paired_mode", no_argument, NULL, 'e'},
+		{"inclusive", no_argument, NULL, 'i'},
+		{"score", required_argument, NULL, 's'},
+		{"help", no_argument, NULL, 'h'},
+		{"interval", required_argument, NULL, 'I'},
+		{"threads", required_argument, NULL, 't'},
+		{"gz_output", no_argument, NULL, 'g'},
+		{"fq", no_argument, &fastq, 1},
+		{"fa", no_argument, &fasta, 1},
+		{"file_list", required_argument, NULL, 'l'},
+		{"version", no_argument, NULL, 'v'},
+		{"multi", required_argument, NULL, 'm'},
+		{"streak", required_argument, NULL, 'r'},
+		{"min_hit_only", no_argument, NULL, 'o'},
+		{"ordered", no_argument, NULL, 'c'},
+		{"stdout_filter", no_argument, NULL, 'd'},
+		{"inverse", no_argument, NULL, 'n'},
+		{"best_hit", no_argument, NULL, 'b'},
+		{"with_score", no_argument, NULL, 'w'},
+		{"score_type", required_argument, NULL, 'S'},
+		{"verbose", no_argument, &verbose, 1},
+		{"dust", no_argument, NULL, 'D'},
+		{"T_dust", required_argument, NULL, 'T'},
+		{"window_dust", required_argument, NULL, 'W'},
+		{"read_status", required_argument, NULL, OPT_READ_STATUS},
+		{"device", required_argument, NULL, OPT_DEVICE},
+		{NULL, 0, NULL, 0}};
+	int c, idx = 0;
+	while ((c = getopt_long(argc, argv, "f:p:hegl:vs:r:t:cdiwI:nm:S:bDT:W:", long_options,
+			&idx)) != -1) {
+		switch (c) {
+		case 's': {
+			stringstream conv(optarg);
+			conv >> p.score;
+			break;
+		}
+		case 'f': filters = optarg; break;
+		case 'p': prefix = optarg; break;
+		case 'h': usage_exit(EXIT_SUCCESS); break;
+		case 'e': paired = true; break;
+		case 'i': p.inclusive = 1; break;
+		case 'I': case 't': case 'm': break;
+		case 'r': {
+			stringstream conv(optarg);
+			if (!(conv >> p.streak_threshold)) {
+				cerr << "Error - Invalid parameter! r: " << optarg << endl;
+				exit(EXIT_FAILURE);
+			}
+			break;
+		}
+		case 'v':
+			cerr << "biobloomcategorizer (bbt-b200) 2.3.4-compatible\n" << endl;
+			exit(EXIT_SUCCESS);
+		case 'g': case 'l': case 'c': case 'd': case 'n': case 'b': case 'w': case 'S':
+		case 'D': case 'T': case 'W': case 'o':
+			unsupported += string(" -") + (char)c;
+			break;
+		case OPT_READ_STATUS: read_status = optarg; break;
+		case OPT_DEVICE: device = atoi(optarg); break;
+		case '?': die = true; break;
+		default: break;
+		}
+	}
+	if (fasta || fastq)
+		unsupported += fasta ? " --fa" : " --fq";
+	vector<string> files;
+	while (optind < argc)
+		files.push_back(argv[optind++]);
+	vector<string> paths = split_ws(filters);
+	if (paired && files.size() != 2) {
+		if (files.size() == 1)
+			unsupported += " (single-file paired input)";
+		else {
+			cerr << "Usage of paired end mode:\n"
+			        "biobloomcategorizer [OPTION]... -f \"[FILTER1]...\" [FILEPAIR1] [FILEPAIR2]\n"
+			     << endl;
+			die = true;
+		}
+	}
+	if (files.empty()) {
+		cerr << "Error: Need Input File" << endl;
+		die = true;
+	}
+	if (paths.empty()) {
+		cerr << "Error: Need Filter File (-f)" << endl;
+		die = true;
+	}
+	if (die) {
+		cerr << "Try '--help' for more information.\n";
+		exit(EXIT_FAILURE);
+	}
+	if (!unsupported.empty()) {
+		cerr << "Error: option(s)" << unsupported << " are not supported by this build" << endl;
+		exit(EXIT_FAILURE);
+	}
+	if (p.score < 0) {
+		cerr << "Error - s must be a positive integer or a floating point between 0 and 1."
+		     << endl;
+		exit(EXIT_FAILURE);
+	}
+	unsigned match_len = (unsigned)p.score;
+	if (match_len > 1) {
+		p.score = match_len;
+		p.scoring = BBT_SCORE_LENGTH;
+		cerr << "Min match length threshold: " << match_len << " bp" << endl;
+	} else {
+		cerr << "Min score threshold: " << p.score << endl;
+	}
+	if (prefix.find('/') != string::npos) {
+		struct stat sb;
+		string dir = prefix.substr(0, prefix.find_last_of('/'));
+		if (stat(dir.c_str(), &sb) != 0 || !S_ISDIR(sb.st_mode)) {
+			cerr << "Error: Output folder does not exist. " << dir << endl;
+			exit(1);
+		}
+	}
+	for (const string &f : paths) {
+		if (!fexists(f)) {
+			cerr << "Error: " + f + " File cannot be opened" << endl;
+			exit(EXIT_FAILURE);
+		}
+	}
+	p.device = device;
+	vector<const char *> cp;
+	for (const string &f : paths)
+		cp.push_back(f.c_str());
+	cerr << "Starting to Load Filters." << endl;
+	bbt_ctx *ctx = nullptr;
+	if (bbt_open(cp.data(), (int)cp.size(), &p, &ctx) != BBT_OK) {
+		cerr << "Error: " << bbt_last_error(nullptr) << endl;
+		exit(1);
+	}
+	for (int i = 0; i < bbt_num_filters(ctx); ++i)
+		cerr << "Loaded Filter: " << bbt_filter_id(ctx, i) << endl;
+	cerr << "Filter Loading Complete." << endl;
+	int rc;
+	const char *rs = read_status.empty() ? nullptr : read_status.c_str();
+	if (paired) {
+		rc = bbt_filter_pair_files(ctx, files[0].c_str(), files[1].c_str(), prefix.c_str(), rs);
+	} else {
+		vector<const char *> fp;
+		for (const string &f : files)
+			fp.push_back(f.c_str());
+		rc = bbt_filter_files(ctx, fp.data(), (int)fp.size(), prefix.c_str(), rs);
+	}
+	if (rc != BBT_OK) {
+		cerr << "Error: " << bbt_last_error(ctx) << endl;
+		bbt_close(ctx);
+		exit(1);
+	}
+	bbt_close(ctx);
+	return 0;
+}

@@ -1,0 +1,65 @@
+/*
+ * ctx.hpp -- the classification context behind the C ABI (bbt_ctx).
+ */
+#ifndef BBT_CTX_HPP
+#define BBT_CTX_HPP
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "bbt.h"
+#include "classify.cuh"
+
+namespace bbt {
+
+/* One staging slot for host batches (inputs in, results out). */
+struct Slot {
+	uint8_t *d_seq[2] = {nullptr, nullptr};
+	uint64_t *d_off[2] = {nullptr, nullptr};
+	uint64_t *d_hits[2] = {nullptr, nullptr};
+	uint32_t *d_cat = nullptr;
+	cudaEvent_t copied = nullptr;   /* inputs are on the device */
+	cudaEvent_t computed = nullptr; /* kernels done */
+	cudaEvent_t done = nullptr;     /* results are back on the host */
+	bool used = false;
+};
+
+void set_global_error(const std::string &msg);
+
+} // namespace bbt
+
+struct bbt_ctx {
+	std::string err;
+	bbt_params p;
+	int dev = 0;
+	int num_sms = 0;
+	cudaStream_t stream = nullptr;  /* kernels */
+	cudaStream_t h2d = nullptr;     /* host -> device copies */
+	cudaStream_t d2h = nullptr;     /* device -> host copies */
+	std::vector<std::string> ids;
+	std::vector<bbt::FilterDev> hf;
+	std::vector<uint32_t *> d_words;
+	bbt::FilterDev *d_filters = nullptr;
+	uint32_t nf = 0, words = 0, kmax = 0;
+	unsigned long long *d_counts = nullptr; /* 2*(nf+2)+2 summary counters */
+	unsigned long long *d_work = nullptr;   /* persistent-kernel read counter */
+	unsigned long long *d_stat = nullptr;   /* probes, frames */
+	uint64_t reads_seen = 0;
+	bbt::Slot slot[2];
+	uint64_t cap_bases = 0, cap_reads = 0;
+	uint64_t *d_tmp_hits[2] = {nullptr, nullptr};
+	uint64_t tmp_hits_cap = 0;
+	cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+	bbt::LaunchConfig lc;
+	bbt_stats last = {0, 0, 0, 0.0};
+};
+
+namespace bbt {
+int fail(bbt_ctx *ctx, int code, const std::string &msg);
+int cuda_fail(bbt_ctx *ctx, cudaError_t e, const char *what);
+std::string summary_text(const bbt_ctx *ctx, const std::vector<uint64_t> &counts, uint64_t reads);
+}
+
+#endif

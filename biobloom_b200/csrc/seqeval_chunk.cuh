@@ -96,17 +96,21 @@ enum { EVAL_OPEN = 0, EVAL_ACCEPT = 1, EVAL_REJECT = 2 };
  * is antiScore and "antiThres <= antiScore" is "anti >= anti_thres".
  */
 struct SimpleState {
-	int64_t score2;
-	int64_t anti;
-	int64_t thres2;
-	int64_t anti_thres;
+	int32_t score2;
+	int32_t anti;
+	int32_t thres2;
+	int32_t anti_thres;
 	int32_t streak;       /* hits in the current streak (saturates at 64) */
 	int32_t started;      /* a valid frame has been visited */
-	int64_t skip_until;   /* frames below this belong to a skip window */
+	int32_t skip_until;   /* frames below this belong to a skip window */
 	int32_t in_window;    /* a skip window is open (frames < skip_until) */
 	int32_t pending;      /* invalid window frames after its last valid one */
 	int32_t decided;      /* EVAL_* */
 };
+
+/* Reads are limited to this many frames so that every counter of the state
+ * machine (at most twice the frame count) fits in 32 bits. */
+constexpr uint64_t kMaxFrames = (1ull << 30) - 1;
 
 /*
  * Thresholds exactly as SeqEval.h:41-45 computes them:
@@ -135,8 +139,8 @@ BBT_HD void simple_init(SimpleState &s, double threshold, double one_minus,
 		fa -= 1.0; /* floor for negative values */
 	s.score2 = 0;
 	s.anti = 0;
-	s.thres2 = (int64_t)c;
-	s.anti_thres = (int64_t)fa;
+	s.thres2 = (int32_t)c;       /* at most 2 * kMaxFrames */
+	s.anti_thres = fa < -1.0 ? -1 : (int32_t)fa;
 	s.streak = 0;
 	s.started = 0;
 	s.skip_until = 0;
@@ -154,7 +158,7 @@ BBT_HD void simple_init(SimpleState &s, double threshold, double one_minus,
  * Frames below s.skip_until are inside a skip window: their H bits are never
  * read, so the caller need not probe them.  Returns s.decided.
  */
-BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int64_t base,
+BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int32_t base,
 		int nf, int k, int streak_thr)
 {
 	if (s.decided)
@@ -166,7 +170,7 @@ BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int64_t base,
 	while (j < nf) {
 		/* ---- skip-window frames ---- */
 		if (s.in_window) {
-			int64_t we = s.skip_until - base;
+			int32_t we = s.skip_until - base;
 			int e = we >= nf ? nf : (int)we;
 			if (e > j) {
 				uint32_t r = range_mask(j, e);
@@ -263,11 +267,11 @@ BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int64_t base,
 		const uint32_t hp = Hr & pre;
 		const uint32_t hp2 = prevhit & pre;
 		const uint32_t ap = (Mr | Cr) & pre;
-		const int64_t dS = popc32(hp) + popc32(hp2);
-		const int64_t dA = popc32(ap);
+		const int32_t dS = popc32(hp) + popc32(hp2);
+		const int32_t dA = popc32(ap);
 		int acc_pos = 32, rej_pos = 32;
 		if (s.score2 + dS >= s.thres2) {
-			int64_t sc = s.score2;
+			int32_t sc = s.score2;
 			uint32_t x = hp;
 			while (x) {
 				int q = lowbit32(x);
@@ -280,7 +284,7 @@ BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int64_t base,
 			}
 		}
 		if (s.anti + dA >= s.anti_thres) {
-			int64_t need = s.anti_thres - s.anti;
+			int32_t need = s.anti_thres - s.anti;
 			rej_pos = need <= 0 ? (ap ? lowbit32(ap) : 32)
 			                    : nth_bit(ap, (int)need);
 		}

@@ -1,0 +1,227 @@
+/*
+ * bbt.h -- C ABI of the B200 read-classification library (libbbt.so).
+ *
+ * This is the drop-in boundary for BioBloom Tools' classification path.  The
+ * reference has no FFI: its boundary is the BioBloomClassifier class and the
+ * biobloomcategorizer CLI.  Each entry point below names the reference
+ * interface it replaces (paths are relative to the biobloom project).
+ *
+ * Conventions
+ *   - Every function returns an int status: BBT_OK (0) or a negative BBT_ERR_*.
+ *     The text of the last error is available from bbt_last_error(ctx) (or
+ *     bbt_last_error(NULL) for errors raised before a context exists).  The
+ *     reference prints and exit(1)s instead (e.g. BioBloomClassifier.cpp:54-57).
+ *   - The caller owns every host buffer; a context owns its device memory.
+ *   - A context is used from one host thread at a time.
+ *   - Streams are passed as void* (a cudaStream_t, or NULL for the context's
+ *     own stream).
+ *   - Sequences are ASCII bases; A, C, G, T in either case are valid bases,
+ *     every other byte ends the k-mers that cover it, as ntHashIterator does.
+ */
+#ifndef BBT_H
+#define BBT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define BBT_OK 0
+#define BBT_ERR_ARG (-1)          /* invalid argument */
+#define BBT_ERR_IO (-2)           /* file cannot be opened / read / written */
+#define BBT_ERR_FORMAT (-3)       /* malformed .bf / .txt / FASTA / FASTQ */
+#define BBT_ERR_CUDA (-4)         /* CUDA runtime error */
+#define BBT_ERR_NOMEM (-5)        /* host or device allocation failed */
+#define BBT_ERR_UNSUPPORTED (-6)  /* option combination not implemented */
+#define BBT_ERR_TIMEOUT (-7)      /* a bounded device wait gave up */
+#define BBT_ERR_NODEVICE (-8)     /* no CUDA device is usable */
+
+/* ---- scoring methods (opt::ScoringMethod, Common/Options.h:75) ---- */
+#define BBT_SCORE_SIMPLE 0
+#define BBT_SCORE_LENGTH 1
+
+/* ---- where batch buffers live ---- */
+#define BBT_HOST 0
+#define BBT_DEVICE 1
+
+/* ---- kernel paths ---- */
+#define BBT_PATH_AUTO 0        /* persistent work-stealing path, tuned */
+#define BBT_PATH_PLAIN 1       /* one warp per read, one launch per batch */
+#define BBT_PATH_PERSISTENT 2  /* persistent work-stealing kernel */
+
+typedef struct bbt_ctx bbt_ctx;
+
+/*
+ * Classification parameters.  Mirrors the options the reference reads from
+ * opt:: inside BioBloomClassifier (BioBloomCategorizer/Options.cpp:14-36,
+ * Common/Options.cpp:7-9) plus the device-side knobs of this library.
+ */
+typedef struct {
+	double score;               /* -s: threshold in [0,1], or an integer > 1 for
+	                               LENGTH scoring (BioBloomCategorizer.cpp:416-441) */
+	unsigned streak_threshold;  /* -r (Common/Options.cpp:9), default 3 */
+	int scoring;                /* BBT_SCORE_*; set from score by bbt_default_params
+	                               semantics when score > 1 */
+	int inclusive;              /* -i (BioBloomClassifier.h:77-79) */
+	int device;                 /* CUDA device ordinal */
+	int path;                   /* BBT_PATH_* */
+	uint32_t warps_per_block;   /* 0 = tuned */
+	uint32_t frames_per_lane;   /* probe chains in flight per lane (1, 2 or 4); 0 = tuned */
+	uint64_t max_batch_bases;   /* device staging capacity per batch (bases); 0 = default */
+	uint64_t max_batch_reads;   /* device staging capacity per batch (reads); 0 = default */
+} bbt_params;
+
+/* Fill p with the reference's defaults (score 0.15, streak 3, SIMPLE). */
+void bbt_default_params(bbt_params *p);
+
+/*
+ * Load filters and upload them to device memory once.
+ * Replaces BioBloomClassifier::BioBloomClassifier / loadFilters
+ * (BioBloomClassifier.cpp:21-28, 950-971): for each "<x>.bf" the sidecar
+ * "<x>.txt" (same stem) supplies the filter id.
+ */
+int bbt_open(const char *const *bf_paths, int n_filters, const bbt_params *params,
+		bbt_ctx **out);
+int bbt_close(bbt_ctx *ctx);
+const char *bbt_last_error(const bbt_ctx *ctx);
+
+int bbt_num_filters(const bbt_ctx *ctx);
+/* Filter id of filter i (BloomFilterInfo::getFilterID, BloomFilterInfo.cpp:141). */
+const char *bbt_filter_id(const bbt_ctx *ctx, int i);
+
+/*
+ * A batch of reads.  Single-end: seq/offsets hold n_reads reads
+ * (read i = seq[offsets[i] .. offsets[i+1])).  Paired: seq2/offsets2 hold the
+ * mates, read i of seq pairs with read i of seq2, and n_reads counts pairs.
+ */
+typedef struct {
+	const char *seq;
+	const uint64_t *offsets;   /* n_reads + 1 entries, offsets[0] may be > 0 */
+	const char *seq2;          /* NULL for single-end */
+	const uint64_t *offsets2;
+	uint64_t n_reads;
+	int location;              /* BBT_HOST or BBT_DEVICE for all four arrays */
+} bbt_batch;
+
+/*
+ * Per-read results.  hits/hits2 (optional): words = (n_filters + 63) / 64
+ * uint64 per read, bit f set when SeqEval accepted the read for filter f
+ * (evaluateReadStd, BioBloomClassifier.cpp:1182-1189).  category (optional):
+ * per read (or pair) the index ResultsManager::updateSummaryData returns
+ * (ResultsManager.hpp:66-189): the filter index for a unique hit, n_filters for
+ * noMatch, n_filters + 1 for multiMatch.
+ */
+typedef struct {
+	uint64_t *hits;
+	uint64_t *hits2;
+	uint32_t *category;
+	int location;              /* BBT_HOST or BBT_DEVICE */
+} bbt_result;
+
+/*
+ * Classify one batch and add it to the context's summary counters.
+ * Replaces the per-read loop of BioBloomClassifier::filter / filterPair
+ * (BioBloomClassifier.cpp:33-100, 217-303).  With BBT_HOST buffers the call
+ * copies inputs in and results out and returns when they are in place; with
+ * BBT_DEVICE buffers it enqueues on `stream` and returns (results are ready
+ * when the stream reaches that point).
+ */
+int bbt_classify_batch(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *result,
+		void *stream);
+
+/* Wait for all work the context enqueued. */
+int bbt_sync(bbt_ctx *ctx);
+
+/*
+ * Summary counters (ResultsManager.hpp:250-261): counts must hold
+ * 2 * (n_filters + 2) + 2 uint64: aboveThreshold[n_filters + 2],
+ * unique[n_filters + 2], multiMatch, noMatch; *reads = reads (or pairs) seen.
+ */
+int bbt_summary(bbt_ctx *ctx, uint64_t *counts, uint64_t *reads);
+int bbt_reset_summary(bbt_ctx *ctx);
+/* summary.tsv text (ResultsManager::getResultsSummary, ResultsManager.hpp:191-237).
+ * Writes at most cap bytes including the NUL; *len receives the full length. */
+int bbt_summary_tsv(bbt_ctx *ctx, char *buf, size_t cap, size_t *len);
+
+/*
+ * File pipeline: parse FASTA/FASTQ (gzip or plain) into pinned, double-
+ * buffered batches, classify, and write "<prefix>_summary.tsv" and, if
+ * read_status is non-NULL, a per-read "<name>\t<category>" file.
+ * Replaces BioBloomClassifier::filter (BioBloomClassifier.cpp:33-100) and
+ * filterPair(file1, file2) (BioBloomClassifier.cpp:217-303).
+ */
+int bbt_filter_files(bbt_ctx *ctx, const char *const *files, int n_files,
+		const char *prefix, const char *read_status);
+int bbt_filter_pair_files(bbt_ctx *ctx, const char *file1, const char *file2,
+		const char *prefix, const char *read_status);
+
+/* Pairs count for a filter when either mate hits (-i; union of the mates' hit
+ * lists) instead of both (intersection, the default).
+ * Replaces BioBloomClassifier::setInclusive (BioBloomClassifier.h:77-79). */
+int bbt_set_inclusive(bbt_ctx *ctx, int inclusive);
+
+/* Kernel path and launch shape (BBT_PATH_*, warps per block 4 or 8, frames
+ * per lane when hashing 4 or 8); 0 keeps the current value.  Used by the
+ * tuner; no reference counterpart (the reference's only knob is -t threads,
+ * BioBloomCategorizer.cpp:243-249). */
+int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int frames_per_lane);
+
+/* Count filter words read and frames hashed in the following batches
+ * (diagnostics; costs atomics).  No reference counterpart. */
+int bbt_set_counting(bbt_ctx *ctx, int on);
+
+/* Counters of the last classified batch: probes issued by the device. */
+typedef struct {
+	uint64_t reads;
+	uint64_t frames;
+	uint64_t probes_issued;     /* filter words read by the kernel */
+	double kernel_ms;           /* classify kernel time of the last batch */
+} bbt_stats;
+int bbt_last_stats(bbt_ctx *ctx, bbt_stats *out);
+
+/*
+ * Build a Bloom filter on the device and write "<stem>.bf" and "<stem>.txt".
+ * Replaces BloomFilterGenerator::generate + BloomFilterInfo sizing
+ * (BioBloomMaker/BloomFilterGenerator.cpp:54-73, BloomFilterGenerator.h:108-188,
+ * Common/BloomFilterInfo.h:57-76, BioBloomMaker.cpp:360-373,427-543).
+ * Sequences (host memory) are seq[offsets[i] .. offsets[i+1]); hash_num 0
+ * picks calcOptimalHashNum(fpr).  entries 0 = sum of (len - k + 1).
+ */
+int bbt_make_filter(const char *seq, const uint64_t *offsets, uint64_t n_seqs,
+		unsigned k, double fpr, unsigned hash_num, uint64_t entries,
+		const char *stem, const char *filter_id, const char *sources, int device);
+
+/* ---- synthetic workloads (host only; no GPU needed) ---- */
+
+typedef struct {
+	uint32_t len_min, len_max;    /* log-uniform length range (equal = fixed) */
+	double long_frac;             /* fraction of long reads */
+	uint32_t long_min, long_max;  /* log-uniform range of long reads */
+	double sub_rate;              /* substitution rate */
+	double n_rate;                /* rate of N bases */
+	uint32_t frag_min, frag_max;  /* paired: fragment length range */
+} bbt_synth_read_params;
+
+/* Random genome: uniform bases at GC fraction gc, then repeat families. */
+int bbt_synth_genome(uint64_t seed, uint64_t len, double gc, double repeat_frac,
+		uint32_t rep_min, uint32_t rep_max, double div_min, double div_max,
+		char *out);
+/* Read lengths: out_off[0..n_reads] (prefix sums). */
+int bbt_synth_read_lengths(uint64_t seed, const bbt_synth_read_params *p,
+		uint64_t n_reads, uint64_t *out_off);
+/* Reads drawn from references (ref_frac[j] of reads from reference j, the rest
+ * uniform random), filled at the offsets from bbt_synth_read_lengths.  Paired
+ * when out2 is non-NULL.  out_src (optional) receives the source index
+ * (n_refs = random). */
+int bbt_synth_reads(uint64_t seed, const char *refs, const uint64_t *ref_off,
+		uint32_t n_refs, const double *ref_frac, const bbt_synth_read_params *p,
+		uint64_t n_reads, const uint64_t *off, char *out1, char *out2,
+		uint32_t *out_src);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
