@@ -15,7 +15,7 @@ BBT_ERR = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "CUDA", -5: "NOMEM", -6: "UNSU
            -7: "TIMEOUT", -8: "NODEVICE"}
 SCORE_SIMPLE, SCORE_LENGTH = 0, 1
 HOST, DEVICE = 0, 1
-PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT = 0, 1, 2
+PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT, PATH_FILTER_MAJOR = 0, 1, 2, 3
 
 
 class LibraryMissing(RuntimeError):
@@ -33,7 +33,7 @@ class Params(ctypes.Structure):
                 ("scoring", ctypes.c_int), ("inclusive", ctypes.c_int), ("device", ctypes.c_int),
                 ("path", ctypes.c_int), ("warps_per_block", ctypes.c_uint32),
                 ("frames_per_lane", ctypes.c_uint32), ("max_batch_bases", ctypes.c_uint64),
-                ("max_batch_reads", ctypes.c_uint64)]
+                ("max_batch_reads", ctypes.c_uint64), ("l2_fetch_bytes", ctypes.c_uint32)]
 
 
 class Batch(ctypes.Structure):
@@ -49,7 +49,8 @@ class Result(ctypes.Structure):
 
 class Stats(ctypes.Structure):
     _fields_ = [("reads", ctypes.c_uint64), ("frames", ctypes.c_uint64),
-                ("probes_issued", ctypes.c_uint64), ("kernel_ms", ctypes.c_double)]
+                ("probes_issued", ctypes.c_uint64), ("probes_algorithmic", ctypes.c_uint64),
+                ("kernel_ms", ctypes.c_double), ("classify_ms", ctypes.c_double)]
 
 
 class SynthReadParams(ctypes.Structure):

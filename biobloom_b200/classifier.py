@@ -31,7 +31,7 @@ def pack(seqs):
 class BioBloomClassifier:
     def __init__(self, filter_paths, score_threshold=0.15, prefix="", postfix="", *,
                  streak_threshold=3, device=0, path=L.PATH_AUTO, warps_per_block=0,
-                 frames_per_lane=0, max_batch_reads=0, max_batch_bases=0):
+                 frames_per_lane=0, max_batch_reads=0, max_batch_bases=0, l2_fetch_bytes=0):
         lib = L.lib()
         p = L.Params()
         lib.bbt_default_params(ctypes.byref(p))
@@ -43,6 +43,7 @@ class BioBloomClassifier:
         p.frames_per_lane = int(frames_per_lane)
         p.max_batch_reads = int(max_batch_reads)
         p.max_batch_bases = int(max_batch_bases)
+        p.l2_fetch_bytes = int(l2_fetch_bytes)
         # BioBloomCategorizer.cpp:423-430: an integer score > 1 is a minimum
         # match length (LENGTH scoring)
         if int(score_threshold) > 1:
@@ -151,7 +152,8 @@ class BioBloomClassifier:
         st = L.Stats()
         L.check(L.lib().bbt_last_stats(self._ctx, ctypes.byref(st)), self._ctx)
         return {"reads": st.reads, "frames": st.frames, "probes_issued": st.probes_issued,
-                "kernel_ms": st.kernel_ms}
+                "probes_algorithmic": st.probes_algorithmic, "kernel_ms": st.kernel_ms,
+                "classify_ms": st.classify_ms}
 
     # -- summary (ResultsManager) ---------------------------------------------
     def summary(self):

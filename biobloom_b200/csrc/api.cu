@@ -147,6 +147,10 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 		cudaEventDestroy(ctx->ev_start);
 	if (ctx->ev_stop)
 		cudaEventDestroy(ctx->ev_stop);
+	if (ctx->ev_k0)
+		cudaEventDestroy(ctx->ev_k0);
+	if (ctx->ev_k1)
+		cudaEventDestroy(ctx->ev_k1);
 	if (ctx->stream)
 		cudaStreamDestroy(ctx->stream);
 	if (ctx->h2d)
@@ -237,7 +241,7 @@ static int alloc_slot(bbt_ctx *ctx, Slot &s, uint64_t bases, uint64_t reads)
 static LaunchConfig pick_config(const bbt_ctx *ctx)
 {
 	LaunchConfig lc;
-	lc.path = ctx->p.path == BBT_PATH_PLAIN ? BBT_PATH_PLAIN : BBT_PATH_PERSISTENT;
+	lc.path = ctx->p.path == BBT_PATH_AUTO ? BBT_PATH_PERSISTENT : ctx->p.path;
 	lc.warps_per_block = ctx->p.warps_per_block ? (int)ctx->p.warps_per_block : 8;
 	lc.seg = ctx->p.frames_per_lane == 8 ? 8 : 4;
 	lc.num_sms = ctx->num_sms;
@@ -291,11 +295,18 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 	} while (0)
 	OPEN_TRY(cudaSetDevice(ctx->dev));
 	OPEN_TRY(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->dev));
+	/* Bloom probes are isolated 4-byte reads at random addresses: fetching
+	 * more than the 32-byte sector per L2 miss only moves bytes nobody reads.
+	 * The limit belongs to this process's context and ends with it. */
+	OPEN_TRY(cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity,
+			ctx->p.l2_fetch_bytes ? ctx->p.l2_fetch_bytes : 32));
 	OPEN_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
 	OPEN_TRY(cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
 	OPEN_TRY(cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
 	OPEN_TRY(cudaEventCreate(&ctx->ev_start));
 	OPEN_TRY(cudaEventCreate(&ctx->ev_stop));
+	OPEN_TRY(cudaEventCreate(&ctx->ev_k0));
+	OPEN_TRY(cudaEventCreate(&ctx->ev_k1));
 	for (Slot &s : ctx->slot) {
 		OPEN_TRY(cudaEventCreateWithFlags(&s.copied, cudaEventDisableTiming));
 		OPEN_TRY(cudaEventCreateWithFlags(&s.computed, cudaEventDisableTiming));
@@ -342,7 +353,8 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 	OPEN_TRY(cudaMalloc(&ctx->d_counts, sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
 	OPEN_TRY(cudaMemset(ctx->d_counts, 0, sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
 	OPEN_TRY(cudaMalloc(&ctx->d_work, sizeof(unsigned long long)));
-	OPEN_TRY(cudaMalloc(&ctx->d_stat, 2 * sizeof(unsigned long long)));
+	OPEN_TRY(cudaMalloc(&ctx->d_stat, 3 * sizeof(unsigned long long)));
+	OPEN_TRY(cudaMemset(ctx->d_stat, 0, 3 * sizeof(unsigned long long)));
 	ctx->cap_reads = ctx->p.max_batch_reads ? ctx->p.max_batch_reads : (1ull << 20);
 	ctx->cap_bases = ctx->p.max_batch_bases ? ctx->p.max_batch_bases : (256ull << 20);
 	for (Slot &s : ctx->slot) {
@@ -390,6 +402,7 @@ static ClassifyArgs base_args(const bbt_ctx *ctx)
 	if (ctx->lc.count) {
 		a.probes = ctx->d_stat;
 		a.frames = ctx->d_stat + 1;
+		a.alg_probes = ctx->d_stat + 2;
 	}
 	return a;
 }
@@ -397,9 +410,18 @@ static ClassifyArgs base_args(const bbt_ctx *ctx)
 /* classify + summarize one staged or device-resident batch on stream s */
 static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStream_t s)
 {
-	if (ctx->lc.path == BBT_PATH_PERSISTENT)
+	if (ctx->lc.path != BBT_PATH_PLAIN)
 		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), s));
+	if (ctx->lc.path == BBT_PATH_FILTER_MAJOR) {
+		/* accepted (filter, read) items OR their bit into zeroed words */
+		const size_t hb = a.n * ctx->words * sizeof(uint64_t);
+		CUDA_TRY(ctx, cudaMemsetAsync(a.hits[0], 0, hb, s));
+		if (a.mates == 2)
+			CUDA_TRY(ctx, cudaMemsetAsync(a.hits[1], 0, hb, s));
+	}
+	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k0, s));
 	CUDA_TRY(ctx, launch_classify(a, ctx->lc, s));
+	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k1, s));
 	CUDA_TRY(ctx, launch_summarize(a.hits[0], a.mates == 2 ? a.hits[1] : nullptr, a.n, ctx->nf,
 			ctx->words, ctx->p.inclusive, d_cat, ctx->d_counts, ctx->num_sms, s));
 	return BBT_OK;
@@ -632,14 +654,17 @@ extern "C" int bbt_last_stats(bbt_ctx *ctx, bbt_stats *out)
 		return BBT_ERR_ARG;
 	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
 	CUDA_TRY(ctx, cudaEventSynchronize(ctx->ev_stop));
-	float ms = 0;
+	float ms = 0, kms = 0;
 	CUDA_TRY(ctx, cudaEventElapsedTime(&ms, ctx->ev_start, ctx->ev_stop));
+	CUDA_TRY(ctx, cudaEventElapsedTime(&kms, ctx->ev_k0, ctx->ev_k1));
 	ctx->last.kernel_ms = ms;
+	ctx->last.classify_ms = kms;
 	if (ctx->lc.count) {
-		unsigned long long st[2];
+		unsigned long long st[3];
 		CUDA_TRY(ctx, cudaMemcpy(st, ctx->d_stat, sizeof st, cudaMemcpyDeviceToHost));
 		ctx->last.probes_issued = st[0];
 		ctx->last.frames = st[1];
+		ctx->last.probes_algorithmic = st[2];
 	}
 	*out = ctx->last;
 	return BBT_OK;
@@ -660,7 +685,7 @@ extern "C" int bbt_set_counting(bbt_ctx *ctx, int on)
 		return BBT_ERR_ARG;
 	ctx->lc.count = on ? 1 : 0;
 	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
-	CUDA_TRY(ctx, cudaMemset(ctx->d_stat, 0, 2 * sizeof(unsigned long long)));
+	CUDA_TRY(ctx, cudaMemset(ctx->d_stat, 0, 3 * sizeof(unsigned long long)));
 	return BBT_OK;
 }
 

@@ -22,10 +22,11 @@
  * inside the last chunk are probed speculatively (they change the bytes read,
  * never the result).
  *
- * Two launch shapes: PLAIN gives each warp one read (one launch per batch);
+ * Launch shapes: PLAIN gives each warp one read (one launch per batch);
  * PERSISTENT keeps one resident grid whose warps take reads from a global
  * counter until the batch is done, which balances reads of very different
- * lengths.
+ * lengths; FILTER_MAJOR is persistent over (filter, read) items in filter
+ * order, so that each filter in turn is probed by the whole GPU out of L2.
  */
 #include "classify.cuh"
 #include "seqeval_chunk.cuh"
@@ -112,9 +113,13 @@ __device__ void hash_window(const uint8_t *__restrict__ s, uint64_t w0, int wn, 
 	__syncwarp();
 }
 
+/* Evaluate read r against filters [f0, f1).  Returns the hit bits of those
+ * filters that fall in word f0 / 64 (bit f % 64); read-major launches call it
+ * with the whole filter range and write every word themselves. */
 template <int SEG, bool COUNT, bool LENGTH_MODE>
-__device__ void classify_read(const ClassifyArgs &a, uint64_t r, const Window<SEG> &win,
-		int lane, unsigned long long &probe_acc, unsigned long long &frame_acc)
+__device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, uint32_t f1,
+		const Window<SEG> &win, int lane, uint64_t &myword, unsigned long long &probe_acc,
+		unsigned long long &frame_acc, unsigned long long &alg_acc)
 {
 	constexpr int W = Window<SEG>::W;
 	const uint32_t mate = r >= a.n ? 1u : 0u;
@@ -123,11 +128,10 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, const Window<SE
 	const uint64_t start = off[i] - a.off_base[mate];
 	const uint64_t len = off[i + 1] - off[i];
 	const uint8_t *s = a.seq[mate] + start;
-	uint64_t myword = 0;
 	unsigned cached_k = 0;
 	int64_t cached_w0 = -1;
 	unsigned reads = 0;
-	for (uint32_t f = 0; f < a.nf; ++f) {
+	for (uint32_t f = f0; f < f1; ++f) {
 		const FilterDev F = a.filters[f];
 		const unsigned k = F.k;
 		if (len < k)
@@ -154,16 +158,21 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, const Window<SE
 			}
 			for (int c = 0; c < wn; c += 32) {
 				const int q = c + lane;
-				const int64_t p = (int64_t)w0 + q;
+				const int32_t p = (int32_t)w0 + q;
 				const bool v = q < wn && win.vld[q];
 				const bool probe = v && (length_mode || p >= st.skip_until);
+				const unsigned r0 = reads;
 				const bool hit = probe && contains(F, win.h0[q], reads);
 				const uint32_t V = __ballot_sync(kFull, v);
 				const uint32_t H = __ballot_sync(kFull, hit);
 				const int nfc = min(32, wn - c);
+				uint32_t alg = 0;
 				decided = length_mode
-						? length_chunk(ls, V, H, (int64_t)w0 + c, nfc)
-						: simple_chunk(st, V, H, (int32_t)w0 + c, nfc, (int)k, (int)a.streak_thr);
+						? length_chunk(ls, V, H, (int64_t)w0 + c, nfc, COUNT ? &alg : nullptr)
+						: simple_chunk(st, V, H, (int32_t)w0 + c, nfc, (int)k, (int)a.streak_thr,
+								COUNT ? &alg : nullptr);
+				if (COUNT && ((alg >> lane) & 1u))
+					alg_acc += reads - r0;
 				if (decided)
 					break;
 			}
@@ -171,13 +180,21 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, const Window<SE
 		if (decided == EVAL_ACCEPT && lane == (int)(f >> 6))
 			myword |= 1ull << (f & 63);
 	}
-	if (lane < (int)a.words)
-		a.hits[mate][i * a.words + lane] = myword;
 	if (COUNT)
 		probe_acc += reads;
 }
 
-template <int SEG, bool PERSISTENT, bool COUNT, bool LENGTH_MODE>
+enum { ORDER_PLAIN = 0, ORDER_READS = 1, ORDER_FILTERS = 2 };
+
+/*
+ * ORDER_PLAIN:   one read per warp, all filters, grid covers the batch.
+ * ORDER_READS:   persistent; warps take reads from a counter, all filters each.
+ * ORDER_FILTERS: persistent; work items are (filter, read) in filter-major
+ *                order, taken 32 at a time, so the whole GPU probes one filter
+ *                at a time and that filter stays resident in L2; accepted
+ *                items OR their bit into the (zeroed) hit words.
+ */
+template <int SEG, int ORDER, bool COUNT, bool LENGTH_MODE>
 __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
@@ -190,8 +207,8 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 	win.vld = reinterpret_cast<uint8_t *>(win.h0 + Window<SEG>::W);
 	win.bases = win.vld + Window<SEG>::W;
 	const uint64_t total = a.n * a.mates;
-	unsigned long long probe_acc = 0, frame_acc = 0;
-	if (PERSISTENT) {
+	unsigned long long probe_acc = 0, frame_acc = 0, alg_acc = 0;
+	if (ORDER == ORDER_READS) {
 		for (;;) {
 			unsigned long long r = 0;
 			if (lane == 0)
@@ -199,23 +216,64 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 			r = __shfl_sync(kFull, r, 0);
 			if (r >= total)
 				break;
-			classify_read<SEG, COUNT, LENGTH_MODE>(a, r, win, lane, probe_acc, frame_acc);
+			uint64_t myword = 0;
+			classify_read<SEG, COUNT, LENGTH_MODE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
+					frame_acc, alg_acc);
+			const uint32_t mate = r >= a.n ? 1u : 0u;
+			if (lane < (int)a.words)
+				a.hits[mate][(r - (mate ? a.n : 0)) * a.words + lane] = myword;
+		}
+	} else if (ORDER == ORDER_FILTERS) {
+		const uint64_t items = total * a.nf;
+		for (;;) {
+			unsigned long long b = 0;
+			if (lane == 0)
+				b = atomicAdd(a.work, 32ull);
+			b = __shfl_sync(kFull, b, 0);
+			if (b >= items)
+				break;
+			uint32_t f = (uint32_t)(b / total);
+			uint64_t r = b - (uint64_t)f * total;
+			const uint64_t e = b + 32 < items ? b + 32 : items;
+			for (uint64_t it = b; it < e; ++it) {
+				uint64_t myword = 0;
+				classify_read<SEG, COUNT, LENGTH_MODE>(a, r, f, f + 1, win, lane, myword,
+						probe_acc, frame_acc, alg_acc);
+				if (myword && lane == (int)(f >> 6)) {
+					const uint32_t mate = r >= a.n ? 1u : 0u;
+					atomicOr((unsigned long long *)&a.hits[mate][(r - (mate ? a.n : 0)) * a.words + lane],
+							(unsigned long long)myword);
+				}
+				if (++r == total) {
+					r = 0;
+					++f;
+				}
+			}
 		}
 	} else {
 		const uint64_t r = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp;
-		if (r < total)
-			classify_read<SEG, COUNT, LENGTH_MODE>(a, r, win, lane, probe_acc, frame_acc);
+		if (r < total) {
+			uint64_t myword = 0;
+			classify_read<SEG, COUNT, LENGTH_MODE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
+					frame_acc, alg_acc);
+			const uint32_t mate = r >= a.n ? 1u : 0u;
+			if (lane < (int)a.words)
+				a.hits[mate][(r - (mate ? a.n : 0)) * a.words + lane] = myword;
+		}
 	}
 	if (COUNT) {
 		for (int o = 16; o; o >>= 1) {
 			probe_acc += __shfl_xor_sync(kFull, probe_acc, o);
 			frame_acc += __shfl_xor_sync(kFull, frame_acc, o);
+			alg_acc += __shfl_xor_sync(kFull, alg_acc, o);
 		}
 		if (lane == 0) {
 			if (a.probes)
 				atomicAdd(a.probes, probe_acc);
 			if (a.frames)
 				atomicAdd(a.frames, frame_acc);
+			if (a.alg_probes)
+				atomicAdd(a.alg_probes, alg_acc);
 		}
 	}
 }
@@ -260,27 +318,28 @@ __global__ void summarize_kernel(const uint64_t *__restrict__ h1, const uint64_t
 			atomicAdd(&counts[j], sc[j]);
 }
 
-template <int SEG, bool P, bool C>
+template <int SEG, int ORDER, bool C>
 cudaError_t launch_one(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
 {
 	const int threads = lc.warps_per_block * 32;
 	const size_t smem = classify_smem_bytes(lc, a.kmax);
-	auto kern = a.scoring == BBT_SCORE_LENGTH ? classify_kernel<SEG, P, C, true>
-	                                          : classify_kernel<SEG, P, C, false>;
+	auto kern = a.scoring == BBT_SCORE_LENGTH ? classify_kernel<SEG, ORDER, C, true>
+	                                          : classify_kernel<SEG, ORDER, C, false>;
 	cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			(int)smem);
 	if (e != cudaSuccess)
 		return e;
 	uint64_t total = a.n * a.mates;
+	uint64_t warps_needed = ORDER == ORDER_FILTERS ? (total * a.nf + 31) / 32 : total;
 	unsigned blocks;
-	if (P) {
+	if (ORDER != ORDER_PLAIN) {
 		int per_sm = 0;
 		e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
 		if (e != cudaSuccess)
 			return e;
 		if (per_sm < 1)
 			per_sm = 1;
-		uint64_t need = (total + lc.warps_per_block - 1) / lc.warps_per_block;
+		uint64_t need = (warps_needed + lc.warps_per_block - 1) / lc.warps_per_block;
 		uint64_t full = (uint64_t)per_sm * lc.num_sms;
 		blocks = (unsigned)(need < full ? need : full);
 	} else {
@@ -290,6 +349,23 @@ cudaError_t launch_one(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream
 		return cudaSuccess;
 	kern<<<blocks, threads, smem, s>>>(a);
 	return cudaGetLastError();
+}
+
+template <int SEG>
+cudaError_t launch_seg(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
+{
+	const bool C = lc.count != 0;
+	switch (lc.path) {
+	case BBT_PATH_PLAIN:
+		return C ? launch_one<SEG, ORDER_PLAIN, true>(a, lc, s)
+		         : launch_one<SEG, ORDER_PLAIN, false>(a, lc, s);
+	case BBT_PATH_FILTER_MAJOR:
+		return C ? launch_one<SEG, ORDER_FILTERS, true>(a, lc, s)
+		         : launch_one<SEG, ORDER_FILTERS, false>(a, lc, s);
+	default:
+		return C ? launch_one<SEG, ORDER_READS, true>(a, lc, s)
+		         : launch_one<SEG, ORDER_READS, false>(a, lc, s);
+	}
 }
 
 } // namespace
@@ -304,16 +380,7 @@ size_t classify_smem_bytes(const LaunchConfig &lc, uint32_t kmax)
 
 cudaError_t launch_classify(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
 {
-	const bool P = lc.path == BBT_PATH_PERSISTENT;
-	const bool C = lc.count != 0;
-	if (lc.seg == 8) {
-		if (P)
-			return C ? launch_one<8, true, true>(a, lc, s) : launch_one<8, true, false>(a, lc, s);
-		return C ? launch_one<8, false, true>(a, lc, s) : launch_one<8, false, false>(a, lc, s);
-	}
-	if (P)
-		return C ? launch_one<4, true, true>(a, lc, s) : launch_one<4, true, false>(a, lc, s);
-	return C ? launch_one<4, false, true>(a, lc, s) : launch_one<4, false, false>(a, lc, s);
+	return lc.seg == 8 ? launch_seg<8>(a, lc, s) : launch_seg<4>(a, lc, s);
 }
 
 cudaError_t launch_summarize(const uint64_t *h1, const uint64_t *h2, uint64_t n, uint32_t nf,

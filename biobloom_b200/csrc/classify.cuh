@@ -33,6 +33,7 @@ struct ClassifyArgs {
 	unsigned long long *work;  /* persistent: next read to take (zeroed) */
 	unsigned long long *probes;/* optional: filter words read */
 	unsigned long long *frames;/* optional: frames hashed */
+	unsigned long long *alg_probes; /* optional: words the sequential algorithm reads */
 };
 
 struct LaunchConfig {

@@ -52,8 +52,9 @@ struct bbt_ctx {
 	uint64_t *d_tmp_hits[2] = {nullptr, nullptr};
 	uint64_t tmp_hits_cap = 0;
 	cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+	cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr; /* around the last classify kernel */
 	bbt::LaunchConfig lc;
-	bbt_stats last = {0, 0, 0, 0.0};
+	bbt_stats last = {0, 0, 0, 0, 0.0, 0.0};
 };
 
 namespace bbt {

@@ -157,9 +157,12 @@ BBT_HD void simple_init(SimpleState &s, double threshold, double one_minus,
  *       end of the read)
  * Frames below s.skip_until are inside a skip window: their H bits are never
  * read, so the caller need not probe them.  Returns s.decided.
+ * alg (optional) receives the frames of this chunk that the sequential
+ * algorithm probes (the ordinary frames up to the decision or the frame that
+ * opens a skip window), for counting algorithmic probes.
  */
 BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int32_t base,
-		int nf, int k, int streak_thr)
+		int nf, int k, int streak_thr, uint32_t *alg = nullptr)
 {
 	if (s.decided)
 		return s.decided;
@@ -289,13 +292,19 @@ BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int32_t base,
 			                    : nth_bit(ap, (int)need);
 		}
 		if (acc_pos < rej_pos) {
+			if (alg)
+				*alg |= V & range_mask(j, acc_pos + 1);
 			s.decided = EVAL_ACCEPT;
 			return s.decided;
 		}
 		if (rej_pos < 32) {
+			if (alg)
+				*alg |= V & range_mask(j, rej_pos + 1);
 			s.decided = EVAL_REJECT;
 			return s.decided;
 		}
+		if (alg)
+			*alg |= V & range_mask(j, t < nf ? t + 1 : nf);
 		s.score2 += dS;
 		s.anti += dA;
 		if (V & pre)
@@ -349,7 +358,7 @@ BBT_HD void length_init(LengthState &s, unsigned min_len, uint64_t len, int k)
 
 /* Advance over one chunk; every valid frame must have been probed. */
 BBT_HD int length_chunk(LengthState &s, uint32_t V, uint32_t H, int64_t base,
-		int nf)
+		int nf, uint32_t *alg = nullptr)
 {
 	if (s.decided)
 		return s.decided;
@@ -365,6 +374,8 @@ BBT_HD int length_chunk(LengthState &s, uint32_t V, uint32_t H, int64_t base,
 		}
 		if (pos != s.prev + 1)
 			s.match = 0;
+		if (alg)
+			*alg |= 1u << q;
 		if ((H >> q) & 1u)
 			s.match = s.match == 0 ? s.k : s.match + 1;
 		else

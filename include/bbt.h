@@ -50,7 +50,8 @@ extern "C" {
 /* ---- kernel paths ---- */
 #define BBT_PATH_AUTO 0        /* persistent work-stealing path, tuned */
 #define BBT_PATH_PLAIN 1       /* one warp per read, one launch per batch */
-#define BBT_PATH_PERSISTENT 2  /* persistent work-stealing kernel */
+#define BBT_PATH_PERSISTENT 2  /* persistent work-stealing kernel, read-major */
+#define BBT_PATH_FILTER_MAJOR 3 /* persistent, (filter, read) items in filter order */
 
 typedef struct bbt_ctx bbt_ctx;
 
@@ -72,6 +73,9 @@ typedef struct {
 	uint32_t frames_per_lane;   /* probe chains in flight per lane (1, 2 or 4); 0 = tuned */
 	uint64_t max_batch_bases;   /* device staging capacity per batch (bases); 0 = default */
 	uint64_t max_batch_reads;   /* device staging capacity per batch (reads); 0 = default */
+	uint32_t l2_fetch_bytes;    /* L2 fetch granularity for this process's context
+	                               (cudaLimitMaxL2FetchGranularity): 32, 64 or 128;
+	                               0 = 32, one DRAM sector per Bloom probe */
 } bbt_params;
 
 /* Fill p with the reference's defaults (score 0.15, streak 3, SIMPLE). */
@@ -173,12 +177,17 @@ int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int frames_per_l
  * (diagnostics; costs atomics).  No reference counterpart. */
 int bbt_set_counting(bbt_ctx *ctx, int on);
 
-/* Counters of the last classified batch: probes issued by the device. */
+/* Counters of the batches classified since counting was switched on (see
+ * bbt_set_counting), and the device time of the last batch. */
 typedef struct {
 	uint64_t reads;
-	uint64_t frames;
-	uint64_t probes_issued;     /* filter words read by the kernel */
-	double kernel_ms;           /* classify kernel time of the last batch */
+	uint64_t frames;              /* frames hashed */
+	uint64_t probes_issued;       /* filter words read by the kernel */
+	uint64_t probes_algorithmic;  /* filter words the sequential reference reads:
+	                                 BloomFilter::contains bit tests up to the first
+	                                 clear bit, for the frames SeqEval visits */
+	double kernel_ms;             /* device time of the last batch (all kernels) */
+	double classify_ms;           /* device time of the last classify kernel */
 } bbt_stats;
 int bbt_last_stats(bbt_ctx *ctx, bbt_stats *out);
 

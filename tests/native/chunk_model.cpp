@@ -2,28 +2,31 @@
  * chunk_model.cpp -- host build of the product's chunked SeqEval state
  * machine (biobloom_b200/csrc/seqeval_chunk.cuh), fed with per-frame hit bits
  * from the CPU oracle.  Used by tests/test_chunk_model.py to check the
- * chunked decision against the oracle's sequential evalSimple /
- * evalMinMatchLen on random reads, without a GPU.
+ * chunked decision, and the count of probes the sequential algorithm makes,
+ * against the oracle's evalSimple / evalMinMatchLen on random reads, without a
+ * GPU.
  */
 #include "seqeval_chunk.cuh"
 #include "bbt_oracle.h"
 #include <vector>
 
 extern "C" int model_eval(const char *seq, uint64_t len, const oracle_bf *bf,
-		double threshold, unsigned streak_thr, int scoring,
-		uint64_t *probed_frames)
+		double threshold, unsigned streak_thr, int scoring, uint64_t *alg_probes)
 {
 	const unsigned k = bf->k;
 	if (len < k)
 		return 0;
 	const uint64_t frames = len - k + 1;
 	std::vector<uint8_t> valid(frames), hit(frames);
-	/* validity and hit bit of every frame, from the oracle's iterator */
+	std::vector<uint32_t> cost(frames);
+	/* validity, hit bit and bit-test count of every frame, from the oracle */
 	oracle_ntitr it;
 	for (oracle_ntitr_init(&it, seq, len, bf->h, k); !oracle_ntitr_end(&it);
 			oracle_ntitr_next(&it)) {
+		uint64_t c = 0;
 		valid[it.pos] = 1;
-		hit[it.pos] = (uint8_t)oracle_bf_contains(bf, it.hv, 0);
+		hit[it.pos] = (uint8_t)oracle_bf_contains(bf, it.hv, &c);
+		cost[it.pos] = (uint32_t)c;
 	}
 	bbt::SimpleState ss;
 	bbt::LengthState ls;
@@ -40,16 +43,16 @@ extern "C" int model_eval(const char *seq, uint64_t len, const oracle_bf *bf,
 				continue;
 			V |= 1u << j;
 			bool probe = scoring == ORACLE_LENGTH || (int64_t)p >= ss.skip_until;
-			if (probe) {
-				if (probed_frames)
-					++*probed_frames;
-				if (hit[p])
-					H |= 1u << j;
-			}
+			if (probe && hit[p])
+				H |= 1u << j;
 		}
+		uint32_t alg = 0;
 		int d = scoring == ORACLE_LENGTH
-				? bbt::length_chunk(ls, V, H, (int64_t)base, nf)
-				: bbt::simple_chunk(ss, V, H, (int64_t)base, nf, (int)k, (int)streak_thr);
+				? bbt::length_chunk(ls, V, H, (int64_t)base, nf, &alg)
+				: bbt::simple_chunk(ss, V, H, (int32_t)base, nf, (int)k, (int)streak_thr, &alg);
+		for (int j = 0; j < nf; ++j)
+			if ((alg >> j) & 1u)
+				*alg_probes += cost[base + j];
 		if (d)
 			return d == bbt::EVAL_ACCEPT;
 	}

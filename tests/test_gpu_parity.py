@@ -35,11 +35,13 @@ def _classifier(paths, score=0.15, streak=3, **kw):
 
 
 PATHS = [dict(path=1), dict(path=2), dict(path=2, frames_per_lane=8),
-         dict(path=1, warps_per_block=4, frames_per_lane=8)]
+         dict(path=1, warps_per_block=4, frames_per_lane=8), dict(path=3),
+         dict(path=3, frames_per_lane=8)]
+PATH_IDS = ["plain", "persistent", "persistent-seg8", "plain-w4-seg8", "filter-major",
+            "filter-major-seg8"]
 
 
-@pytest.mark.parametrize("launch", PATHS, ids=["plain", "persistent", "persistent-seg8",
-                                               "plain-w4-seg8"])
+@pytest.mark.parametrize("launch", PATHS, ids=PATH_IDS)
 @pytest.mark.parametrize("name,score,streak", [("se_s0.15_r3", 0.15, 3), ("se_s0.5_r1", 0.5, 1),
                                                ("se_s0.05_r0", 0.05, 0), ("se_s40", 40, 3)])
 def test_golden_single_end(name, score, streak, launch):
@@ -51,7 +53,8 @@ def test_golden_single_end(name, score, streak, launch):
         assert bbc.summary_tsv() == summary
 
 
-@pytest.mark.parametrize("launch", PATHS[:2], ids=["plain", "persistent"])
+@pytest.mark.parametrize("launch", [PATHS[0], PATHS[1], PATHS[4]],
+                         ids=["plain", "persistent", "filter-major"])
 def test_golden_pairs(launch):
     r1 = read_fastx(golden("reads_1.fq.gz"))
     r2 = read_fastx(golden("reads_2.fq.gz"))
@@ -151,8 +154,7 @@ def _random_reads(rng, genomes, n, lmin=20, lmax=400, nrate=0.02, sub=0.01):
 @pytest.mark.parametrize("seed,k,h,score,streak", [
     (1, 25, 0, 0.15, 3), (2, 21, 2, 0.3, 2), (3, 31, 4, 0.05, 1), (4, 17, 1, 0.9, 5),
     (5, 25, 3, 0.0, 3), (6, 25, 3, 1.0, 3), (7, 12, 3, 0.4, 0), (8, 64, 3, 0.15, 3)])
-@pytest.mark.parametrize("launch", PATHS, ids=["plain", "persistent", "persistent-seg8",
-                                               "plain-w4-seg8"])
+@pytest.mark.parametrize("launch", PATHS, ids=PATH_IDS)
 def test_random_parity_with_oracle(seed, k, h, score, streak, launch, tmp_path):
     rng, genomes, filters = _random_case(seed, k=k, h=h, fpr=0.2)
     paths = []
