@@ -53,6 +53,11 @@ class Stats(ctypes.Structure):
                 ("kernel_ms", ctypes.c_double), ("classify_ms", ctypes.c_double)]
 
 
+class FilterView(ctypes.Structure):
+    _fields_ = [("words", ctypes.c_void_p), ("m", ctypes.c_uint64), ("h", ctypes.c_uint),
+                ("k", ctypes.c_uint)]
+
+
 class SynthReadParams(ctypes.Structure):
     _fields_ = [("len_min", ctypes.c_uint32), ("len_max", ctypes.c_uint32),
                 ("long_frac", ctypes.c_double), ("long_min", ctypes.c_uint32),
@@ -96,6 +101,7 @@ def lib():
         "bbt_set_counting": (i32, [vp, i32]),
         "bbt_set_launch": (i32, [vp, i32, i32, i32]),
         "bbt_set_inclusive": (i32, [vp, i32]),
+        "bbt_classify_noalloc": (i32, [P(FilterView), i32, P(Params), P(Batch), vp, vp, vp]),
         "bbt_make_filter": (i32, [vp, P(u64), u64, u32, dbl, u32, u64, cp, cp, cp, i32]),
         "bbt_synth_genome": (i32, [u64, u64, dbl, dbl, ctypes.c_uint32, ctypes.c_uint32, dbl, dbl,
                                    vp]),

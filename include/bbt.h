@@ -203,6 +203,39 @@ int bbt_make_filter(const char *seq, const uint64_t *offsets, uint64_t n_seqs,
 		unsigned k, double fpr, unsigned hash_num, uint64_t entries,
 		const char *stem, const char *filter_id, const char *sources, int device);
 
+/*
+ * Classification that allocates no memory, for callers that cannot call
+ * cudaMalloc: their device memory belongs to another allocator (a framework's
+ * caching allocator, a pool reserved up front with a fixed budget), or they run
+ * where cudaMalloc / cudaFree, which can synchronize the whole device, are not
+ * acceptable.  No counterpart in the reference.
+ *
+ * The caller passes device pointers: the filters' bit arrays (bbt_filter_view,
+ * as bbt_open would load them from .bf files), the reads (batch->location must
+ * be BBT_DEVICE) and the hit words (hits, and hits2 for pairs; same layout as
+ * bbt_result).  Results are the same as bbt_classify_batch's hits; no summary
+ * counters are kept.  The call is enqueued on `stream` on device
+ * params->device.
+ *
+ * Limits and sharing: at most BBT_NOALLOC_MAX_FILTERS filters (more is
+ * rejected with BBT_ERR_ARG).  The kernel's scratch (filter table and work
+ * counter) is one small array of device memory per GPU that lives as long as
+ * the library is loaded; every call on that GPU shares it, so calls that
+ * overlap on the GPU race and must be issued one after another.  The first
+ * call on each GPU looks up the array's device address, so make that first
+ * call before any stream capture.
+ */
+#define BBT_NOALLOC_MAX_FILTERS 64
+typedef struct {
+	const void *words;   /* device pointer to the m/8-byte bit array */
+	uint64_t m;          /* size in bits, a multiple of 64 */
+	unsigned h;          /* hash functions */
+	unsigned k;          /* k-mer size */
+} bbt_filter_view;
+int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filters,
+		const bbt_params *params, const bbt_batch *batch, uint64_t *hits,
+		uint64_t *hits2, void *stream);
+
 /* ---- synthetic workloads (host only; no GPU needed) ---- */
 
 typedef struct {
