@@ -18,6 +18,7 @@
 #include "classify.cuh"
 #include "ctx.hpp"
 #include "formats.hpp"
+#include "twopass.cuh"
 
 namespace bbt {
 
@@ -134,6 +135,11 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 	cudaFree(ctx->d_stat);
 	cudaFree(ctx->d_tmp_hits[0]);
 	cudaFree(ctx->d_tmp_hits[1]);
+	cudaFree(ctx->d_tp_local);
+	cudaFree(ctx->d_tp_sums);
+	cudaFreeHost(ctx->h_tp_sums);
+	cudaFree(ctx->d_tp_h0);
+	cudaFree(ctx->d_tp_vmask);
 	for (Slot &s : ctx->slot) {
 		free_slot(s);
 		if (s.copied)
@@ -238,10 +244,25 @@ static int alloc_slot(bbt_ctx *ctx, Slot &s, uint64_t bases, uint64_t reads)
 	return BBT_OK;
 }
 
+/* The tuned path: with two or more filters of one k that each fit in L2,
+ * probe them one at a time out of L2 (two-pass filter-major); otherwise the
+ * persistent read-major kernel. */
+static int auto_path(const bbt_ctx *ctx)
+{
+	if (ctx->nf < 2 || !ctx->same_k)
+		return BBT_PATH_PERSISTENT;
+	int l2 = 0;
+	cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->dev);
+	for (const FilterDev &f : ctx->hf)
+		if (f.m / 8 > (uint64_t)l2 * 3 / 4)
+			return BBT_PATH_PERSISTENT;
+	return BBT_PATH_FILTER_MAJOR;
+}
+
 static LaunchConfig pick_config(const bbt_ctx *ctx)
 {
 	LaunchConfig lc;
-	lc.path = ctx->p.path == BBT_PATH_AUTO ? BBT_PATH_PERSISTENT : ctx->p.path;
+	lc.path = ctx->p.path == BBT_PATH_AUTO ? auto_path(ctx) : ctx->p.path;
 	lc.warps_per_block = ctx->p.warps_per_block ? (int)ctx->p.warps_per_block : 8;
 	lc.seg = ctx->p.frames_per_lane == 8 ? 8 : 4;
 	lc.num_sms = ctx->num_sms;
@@ -336,16 +357,12 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 		if (rc != BBT_OK)
 			goto fail_out;
 		ctx->d_words.push_back(d);
-		FilterDev fd;
-		fd.words = d;
-		fd.m = hd.m;
-		fd.minv = ~0ull / hd.m;
-		fd.h = hd.h;
-		fd.k = hd.k;
-		ctx->hf.push_back(fd);
+		ctx->hf.push_back(make_filter_dev(d, hd.m, hd.h, hd.k));
 		ctx->kmax = std::max(ctx->kmax, hd.k);
 	}
 	ctx->nf = (uint32_t)n_filters;
+	for (const FilterDev &fd : ctx->hf)
+		ctx->same_k = ctx->same_k && fd.k == ctx->hf[0].k;
 	ctx->words = (ctx->nf + 63) / 64;
 	OPEN_TRY(cudaMalloc(&ctx->d_filters, sizeof(FilterDev) * ctx->nf));
 	OPEN_TRY(cudaMemcpy(ctx->d_filters, ctx->hf.data(), sizeof(FilterDev) * ctx->nf,
@@ -407,20 +424,110 @@ static ClassifyArgs base_args(const bbt_ctx *ctx)
 	return a;
 }
 
+/* Grow a device buffer to hold at least n elements (contents not kept). */
+template <typename T>
+static int grow(bbt_ctx *ctx, T **buf, uint64_t &cap, uint64_t n)
+{
+	if (n <= cap)
+		return BBT_OK;
+	cudaFree(*buf);
+	*buf = nullptr;
+	cap = 0;
+	CUDA_TRY(ctx, cudaMalloc(buf, std::max<uint64_t>(n, 1) * sizeof(T)));
+	cap = n;
+	return BBT_OK;
+}
+
+/* Two-pass filter-major classification of one batch (all filters share k):
+ * scan of padded frame counts, a host read of the per-block totals to cut the
+ * batch into sub-batches whose frames fit the scratch, then hash pass and
+ * filter pass per sub-batch. */
+static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
+{
+	const uint64_t total = a.n * a.mates;
+	const uint64_t B = two_pass_block_reads();
+	const uint64_t nb = (total + B - 1) / B;
+	const unsigned k = ctx->hf[0].k;
+	int rc = grow(ctx, &ctx->d_tp_local, ctx->tp_local_cap, total);
+	if (rc)
+		return rc;
+	if (nb + 1 > ctx->tp_sums_cap) {
+		cudaFree(ctx->d_tp_sums);
+		cudaFreeHost(ctx->h_tp_sums);
+		ctx->d_tp_sums = nullptr;
+		ctx->h_tp_sums = nullptr;
+		ctx->tp_sums_cap = 0;
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_tp_sums, (nb + 1) * sizeof(unsigned long long)));
+		CUDA_TRY(ctx, cudaMallocHost(&ctx->h_tp_sums, (nb + 1) * sizeof(unsigned long long)));
+		ctx->tp_sums_cap = nb + 1;
+	}
+	CUDA_TRY(ctx, two_pass_scan(a, k, ctx->d_tp_local, ctx->d_tp_sums, s));
+	CUDA_TRY(ctx, cudaMemcpyAsync(ctx->h_tp_sums, ctx->d_tp_sums,
+			(nb + 1) * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+	CUDA_TRY(ctx, cudaStreamSynchronize(s));
+	const unsigned long long *sums = ctx->h_tp_sums;
+	/* frame slots per sub-batch (8 bytes of hash each) */
+	const uint64_t budget = ctx->p.max_batch_bases ? std::max<uint64_t>(ctx->p.max_batch_bases, 32)
+	                                               : (512ull << 20);
+	std::vector<uint64_t> cuts(1, 0);
+	uint64_t most = 0;
+	while (cuts.back() < nb) {
+		const uint64_t b0 = cuts.back();
+		uint64_t b1 = b0 + 1;
+		while (b1 < nb && sums[b1 + 1] - sums[b0] <= budget)
+			++b1;
+		most = std::max<uint64_t>(most, sums[b1] - sums[b0]);
+		cuts.push_back(b1);
+	}
+	if (most > ctx->tp_frames_cap) {
+		cudaFree(ctx->d_tp_h0);
+		cudaFree(ctx->d_tp_vmask);
+		ctx->d_tp_h0 = nullptr;
+		ctx->d_tp_vmask = nullptr;
+		ctx->tp_frames_cap = 0;
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_tp_h0, most * sizeof(uint64_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_tp_vmask, (most / 32 + 1) * sizeof(uint32_t)));
+		ctx->tp_frames_cap = most;
+	}
+	for (size_t c = 0; c + 1 < cuts.size(); ++c) {
+		TwoPassArgs p;
+		p.t0 = cuts[c] * B;
+		p.t1 = std::min(total, cuts[c + 1] * B);
+		p.r_first = 0;
+		p.local = ctx->d_tp_local;
+		p.sums = ctx->d_tp_sums;
+		p.s0 = sums[cuts[c]];
+		p.k = k;
+		p.h0 = ctx->d_tp_h0;
+		p.vmask = ctx->d_tp_vmask;
+		p.work = ctx->d_work;
+		CUDA_TRY(ctx, two_pass_sub_batch(a, p, ctx->lc, s));
+	}
+	return BBT_OK;
+}
+
 /* classify + summarize one staged or device-resident batch on stream s */
 static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStream_t s)
 {
-	if (ctx->lc.path != BBT_PATH_PLAIN)
-		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), s));
-	if (ctx->lc.path == BBT_PATH_FILTER_MAJOR) {
+	const bool two_pass = ctx->lc.path == BBT_PATH_FILTER_MAJOR && ctx->same_k;
+	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k0, s));
+	if (two_pass) {
 		/* accepted (filter, read) items OR their bit into zeroed words */
 		const size_t hb = a.n * ctx->words * sizeof(uint64_t);
 		CUDA_TRY(ctx, cudaMemsetAsync(a.hits[0], 0, hb, s));
 		if (a.mates == 2)
 			CUDA_TRY(ctx, cudaMemsetAsync(a.hits[1], 0, hb, s));
+		int rc = run_two_pass(ctx, a, s);
+		if (rc)
+			return rc;
+	} else {
+		LaunchConfig lc = ctx->lc;
+		if (lc.path == BBT_PATH_FILTER_MAJOR)
+			lc.path = BBT_PATH_PERSISTENT; /* filters of different k */
+		if (lc.path != BBT_PATH_PLAIN)
+			CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), s));
+		CUDA_TRY(ctx, launch_classify(a, lc, s));
 	}
-	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k0, s));
-	CUDA_TRY(ctx, launch_classify(a, ctx->lc, s));
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k1, s));
 	CUDA_TRY(ctx, launch_summarize(a.hits[0], a.mates == 2 ? a.hits[1] : nullptr, a.n, ctx->nf,
 			ctx->words, ctx->p.inclusive, d_cat, ctx->d_counts, ctx->num_sms, s));

@@ -35,9 +35,23 @@ struct FilterDev {
 	const uint32_t *words; /* m / 32 words */
 	uint64_t m;            /* bits (a multiple of 64) */
 	uint64_t minv;         /* floor((2^64 - 1) / m), for the reduction */
+	uint64_t kmul;         /* k * kMultiSeed, for the extra hashes */
 	uint32_t h;            /* hash functions */
 	uint32_t k;            /* k-mer size */
 };
+
+/* Descriptor of a filter whose bit array is at `words` (device memory). */
+inline FilterDev make_filter_dev(const void *words, uint64_t m, unsigned h, unsigned k)
+{
+	FilterDev f;
+	f.words = (const uint32_t *)words;
+	f.m = m;
+	f.minv = ~0ull / m;
+	f.kmul = (uint64_t)k * kMultiSeed;
+	f.h = h;
+	f.k = k;
+	return f;
+}
 
 #if defined(__CUDACC__)
 
@@ -85,17 +99,14 @@ __device__ __forceinline__ uint64_t extra_hash(uint64_t canon, unsigned k, unsig
 	return t ^ (t >> kMultiShift);
 }
 
-/* v mod m by Barrett reduction with minv = floor((2^64-1)/m): the estimate is
- * at most two below the true quotient. */
+/* v mod m by Barrett reduction with minv = floor((2^64-1)/m).  Since
+ * v/m - 1 < v*minv/2^64 <= v/m, the quotient estimate is the true quotient or
+ * one below it, so one correction suffices. */
 __device__ __forceinline__ uint64_t reduce(uint64_t v, uint64_t m, uint64_t minv)
 {
-	uint64_t q = __umul64hi(v, minv);
-	uint64_t r = v - q * m;
-	if (r >= m)
-		r -= m;
-	if (r >= m)
-		r -= m;
-	return r;
+	const uint64_t q = __umul64hi(v, minv);
+	const uint64_t r = v - q * m;
+	return r >= m ? r - m : r;
 }
 
 /* One 4-byte read through the read-only path.  On this GPU an isolated
@@ -118,10 +129,74 @@ __device__ __forceinline__ bool contains(const FilterDev &f, uint64_t canon, uns
 	++reads;
 	for (unsigned i = 1; i < f.h; ++i) {
 		++reads;
-		if (!test_bit(f.words, reduce(extra_hash(canon, f.k, i), f.m, f.minv)))
+		uint64_t t = canon * ((uint64_t)i ^ f.kmul); /* extra_hash(canon, k, i) */
+		t ^= t >> kMultiShift;
+		if (!test_bit(f.words, reduce(t, f.m, f.minv)))
 			return false;
 	}
 	return true;
+}
+
+/* Loads of data read once per pass (the two-pass path's stored hashes):
+ * marked evict-first in L2 so that they do not push the filter being probed
+ * out of L2, and not allocated in L1. */
+__device__ __forceinline__ uint64_t evict_first_policy()
+{
+	uint64_t pol;
+	asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+	return pol;
+}
+
+__device__ __forceinline__ uint64_t ld_stream_u64(const uint64_t *p, uint64_t pol)
+{
+	uint64_t v;
+	asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b64 %0, [%1], %2;"
+			: "=l"(v) : "l"(p), "l"(pol));
+	return v;
+}
+
+__device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t *p, uint64_t pol)
+{
+	uint32_t v;
+	asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;"
+			: "=r"(v) : "l"(p), "l"(pol));
+	return v;
+}
+
+/* Two independent BloomFilter::contains chains per lane, their rounds
+ * interleaved so that both probes of a round are in flight together.
+ * pa / pb: whether frame a / b is probed at all.  Word reads are counted in
+ * ra / rb exactly as contains() counts them. */
+__device__ __forceinline__ void contains2(const FilterDev &f, uint64_t ca, bool pa, uint64_t cb,
+		bool pb, bool &ha, bool &hb, unsigned &ra, unsigned &rb)
+{
+	bool la = pa, lb = pb;
+	for (unsigned i = 0; i < f.h && (la || lb); ++i) {
+		uint64_t va = ca, vb = cb;
+		if (i) {
+			const uint64_t mul = (uint64_t)i ^ f.kmul;
+			va = ca * mul;
+			va ^= va >> kMultiShift;
+			vb = cb * mul;
+			vb ^= vb >> kMultiShift;
+		}
+		uint32_t wa = 0, wb = 0;
+		uint64_t ba = 0, bb = 0;
+		if (la) {
+			ba = reduce(va, f.m, f.minv);
+			wa = __ldg(f.words + (ba >> 5));
+		}
+		if (lb) {
+			bb = reduce(vb, f.m, f.minv);
+			wb = __ldg(f.words + (bb >> 5));
+		}
+		ra += la;
+		rb += lb;
+		la = la && ((wa >> (ba & 31u)) & 1u);
+		lb = lb && ((wb >> (bb & 31u)) & 1u);
+	}
+	ha = la;
+	hb = lb;
 }
 
 #endif /* __CUDACC__ */

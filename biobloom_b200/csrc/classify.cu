@@ -25,93 +25,18 @@
  * Launch shapes: PLAIN gives each warp one read (one launch per batch);
  * PERSISTENT keeps one resident grid whose warps take reads from a global
  * counter until the batch is done, which balances reads of very different
- * lengths; FILTER_MAJOR is persistent over (filter, read) items in filter
- * order, so that each filter in turn is probed by the whole GPU out of L2.
+ * lengths.  The filter-major order for several L2-sized filters is in
+ * twopass.cu.
  */
 #include "classify.cuh"
 #include "seqeval_chunk.cuh"
+#include "window.cuh"
 
 #include "bbt.h"
 
 namespace bbt {
 
 namespace {
-
-constexpr unsigned kFull = 0xffffffffu;
-
-/* Per-warp shared-memory window. */
-template <int SEG>
-struct Window {
-	static constexpr int W = 32 * SEG;
-	uint64_t *roll;   /* [8]: rol(seed_fw(A,C,G,T), k), rol(seed_rc(A,C,G,T), k-1) */
-	uint64_t *h0;     /* canonical hash of frame q (window-relative) */
-	uint8_t *vld;     /* 1 if frame q holds only ACGT */
-	uint8_t *bases;   /* bases [w0, w0 + wn + k - 1) */
-};
-
-template <int SEG>
-__device__ __forceinline__ size_t window_stride(uint32_t kmax)
-{
-	size_t b = 64 + (size_t)Window<SEG>::W * 9 + Window<SEG>::W + kmax;
-	return (b + 15) & ~(size_t)15;
-}
-
-/* Per-k constants of the rolling update (lanes 0-7 write one each). */
-template <int SEG>
-__device__ __forceinline__ void set_roll(const Window<SEG> &win, unsigned k, int lane)
-{
-	if (lane < 8) {
-		const uint64_t seeds[4] = {kSeedA, kSeedC, kSeedG, kSeedT};
-		win.roll[lane] = lane < 4 ? rolk(seeds[lane], k) : rolk(seeds[7 - lane], k - 1);
-	}
-	__syncwarp();
-}
-
-__device__ __forceinline__ int base_code(uint8_t c)
-{
-	uint8_t u = c & 0xDF;
-	return u == 'A' ? 0 : u == 'C' ? 1 : u == 'G' ? 2 : u == 'T' ? 3 : -1;
-}
-
-/* Hash frames [w0, w0 + wn) of the read at s (len bases) into the window. */
-template <int SEG>
-__device__ void hash_window(const uint8_t *__restrict__ s, uint64_t w0, int wn, unsigned k,
-		const Window<SEG> &win, int lane)
-{
-	const int nb = wn + (int)k - 1;
-	for (int b = lane; b < nb; b += 32)
-		win.bases[b] = s[w0 + b];
-	__syncwarp();
-	const int S = (wn + 31) >> 5; /* frames per lane in this window */
-	const int q0 = lane * S;
-	if (q0 < wn) {
-		const uint8_t *bb = win.bases + q0;
-		uint64_t fh = 0, rh = 0;
-		int lb = -1; /* last invalid base, window-relative */
-		for (unsigned i = 0; i < k; ++i) {
-			uint8_t c = bb[i];
-			fh = rol1(fh) ^ seed_fw(c);
-			if (!base_ok(c))
-				lb = q0 + (int)i;
-		}
-		for (int i = (int)k - 1; i >= 0; --i)
-			rh = rol1(rh) ^ seed_rc(bb[i]);
-		win.h0[q0] = fh < rh ? fh : rh;
-		win.vld[q0] = lb < q0;
-		const int qe = min(q0 + S, wn);
-		for (int q = q0 + 1; q < qe; ++q) {
-			uint8_t out = win.bases[q - 1], in = win.bases[q + k - 1];
-			const int co = base_code(out), ci = base_code(in);
-			fh = rol1(fh) ^ (co >= 0 ? win.roll[co] : 0ull) ^ seed_fw(in);
-			rh = ror1(rh) ^ ror1(seed_rc(out)) ^ (ci >= 0 ? win.roll[4 + ci] : 0ull);
-			if (!base_ok(in))
-				lb = q + (int)k - 1;
-			win.h0[q] = fh < rh ? fh : rh;
-			win.vld[q] = lb < q;
-		}
-	}
-	__syncwarp();
-}
 
 /* Evaluate read r against filters [f0, f1).  Returns the hit bits of those
  * filters that fall in word f0 / 64 (bit f % 64); read-major launches call it
@@ -149,7 +74,7 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 			const int wn = (int)min((uint64_t)W, frames - w0);
 			if (cached_k != k || cached_w0 != (int64_t)w0) {
 				if (cached_k != k)
-					set_roll<SEG>(win, k, lane);
+					set_tables<SEG>(win, k, lane);
 				hash_window<SEG>(s, w0, wn, k, win, lane);
 				cached_k = k;
 				cached_w0 = (int64_t)w0;
@@ -159,11 +84,11 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 			for (int c = 0; c < wn; c += 32) {
 				const int q = c + lane;
 				const int32_t p = (int32_t)w0 + q;
-				const bool v = q < wn && win.vld[q];
+				const uint32_t V = win.vmask[c >> 5];
+				const bool v = (V >> lane) & 1u;
 				const bool probe = v && (length_mode || p >= st.skip_until);
 				const unsigned r0 = reads;
 				const bool hit = probe && contains(F, win.h0[q], reads);
-				const uint32_t V = __ballot_sync(kFull, v);
 				const uint32_t H = __ballot_sync(kFull, hit);
 				const int nfc = min(32, wn - c);
 				uint32_t alg = 0;
@@ -184,15 +109,12 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 		probe_acc += reads;
 }
 
-enum { ORDER_PLAIN = 0, ORDER_READS = 1, ORDER_FILTERS = 2 };
+enum { ORDER_PLAIN = 0, ORDER_READS = 1 };
 
 /*
  * ORDER_PLAIN:   one read per warp, all filters, grid covers the batch.
  * ORDER_READS:   persistent; warps take reads from a counter, all filters each.
- * ORDER_FILTERS: persistent; work items are (filter, read) in filter-major
- *                order, taken 32 at a time, so the whole GPU probes one filter
- *                at a time and that filter stays resident in L2; accepted
- *                items OR their bit into the (zeroed) hit words.
+ * (The filter-major order is the two-pass path in twopass.cu.)
  */
 template <int SEG, int ORDER, bool COUNT, bool LENGTH_MODE>
 __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
@@ -200,12 +122,7 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 	extern __shared__ __align__(16) unsigned char smem[];
 	const int lane = threadIdx.x & 31;
 	const int warp = threadIdx.x >> 5;
-	const size_t stride = window_stride<SEG>(a.kmax);
-	Window<SEG> win;
-	win.roll = reinterpret_cast<uint64_t *>(smem + warp * stride);
-	win.h0 = win.roll + 8;
-	win.vld = reinterpret_cast<uint8_t *>(win.h0 + Window<SEG>::W);
-	win.bases = win.vld + Window<SEG>::W;
+	const Window<SEG> win = window_at<SEG>(smem + warp * window_stride<SEG>(a.kmax));
 	const uint64_t total = a.n * a.mates;
 	unsigned long long probe_acc = 0, frame_acc = 0, alg_acc = 0;
 	if (ORDER == ORDER_READS) {
@@ -222,33 +139,6 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 			const uint32_t mate = r >= a.n ? 1u : 0u;
 			if (lane < (int)a.words)
 				a.hits[mate][(r - (mate ? a.n : 0)) * a.words + lane] = myword;
-		}
-	} else if (ORDER == ORDER_FILTERS) {
-		const uint64_t items = total * a.nf;
-		for (;;) {
-			unsigned long long b = 0;
-			if (lane == 0)
-				b = atomicAdd(a.work, 32ull);
-			b = __shfl_sync(kFull, b, 0);
-			if (b >= items)
-				break;
-			uint32_t f = (uint32_t)(b / total);
-			uint64_t r = b - (uint64_t)f * total;
-			const uint64_t e = b + 32 < items ? b + 32 : items;
-			for (uint64_t it = b; it < e; ++it) {
-				uint64_t myword = 0;
-				classify_read<SEG, COUNT, LENGTH_MODE>(a, r, f, f + 1, win, lane, myword,
-						probe_acc, frame_acc, alg_acc);
-				if (myword && lane == (int)(f >> 6)) {
-					const uint32_t mate = r >= a.n ? 1u : 0u;
-					atomicOr((unsigned long long *)&a.hits[mate][(r - (mate ? a.n : 0)) * a.words + lane],
-							(unsigned long long)myword);
-				}
-				if (++r == total) {
-					r = 0;
-					++f;
-				}
-			}
 		}
 	} else {
 		const uint64_t r = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp;
@@ -330,7 +220,7 @@ cudaError_t launch_one(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream
 	if (e != cudaSuccess)
 		return e;
 	uint64_t total = a.n * a.mates;
-	uint64_t warps_needed = ORDER == ORDER_FILTERS ? (total * a.nf + 31) / 32 : total;
+	uint64_t warps_needed = total;
 	unsigned blocks;
 	if (ORDER != ORDER_PLAIN) {
 		int per_sm = 0;
@@ -359,9 +249,6 @@ cudaError_t launch_seg(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream
 	case BBT_PATH_PLAIN:
 		return C ? launch_one<SEG, ORDER_PLAIN, true>(a, lc, s)
 		         : launch_one<SEG, ORDER_PLAIN, false>(a, lc, s);
-	case BBT_PATH_FILTER_MAJOR:
-		return C ? launch_one<SEG, ORDER_FILTERS, true>(a, lc, s)
-		         : launch_one<SEG, ORDER_FILTERS, false>(a, lc, s);
 	default:
 		return C ? launch_one<SEG, ORDER_READS, true>(a, lc, s)
 		         : launch_one<SEG, ORDER_READS, false>(a, lc, s);
@@ -372,10 +259,8 @@ cudaError_t launch_seg(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream
 
 size_t classify_smem_bytes(const LaunchConfig &lc, uint32_t kmax)
 {
-	size_t W = 32 * (size_t)lc.seg;
-	size_t b = 64 + W * 9 + W + kmax;
-	b = (b + 15) & ~(size_t)15;
-	return b * (size_t)lc.warps_per_block;
+	const size_t per_warp = lc.seg == 8 ? window_stride<8>(kmax) : window_stride<4>(kmax);
+	return per_warp * (size_t)lc.warps_per_block;
 }
 
 cudaError_t launch_classify(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)

@@ -51,6 +51,17 @@ struct bbt_ctx {
 	uint64_t cap_bases = 0, cap_reads = 0;
 	uint64_t *d_tmp_hits[2] = {nullptr, nullptr};
 	uint64_t tmp_hits_cap = 0;
+	/* two-pass filter-major scratch: padded frame offsets, per-block sums,
+	 * per-frame canonical hashes and validity words of one sub-batch */
+	uint64_t *d_tp_local = nullptr;
+	uint64_t tp_local_cap = 0;
+	unsigned long long *d_tp_sums = nullptr;
+	unsigned long long *h_tp_sums = nullptr; /* pinned copy */
+	uint64_t tp_sums_cap = 0;
+	uint64_t *d_tp_h0 = nullptr;
+	uint32_t *d_tp_vmask = nullptr;
+	uint64_t tp_frames_cap = 0;
+	bool same_k = true;
 	cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 	cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr; /* around the last classify kernel */
 	bbt::LaunchConfig lc;

@@ -105,11 +105,7 @@ extern "C" int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filter
 		if (!v.words || v.m == 0 || v.m % 64 || v.h == 0 || v.h > 64 || v.k == 0 || v.k > 255)
 			return fail(nullptr, BBT_ERR_ARG, "bbt_classify_noalloc: filter " +
 					std::to_string(i) + " has a null array or out-of-range m, h or k");
-		table[i].words = (const uint32_t *)v.words;
-		table[i].m = v.m;
-		table[i].minv = ~0ull / v.m;
-		table[i].h = v.h;
-		table[i].k = v.k;
+		table[i] = make_filter_dev(v.words, v.m, v.h, v.k);
 		kmax = v.k > kmax ? v.k : kmax;
 	}
 	if (batch->n_reads == 0)

@@ -90,6 +90,43 @@ BBT_HD int nth_bit(uint32_t x, int n)
 enum { EVAL_OPEN = 0, EVAL_ACCEPT = 1, EVAL_REJECT = 2 };
 
 /*
+ * Where a chunk's running totals cross their thresholds.  Frame j of the chunk
+ * (restricted to `pre`) accepts when it is a hit and
+ *   score2 + popc(H & frames<=j) + popc(P2 & frames<=j) >= thres2,
+ * and rejects when it adds to antiScore and anti + popc(A & frames<=j) >=
+ * anti_thres.  On the device every lane evaluates its own frame and two
+ * ballots collect the answers (all 32 lanes of the warp must be here); on the
+ * host the lanes are looped over.
+ */
+BBT_HD void crossing_masks(uint32_t H, uint32_t P2, uint32_t A, uint32_t pre, int32_t score2,
+		int32_t anti, int32_t thres2, int32_t anti_thres, uint32_t &acc, uint32_t &rej)
+{
+	H &= pre;
+	P2 &= pre;
+	A &= pre;
+#if defined(__CUDA_ARCH__)
+	unsigned lane;
+	asm("mov.u32 %0, %%laneid;" : "=r"(lane));
+	const uint32_t le = 0xffffffffu >> (31 - lane);
+	const int32_t sc = score2 + __popc(H & le) + __popc(P2 & le);
+	const int32_t an = anti + __popc(A & le);
+	acc = __ballot_sync(0xffffffffu, ((H >> lane) & 1u) && sc >= thres2);
+	rej = __ballot_sync(0xffffffffu, ((A >> lane) & 1u) && an >= anti_thres);
+#else
+	acc = rej = 0;
+	for (unsigned lane = 0; lane < 32; ++lane) {
+		const uint32_t le = 0xffffffffu >> (31 - lane);
+		const int32_t sc = score2 + popc32(H & le) + popc32(P2 & le);
+		const int32_t an = anti + popc32(A & le);
+		if (((H >> lane) & 1u) && sc >= thres2)
+			acc |= 1u << lane;
+		if (((A >> lane) & 1u) && an >= anti_thres)
+			rej |= 1u << lane;
+	}
+#endif
+}
+
+/*
  * State of one (read, filter) evaluation under SIMPLE scoring.
  * score2 is twice the reference's double score (a multiple of 0.5), so
  * "thres <= score" is "score2 >= thres2" with thres2 = ceil(2*thres); anti
@@ -169,6 +206,62 @@ BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int32_t base,
 	const uint32_t inread = low_mask(nf);
 	V &= inread;
 	H &= V;
+	/* Fast path: no skip window open.  Frames before the first skip trigger
+	 * (a miss after at least streak_thr hits) are settled here, including an
+	 * accept or reject among them; a chunk that reaches a trigger undecided
+	 * continues in the general loop below, from its start.  (The first
+	 * visited frame can never trigger: its streak is 0.) */
+	if (!s.in_window && streak_thr >= 1 && streak_thr <= 31) {
+		const int st = s.streak;
+		/* bit 31-i of lowc is "frame base-1-i was a hit", i < streak */
+		const uint32_t lowc = st <= 0 ? 0u : (st >= 32 ? 0xffffffffu : (0xffffffffu << (32 - st)));
+		uint32_t run = 0xffffffffu; /* frames preceded by streak_thr hits */
+		for (int q = 1; q <= streak_thr; ++q)
+			run &= (H << q) | (lowc >> (32 - q));
+		const uint32_t M = V & ~H;
+		const uint32_t trig = M & run;
+		const uint32_t pre = trig ? low_mask(lowbit32(trig)) : inread;
+		const uint32_t prevhit = H & ((H << 1) | (st > 0 ? 1u : 0u));
+		/* invalid frames count, except those before the first valid one */
+		const uint32_t C = s.started ? (~V & inread)
+		                             : (V ? (~V & inread & ~low_mask(lowbit32(V))) : 0u);
+		const uint32_t A = M | C;
+		const int32_t dS = popc32(H & pre) + popc32(prevhit & pre);
+		const int32_t dA = popc32(A & pre);
+		if (s.score2 + dS >= s.thres2 || s.anti + dA >= s.anti_thres) {
+			uint32_t acc, rej;
+			crossing_masks(H, prevhit, A, pre, s.score2, s.anti, s.thres2, s.anti_thres, acc, rej);
+			const int ap = acc ? lowbit32(acc) : 32;
+			const int rp = rej ? lowbit32(rej) : 32;
+			if (ap < rp) {
+				if (alg)
+					*alg |= V & low_mask(ap + 1);
+				s.decided = EVAL_ACCEPT;
+				return s.decided;
+			}
+			if (rp < 32) {
+				if (alg)
+					*alg |= V & low_mask(rp + 1);
+				s.decided = EVAL_REJECT;
+				return s.decided;
+			}
+		}
+		if (!trig) {
+			s.score2 += dS;
+			s.anti += dA;
+			s.started |= V != 0;
+			if (alg)
+				*alg |= V;
+			const uint32_t nonhit = ~H & inread;
+			if (nonhit) {
+				s.streak = popc32(H & ~low_mask(highbit32(nonhit) + 1));
+			} else {
+				const int ns = st + nf;
+				s.streak = ns > 64 ? 64 : ns;
+			}
+			return EVAL_OPEN;
+		}
+	}
 	int j = 0;
 	while (j < nf) {
 		/* ---- skip-window frames ---- */

@@ -1,0 +1,131 @@
+/*
+ * window.cuh -- per-warp hash window of the classification kernels: a run of
+ * up to 32*SEG frames of one read, with the canonical ntHash and validity of
+ * each frame in shared memory.
+ */
+#ifndef BBT_WINDOW_CUH
+#define BBT_WINDOW_CUH
+
+#include <stdint.h>
+
+#include "bbt_device.cuh"
+
+namespace bbt {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+/* Per-warp shared-memory window. */
+template <int SEG>
+struct Window {
+	static constexpr int W = 32 * SEG;
+	uint64_t *tab;    /* [20]: seed_fw, seed_rc, rol(seed_fw, k), rol(seed_rc, k-1) of
+	                     codes A,C,G,T (4 each), then 4 zeros for code 4 (not ACGT) */
+	uint64_t *h0;     /* [W] canonical hash of frame q (window-relative) */
+	uint32_t *vmask;  /* [SEG] bit j of word c: frame 32c+j holds only ACGT */
+	uint8_t *vld;     /* [W] 1 if frame q holds only ACGT */
+	uint8_t *code;    /* [W + kmax] base codes 0..3, 4 = not ACGT */
+};
+
+template <int SEG>
+__host__ __device__ __forceinline__ size_t window_stride(uint32_t kmax)
+{
+	size_t b = 20 * 8 + (size_t)Window<SEG>::W * 8 + SEG * 4 + Window<SEG>::W +
+			Window<SEG>::W + kmax;
+	return (b + 15) & ~(size_t)15;
+}
+
+template <int SEG>
+__device__ __forceinline__ Window<SEG> window_at(unsigned char *base)
+{
+	Window<SEG> w;
+	w.tab = reinterpret_cast<uint64_t *>(base);
+	w.h0 = w.tab + 20;
+	w.vmask = reinterpret_cast<uint32_t *>(w.h0 + Window<SEG>::W);
+	w.vld = reinterpret_cast<uint8_t *>(w.vmask + SEG);
+	w.code = w.vld + Window<SEG>::W;
+	return w;
+}
+
+/* Seed tables of the current k (lanes 0-19 write one entry each).  Entries
+ * 16-19 are 0: a base that is not ACGT has seed 0, which is what keeps the
+ * rolling update exact across invalid bases. */
+template <int SEG>
+__device__ __forceinline__ void set_tables(const Window<SEG> &win, unsigned k, int lane)
+{
+	if (lane < 20) {
+		const int c = lane & 3, which = lane >> 2;
+		const uint64_t fw = c == 0 ? kSeedA : c == 1 ? kSeedC : c == 2 ? kSeedG : kSeedT;
+		const uint64_t rc = c == 0 ? kSeedT : c == 1 ? kSeedG : c == 2 ? kSeedC : kSeedA;
+		const uint64_t v = which == 0 ? fw : which == 1 ? rc : which == 2 ? rolk(fw, k)
+		                 : rolk(rc, k - 1);
+		win.tab[lane] = which == 4 ? 0ull : v;
+	}
+	__syncwarp();
+}
+
+__device__ __forceinline__ uint8_t base_code(uint8_t c)
+{
+	const uint8_t u = c & 0xDF;
+	return u == 'A' ? 0 : u == 'C' ? 1 : u == 'G' ? 2 : u == 'T' ? 3 : 4;
+}
+
+/* table entry `which` (0 fw, 1 rc, 2 fw rolled by k, 3 rc rolled by k-1) of a
+ * base code; code 4 reads one of the zero entries */
+__device__ __forceinline__ uint64_t seed_of(const uint64_t *tab, int which, uint8_t code)
+{
+	return tab[code < 4 ? which * 4 + code : 16];
+}
+
+/* Hash frames [w0, w0 + wn) of the read at s into the window: base codes are
+ * staged with coalesced loads, then each lane hashes S consecutive frames
+ * (Horner over its first k-mer, rolling after), and the validity of the frames
+ * is balloted into one mask word per 32 frames. */
+template <int SEG>
+__device__ void hash_window(const uint8_t *__restrict__ s, uint64_t w0, int wn, unsigned k,
+		const Window<SEG> &win, int lane)
+{
+	const int nb = wn + (int)k - 1;
+	for (int b = lane; b < nb; b += 32)
+		win.code[b] = base_code(s[w0 + b]);
+	__syncwarp();
+	const int S = (wn + 31) >> 5; /* frames per lane in this window */
+	const int q0 = lane * S;
+	const uint64_t *tab = win.tab;
+	if (q0 < wn) {
+		const uint8_t *cc = win.code + q0;
+		uint64_t fh = 0, rh = 0;
+		int lb = -1; /* last invalid base, window-relative */
+		for (unsigned i = 0; i < k; ++i) {
+			const uint8_t c = cc[i];
+			fh = rol1(fh) ^ seed_of(tab, 0, c);
+			if (c == 4)
+				lb = q0 + (int)i;
+		}
+		for (int i = (int)k - 1; i >= 0; --i)
+			rh = rol1(rh) ^ seed_of(tab, 1, cc[i]);
+		win.h0[q0] = fh < rh ? fh : rh;
+		win.vld[q0] = lb < q0;
+		const int qe = min(q0 + S, wn);
+		for (int q = q0 + 1; q < qe; ++q) {
+			const uint8_t out = win.code[q - 1], in = win.code[q + k - 1];
+			fh = rol1(fh) ^ seed_of(tab, 2, out) ^ seed_of(tab, 0, in);
+			rh = ror1(rh) ^ ror1(seed_of(tab, 1, out)) ^ seed_of(tab, 3, in);
+			if (in == 4)
+				lb = q + (int)k - 1;
+			win.h0[q] = fh < rh ? fh : rh;
+			win.vld[q] = lb < q;
+		}
+	}
+	__syncwarp();
+	for (int c = 0; c < wn; c += 32) {
+		const int q = c + lane;
+		const uint32_t v = __ballot_sync(kFull, q < wn && win.vld[q]);
+		if (lane == 0)
+			win.vmask[c >> 5] = v;
+	}
+	__syncwarp();
+}
+
+} // namespace bbt
+
+#endif
