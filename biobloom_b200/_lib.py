@@ -50,7 +50,8 @@ class Result(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [("reads", ctypes.c_uint64), ("frames", ctypes.c_uint64),
                 ("probes_issued", ctypes.c_uint64), ("probes_algorithmic", ctypes.c_uint64),
-                ("kernel_ms", ctypes.c_double), ("classify_ms", ctypes.c_double)]
+                ("kernel_ms", ctypes.c_double), ("classify_ms", ctypes.c_double),
+                ("kernels", ctypes.c_uint64)]
 
 
 class FilterView(ctypes.Structure):

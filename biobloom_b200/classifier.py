@@ -153,7 +153,7 @@ class BioBloomClassifier:
         L.check(L.lib().bbt_last_stats(self._ctx, ctypes.byref(st)), self._ctx)
         return {"reads": st.reads, "frames": st.frames, "probes_issued": st.probes_issued,
                 "probes_algorithmic": st.probes_algorithmic, "kernel_ms": st.kernel_ms,
-                "classify_ms": st.classify_ms}
+                "classify_ms": st.classify_ms, "kernels": st.kernels}
 
     # -- summary (ResultsManager) ---------------------------------------------
     def summary(self):

@@ -489,6 +489,7 @@ static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_tp_vmask, (most / 32 + 1) * sizeof(uint32_t)));
 		ctx->tp_frames_cap = most;
 	}
+	ctx->last.kernels += 2 + 2 * (cuts.size() - 1); /* scans, then hash + filter passes */
 	for (size_t c = 0; c + 1 < cuts.size(); ++c) {
 		TwoPassArgs p;
 		p.t0 = cuts[c] * B;
@@ -509,6 +510,7 @@ static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 /* classify + summarize one staged or device-resident batch on stream s */
 static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStream_t s)
 {
+	ctx->last.kernels = 2; /* classification (counted below for two-pass) + summary */
 	const bool two_pass = ctx->lc.path == BBT_PATH_FILTER_MAJOR && ctx->same_k;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k0, s));
 	if (two_pass) {
@@ -517,6 +519,7 @@ static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStrea
 		CUDA_TRY(ctx, cudaMemsetAsync(a.hits[0], 0, hb, s));
 		if (a.mates == 2)
 			CUDA_TRY(ctx, cudaMemsetAsync(a.hits[1], 0, hb, s));
+		ctx->last.kernels = 1;
 		int rc = run_two_pass(ctx, a, s);
 		if (rc)
 			return rc;

@@ -65,7 +65,7 @@ struct bbt_ctx {
 	cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 	cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr; /* around the last classify kernel */
 	bbt::LaunchConfig lc;
-	bbt_stats last = {0, 0, 0, 0, 0.0, 0.0};
+	bbt_stats last = {0, 0, 0, 0, 0.0, 0.0, 0};
 };
 
 namespace bbt {

@@ -187,7 +187,9 @@ typedef struct {
 	                                 BloomFilter::contains bit tests up to the first
 	                                 clear bit, for the frames SeqEval visits */
 	double kernel_ms;             /* device time of the last batch (all kernels) */
-	double classify_ms;           /* device time of the last classify kernel */
+	double classify_ms;           /* device time of the last batch's classification
+	                                 kernels (without the summary kernel) */
+	uint64_t kernels;             /* kernels the last batch launched */
 } bbt_stats;
 int bbt_last_stats(bbt_ctx *ctx, bbt_stats *out);
 
