@@ -217,3 +217,128 @@ def summary_tsv(counts, ids, read_count):
     n = lib().oracle_summary_tsv(_u64p(np.ascontiguousarray(counts, dtype=np.uint64)), nf, arr,
                                  read_count, buf, cap)
     return buf.raw[:n].decode()
+
+
+# ---------------------------------------------------------------- miBF oracle
+
+class _MIBF(ctypes.Structure):
+    _fields_ = [("m", ctypes.c_uint64), ("h", ctypes.c_uint), ("k", ctypes.c_uint),
+                ("nseeds", ctypes.c_uint), ("seeds", (ctypes.c_char * 256) * 16),
+                ("bv", ctypes.POINTER(ctypes.c_uint64)),
+                ("rank_word", ctypes.POINTER(ctypes.c_uint64)),
+                ("ids", ctypes.POINTER(ctypes.c_uint16)), ("pop", ctypes.c_uint64)]
+
+
+class _QRes(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint16), ("nonSatFrameCount", ctypes.c_uint32),
+                ("solidCount", ctypes.c_uint32), ("count", ctypes.c_uint32),
+                ("nonSatCount", ctypes.c_uint32), ("totalNonSatCount", ctypes.c_uint32),
+                ("totalCount", ctypes.c_uint32)]
+
+
+_mibf_sig_done = False
+
+
+def _mibf_lib():
+    global _mibf_sig_done
+    L = lib()
+    if not _mibf_sig_done:
+        P = ctypes.POINTER
+        L.oracle_mibf_build.argtypes = [P(_MIBF), P(ctypes.c_char_p), P(ctypes.c_uint64),
+                                        P(ctypes.c_uint16), ctypes.c_size_t,
+                                        P(ctypes.c_char_p), ctypes.c_uint, ctypes.c_uint,
+                                        ctypes.c_uint, ctypes.c_double]
+        L.oracle_mibf_free.argtypes = [P(_MIBF)]
+        L.oracle_mibf_store.argtypes = [P(_MIBF), ctypes.c_char_p]
+        L.oracle_mibf_load.argtypes = [P(_MIBF), ctypes.c_char_p]
+        L.oracle_mibf_frame_probs.restype = ctypes.c_double
+        L.oracle_mibf_frame_probs.argtypes = [P(_MIBF), P(ctypes.c_double), ctypes.c_uint,
+                                              ctypes.c_uint]
+        L.oracle_mibf_query.restype = ctypes.c_uint
+        L.oracle_mibf_query.argtypes = [P(_MIBF), ctypes.c_char_p, ctypes.c_size_t,
+                                        ctypes.c_char_p, ctypes.c_size_t, P(ctypes.c_uint32),
+                                        ctypes.c_uint, ctypes.c_double, ctypes.c_uint,
+                                        ctypes.c_uint, ctypes.c_int, P(_QRes), ctypes.c_uint,
+                                        P(ctypes.c_uint32), P(ctypes.c_uint64)]
+        L.oracle_binom_upper_quantile.restype = ctypes.c_uint
+        L.oracle_binom_upper_quantile.argtypes = [ctypes.c_uint, ctypes.c_double,
+                                                  ctypes.c_double]
+        L.oracle_st_hash.restype = ctypes.c_uint64
+        L.oracle_st_hash.argtypes = [ctypes.c_char_p, ctypes.c_uint, ctypes.c_char_p]
+        _mibf_sig_done = True
+    return L
+
+
+class MIBF:
+    """A multi-index Bloom filter held by the oracle."""
+
+    def __init__(self):
+        self.f = _MIBF()
+        self._owned = False
+
+    @classmethod
+    def build(cls, seqs, ids, seeds=None, k=25, h=3, occupancy=0.5):
+        L = _mibf_lib()
+        o = cls()
+        arr = (ctypes.c_char_p * len(seqs))(*seqs)
+        lens = np.array([len(s) for s in seqs], dtype=np.uint64)
+        idv = np.array(ids, dtype=np.uint16)
+        sarr = (ctypes.c_char_p * max(1, len(seeds or [])))(*[s.encode() for s in seeds or []])
+        kk = len(seeds[0]) if seeds else k
+        rc = L.oracle_mibf_build(ctypes.byref(o.f), arr, _u64p(lens),
+                                 idv.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), len(seqs),
+                                 sarr, len(seeds or []), kk, h, occupancy)
+        if rc:
+            raise RuntimeError(f"oracle_mibf_build = {rc}")
+        o._owned = True
+        return o
+
+    @classmethod
+    def load(cls, path):
+        o = cls()
+        rc = _mibf_lib().oracle_mibf_load(ctypes.byref(o.f), path.encode())
+        if rc:
+            raise IOError(f"oracle_mibf_load({path}) = {rc}")
+        o._owned = True
+        return o
+
+    def __del__(self):
+        if getattr(self, "_owned", False) and _lib is not None:
+            _lib.oracle_mibf_free(ctypes.byref(self.f))
+
+    def store(self, prefix):
+        if _mibf_lib().oracle_mibf_store(ctypes.byref(self.f), prefix.encode()):
+            raise IOError(prefix)
+
+    def frame_probs(self, nids, allowed_miss):
+        probs = np.zeros(nids, dtype=np.float64)
+        sat = _mibf_lib().oracle_mibf_frame_probs(
+            ctypes.byref(self.f), probs.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nids,
+            allowed_miss)
+        return probs, sat
+
+    def bits(self):
+        return np.ctypeslib.as_array(self.f.bv, shape=(self.f.m // 64,)).copy()
+
+    def ids(self):
+        return np.ctypeslib.as_array(self.f.ids, shape=(self.f.pop,)).copy()
+
+    def query(self, seq, min_count, seq2=None, multi=1.0, allowed_miss=2, min_nonsat=0,
+              best_agree=False):
+        L = _mibf_lib()
+        nids = len(min_count)
+        mc = np.ascontiguousarray(min_count, dtype=np.uint32)
+        out = (_QRes * max(1, nids))()
+        sat = ctypes.c_uint32()
+        n = L.oracle_mibf_query(ctypes.byref(self.f), seq, len(seq), seq2,
+                                len(seq2) if seq2 is not None else 0,
+                                mc.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32)), nids, multi,
+                                allowed_miss, min_nonsat, int(best_agree), out, max(1, nids),
+                                ctypes.byref(sat), None)
+        res = [(r.id, r.nonSatFrameCount, r.solidCount, r.count, r.nonSatCount,
+                r.totalNonSatCount, r.totalCount) for r in out[:n]]
+        return res, sat.value
+
+
+def binom_upper_quantile(n, p, q):
+    return _mibf_lib().oracle_binom_upper_quantile(n, p, q)
