@@ -12,7 +12,9 @@ LIB_PATH = os.path.join(PKG, "lib", "libbbt.so")
 
 BBT_OK = 0
 BBT_ERR = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "CUDA", -5: "NOMEM", -6: "UNSUPPORTED",
-           -7: "TIMEOUT", -8: "NODEVICE"}
+           -7: "TIMEOUT", -8: "NODEVICE", -9: "OVERFLOW"}
+ERR_OVERFLOW = -9
+MIBF_OUT_TSV, MIBF_OUT_FASTA, MIBF_OUT_FASTQ = 0, 1, 2
 SCORE_SIMPLE, SCORE_LENGTH = 0, 1
 HOST, DEVICE = 0, 1
 PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT, PATH_FILTER_MAJOR = 0, 1, 2, 3
@@ -67,6 +69,27 @@ class SynthReadParams(ctypes.Structure):
                 ("frag_max", ctypes.c_uint32)]
 
 
+class MibfParams(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_double), ("frame_matches", ctypes.c_uint),
+                ("multi_thresh", ctypes.c_double), ("streak", ctypes.c_uint),
+                ("min_nonsat", ctypes.c_uint), ("best_hit_agree", ctypes.c_int),
+                ("hit_only", ctypes.c_int), ("device", ctypes.c_int),
+                ("max_batch_bases", ctypes.c_uint64), ("max_batch_reads", ctypes.c_uint64)]
+
+
+class MibfHit(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_uint32), ("nonSatFrameCount", ctypes.c_uint32),
+                ("solidCount", ctypes.c_uint32), ("count", ctypes.c_uint32),
+                ("nonSatCount", ctypes.c_uint32), ("totalNonSatCount", ctypes.c_uint32),
+                ("totalCount", ctypes.c_uint32)]
+
+
+class MibfResult(ctypes.Structure):
+    _fields_ = [("hits", ctypes.c_void_p), ("max_hits", ctypes.c_uint32),
+                ("n_hits", ctypes.c_void_p), ("sat_count", ctypes.c_void_p),
+                ("location", ctypes.c_int)]
+
+
 _lib = None
 
 
@@ -109,6 +132,30 @@ def lib():
         "bbt_synth_read_lengths": (i32, [u64, P(SynthReadParams), u64, vp]),
         "bbt_synth_reads": (i32, [u64, vp, vp, ctypes.c_uint32, vp, P(SynthReadParams), u64, vp,
                                   vp, vp, vp]),
+        "bbt_mibf_default_params": (None, [P(MibfParams)]),
+        "bbt_mibf_open": (i32, [cp, P(MibfParams), P(vp)]),
+        "bbt_mibf_open_host": (i32, [cp, P(MibfParams), P(vp)]),
+        "bbt_mibf_close": (i32, [vp]),
+        "bbt_mibf_last_error": (cp, [vp]),
+        "bbt_mibf_num_ids": (u32, [vp]),
+        "bbt_mibf_id_name": (cp, [vp, u32]),
+        "bbt_mibf_info": (i32, [vp, P(u64), P(u32), P(u32), P(u32)]),
+        "bbt_mibf_frame_probs": (i32, [vp, P(dbl), P(dbl)]),
+        "bbt_mibf_classify_batch": (i32, [vp, P(Batch), P(MibfResult), vp]),
+        "bbt_mibf_sync": (i32, [vp]),
+        "bbt_mibf_last_kernel_ms": (dbl, [vp]),
+        "bbt_mibf_summary": (i32, [vp, P(u64), P(u64)]),
+        "bbt_mibf_reset_summary": (i32, [vp]),
+        "bbt_mibf_summary_tsv": (i32, [vp, u64, ctypes.c_char_p, ctypes.c_size_t,
+                                       P(ctypes.c_size_t)]),
+        "bbt_mibf_filter_files": (i32, [vp, P(cp), i32, cp, i32, vp]),
+        "bbt_mibf_filter_pair_files": (i32, [vp, cp, cp, cp, i32, vp]),
+        "bbt_mibf_min_count": (u32, [u32, dbl, dbl, u32]),
+        "bbt_mibf_format_record": (i32, [vp, i32, cp, cp, cp, cp, P(MibfHit), ctypes.c_uint32,
+                                         ctypes.c_uint32, ctypes.c_char_p, ctypes.c_size_t,
+                                         P(ctypes.c_size_t)]),
+        "bbt_mibf_make": (i32, [vp, vp, vp, u64, P(cp), u32, P(cp), u32, u32, u32, dbl, i32,
+                                cp, i32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -121,5 +168,12 @@ def lib():
 def check(rc, ctx=None):
     if rc != BBT_OK:
         msg = lib().bbt_last_error(ctx)
+        raise BBTError(rc, msg.decode() if msg else "")
+    return rc
+
+
+def check_mibf(rc, ctx=None):
+    if rc != BBT_OK:
+        msg = lib().bbt_mibf_last_error(ctx)
         raise BBTError(rc, msg.decode() if msg else "")
     return rc

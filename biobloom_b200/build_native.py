@@ -1,7 +1,8 @@
 """Build the native parts of biobloom_b200 in-tree.
 
   biobloom_b200/lib/libbbt.so          CUDA kernels + C ABI (include/bbt.h)
-  biobloom_b200/bin/biobloomcategorizer  CLI over the C ABI
+  biobloom_b200/bin/biobloomcategorizer    CLI over the C ABI (Bloom filters)
+  biobloom_b200/bin/biobloommicategorizer  CLI over the C ABI (miBF, include/bbt_mibf.h)
 
 Device code is compiled for sm_100a only.  Objects go to biobloom_b200/_build/
 and are rebuilt when a source or header is newer.
@@ -21,12 +22,16 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC,
           "-Xcompiler", "-fPIC,-fopenmp,-O3,-Wall", "-ccbin", "/usr/bin/g++"]
-LIB_SOURCES = ["classify.cu", "twopass.cu", "api.cu", "noalloc.cu", "maker.cu", "formats.cpp", "fastx.cpp", "synth.cpp"]
+LIB_SOURCES = ["classify.cu", "twopass.cu", "api.cu", "noalloc.cu", "maker.cu", "mibf.cu",
+               "mibf_make.cu", "formats.cpp", "fastx.cpp", "synth.cpp", "mibf_host.cpp",
+               "mibf_pipeline.cpp"]
+CLIS = [("biobloomcategorizer", "cli_categorizer.cpp"),
+        ("biobloommicategorizer", "cli_micategorizer.cpp")]
 
 
 def _headers():
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
-    return hs + [os.path.join(ROOT, "include", "bbt.h")]
+    return hs + [os.path.join(ROOT, "include", "bbt.h"), os.path.join(ROOT, "include", "bbt_mibf.h")]
 
 
 def _newer(target, deps):
@@ -64,12 +69,13 @@ def build(verbose=False, ptxas_info=False):
     if _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs +
              ["-Xcompiler", "-fopenmp", "-lz", "-ccbin", "/usr/bin/g++"], verbose)
-    cli = os.path.join(BIN, "biobloomcategorizer")
-    cli_src = os.path.join(CSRC, "cli_categorizer.cpp")
-    if _newer(cli, [cli_src, LIB] + hdrs):
-        _run(["/usr/bin/g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), cli_src,
-              "-o", cli, "-L" + os.path.dirname(LIB), "-lbbt",
-              "-Wl,-rpath,$ORIGIN/../lib"], verbose)
+    for name, src in CLIS:
+        cli = os.path.join(BIN, name)
+        cli_src = os.path.join(CSRC, src)
+        if _newer(cli, [cli_src, LIB] + hdrs):
+            _run(["/usr/bin/g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+                  cli_src, "-o", cli, "-L" + os.path.dirname(LIB), "-lbbt",
+                  "-Wl,-rpath,$ORIGIN/../lib"], verbose)
     return LIB
 
 

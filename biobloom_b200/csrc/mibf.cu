@@ -1,0 +1,1024 @@
+/*
+ * mibf.cu -- the miBF query path on the GPU: device layout of the filter, the
+ * classification kernel, and the bbt_mibf_* entry points that drive it.
+ *
+ * Device layout.  The bit vector is cut into 32-byte blocks of 224 bits:
+ * word 0 of a block is the number of set bits before the block counted from
+ * the start of its superblock (2^20 blocks), words 1-7 hold bits
+ * [224 b, 224 b + 224).  A probe of bit p reads one block (one DRAM sector) and
+ * gets both the bit and its rank: superblock base (a small table that stays
+ * in L1/L2) + block count + popcounts of the words before p in the block.  The
+ * ID of a set bit is ids[rank] (a second, dependent read).  The reference's
+ * MIBloomFilter keeps the same bits with sdsl rank support (a separate rank
+ * structure); here rank and bits share the sector.
+ *
+ * Kernel.  One warp classifies one read (pair) at a time, taking reads from a
+ * work counter four at a time.  Bases are staged 512 at a time as 2-bit codes
+ * (one 64-bit word per 32 bases, built with three ballots over coalesced byte
+ * loads) plus an invalid-base mask; each lane then takes one frame, computes
+ * its h seed values from per-seed position tables in shared memory, issues
+ * the h block reads, then the ID reads.  Per-frame, per-ID increments are
+ * merged across the warp with __match_any_sync and added to a per-warp tally
+ * table in shared memory (one slot per target ID), from which the warp picks
+ * the significant IDs and writes the result list and the summary counters.
+ */
+#include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "bbt_device.cuh"
+#include "mibf_ctx.hpp"
+#include "window.cuh"
+
+namespace bbt {
+
+constexpr int kBlockBits = 224;
+constexpr int kSuperShift = 20;
+constexpr int kStageBases = 512;
+constexpr int kReadsPerGrab = 4;
+
+struct MibfDev {
+	const uint4 *blocks;
+	const unsigned long long *super;
+	const uint16_t *ids;
+	uint64_t m, minv;
+	uint32_t h, k, nse, nids;
+	int kmer_mode;
+};
+
+struct MibfArgs {
+	MibfDev f;
+	const uint8_t *seq;
+	const uint64_t *off;
+	const uint8_t *seq2;
+	const uint64_t *off2;
+	uint64_t n_reads;
+	const uint32_t *minc;
+	uint32_t need, min_nonsat;
+	int best_agree, skip_empty_summary;
+	double multi;
+	const unsigned long long *tables;
+	bbt_mibf_hit *hits;
+	uint32_t max_hits;
+	uint32_t *n_hits, *sat;
+	unsigned long long *counts; /* this batch's summary counters */
+	unsigned long long *work;
+	unsigned int *flags;
+	uint32_t T;                 /* tally slots per warp, a multiple of 32 */
+};
+
+__host__ __device__ inline size_t mibf_warp_bytes(uint32_t T)
+{
+	return 17 * 8 + 18 * 4 + (size_t)3 * T * 8; /* codes, invalid words, tally */
+}
+
+__host__ inline size_t mibf_smem_bytes(uint32_t nse, uint32_t T, int warps)
+{
+	return (size_t)nse * 32 * 4 * 16 + (size_t)warps * mibf_warp_bytes(T);
+}
+
+__device__ __forceinline__ uint64_t spread_bits(uint32_t v)
+{
+	uint64_t x = v;
+	x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
+	x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
+	x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
+	x = (x | (x << 2)) & 0x3333333333333333ull;
+	x = (x | (x << 1)) & 0x5555555555555555ull;
+	return x;
+}
+
+/* min(F, R) of one seed over the 2-bit codes w (base j at bits 2j, 2j+1). */
+__device__ __forceinline__ uint64_t seed_value(const ulonglong2 *tab, uint64_t w, uint32_t k)
+{
+	uint64_t F = 0, R = 0;
+#pragma unroll
+	for (int j = 0; j < 32; ++j) {
+		if (j < (int)k) {
+			const ulonglong2 e = tab[j * 4 + (int)((w >> (2 * j)) & 3u)];
+			F ^= e.x;
+			R ^= e.y;
+		}
+	}
+	return F < R ? F : R;
+}
+
+/* Tally word order: A = count | nonSatCount << 32, B = solidCount |
+ * totalCount << 32, C = totalNonSatCount | nonSatFrameCount << 32. */
+struct Cand {
+	unsigned long long k1, k2; /* (count, nonSat), (total, ~id): larger is better */
+};
+
+__device__ __forceinline__ bool cand_less(const Cand &a, const Cand &b)
+{
+	return a.k1 < b.k1 || (a.k1 == b.k1 && a.k2 < b.k2);
+}
+
+__device__ __forceinline__ Cand warp_best(Cand c)
+{
+#pragma unroll
+	for (int o = 16; o; o >>= 1) {
+		Cand x;
+		x.k1 = __shfl_xor_sync(kFull, c.k1, o);
+		x.k2 = __shfl_xor_sync(kFull, c.k2, o);
+		if (cand_less(c, x))
+			c = x;
+	}
+	return c;
+}
+
+template <int H>
+__device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglong2 *tab,
+		uint64_t *cw, uint32_t *iw, unsigned long long *TA, unsigned long long *TB,
+		unsigned long long *TC, const uint8_t *__restrict__ s, uint64_t len, uint32_t &satc,
+		int lane)
+{
+	const uint32_t k = a.f.k, h = a.f.h, nids = a.f.nids, need = a.need;
+	const uint64_t kmask = (k >= 64) ? ~0ull : ((1ull << k) - 1);
+	if (len < k)
+		return;
+	for (uint64_t c0 = 0; c0 + k <= len; c0 += kStageBases - k + 1) {
+		__syncwarp();
+#pragma unroll 4
+		for (int it = 0; it < kStageBases / 32; ++it) {
+			const uint64_t pos = c0 + (uint64_t)it * 32 + lane;
+			const uint8_t c = base_code(pos < len ? s[pos] : (uint8_t)'N');
+			const uint32_t lo = __ballot_sync(kFull, c & 1u);
+			const uint32_t hi = __ballot_sync(kFull, (c >> 1) & 1u);
+			const uint32_t inv = __ballot_sync(kFull, c >> 2);
+			if (lane == it) {
+				cw[it] = spread_bits(lo) | (spread_bits(hi) << 1);
+				iw[it] = inv;
+			}
+		}
+		if (lane == 16) {
+			cw[16] = 0;
+			iw[16] = ~0u;
+		}
+		__syncwarp();
+		const uint64_t avail = len - c0 < (uint64_t)kStageBases ? len - c0 : kStageBases;
+		const uint32_t nfr = (uint32_t)avail - k + 1;
+		for (uint32_t q0 = 0; q0 < nfr; q0 += 32) {
+			const uint32_t q = q0 + lane;
+			bool ok = false;
+			uint64_t w = 0;
+			if (q < nfr) {
+				const uint32_t idx = q >> 5, sh = q & 31;
+				const uint64_t lo = cw[idx], hi = cw[idx + 1];
+				w = sh ? (lo >> (2 * sh)) | (hi << (64 - 2 * sh)) : lo;
+				const uint64_t inv = ((uint64_t)iw[idx] | ((uint64_t)iw[idx + 1] << 32)) >> sh;
+				ok = (inv & kmask) == 0;
+			}
+			uint64_t vals[H];
+			if (a.f.kmer_mode) {
+				const uint64_t c = ok ? seed_value(tab, w, k) : 0;
+				vals[0] = c;
+#pragma unroll
+				for (int v = 1; v < H; ++v)
+					vals[v] = extra_hash(c, k, v);
+			} else {
+#pragma unroll
+				for (int v = 0; v < H; ++v)
+					vals[v] = (ok && v < (int)h) ? seed_value(tab + v * 128, w, k) : 0;
+			}
+			/* block reads, all h in flight */
+			uint4 q0v[H], q1v[H];
+			uint32_t rr[H];
+			uint64_t blk[H];
+#pragma unroll
+			for (int v = 0; v < H; ++v) {
+				if (ok && v < (int)h) {
+					const uint64_t p = reduce(vals[v], a.f.m, a.f.minv);
+					blk[v] = p / kBlockBits;
+					rr[v] = (uint32_t)(p - blk[v] * kBlockBits);
+					q0v[v] = __ldg(a.f.blocks + 2 * blk[v]);
+					q1v[v] = __ldg(a.f.blocks + 2 * blk[v] + 1);
+				}
+			}
+			/* bit, rank, ID reads */
+			uint32_t e[H];
+			bool hit[H];
+#pragma unroll
+			for (int v = 0; v < H; ++v) {
+				hit[v] = false;
+				e[v] = 0;
+				if (ok && v < (int)h) {
+					const uint32_t d[7] = {q0v[v].y, q0v[v].z, q0v[v].w, q1v[v].x, q1v[v].y,
+							q1v[v].z, q1v[v].w};
+					const uint32_t ws = rr[v] >> 5, bit = rr[v] & 31u;
+					uint32_t acc = 0, word = 0;
+#pragma unroll
+					for (int i = 0; i < 7; ++i) {
+						if ((uint32_t)i < ws)
+							acc += __popc(d[i]);
+						if ((uint32_t)i == ws)
+							word = d[i];
+					}
+					if ((word >> bit) & 1u) {
+						acc += __popc(word & ((1u << bit) - 1u));
+						const uint64_t rank = a.f.super[blk[v] >> kSuperShift] + q0v[v].x + acc;
+						hit[v] = true;
+						e[v] = __ldg(a.f.ids + rank);
+					}
+				}
+			}
+			bool anysat = false;
+#pragma unroll
+			for (int v = 0; v < H; ++v)
+				anysat |= hit[v] && (e[v] & kMibfSat);
+			satc += __popc(__ballot_sync(kFull, anysat));
+			/* per-frame, per-ID records, merged across the warp */
+#pragma unroll
+			for (int r = 0; r < H; ++r) {
+				uint32_t key = 0xFFFFFFFFu, id = 0, hits = 0, nsh = 0;
+				if (hit[r]) {
+					id = e[r] & 0x7FFFu;
+					bool first = id != 0 && id < nids;
+#pragma unroll
+					for (int u = 0; u < r; ++u)
+						if (hit[u] && (e[u] & 0x7FFFu) == id)
+							first = false;
+					if (first) {
+#pragma unroll
+						for (int u = 0; u < H; ++u)
+							if (hit[u] && (e[u] & 0x7FFFu) == id) {
+								++hits;
+								nsh += (e[u] & kMibfSat) ? 0u : 1u;
+							}
+						key = id | (hits << 16) | (nsh << 21) | ((anysat ? 1u : 0u) << 26);
+					}
+				}
+				const uint32_t grp = __match_any_sync(kFull, key);
+				if (key != 0xFFFFFFFFu && lane == __ffs(grp) - 1) {
+					const unsigned long long n = (unsigned long long)__popc(grp);
+					const uint32_t cnt = hits >= need, ns = nsh >= need, sol = hits == h;
+					const uint32_t nsf = cnt && !anysat;
+					const unsigned long long ia = cnt | ((unsigned long long)ns << 32);
+					const unsigned long long ib = sol | ((unsigned long long)hits << 32);
+					const unsigned long long ic = nsh | ((unsigned long long)nsf << 32);
+					if (ia)
+						atomicAdd(TA + id, n * ia);
+					atomicAdd(TB + id, n * ib);
+					if (ic)
+						atomicAdd(TC + id, n * ic);
+				}
+			}
+		}
+	}
+	__syncwarp();
+}
+
+template <int H>
+__global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
+{
+	extern __shared__ __align__(16) unsigned char smem[];
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	const uint32_t nse = a.f.nse, T = a.T, nids = a.f.nids;
+	unsigned long long *tabw = reinterpret_cast<unsigned long long *>(smem);
+	for (uint32_t i = threadIdx.x; i < nse * 256; i += blockDim.x)
+		tabw[i] = a.tables[i];
+	unsigned char *wb = smem + (size_t)nse * 2048 + (size_t)wib * mibf_warp_bytes(T);
+	uint64_t *cw = reinterpret_cast<uint64_t *>(wb);
+	uint32_t *iw = reinterpret_cast<uint32_t *>(wb + 17 * 8);
+	unsigned long long *TA = reinterpret_cast<unsigned long long *>(wb + 17 * 8 + 18 * 4);
+	unsigned long long *TB = TA + T, *TC = TB + T;
+	for (uint32_t i = lane; i < 3 * T; i += 32)
+		TA[i] = 0;
+	__syncthreads();
+	const ulonglong2 *tab = reinterpret_cast<const ulonglong2 *>(smem);
+	const uint32_t k = a.f.k;
+	unsigned long long *above = a.counts, *unique = a.counts + (nids + 2);
+	for (;;) {
+		unsigned long long r0 = 0;
+		if (lane == 0)
+			r0 = atomicAdd(a.work, (unsigned long long)kReadsPerGrab);
+		r0 = __shfl_sync(kFull, r0, 0);
+		if (r0 >= a.n_reads)
+			break;
+		const uint64_t r1 = r0 + kReadsPerGrab < a.n_reads ? r0 + kReadsPerGrab : a.n_reads;
+		for (uint64_t r = r0; r < r1; ++r) {
+			const uint64_t b1 = a.off[r], len1 = a.off[r + 1] - b1;
+			uint64_t b2 = 0, len2 = 0;
+			if (a.seq2) {
+				b2 = a.off2[r];
+				len2 = a.off2[r + 1] - b2;
+			}
+			/* frameCount (MIBFClassifier.hpp:774, 802-803) */
+			const uint32_t fc = len1 >= k ? (uint32_t)(len1 - k + 1)
+					: (len2 >= k ? (uint32_t)(len2 - k + 1) : 0u);
+			uint32_t satc = 0;
+			if (fc) {
+				mibf_scan_mate<H>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1, satc, lane);
+				if (a.seq2)
+					mibf_scan_mate<H>(a, tab, cw, iw, TA, TB, TC, a.seq2 + b2, len2, satc,
+							lane);
+			}
+			/* significant IDs */
+			uint32_t cmask = 0, maxns = 0;
+			Cand best = {0ull, 0ull};
+			if (fc) {
+				const uint32_t *mrow = a.minc + (size_t)fc * nids;
+				for (uint32_t j = 0; j < T / 32; ++j) {
+					const uint32_t s = lane + 32 * j;
+					const unsigned long long A = TA[s];
+					const uint32_t cnt = (uint32_t)A, ns = (uint32_t)(A >> 32);
+					if (s >= 1 && s < nids && cnt > 0 && cnt >= __ldg(mrow + s) &&
+							(a.min_nonsat == 0 || ns >= a.min_nonsat)) {
+						cmask |= 1u << j;
+						Cand c = {A, ((TB[s] >> 32) << 32) | (0xFFFFFFFFull - s)};
+						if (cand_less(best, c))
+							best = c;
+						maxns = ns > maxns ? ns : maxns;
+					}
+				}
+			}
+			best = warp_best(best);
+			maxns = __reduce_max_sync(kFull, maxns);
+			uint32_t n_out = 0;
+			if (best.k1 && !(a.best_agree && maxns > (uint32_t)(best.k1 >> 32))) {
+				const double thr = (double)(uint32_t)best.k1 - a.multi;
+				Cand cur = best;
+				for (;;) {
+					const uint32_t id = 0xFFFFFFFFu - (uint32_t)cur.k2;
+					if (lane == 0) {
+						if (n_out < a.max_hits) {
+							const unsigned long long A = TA[id], B = TB[id], C = TC[id];
+							bbt_mibf_hit o;
+							o.id = id;
+							o.nonSatFrameCount = (uint32_t)(C >> 32);
+							o.solidCount = (uint32_t)B;
+							o.count = (uint32_t)A;
+							o.nonSatCount = (uint32_t)(A >> 32);
+							o.totalNonSatCount = (uint32_t)C;
+							o.totalCount = (uint32_t)(B >> 32);
+							a.hits[r * a.max_hits + n_out] = o;
+						}
+						atomicAdd(above + id, 1ull);
+					}
+					++n_out;
+					/* next: the best candidate below cur that passes the threshold */
+					Cand nx = {0ull, 0ull};
+					for (uint32_t j = 0; j < T / 32; ++j) {
+						if (!((cmask >> j) & 1u))
+							continue;
+						const uint32_t s = lane + 32 * j;
+						const unsigned long long A = TA[s];
+						Cand c = {A, ((TB[s] >> 32) << 32) | (0xFFFFFFFFull - s)};
+						if (cand_less(c, cur) && (double)(uint32_t)A > thr && cand_less(nx, c))
+							nx = c;
+					}
+					nx = warp_best(nx);
+					if (!nx.k1)
+						break;
+					cur = nx;
+				}
+			}
+			if (lane == 0) {
+				a.n_hits[r] = n_out;
+				a.sat[r] = satc;
+				if (n_out > a.max_hits)
+					atomicOr(a.flags, 1u);
+				if (n_out == 0) {
+					if (!a.skip_empty_summary)
+						atomicAdd(a.counts + 2 * (nids + 2) + 1, 1ull);
+				} else if (n_out == 1) {
+					atomicAdd(unique + (0xFFFFFFFFu - (uint32_t)best.k2), 1ull);
+				} else {
+					atomicAdd(a.counts + 2 * (nids + 2), 1ull);
+				}
+			}
+			__syncwarp();
+			for (uint32_t j = 0; j < T / 32; ++j) {
+				const uint32_t s = lane + 32 * j;
+				TA[s] = 0;
+				TB[s] = 0;
+				TC[s] = 0;
+			}
+			__syncwarp();
+		}
+	}
+}
+
+/* Add a batch's summary counters to the context's, unless a read of the
+ * batch overflowed its result slots (the caller then runs the batch again). */
+__global__ void mibf_commit_kernel(const unsigned long long *batch, unsigned long long *total,
+		uint32_t n, const unsigned int *flags, uint64_t reads)
+{
+	if (flags[0])
+		return;
+	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+		total[i] += batch[i];
+	if (blockIdx.x == 0 && threadIdx.x == 0)
+		total[n] += reads;
+}
+
+/* Largest frame count of a device batch and a bitmap of the frame counts
+ * below 65536 that occur. */
+__global__ void mibf_frame_counts_kernel(const uint64_t *off, const uint64_t *off2, uint64_t n,
+		uint32_t k, unsigned int *out)
+{
+	for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n;
+			r += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t l1 = off[r + 1] - off[r];
+		const uint64_t l2 = off2 ? off2[r + 1] - off2[r] : 0;
+		const uint64_t f64 = l1 >= k ? l1 - k + 1 : (l2 >= k ? l2 - k + 1 : 0);
+		const uint32_t fc = f64 > 0xFFFFFFFFull ? 0xFFFFFFFFu : (uint32_t)f64;
+		atomicMax(out, fc);
+		if (fc < 65536u)
+			atomicOr(out + 1 + (fc >> 5), 1u << (fc & 31));
+	}
+}
+
+/* Block popcounts of the raw bit vector (words of 32 bits). */
+__global__ void mibf_block_pop_kernel(const uint32_t *raw, uint64_t nwords, uint64_t nblocks,
+		unsigned long long *pop)
+{
+	for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < nblocks;
+			b += (uint64_t)gridDim.x * blockDim.x) {
+		unsigned c = 0;
+		for (int i = 0; i < 7; ++i) {
+			const uint64_t w = b * 7 + i;
+			c += w < nwords ? __popc(raw[w]) : 0;
+		}
+		pop[b] = c;
+	}
+}
+
+/* Blocks from the raw words and the exclusive scan of block popcounts. */
+__global__ void mibf_block_build_kernel(const uint32_t *raw, uint64_t nwords, uint64_t nblocks,
+		const unsigned long long *rank, unsigned long long *super, uint4 *blocks)
+{
+	for (uint64_t b = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; b < nblocks;
+			b += (uint64_t)gridDim.x * blockDim.x) {
+		uint32_t d[7];
+		for (int i = 0; i < 7; ++i) {
+			const uint64_t w = b * 7 + i;
+			d[i] = w < nwords ? raw[w] : 0u;
+		}
+		const uint64_t sb = b >> kSuperShift;
+		if ((b & ((1ull << kSuperShift) - 1)) == 0)
+			super[sb] = rank[b];
+		const unsigned long long base = rank[b & ~((1ull << kSuperShift) - 1)];
+		blocks[2 * b] = make_uint4((uint32_t)(rank[b] - base), d[0], d[1], d[2]);
+		blocks[2 * b + 1] = make_uint4(d[3], d[4], d[5], d[6]);
+	}
+}
+
+} // namespace bbt
+
+using namespace bbt;
+
+#define MIBF_TRY(ctx, call)                                                                \
+	do {                                                                                   \
+		cudaError_t e_ = (call);                                                           \
+		if (e_ != cudaSuccess)                                                             \
+			return mibf_fail((ctx), e_ == cudaErrorMemoryAllocation ? BBT_ERR_NOMEM        \
+					: BBT_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));  \
+	} while (0)
+
+static uint32_t tally_slots(uint32_t nids)
+{
+	return (nids + 31) & ~31u;
+}
+
+static int pick_h(unsigned h)
+{
+	return h <= 1 ? 1 : h <= 2 ? 2 : h <= 3 ? 3 : h <= 4 ? 4 : h <= 6 ? 6 : h <= 8 ? 8 : 16;
+}
+
+template <int H>
+static cudaError_t launch_h(const MibfArgs &a, int grid, size_t smem, cudaStream_t s)
+{
+	mibf_query_kernel<H><<<grid, 128, smem, s>>>(a);
+	return cudaGetLastError();
+}
+
+/* Blocks per SM of the H variant with smem bytes of shared memory (also sets
+ * the variant's shared-memory limit, which must precede its launch). */
+template <int H>
+static int occupancy_h(size_t smem)
+{
+	cudaFuncSetAttribute(mibf_query_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			(int)smem);
+	int nb = 0;
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mibf_query_kernel<H>, 128, smem);
+	return nb > 0 ? nb : 1;
+}
+
+static cudaError_t launch_query(const MibfArgs &a, int hsel, int grid, size_t smem,
+		cudaStream_t s)
+{
+	switch (hsel) {
+	case 1: return launch_h<1>(a, grid, smem, s);
+	case 2: return launch_h<2>(a, grid, smem, s);
+	case 3: return launch_h<3>(a, grid, smem, s);
+	case 4: return launch_h<4>(a, grid, smem, s);
+	case 6: return launch_h<6>(a, grid, smem, s);
+	case 8: return launch_h<8>(a, grid, smem, s);
+	default: return launch_h<16>(a, grid, smem, s);
+	}
+}
+
+static int query_occupancy(int hsel, size_t smem)
+{
+	switch (hsel) {
+	case 1: return occupancy_h<1>(smem);
+	case 2: return occupancy_h<2>(smem);
+	case 3: return occupancy_h<3>(smem);
+	case 4: return occupancy_h<4>(smem);
+	case 6: return occupancy_h<6>(smem);
+	case 8: return occupancy_h<8>(smem);
+	default: return occupancy_h<16>(smem);
+	}
+}
+
+/* Upload the bit vector and build the rank blocks. */
+static int upload_bits(bbt_mibf *ctx, const std::string &sdsl)
+{
+	const uint64_t m = ctx->hd.m, nwords = m / 32, bytes = m / 8;
+	FILE *f = fopen(sdsl.c_str(), "rb");
+	if (!f)
+		return mibf_fail(ctx, BBT_ERR_IO, "Error: " + sdsl + " File cannot be opened");
+	uint32_t *d_raw = nullptr;
+	cudaError_t e = cudaMalloc(&d_raw, bytes);
+	if (e != cudaSuccess) {
+		fclose(f);
+		return mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(bit vector)");
+	}
+	std::vector<char> buf(std::min<uint64_t>(bytes, 64ull << 20));
+	int rc = BBT_OK;
+	for (uint64_t done = 0; done < bytes && rc == BBT_OK;) {
+		const size_t n = (size_t)std::min<uint64_t>(buf.size(), bytes - done);
+		if (fread(buf.data(), 1, n, f) != n)
+			rc = mibf_fail(ctx, BBT_ERR_FORMAT, sdsl + ": shorter than BitVectorSize / 8");
+		else if (cudaMemcpy((char *)d_raw + done, buf.data(), n, cudaMemcpyHostToDevice) !=
+				cudaSuccess)
+			rc = mibf_fail(ctx, BBT_ERR_CUDA, "cudaMemcpy(bit vector)");
+		done += n;
+	}
+	fclose(f);
+	const uint64_t nblocks = (m + kBlockBits - 1) / kBlockBits;
+	const uint64_t nsuper = (nblocks >> kSuperShift) + 1;
+	unsigned long long *d_pop = nullptr, *d_rank = nullptr;
+	void *d_tmp = nullptr;
+	size_t tmp_bytes = 0;
+	if (rc == BBT_OK) {
+		if (cudaMalloc(&d_pop, nblocks * 8) != cudaSuccess ||
+				cudaMalloc(&d_rank, nblocks * 8) != cudaSuccess ||
+				cudaMalloc(&ctx->d_blocks, nblocks * 32) != cudaSuccess ||
+				cudaMalloc(&ctx->d_super, nsuper * 8) != cudaSuccess)
+			rc = mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(rank blocks)");
+	}
+	if (rc == BBT_OK) {
+		const int grid = ctx->num_sms * 8;
+		mibf_block_pop_kernel<<<grid, 256>>>(d_raw, nwords, nblocks, d_pop);
+		cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_pop, d_rank, (int64_t)nblocks);
+		if (cudaMalloc(&d_tmp, tmp_bytes) != cudaSuccess)
+			rc = mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(scan)");
+		else {
+			cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_pop, d_rank, (int64_t)nblocks);
+			mibf_block_build_kernel<<<grid, 256>>>(d_raw, nwords, nblocks, d_rank, ctx->d_super,
+					ctx->d_blocks);
+			e = cudaDeviceSynchronize();
+			if (e != cudaSuccess)
+				rc = mibf_fail(ctx, BBT_ERR_CUDA, std::string("rank blocks: ") +
+						cudaGetErrorString(e));
+		}
+	}
+	cudaFree(d_tmp);
+	cudaFree(d_pop);
+	cudaFree(d_rank);
+	cudaFree(d_raw);
+	return rc;
+}
+
+extern "C" int bbt_mibf_close(bbt_mibf *ctx)
+{
+	if (!ctx)
+		return BBT_OK;
+	if (!ctx->host_only) {
+		cudaSetDevice(ctx->dev);
+		cudaFree(ctx->d_blocks);
+		cudaFree(ctx->d_super);
+		cudaFree(ctx->d_ids);
+		cudaFree(ctx->d_tables);
+		cudaFree(ctx->d_counts);
+		cudaFree(ctx->d_work);
+		cudaFree(ctx->d_flags);
+		cudaFree(ctx->d_minc);
+		cudaFree(ctx->d_fcmax);
+		for (int i = 0; i < 2; ++i) {
+			cudaFree(ctx->d_seq[i]);
+			cudaFree(ctx->d_off[i]);
+		}
+		cudaFree(ctx->d_hits);
+		cudaFree(ctx->d_nhits);
+		cudaFree(ctx->d_sat);
+		if (ctx->ev0)
+			cudaEventDestroy(ctx->ev0);
+		if (ctx->ev1)
+			cudaEventDestroy(ctx->ev1);
+		if (ctx->stream)
+			cudaStreamDestroy(ctx->stream);
+	}
+	delete ctx;
+	return BBT_OK;
+}
+
+static size_t counts_len(const bbt_mibf *ctx)
+{
+	return 2 * (ctx->names.size() + 2) + 2;
+}
+
+extern "C" int bbt_mibf_open(const char *bf_path, const bbt_mibf_params *params, bbt_mibf **out)
+{
+	if (!out || !bf_path)
+		return mibf_fail(nullptr, BBT_ERR_ARG, "bbt_mibf_open: need a path and an out pointer");
+	*out = nullptr;
+	int ndev = 0;
+	if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+		return mibf_fail(nullptr, BBT_ERR_NODEVICE, "no CUDA device is available");
+	bbt_mibf *ctx = new bbt_mibf();
+	if (params)
+		ctx->p = *params;
+	else
+		bbt_mibf_default_params(&ctx->p);
+	ctx->dev = ctx->p.device;
+	auto bail = [&](int rc) {
+		mibf_fail(nullptr, rc, ctx->err);
+		bbt_mibf_close(ctx);
+		return rc;
+	};
+	if (cudaSetDevice(ctx->dev) != cudaSuccess) {
+		ctx->host_only = true;
+		mibf_fail(ctx, BBT_ERR_NODEVICE, "cannot use CUDA device " + std::to_string(ctx->dev));
+		return bail(BBT_ERR_NODEVICE);
+	}
+	cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, ctx->dev);
+	std::vector<uint16_t> ids;
+	int rc = mibf_load_host(ctx, bf_path, &ids);
+	if (rc)
+		return bail(rc);
+	if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+			cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
+		return bail(mibf_fail(ctx, BBT_ERR_CUDA, "cannot create a stream"));
+	rc = upload_bits(ctx, mibf_sdsl_path(bf_path));
+	if (rc)
+		return bail(rc);
+	const uint64_t nid = ctx->hd.pop ? ctx->hd.pop : 1;
+	if (cudaMalloc(&ctx->d_ids, nid * 2) != cudaSuccess)
+		return bail(mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(IDs)"));
+	if (ctx->hd.pop && cudaMemcpy(ctx->d_ids, ids.data(), ctx->hd.pop * 2,
+			cudaMemcpyHostToDevice) != cudaSuccess)
+		return bail(mibf_fail(ctx, BBT_ERR_CUDA, "cudaMemcpy(IDs)"));
+	std::vector<uint16_t>().swap(ids);
+	std::vector<unsigned long long> tabs = mibf_seed_tables(ctx->hd.seeds, ctx->hd.k);
+	const size_t nc = counts_len(ctx) + 1; /* + reads */
+	if (cudaMalloc(&ctx->d_tables, tabs.size() * 8) != cudaSuccess ||
+			cudaMalloc(&ctx->d_counts, 2 * nc * 8) != cudaSuccess ||
+			cudaMalloc(&ctx->d_work, 8) != cudaSuccess ||
+			cudaMalloc(&ctx->d_flags, 4) != cudaSuccess ||
+			cudaMalloc(&ctx->d_fcmax, (1 + 2048) * 4) != cudaSuccess)
+		return bail(mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(context)"));
+	cudaMemcpy(ctx->d_tables, tabs.data(), tabs.size() * 8, cudaMemcpyHostToDevice);
+	cudaMemset(ctx->d_counts, 0, 2 * nc * 8);
+	if (cudaDeviceSynchronize() != cudaSuccess)
+		return bail(mibf_fail(ctx, BBT_ERR_CUDA, "loading the miBF failed"));
+	*out = ctx;
+	return BBT_OK;
+}
+
+/* Make minCount rows present for the frame counts in fcs (sorted, unique). */
+static int ensure_min_count(bbt_mibf *ctx, const std::vector<uint32_t> &fcs, cudaStream_t s)
+{
+	if (fcs.empty())
+		return BBT_OK;
+	const unsigned nids = (unsigned)ctx->names.size();
+	const uint32_t need_rows = fcs.back() + 1;
+	std::lock_guard<std::mutex> lk(ctx->mc_mu);
+	if (ctx->minc_have.size() < need_rows) {
+		ctx->minc_have.resize(need_rows, 0);
+		ctx->h_minc.resize((size_t)need_rows * nids, 0);
+	}
+	std::vector<uint32_t> missing;
+	for (uint32_t fc : fcs)
+		if (fc && !ctx->minc_have[fc])
+			missing.push_back(fc);
+	if (missing.empty() && ctx->minc_rows >= need_rows)
+		return BBT_OK;
+	const long long nm = (long long)missing.size();
+#pragma omp parallel for schedule(dynamic, 16)
+	for (long long t = 0; t < nm * (long long)nids; ++t) {
+		const uint32_t fc = missing[t / nids];
+		const unsigned id = (unsigned)(t % nids);
+		ctx->h_minc[(size_t)fc * nids + id] = id == 0 ? 0u
+				: mibf_min_count(fc, ctx->frame_prob[id], ctx->p.score, nids);
+	}
+	for (uint32_t fc : missing)
+		ctx->minc_have[fc] = 1;
+	if (ctx->minc_rows < need_rows) {
+		uint32_t rows = std::max<uint32_t>(need_rows, ctx->minc_rows * 2);
+		rows = std::max<uint32_t>(rows, 256);
+		uint32_t *d = nullptr;
+		MIBF_TRY(ctx, cudaMalloc(&d, (size_t)rows * nids * 4));
+		MIBF_TRY(ctx, cudaStreamSynchronize(s));
+		cudaFree(ctx->d_minc);
+		ctx->d_minc = d;
+		ctx->minc_rows = rows;
+		if (ctx->h_minc.size() < (size_t)rows * nids) {
+			ctx->h_minc.resize((size_t)rows * nids, 0);
+			ctx->minc_have.resize(rows, 0);
+		}
+		MIBF_TRY(ctx, cudaMemcpyAsync(d, ctx->h_minc.data(), (size_t)rows * nids * 4,
+				cudaMemcpyHostToDevice, s));
+		MIBF_TRY(ctx, cudaStreamSynchronize(s));
+		return BBT_OK;
+	}
+	for (uint32_t fc : missing)
+		MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_minc + (size_t)fc * nids,
+				ctx->h_minc.data() + (size_t)fc * nids, nids * 4, cudaMemcpyHostToDevice, s));
+	MIBF_TRY(ctx, cudaStreamSynchronize(s));
+	return BBT_OK;
+}
+
+static std::vector<uint32_t> host_frame_counts(const bbt_batch *b, unsigned k)
+{
+	std::vector<uint32_t> fcs;
+	std::vector<uint8_t> seen;
+	for (uint64_t r = 0; r < b->n_reads; ++r) {
+		const uint64_t l1 = b->offsets[r + 1] - b->offsets[r];
+		const uint64_t l2 = b->seq2 ? b->offsets2[r + 1] - b->offsets2[r] : 0;
+		const uint64_t fc = l1 >= k ? l1 - k + 1 : (l2 >= k ? l2 - k + 1 : 0);
+		if (fc >= seen.size())
+			seen.resize(fc + 1, 0);
+		if (!seen[fc]) {
+			seen[fc] = 1;
+			fcs.push_back((uint32_t)fc);
+		}
+	}
+	std::sort(fcs.begin(), fcs.end());
+	return fcs;
+}
+
+static int device_frame_counts(bbt_mibf *ctx, const bbt_batch *b, cudaStream_t s,
+		std::vector<uint32_t> &fcs)
+{
+	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_fcmax, 0, (1 + 2048) * 4, s));
+	mibf_frame_counts_kernel<<<ctx->num_sms * 4, 256, 0, s>>>(b->offsets,
+			b->seq2 ? b->offsets2 : nullptr, b->n_reads, ctx->hd.k, ctx->d_fcmax);
+	std::vector<unsigned int> h(1 + 2048);
+	MIBF_TRY(ctx, cudaMemcpyAsync(h.data(), ctx->d_fcmax, h.size() * 4, cudaMemcpyDeviceToHost,
+			s));
+	MIBF_TRY(ctx, cudaStreamSynchronize(s));
+	const uint32_t mx = h[0];
+	for (uint32_t fc = 0; fc < 65536 && fc <= mx; ++fc)
+		if ((h[1 + (fc >> 5)] >> (fc & 31)) & 1u)
+			fcs.push_back(fc);
+	if (mx >= 65536) /* rare: rows for every longer count up to the maximum */
+		for (uint32_t fc = 65536; fc <= mx; ++fc)
+			fcs.push_back(fc);
+	return BBT_OK;
+}
+
+static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, const uint64_t *off,
+		const uint8_t *seq2, const uint64_t *off2, bbt_mibf_hit *hits, uint32_t max_hits,
+		uint32_t *n_hits, uint32_t *sat, cudaStream_t s)
+{
+	const unsigned nids = (unsigned)ctx->names.size();
+	const size_t nc = counts_len(ctx);
+	unsigned long long *batch_counts = ctx->d_counts + nc + 1;
+	MibfArgs a;
+	a.f.blocks = ctx->d_blocks;
+	a.f.super = ctx->d_super;
+	a.f.ids = ctx->d_ids;
+	a.f.m = ctx->hd.m;
+	a.f.minv = ~0ull / ctx->hd.m;
+	a.f.h = ctx->hd.h;
+	a.f.k = ctx->hd.k;
+	a.f.kmer_mode = ctx->hd.seeds.empty();
+	a.f.nse = a.f.kmer_mode ? 1 : ctx->hd.h;
+	a.f.nids = nids;
+	a.seq = seq;
+	a.off = off;
+	a.seq2 = seq2;
+	a.off2 = off2;
+	a.n_reads = b->n_reads;
+	a.minc = ctx->d_minc;
+	a.need = ctx->need;
+	a.min_nonsat = ctx->p.min_nonsat;
+	a.best_agree = ctx->p.best_hit_agree;
+	a.skip_empty_summary = (seq2 && ctx->p.hit_only) ? 1 : 0;
+	a.multi = ctx->p.multi_thresh;
+	a.tables = ctx->d_tables;
+	a.hits = hits;
+	a.max_hits = max_hits;
+	a.n_hits = n_hits;
+	a.sat = sat;
+	a.counts = batch_counts;
+	a.work = ctx->d_work;
+	a.flags = ctx->d_flags;
+	a.T = tally_slots(nids);
+	const int hsel = pick_h(ctx->hd.h);
+	const size_t smem = mibf_smem_bytes(a.f.nse, a.T, 4);
+	const int grid = ctx->num_sms * query_occupancy(hsel, smem);
+	MIBF_TRY(ctx, cudaMemsetAsync(batch_counts, 0, nc * 8, s));
+	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, 8, s));
+	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_flags, 0, 4, s));
+	MIBF_TRY(ctx, cudaEventRecord(ctx->ev0, s));
+	if (b->n_reads)
+		MIBF_TRY(ctx, launch_query(a, hsel, grid, smem, s));
+	MIBF_TRY(ctx, cudaEventRecord(ctx->ev1, s));
+	mibf_commit_kernel<<<1, 256, 0, s>>>(batch_counts, ctx->d_counts, (uint32_t)nc,
+			ctx->d_flags, b->n_reads);
+	MIBF_TRY(ctx, cudaGetLastError());
+	return BBT_OK;
+}
+
+static int grow_staging(bbt_mibf *ctx, uint64_t bases, uint64_t reads, uint32_t max_hits)
+{
+	if (bases > ctx->cap_bases || reads > ctx->cap_reads) {
+		const uint64_t nb = std::max<uint64_t>(bases, ctx->cap_bases);
+		const uint64_t nr = std::max<uint64_t>(reads, ctx->cap_reads);
+		for (int i = 0; i < 2; ++i) {
+			cudaFree(ctx->d_seq[i]);
+			cudaFree(ctx->d_off[i]);
+			ctx->d_seq[i] = nullptr;
+			ctx->d_off[i] = nullptr;
+			MIBF_TRY(ctx, cudaMalloc(&ctx->d_seq[i], std::max<uint64_t>(nb, 16)));
+			MIBF_TRY(ctx, cudaMalloc(&ctx->d_off[i], (nr + 1) * 8));
+		}
+		ctx->cap_bases = nb;
+		ctx->cap_reads = nr;
+	}
+	if (reads > ctx->res_cap_reads || max_hits > ctx->res_cap_hits ||
+			(uint64_t)reads * max_hits > (uint64_t)ctx->res_cap_reads * ctx->res_cap_hits) {
+		const uint64_t nr = std::max<uint64_t>(reads, ctx->res_cap_reads);
+		const uint32_t nh = std::max<uint32_t>(max_hits, ctx->res_cap_hits);
+		cudaFree(ctx->d_hits);
+		cudaFree(ctx->d_nhits);
+		cudaFree(ctx->d_sat);
+		ctx->d_hits = nullptr;
+		ctx->d_nhits = ctx->d_sat = nullptr;
+		MIBF_TRY(ctx, cudaMalloc(&ctx->d_hits, std::max<uint64_t>(nr * nh, 1) *
+				sizeof(bbt_mibf_hit)));
+		MIBF_TRY(ctx, cudaMalloc(&ctx->d_nhits, std::max<uint64_t>(nr, 1) * 4));
+		MIBF_TRY(ctx, cudaMalloc(&ctx->d_sat, std::max<uint64_t>(nr, 1) * 4));
+		ctx->res_cap_reads = nr;
+		ctx->res_cap_hits = nh;
+	}
+	return BBT_OK;
+}
+
+extern "C" int bbt_mibf_classify_batch(bbt_mibf *ctx, const bbt_batch *b, bbt_mibf_result *res,
+		void *stream)
+{
+	if (!ctx || !b || !res)
+		return mibf_fail(ctx, BBT_ERR_ARG, "bbt_mibf_classify_batch: NULL argument");
+	if (ctx->host_only)
+		return mibf_fail(ctx, BBT_ERR_ARG, "context was opened without a device");
+	if (b->n_reads && (!b->seq || !b->offsets || (b->seq2 && !b->offsets2)))
+		return mibf_fail(ctx, BBT_ERR_ARG, "bbt_mibf_classify_batch: batch arrays missing");
+	if (!res->n_hits || !res->sat_count || (res->max_hits && !res->hits))
+		return mibf_fail(ctx, BBT_ERR_ARG, "bbt_mibf_classify_batch: result arrays missing");
+	if (res->location != b->location)
+		return mibf_fail(ctx, BBT_ERR_ARG, "batch and result must live on the same side");
+	MIBF_TRY(ctx, cudaSetDevice(ctx->dev));
+	cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+	int rc;
+	if (b->location == BBT_DEVICE) {
+		std::vector<uint32_t> fcs;
+		rc = device_frame_counts(ctx, b, s, fcs);
+		if (rc)
+			return rc;
+		rc = ensure_min_count(ctx, fcs, s);
+		if (rc)
+			return rc;
+		return run_query(ctx, b, (const uint8_t *)b->seq, b->offsets, (const uint8_t *)b->seq2,
+				b->offsets2, res->hits, res->max_hits, res->n_hits, res->sat_count, s);
+	}
+	/* host batch: stage in, classify, copy out */
+	const uint64_t n = b->n_reads;
+	const uint64_t s1 = n ? b->offsets[0] : 0, e1 = n ? b->offsets[n] : 0;
+	const uint64_t s2 = (n && b->seq2) ? b->offsets2[0] : 0;
+	const uint64_t e2 = (n && b->seq2) ? b->offsets2[n] : 0;
+	rc = grow_staging(ctx, std::max(e1 - s1, e2 - s2), n, res->max_hits);
+	if (rc)
+		return rc;
+	rc = ensure_min_count(ctx, host_frame_counts(b, ctx->hd.k), s);
+	if (rc)
+		return rc;
+	std::vector<uint64_t> o1(n + 1), o2(b->seq2 ? n + 1 : 0);
+	for (uint64_t i = 0; i <= n; ++i)
+		o1[i] = b->offsets[i] - s1;
+	if (b->seq2)
+		for (uint64_t i = 0; i <= n; ++i)
+			o2[i] = b->offsets2[i] - s2;
+	if (n) {
+		MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_seq[0], b->seq + s1, e1 - s1, cudaMemcpyHostToDevice,
+				s));
+		MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_off[0], o1.data(), (n + 1) * 8,
+				cudaMemcpyHostToDevice, s));
+		if (b->seq2) {
+			MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_seq[1], b->seq2 + s2, e2 - s2,
+					cudaMemcpyHostToDevice, s));
+			MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_off[1], o2.data(), (n + 1) * 8,
+					cudaMemcpyHostToDevice, s));
+		}
+	}
+	rc = run_query(ctx, b, ctx->d_seq[0], ctx->d_off[0], b->seq2 ? ctx->d_seq[1] : nullptr,
+			b->seq2 ? ctx->d_off[1] : nullptr, ctx->d_hits, res->max_hits, ctx->d_nhits,
+			ctx->d_sat, s);
+	if (rc)
+		return rc;
+	unsigned int flag = 0;
+	if (n) {
+		MIBF_TRY(ctx, cudaMemcpyAsync(res->n_hits, ctx->d_nhits, n * 4, cudaMemcpyDeviceToHost, s));
+		MIBF_TRY(ctx, cudaMemcpyAsync(res->sat_count, ctx->d_sat, n * 4, cudaMemcpyDeviceToHost,
+				s));
+		if (res->max_hits)
+			MIBF_TRY(ctx, cudaMemcpyAsync(res->hits, ctx->d_hits,
+					n * res->max_hits * sizeof(bbt_mibf_hit), cudaMemcpyDeviceToHost, s));
+	}
+	MIBF_TRY(ctx, cudaMemcpyAsync(&flag, ctx->d_flags, 4, cudaMemcpyDeviceToHost, s));
+	MIBF_TRY(ctx, cudaStreamSynchronize(s));
+	float ms = 0;
+	cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+	ctx->last_kernel_ms = ms;
+	if (flag)
+		return mibf_fail(ctx, BBT_ERR_OVERFLOW, "a read has more significant IDs than max_hits");
+	return BBT_OK;
+}
+
+extern "C" int bbt_mibf_sync(bbt_mibf *ctx)
+{
+	if (!ctx || ctx->host_only)
+		return BBT_ERR_ARG;
+	MIBF_TRY(ctx, cudaSetDevice(ctx->dev));
+	MIBF_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+	MIBF_TRY(ctx, cudaDeviceSynchronize());
+	float ms = 0;
+	if (cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1) == cudaSuccess)
+		ctx->last_kernel_ms = ms;
+	unsigned int flag = 0;
+	MIBF_TRY(ctx, cudaMemcpy(&flag, ctx->d_flags, 4, cudaMemcpyDeviceToHost));
+	if (flag)
+		return mibf_fail(ctx, BBT_ERR_OVERFLOW, "a read has more significant IDs than max_hits");
+	return BBT_OK;
+}
+
+extern "C" int bbt_mibf_summary(bbt_mibf *ctx, uint64_t *counts, uint64_t *reads)
+{
+	if (!ctx || ctx->host_only)
+		return BBT_ERR_ARG;
+	MIBF_TRY(ctx, cudaSetDevice(ctx->dev));
+	const size_t nc = counts_len(ctx);
+	std::vector<uint64_t> h(nc + 1);
+	MIBF_TRY(ctx, cudaDeviceSynchronize());
+	MIBF_TRY(ctx, cudaMemcpy(h.data(), ctx->d_counts, (nc + 1) * 8, cudaMemcpyDeviceToHost));
+	if (counts)
+		memcpy(counts, h.data(), nc * 8);
+	if (reads)
+		*reads = h[nc];
+	return BBT_OK;
+}
+
+extern "C" int bbt_mibf_reset_summary(bbt_mibf *ctx)
+{
+	if (!ctx || ctx->host_only)
+		return BBT_ERR_ARG;
+	MIBF_TRY(ctx, cudaSetDevice(ctx->dev));
+	MIBF_TRY(ctx, cudaDeviceSynchronize());
+	MIBF_TRY(ctx, cudaMemset(ctx->d_counts, 0, (counts_len(ctx) + 1) * 8));
+	return BBT_OK;
+}
+
+extern "C" int bbt_mibf_summary_tsv(bbt_mibf *ctx, uint64_t read_count, char *buf, size_t cap,
+		size_t *len)
+{
+	std::vector<uint64_t> c(counts_len(ctx));
+	int rc = bbt_mibf_summary(ctx, c.data(), nullptr);
+	if (rc)
+		return rc;
+	std::string s = mibf_summary_text(ctx->names, c, read_count);
+	if (len)
+		*len = s.size();
+	if (buf && cap) {
+		size_t n = std::min(cap - 1, s.size());
+		memcpy(buf, s.data(), n);
+		buf[n] = 0;
+	}
+	return BBT_OK;
+}
+
+/* Device time of the last batch's query kernel, in ms. */
+extern "C" double bbt_mibf_last_kernel_ms(bbt_mibf *ctx)
+{
+	return ctx ? ctx->last_kernel_ms : 0.0;
+}

@@ -1,0 +1,118 @@
+/*
+ * mibf_ctx.hpp -- the multi-index Bloom filter context behind bbt_mibf.h, and
+ * the host-side pieces shared by the device code, the file pipeline and the
+ * maker.
+ */
+#ifndef BBT_MIBF_CTX_HPP
+#define BBT_MIBF_CTX_HPP
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "bbt_mibf.h"
+
+namespace bbt {
+
+constexpr unsigned kMibfMaxSeeds = 16;
+constexpr unsigned kMibfMaxK = 32;
+constexpr unsigned kMibfMaxIds = 1024;   /* per-read tally table of the query kernel */
+constexpr uint16_t kMibfSat = 0x8000u;
+
+/* Header of a "<p>.bf" miBF file. */
+struct MibfHeader {
+	uint64_t m = 0;
+	unsigned h = 0;
+	unsigned k = 0;
+	unsigned id_width = 16;
+	uint64_t pop = 0;
+	std::vector<std::string> seeds;
+};
+
+/* Parse the text header of an open "<p>.bf"; leaves the stream at the IDs.
+ * Returns an empty string or an error message. */
+std::string read_mibf_header(FILE *f, MibfHeader &h);
+int write_mibf_header(FILE *f, const MibfHeader &h);
+
+/* "<p>_ids.txt" of "<p>.bf" (MIBFClassifier.hpp:52-53). */
+std::string mibf_ids_path(const std::string &bf_path);
+/* "<p>.sdsl" of "<p>.bf". */
+std::string mibf_sdsl_path(const std::string &bf_path);
+
+/* m_fullIDs: "repeat", then the second field of each ID-file line, in order
+ * (MIBFClassifier.hpp:64-77). */
+bool read_mibf_names(const std::string &path, std::vector<std::string> &names);
+
+/* P(at least need of h values hit an ID) for per-value probability p. */
+double mibf_frame_prob(double p, unsigned h, unsigned need);
+/* Binomial(n, p): smallest x with P(X > x) <= q, from the top of the tail. */
+unsigned binom_upper_quantile(unsigned n, double p, double q);
+unsigned mibf_min_count(unsigned frame_count, double frame_prob, double score, unsigned num_ids);
+
+/* Per-value seed tables of the query and build kernels: for seed s, position
+ * j < k and base code c, {rol(seed(c), k-1-j), rol(seed_rc(c), j)} when j is a
+ * care position of s, else {0, 0}; 32 positions per seed. */
+std::vector<unsigned long long> mibf_seed_tables(const std::vector<std::string> &seeds,
+		unsigned k);
+
+/* summary.tsv text over `names` (ResultsManager::getResultsSummary). */
+std::string mibf_summary_text(const std::vector<std::string> &names,
+		const std::vector<uint64_t> &counts, uint64_t reads);
+
+/* One output record (formatOutStr, MIBFClassifier.hpp:675-736). */
+void mibf_format_record(std::string &out, const std::vector<std::string> &names, int out_type,
+		const char *name, const char *comment, const char *seq, const char *qual,
+		const bbt_mibf_hit *hits, uint32_t n_hits, uint32_t sat_count);
+
+} // namespace bbt
+
+struct bbt_mibf {
+	std::string err;
+	bbt_mibf_params p;
+	bbt::MibfHeader hd;
+	std::vector<std::string> names;      /* m_fullIDs */
+	std::vector<double> frame_prob;      /* m_perFrameProb */
+	double rate_saturated = 0;
+	unsigned allowed_miss = 0, need = 0;
+	bool host_only = false;
+	/* device state */
+	int dev = 0;
+	int num_sms = 0;
+	cudaStream_t stream = nullptr, h2d = nullptr, d2h = nullptr;
+	uint4 *d_blocks = nullptr;            /* 32-byte rank blocks */
+	unsigned long long *d_super = nullptr; /* rank at each superblock start */
+	uint16_t *d_ids = nullptr;
+	unsigned long long *d_tables = nullptr;
+	unsigned long long *d_counts = nullptr;
+	unsigned long long *d_work = nullptr;
+	unsigned int *d_flags = nullptr;       /* [0] result overflow */
+	/* minCount rows, frame count -> num_ids entries; host copy and device copy */
+	std::mutex mc_mu;
+	std::vector<uint32_t> h_minc;
+	std::vector<uint8_t> minc_have;
+	uint32_t *d_minc = nullptr;
+	uint32_t minc_rows = 0;               /* rows allocated on the device */
+	/* host-batch staging */
+	uint8_t *d_seq[2] = {nullptr, nullptr};
+	uint64_t *d_off[2] = {nullptr, nullptr};
+	uint64_t cap_bases = 0, cap_reads = 0;
+	bbt_mibf_hit *d_hits = nullptr;
+	uint32_t *d_nhits = nullptr, *d_sat = nullptr;
+	uint64_t res_cap_reads = 0;
+	uint32_t res_cap_hits = 0;
+	unsigned int *d_fcmax = nullptr;
+	uint64_t reads_seen = 0;
+	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+	double last_kernel_ms = 0;
+};
+
+namespace bbt {
+int mibf_fail(bbt_mibf *ctx, int code, const std::string &msg);
+/* load the header, IDs file names, ID array (host) and frame probabilities */
+int mibf_load_host(bbt_mibf *ctx, const char *bf_path, std::vector<uint16_t> *ids_out);
+}
+
+#endif

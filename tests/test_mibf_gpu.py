@@ -1,0 +1,230 @@
+"""miBF path on the GPU: the biobloommicategorizer CLI against the reference
+CLI's golden output, the C ABI (host and device batches) against the oracle on
+seeded inputs, and the GPU maker against the oracle's build, byte for byte."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from tests import mibf_util as mu
+from tests import oracle_lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CLI = os.path.join(ROOT, "biobloom_b200", "bin", "biobloommicategorizer")
+BASES = np.frombuffer(b"ACGT", dtype=np.uint8)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("case", sorted(mu.CASES))
+def test_cli_matches_reference_cli(case, tmp_path):
+    prefix, args, paired = mu.CASES[case]
+    if paired is None:
+        inputs = [mu.g("reads_edge.fa.gz")]
+    elif paired:
+        inputs = ["-e", mu.g("reads_1.fq.gz"), mu.g("reads_2.fq.gz")]
+    else:
+        inputs = [mu.g("reads_se.fa.gz")]
+    p = subprocess.run([CLI, "-p", str(tmp_path / "out"), "-f", mu.g(f"{prefix}.bf")] + args +
+                       inputs, capture_output=True)
+    assert p.returncode == 0, p.stderr.decode()
+    with open(mu.g(f"mi_{case}.tsv"), "rb") as f:
+        assert p.stdout == f.read()
+    summary = (tmp_path / "out_summary.tsv").read_text()
+    if paired is None:
+        results, names, o, _ = mu.oracle_results(case)
+        assert summary == mu.summary_text(names, results, False, o["hit_only"])
+    else:
+        with open(mu.g(f"mi_{case}_summary.tsv")) as f:
+            assert summary == f.read()
+
+
+def _genome(rng, n, gc=0.5):
+    u = rng.random(n)
+    return np.where(u < gc / 2, ord("C"), np.where(u < gc, ord("G"),
+                    np.where(u < gc + (1 - gc) / 2, ord("A"), ord("T")))).astype(np.uint8)
+
+
+def _targets(rng, n_targets=24, length=12000):
+    seqs = [_genome(rng, length, float(rng.uniform(0.35, 0.65))) for _ in range(n_targets)]
+    for i in range(0, n_targets - 1, 3):  # shared blocks between target pairs
+        a = int(rng.integers(0, length - 3000))
+        b = int(rng.integers(0, length - 3000))
+        seqs[i + 1][b:b + 2000] = seqs[i][a:a + 2000]
+    seqs[5][100:6100] = np.tile(_genome(rng, 40), 150)  # a repeat-rich target
+    return [s.tobytes() for s in seqs]
+
+
+def _reads(rng, targets, n, paired=False, long_frac=0.05):
+    comp = bytes.maketrans(b"ACGTN", b"TGCAN")
+    out1, out2 = [], []
+    for i in range(n):
+        L = int(rng.integers(1, 300))
+        if rng.random() < long_frac:
+            L = int(rng.integers(500, 3000))  # several staging chunks
+        t = int(rng.integers(-1, len(targets)))
+        if t < 0 or L > len(targets[t]) - 1:
+            s = BASES[rng.integers(0, 4, L)].tobytes()
+        else:
+            st = int(rng.integers(0, len(targets[t]) - L))
+            s = targets[t][st:st + L]
+            a = np.frombuffer(s, dtype=np.uint8).copy()
+            m = rng.random(L) < 0.01
+            a[m] = BASES[rng.integers(0, 4, int(m.sum()))]
+            if rng.random() < 0.2:
+                a[rng.random(L) < 0.02] = ord("N")
+            if rng.random() < 0.2:
+                a[rng.random(L) < 0.3] |= 0x20
+            s = a.tobytes()
+            if rng.random() < 0.5:
+                s = s.translate(comp)[::-1]
+        out1.append(s)
+        if paired:
+            out2.append(BASES[rng.integers(0, 4, int(rng.integers(1, 200)))].tobytes()
+                        if rng.random() < 0.3 else s[::-1].translate(comp))
+    return out1, (out2 if paired else None)
+
+
+@pytest.fixture(scope="module")
+def built(tmp_path_factory):
+    """A 24-target miBF (3 spaced seeds) and a k-mer-mode one, built by the oracle."""
+    rng = np.random.default_rng(11)
+    targets = _targets(rng)
+    d = tmp_path_factory.mktemp("mibf")
+    seeds = ["1111011101110010111011111", "1101111101001011111011011",
+             "1111101011100111010111111"]
+    names = [f"target{i + 1}" for i in range(len(targets))]
+    out = {}
+    for tag, sd in (("ss", seeds), ("km", None)):
+        f = oracle_lib.MIBF.build(targets, list(range(1, len(targets) + 1)), seeds=sd, k=25, h=3,
+                                  occupancy=0.5)
+        f.store(str(d / tag))
+        with open(d / f"{tag}_ids.txt", "w") as fh:
+            for i, n in enumerate(names):
+                fh.write(f"{i + 1}\t{n}\n")
+        out[tag] = (str(d / f"{tag}.bf"), f)
+    return targets, out, seeds, names
+
+
+def _oracle_query(f, names, reads, reads2, o):
+    h = f.f.h
+    allowed = 0 if (o["frame_matches"] > h or f.f.nseeds == 0) else h - o["frame_matches"]
+    probs, _ = f.frame_probs(len(names) + 1, allowed)
+    cache = {}
+    res = []
+    for i, s in enumerate(reads):
+        s2 = reads2[i] if reads2 is not None else None
+        fc = mu.frame_count(len(s), len(s2) if s2 is not None else 0, f.f.k, s2 is not None)
+        if fc == 0:
+            res.append(([], 0))
+            continue
+        if fc not in cache:
+            cache[fc] = mu.min_counts(fc, probs, o["score"])
+        res.append(f.query(s, cache[fc], seq2=s2, multi=o["multi"], allowed_miss=allowed,
+                           min_nonsat=o["min_nonsat"], best_agree=o["best"]))
+    return res
+
+
+OPTS = [
+    {},
+    {"multi": 3.0},
+    {"frame_matches": 2, "min_nonsat": 2},
+    {"frame_matches": 3, "best": True},
+    {"score": 1e-3, "multi": 100.0},
+]
+
+
+def _opts(d):
+    o = {"score": 1e-10, "multi": 1.0, "frame_matches": 1, "min_nonsat": 0, "best": False}
+    o.update(d)
+    return o
+
+
+@pytest.mark.parametrize("tag", ["ss", "km"])
+@pytest.mark.parametrize("paired", [False, True])
+@pytest.mark.parametrize("oi", range(len(OPTS)))
+def test_abi_host_batch_matches_oracle(built, tag, paired, oi):
+    from biobloom_b200.mibf import MIBFClassifier
+    targets, filters, _, names = built
+    path, f = filters[tag]
+    o = _opts(OPTS[oi])
+    rng = np.random.default_rng(100 + oi + 10 * paired)
+    reads, reads2 = _reads(rng, targets, 700, paired=paired)
+    want = _oracle_query(f, names, reads, reads2, o)
+    mc = MIBFClassifier(path, score=o["score"], frame_matches=o["frame_matches"],
+                        multi=o["multi"], min_nonsat=o["min_nonsat"], best_hit_agree=o["best"])
+    got, sat = mc.classify(reads, reads2, max_hits=2)  # max_hits 2 exercises the retry
+    for i, (res, s) in enumerate(want):
+        assert (got[i], int(sat[i])) == (res, s), i
+    counts, n = mc.summary()
+    assert n == len(reads)
+    nf = len(names) + 1
+    assert counts[2 * (nf + 2) + 1] == sum(1 for r, _ in want if not r)
+    assert counts[2 * (nf + 2)] == sum(1 for r, _ in want if len(r) > 1)
+    mc.close()
+
+
+def test_abi_device_batch_matches_host_batch(built):
+    import torch
+    from biobloom_b200.mibf import MIBFClassifier
+    from biobloom_b200.classifier import pack
+    targets, filters, _, names = built
+    path, f = filters["ss"]
+    rng = np.random.default_rng(5)
+    reads, _ = _reads(rng, targets, 3000)
+    mc = MIBFClassifier(path)
+    want, wsat = mc.classify(reads)
+    seq, off = pack(reads)
+    dseq = torch.from_numpy(seq.copy()).cuda()
+    doff = torch.from_numpy(off.astype(np.int64)).cuda()
+    hits, nh, sat = mc.classify_device(dseq, doff, max_hits=mc.num_ids)
+    mc.sync()
+    torch.cuda.synchronize()
+    hits, nh, sat = hits.cpu().numpy(), nh.cpu().numpy(), sat.cpu().numpy()
+    for i in range(len(reads)):
+        got = [tuple(int(x) for x in hits[i, j]) for j in range(int(nh[i]))]
+        assert got == want[i] and int(sat[i]) == int(wsat[i]), i
+
+
+def test_results_are_the_same_alone_and_in_a_batch(built):
+    from biobloom_b200.mibf import MIBFClassifier
+    targets, filters, _, names = built
+    path, _ = filters["ss"]
+    rng = np.random.default_rng(9)
+    reads, _ = _reads(rng, targets, 400)
+    mc = MIBFClassifier(path)
+    batch, bsat = mc.classify(reads)
+    for i in range(0, 400, 37):
+        one, osat = mc.classify([reads[i]])
+        assert one[0] == batch[i] and osat[0] == bsat[i]
+
+
+@pytest.mark.parametrize("tag", ["ss", "km"])
+def test_gpu_maker_matches_oracle_build(built, tag, tmp_path):
+    from biobloom_b200.mibf import make_mibf
+    targets, filters, seeds, names = built
+    path, _ = filters[tag]
+    make_mibf(str(tmp_path / "g"), targets, list(range(1, len(targets) + 1)), names,
+              seeds=seeds if tag == "ss" else None, k=25, hash_num=3, occupancy=0.5)
+    for ext in (".bf", ".sdsl", "_ids.txt"):
+        with open(path[:-3] + ext, "rb") as a, open(str(tmp_path / "g") + ext, "rb") as b:
+            assert a.read() == b.read(), ext
+
+
+def test_gpu_maker_multi_contig_ids(tmp_path):
+    """Several sequences per ID, sequences shorter than k, and N runs."""
+    from biobloom_b200.mibf import make_mibf
+    rng = np.random.default_rng(21)
+    seqs = [_genome(rng, int(rng.integers(10, 4000))).tobytes() for _ in range(30)]
+    seqs[3] = b"ACGTN" * 40
+    seqs[7] = b"ACGTACGTACGTACGT"  # k - 1 bases: no frames
+    ids = [int(rng.integers(1, 9)) for _ in seqs]
+    names = [f"n{i}" for i in range(1, 9)]
+    seeds = ["11011111111111011", "11111011111101111"]
+    f = oracle_lib.MIBF.build(seqs, ids, seeds=seeds, k=17, h=2, occupancy=0.3)
+    f.store(str(tmp_path / "o"))
+    make_mibf(str(tmp_path / "g"), seqs, ids, names, seeds=seeds, k=17, occupancy=0.3)
+    for ext in (".bf", ".sdsl"):
+        with open(str(tmp_path / "o") + ext, "rb") as a, open(str(tmp_path / "g") + ext, "rb") as b:
+            assert a.read() == b.read(), ext
