@@ -113,8 +113,14 @@ __device__ __forceinline__ uint64_t seed_value(const ulonglong2 *tab, uint64_t w
 /* Tally word order: A = count | nonSatCount << 32, B = solidCount |
  * totalCount << 32, C = totalNonSatCount | nonSatFrameCount << 32. */
 struct Cand {
-	unsigned long long k1, k2; /* (count, nonSat), (total, ~id): larger is better */
+	unsigned long long k1, k2; /* count << 32 | nonSat, total << 32 | ~id: larger is better */
 };
+
+/* k1 of a candidate from its A tally word (count low, nonSat high). */
+__device__ __forceinline__ unsigned long long cand_k1(unsigned long long A)
+{
+	return (A << 32) | (A >> 32);
+}
 
 __device__ __forceinline__ bool cand_less(const Cand &a, const Cand &b)
 {
@@ -332,7 +338,7 @@ __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 					if (s >= 1 && s < nids && cnt > 0 && cnt >= __ldg(mrow + s) &&
 							(a.min_nonsat == 0 || ns >= a.min_nonsat)) {
 						cmask |= 1u << j;
-						Cand c = {A, ((TB[s] >> 32) << 32) | (0xFFFFFFFFull - s)};
+						Cand c = {cand_k1(A), ((TB[s] >> 32) << 32) | (0xFFFFFFFFull - s)};
 						if (cand_less(best, c))
 							best = c;
 						maxns = ns > maxns ? ns : maxns;
@@ -342,8 +348,8 @@ __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 			best = warp_best(best);
 			maxns = __reduce_max_sync(kFull, maxns);
 			uint32_t n_out = 0;
-			if (best.k1 && !(a.best_agree && maxns > (uint32_t)(best.k1 >> 32))) {
-				const double thr = (double)(uint32_t)best.k1 - a.multi;
+			if (best.k1 && !(a.best_agree && maxns > (uint32_t)best.k1)) {
+				const double thr = (double)(uint32_t)(best.k1 >> 32) - a.multi;
 				Cand cur = best;
 				for (;;) {
 					const uint32_t id = 0xFFFFFFFFu - (uint32_t)cur.k2;
@@ -370,7 +376,7 @@ __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 							continue;
 						const uint32_t s = lane + 32 * j;
 						const unsigned long long A = TA[s];
-						Cand c = {A, ((TB[s] >> 32) << 32) | (0xFFFFFFFFull - s)};
+						Cand c = {cand_k1(A), ((TB[s] >> 32) << 32) | (0xFFFFFFFFull - s)};
 						if (cand_less(c, cur) && (double)(uint32_t)A > thr && cand_less(nx, c))
 							nx = c;
 					}
