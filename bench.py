@@ -16,7 +16,15 @@ with pinned host buffers (host->device copies of the reads and device->host
 copies of the per-read results inside the timed region); `plain` is the
 one-warp-per-read, one-launch-per-batch kernel on the same data.
 
+With --workload mibf: the multi-index workload -- a miBF over 500 targets,
+each a seeded 2 Mbp reference at 35-65% GC (uniform per target) with 20% of
+its sequence copied from another random target; 3 spaced seeds of span 25 and
+weight 19 drawn from the seed; 20M single-end 150 bp reads, 90% from the
+targets with 1% substitutions, 10% uniform random.  A step classifies all
+reads once (reads and the 5 GB filter resident in HBM, far above L2).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+                  [--workload bf|mibf]
 """
 import argparse
 import json
@@ -486,6 +494,322 @@ def check_sample(paths, s1, s2, off, hits1, hits2, n):
                                                         (g2 != w2).any(1).sum())}
 
 
+# ---------------------------------------------------------------- miBF workload
+
+MI_TARGET_LEN = 2_000_000
+MI_SHARED = 0.20
+MI_SUB = 0.01
+MI_METRIC = "reads/s on 1 B200, miBF classification, % HBM sector peak"
+
+
+def mi_workload(n_targets, n_reads):
+    return (f"miBF over {n_targets} targets x 2 Mbp (35-65% GC, 20% shared between random "
+            f"target pairs), 3 spaced seeds span 25 weight 19, {n_reads} single-end 150 bp "
+            f"reads (90% from targets with 1% substitutions, 10% random)")
+
+
+def mi_seeds(rng):
+    out = []
+    for _ in range(3):
+        zeros = set(int(x) for x in rng.choice(np.arange(1, 24), 6, replace=False))
+        out.append("".join("0" if i in zeros else "1" for i in range(25)))
+    return out
+
+
+def mi_targets(n_targets):
+    from biobloom_b200 import synth
+    rng = np.random.default_rng(4004)
+    gcs = rng.uniform(0.35, 0.65, n_targets)
+    pristine = [synth.genome(4_000_000 + i, MI_TARGET_LEN, gc=float(gcs[i]))
+                for i in range(n_targets)]
+    out = [g.copy() for g in pristine]
+    blk = int(MI_SHARED * MI_TARGET_LEN)
+    for i in range(n_targets):
+        j = int(rng.integers(0, n_targets - 1))
+        j += j >= i
+        a = int(rng.integers(0, MI_TARGET_LEN - blk))
+        b = int(rng.integers(0, MI_TARGET_LEN - blk))
+        out[i][b:b + blk] = pristine[j][a:a + blk]
+    return out, mi_seeds(rng)
+
+
+def mi_build(d, n_targets, device):
+    from biobloom_b200.mibf import make_mibf
+    t0 = time.time()
+    targets, seeds = mi_targets(n_targets)
+    path = os.path.join(d, "targets.bf")
+    if not all(os.path.exists(path[:-3] + e) for e in (".bf", ".sdsl", "_ids.txt")):
+        make_mibf(path[:-3], [t.tobytes() for t in targets], list(range(1, n_targets + 1)),
+                  [f"target{i + 1}" for i in range(n_targets)], seeds=seeds, occupancy=0.5,
+                  device=device)
+    log(f"targets + miBF: {time.time() - t0:.1f} s")
+    return path, targets, seeds
+
+
+def mi_reads(targets, n_reads, seed):
+    from biobloom_b200 import synth
+    p = synth.read_params(READ_LEN, READ_LEN, sub_rate=MI_SUB)
+    frac = [0.9 / len(targets)] * len(targets)
+    s1, off, _, _ = synth.reads(seed, targets, frac, n_reads, p)
+    return s1, off
+
+
+def mi_cpu_run(d, path, s1, off, n, threads):
+    """The reference's MI categorizer (oracle/_ref/biobloommicategorizer) on the
+    first n reads; returns (seconds of its own classification timer, None)."""
+    cli = os.path.join(ROOT, "oracle", "_ref", "biobloommicategorizer")
+    if not os.path.exists(cli):
+        return None, "oracle/_ref/biobloommicategorizer is not built"
+    fa = os.path.join(d, f"sample_{n}.fa")
+    if not os.path.exists(fa):
+        with open(fa, "wb") as f:
+            f.write(b"".join(b">r%d\n%s\n" % (i, s1[off[i]:off[i + 1]].tobytes())
+                             for i in range(n)))
+    p = subprocess.run([cli, "-t", str(threads), "-p", os.path.join(d, "refcpu"), "-f", path, fa],
+                       stdout=subprocess.DEVNULL, stderr=subprocess.PIPE, text=True)
+    if p.returncode:
+        return None, "reference MI categorizer failed: " + p.stderr[-300:]
+    for line in p.stderr.splitlines():
+        if line.startswith("Classification time (s):"):
+            return float(line.split(":")[1]), None
+    return None, "no classification time in the reference's output"
+
+
+def mi_cpu_baseline(d, path, s1, off, budget_s=15.0):
+    threads = os.cpu_count() or 1
+    probe = 20000
+    sec, err = mi_cpu_run(d, path, s1, off, probe, threads)
+    if sec is None:
+        return None, err
+    n = int(min(len(off) - 1, max(probe, probe / max(sec, 1e-6) * budget_s)))
+    n = max(probe, (n // 10000) * 10000)
+    sec, err = mi_cpu_run(d, path, s1, off, n, threads)
+    if sec is None:
+        return None, err
+    return {"value": n / sec, "unit": "reads/s", "cores": threads, "kind": "reference",
+            "sample": f"first {n} reads of the workload; the reference's MIBFClassifier::filter "
+                      f"(BioBloomCategorizer sources) over the oracle's miBF structures, "
+                      f"{threads} OpenMP threads, its own classification timer (filter load "
+                      f"excluded)", "seconds": sec}, None
+
+
+def mi_check_sample(path, s1, off, hits, nh, sat, n):
+    try:
+        from tests import mibf_util as mu
+        from tests import oracle_lib as ol
+    except Exception as e:
+        return {"checked": 0, "error": str(e)}
+    f = ol.MIBF.load(path)
+    nids = 1
+    with open(path[:-3] + "_ids.txt") as fh:
+        nids += sum(1 for _ in fh)
+    probs, _ = f.frame_probs(nids, f.f.h - 1)
+    mc = mu.min_counts(READ_LEN - f.f.k + 1, probs, 1e-10)
+    hits = hits[:n].cpu().numpy()
+    nh = nh[:n].cpu().numpy()
+    sat = sat[:n].cpu().numpy()
+    bad = 0
+    for i in range(n):
+        s = s1[off[i]:off[i + 1]].tobytes()
+        fc = len(s) - f.f.k + 1
+        mcount = mc if fc == READ_LEN - f.f.k + 1 else mu.min_counts(fc, probs, 1e-10)
+        want, wsat = f.query(s, mcount, allowed_miss=f.f.h - 1)
+        got = [tuple(int(x) for x in hits[i, j]) for j in range(min(int(nh[i]), hits.shape[1]))]
+        bad += (got != want) or int(sat[i]) != wsat or int(nh[i]) != len(want)
+    return {"checked_reads": n, "mismatched_reads": int(bad)}
+
+
+def run_mibf(args):
+    import ctypes
+
+    import torch
+
+    from biobloom_b200 import _lib as L
+    from biobloom_b200.mibf import MIBFClassifier
+
+    world, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    d = os.path.join(tempfile.gettempdir(), f"bbt_bench_mibf_{args.targets}")
+    os.makedirs(d, exist_ok=True)
+    path, targets, _ = mi_build(d, args.targets, local)
+    n = args.reads
+    s1, off = mi_reads(targets, n, 6000 + rank)
+    del targets
+    bases = int(off[-1])
+    h1 = torch.from_numpy(s1[:bases]).pin_memory()
+    hoff = torch.from_numpy(off.view(np.int64)).pin_memory()
+    d1, doff = h1.to(dev), hoff.to(dev)
+    t0 = time.time()
+    mc = MIBFClassifier(path, device=local)
+    log(f"miBF load: {time.time() - t0:.1f} s")
+    MH = 4
+    hits = torch.empty((n, MH, 7), dtype=torch.int32, device=dev)
+    nh = torch.empty(n, dtype=torch.int32, device=dev)
+    sat = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    def step():
+        mc.classify_device(d1, doff, stream=stream, out=(hits, nh, sat))
+
+    for _ in range(args.warmup):
+        step()
+        mc.sync()
+    counts = mc.last_counts()
+    if pg:
+        pg.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    kms = []
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+        mc.sync()
+        kms.append(mc.last_kernel_ms())
+    e1.record(stream)
+    e1.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    kernel_ms = sum(kms) / len(kms)
+    if pg:
+        t = torch.tensor([ms], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+
+    parity = None
+    if rank == 0 and not args.no_check:
+        parity = mi_check_sample(path, s1, off, hits, nh, sat, 2000)
+
+    # e2e: the C ABI with pinned host buffers (reads in, results out)
+    hh = torch.empty((n, MH, 7), dtype=torch.int32).pin_memory()
+    hn = torch.empty(n, dtype=torch.int32).pin_memory()
+    hs = torch.empty(n, dtype=torch.int32).pin_memory()
+
+    def e2e_step():
+        b = L.Batch()
+        b.seq, b.offsets, b.n_reads, b.location = h1.data_ptr(), hoff.data_ptr(), n, L.HOST
+        r = L.MibfResult()
+        r.hits, r.max_hits, r.n_hits, r.sat_count, r.location = (
+            hh.data_ptr(), MH, hn.data_ptr(), hs.data_ptr(), L.HOST)
+        L.check_mibf(L.lib().bbt_mibf_classify_batch(mc._ctx, ctypes.byref(b), ctypes.byref(r),
+                                                     None), mc._ctx)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    if pg:
+        pg.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if pg:
+        t = torch.tensor([e2e_s], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_ok = bool(torch.equal(hn, nh.cpu()) and torch.equal(hs, sat.cpu()))
+
+    if rank != 0:
+        mc.close()
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    cpu, cpu_err = (None, "skipped (--no-cpu)")
+    if world == 1 and not args.no_cpu:
+        cpu, cpu_err = mi_cpu_baseline(d, path, s1, off)
+    frames, probes, phits = counts
+    peak, peak_kind = measured_peaks()
+    alg_bytes = 32.0 * probes + 32.0 * phits + bases / 4.0 + 8.0 * n
+    achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
+    tpr = None
+    tp = os.path.join(ROOT, "profiles", "mibf_query_dram.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tpr = json.load(f).get("dram_bytes_per_read")
+    line = {
+        "metric": MI_METRIC, "value": world * n / (ms * 1e-3), "unit": "reads/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic",
+        "config": {"workload": mi_workload(args.targets, n), "reads_per_gpu": n,
+                   "targets": args.targets,
+                   "filter_bytes": int(os.path.getsize(path) + os.path.getsize(path[:-3] +
+                                                                             ".sdsl")),
+                   "l2": "inputs larger than L2 (3 GB reads + 5 GB miBF)",
+                   "parallelism": f"replicas x{world} (reads sharded, miBF replicated)"},
+        "frames_per_step": frames, "probes_per_step": probes, "probe_hits_per_step": phits,
+        "probes_per_s": world * probes / (ms * 1e-3),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": (tpr * n if tpr else None),
+                     "kernel": "mibf_query_kernel", "kernel_ms": kernel_ms,
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "algorithmic_bytes_note": "32 B block sector per probe + 32 B ID sector per "
+                                               "hit + 2-bit bases + 8 B results per read"},
+        "cpu_baseline": cpu if cpu else {"value": None, "unavailable": cpu_err},
+        "e2e": {"value": world * n / e2e_s, "unit": "reads/s",
+                "h2d_bytes_per_step": int(bases + (n + 1) * 8),
+                "d2h_bytes_per_step": int(n * (MH * 28 + 8)),
+                "matches_device_results": e2e_ok},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clk,
+        "parity_sample": parity,
+    }
+    print(json.dumps(line), flush=True)
+    mc.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def run_mibf_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    if rank != 0:
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    d = os.path.join(tempfile.gettempdir(), f"bbt_bench_mibf_{args.targets}")
+    os.makedirs(d, exist_ok=True)
+    path, targets, _ = mi_build(d, args.targets, local)
+    s1, off = mi_reads(targets, 400_000, 6000)
+    threads = os.cpu_count() or 1
+    sec, err = mi_cpu_run(d, path, s1, off, 20000, threads)
+    if sec is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    n = int(min(400_000, max(20000, 20000 / max(sec, 1e-6) * 10.0)))
+    n = (n // 10000) * 10000
+    times = []
+    for i in range(args.warmup + args.steps):
+        sec, err = mi_cpu_run(d, path, s1, off, n, threads)
+        if sec is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}))
+            return
+        if i >= args.warmup:
+            times.append(sec)
+    sec = sum(times) / len(times)
+    value = n / sec
+    line = {"impl": "reference", "metric": MI_METRIC, "value": value, "unit": "reads/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": mi_workload(args.targets, n), "reads_per_step": n},
+            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads,
+                             "kind": "reference",
+                             "sample": f"{n} reads per step, MIBFClassifier::filter from the "
+                                       "reference sources over the oracle's miBF structures"},
+            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -496,10 +820,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity (bytes)")
+    ap.add_argument("--workload", default="bf", choices=["bf", "mibf"])
+    ap.add_argument("--targets", type=int, default=500, help="miBF targets (--workload mibf)")
+    ap.add_argument("--reads", type=int, default=20_000_000, help="reads (--workload mibf)")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")
-    if args.impl == "reference":
+    if args.workload == "mibf":
+        (run_mibf_reference if args.impl == "reference" else run_mibf)(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_gpu(args)

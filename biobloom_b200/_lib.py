@@ -144,6 +144,7 @@ def lib():
         "bbt_mibf_classify_batch": (i32, [vp, P(Batch), P(MibfResult), vp]),
         "bbt_mibf_sync": (i32, [vp]),
         "bbt_mibf_last_kernel_ms": (dbl, [vp]),
+        "bbt_mibf_last_counts": (i32, [vp, P(u64)]),
         "bbt_mibf_summary": (i32, [vp, P(u64), P(u64)]),
         "bbt_mibf_reset_summary": (i32, [vp]),
         "bbt_mibf_summary_tsv": (i32, [vp, u64, ctypes.c_char_p, ctypes.c_size_t,

@@ -71,7 +71,12 @@ struct MibfArgs {
 	unsigned long long *counts; /* this batch's summary counters */
 	unsigned long long *work;
 	unsigned int *flags;
+	unsigned long long *stat;   /* frames visited, values probed, probes that hit */
 	uint32_t T;                 /* tally slots per warp, a multiple of 32 */
+};
+
+struct LaneCounts {
+	unsigned long long frames = 0, probes = 0, hits = 0;
 };
 
 __host__ __device__ inline size_t mibf_warp_bytes(uint32_t T)
@@ -144,7 +149,7 @@ template <int H>
 __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglong2 *tab,
 		uint64_t *cw, uint32_t *iw, unsigned long long *TA, unsigned long long *TB,
 		unsigned long long *TC, const uint8_t *__restrict__ s, uint64_t len, uint32_t &satc,
-		int lane)
+		LaneCounts &lc, int lane)
 {
 	const uint32_t k = a.f.k, h = a.f.h, nids = a.f.nids, need = a.need;
 	const uint64_t kmask = (k >= 64) ? ~0ull : ((1ull << k) - 1);
@@ -237,8 +242,12 @@ __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglon
 			}
 			bool anysat = false;
 #pragma unroll
-			for (int v = 0; v < H; ++v)
+			for (int v = 0; v < H; ++v) {
 				anysat |= hit[v] && (e[v] & kMibfSat);
+				lc.hits += hit[v] ? 1u : 0u;
+			}
+			lc.frames += ok ? 1u : 0u;
+			lc.probes += ok ? h : 0u;
 			satc += __popc(__ballot_sync(kFull, anysat));
 			/* per-frame, per-ID records, merged across the warp */
 #pragma unroll
@@ -301,6 +310,7 @@ __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 	const ulonglong2 *tab = reinterpret_cast<const ulonglong2 *>(smem);
 	const uint32_t k = a.f.k;
 	unsigned long long *above = a.counts, *unique = a.counts + (nids + 2);
+	LaneCounts lc;
 	for (;;) {
 		unsigned long long r0 = 0;
 		if (lane == 0)
@@ -321,9 +331,10 @@ __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 					: (len2 >= k ? (uint32_t)(len2 - k + 1) : 0u);
 			uint32_t satc = 0;
 			if (fc) {
-				mibf_scan_mate<H>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1, satc, lane);
+				mibf_scan_mate<H>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1, satc, lc,
+						lane);
 				if (a.seq2)
-					mibf_scan_mate<H>(a, tab, cw, iw, TA, TB, TC, a.seq2 + b2, len2, satc,
+					mibf_scan_mate<H>(a, tab, cw, iw, TA, TB, TC, a.seq2 + b2, len2, satc, lc,
 							lane);
 			}
 			/* significant IDs */
@@ -409,6 +420,17 @@ __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 			}
 			__syncwarp();
 		}
+	}
+#pragma unroll
+	for (int o = 16; o; o >>= 1) {
+		lc.frames += __shfl_xor_sync(kFull, lc.frames, o);
+		lc.probes += __shfl_xor_sync(kFull, lc.probes, o);
+		lc.hits += __shfl_xor_sync(kFull, lc.hits, o);
+	}
+	if (lane == 0 && (lc.frames || lc.probes)) {
+		atomicAdd(a.stat, lc.frames);
+		atomicAdd(a.stat + 1, lc.probes);
+		atomicAdd(a.stat + 2, lc.hits);
 	}
 }
 
@@ -618,6 +640,7 @@ extern "C" int bbt_mibf_close(bbt_mibf *ctx)
 		cudaFree(ctx->d_counts);
 		cudaFree(ctx->d_work);
 		cudaFree(ctx->d_flags);
+		cudaFree(ctx->d_stat);
 		cudaFree(ctx->d_minc);
 		cudaFree(ctx->d_fcmax);
 		for (int i = 0; i < 2; ++i) {
@@ -691,6 +714,7 @@ extern "C" int bbt_mibf_open(const char *bf_path, const bbt_mibf_params *params,
 			cudaMalloc(&ctx->d_counts, 2 * nc * 8) != cudaSuccess ||
 			cudaMalloc(&ctx->d_work, 8) != cudaSuccess ||
 			cudaMalloc(&ctx->d_flags, 4) != cudaSuccess ||
+			cudaMalloc(&ctx->d_stat, 3 * 8) != cudaSuccess ||
 			cudaMalloc(&ctx->d_fcmax, (1 + 2048) * 4) != cudaSuccess)
 		return bail(mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(context)"));
 	cudaMemcpy(ctx->d_tables, tabs.data(), tabs.size() * 8, cudaMemcpyHostToDevice);
@@ -830,6 +854,7 @@ static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, cons
 	a.counts = batch_counts;
 	a.work = ctx->d_work;
 	a.flags = ctx->d_flags;
+	a.stat = ctx->d_stat;
 	a.T = tally_slots(nids);
 	const int hsel = pick_h(ctx->hd.h);
 	const size_t smem = mibf_smem_bytes(a.f.nse, a.T, 4);
@@ -837,6 +862,7 @@ static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, cons
 	MIBF_TRY(ctx, cudaMemsetAsync(batch_counts, 0, nc * 8, s));
 	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, 8, s));
 	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_flags, 0, 4, s));
+	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_stat, 0, 3 * 8, s));
 	MIBF_TRY(ctx, cudaEventRecord(ctx->ev0, s));
 	if (b->n_reads)
 		MIBF_TRY(ctx, launch_query(a, hsel, grid, smem, s));
@@ -920,21 +946,30 @@ extern "C" int bbt_mibf_classify_batch(bbt_mibf *ctx, const bbt_batch *b, bbt_mi
 	rc = ensure_min_count(ctx, host_frame_counts(b, ctx->hd.k), s);
 	if (rc)
 		return rc;
-	std::vector<uint64_t> o1(n + 1), o2(b->seq2 ? n + 1 : 0);
-	for (uint64_t i = 0; i <= n; ++i)
-		o1[i] = b->offsets[i] - s1;
-	if (b->seq2)
+	/* offsets are copied as they are when they start at 0, else rebased */
+	std::vector<uint64_t> o1, o2;
+	const uint64_t *h_o1 = b->offsets, *h_o2 = b->offsets2;
+	if (n && s1) {
+		o1.resize(n + 1);
+		for (uint64_t i = 0; i <= n; ++i)
+			o1[i] = b->offsets[i] - s1;
+		h_o1 = o1.data();
+	}
+	if (n && b->seq2 && s2) {
+		o2.resize(n + 1);
 		for (uint64_t i = 0; i <= n; ++i)
 			o2[i] = b->offsets2[i] - s2;
+		h_o2 = o2.data();
+	}
 	if (n) {
 		MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_seq[0], b->seq + s1, e1 - s1, cudaMemcpyHostToDevice,
 				s));
-		MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_off[0], o1.data(), (n + 1) * 8,
-				cudaMemcpyHostToDevice, s));
+		MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_off[0], h_o1, (n + 1) * 8, cudaMemcpyHostToDevice,
+				s));
 		if (b->seq2) {
 			MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_seq[1], b->seq2 + s2, e2 - s2,
 					cudaMemcpyHostToDevice, s));
-			MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_off[1], o2.data(), (n + 1) * 8,
+			MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_off[1], h_o2, (n + 1) * 8,
 					cudaMemcpyHostToDevice, s));
 		}
 	}
@@ -1020,6 +1055,16 @@ extern "C" int bbt_mibf_summary_tsv(bbt_mibf *ctx, uint64_t read_count, char *bu
 		memcpy(buf, s.data(), n);
 		buf[n] = 0;
 	}
+	return BBT_OK;
+}
+
+extern "C" int bbt_mibf_last_counts(bbt_mibf *ctx, uint64_t *out)
+{
+	if (!ctx || ctx->host_only || !out)
+		return BBT_ERR_ARG;
+	MIBF_TRY(ctx, cudaSetDevice(ctx->dev));
+	MIBF_TRY(ctx, cudaDeviceSynchronize());
+	MIBF_TRY(ctx, cudaMemcpy(out, ctx->d_stat, 3 * 8, cudaMemcpyDeviceToHost));
 	return BBT_OK;
 }
 

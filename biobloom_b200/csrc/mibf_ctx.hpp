@@ -89,6 +89,7 @@ struct bbt_mibf {
 	unsigned long long *d_counts = nullptr;
 	unsigned long long *d_work = nullptr;
 	unsigned int *d_flags = nullptr;       /* [0] result overflow */
+	unsigned long long *d_stat = nullptr;  /* frames, probes, hits of the last batch */
 	/* minCount rows, frame count -> num_ids entries; host copy and device copy */
 	std::mutex mc_mu;
 	std::vector<uint32_t> h_minc;

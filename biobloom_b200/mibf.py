@@ -123,16 +123,21 @@ class MIBFClassifier:
             out.append([tuple(int(x) for x in hits[i, j]) for j in range(int(nh[i]))])
         return out, sat[:n].copy()
 
-    def classify_device(self, seq, off, seq2=None, off2=None, max_hits=8, stream=None):
+    def classify_device(self, seq, off, seq2=None, off2=None, max_hits=8, stream=None, out=None):
         """Classify reads resident on the GPU (torch uint8 / int64 tensors).
         Enqueued on `stream` (default: the current stream).  Returns
-        (hits [n, max_hits, 7] int32 tensor, n_hits, sat_count)."""
+        (hits [n, max_hits, 7] int32 tensor, n_hits, sat_count); `out` may
+        pass those three tensors in to be filled."""
         import torch
         n = off.numel() - 1
         dev = seq.device
-        hits = torch.zeros((max(n, 1), max_hits, 7), dtype=torch.int32, device=dev)
-        nh = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
-        sat = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
+        if out is not None:
+            hits, nh, sat = out
+            max_hits = hits.shape[1]
+        else:
+            hits = torch.zeros((max(n, 1), max_hits, 7), dtype=torch.int32, device=dev)
+            nh = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
+            sat = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
         b = L.Batch()
         b.seq, b.offsets, b.n_reads, b.location = seq.data_ptr(), off.data_ptr(), n, L.DEVICE
         if seq2 is not None:
@@ -150,6 +155,12 @@ class MIBFClassifier:
 
     def last_kernel_ms(self):
         return L.lib().bbt_mibf_last_kernel_ms(self._ctx)
+
+    def last_counts(self):
+        """(frames visited, values probed, probes that hit) of the last batch."""
+        out = (ctypes.c_uint64 * 3)()
+        L.check_mibf(L.lib().bbt_mibf_last_counts(self._ctx, out), self._ctx)
+        return tuple(int(x) for x in out)
 
     # -- file pipeline ---------------------------------------------------------
     def filter(self, input_files, prefix="", out_type=L.MIBF_OUT_TSV, out_path=None):

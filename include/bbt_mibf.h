@@ -141,6 +141,10 @@ int bbt_mibf_sync(bbt_mibf *ctx);
 /* Device time of the query kernel of the last batch, in milliseconds (known
  * once the batch is done: after a host batch returns, or after bbt_mibf_sync). */
 double bbt_mibf_last_kernel_ms(bbt_mibf *ctx);
+/* Work of the last batch (waits for it): out[0] frames visited (spans of k
+ * valid bases), out[1] values probed (frames x h), out[2] probes that found a
+ * set bit (each of which read an ID).  No reference counterpart. */
+int bbt_mibf_last_counts(bbt_mibf *ctx, uint64_t *out);
 
 /*
  * Summary counters (ResultsManager<ID>::updateSummaryData over query results,
