@@ -641,7 +641,7 @@ def run_mibf(args):
     hoff = torch.from_numpy(off.view(np.int64)).pin_memory()
     d1, doff = h1.to(dev), hoff.to(dev)
     t0 = time.time()
-    mc = MIBFClassifier(path, device=local)
+    mc = MIBFClassifier(path, device=local, layout=args.layout)
     log(f"miBF load: {time.time() - t0:.1f} s")
     MH = 4
     hits = torch.empty((n, MH, 7), dtype=torch.int32, device=dev)
@@ -722,7 +722,10 @@ def run_mibf(args):
         cpu, cpu_err = mi_cpu_baseline(d, path, s1, off)
     frames, probes, phits = counts
     peak, peak_kind = measured_peaks()
-    alg_bytes = 32.0 * probes + 32.0 * phits + bases / 4.0 + 8.0 * n
+    dense = mc.layout == L.MIBF_LAYOUT_DENSE
+    # one 32-byte sector per random read: dense = one read per probe; rank
+    # layout = a block read per probe and an ID read per hit
+    alg_bytes = 32.0 * probes + (0.0 if dense else 32.0 * phits) + bases / 4.0 + 8.0 * n
     achieved = alg_bytes / (kernel_ms * 1e-3) / 1e9
     tpr = None
     tp = os.path.join(ROOT, "profiles", "mibf_query_dram.json")
@@ -736,6 +739,7 @@ def run_mibf(args):
         "data": "synthetic",
         "config": {"workload": mi_workload(args.targets, n), "reads_per_gpu": n,
                    "targets": args.targets,
+                   "layout": "dense ID map" if dense else "rank blocks + ID array",
                    "filter_bytes": int(os.path.getsize(path) + os.path.getsize(path[:-3] +
                                                                              ".sdsl")),
                    "l2": "inputs larger than L2 (3 GB reads + 5 GB miBF)",
@@ -747,8 +751,10 @@ def run_mibf(args):
                      "traffic": (tpr * n if tpr else None),
                      "kernel": "mibf_query_kernel", "kernel_ms": kernel_ms,
                      "algorithmic_bytes_per_launch": alg_bytes,
-                     "algorithmic_bytes_note": "32 B block sector per probe + 32 B ID sector per "
-                                               "hit + 2-bit bases + 8 B results per read"},
+                     "algorithmic_bytes_note": ("32 B sector per probe (dense ID map)" if dense else
+                                                "32 B block sector per probe + 32 B ID sector "
+                                                "per hit") + " + 2-bit bases + 8 B results per "
+                                                             "read"},
         "cpu_baseline": cpu if cpu else {"value": None, "unavailable": cpu_err},
         "e2e": {"value": world * n / e2e_s, "unit": "reads/s",
                 "h2d_bytes_per_step": int(bases + (n + 1) * 8),
@@ -823,6 +829,7 @@ def main():
     ap.add_argument("--workload", default="bf", choices=["bf", "mibf"])
     ap.add_argument("--targets", type=int, default=500, help="miBF targets (--workload mibf)")
     ap.add_argument("--reads", type=int, default=20_000_000, help="reads (--workload mibf)")
+    ap.add_argument("--layout", type=int, default=0, help="miBF layout: 0 auto, 1 rank, 2 dense")
     args = ap.parse_args()
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")

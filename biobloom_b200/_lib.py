@@ -15,6 +15,7 @@ BBT_ERR = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "CUDA", -5: "NOMEM", -6: "UNSU
            -7: "TIMEOUT", -8: "NODEVICE", -9: "OVERFLOW"}
 ERR_OVERFLOW = -9
 MIBF_OUT_TSV, MIBF_OUT_FASTA, MIBF_OUT_FASTQ = 0, 1, 2
+MIBF_LAYOUT_AUTO, MIBF_LAYOUT_RANK, MIBF_LAYOUT_DENSE = 0, 1, 2
 SCORE_SIMPLE, SCORE_LENGTH = 0, 1
 HOST, DEVICE = 0, 1
 PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT, PATH_FILTER_MAJOR = 0, 1, 2, 3
@@ -74,7 +75,8 @@ class MibfParams(ctypes.Structure):
                 ("multi_thresh", ctypes.c_double), ("streak", ctypes.c_uint),
                 ("min_nonsat", ctypes.c_uint), ("best_hit_agree", ctypes.c_int),
                 ("hit_only", ctypes.c_int), ("device", ctypes.c_int),
-                ("max_batch_bases", ctypes.c_uint64), ("max_batch_reads", ctypes.c_uint64)]
+                ("max_batch_bases", ctypes.c_uint64), ("max_batch_reads", ctypes.c_uint64),
+                ("layout", ctypes.c_int)]
 
 
 class MibfHit(ctypes.Structure):
@@ -138,6 +140,7 @@ def lib():
         "bbt_mibf_close": (i32, [vp]),
         "bbt_mibf_last_error": (cp, [vp]),
         "bbt_mibf_num_ids": (u32, [vp]),
+        "bbt_mibf_layout": (i32, [vp]),
         "bbt_mibf_id_name": (cp, [vp, u32]),
         "bbt_mibf_info": (i32, [vp, P(u64), P(u32), P(u32), P(u32)]),
         "bbt_mibf_frame_probs": (i32, [vp, P(dbl), P(dbl)]),

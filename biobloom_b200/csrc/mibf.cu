@@ -12,6 +12,13 @@
  * MIBloomFilter keeps the same bits with sdsl rank support (a separate rank
  * structure); here rank and bits share the sector.
  *
+ * Dense layout (the default when it fits in a fraction of free HBM): one
+ * 16-bit entry per bit position, 0 for a clear bit, else the slot's ID with its
+ * saturation bit, IDs outside 1 .. num_ids-1 stored as 0x7FFF (they count as
+ * hits but tally nothing, as in the rank layout).  A probe is then a single
+ * random 2-byte read instead of a block read followed by an ID read: twice the
+ * bytes of the compact form for 40% fewer random DRAM accesses per read.
+ *
  * Kernel.  One warp classifies one read (pair) at a time, taking reads from a
  * work counter four at a time.  Bases are staged 512 at a time as 2-bit codes
  * (one 64-bit word per 32 bases, built with three ballots over coalesced byte
@@ -48,6 +55,7 @@ struct MibfDev {
 	const uint4 *blocks;
 	const unsigned long long *super;
 	const uint16_t *ids;
+	const uint16_t *dense;
 	uint64_t m, minv;
 	uint32_t h, k, nse, nids;
 	int kmer_mode;
@@ -145,7 +153,7 @@ __device__ __forceinline__ Cand warp_best(Cand c)
 	return c;
 }
 
-template <int H>
+template <int H, bool DENSE>
 __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglong2 *tab,
 		uint64_t *cw, uint32_t *iw, unsigned long long *TA, unsigned long long *TB,
 		unsigned long long *TC, const uint8_t *__restrict__ s, uint64_t len, uint32_t &satc,
@@ -199,44 +207,55 @@ __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglon
 				for (int v = 0; v < H; ++v)
 					vals[v] = (ok && v < (int)h) ? seed_value(tab + v * 128, w, k) : 0;
 			}
-			/* block reads, all h in flight */
-			uint4 q0v[H], q1v[H];
-			uint32_t rr[H];
-			uint64_t blk[H];
-#pragma unroll
-			for (int v = 0; v < H; ++v) {
-				if (ok && v < (int)h) {
-					const uint64_t p = reduce(vals[v], a.f.m, a.f.minv);
-					blk[v] = p / kBlockBits;
-					rr[v] = (uint32_t)(p - blk[v] * kBlockBits);
-					q0v[v] = __ldg(a.f.blocks + 2 * blk[v]);
-					q1v[v] = __ldg(a.f.blocks + 2 * blk[v] + 1);
-				}
-			}
-			/* bit, rank, ID reads */
 			uint32_t e[H];
 			bool hit[H];
+			if (DENSE) {
+				/* one 2-byte read per value, all h in flight */
 #pragma unroll
-			for (int v = 0; v < H; ++v) {
-				hit[v] = false;
-				e[v] = 0;
-				if (ok && v < (int)h) {
-					const uint32_t d[7] = {q0v[v].y, q0v[v].z, q0v[v].w, q1v[v].x, q1v[v].y,
-							q1v[v].z, q1v[v].w};
-					const uint32_t ws = rr[v] >> 5, bit = rr[v] & 31u;
-					uint32_t acc = 0, word = 0;
-#pragma unroll
-					for (int i = 0; i < 7; ++i) {
-						if ((uint32_t)i < ws)
-							acc += __popc(d[i]);
-						if ((uint32_t)i == ws)
-							word = d[i];
+				for (int v = 0; v < H; ++v) {
+					e[v] = 0;
+					if (ok && v < (int)h)
+						e[v] = __ldg(a.f.dense + reduce(vals[v], a.f.m, a.f.minv));
+					hit[v] = e[v] != 0;
+				}
+			} else {
+				/* block reads, all h in flight */
+				uint4 q0v[H], q1v[H];
+				uint32_t rr[H];
+				uint64_t blk[H];
+	#pragma unroll
+				for (int v = 0; v < H; ++v) {
+					if (ok && v < (int)h) {
+						const uint64_t p = reduce(vals[v], a.f.m, a.f.minv);
+						blk[v] = p / kBlockBits;
+						rr[v] = (uint32_t)(p - blk[v] * kBlockBits);
+						q0v[v] = __ldg(a.f.blocks + 2 * blk[v]);
+						q1v[v] = __ldg(a.f.blocks + 2 * blk[v] + 1);
 					}
-					if ((word >> bit) & 1u) {
-						acc += __popc(word & ((1u << bit) - 1u));
-						const uint64_t rank = a.f.super[blk[v] >> kSuperShift] + q0v[v].x + acc;
-						hit[v] = true;
-						e[v] = __ldg(a.f.ids + rank);
+				}
+				/* bit, rank, ID reads */
+	#pragma unroll
+				for (int v = 0; v < H; ++v) {
+					hit[v] = false;
+					e[v] = 0;
+					if (ok && v < (int)h) {
+						const uint32_t d[7] = {q0v[v].y, q0v[v].z, q0v[v].w, q1v[v].x, q1v[v].y,
+								q1v[v].z, q1v[v].w};
+						const uint32_t ws = rr[v] >> 5, bit = rr[v] & 31u;
+						uint32_t acc = 0, word = 0;
+	#pragma unroll
+						for (int i = 0; i < 7; ++i) {
+							if ((uint32_t)i < ws)
+								acc += __popc(d[i]);
+							if ((uint32_t)i == ws)
+								word = d[i];
+						}
+						if ((word >> bit) & 1u) {
+							acc += __popc(word & ((1u << bit) - 1u));
+							const uint64_t rank = a.f.super[blk[v] >> kSuperShift] + q0v[v].x + acc;
+							hit[v] = true;
+							e[v] = __ldg(a.f.ids + rank);
+						}
 					}
 				}
 			}
@@ -290,7 +309,7 @@ __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglon
 	__syncwarp();
 }
 
-template <int H>
+template <int H, bool DENSE>
 __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
@@ -331,11 +350,11 @@ __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 					: (len2 >= k ? (uint32_t)(len2 - k + 1) : 0u);
 			uint32_t satc = 0;
 			if (fc) {
-				mibf_scan_mate<H>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1, satc, lc,
-						lane);
+				mibf_scan_mate<H, DENSE>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1, satc,
+						lc, lane);
 				if (a.seq2)
-					mibf_scan_mate<H>(a, tab, cw, iw, TA, TB, TC, a.seq2 + b2, len2, satc, lc,
-							lane);
+					mibf_scan_mate<H, DENSE>(a, tab, cw, iw, TA, TB, TC, a.seq2 + b2, len2,
+							satc, lc, lane);
 			}
 			/* significant IDs */
 			uint32_t cmask = 0, maxns = 0;
@@ -499,6 +518,37 @@ __global__ void mibf_block_build_kernel(const uint32_t *raw, uint64_t nwords, ui
 	}
 }
 
+/* Popcount of each 64-bit word of the bit vector. */
+__global__ void mibf_word_pop_kernel(const uint64_t *raw, uint64_t n, unsigned long long *pop)
+{
+	for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+			i += (uint64_t)gridDim.x * blockDim.x)
+		pop[i] = (unsigned long long)__popcll(raw[i]);
+}
+
+/* Dense ID map: two entries (bit positions 2t, 2t+1) per thread, so that the
+ * 32-bit stores of a warp are contiguous. */
+__global__ void mibf_dense_build_kernel(const uint64_t *raw, uint64_t m,
+		const unsigned long long *rank, const uint16_t *ids, uint32_t nids, uint32_t *dense2)
+{
+	for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < m / 2;
+			t += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t p = 2 * t, w = raw[p >> 6];
+		const unsigned b = (unsigned)(p & 63);
+		uint64_t r = rank[p >> 6] + (uint64_t)__popcll(b ? (w & ((1ull << b) - 1)) : 0ull);
+		uint32_t out = 0;
+		for (int j = 0; j < 2; ++j) {
+			if ((w >> (b + j)) & 1ull) {
+				const uint32_t e = ids[r++];
+				const uint32_t id = e & 0x7FFFu;
+				const uint32_t v = (e & kMibfSat) | ((id >= 1 && id < nids) ? id : 0x7FFFu);
+				out |= v << (16 * j);
+			}
+		}
+		dense2[t] = out;
+	}
+}
+
 } // namespace bbt
 
 using namespace bbt;
@@ -521,62 +571,156 @@ static int pick_h(unsigned h)
 	return h <= 1 ? 1 : h <= 2 ? 2 : h <= 3 ? 3 : h <= 4 ? 4 : h <= 6 ? 6 : h <= 8 ? 8 : 16;
 }
 
-template <int H>
+template <int H, bool D>
 static cudaError_t launch_h(const MibfArgs &a, int grid, size_t smem, cudaStream_t s)
 {
-	mibf_query_kernel<H><<<grid, 128, smem, s>>>(a);
+	mibf_query_kernel<H, D><<<grid, 128, smem, s>>>(a);
 	return cudaGetLastError();
 }
 
-/* Blocks per SM of the H variant with smem bytes of shared memory (also sets
- * the variant's shared-memory limit, which must precede its launch). */
-template <int H>
+/* Blocks per SM of a variant with smem bytes of shared memory (also sets the
+ * variant's shared-memory limit, which must precede its launch). */
+template <int H, bool D>
 static int occupancy_h(size_t smem)
 {
-	cudaFuncSetAttribute(mibf_query_kernel<H>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	cudaFuncSetAttribute(mibf_query_kernel<H, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			(int)smem);
 	int nb = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mibf_query_kernel<H>, 128, smem);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mibf_query_kernel<H, D>, 128, smem);
 	return nb > 0 ? nb : 1;
 }
 
-static cudaError_t launch_query(const MibfArgs &a, int hsel, int grid, size_t smem,
+template <bool D>
+static cudaError_t launch_query_d(const MibfArgs &a, int hsel, int grid, size_t smem,
 		cudaStream_t s)
 {
 	switch (hsel) {
-	case 1: return launch_h<1>(a, grid, smem, s);
-	case 2: return launch_h<2>(a, grid, smem, s);
-	case 3: return launch_h<3>(a, grid, smem, s);
-	case 4: return launch_h<4>(a, grid, smem, s);
-	case 6: return launch_h<6>(a, grid, smem, s);
-	case 8: return launch_h<8>(a, grid, smem, s);
-	default: return launch_h<16>(a, grid, smem, s);
+	case 1: return launch_h<1, D>(a, grid, smem, s);
+	case 2: return launch_h<2, D>(a, grid, smem, s);
+	case 3: return launch_h<3, D>(a, grid, smem, s);
+	case 4: return launch_h<4, D>(a, grid, smem, s);
+	case 6: return launch_h<6, D>(a, grid, smem, s);
+	case 8: return launch_h<8, D>(a, grid, smem, s);
+	default: return launch_h<16, D>(a, grid, smem, s);
 	}
 }
 
-static int query_occupancy(int hsel, size_t smem)
+template <bool D>
+static int query_occupancy_d(int hsel, size_t smem)
 {
 	switch (hsel) {
-	case 1: return occupancy_h<1>(smem);
-	case 2: return occupancy_h<2>(smem);
-	case 3: return occupancy_h<3>(smem);
-	case 4: return occupancy_h<4>(smem);
-	case 6: return occupancy_h<6>(smem);
-	case 8: return occupancy_h<8>(smem);
-	default: return occupancy_h<16>(smem);
+	case 1: return occupancy_h<1, D>(smem);
+	case 2: return occupancy_h<2, D>(smem);
+	case 3: return occupancy_h<3, D>(smem);
+	case 4: return occupancy_h<4, D>(smem);
+	case 6: return occupancy_h<6, D>(smem);
+	case 8: return occupancy_h<8, D>(smem);
+	default: return occupancy_h<16, D>(smem);
 	}
 }
 
-/* Upload the bit vector and build the rank blocks. */
-static int upload_bits(bbt_mibf *ctx, const std::string &sdsl)
+static cudaError_t launch_query(const MibfArgs &a, bool dense, int hsel, int grid, size_t smem,
+		cudaStream_t s)
 {
-	const uint64_t m = ctx->hd.m, nwords = m / 32, bytes = m / 8;
+	return dense ? launch_query_d<true>(a, hsel, grid, smem, s)
+	             : launch_query_d<false>(a, hsel, grid, smem, s);
+}
+
+static int query_occupancy(bool dense, int hsel, size_t smem)
+{
+	return dense ? query_occupancy_d<true>(hsel, smem) : query_occupancy_d<false>(hsel, smem);
+}
+
+/* Exclusive scan of n 64-bit counts into out (cub). */
+static int scan_counts(bbt_mibf *ctx, const unsigned long long *in, unsigned long long *out,
+		uint64_t n)
+{
+	size_t tmp_bytes = 0;
+	cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, in, out, (int64_t)n);
+	void *tmp = nullptr;
+	if (cudaMalloc(&tmp, tmp_bytes) != cudaSuccess)
+		return mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(scan)");
+	cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, in, out, (int64_t)n);
+	cudaError_t e = cudaDeviceSynchronize();
+	cudaFree(tmp);
+	if (e != cudaSuccess)
+		return mibf_fail(ctx, BBT_ERR_CUDA, std::string("scan: ") + cudaGetErrorString(e));
+	return BBT_OK;
+}
+
+/* Rank blocks (32 bytes per 224 bits) from the raw bit vector. */
+static int build_blocks(bbt_mibf *ctx, const uint32_t *d_raw)
+{
+	const uint64_t m = ctx->hd.m, nwords = m / 32;
+	const uint64_t nblocks = (m + kBlockBits - 1) / kBlockBits;
+	const uint64_t nsuper = (nblocks >> kSuperShift) + 1;
+	unsigned long long *d_pop = nullptr, *d_rank = nullptr;
+	int rc = BBT_OK;
+	if (cudaMalloc(&d_pop, nblocks * 8) != cudaSuccess ||
+			cudaMalloc(&d_rank, nblocks * 8) != cudaSuccess ||
+			cudaMalloc(&ctx->d_blocks, nblocks * 32) != cudaSuccess ||
+			cudaMalloc(&ctx->d_super, nsuper * 8) != cudaSuccess)
+		rc = mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(rank blocks)");
+	const int grid = ctx->num_sms * 8;
+	if (rc == BBT_OK) {
+		mibf_block_pop_kernel<<<grid, 256>>>(d_raw, nwords, nblocks, d_pop);
+		rc = scan_counts(ctx, d_pop, d_rank, nblocks);
+	}
+	if (rc == BBT_OK) {
+		mibf_block_build_kernel<<<grid, 256>>>(d_raw, nwords, nblocks, d_rank, ctx->d_super,
+				ctx->d_blocks);
+		cudaError_t e = cudaDeviceSynchronize();
+		if (e != cudaSuccess)
+			rc = mibf_fail(ctx, BBT_ERR_CUDA, std::string("rank blocks: ") +
+					cudaGetErrorString(e));
+	}
+	cudaFree(d_pop);
+	cudaFree(d_rank);
+	return rc;
+}
+
+/* Dense ID map from the raw bit vector and the ID array. */
+static int build_dense(bbt_mibf *ctx, const uint32_t *d_raw, const std::vector<uint16_t> &ids)
+{
+	const uint64_t m = ctx->hd.m, nw = m / 64, pop = ctx->hd.pop;
+	unsigned long long *d_pop = nullptr, *d_rank = nullptr;
+	uint16_t *d_ids = nullptr;
+	int rc = BBT_OK;
+	if (cudaMalloc(&d_pop, nw * 8) != cudaSuccess || cudaMalloc(&d_rank, nw * 8) != cudaSuccess ||
+			cudaMalloc(&d_ids, std::max<uint64_t>(pop, 1) * 2) != cudaSuccess ||
+			cudaMalloc(&ctx->d_dense, m * 2) != cudaSuccess)
+		rc = mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(dense ID map)");
+	if (rc == BBT_OK && pop &&
+			cudaMemcpy(d_ids, ids.data(), pop * 2, cudaMemcpyHostToDevice) != cudaSuccess)
+		rc = mibf_fail(ctx, BBT_ERR_CUDA, "cudaMemcpy(IDs)");
+	const int grid = ctx->num_sms * 8;
+	if (rc == BBT_OK) {
+		mibf_word_pop_kernel<<<grid, 256>>>((const uint64_t *)d_raw, nw, d_pop);
+		rc = scan_counts(ctx, d_pop, d_rank, nw);
+	}
+	if (rc == BBT_OK) {
+		mibf_dense_build_kernel<<<grid, 256>>>((const uint64_t *)d_raw, m, d_rank, d_ids,
+				(uint32_t)ctx->names.size(), (uint32_t *)ctx->d_dense);
+		cudaError_t e = cudaDeviceSynchronize();
+		if (e != cudaSuccess)
+			rc = mibf_fail(ctx, BBT_ERR_CUDA, std::string("dense ID map: ") +
+					cudaGetErrorString(e));
+	}
+	cudaFree(d_pop);
+	cudaFree(d_rank);
+	cudaFree(d_ids);
+	return rc;
+}
+
+/* Upload the bit vector, then build the layout the parameters ask for. */
+static int load_device(bbt_mibf *ctx, const std::string &sdsl, const std::vector<uint16_t> &ids)
+{
+	const uint64_t m = ctx->hd.m, bytes = m / 8, pop = ctx->hd.pop;
 	FILE *f = fopen(sdsl.c_str(), "rb");
 	if (!f)
 		return mibf_fail(ctx, BBT_ERR_IO, "Error: " + sdsl + " File cannot be opened");
 	uint32_t *d_raw = nullptr;
-	cudaError_t e = cudaMalloc(&d_raw, bytes);
-	if (e != cudaSuccess) {
+	if (cudaMalloc(&d_raw, bytes) != cudaSuccess) {
 		fclose(f);
 		return mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(bit vector)");
 	}
@@ -592,37 +736,23 @@ static int upload_bits(bbt_mibf *ctx, const std::string &sdsl)
 		done += n;
 	}
 	fclose(f);
-	const uint64_t nblocks = (m + kBlockBits - 1) / kBlockBits;
-	const uint64_t nsuper = (nblocks >> kSuperShift) + 1;
-	unsigned long long *d_pop = nullptr, *d_rank = nullptr;
-	void *d_tmp = nullptr;
-	size_t tmp_bytes = 0;
-	if (rc == BBT_OK) {
-		if (cudaMalloc(&d_pop, nblocks * 8) != cudaSuccess ||
-				cudaMalloc(&d_rank, nblocks * 8) != cudaSuccess ||
-				cudaMalloc(&ctx->d_blocks, nblocks * 32) != cudaSuccess ||
-				cudaMalloc(&ctx->d_super, nsuper * 8) != cudaSuccess)
-			rc = mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(rank blocks)");
+	int layout = ctx->p.layout;
+	if (rc == BBT_OK && layout == BBT_MIBF_LAYOUT_AUTO) {
+		size_t free_b = 0, total_b = 0;
+		cudaMemGetInfo(&free_b, &total_b);
+		const double need = 2.0 * m + 2.0 * pop + m / 8.0 + (1ull << 30);
+		layout = need < 0.7 * (double)free_b ? BBT_MIBF_LAYOUT_DENSE : BBT_MIBF_LAYOUT_RANK;
 	}
-	if (rc == BBT_OK) {
-		const int grid = ctx->num_sms * 8;
-		mibf_block_pop_kernel<<<grid, 256>>>(d_raw, nwords, nblocks, d_pop);
-		cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_pop, d_rank, (int64_t)nblocks);
-		if (cudaMalloc(&d_tmp, tmp_bytes) != cudaSuccess)
-			rc = mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(scan)");
-		else {
-			cub::DeviceScan::ExclusiveSum(d_tmp, tmp_bytes, d_pop, d_rank, (int64_t)nblocks);
-			mibf_block_build_kernel<<<grid, 256>>>(d_raw, nwords, nblocks, d_rank, ctx->d_super,
-					ctx->d_blocks);
-			e = cudaDeviceSynchronize();
-			if (e != cudaSuccess)
-				rc = mibf_fail(ctx, BBT_ERR_CUDA, std::string("rank blocks: ") +
-						cudaGetErrorString(e));
-		}
+	if (rc == BBT_OK && layout == BBT_MIBF_LAYOUT_DENSE) {
+		rc = build_dense(ctx, d_raw, ids);
+	} else if (rc == BBT_OK) {
+		rc = build_blocks(ctx, d_raw);
+		if (rc == BBT_OK && cudaMalloc(&ctx->d_ids, std::max<uint64_t>(pop, 1) * 2) != cudaSuccess)
+			rc = mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(IDs)");
+		if (rc == BBT_OK && pop &&
+				cudaMemcpy(ctx->d_ids, ids.data(), pop * 2, cudaMemcpyHostToDevice) != cudaSuccess)
+			rc = mibf_fail(ctx, BBT_ERR_CUDA, "cudaMemcpy(IDs)");
 	}
-	cudaFree(d_tmp);
-	cudaFree(d_pop);
-	cudaFree(d_rank);
 	cudaFree(d_raw);
 	return rc;
 }
@@ -636,6 +766,7 @@ extern "C" int bbt_mibf_close(bbt_mibf *ctx)
 		cudaFree(ctx->d_blocks);
 		cudaFree(ctx->d_super);
 		cudaFree(ctx->d_ids);
+		cudaFree(ctx->d_dense);
 		cudaFree(ctx->d_tables);
 		cudaFree(ctx->d_counts);
 		cudaFree(ctx->d_work);
@@ -698,15 +829,9 @@ extern "C" int bbt_mibf_open(const char *bf_path, const bbt_mibf_params *params,
 	if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
 			cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess)
 		return bail(mibf_fail(ctx, BBT_ERR_CUDA, "cannot create a stream"));
-	rc = upload_bits(ctx, mibf_sdsl_path(bf_path));
+	rc = load_device(ctx, mibf_sdsl_path(bf_path), ids);
 	if (rc)
 		return bail(rc);
-	const uint64_t nid = ctx->hd.pop ? ctx->hd.pop : 1;
-	if (cudaMalloc(&ctx->d_ids, nid * 2) != cudaSuccess)
-		return bail(mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(IDs)"));
-	if (ctx->hd.pop && cudaMemcpy(ctx->d_ids, ids.data(), ctx->hd.pop * 2,
-			cudaMemcpyHostToDevice) != cudaSuccess)
-		return bail(mibf_fail(ctx, BBT_ERR_CUDA, "cudaMemcpy(IDs)"));
 	std::vector<uint16_t>().swap(ids);
 	std::vector<unsigned long long> tabs = mibf_seed_tables(ctx->hd.seeds, ctx->hd.k);
 	const size_t nc = counts_len(ctx) + 1; /* + reads */
@@ -828,6 +953,7 @@ static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, cons
 	a.f.blocks = ctx->d_blocks;
 	a.f.super = ctx->d_super;
 	a.f.ids = ctx->d_ids;
+	a.f.dense = ctx->d_dense;
 	a.f.m = ctx->hd.m;
 	a.f.minv = ~0ull / ctx->hd.m;
 	a.f.h = ctx->hd.h;
@@ -858,14 +984,15 @@ static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, cons
 	a.T = tally_slots(nids);
 	const int hsel = pick_h(ctx->hd.h);
 	const size_t smem = mibf_smem_bytes(a.f.nse, a.T, 4);
-	const int grid = ctx->num_sms * query_occupancy(hsel, smem);
+	const bool dense = ctx->d_dense != nullptr;
+	const int grid = ctx->num_sms * query_occupancy(dense, hsel, smem);
 	MIBF_TRY(ctx, cudaMemsetAsync(batch_counts, 0, nc * 8, s));
 	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, 8, s));
 	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_flags, 0, 4, s));
 	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_stat, 0, 3 * 8, s));
 	MIBF_TRY(ctx, cudaEventRecord(ctx->ev0, s));
 	if (b->n_reads)
-		MIBF_TRY(ctx, launch_query(a, hsel, grid, smem, s));
+		MIBF_TRY(ctx, launch_query(a, dense, hsel, grid, smem, s));
 	MIBF_TRY(ctx, cudaEventRecord(ctx->ev1, s));
 	mibf_commit_kernel<<<1, 256, 0, s>>>(batch_counts, ctx->d_counts, (uint32_t)nc,
 			ctx->d_flags, b->n_reads);
@@ -1056,6 +1183,13 @@ extern "C" int bbt_mibf_summary_tsv(bbt_mibf *ctx, uint64_t read_count, char *bu
 		buf[n] = 0;
 	}
 	return BBT_OK;
+}
+
+extern "C" int bbt_mibf_layout(const bbt_mibf *ctx)
+{
+	if (!ctx || ctx->host_only)
+		return BBT_ERR_ARG;
+	return ctx->d_dense ? BBT_MIBF_LAYOUT_DENSE : BBT_MIBF_LAYOUT_RANK;
 }
 
 extern "C" int bbt_mibf_last_counts(bbt_mibf *ctx, uint64_t *out)

@@ -85,6 +85,7 @@ struct bbt_mibf {
 	uint4 *d_blocks = nullptr;            /* 32-byte rank blocks */
 	unsigned long long *d_super = nullptr; /* rank at each superblock start */
 	uint16_t *d_ids = nullptr;
+	uint16_t *d_dense = nullptr;          /* dense ID map (one entry per bit), or null */
 	unsigned long long *d_tables = nullptr;
 	unsigned long long *d_counts = nullptr;
 	unsigned long long *d_work = nullptr;

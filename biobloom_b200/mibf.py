@@ -31,7 +31,7 @@ def min_fpr_to_score(min_fpr):
 class MIBFClassifier:
     def __init__(self, filter_file, *, score=1e-10, frame_matches=1, multi=1.0, streak=3,
                  min_nonsat=0, best_hit_agree=False, hit_only=False, device=0,
-                 host_only=False):
+                 host_only=False, layout=L.MIBF_LAYOUT_AUTO):
         lib = L.lib()
         p = L.MibfParams()
         lib.bbt_mibf_default_params(ctypes.byref(p))
@@ -43,6 +43,7 @@ class MIBFClassifier:
         p.best_hit_agree = int(bool(best_hit_agree))
         p.hit_only = int(bool(hit_only))
         p.device = int(device)
+        p.layout = int(layout)
         ctx = ctypes.c_void_p()
         opener = lib.bbt_mibf_open_host if host_only else lib.bbt_mibf_open
         L.check_mibf(opener(str(filter_file).encode(), ctypes.byref(p), ctypes.byref(ctx)))
@@ -54,6 +55,7 @@ class MIBFClassifier:
         m, h, k, ns = ctypes.c_uint64(), ctypes.c_uint(), ctypes.c_uint(), ctypes.c_uint()
         lib.bbt_mibf_info(ctx, ctypes.byref(m), ctypes.byref(h), ctypes.byref(k), ctypes.byref(ns))
         self.m, self.h, self.k, self.n_seeds = m.value, h.value, k.value, ns.value
+        self.layout = None if host_only else lib.bbt_mibf_layout(ctx)
 
     # -- host-side pieces ------------------------------------------------------
     def frame_probs(self):

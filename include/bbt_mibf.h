@@ -68,6 +68,13 @@ typedef struct bbt_mibf bbt_mibf;
 #define BBT_MIBF_OUT_FASTA 1
 #define BBT_MIBF_OUT_FASTQ 2
 
+/* Device layouts of the filter (bbt_mibf_params.layout). */
+#define BBT_MIBF_LAYOUT_AUTO 0   /* dense when it fits comfortably in free HBM */
+#define BBT_MIBF_LAYOUT_RANK 1   /* bit vector in 32-byte rank blocks + ID array:
+                                    m/7 + 2*PopCount bytes, two reads per hit */
+#define BBT_MIBF_LAYOUT_DENSE 2  /* one 16-bit entry per bit: 2*m bytes, one read
+                                    per probe */
+
 /* Options of biobloommicategorizer (BioBloomMICategorizer.cpp:78-122). */
 typedef struct {
 	double score;            /* p-value threshold; -s N sets 10^(-N/10). [1e-10] */
@@ -81,6 +88,7 @@ typedef struct {
 	int device;              /* CUDA device ordinal */
 	uint64_t max_batch_bases;  /* staging capacity per host batch; 0 = default */
 	uint64_t max_batch_reads;
+	int layout;              /* BBT_MIBF_LAYOUT_*; no reference counterpart */
 } bbt_mibf_params;
 
 void bbt_mibf_default_params(bbt_mibf_params *p);
@@ -95,6 +103,8 @@ void bbt_mibf_default_params(bbt_mibf_params *p);
 int bbt_mibf_open(const char *bf_path, const bbt_mibf_params *params, bbt_mibf **out);
 int bbt_mibf_close(bbt_mibf *ctx);
 const char *bbt_mibf_last_error(const bbt_mibf *ctx);
+/* The layout the context built (BBT_MIBF_LAYOUT_RANK or _DENSE). */
+int bbt_mibf_layout(const bbt_mibf *ctx);
 /* Targets + 1 (m_fullIDs.size()). */
 unsigned bbt_mibf_num_ids(const bbt_mibf *ctx);
 const char *bbt_mibf_id_name(const bbt_mibf *ctx, unsigned id);

@@ -141,10 +141,11 @@ def _opts(d):
     return o
 
 
+@pytest.mark.parametrize("layout", [1, 2])
 @pytest.mark.parametrize("tag", ["ss", "km"])
 @pytest.mark.parametrize("paired", [False, True])
 @pytest.mark.parametrize("oi", range(len(OPTS)))
-def test_abi_host_batch_matches_oracle(built, tag, paired, oi):
+def test_abi_host_batch_matches_oracle(built, tag, paired, oi, layout):
     from biobloom_b200.mibf import MIBFClassifier
     targets, filters, _, names = built
     path, f = filters[tag]
@@ -153,7 +154,9 @@ def test_abi_host_batch_matches_oracle(built, tag, paired, oi):
     reads, reads2 = _reads(rng, targets, 700, paired=paired)
     want = _oracle_query(f, names, reads, reads2, o)
     mc = MIBFClassifier(path, score=o["score"], frame_matches=o["frame_matches"],
-                        multi=o["multi"], min_nonsat=o["min_nonsat"], best_hit_agree=o["best"])
+                        multi=o["multi"], min_nonsat=o["min_nonsat"], best_hit_agree=o["best"],
+                        layout=layout)
+    assert mc.layout == layout
     got, sat = mc.classify(reads, reads2, max_hits=2)  # max_hits 2 exercises the retry
     for i, (res, s) in enumerate(want):
         assert (got[i], int(sat[i])) == (res, s), i
@@ -165,7 +168,8 @@ def test_abi_host_batch_matches_oracle(built, tag, paired, oi):
     mc.close()
 
 
-def test_abi_device_batch_matches_host_batch(built):
+@pytest.mark.parametrize("layout", [1, 2])
+def test_abi_device_batch_matches_host_batch(built, layout):
     import torch
     from biobloom_b200.mibf import MIBFClassifier
     from biobloom_b200.classifier import pack
@@ -173,7 +177,7 @@ def test_abi_device_batch_matches_host_batch(built):
     path, f = filters["ss"]
     rng = np.random.default_rng(5)
     reads, _ = _reads(rng, targets, 3000)
-    mc = MIBFClassifier(path)
+    mc = MIBFClassifier(path, layout=layout)
     want, wsat = mc.classify(reads)
     seq, off = pack(reads)
     dseq = torch.from_numpy(seq.copy()).cuda()
@@ -210,6 +214,26 @@ def test_gpu_maker_matches_oracle_build(built, tag, tmp_path):
     for ext in (".bf", ".sdsl", "_ids.txt"):
         with open(path[:-3] + ext, "rb") as a, open(str(tmp_path / "g") + ext, "rb") as b:
             assert a.read() == b.read(), ext
+
+
+def test_ids_outside_the_names_file_tally_nothing(tmp_path):
+    """IDs in the filter that the ID file does not name (and ID 0) count as hits
+    and saturation but are never results, in both layouts."""
+    import shutil
+    from biobloom_b200.mibf import MIBFClassifier
+    rng = np.random.default_rng(8)
+    seqs = [_genome(rng, 3000).tobytes() for _ in range(6)]
+    f = oracle_lib.MIBF.build(seqs, [1, 2, 3, 4, 5, 6], k=21, h=2, occupancy=0.5)
+    f.store(str(tmp_path / "x"))
+    with open(tmp_path / "x_ids.txt", "w") as fh:   # names only IDs 1-3
+        fh.write("1\ta\n2\tb\n3\tc\n")
+    reads, _ = _reads(rng, seqs, 300)
+    want = _oracle_query(f, ["a", "b", "c"], reads, None, _opts({}))
+    for layout in (1, 2):
+        mc = MIBFClassifier(str(tmp_path / "x.bf"), layout=layout)
+        got, sat = mc.classify(reads)
+        assert [(g, int(s)) for g, s in zip(got, sat)] == [(r, s) for r, s in want]
+        assert mc.last_counts()[2] > 0
 
 
 def test_gpu_maker_multi_contig_ids(tmp_path):
