@@ -23,8 +23,19 @@ weight 19 drawn from the seed; 20M single-end 150 bp reads, 90% from the
 targets with 1% substitutions, 10% uniform random.  A step classifies all
 reads once (reads and the 5 GB filter resident in HBM, far above L2).
 
+With --workload varlen: one filter (k=25, FPR 0.075, 2.12 GB) from a seeded
+3.1 Gbp reference (41% GC, 45% of bases in repeat families of 300 bp - 6 kb at
+10-20% divergence); 50M single-end reads, 95% log-uniform over 50-300 bp and
+5% log-uniform over 300 bp - 10 kb, 70% from the reference with 1%
+substitutions, 30% random.  The batched path (autotuned persistent kernel,
+long reads first, launches captured in one CUDA graph) is timed against the
+plain path (one warp per read, one launch per batch of 256k reads).
+With --workload small: one filter from a seeded 5 Mbp uniform reference,
+1M single-end 150 bp reads, 50% from the reference with 1% substitutions
+(the filter, 3.4 MB, is L2-resident).
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--workload bf|mibf]
+                  [--workload bf|mibf|varlen|small]
 """
 import argparse
 import json
@@ -494,6 +505,301 @@ def check_sample(paths, s1, s2, off, hits1, hits2, n):
                                                         (g2 != w2).any(1).sum())}
 
 
+# ------------------------------------------------- single-filter workloads
+
+SINGLE = {
+    "varlen": dict(name="3.1 Gbp", glen=3_100_000_000, gc=0.41, repeat_frac=0.45, rep_min=300,
+                   rep_max=6000, div_min=0.10, div_max=0.20, reads=50_000_000, len_min=50,
+                   len_max=300, long_frac=0.05, long_min=300, long_max=10_000, ref_frac=0.7,
+                   sub=0.01, seed=3003,
+                   workload="1 filter from a 3.1 Gbp reference (41% GC, 45% repeats 300 bp-6 kb "
+                            "at 10-20% divergence; k=25, FPR 0.075, 2.12 GB), 50M single-end "
+                            "reads 50-300 bp log-uniform with 5% 300 bp-10 kb, 70% from the "
+                            "reference with 1% substitutions, score 0.15"),
+    "small": dict(name="5 Mbp", glen=5_000_000, gc=0.5, repeat_frac=0.0, rep_min=0, rep_max=0,
+                  div_min=0.0, div_max=0.0, reads=1_000_000, len_min=150, len_max=150,
+                  long_frac=0.0, long_min=0, long_max=0, ref_frac=0.5, sub=0.01, seed=1001,
+                  workload="1 filter from a 5 Mbp uniform reference (k=25, FPR 0.075, 3.4 MB), "
+                           "1M single-end 150 bp reads, 50% from the reference with 1% "
+                           "substitutions, score 0.15"),
+}
+PLAIN_BATCH = 1 << 18   # reads per launch of the plain path (the CLI's batch)
+SINGLE_METRIC = "reads/s & Bloom probes/s on 1 B200: batched vs plain kernel, % HBM sector peak"
+
+
+def single_setup(cfg, device, n_reads, rank=0):
+    from biobloom_b200 import synth
+    d = os.path.join(tempfile.gettempdir(), f"bbt_bench_{cfg['seed']}")
+    os.makedirs(d, exist_ok=True)
+    t0 = time.time()
+    g = synth.genome(cfg["seed"], cfg["glen"], gc=cfg["gc"], repeat_frac=cfg["repeat_frac"],
+                     rep_min=cfg["rep_min"], rep_max=cfg["rep_max"], div_min=cfg["div_min"],
+                     div_max=cfg["div_max"])
+    path = os.path.join(d, "genome.bf")
+    if not (os.path.exists(path) and os.path.exists(path[:-2] + "txt")):
+        synth.make_filter([g], path[:-3], "genome", k=K, fpr=FPR, device=device,
+                          sources="genome.fa")
+    log(f"reference + filter: {time.time() - t0:.1f} s")
+    t0 = time.time()
+    p = synth.read_params(cfg["len_min"], cfg["len_max"], long_frac=cfg["long_frac"],
+                          long_min=cfg["long_min"], long_max=cfg["long_max"], sub_rate=cfg["sub"])
+    s1, off, _, _ = synth.reads(cfg["seed"] + 17 + rank, [g], [cfg["ref_frac"]], n_reads, p)
+    log(f"reads: {n_reads} in {time.time() - t0:.1f} s, {int(off[-1])} bases")
+    return d, path, s1, off
+
+
+def single_cpu(d, path, s1, off, budget_s=15.0):
+    """The reference's BioBloomClassifier::filter (oracle/_ref/ref_harness) on a
+    bounded sample of the workload's reads, all host threads."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return None, "oracle/_ref/ref_harness is not built"
+    threads = os.cpu_count() or 1
+
+    def run(n):
+        fq = os.path.join(d, f"sample_{n}.fq")
+        if not os.path.exists(fq):
+            with open(fq, "wb") as f:
+                f.write(b"".join(b"@r%d\n%s\n+\n%s\n" % (i, s1[off[i]:off[i + 1]].tobytes(),
+                                                        b"I" * int(off[i + 1] - off[i]))
+                                 for i in range(n)))
+        pr = subprocess.run([harness, "time", str(SCORE), str(STREAK), str(threads), "0",
+                             os.path.join(d, "refcpu"), path, fq], capture_output=True, text=True)
+        if pr.returncode:
+            return None, "ref_harness failed: " + pr.stderr[-300:]
+        return json.loads([x for x in pr.stdout.splitlines() if x.startswith("{")][-1]), None
+
+    probe = 20000
+    r, err = run(probe)
+    if r is None:
+        return None, err
+    n = int(min(len(off) - 1, max(probe, probe / max(r["seconds"], 1e-6) * budget_s)))
+    n = max(probe, (n // 10000) * 10000)
+    r, err = run(n)
+    if r is None:
+        return None, err
+    return {"value": r["records"] / r["seconds"], "unit": "reads/s", "cores": r["threads"],
+            "kind": "reference",
+            "sample": f"first {r['records']} reads of the workload, BioBloomClassifier::filter "
+                      f"from the reference sources, {r['threads']} OpenMP threads, filter load "
+                      f"excluded", "seconds": r["seconds"]}, None
+
+
+def run_single(args):
+    import ctypes
+
+    import torch
+
+    from biobloom_b200 import BioBloomClassifier
+    from biobloom_b200 import _lib as L
+
+    cfg = SINGLE[args.workload]
+    world, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    n = args.reads if args.reads_set else cfg["reads"]
+    d, path, s1, off = single_setup(cfg, local, n, rank)
+    bases = int(off[-1])
+    h1 = torch.from_numpy(s1[:max(bases, 1)]).pin_memory()
+    hoff = torch.from_numpy(off.view(np.int64)).pin_memory()
+    d1, doff = h1.to(dev), hoff.to(dev)
+    torch.cuda.synchronize()
+    bbc = BioBloomClassifier([path], SCORE, streak_threshold=STREAK, device=local)
+    hits = torch.zeros((n, 1), dtype=torch.int64, device=dev)
+    cat = torch.zeros(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.Stream(device=dev)
+
+    def timed(step):
+        for _ in range(args.warmup):
+            step()
+        stream.synchronize()
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        if pg:
+            t = torch.tensor([ms], device=dev)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # algorithmic probes of the workload (counting pass, outside the timed region)
+    bbc.set_launch(path=L.PATH_PERSISTENT)
+    bbc.set_counting(True)
+    bbc.classify_device(d1, doff, hits=hits, category=cat, stream=stream)
+    stream.synchronize()
+    st = bbc.last_stats()
+    bbc.set_counting(False)
+    alg_probes, issued, frames = st["probes_algorithmic"], st["probes_issued"], st["frames"]
+    want_hits = hits.clone()
+
+    # plain: one warp per read, one launch per batch of PLAIN_BATCH reads
+    bbc.set_launch(path=L.PATH_PLAIN, warps_per_block=8, frames_per_lane=4)
+    bbc.set_schedule(0)
+
+    def plain_step():
+        for i in range(0, n, PLAIN_BATCH):
+            j = min(n, i + PLAIN_BATCH)
+            bbc.classify_device(d1, doff[i:j + 1], hits=hits[i:j], category=cat[i:j],
+                                stream=stream)
+
+    ms_plain = timed(plain_step)
+    plain_launches = 2 * ((n + PLAIN_BATCH - 1) // PLAIN_BATCH)
+    plain_ok = bool(torch.equal(hits, want_hits))
+
+    # batched: autotuned configuration, launches captured in one CUDA graph
+    sample = min(n, 2_000_000)
+    tune = bbc.autotune(d1, doff[:sample + 1])
+    log(f"autotune: {tune}")
+    if tune["path"] == L.PATH_FILTER_MAJOR:  # not capturable; one filter never picks it
+        bbc.set_launch(path=L.PATH_PERSISTENT)
+    bbc.classify_device(d1, doff, hits=hits, category=cat, stream=stream)  # warm-up, same sizes
+    stream.synchronize()
+    hits.zero_()
+    graph = bbc.graph(d1, doff, hits, category=cat, reads_per_launch=tune["reads_per_launch"])
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_batched = timed(lambda: graph.launch(stream))
+    clk = clocks.stop()
+    batched_ok = bool(torch.equal(hits, want_hits))
+    kernels_per_launch = 3 if (tune["long_bases"] and tune["path"] != L.PATH_PLAIN) else 2
+    batched_launches = graph.launches * kernels_per_launch
+
+    # kernel time of one launch of the whole batch in the tuned configuration
+    bbc.classify_device(d1, doff, hits=hits, category=cat, stream=stream)
+    stream.synchronize()
+    k_ms = bbc.last_stats()["classify_ms"]
+
+    parity = None
+    if rank == 0 and not args.no_check:
+        try:
+            from tests import oracle_lib as ol
+            f = ol.Filter.load(path)
+            m = 2000
+            o = off[:m + 1]
+            w, _ = ol.classify(s1[:o[-1]].tobytes(), o, [f], SCORE, STREAK)
+            g = hits[:m].cpu().numpy().view(np.uint64)
+            parity = {"checked_reads": m, "mismatched_reads": int((g != w).any(1).sum())}
+        except Exception as e:  # the oracle is test infrastructure: report, do not fail
+            parity = {"checked_reads": 0, "error": str(e)}
+
+    # e2e: the C ABI with pinned host buffers (staged, pipelined copies)
+    hh = torch.empty((n, 1), dtype=torch.int64).pin_memory()
+    hc = torch.empty(n, dtype=torch.int32).pin_memory()
+
+    def e2e_step():
+        b = L.Batch()
+        b.seq, b.offsets, b.n_reads, b.location = h1.data_ptr(), hoff.data_ptr(), n, L.HOST
+        r = L.Result()
+        r.hits, r.category, r.location = hh.data_ptr(), hc.data_ptr(), L.HOST
+        L.check(L.lib().bbt_classify_batch(bbc._ctx, ctypes.byref(b), ctypes.byref(r), None),
+                bbc._ctx)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if pg:
+        t = torch.tensor([e2e_s], device=dev)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_ok = bool(torch.equal(hh, want_hits.cpu()))
+    if rank != 0:
+        graph.close()
+        bbc.close()
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    cpu, cpu_err = (None, "skipped (--no-cpu)")
+    if world == 1 and not args.no_cpu:
+        cpu, cpu_err = single_cpu(d, path, s1, off)
+    peak, peak_kind = measured_peaks()
+    alg_bytes = 32.0 * alg_probes + bases / 4.0 + n * (8 + 4)
+    achieved = alg_bytes / (k_ms * 1e-3) / 1e9
+    fbytes = os.path.getsize(path)
+    l2_resident = fbytes < 96 << 20
+    line = {
+        "metric": SINGLE_METRIC, "value": world * n / (ms_batched * 1e-3), "unit": "reads/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batched,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic",
+        "config": {"workload": cfg["workload"], "reads_per_gpu": n, "bases_per_gpu": bases,
+                   "filter_bytes": fbytes, "tuned": tune,
+                   "l2": ("filter L2-resident (3.4 MB); reads larger than L2" if l2_resident
+                          else "inputs larger than L2"),
+                   "parallelism": f"replicas x{world} (reads sharded, filter replicated)"},
+        "probes_per_s": world * alg_probes / (ms_batched * 1e-3),
+        "probes_algorithmic_per_step": alg_probes, "probes_issued_per_step": issued,
+        "frames_hashed_per_step": frames,
+        "plain": {"value": world * n / (ms_plain * 1e-3), "unit": "reads/s",
+                  "ms_per_step": ms_plain, "launches_per_step": plain_launches,
+                  "reads_per_launch": PLAIN_BATCH, "equals_batched": plain_ok},
+        "batched_over_plain": ms_plain / ms_batched,
+        "batched_equals_counting_pass": batched_ok,
+        "roofline": {"bound": "l2" if l2_resident else "hbm", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": None, "kernel": "classify_kernel (tuned configuration)",
+                     "classify_ms": k_ms, "algorithmic_bytes_per_launch": alg_bytes},
+        "cpu_baseline": cpu if cpu else {"value": None, "unavailable": cpu_err},
+        "e2e": {"value": world * n / e2e_s, "unit": "reads/s",
+                "h2d_bytes_per_step": int(bases + (n + 1) * 8),
+                "d2h_bytes_per_step": int(n * (8 + 4)), "matches_device_results": e2e_ok},
+        "gpu_launches": batched_launches * args.steps,
+        "graph_launches_per_step": 1,
+        "clocks": clk,
+        "parity_sample": parity,
+    }
+    print(json.dumps(line), flush=True)
+    graph.close()
+    bbc.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def run_single_reference(args):
+    world, rank, local, pg = dist_setup(args)
+    if rank != 0:
+        if pg:
+            pg.barrier()
+            pg.destroy_process_group()
+        return
+    cfg = SINGLE[args.workload]
+    d, path, s1, off = single_setup(cfg, local, min(cfg["reads"], 2_000_000))
+    times, n = [], None
+    for i in range(args.warmup + args.steps):
+        r, err = single_cpu(d, path, s1, off, budget_s=8.0)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": err}))
+            return
+        if i >= args.warmup:
+            times.append(r["value"])
+            n = r["sample"]
+    value = sum(times) / len(times)
+    line = {"impl": "reference", "metric": SINGLE_METRIC, "value": value, "unit": "reads/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic", "config": {"workload": cfg["workload"]},
+            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": os.cpu_count() or 1,
+                             "kind": "reference", "sample": n},
+            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
 # ---------------------------------------------------------------- miBF workload
 
 MI_TARGET_LEN = 2_000_000
@@ -826,15 +1132,21 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity (bytes)")
-    ap.add_argument("--workload", default="bf", choices=["bf", "mibf"])
+    ap.add_argument("--workload", default="bf", choices=["bf", "mibf", "varlen", "small"])
     ap.add_argument("--targets", type=int, default=500, help="miBF targets (--workload mibf)")
-    ap.add_argument("--reads", type=int, default=20_000_000, help="reads (--workload mibf)")
+    ap.add_argument("--reads", type=int, default=None,
+                    help="reads (--workload mibf / varlen / small; default: the workload's)")
     ap.add_argument("--layout", type=int, default=0, help="miBF layout: 0 auto, 1 rank, 2 dense")
     args = ap.parse_args()
+    args.reads_set = args.reads is not None
+    if args.reads is None:
+        args.reads = 20_000_000
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")
     if args.workload == "mibf":
         (run_mibf_reference if args.impl == "reference" else run_mibf)(args)
+    elif args.workload in SINGLE:
+        (run_single_reference if args.impl == "reference" else run_single)(args)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -62,6 +62,12 @@ class FilterView(ctypes.Structure):
                 ("k", ctypes.c_uint)]
 
 
+class Tune(ctypes.Structure):
+    _fields_ = [("path", ctypes.c_int), ("warps_per_block", ctypes.c_int),
+                ("frames_per_lane", ctypes.c_int), ("long_bases", ctypes.c_uint64),
+                ("reads_per_launch", ctypes.c_uint64), ("reads_per_s", ctypes.c_double)]
+
+
 class SynthReadParams(ctypes.Structure):
     _fields_ = [("len_min", ctypes.c_uint32), ("len_max", ctypes.c_uint32),
                 ("long_frac", ctypes.c_double), ("long_min", ctypes.c_uint32),
@@ -127,6 +133,12 @@ def lib():
         "bbt_set_counting": (i32, [vp, i32]),
         "bbt_set_launch": (i32, [vp, i32, i32, i32]),
         "bbt_set_inclusive": (i32, [vp, i32]),
+        "bbt_set_schedule": (i32, [vp, u64]),
+        "bbt_autotune": (i32, [vp, P(Batch), P(Tune)]),
+        "bbt_graph_create": (i32, [vp, P(Batch), P(Result), u64, P(vp)]),
+        "bbt_graph_launch": (i32, [vp, vp]),
+        "bbt_graph_launches": (i32, [vp, P(u64)]),
+        "bbt_graph_destroy": (i32, [vp]),
         "bbt_classify_noalloc": (i32, [P(FilterView), i32, P(Params), P(Batch), vp, vp, vp]),
         "bbt_make_filter": (i32, [vp, P(u64), u64, u32, dbl, u32, u64, cp, cp, cp, i32]),
         "bbt_synth_genome": (i32, [u64, u64, dbl, dbl, ctypes.c_uint32, ctypes.c_uint32, dbl, dbl,

@@ -76,6 +76,31 @@ class BioBloomClassifier:
         L.check(L.lib().bbt_set_launch(self._ctx, path, warps_per_block, frames_per_lane),
                 self._ctx)
 
+    def set_schedule(self, long_bases=0):
+        """Persistent kernel read order: reads of at least long_bases bases
+        first (0 = index order)."""
+        L.check(L.lib().bbt_set_schedule(self._ctx, int(long_bases)), self._ctx)
+
+    def autotune(self, seq, off, seq2=None, off2=None):
+        """Time the kernel configurations on a device-resident sample and keep
+        the fastest (bbt_autotune); returns the chosen configuration."""
+        b = L.Batch()
+        b.seq, b.offsets, b.n_reads, b.location = (seq.data_ptr(), off.data_ptr(),
+                                                   off.numel() - 1, L.DEVICE)
+        if seq2 is not None:
+            b.seq2, b.offsets2 = seq2.data_ptr(), off2.data_ptr()
+        t = L.Tune()
+        L.check(L.lib().bbt_autotune(self._ctx, ctypes.byref(b), ctypes.byref(t)), self._ctx)
+        return {"path": t.path, "warps_per_block": t.warps_per_block,
+                "frames_per_lane": t.frames_per_lane, "long_bases": t.long_bases,
+                "reads_per_launch": t.reads_per_launch, "reads_per_s": t.reads_per_s}
+
+    def graph(self, seq, off, hits, seq2=None, off2=None, hits2=None, category=None,
+              reads_per_launch=0):
+        """A CUDA graph classifying this device batch into these result tensors
+        (bbt_graph_create); call .launch(stream) to run it."""
+        return ClassifyGraph(self, seq, off, hits, seq2, off2, hits2, category, reads_per_launch)
+
     def set_counting(self, on=True):
         L.check(L.lib().bbt_set_counting(self._ctx, int(on)), self._ctx)
 
@@ -192,3 +217,46 @@ class BioBloomClassifier:
 
     def __exit__(self, *a):
         self.close()
+
+
+class ClassifyGraph:
+    """bbt_graph_*: a captured classification of fixed device buffers."""
+
+    def __init__(self, bbc, seq, off, hits, seq2, off2, hits2, category, reads_per_launch):
+        self._bbc = bbc
+        self._keep = (seq, off, hits, seq2, off2, hits2, category)
+        b = L.Batch()
+        b.seq, b.offsets, b.n_reads, b.location = (seq.data_ptr(), off.data_ptr(),
+                                                   off.numel() - 1, L.DEVICE)
+        r = L.Result()
+        r.hits, r.location = hits.data_ptr(), L.DEVICE
+        if seq2 is not None:
+            b.seq2, b.offsets2 = seq2.data_ptr(), off2.data_ptr()
+            r.hits2 = hits2.data_ptr()
+        if category is not None:
+            r.category = category.data_ptr()
+        g = ctypes.c_void_p()
+        L.check(L.lib().bbt_graph_create(bbc._ctx, ctypes.byref(b), ctypes.byref(r),
+                                         int(reads_per_launch), ctypes.byref(g)), bbc._ctx)
+        self._g = g
+
+    @property
+    def launches(self):
+        n = ctypes.c_uint64()
+        L.check(L.lib().bbt_graph_launches(self._g, ctypes.byref(n)), self._bbc._ctx)
+        return n.value
+
+    def launch(self, stream=None):
+        s = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+        L.check(L.lib().bbt_graph_launch(self._g, s), self._bbc._ctx)
+
+    def close(self):
+        if getattr(self, "_g", None):
+            L.lib().bbt_graph_destroy(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

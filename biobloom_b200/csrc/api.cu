@@ -132,6 +132,8 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 	cudaFree(ctx->d_filters);
 	cudaFree(ctx->d_counts);
 	cudaFree(ctx->d_work);
+	cudaFree(ctx->d_order);
+	cudaFree(ctx->d_order_cnt);
 	cudaFree(ctx->d_stat);
 	cudaFree(ctx->d_tmp_hits[0]);
 	cudaFree(ctx->d_tmp_hits[1]);
@@ -370,6 +372,7 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 	OPEN_TRY(cudaMalloc(&ctx->d_counts, sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
 	OPEN_TRY(cudaMemset(ctx->d_counts, 0, sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
 	OPEN_TRY(cudaMalloc(&ctx->d_work, sizeof(unsigned long long)));
+	OPEN_TRY(cudaMalloc(&ctx->d_order_cnt, 2 * sizeof(unsigned long long)));
 	OPEN_TRY(cudaMalloc(&ctx->d_stat, 3 * sizeof(unsigned long long)));
 	OPEN_TRY(cudaMemset(ctx->d_stat, 0, 3 * sizeof(unsigned long long)));
 	ctx->cap_reads = ctx->p.max_batch_reads ? ctx->p.max_batch_reads : (1ull << 20);
@@ -529,6 +532,16 @@ static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStrea
 			lc.path = BBT_PATH_PERSISTENT; /* filters of different k */
 		if (lc.path != BBT_PATH_PLAIN)
 			CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), s));
+		if (lc.path != BBT_PATH_PLAIN && ctx->long_bases) {
+			int rc = grow(ctx, &ctx->d_order, ctx->order_cap, a.n * a.mates);
+			if (rc)
+				return rc;
+			CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_order_cnt, 0, 2 * sizeof(unsigned long long), s));
+			CUDA_TRY(ctx, launch_long_first(a, ctx->long_bases, ctx->d_order, ctx->d_order_cnt,
+					ctx->num_sms, s));
+			a.order = ctx->d_order;
+			ctx->last.kernels += 1;
+		}
 		CUDA_TRY(ctx, launch_classify(a, lc, s));
 	}
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k1, s));
@@ -813,5 +826,249 @@ extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int s
 	int cnt = ctx->lc.count;
 	ctx->lc = pick_config(ctx);
 	ctx->lc.count = cnt;
+	return BBT_OK;
+}
+
+extern "C" int bbt_set_schedule(bbt_ctx *ctx, uint64_t long_bases)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	ctx->long_bases = long_bases;
+	return BBT_OK;
+}
+
+/* ---- autotuner ---- */
+
+namespace {
+
+/* One timed pass of the device batch b in launches of `chunk` reads. */
+int time_pass(bbt_ctx *ctx, const bbt_batch *b, uint64_t chunk, uint64_t *h1, uint64_t *h2,
+		cudaEvent_t e0, cudaEvent_t e1, float *ms)
+{
+	cudaStream_t s = ctx->stream;
+	CUDA_TRY(ctx, cudaEventRecord(e0, s));
+	for (uint64_t i = 0; i < b->n_reads; i += chunk) {
+		bbt_batch sb = *b;
+		sb.n_reads = std::min(chunk, b->n_reads - i);
+		sb.offsets = b->offsets + i;
+		if (b->seq2)
+			sb.offsets2 = b->offsets2 + i;
+		bbt_result r;
+		r.hits = h1 + i * ctx->words;
+		r.hits2 = b->seq2 ? h2 + i * ctx->words : nullptr;
+		r.category = nullptr;
+		r.location = BBT_DEVICE;
+		int rc = classify_device(ctx, &sb, &r, s);
+		if (rc)
+			return rc;
+	}
+	CUDA_TRY(ctx, cudaEventRecord(e1, s));
+	CUDA_TRY(ctx, cudaEventSynchronize(e1));
+	CUDA_TRY(ctx, cudaEventElapsedTime(ms, e0, e1));
+	return BBT_OK;
+}
+
+} // namespace
+
+extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
+{
+	if (!ctx || !b || b->location != BBT_DEVICE || b->n_reads == 0)
+		return fail(ctx, BBT_ERR_ARG, "bbt_autotune: needs a non-empty device batch");
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	const uint64_t n = b->n_reads;
+	const size_t nc = 2 * (ctx->nf + 2) + 2;
+	std::vector<unsigned long long> saved(nc);
+	CUDA_TRY(ctx, cudaDeviceSynchronize());
+	CUDA_TRY(ctx, cudaMemcpy(saved.data(), ctx->d_counts, nc * 8, cudaMemcpyDeviceToHost));
+	const uint64_t saved_reads = ctx->reads_seen;
+	const bbt_params saved_p = ctx->p;
+	const uint64_t saved_long = ctx->long_bases;
+	uint64_t *h1 = nullptr, *h2 = nullptr;
+	cudaEvent_t e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	int rc = BBT_OK;
+	if (cudaMalloc(&h1, n * ctx->words * 8) != cudaSuccess ||
+			(b->seq2 && cudaMalloc(&h2, n * ctx->words * 8) != cudaSuccess))
+		rc = fail(ctx, BBT_ERR_NOMEM, "bbt_autotune: cudaMalloc(results)");
+	bbt_tune best;
+	memset(&best, 0, sizeof best);
+	float best_ms = 1e30f;
+	struct Cand {
+		int path, warps, seg;
+		uint64_t long_bases;
+	};
+	std::vector<Cand> cands;
+	for (int w : {4, 8})
+		for (int sg : {4, 8}) {
+			cands.push_back({BBT_PATH_PLAIN, w, sg, 0});
+			cands.push_back({BBT_PATH_PERSISTENT, w, sg, 0});
+			cands.push_back({BBT_PATH_PERSISTENT, w, sg, 1024});
+			if (auto_path(ctx) == BBT_PATH_FILTER_MAJOR)
+				cands.push_back({BBT_PATH_FILTER_MAJOR, w, sg, 0});
+		}
+	const int cnt = ctx->lc.count;
+	for (const Cand &c : cands) {
+		if (rc)
+			break;
+		ctx->p.path = c.path;
+		ctx->p.warps_per_block = c.warps;
+		ctx->p.frames_per_lane = c.seg;
+		ctx->lc = pick_config(ctx);
+		ctx->lc.count = 0;
+		ctx->long_bases = c.long_bases;
+		float ms = 0;
+		rc = time_pass(ctx, b, n, h1, h2, e0, e1, &ms); /* warm */
+		if (!rc)
+			rc = time_pass(ctx, b, n, h1, h2, e0, e1, &ms);
+		if (!rc && ms < best_ms) {
+			best_ms = ms;
+			best.path = c.path;
+			best.warps_per_block = c.warps;
+			best.frames_per_lane = c.seg;
+			best.long_bases = c.long_bases;
+		}
+	}
+	/* reads per launch for the best kernel configuration */
+	best.reads_per_launch = n;
+	if (!rc) {
+		ctx->p.path = best.path;
+		ctx->p.warps_per_block = best.warps_per_block;
+		ctx->p.frames_per_lane = best.frames_per_lane;
+		ctx->lc = pick_config(ctx);
+		ctx->lc.count = 0;
+		ctx->long_bases = best.long_bases;
+		float chunk_ms = best_ms;
+		for (uint64_t ch : {1ull << 16, 1ull << 18, 1ull << 20}) {
+			if (ch >= n || rc)
+				break;
+			float ms = 0;
+			rc = time_pass(ctx, b, ch, h1, h2, e0, e1, &ms);
+			if (!rc && ms < chunk_ms * 0.98f) {
+				chunk_ms = ms;
+				best.reads_per_launch = ch;
+			}
+		}
+		best.reads_per_s = (double)n * (b->seq2 ? 2 : 1) / (std::min(best_ms, chunk_ms) * 1e-3);
+	}
+	cudaFree(h1);
+	cudaFree(h2);
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	/* the tuning passes leave the summary as it was */
+	cudaMemcpy(ctx->d_counts, saved.data(), nc * 8, cudaMemcpyHostToDevice);
+	ctx->reads_seen = saved_reads;
+	if (rc) {
+		ctx->p = saved_p;
+		ctx->long_bases = saved_long;
+		ctx->lc = pick_config(ctx);
+		ctx->lc.count = cnt;
+		return rc;
+	}
+	ctx->lc.count = cnt;
+	if (out)
+		*out = best;
+	return BBT_OK;
+}
+
+/* ---- CUDA graphs over device batches ---- */
+
+struct bbt_graph {
+	bbt_ctx *ctx = nullptr;
+	cudaGraph_t graph = nullptr;
+	cudaGraphExec_t exec = nullptr;
+	cudaStream_t capture = nullptr;
+	uint64_t reads = 0, launches = 0;
+};
+
+extern "C" int bbt_graph_create(bbt_ctx *ctx, const bbt_batch *b, const bbt_result *r,
+		uint64_t reads_per_launch, bbt_graph **out)
+{
+	if (!ctx || !b || !r || !out || b->location != BBT_DEVICE || r->location != BBT_DEVICE)
+		return fail(ctx, BBT_ERR_ARG, "bbt_graph_create: needs device batch and results");
+	if (!r->hits || (b->seq2 && !r->hits2))
+		return fail(ctx, BBT_ERR_ARG, "bbt_graph_create: result hit arrays are required");
+	if (ctx->lc.path == BBT_PATH_FILTER_MAJOR)
+		return fail(ctx, BBT_ERR_UNSUPPORTED, "bbt_graph_create: the filter-major path reads "
+				"block sums on the host; use the plain or persistent path in a graph");
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	const uint64_t n = b->n_reads;
+	const uint64_t chunk = reads_per_launch ? std::min(reads_per_launch, std::max<uint64_t>(n, 1))
+	                                        : std::max<uint64_t>(n, 1);
+	/* buffers the launches grow must exist before capture */
+	if (ctx->long_bases && ctx->lc.path != BBT_PATH_PLAIN) {
+		int rc = grow(ctx, &ctx->d_order, ctx->order_cap, chunk * (b->seq2 ? 2 : 1));
+		if (rc)
+			return rc;
+	}
+	bbt_graph *g = new bbt_graph();
+	g->ctx = ctx;
+	g->reads = n;
+	cudaError_t e = cudaStreamCreateWithFlags(&g->capture, cudaStreamNonBlocking);
+	if (e == cudaSuccess)
+		e = cudaStreamBeginCapture(g->capture, cudaStreamCaptureModeThreadLocal);
+	int rc = e == cudaSuccess ? BBT_OK : cuda_fail(ctx, e, "cudaStreamBeginCapture");
+	for (uint64_t i = 0; rc == BBT_OK && i < n; i += chunk) {
+		bbt_batch sb = *b;
+		sb.n_reads = std::min(chunk, n - i);
+		sb.offsets = b->offsets + i;
+		if (b->seq2)
+			sb.offsets2 = b->offsets2 + i;
+		bbt_result sr = *r;
+		sr.hits = r->hits + i * ctx->words;
+		sr.hits2 = b->seq2 ? r->hits2 + i * ctx->words : nullptr;
+		sr.category = r->category ? r->category + i : nullptr;
+		rc = classify_device(ctx, &sb, &sr, g->capture);
+		++g->launches;
+	}
+	cudaGraph_t graph = nullptr;
+	e = cudaStreamEndCapture(g->capture, &graph);
+	if (rc == BBT_OK && e != cudaSuccess)
+		rc = cuda_fail(ctx, e, "cudaStreamEndCapture");
+	g->graph = graph;
+	if (rc == BBT_OK) {
+		e = cudaGraphInstantiate(&g->exec, graph, 0);
+		if (e != cudaSuccess)
+			rc = cuda_fail(ctx, e, "cudaGraphInstantiate");
+	}
+	ctx->reads_seen -= std::min(ctx->reads_seen, n); /* capture did not run anything */
+	if (rc) {
+		bbt_graph_destroy(g);
+		return rc;
+	}
+	*out = g;
+	return BBT_OK;
+}
+
+extern "C" int bbt_graph_launch(bbt_graph *g, void *stream)
+{
+	if (!g || !g->exec)
+		return BBT_ERR_ARG;
+	bbt_ctx *ctx = g->ctx;
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	CUDA_TRY(ctx, cudaGraphLaunch(g->exec, stream ? (cudaStream_t)stream : ctx->stream));
+	ctx->reads_seen += g->reads;
+	return BBT_OK;
+}
+
+extern "C" int bbt_graph_launches(const bbt_graph *g, uint64_t *launches)
+{
+	if (!g || !launches)
+		return BBT_ERR_ARG;
+	*launches = g->launches;
+	return BBT_OK;
+}
+
+extern "C" int bbt_graph_destroy(bbt_graph *g)
+{
+	if (!g)
+		return BBT_OK;
+	if (g->exec)
+		cudaGraphExecDestroy(g->exec);
+	if (g->graph)
+		cudaGraphDestroy(g->graph);
+	if (g->capture)
+		cudaStreamDestroy(g->capture);
+	delete g;
 	return BBT_OK;
 }

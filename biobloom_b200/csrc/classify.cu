@@ -133,6 +133,8 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 			r = __shfl_sync(kFull, r, 0);
 			if (r >= total)
 				break;
+			if (a.order)
+				r = a.order[r];
 			uint64_t myword = 0;
 			classify_read<SEG, COUNT, LENGTH_MODE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
 					frame_acc, alg_acc);
@@ -208,6 +210,41 @@ __global__ void summarize_kernel(const uint64_t *__restrict__ h1, const uint64_t
 			atomicAdd(&counts[j], sc[j]);
 }
 
+/* Warp-aggregated split of the reads into long (front of order, in counter 0)
+ * and short (back of order, in counter 1). */
+__global__ void long_first_kernel(ClassifyArgs a, uint64_t long_bases, uint64_t *order,
+		unsigned long long *counters)
+{
+	const uint64_t total = a.n * a.mates;
+	const int lane = threadIdx.x & 31;
+	const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+	for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < total; base += stride) {
+		const uint64_t r = base + threadIdx.x;
+		bool valid = r < total, is_long = false;
+		if (valid) {
+			const uint32_t mate = r >= a.n ? 1u : 0u;
+			const uint64_t i = r - (mate ? a.n : 0);
+			is_long = a.off[mate][i + 1] - a.off[mate][i] >= long_bases;
+		}
+		const unsigned lm = __ballot_sync(kFull, valid && is_long);
+		const unsigned sm = __ballot_sync(kFull, valid && !is_long);
+		unsigned long long b0 = 0, b1 = 0;
+		if (lane == 0) {
+			if (lm)
+				b0 = atomicAdd(counters, (unsigned long long)__popc(lm));
+			if (sm)
+				b1 = atomicAdd(counters + 1, (unsigned long long)__popc(sm));
+		}
+		b0 = __shfl_sync(kFull, b0, 0);
+		b1 = __shfl_sync(kFull, b1, 0);
+		const unsigned below = (1u << lane) - 1u;
+		if (valid && is_long)
+			order[b0 + __popc(lm & below)] = r;
+		else if (valid)
+			order[total - 1 - (b1 + __popc(sm & below))] = r;
+	}
+}
+
 template <int SEG, int ORDER, bool C>
 cudaError_t launch_one(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
 {
@@ -266,6 +303,19 @@ size_t classify_smem_bytes(const LaunchConfig &lc, uint32_t kmax)
 cudaError_t launch_classify(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
 {
 	return lc.seg == 8 ? launch_seg<8>(a, lc, s) : launch_seg<4>(a, lc, s);
+}
+
+cudaError_t launch_long_first(const ClassifyArgs &a, uint64_t long_bases, uint64_t *order,
+		unsigned long long *counters, int num_sms, cudaStream_t s)
+{
+	const uint64_t total = a.n * a.mates;
+	if (total == 0)
+		return cudaSuccess;
+	const uint64_t need = (total + 255) / 256;
+	const uint64_t cap = (uint64_t)num_sms * 8;
+	long_first_kernel<<<(unsigned)(need < cap ? need : cap), 256, 0, s>>>(a, long_bases, order,
+			counters);
+	return cudaGetLastError();
 }
 
 cudaError_t launch_summarize(const uint64_t *h1, const uint64_t *h2, uint64_t n, uint32_t nf,

@@ -31,6 +31,8 @@ struct ClassifyArgs {
 	uint32_t kmax;             /* largest k among the filters */
 	uint64_t *hits[2];         /* n x words per mate array */
 	unsigned long long *work;  /* persistent: next read to take (zeroed) */
+	const uint64_t *order;     /* persistent: optional order of the reads (a permutation
+	                              of [0, n * mates)); NULL = index order */
 	unsigned long long *probes;/* optional: filter words read */
 	unsigned long long *frames;/* optional: frames hashed */
 	unsigned long long *alg_probes; /* optional: words the sequential algorithm reads */
@@ -47,6 +49,12 @@ struct LaunchConfig {
 /* Dynamic shared memory one block needs. */
 size_t classify_smem_bytes(const LaunchConfig &lc, uint32_t kmax);
 cudaError_t launch_classify(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s);
+
+/* Long-first read order for the persistent kernel: reads with at least
+ * long_bases bases first, then the others (order within each group is not
+ * specified; results do not depend on it).  counters: two zeroed words. */
+cudaError_t launch_long_first(const ClassifyArgs &a, uint64_t long_bases, uint64_t *order,
+		unsigned long long *counters, int num_sms, cudaStream_t s);
 
 /* Categories and summary counters for n reads (or pairs when h2 != NULL):
  * counts = aboveThreshold[nf+2], unique[nf+2], multiMatch, noMatch. */

@@ -62,6 +62,11 @@ struct bbt_ctx {
 	uint32_t *d_tp_vmask = nullptr;
 	uint64_t tp_frames_cap = 0;
 	bool same_k = true;
+	/* long-first read order of the persistent kernel (0 = index order) */
+	uint64_t long_bases = 0;
+	uint64_t *d_order = nullptr;
+	uint64_t order_cap = 0;
+	unsigned long long *d_order_cnt = nullptr;
 	cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 	cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr; /* around the last classify kernel */
 	bbt::LaunchConfig lc;

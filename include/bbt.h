@@ -173,6 +173,48 @@ int bbt_set_inclusive(bbt_ctx *ctx, int inclusive);
  * BioBloomCategorizer.cpp:243-249). */
 int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int frames_per_lane);
 
+/* Read order of the persistent kernel: reads of at least long_bases bases are
+ * started first (longest-processing-first scheduling, so that a long read does
+ * not start last and hold the end of the launch); 0 = index order.  Results do
+ * not depend on it.  No reference counterpart. */
+int bbt_set_schedule(bbt_ctx *ctx, uint64_t long_bases);
+
+/*
+ * Autotuner: time every kernel configuration on a device-resident sample
+ * (path plain / persistent / persistent long-first / filter-major when the
+ * filters fit in L2; 4 or 8 warps per block; 4 or 8 frames per lane), keep
+ * the fastest, then pick the reads per launch (64k, 256k, 1M or the whole
+ * sample) for it, and leave the context set to the result.  The summary
+ * counters are left as they were.  No reference counterpart (the reference's
+ * only knob is -t).
+ */
+typedef struct {
+	int path;
+	int warps_per_block;
+	int frames_per_lane;
+	uint64_t long_bases;        /* bbt_set_schedule value */
+	uint64_t reads_per_launch;
+	double reads_per_s;         /* on the sample */
+} bbt_tune;
+int bbt_autotune(bbt_ctx *ctx, const bbt_batch *sample, bbt_tune *out);
+
+/*
+ * CUDA graph of the classification of one device batch in launches of
+ * reads_per_launch reads (0 = one launch), captured once and replayed by
+ * bbt_graph_launch: the launch sequence (work-counter resets, read order,
+ * classification and summary kernels per launch) costs one graph launch.  The
+ * graph is bound to the batch's and results' device pointers: refill those
+ * buffers between launches.  Summary counters are updated at each launch.
+ * Plain and persistent paths only (the filter-major path reads block sums on
+ * the host).  Create it after a warm-up call with the same sizes.
+ */
+typedef struct bbt_graph bbt_graph;
+int bbt_graph_create(bbt_ctx *ctx, const bbt_batch *batch, const bbt_result *result,
+		uint64_t reads_per_launch, bbt_graph **out);
+int bbt_graph_launch(bbt_graph *g, void *stream);
+int bbt_graph_launches(const bbt_graph *g, uint64_t *launches);
+int bbt_graph_destroy(bbt_graph *g);
+
 /* Count filter words read and frames hashed in the following batches
  * (diagnostics; costs atomics).  No reference counterpart. */
 int bbt_set_counting(bbt_ctx *ctx, int on);

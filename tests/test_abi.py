@@ -1,5 +1,5 @@
 """The C ABI library: it loads without a GPU, exports every function that
-include/bbt.h declares, and its host-only entry points (synthetic workloads)
+include/*.h declare, and its host-only entry points (synthetic workloads)
 work on the CPU."""
 import ctypes
 import os
@@ -13,9 +13,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared_functions():
-    txt = open(os.path.join(ROOT, "include", "bbt.h")).read()
-    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
-    return sorted(set(re.findall(r"\b(bbt_[a-z0-9_]+)\s*\(", txt)))
+    inc = os.path.join(ROOT, "include")
+    names = set()
+    for h in sorted(os.listdir(inc)):
+        if h.endswith(".h"):
+            txt = re.sub(r"/\*.*?\*/", "", open(os.path.join(inc, h)).read(), flags=re.S)
+            names.update(re.findall(r"\b(bbt_[a-z0-9_]+)\s*\(", txt))
+    return sorted(names)
 
 
 @pytest.fixture(scope="module")
@@ -30,7 +34,8 @@ def lib():
 def test_header_declares_entry_points():
     names = declared_functions()
     for n in ("bbt_open", "bbt_classify_batch", "bbt_summary", "bbt_close", "bbt_last_error",
-              "bbt_make_filter", "bbt_filter_files", "bbt_filter_pair_files"):
+              "bbt_make_filter", "bbt_filter_files", "bbt_filter_pair_files", "bbt_mibf_open",
+              "bbt_mibf_classify_batch", "bbt_mibf_make", "bbt_mibf_filter_files"):
         assert n in names
 
 

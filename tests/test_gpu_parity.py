@@ -196,6 +196,70 @@ def test_device_batches_and_long_reads(tmp_path):
             assert np.array_equal(hits.cpu().numpy().view(np.uint64), want)
 
 
+def _store(filters, tmp_path, tag):
+    paths = []
+    for i, f in enumerate(filters):
+        stem = str(tmp_path / f"{tag}{i}")
+        f.store(stem + ".bf")
+        ol.write_info(stem + ".txt", f"{tag}{i}", f.k, 0.075, f.h, 1, "x", f.m, 1, 0.1, 0, 0.1)
+        paths.append(stem + ".bf")
+    return paths
+
+
+def test_long_first_schedule_autotune_and_graph(tmp_path):
+    """Mixed-length reads (20 bp - 10 kb) on the device: the long-first read
+    order, the autotuned configuration and a CUDA graph of odd-sized launches
+    all give the oracle's hits; autotuning leaves the summary untouched and
+    each graph launch adds one batch to it."""
+    import torch
+    rng, genomes, filters = _random_case(13, n_filters=2, glen=60000)
+    paths = _store(filters, tmp_path, "v")
+    reads = _random_reads(rng, genomes, 1500, lmin=20, lmax=300)
+    reads += _random_reads(rng, genomes, 100, lmin=300, lmax=10000, nrate=0.001)
+    order = rng.permutation(len(reads))
+    reads = [reads[i] for i in order]
+    seq, off = ol.pack_reads(reads)
+    want, _ = ol.classify(seq, off, filters, 0.15, 3)
+    wc, wcat = ol.summary_counts(want, 2)
+    dseq = torch.tensor(np.frombuffer(seq, dtype=np.uint8), device="cuda")
+    doff = torch.tensor(off.astype(np.int64), device="cuda")
+    with _classifier(paths, path=2) as bbc:
+        for lb in (0, 500, 1):
+            bbc.set_schedule(lb)
+            hits, _, cat = bbc.classify_device(dseq, doff)
+            torch.cuda.synchronize()
+            assert np.array_equal(hits.cpu().numpy().view(np.uint64), want), lb
+        before = bbc.summary()
+        tune = bbc.autotune(dseq, doff)
+        after = bbc.summary()
+        assert np.array_equal(before[0], after[0]) and before[1] == after[1]
+        assert tune["path"] in (1, 2, 3) and tune["reads_per_s"] > 0
+        hits, _, cat = bbc.classify_device(dseq, doff)
+        torch.cuda.synchronize()
+        assert np.array_equal(hits.cpu().numpy().view(np.uint64), want)
+    for launch in (dict(path=1), dict(path=2)):
+        with _classifier(paths, **launch) as bbc:
+            bbc.set_schedule(1000)
+            n = len(reads)
+            hits = torch.zeros((n, 1), dtype=torch.int64, device="cuda")
+            cat = torch.zeros(n, dtype=torch.int32, device="cuda")
+            bbc.classify_device(dseq, doff, hits=hits, category=cat)  # warm-up, same sizes
+            torch.cuda.synchronize()
+            bbc.reset_summary()
+            hits.zero_()
+            g = bbc.graph(dseq, doff, hits, category=cat, reads_per_launch=97)
+            assert g.launches == (n + 96) // 97
+            s = torch.cuda.Stream()
+            g.launch(s)
+            g.launch(s)
+            s.synchronize()
+            assert np.array_equal(hits.cpu().numpy().view(np.uint64), want)
+            assert np.array_equal(cat.cpu().numpy(), wcat)
+            counts, seen = bbc.summary()
+            assert np.array_equal(counts, 2 * wc) and seen == 2 * n
+            g.close()
+
+
 def test_staging_splits_large_host_batches(tmp_path):
     """Host batches larger than the staging slots are split and pipelined."""
     rng, genomes, filters = _random_case(12)
