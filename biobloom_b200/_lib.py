@@ -98,6 +98,28 @@ class MibfResult(ctypes.Structure):
                 ("location", ctypes.c_int)]
 
 
+class ServerParams(ctypes.Structure):
+    _fields_ = [("mem_budget", ctypes.c_uint64), ("slots", ctypes.c_uint32),
+                ("chunk_reads", ctypes.c_uint64), ("max_frames", ctypes.c_uint32)]
+
+
+class Request(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("seq", ctypes.c_void_p), ("offsets", ctypes.c_void_p),
+                ("seq2", ctypes.c_void_p), ("offsets2", ctypes.c_void_p),
+                ("n_reads", ctypes.c_uint64), ("hits", ctypes.c_void_p), ("hits2", ctypes.c_void_p),
+                ("category", ctypes.c_void_p), ("mi_hits", ctypes.c_void_p),
+                ("mi_max_hits", ctypes.c_uint32), ("mi_n_hits", ctypes.c_void_p),
+                ("mi_sat", ctypes.c_void_p)]
+
+
+class RequestStats(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("t_submit", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
+                ("device_bytes", ctypes.c_uint64), ("slot", ctypes.c_uint32)]
+
+
+REQ_BLOOM, REQ_MIBF = 0, 1
+
 _lib = None
 
 
@@ -146,6 +168,12 @@ def lib():
         "bbt_synth_read_lengths": (i32, [u64, P(SynthReadParams), u64, vp]),
         "bbt_synth_reads": (i32, [u64, vp, vp, ctypes.c_uint32, vp, P(SynthReadParams), u64, vp,
                                   vp, vp, vp]),
+        "bbt_server_create": (i32, [vp, vp, P(ServerParams), P(vp)]),
+        "bbt_server_submit": (i32, [vp, P(Request), P(u64)]),
+        "bbt_server_wait": (i32, [vp, u64, dbl, P(RequestStats)]),
+        "bbt_server_load": (i32, [vp, P(u64), P(u64), P(u64)]),
+        "bbt_server_destroy": (i32, [vp]),
+        "bbt_server_last_error": (cp, [vp]),
         "bbt_mibf_default_params": (None, [P(MibfParams)]),
         "bbt_mibf_open": (i32, [cp, P(MibfParams), P(vp)]),
         "bbt_mibf_open_host": (i32, [cp, P(MibfParams), P(vp)]),

@@ -24,14 +24,15 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-I" + os.path.join(ROOT, "include")
           "-Xcompiler", "-fPIC,-fopenmp,-O3,-Wall", "-ccbin", "/usr/bin/g++"]
 LIB_SOURCES = ["classify.cu", "twopass.cu", "api.cu", "noalloc.cu", "maker.cu", "mibf.cu",
                "mibf_make.cu", "formats.cpp", "fastx.cpp", "synth.cpp", "mibf_host.cpp",
-               "mibf_pipeline.cpp"]
+               "mibf_pipeline.cpp", "server.cpp"]
 CLIS = [("biobloomcategorizer", "cli_categorizer.cpp"),
         ("biobloommicategorizer", "cli_micategorizer.cpp")]
 
 
 def _headers():
     hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
-    return hs + [os.path.join(ROOT, "include", "bbt.h"), os.path.join(ROOT, "include", "bbt_mibf.h")]
+    inc = os.path.join(ROOT, "include")
+    return hs + [os.path.join(inc, f) for f in os.listdir(inc) if f.endswith(".h")]
 
 
 def _newer(target, deps):

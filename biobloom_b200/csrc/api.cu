@@ -950,6 +950,8 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 			}
 		}
 		best.reads_per_s = (double)n * (b->seq2 ? 2 : 1) / (std::min(best_ms, chunk_ms) * 1e-3);
+		if (best.reads_per_launch == n)
+			best.reads_per_launch = 0; /* no split beat one launch: launch whole batches */
 	}
 	cudaFree(h1);
 	cudaFree(h2);
@@ -1070,5 +1072,62 @@ extern "C" int bbt_graph_destroy(bbt_graph *g)
 	if (g->capture)
 		cudaStreamDestroy(g->capture);
 	delete g;
+	return BBT_OK;
+}
+
+/* ---- concurrent classification for the serving engine ---- */
+
+int bbt::bf_scratch_init(bbt_ctx *ctx, BfScratch &sc, uint64_t max_reads)
+{
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	CUDA_TRY(ctx, cudaMalloc(&sc.work, sizeof(unsigned long long)));
+	CUDA_TRY(ctx, cudaMalloc(&sc.order_cnt, 2 * sizeof(unsigned long long)));
+	CUDA_TRY(ctx, cudaMalloc(&sc.order, std::max<uint64_t>(max_reads, 1) * 2 * sizeof(uint64_t)));
+	sc.order_cap = std::max<uint64_t>(max_reads, 1) * 2;
+	return BBT_OK;
+}
+
+void bbt::bf_scratch_free(BfScratch &sc)
+{
+	cudaFree(sc.work);
+	cudaFree(sc.order_cnt);
+	cudaFree(sc.order);
+	sc = BfScratch();
+}
+
+int bbt::bf_classify_slot(bbt_ctx *ctx, const uint8_t *seq, const uint64_t *off,
+		const uint8_t *seq2, const uint64_t *off2, uint64_t n, uint64_t *hits, uint64_t *hits2,
+		uint32_t *category, cudaStream_t s, BfScratch &sc)
+{
+	if (n == 0)
+		return BBT_OK;
+	const bool paired = seq2 != nullptr;
+	ClassifyArgs a = base_args(ctx);
+	a.probes = a.frames = a.alg_probes = nullptr;
+	a.seq[0] = seq;
+	a.off[0] = off;
+	a.seq[1] = paired ? seq2 : seq;
+	a.off[1] = paired ? off2 : off;
+	a.n = n;
+	a.mates = paired ? 2 : 1;
+	a.hits[0] = hits;
+	a.hits[1] = paired ? hits2 : nullptr;
+	a.work = sc.work;
+	LaunchConfig lc = ctx->lc;
+	lc.count = 0;
+	if (lc.path == BBT_PATH_FILTER_MAJOR)
+		lc.path = BBT_PATH_PERSISTENT;
+	if (lc.path != BBT_PATH_PLAIN) {
+		CUDA_TRY(ctx, cudaMemsetAsync(sc.work, 0, sizeof(unsigned long long), s));
+		if (ctx->long_bases && n * a.mates <= sc.order_cap) {
+			CUDA_TRY(ctx, cudaMemsetAsync(sc.order_cnt, 0, 2 * sizeof(unsigned long long), s));
+			CUDA_TRY(ctx, launch_long_first(a, ctx->long_bases, sc.order, sc.order_cnt,
+					ctx->num_sms, s));
+			a.order = sc.order;
+		}
+	}
+	CUDA_TRY(ctx, launch_classify(a, lc, s));
+	CUDA_TRY(ctx, launch_summarize(a.hits[0], paired ? a.hits[1] : nullptr, n, ctx->nf,
+			ctx->words, ctx->p.inclusive, category, ctx->d_counts, ctx->num_sms, s));
 	return BBT_OK;
 }

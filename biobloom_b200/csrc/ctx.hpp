@@ -75,6 +75,25 @@ struct bbt_ctx {
 
 namespace bbt {
 int fail(bbt_ctx *ctx, int code, const std::string &msg);
+
+/* Per-stream scratch for classification calls that run concurrently on
+ * several streams of one context (the serving engine): each stream needs its
+ * own work counter and read-order buffer. */
+struct BfScratch {
+	unsigned long long *work = nullptr;
+	unsigned long long *order_cnt = nullptr;
+	uint64_t *order = nullptr;
+	uint64_t order_cap = 0;
+};
+int bf_scratch_init(bbt_ctx *ctx, BfScratch &sc, uint64_t max_reads);
+void bf_scratch_free(BfScratch &sc);
+/* Classify n reads (n pairs when seq2) resident on the device, offsets
+ * relative to seq / seq2, into hits (hits2) and category on stream s, adding to
+ * the summary counters; no host synchronization.  Plain or persistent kernel
+ * (the tuned filter-major order is replaced by the persistent one). */
+int bf_classify_slot(bbt_ctx *ctx, const uint8_t *seq, const uint64_t *off, const uint8_t *seq2,
+		const uint64_t *off2, uint64_t n, uint64_t *hits, uint64_t *hits2, uint32_t *category,
+		cudaStream_t s, BfScratch &sc);
 int cuda_fail(bbt_ctx *ctx, cudaError_t e, const char *what);
 std::string summary_text(const bbt_ctx *ctx, const std::vector<uint64_t> &counts, uint64_t reads);
 }

@@ -461,9 +461,10 @@ __global__ void mibf_commit_kernel(const unsigned long long *batch, unsigned lon
 	if (flags[0])
 		return;
 	for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-		total[i] += batch[i];
+		if (batch[i])
+			atomicAdd(total + i, batch[i]); /* batches on other streams commit too */
 	if (blockIdx.x == 0 && threadIdx.x == 0)
-		total[n] += reads;
+		atomicAdd(total + n, (unsigned long long)reads);
 }
 
 /* Largest frame count of a device batch and a bitmap of the frame counts
@@ -903,6 +904,44 @@ static int ensure_min_count(bbt_mibf *ctx, const std::vector<uint32_t> &fcs, cud
 	return BBT_OK;
 }
 
+int bbt::mibf_reserve_rows(bbt_mibf *ctx, uint32_t rows)
+{
+	const unsigned nids = (unsigned)ctx->names.size();
+	std::lock_guard<std::mutex> lk(ctx->mc_mu);
+	if (ctx->minc_rows >= rows)
+		return BBT_OK;
+	uint32_t *d = nullptr;
+	MIBF_TRY(ctx, cudaDeviceSynchronize());
+	MIBF_TRY(ctx, cudaMalloc(&d, (size_t)rows * nids * 4));
+	if (ctx->h_minc.size() < (size_t)rows * nids) {
+		ctx->h_minc.resize((size_t)rows * nids, 0);
+		ctx->minc_have.resize(rows, 0);
+	}
+	MIBF_TRY(ctx, cudaMemcpy(d, ctx->h_minc.data(), (size_t)rows * nids * 4,
+			cudaMemcpyHostToDevice));
+	cudaFree(ctx->d_minc);
+	ctx->d_minc = d;
+	ctx->minc_rows = rows;
+	return BBT_OK;
+}
+
+static std::vector<uint32_t> host_frame_counts(const bbt_batch *b, unsigned k);
+
+int bbt::mibf_rows_for(bbt_mibf *ctx, const uint64_t *off, const uint64_t *off2, uint64_t n)
+{
+	bbt_batch b;
+	memset(&b, 0, sizeof b);
+	b.offsets = off;
+	b.offsets2 = off2;
+	b.seq2 = off2 ? "" : nullptr;
+	b.n_reads = n;
+	std::vector<uint32_t> fcs = host_frame_counts(&b, ctx->hd.k);
+	if (!fcs.empty() && fcs.back() >= ctx->minc_rows)
+		return mibf_fail(ctx, BBT_ERR_ARG, "a read is longer than the minCount rows reserved "
+				"for serving");
+	return ensure_min_count(ctx, fcs, ctx->stream);
+}
+
 static std::vector<uint32_t> host_frame_counts(const bbt_batch *b, unsigned k)
 {
 	std::vector<uint32_t> fcs;
@@ -942,13 +981,13 @@ static int device_frame_counts(bbt_mibf *ctx, const bbt_batch *b, cudaStream_t s
 	return BBT_OK;
 }
 
-static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, const uint64_t *off,
+static int run_query_sc(bbt_mibf *ctx, uint64_t n_reads, const uint8_t *seq, const uint64_t *off,
 		const uint8_t *seq2, const uint64_t *off2, bbt_mibf_hit *hits, uint32_t max_hits,
-		uint32_t *n_hits, uint32_t *sat, cudaStream_t s)
+		uint32_t *n_hits, uint32_t *sat, cudaStream_t s, const MibfScratch &sc, bool timed)
 {
 	const unsigned nids = (unsigned)ctx->names.size();
 	const size_t nc = counts_len(ctx);
-	unsigned long long *batch_counts = ctx->d_counts + nc + 1;
+	unsigned long long *batch_counts = sc.counts;
 	MibfArgs a;
 	a.f.blocks = ctx->d_blocks;
 	a.f.super = ctx->d_super;
@@ -965,7 +1004,7 @@ static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, cons
 	a.off = off;
 	a.seq2 = seq2;
 	a.off2 = off2;
-	a.n_reads = b->n_reads;
+	a.n_reads = n_reads;
 	a.minc = ctx->d_minc;
 	a.need = ctx->need;
 	a.min_nonsat = ctx->p.min_nonsat;
@@ -978,26 +1017,73 @@ static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, cons
 	a.n_hits = n_hits;
 	a.sat = sat;
 	a.counts = batch_counts;
-	a.work = ctx->d_work;
-	a.flags = ctx->d_flags;
-	a.stat = ctx->d_stat;
+	a.work = sc.work;
+	a.flags = sc.flags;
+	a.stat = sc.stat;
 	a.T = tally_slots(nids);
 	const int hsel = pick_h(ctx->hd.h);
 	const size_t smem = mibf_smem_bytes(a.f.nse, a.T, 4);
 	const bool dense = ctx->d_dense != nullptr;
 	const int grid = ctx->num_sms * query_occupancy(dense, hsel, smem);
 	MIBF_TRY(ctx, cudaMemsetAsync(batch_counts, 0, nc * 8, s));
-	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, 8, s));
-	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_flags, 0, 4, s));
-	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_stat, 0, 3 * 8, s));
-	MIBF_TRY(ctx, cudaEventRecord(ctx->ev0, s));
-	if (b->n_reads)
+	MIBF_TRY(ctx, cudaMemsetAsync(sc.work, 0, 8, s));
+	MIBF_TRY(ctx, cudaMemsetAsync(sc.flags, 0, 4, s));
+	MIBF_TRY(ctx, cudaMemsetAsync(sc.stat, 0, 3 * 8, s));
+	if (timed)
+		MIBF_TRY(ctx, cudaEventRecord(ctx->ev0, s));
+	if (n_reads)
 		MIBF_TRY(ctx, launch_query(a, dense, hsel, grid, smem, s));
-	MIBF_TRY(ctx, cudaEventRecord(ctx->ev1, s));
-	mibf_commit_kernel<<<1, 256, 0, s>>>(batch_counts, ctx->d_counts, (uint32_t)nc,
-			ctx->d_flags, b->n_reads);
+	if (timed)
+		MIBF_TRY(ctx, cudaEventRecord(ctx->ev1, s));
+	mibf_commit_kernel<<<1, 256, 0, s>>>(batch_counts, ctx->d_counts, (uint32_t)nc, sc.flags,
+			n_reads);
 	MIBF_TRY(ctx, cudaGetLastError());
 	return BBT_OK;
+}
+
+/* The context's own scratch (single-stream entry points). */
+static MibfScratch ctx_scratch(bbt_mibf *ctx)
+{
+	MibfScratch sc;
+	sc.work = ctx->d_work;
+	sc.counts = ctx->d_counts + counts_len(ctx) + 1;
+	sc.stat = ctx->d_stat;
+	sc.flags = ctx->d_flags;
+	return sc;
+}
+
+static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, const uint64_t *off,
+		const uint8_t *seq2, const uint64_t *off2, bbt_mibf_hit *hits, uint32_t max_hits,
+		uint32_t *n_hits, uint32_t *sat, cudaStream_t s)
+{
+	return run_query_sc(ctx, b->n_reads, seq, off, seq2, off2, hits, max_hits, n_hits, sat, s,
+			ctx_scratch(ctx), true);
+}
+
+int bbt::mibf_scratch_init(bbt_mibf *ctx, MibfScratch &sc)
+{
+	MIBF_TRY(ctx, cudaSetDevice(ctx->dev));
+	MIBF_TRY(ctx, cudaMalloc(&sc.work, 8));
+	MIBF_TRY(ctx, cudaMalloc(&sc.counts, counts_len(ctx) * 8));
+	MIBF_TRY(ctx, cudaMalloc(&sc.stat, 3 * 8));
+	MIBF_TRY(ctx, cudaMalloc(&sc.flags, 4));
+	return BBT_OK;
+}
+
+void bbt::mibf_scratch_free(MibfScratch &sc)
+{
+	cudaFree(sc.work);
+	cudaFree(sc.counts);
+	cudaFree(sc.stat);
+	cudaFree(sc.flags);
+	sc = MibfScratch();
+}
+
+int bbt::mibf_classify_slot(bbt_mibf *ctx, uint64_t n, const uint8_t *seq, const uint64_t *off,
+		const uint8_t *seq2, const uint64_t *off2, bbt_mibf_hit *hits, uint32_t max_hits,
+		uint32_t *n_hits, uint32_t *sat, cudaStream_t s, MibfScratch &sc)
+{
+	return run_query_sc(ctx, n, seq, off, seq2, off2, hits, max_hits, n_hits, sat, s, sc, false);
 }
 
 static int grow_staging(bbt_mibf *ctx, uint64_t bases, uint64_t reads, uint32_t max_hits)

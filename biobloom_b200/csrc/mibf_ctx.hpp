@@ -113,6 +113,28 @@ struct bbt_mibf {
 
 namespace bbt {
 int mibf_fail(bbt_mibf *ctx, int code, const std::string &msg);
+
+/* Per-stream scratch for concurrent miBF classification (serving engine). */
+struct MibfScratch {
+	unsigned long long *work = nullptr;
+	unsigned long long *counts = nullptr; /* a batch's summary counters */
+	unsigned long long *stat = nullptr;
+	unsigned int *flags = nullptr;
+};
+int mibf_scratch_init(bbt_mibf *ctx, MibfScratch &sc);
+void mibf_scratch_free(MibfScratch &sc);
+/* Allocate minCount rows for frame counts below `rows` up front, so that later
+ * requests only fill rows and never move the table under running kernels. */
+int mibf_reserve_rows(bbt_mibf *ctx, uint32_t rows);
+/* Make the minCount rows of these reads (host offsets) present on the device
+ * (computed and copied under the context's lock, complete when it returns). */
+int mibf_rows_for(bbt_mibf *ctx, const uint64_t *off, const uint64_t *off2, uint64_t n);
+/* Classify n reads (pairs) on the device on stream s with this scratch; the
+ * batch's summary is committed unless a read overflowed max_hits, which sets
+ * sc.flags[0] (read it after the stream completes). */
+int mibf_classify_slot(bbt_mibf *ctx, uint64_t n, const uint8_t *seq, const uint64_t *off,
+		const uint8_t *seq2, const uint64_t *off2, bbt_mibf_hit *hits, uint32_t max_hits,
+		uint32_t *n_hits, uint32_t *sat, cudaStream_t s, MibfScratch &sc);
 /* load the header, IDs file names, ID array (host) and frame probabilities */
 int mibf_load_host(bbt_mibf *ctx, const char *bf_path, std::vector<uint16_t> *ids_out);
 }

@@ -193,7 +193,7 @@ typedef struct {
 	int warps_per_block;
 	int frames_per_lane;
 	uint64_t long_bases;        /* bbt_set_schedule value */
-	uint64_t reads_per_launch;
+	uint64_t reads_per_launch;  /* 0 = whole batches (no split was faster) */
 	double reads_per_s;         /* on the sample */
 } bbt_tune;
 int bbt_autotune(bbt_ctx *ctx, const bbt_batch *sample, bbt_tune *out);
