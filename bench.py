@@ -34,8 +34,15 @@ With --workload small: one filter from a seeded 5 Mbp uniform reference,
 1M single-end 150 bp reads, 50% from the reference with 1% substitutions
 (the filter, 3.4 MB, is L2-resident).
 
+With --workload serve: the serving engine with the 3.1 Gbp filter and the
+500-target miBF resident.  Requests of 1k to 1M reads (log-uniform), half
+Bloom and half miBF, read lengths 75-300 bp with 10% of 1-10 kb reads and 5%
+substitutions, arrive as a seeded Poisson process at a fixed offered load
+(a fraction of the capacity measured by submitting the same requests all at
+once, the offline batched run); reports p50/p99 request latency and reads/s.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--workload bf|mibf|varlen|small]
+                  [--workload bf|mibf|varlen|small|serve]
 """
 import argparse
 import json
@@ -800,6 +807,154 @@ def run_single_reference(args):
         pg.destroy_process_group()
 
 
+# ---------------------------------------------------------------- serving workload
+
+SERVE_METRIC = "p50/p99 request latency and reads/s at fixed offered load, 1 B200"
+
+
+def serve_pool(refs, frac, n, seed):
+    from biobloom_b200 import synth
+    p = synth.read_params(75, 300, long_frac=0.10, long_min=1000, long_max=10_000,
+                          sub_rate=0.05)
+    s1, off, _, _ = synth.reads(seed, refs, frac, n, p)
+    return s1, off
+
+
+def run_serve(args):
+    import threading
+
+    import torch
+
+    from biobloom_b200 import BioBloomClassifier
+    from biobloom_b200.mibf import MIBFClassifier
+    from biobloom_b200.server import Server
+
+    world, rank, local, pg = dist_setup(args)
+    torch.cuda.set_device(local)
+    cfg = SINGLE["varlen"]
+    from biobloom_b200 import synth
+    t0 = time.time()
+    d = os.path.join(tempfile.gettempdir(), f"bbt_bench_{cfg['seed']}")
+    os.makedirs(d, exist_ok=True)
+    g = synth.genome(cfg["seed"], cfg["glen"], gc=cfg["gc"], repeat_frac=cfg["repeat_frac"],
+                     rep_min=cfg["rep_min"], rep_max=cfg["rep_max"], div_min=cfg["div_min"],
+                     div_max=cfg["div_max"])
+    bf_path = os.path.join(d, "genome.bf")
+    if not (os.path.exists(bf_path) and os.path.exists(bf_path[:-2] + "txt")):
+        synth.make_filter([g], bf_path[:-3], "genome", k=K, fpr=FPR, device=local,
+                          sources="genome.fa")
+    md = os.path.join(tempfile.gettempdir(), f"bbt_bench_mibf_{args.targets}")
+    os.makedirs(md, exist_ok=True)
+    mi_path, targets, _ = mi_build(md, args.targets, local)
+    pool_n = 2_000_000
+    bs, boff = serve_pool([g], [0.8], pool_n, 5151 + rank)
+    ms, moff = serve_pool(targets, [0.9 / len(targets)] * len(targets), pool_n, 5252 + rank)
+    del g, targets
+    pools = {}
+    for kind, (sq, of) in (("bloom", (bs, boff)), ("mibf", (ms, moff))):
+        pools[kind] = (torch.from_numpy(sq[:int(of[-1])]).pin_memory(),
+                       torch.from_numpy(of.view(np.int64)).pin_memory())
+    log(f"serving setup: {time.time() - t0:.1f} s")
+    bbc = BioBloomClassifier([bf_path], SCORE, streak_threshold=STREAK, device=local)
+    bbc.set_launch(path=2, warps_per_block=8, frames_per_lane=8)
+    bbc.set_schedule(1024)
+    mc = MIBFClassifier(mi_path, device=local)
+    rng = np.random.default_rng(555 + rank)
+    n_req = args.requests
+    sizes = np.exp(rng.uniform(np.log(1e3), np.log(1e6), n_req)).astype(np.int64)
+    kinds = ["bloom" if k else "mibf" for k in rng.integers(0, 2, n_req)]
+    starts = [int(rng.integers(0, pool_n - n)) for n in sizes]
+
+    def prepare(srv):
+        reqs = []
+        for kind, n, st in zip(kinds, sizes, starts):
+            sq, of = pools[kind]
+            o = of[st:st + n + 1]
+            if kind == "bloom":
+                reqs.append(srv.submit_bloom(sq, o, submit=False))
+            else:
+                reqs.append(srv.submit_mibf(sq, o, max_hits=4, submit=False))
+        return reqs
+
+    total_reads = int(sizes.sum())
+    total_bases = 0
+    for kind, n, st in zip(kinds, sizes, starts):
+        of = pools[kind][1]
+        total_bases += int(of[st + n] - of[st])
+    with Server(bbc, mc, slots=args.slots) as srv:
+        reqs = prepare(srv)
+        # warm-up and offline capacity: everything submitted at once
+        offline = []
+        for rep in range(2):
+            t_start = time.perf_counter()
+            for q in reqs:
+                srv.submit_prepared(q)
+            st = [srv.wait(q) for q in reqs]
+            wall = time.perf_counter() - t_start
+            offline.append(wall)
+        off_s = min(offline)
+        capacity = total_reads / off_s
+        # online: Poisson arrivals at load x the offline request rate
+        lam = args.load * n_req / off_s
+        gaps = np.random.default_rng(777).exponential(1.0 / lam, n_req)
+        arrivals = np.cumsum(gaps)
+        clocks = ClockSampler(local)
+        clocks.start()
+        t_start = time.perf_counter()
+
+        def submitter():
+            for q, a in zip(reqs, arrivals):
+                delay = t_start + a - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                srv.submit_prepared(q)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        stats = [srv.wait(q) for q in reqs]
+        wall = time.perf_counter() - t_start
+        clk = clocks.stop()
+    lat = np.array([s["t_done"] - s["t_submit"] for s in stats])
+    queue = np.array([s["t_admit"] - s["t_submit"] for s in stats])
+    span = max(s["t_done"] for s in stats) - min(s["t_submit"] for s in stats)
+    small = lat[sizes < 10_000]
+    line = {
+        "metric": SERVE_METRIC, "value": total_reads / span, "unit": "reads/s",
+        "n_gpus": world, "steps": 1, "warmup": 2, "ms_per_step": span * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic",
+        "config": {"workload": ("serving: 3.1 Gbp filter + 500-target miBF resident; "
+                                f"{n_req} requests of 1k-1M reads (log-uniform), half Bloom "
+                                "half miBF, 75-300 bp with 10% 1-10 kb reads, 5% "
+                                "substitutions, Poisson arrivals"),
+                   "requests": n_req, "reads": total_reads, "bases": total_bases,
+                   "offered_load": args.load, "slots": args.slots,
+                   "arrival_rate_per_s": lam},
+        "latency_ms": {"p50": float(np.percentile(lat, 50) * 1e3),
+                       "p99": float(np.percentile(lat, 99) * 1e3),
+                       "max": float(lat.max() * 1e3),
+                       "p50_small_requests": (float(np.percentile(small, 50) * 1e3)
+                                              if len(small) else None),
+                       "queue_p50": float(np.percentile(queue, 50) * 1e3),
+                       "queue_p99": float(np.percentile(queue, 99) * 1e3)},
+        "offline": {"value": capacity, "unit": "reads/s", "seconds": off_s,
+                    "note": "the same requests submitted all at once"},
+        "e2e": {"value": total_reads / span, "unit": "reads/s",
+                "h2d_bytes_per_step": int(total_bases + 8 * (total_reads + n_req)),
+                "d2h_bytes_per_step": int(sum(n * (12 if k == "bloom" else 4 * 28 + 8)
+                                              for k, n in zip(kinds, sizes)))},
+        "cpu_baseline": {"value": None, "unavailable": "serving has no reference counterpart"},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+    bbc.close()
+    mc.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
 # ---------------------------------------------------------------- miBF workload
 
 MI_TARGET_LEN = 2_000_000
@@ -1132,7 +1287,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity (bytes)")
-    ap.add_argument("--workload", default="bf", choices=["bf", "mibf", "varlen", "small"])
+    ap.add_argument("--workload", default="bf",
+                    choices=["bf", "mibf", "varlen", "small", "serve"])
+    ap.add_argument("--requests", type=int, default=200, help="requests (--workload serve)")
+    ap.add_argument("--load", type=float, default=0.7,
+                    help="offered load, fraction of offline capacity (--workload serve)")
+    ap.add_argument("--slots", type=int, default=4, help="server slots (--workload serve)")
     ap.add_argument("--targets", type=int, default=500, help="miBF targets (--workload mibf)")
     ap.add_argument("--reads", type=int, default=None,
                     help="reads (--workload mibf / varlen / small; default: the workload's)")
@@ -1143,7 +1303,13 @@ def main():
         args.reads = 20_000_000
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")
-    if args.workload == "mibf":
+    if args.workload == "serve":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "the serving engine has no counterpart in the reference"}))
+        else:
+            run_serve(args)
+    elif args.workload == "mibf":
         (run_mibf_reference if args.impl == "reference" else run_mibf)(args)
     elif args.workload in SINGLE:
         (run_single_reference if args.impl == "reference" else run_single)(args)

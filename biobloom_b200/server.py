@@ -69,7 +69,6 @@ class Server:
             msg = L.lib().bbt_server_last_error(self._srv)
             raise L.BBTError(rc, msg.decode() if msg else "")
         req.ticket = t.value
-        req._keep.append(r)
         return req
 
     def _reads(self, req, r, seq, off, seq2, off2):
@@ -90,9 +89,13 @@ class Server:
         r.n_reads = n
         return n
 
-    def submit_bloom(self, seq, off=None, seq2=None, off2=None):
+    def submit_prepared(self, req):
+        """Queue a request made with submit=False (its buffers already exist)."""
+        return self._submit(req, req._req)
+
+    def submit_bloom(self, seq, off=None, seq2=None, off2=None, submit=True):
         """Queue a Bloom-filter request (reads as a list of bytes, or
-        (uint8 array, uint64 offsets))."""
+        (uint8 array, uint64 offsets)); submit=False only prepares it."""
         r = L.Request()
         r.kind = L.REQ_BLOOM
         req = ServedRequest(L.REQ_BLOOM, 0)
@@ -106,9 +109,10 @@ class Server:
             k2, req.hits2 = _pinned((max(n, 1), self.words), np.uint64)
             req._keep.append(k2)
             r.hits2 = req.hits2.ctypes.data
-        return self._submit(req, r)
+        req._req = r
+        return self._submit(req, r) if submit else req
 
-    def submit_mibf(self, seq, off=None, seq2=None, off2=None, max_hits=4):
+    def submit_mibf(self, seq, off=None, seq2=None, off2=None, max_hits=4, submit=True):
         """Queue a miBF request; results are (id, nonSatFrameCount, solidCount,
         count, nonSatCount, totalNonSatCount, totalCount) rows."""
         r = L.Request()
@@ -123,7 +127,8 @@ class Server:
         req._keep += [kh, hv, kn, ks]
         r.mi_hits, r.mi_max_hits = hv.ctypes.data, int(max_hits)
         r.mi_n_hits, r.mi_sat = req.n_hits.ctypes.data, req.sat.ctypes.data
-        return self._submit(req, r)
+        req._req = r
+        return self._submit(req, r) if submit else req
 
     def wait(self, req, timeout=-1.0):
         """Wait for a request; returns its stats (raises on a failed request)."""
