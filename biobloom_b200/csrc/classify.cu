@@ -81,16 +81,22 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 				if (COUNT)
 					frame_acc += (lane == 0) ? (unsigned long long)wn : 0ull;
 			}
-			for (int c = 0; c < wn; c += 32) {
+			for (int c = 0; c < wn;) {
+				/* frames [c, c + nfc) of the window this step */
+				const int nfc = min(length_mode ? 32 : simple_step_frames(st), wn - c);
 				const int q = c + lane;
 				const int32_t p = (int32_t)w0 + q;
-				const uint32_t V = win.vmask[c >> 5];
+				const int vi = c >> 5, vs = c & 31;
+				uint32_t V = win.vmask[vi] >> vs;
+				if (vs && vi + 1 < SEG)
+					V |= win.vmask[vi + 1] << (32 - vs);
+				if (nfc < 32)
+					V &= (1u << nfc) - 1u;
 				const bool v = (V >> lane) & 1u;
 				const bool probe = v && (length_mode || p >= st.skip_until);
 				const unsigned r0 = reads;
 				const bool hit = probe && contains(F, win.h0[q], reads);
 				const uint32_t H = __ballot_sync(kFull, hit);
-				const int nfc = min(32, wn - c);
 				uint32_t alg = 0;
 				decided = length_mode
 						? length_chunk(ls, V, H, (int64_t)w0 + c, nfc, COUNT ? &alg : nullptr)
@@ -100,6 +106,7 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 					alg_acc += reads - r0;
 				if (decided)
 					break;
+				c += nfc;
 			}
 		}
 		if (decided == EVAL_ACCEPT && lane == (int)(f >> 6))

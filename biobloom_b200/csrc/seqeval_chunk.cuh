@@ -187,6 +187,24 @@ BBT_HD void simple_init(SimpleState &s, double threshold, double one_minus,
 }
 
 /*
+ * How many frames the next step should probe (1..32): no fewer than the
+ * valid frames that could still accept the read if all of them hit (the
+ * score grows by 1 for a hit that starts a streak, else by 2, in score2
+ * units), at least 8 so that a step keeps several probes in flight per warp.
+ * A step of that size wastes no probes on a read that accepts in it; the
+ * frames after an early decision are the only probes the state machine does
+ * not need.  The decision itself does not depend on the step sizes.
+ */
+BBT_HD int simple_step_frames(const SimpleState &s)
+{
+	const int32_t gap = s.thres2 - s.score2;
+	if (gap <= 0)
+		return 32;
+	const int32_t need = s.streak > 0 ? (gap + 1) / 2 : 1 + gap / 2;
+	return need < 8 ? 8 : (need > 32 ? 32 : (int)need);
+}
+
+/*
  * Advance over one chunk of 32 frames starting at frame `base`.
  *   V:  valid frames (bit j = frame base+j), already limited to the read
  *   H:  hits among V (only bits the caller probed matter; see below)

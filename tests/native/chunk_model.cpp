@@ -34,8 +34,10 @@ extern "C" int model_eval(const char *seq, uint64_t len, const oracle_bf *bf,
 		bbt::length_init(ls, (unsigned)(threshold + 0.5), len, (int)k);
 	else
 		bbt::simple_init(ss, threshold, 1.0 - threshold, frames);
-	for (uint64_t base = 0; base < frames; base += 32) {
-		int nf = frames - base >= 32 ? 32 : (int)(frames - base);
+	for (uint64_t base = 0; base < frames;) {
+		/* step sizes as the kernel takes them (classify.cu) */
+		const int step = scoring == ORACLE_LENGTH ? 32 : bbt::simple_step_frames(ss);
+		int nf = frames - base >= (uint64_t)step ? step : (int)(frames - base);
 		uint32_t V = 0, H = 0;
 		for (int j = 0; j < nf; ++j) {
 			uint64_t p = base + j;
@@ -55,6 +57,7 @@ extern "C" int model_eval(const char *seq, uint64_t len, const oracle_bf *bf,
 				*alg_probes += cost[base + j];
 		if (d)
 			return d == bbt::EVAL_ACCEPT;
+		base += nf;
 	}
 	return 0;
 }
