@@ -187,18 +187,20 @@ BBT_HD void simple_init(SimpleState &s, double threshold, double one_minus,
 }
 
 /*
- * How many frames the next step should probe (1..32): no fewer than the
- * valid frames that could still accept the read if all of them hit (the
- * score grows by 1 for a hit that starts a streak, else by 2, in score2
- * units), at least 8 so that a step keeps several probes in flight per warp.
- * A step of that size wastes no probes on a read that accepts in it; the
- * frames after an early decision are the only probes the state machine does
- * not need.  The decision itself does not depend on the step sizes.
+ * How many frames the next step should probe (8..32).  At the start of a read
+ * and while it is on a run of hits, the step is the number of valid frames
+ * that could still accept it if all of them hit (a hit that starts a streak
+ * adds 1 to score2, any other hit 2), so a read that accepts wastes no probes
+ * on frames after its decision; otherwise (a read that is missing, which
+ * rarely accepts) the full 32 frames, which keeps the number of dependent
+ * steps, and so the latency of a read, as low as before.  At least 8 frames
+ * keep several probes in flight per warp.  The decision itself does not
+ * depend on the step sizes.
  */
 BBT_HD int simple_step_frames(const SimpleState &s)
 {
 	const int32_t gap = s.thres2 - s.score2;
-	if (gap <= 0)
+	if (gap <= 0 || (s.started && s.streak == 0))
 		return 32;
 	const int32_t need = s.streak > 0 ? (gap + 1) / 2 : 1 + gap / 2;
 	return need < 8 ? 8 : (need > 32 ? 32 : (int)need);
