@@ -83,7 +83,8 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 			}
 			for (int c = 0; c < wn;) {
 				/* frames [c, c + nfc) of the window this step */
-				const int nfc = min(length_mode ? 32 : simple_step_frames(st), wn - c);
+				const int nfc = min((length_mode || !a.tight_steps) ? 32 : simple_step_frames(st),
+						wn - c);
 				const int q = c + lane;
 				const int32_t p = (int32_t)w0 + q;
 				const int vi = c >> 5, vs = c & 31;
@@ -307,8 +308,14 @@ size_t classify_smem_bytes(const LaunchConfig &lc, uint32_t kmax)
 	return per_warp * (size_t)lc.warps_per_block;
 }
 
-cudaError_t launch_classify(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
+cudaError_t launch_classify(const ClassifyArgs &a0, const LaunchConfig &lc, cudaStream_t s)
 {
+	/* The persistent kernel is bound by DRAM traffic: it takes steps sized to
+	 * the read's decision, which probe fewer frames.  The plain kernel is
+	 * bound by the latency of each warp's chain of steps: it keeps 32-frame
+	 * steps, which take fewer of them. */
+	ClassifyArgs a = a0;
+	a.tight_steps = lc.path != BBT_PATH_PLAIN;
 	return lc.seg == 8 ? launch_seg<8>(a, lc, s) : launch_seg<4>(a, lc, s);
 }
 

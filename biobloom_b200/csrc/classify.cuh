@@ -33,6 +33,9 @@ struct ClassifyArgs {
 	unsigned long long *work;  /* persistent: next read to take (zeroed) */
 	const uint64_t *order;     /* persistent: optional order of the reads (a permutation
 	                              of [0, n * mates)); NULL = index order */
+	int tight_steps;           /* SIMPLE scoring: size probe steps by the frames that could
+	                              still accept the read (seqeval_chunk.cuh,
+	                              simple_step_frames) instead of 32 frames per step */
 	unsigned long long *probes;/* optional: filter words read */
 	unsigned long long *frames;/* optional: frames hashed */
 	unsigned long long *alg_probes; /* optional: words the sequential algorithm reads */

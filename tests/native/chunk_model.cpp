@@ -10,8 +10,25 @@
 #include "bbt_oracle.h"
 #include <vector>
 
+static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
+		double threshold, unsigned streak_thr, int scoring, uint64_t *alg_probes, int tight);
+
 extern "C" int model_eval(const char *seq, uint64_t len, const oracle_bf *bf,
 		double threshold, unsigned streak_thr, int scoring, uint64_t *alg_probes)
+{
+	/* both step policies of the kernel must give the oracle's decision and
+	 * algorithmic probe count */
+	uint64_t a1 = 0, a2 = 0;
+	const int d1 = model_eval_steps(seq, len, bf, threshold, streak_thr, scoring, &a1, 1);
+	const int d2 = model_eval_steps(seq, len, bf, threshold, streak_thr, scoring, &a2, 0);
+	if (d1 != d2 || a1 != a2)
+		return -1;
+	*alg_probes += a1;
+	return d1;
+}
+
+static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
+		double threshold, unsigned streak_thr, int scoring, uint64_t *alg_probes, int tight)
 {
 	const unsigned k = bf->k;
 	if (len < k)
@@ -36,7 +53,7 @@ extern "C" int model_eval(const char *seq, uint64_t len, const oracle_bf *bf,
 		bbt::simple_init(ss, threshold, 1.0 - threshold, frames);
 	for (uint64_t base = 0; base < frames;) {
 		/* step sizes as the kernel takes them (classify.cu) */
-		const int step = scoring == ORACLE_LENGTH ? 32 : bbt::simple_step_frames(ss);
+		const int step = (scoring == ORACLE_LENGTH || !tight) ? 32 : bbt::simple_step_frames(ss);
 		int nf = frames - base >= (uint64_t)step ? step : (int)(frames - base);
 		uint32_t V = 0, H = 0;
 		for (int j = 0; j < nf; ++j) {
