@@ -153,13 +153,159 @@ __device__ __forceinline__ Cand warp_best(Cand c)
 	return c;
 }
 
-template <int H, bool DENSE>
+/* The 2-bit codes (w) and validity of frame q of the staged bases. */
+__device__ __forceinline__ bool frame_word(const uint64_t *cw, const uint32_t *iw, uint32_t q,
+		uint32_t nfr, uint64_t kmask, uint64_t &w)
+{
+	w = 0;
+	if (q >= nfr)
+		return false;
+	const uint32_t idx = q >> 5, sh = q & 31;
+	const uint64_t lo = cw[idx], hi = cw[idx + 1];
+	w = sh ? (lo >> (2 * sh)) | (hi << (64 - 2 * sh)) : lo;
+	const uint64_t inv = ((uint64_t)iw[idx] | ((uint64_t)iw[idx + 1] << 32)) >> sh;
+	return (inv & kmask) == 0;
+}
+
+/* The h values of a frame (seed hashes, or ntHash and its extra hashes). */
+template <int H>
+__device__ __forceinline__ void frame_values(const MibfArgs &a, const ulonglong2 *tab, bool ok,
+		uint64_t w, uint64_t *vals)
+{
+	const uint32_t k = a.f.k, h = a.f.h;
+	if (a.f.kmer_mode) {
+		const uint64_t c = ok ? seed_value(tab, w, k) : 0;
+		vals[0] = c;
+#pragma unroll
+		for (int v = 1; v < H; ++v)
+			vals[v] = extra_hash(c, k, v);
+	} else {
+#pragma unroll
+		for (int v = 0; v < H; ++v)
+			vals[v] = (ok && v < (int)h) ? seed_value(tab + v * 128, w, k) : 0;
+	}
+}
+
+/* Dense layout: one 2-byte read per value; e = ID entry, 0 for a clear bit. */
+template <int H>
+__device__ __forceinline__ void probe_dense(const MibfArgs &a, bool ok, const uint64_t *vals,
+		uint32_t *e)
+{
+#pragma unroll
+	for (int v = 0; v < H; ++v) {
+		e[v] = 0;
+		if (ok && v < (int)a.f.h)
+			e[v] = __ldg(a.f.dense + reduce(vals[v], a.f.m, a.f.minv));
+	}
+}
+
+/* Rank layout: a block read per value, then an ID read per set bit. */
+template <int H>
+__device__ __forceinline__ void probe_rank(const MibfArgs &a, bool ok, const uint64_t *vals,
+		uint32_t *e, bool *hit)
+{
+	uint4 q0v[H], q1v[H];
+	uint32_t rr[H];
+	uint64_t blk[H];
+#pragma unroll
+	for (int v = 0; v < H; ++v) {
+		if (ok && v < (int)a.f.h) {
+			const uint64_t p = reduce(vals[v], a.f.m, a.f.minv);
+			blk[v] = p / kBlockBits;
+			rr[v] = (uint32_t)(p - blk[v] * kBlockBits);
+			q0v[v] = __ldg(a.f.blocks + 2 * blk[v]);
+			q1v[v] = __ldg(a.f.blocks + 2 * blk[v] + 1);
+		}
+	}
+#pragma unroll
+	for (int v = 0; v < H; ++v) {
+		hit[v] = false;
+		e[v] = 0;
+		if (ok && v < (int)a.f.h) {
+			const uint32_t d[7] = {q0v[v].y, q0v[v].z, q0v[v].w, q1v[v].x, q1v[v].y, q1v[v].z,
+					q1v[v].w};
+			const uint32_t ws = rr[v] >> 5, bit = rr[v] & 31u;
+			uint32_t acc = 0, word = 0;
+#pragma unroll
+			for (int i = 0; i < 7; ++i) {
+				if ((uint32_t)i < ws)
+					acc += __popc(d[i]);
+				if ((uint32_t)i == ws)
+					word = d[i];
+			}
+			if ((word >> bit) & 1u) {
+				acc += __popc(word & ((1u << bit) - 1u));
+				const uint64_t rank = a.f.super[blk[v] >> kSuperShift] + q0v[v].x + acc;
+				hit[v] = true;
+				e[v] = __ldg(a.f.ids + rank);
+			}
+		}
+	}
+}
+
+/* A frame's per-ID increments, merged across the warp with __match_any_sync
+ * and added to the warp's tally table. */
+template <int H>
+__device__ __forceinline__ void frame_tally(const MibfArgs &a, bool ok, const uint32_t *e,
+		const bool *hit, unsigned long long *TA, unsigned long long *TB, unsigned long long *TC,
+		uint32_t &satc, LaneCounts &lc, int lane)
+{
+	const uint32_t h = a.f.h, nids = a.f.nids, need = a.need;
+	bool anysat = false;
+#pragma unroll
+	for (int v = 0; v < H; ++v) {
+		anysat |= hit[v] && (e[v] & kMibfSat);
+		lc.hits += hit[v] ? 1u : 0u;
+	}
+	lc.frames += ok ? 1u : 0u;
+	lc.probes += ok ? h : 0u;
+	satc += __popc(__ballot_sync(kFull, anysat));
+#pragma unroll
+	for (int r = 0; r < H; ++r) {
+		uint32_t key = 0xFFFFFFFFu, id = 0, hits = 0, nsh = 0;
+		if (hit[r]) {
+			id = e[r] & 0x7FFFu;
+			bool first = id != 0 && id < nids;
+#pragma unroll
+			for (int u = 0; u < r; ++u)
+				if (hit[u] && (e[u] & 0x7FFFu) == id)
+					first = false;
+			if (first) {
+#pragma unroll
+				for (int u = 0; u < H; ++u)
+					if (hit[u] && (e[u] & 0x7FFFu) == id) {
+						++hits;
+						nsh += (e[u] & kMibfSat) ? 0u : 1u;
+					}
+				key = id | (hits << 16) | (nsh << 21) | ((anysat ? 1u : 0u) << 26);
+			}
+		}
+		const uint32_t grp = __match_any_sync(kFull, key);
+		if (key != 0xFFFFFFFFu && lane == __ffs(grp) - 1) {
+			const unsigned long long n = (unsigned long long)__popc(grp);
+			const uint32_t cnt = hits >= need, ns = nsh >= need, sol = hits == h;
+			const uint32_t nsf = cnt && !anysat;
+			const unsigned long long ia = cnt | ((unsigned long long)ns << 32);
+			const unsigned long long ib = sol | ((unsigned long long)hits << 32);
+			const unsigned long long ic = nsh | ((unsigned long long)nsf << 32);
+			if (ia)
+				atomicAdd(TA + id, n * ia);
+			atomicAdd(TB + id, n * ib);
+			if (ic)
+				atomicAdd(TC + id, n * ic);
+		}
+	}
+}
+
+/* All frames of one mate: bases staged 512 at a time, then steps of 32 * FPL
+ * frames, each lane holding FPL frames (FPL * h reads in flight per lane). */
+template <int H, bool DENSE, int FPL>
 __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglong2 *tab,
 		uint64_t *cw, uint32_t *iw, unsigned long long *TA, unsigned long long *TB,
 		unsigned long long *TC, const uint8_t *__restrict__ s, uint64_t len, uint32_t &satc,
 		LaneCounts &lc, int lane)
 {
-	const uint32_t k = a.f.k, h = a.f.h, nids = a.f.nids, need = a.need;
+	const uint32_t k = a.f.k;
 	const uint64_t kmask = (k >= 64) ? ~0ull : ((1ull << k) - 1);
 	if (len < k)
 		return;
@@ -184,132 +330,40 @@ __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglon
 		__syncwarp();
 		const uint64_t avail = len - c0 < (uint64_t)kStageBases ? len - c0 : kStageBases;
 		const uint32_t nfr = (uint32_t)avail - k + 1;
-		for (uint32_t q0 = 0; q0 < nfr; q0 += 32) {
-			const uint32_t q = q0 + lane;
-			bool ok = false;
-			uint64_t w = 0;
-			if (q < nfr) {
-				const uint32_t idx = q >> 5, sh = q & 31;
-				const uint64_t lo = cw[idx], hi = cw[idx + 1];
-				w = sh ? (lo >> (2 * sh)) | (hi << (64 - 2 * sh)) : lo;
-				const uint64_t inv = ((uint64_t)iw[idx] | ((uint64_t)iw[idx + 1] << 32)) >> sh;
-				ok = (inv & kmask) == 0;
-			}
-			uint64_t vals[H];
-			if (a.f.kmer_mode) {
-				const uint64_t c = ok ? seed_value(tab, w, k) : 0;
-				vals[0] = c;
+		for (uint32_t q0 = 0; q0 < nfr; q0 += 32 * FPL) {
+			bool ok[FPL];
+			uint64_t vals[FPL][H];
+			uint32_t e[FPL][H];
+			bool hit[FPL][H];
 #pragma unroll
-				for (int v = 1; v < H; ++v)
-					vals[v] = extra_hash(c, k, v);
-			} else {
-#pragma unroll
-				for (int v = 0; v < H; ++v)
-					vals[v] = (ok && v < (int)h) ? seed_value(tab + v * 128, w, k) : 0;
+			for (int f = 0; f < FPL; ++f) {
+				uint64_t w;
+				ok[f] = frame_word(cw, iw, q0 + 32 * f + lane, nfr, kmask, w);
+				frame_values<H>(a, tab, ok[f], w, vals[f]);
 			}
-			uint32_t e[H];
-			bool hit[H];
 			if (DENSE) {
-				/* one 2-byte read per value, all h in flight */
 #pragma unroll
-				for (int v = 0; v < H; ++v) {
-					e[v] = 0;
-					if (ok && v < (int)h)
-						e[v] = __ldg(a.f.dense + reduce(vals[v], a.f.m, a.f.minv));
-					hit[v] = e[v] != 0;
-				}
+				for (int f = 0; f < FPL; ++f)
+					probe_dense<H>(a, ok[f], vals[f], e[f]);
+#pragma unroll
+				for (int f = 0; f < FPL; ++f)
+#pragma unroll
+					for (int v = 0; v < H; ++v)
+						hit[f][v] = e[f][v] != 0;
 			} else {
-				/* block reads, all h in flight */
-				uint4 q0v[H], q1v[H];
-				uint32_t rr[H];
-				uint64_t blk[H];
-	#pragma unroll
-				for (int v = 0; v < H; ++v) {
-					if (ok && v < (int)h) {
-						const uint64_t p = reduce(vals[v], a.f.m, a.f.minv);
-						blk[v] = p / kBlockBits;
-						rr[v] = (uint32_t)(p - blk[v] * kBlockBits);
-						q0v[v] = __ldg(a.f.blocks + 2 * blk[v]);
-						q1v[v] = __ldg(a.f.blocks + 2 * blk[v] + 1);
-					}
-				}
-				/* bit, rank, ID reads */
-	#pragma unroll
-				for (int v = 0; v < H; ++v) {
-					hit[v] = false;
-					e[v] = 0;
-					if (ok && v < (int)h) {
-						const uint32_t d[7] = {q0v[v].y, q0v[v].z, q0v[v].w, q1v[v].x, q1v[v].y,
-								q1v[v].z, q1v[v].w};
-						const uint32_t ws = rr[v] >> 5, bit = rr[v] & 31u;
-						uint32_t acc = 0, word = 0;
-	#pragma unroll
-						for (int i = 0; i < 7; ++i) {
-							if ((uint32_t)i < ws)
-								acc += __popc(d[i]);
-							if ((uint32_t)i == ws)
-								word = d[i];
-						}
-						if ((word >> bit) & 1u) {
-							acc += __popc(word & ((1u << bit) - 1u));
-							const uint64_t rank = a.f.super[blk[v] >> kSuperShift] + q0v[v].x + acc;
-							hit[v] = true;
-							e[v] = __ldg(a.f.ids + rank);
-						}
-					}
-				}
+#pragma unroll
+				for (int f = 0; f < FPL; ++f)
+					probe_rank<H>(a, ok[f], vals[f], e[f], hit[f]);
 			}
-			bool anysat = false;
 #pragma unroll
-			for (int v = 0; v < H; ++v) {
-				anysat |= hit[v] && (e[v] & kMibfSat);
-				lc.hits += hit[v] ? 1u : 0u;
-			}
-			lc.frames += ok ? 1u : 0u;
-			lc.probes += ok ? h : 0u;
-			satc += __popc(__ballot_sync(kFull, anysat));
-			/* per-frame, per-ID records, merged across the warp */
-#pragma unroll
-			for (int r = 0; r < H; ++r) {
-				uint32_t key = 0xFFFFFFFFu, id = 0, hits = 0, nsh = 0;
-				if (hit[r]) {
-					id = e[r] & 0x7FFFu;
-					bool first = id != 0 && id < nids;
-#pragma unroll
-					for (int u = 0; u < r; ++u)
-						if (hit[u] && (e[u] & 0x7FFFu) == id)
-							first = false;
-					if (first) {
-#pragma unroll
-						for (int u = 0; u < H; ++u)
-							if (hit[u] && (e[u] & 0x7FFFu) == id) {
-								++hits;
-								nsh += (e[u] & kMibfSat) ? 0u : 1u;
-							}
-						key = id | (hits << 16) | (nsh << 21) | ((anysat ? 1u : 0u) << 26);
-					}
-				}
-				const uint32_t grp = __match_any_sync(kFull, key);
-				if (key != 0xFFFFFFFFu && lane == __ffs(grp) - 1) {
-					const unsigned long long n = (unsigned long long)__popc(grp);
-					const uint32_t cnt = hits >= need, ns = nsh >= need, sol = hits == h;
-					const uint32_t nsf = cnt && !anysat;
-					const unsigned long long ia = cnt | ((unsigned long long)ns << 32);
-					const unsigned long long ib = sol | ((unsigned long long)hits << 32);
-					const unsigned long long ic = nsh | ((unsigned long long)nsf << 32);
-					if (ia)
-						atomicAdd(TA + id, n * ia);
-					atomicAdd(TB + id, n * ib);
-					if (ic)
-						atomicAdd(TC + id, n * ic);
-				}
-			}
+			for (int f = 0; f < FPL; ++f)
+				frame_tally<H>(a, ok[f], e[f], hit[f], TA, TB, TC, satc, lc, lane);
 		}
 	}
 	__syncwarp();
 }
 
-template <int H, bool DENSE>
+template <int H, bool DENSE, int FPL>
 __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
@@ -350,11 +404,11 @@ __global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
 					: (len2 >= k ? (uint32_t)(len2 - k + 1) : 0u);
 			uint32_t satc = 0;
 			if (fc) {
-				mibf_scan_mate<H, DENSE>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1, satc,
-						lc, lane);
+				mibf_scan_mate<H, DENSE, FPL>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1,
+						satc, lc, lane);
 				if (a.seq2)
-					mibf_scan_mate<H, DENSE>(a, tab, cw, iw, TA, TB, TC, a.seq2 + b2, len2,
-							satc, lc, lane);
+					mibf_scan_mate<H, DENSE, FPL>(a, tab, cw, iw, TA, TB, TC, a.seq2 + b2,
+							len2, satc, lc, lane);
 			}
 			/* significant IDs */
 			uint32_t cmask = 0, maxns = 0;
@@ -572,10 +626,17 @@ static int pick_h(unsigned h)
 	return h <= 1 ? 1 : h <= 2 ? 2 : h <= 3 ? 3 : h <= 4 ? 4 : h <= 6 ? 6 : h <= 8 ? 8 : 16;
 }
 
+/* Frames per lane per step: two for the dense layout (its probes are single
+ * reads, so twice the reads in flight fit the registers), one otherwise. */
+template <int H, bool D>
+struct Fpl {
+	static constexpr int value = (D && H <= 4) ? 2 : 1;
+};
+
 template <int H, bool D>
 static cudaError_t launch_h(const MibfArgs &a, int grid, size_t smem, cudaStream_t s)
 {
-	mibf_query_kernel<H, D><<<grid, 128, smem, s>>>(a);
+	mibf_query_kernel<H, D, Fpl<H, D>::value><<<grid, 128, smem, s>>>(a);
 	return cudaGetLastError();
 }
 
@@ -584,10 +645,10 @@ static cudaError_t launch_h(const MibfArgs &a, int grid, size_t smem, cudaStream
 template <int H, bool D>
 static int occupancy_h(size_t smem)
 {
-	cudaFuncSetAttribute(mibf_query_kernel<H, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			(int)smem);
+	auto kern = mibf_query_kernel<H, D, Fpl<H, D>::value>;
+	cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 	int nb = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, mibf_query_kernel<H, D>, 128, smem);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 128, smem);
 	return nb > 0 ? nb : 1;
 }
 
