@@ -92,9 +92,19 @@ __host__ __device__ inline size_t mibf_warp_bytes(uint32_t T)
 	return 17 * 8 + 18 * 4 + (size_t)3 * T * 8; /* codes, invalid words, tally */
 }
 
+/* Seed tables: with BBT_MIBF_PAIR_TABLES (the default) one entry per pair of
+ * positions and pair of base codes (16 x 16 per seed: a value costs 13 table
+ * reads for k = 25), else one per position and base code (32 x 4). */
+#ifndef BBT_MIBF_PAIR_TABLES
+#define BBT_MIBF_PAIR_TABLES 1
+#endif
+constexpr int kTabEntries = BBT_MIBF_PAIR_TABLES ? 256 : 128; /* ulonglong2 per seed */
+constexpr int kQueryThreads = BBT_MIBF_PAIR_TABLES ? 256 : 128;
+constexpr int kQueryMinBlocks = BBT_MIBF_PAIR_TABLES ? 2 : 4;
+
 __host__ inline size_t mibf_smem_bytes(uint32_t nse, uint32_t T, int warps)
 {
-	return (size_t)nse * 32 * 4 * 16 + (size_t)warps * mibf_warp_bytes(T);
+	return (size_t)nse * kTabEntries * 16 + (size_t)warps * mibf_warp_bytes(T);
 }
 
 __device__ __forceinline__ uint64_t spread_bits(uint32_t v)
@@ -108,11 +118,31 @@ __device__ __forceinline__ uint64_t spread_bits(uint32_t v)
 	return x;
 }
 
-/* min(F, R) of one seed over the 2-bit codes w (base j at bits 2j, 2j+1). */
-__device__ __forceinline__ uint64_t seed_value(const ulonglong2 *tab, uint64_t w, uint32_t k)
+/* min(F, R) of one seed over the 2-bit codes w (base j at bits 2j, 2j+1),
+ * from the pair tables: entry p * 16 + (codes of bases 2p, 2p+1). */
+__device__ __forceinline__ uint64_t seed_value_pairs(const ulonglong2 *tab, uint64_t w, uint32_t k)
 {
 	uint64_t F = 0, R = 0;
 #pragma unroll
+	for (int p = 0; p < 16; ++p) {
+		if (2 * p < (int)k) {
+			const ulonglong2 e = tab[p * 16 + (int)((w >> (4 * p)) & 15u)];
+			F ^= e.x;
+			R ^= e.y;
+		}
+	}
+	return F < R ? F : R;
+}
+
+/* min(F, R) of one seed over the 2-bit codes w (base j at bits 2j, 2j+1). */
+#ifndef BBT_MIBF_SEED_UNROLL
+#define BBT_MIBF_SEED_UNROLL 32
+#endif
+constexpr int kSeedUnroll = BBT_MIBF_SEED_UNROLL;
+__device__ __forceinline__ uint64_t seed_value(const ulonglong2 *tab, uint64_t w, uint32_t k)
+{
+	uint64_t F = 0, R = 0;
+#pragma unroll kSeedUnroll
 	for (int j = 0; j < 32; ++j) {
 		if (j < (int)k) {
 			const ulonglong2 e = tab[j * 4 + (int)((w >> (2 * j)) & 3u)];
@@ -174,7 +204,8 @@ __device__ __forceinline__ void frame_values(const MibfArgs &a, const ulonglong2
 {
 	const uint32_t k = a.f.k, h = a.f.h;
 	if (a.f.kmer_mode) {
-		const uint64_t c = ok ? seed_value(tab, w, k) : 0;
+		const uint64_t c = ok ? (BBT_MIBF_PAIR_TABLES ? seed_value_pairs(tab, w, k)
+		                                              : seed_value(tab, w, k)) : 0;
 		vals[0] = c;
 #pragma unroll
 		for (int v = 1; v < H; ++v)
@@ -182,7 +213,10 @@ __device__ __forceinline__ void frame_values(const MibfArgs &a, const ulonglong2
 	} else {
 #pragma unroll
 		for (int v = 0; v < H; ++v)
-			vals[v] = (ok && v < (int)h) ? seed_value(tab + v * 128, w, k) : 0;
+			vals[v] = (ok && v < (int)h)
+					? (BBT_MIBF_PAIR_TABLES ? seed_value_pairs(tab + v * kTabEntries, w, k)
+					                        : seed_value(tab + v * kTabEntries, w, k))
+					: 0;
 	}
 }
 
@@ -364,15 +398,15 @@ __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglon
 }
 
 template <int H, bool DENSE, int FPL>
-__global__ void __launch_bounds__(128, 4) mibf_query_kernel(MibfArgs a)
+__global__ void __launch_bounds__(kQueryThreads, kQueryMinBlocks) mibf_query_kernel(MibfArgs a)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
 	const uint32_t nse = a.f.nse, T = a.T, nids = a.f.nids;
 	unsigned long long *tabw = reinterpret_cast<unsigned long long *>(smem);
-	for (uint32_t i = threadIdx.x; i < nse * 256; i += blockDim.x)
+	for (uint32_t i = threadIdx.x; i < nse * kTabEntries * 2; i += blockDim.x)
 		tabw[i] = a.tables[i];
-	unsigned char *wb = smem + (size_t)nse * 2048 + (size_t)wib * mibf_warp_bytes(T);
+	unsigned char *wb = smem + (size_t)nse * kTabEntries * 16 + (size_t)wib * mibf_warp_bytes(T);
 	uint64_t *cw = reinterpret_cast<uint64_t *>(wb);
 	uint32_t *iw = reinterpret_cast<uint32_t *>(wb + 17 * 8);
 	unsigned long long *TA = reinterpret_cast<unsigned long long *>(wb + 17 * 8 + 18 * 4);
@@ -626,17 +660,21 @@ static int pick_h(unsigned h)
 	return h <= 1 ? 1 : h <= 2 ? 2 : h <= 3 ? 3 : h <= 4 ? 4 : h <= 6 ? 6 : h <= 8 ? 8 : 16;
 }
 
-/* Frames per lane per step: two for the dense layout (its probes are single
- * reads, so twice the reads in flight fit the registers), one otherwise. */
+/* Frames per lane per step (BBT_MIBF_FPL for the dense layout, whose probes
+ * are single reads; one for the rank layout).  Two frames per lane measured
+ * slower than one on the 500-target workload. */
+#ifndef BBT_MIBF_FPL
+#define BBT_MIBF_FPL 1
+#endif
 template <int H, bool D>
 struct Fpl {
-	static constexpr int value = (D && H <= 4) ? 2 : 1;
+	static constexpr int value = (D && H <= 4) ? BBT_MIBF_FPL : 1;
 };
 
 template <int H, bool D>
 static cudaError_t launch_h(const MibfArgs &a, int grid, size_t smem, cudaStream_t s)
 {
-	mibf_query_kernel<H, D, Fpl<H, D>::value><<<grid, 128, smem, s>>>(a);
+	mibf_query_kernel<H, D, Fpl<H, D>::value><<<grid, kQueryThreads, smem, s>>>(a);
 	return cudaGetLastError();
 }
 
@@ -648,7 +686,7 @@ static int occupancy_h(size_t smem)
 	auto kern = mibf_query_kernel<H, D, Fpl<H, D>::value>;
 	cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 	int nb = 0;
-	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 128, smem);
+	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kQueryThreads, smem);
 	return nb > 0 ? nb : 1;
 }
 
@@ -896,6 +934,21 @@ extern "C" int bbt_mibf_open(const char *bf_path, const bbt_mibf_params *params,
 		return bail(rc);
 	std::vector<uint16_t>().swap(ids);
 	std::vector<unsigned long long> tabs = mibf_seed_tables(ctx->hd.seeds, ctx->hd.k);
+	if (BBT_MIBF_PAIR_TABLES) {
+		/* pair entry (p, c0 | c1 << 2) = entry (2p, c0) ^ entry (2p + 1, c1) */
+		const size_t nse = tabs.size() / (32 * 4 * 2);
+		std::vector<unsigned long long> pairs(nse * 16 * 16 * 2, 0ull);
+		for (size_t sd = 0; sd < nse; ++sd)
+			for (int pp = 0; pp < 16; ++pp)
+				for (int c = 0; c < 16; ++c)
+					for (int half = 0; half < 2; ++half) {
+						const unsigned long long *a0 = &tabs[((sd * 32 + 2 * pp) * 4 + (c & 3)) * 2];
+						const unsigned long long *a1 =
+								&tabs[((sd * 32 + 2 * pp + 1) * 4 + (c >> 2)) * 2];
+						pairs[((sd * 16 + pp) * 16 + c) * 2 + half] = a0[half] ^ a1[half];
+					}
+		tabs.swap(pairs);
+	}
 	const size_t nc = counts_len(ctx) + 1; /* + reads */
 	if (cudaMalloc(&ctx->d_tables, tabs.size() * 8) != cudaSuccess ||
 			cudaMalloc(&ctx->d_counts, 2 * nc * 8) != cudaSuccess ||
@@ -1083,7 +1136,7 @@ static int run_query_sc(bbt_mibf *ctx, uint64_t n_reads, const uint8_t *seq, con
 	a.stat = sc.stat;
 	a.T = tally_slots(nids);
 	const int hsel = pick_h(ctx->hd.h);
-	const size_t smem = mibf_smem_bytes(a.f.nse, a.T, 4);
+	const size_t smem = mibf_smem_bytes(a.f.nse, a.T, kQueryThreads / 32);
 	const bool dense = ctx->d_dense != nullptr;
 	const int grid = ctx->num_sms * query_occupancy(dense, hsel, smem);
 	MIBF_TRY(ctx, cudaMemsetAsync(batch_counts, 0, nc * 8, s));
