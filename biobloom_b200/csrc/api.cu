@@ -1131,3 +1131,12 @@ int bbt::bf_classify_slot(bbt_ctx *ctx, const uint8_t *seq, const uint64_t *off,
 			ctx->words, ctx->p.inclusive, category, ctx->d_counts, ctx->num_sms, s));
 	return BBT_OK;
 }
+
+extern "C" int bbt_set_stdout(bbt_ctx *ctx, int on, int inverse)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	ctx->to_stdout = on != 0;
+	ctx->inverse = inverse != 0;
+	return BBT_OK;
+}

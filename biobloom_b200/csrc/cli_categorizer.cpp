@@ -6,9 +6,11 @@
  * :416-441), the filter existence check (:444-452) and the mode dispatch
  * (:458-532) follow it.  Output: "<prefix>_summary.tsv" and, with
  * --read_status FILE, one "<read>\t<category>" line per read (pair).
- * Options whose outputs this build does not produce yet (--fa/--fq, -d, -n,
- * -b, -w, -c, -S, -D, -l, single-file paired input) are refused with a message
- * instead of being ignored.
+ * --fa / --fq (with -g) write the reads of each category to their own files,
+ * -d / -n print the first filter's reads (or all others) to stdout.  Options
+ * whose outputs this build does not produce yet (-b, -w, -c, -S, -D, -l,
+ * single-file paired input) are refused with a message instead of being
+ * ignored.
  */
 #include <getopt.h>
 #include <sys/stat.h>
@@ -42,6 +44,12 @@ static void usage_exit(int code)
 	        "                         between 0 and 1, or a positive integer minimum match\n"
 	        "                         length in bases. [0.15]\n"
 	        "  -t, --threads=N        Accepted for compatibility (work runs on the GPU).\n"
+	        "  -g, --gz_output        Outputs all output files in compressed gzip.\n"
+	        "      --fa               Output categorized reads in Fasta files.\n"
+	        "      --fq               Output categorized reads in Fastq files.\n"
+	        "  -d, --stdout_filter    Outputs all matching reads to stdout for the first\n"
+	        "                         filter listed by -f.\n"
+	        "  -n, --inverse          Inverts the output of -d (everything but first filter).\n"
 	        "  -r, --streak=N         Hits tiling in second pass needed to jump several tiles\n"
 	        "                         upon a miss. [3]\n"
 	        "  -I, --interval         Accepted for compatibility.\n"
@@ -72,8 +80,8 @@ int main(int argc, char **argv)
 {
 	bbt_params p;
 	bbt_default_params(&p);
-	string filters, prefix, read_status;
-	bool paired = false, die = false;
+	string filters, prefix, read_status, postfix;
+	bool paired = false, die = false, to_stdout = false, inverse = false;
 	int fastq = 0, fasta = 0, verbose = 0;
 	int device = 0;
 	string unsupported;
@@ -134,7 +142,10 @@ int main(int argc, char **argv)
 		case 'v':
 			cerr << "biobloomcategorizer (bbt-b200) 2.3.4-compatible\n" << endl;
 			exit(EXIT_SUCCESS);
-		case 'g': case 'l': case 'c': case 'd': case 'n': case 'b': case 'w': case 'S':
+		case 'g': postfix = ".gz"; break;
+		case 'd': to_stdout = true; break;
+		case 'n': inverse = true; break;
+		case 'l': case 'c': case 'b': case 'w': case 'S':
 		case 'D': case 'T': case 'W': case 'o':
 			unsupported += string(" -") + (char)c;
 			break;
@@ -144,8 +155,15 @@ int main(int argc, char **argv)
 		default: break;
 		}
 	}
-	if (fasta || fastq)
-		unsupported += fasta ? " --fa" : " --fq";
+	string out_type;
+	if (fasta && fastq) {
+		cerr << "Error: fasta (--fa) and fastq (--fq) outputs types cannot be both set" << endl;
+		exit(1);
+	} else if (fastq) {
+		out_type = "fq";
+	} else if (fasta) {
+		out_type = "fa";
+	}
 	vector<string> files;
 	while (optind < argc)
 		files.push_back(argv[optind++]);
@@ -218,13 +236,21 @@ int main(int argc, char **argv)
 	cerr << "Filter Loading Complete." << endl;
 	int rc;
 	const char *rs = read_status.empty() ? nullptr : read_status.c_str();
+	if (to_stdout)
+		bbt_set_stdout(ctx, 1, inverse ? 1 : 0);
 	if (paired) {
-		rc = bbt_filter_pair_files(ctx, files[0].c_str(), files[1].c_str(), prefix.c_str(), rs);
+		rc = out_type.empty()
+				? bbt_filter_pair_files(ctx, files[0].c_str(), files[1].c_str(), prefix.c_str(), rs)
+				: bbt_filter_pair_files_print(ctx, files[0].c_str(), files[1].c_str(),
+						prefix.c_str(), out_type.c_str(), postfix.c_str(), rs);
 	} else {
 		vector<const char *> fp;
 		for (const string &f : files)
 			fp.push_back(f.c_str());
-		rc = bbt_filter_files(ctx, fp.data(), (int)fp.size(), prefix.c_str(), rs);
+		rc = out_type.empty()
+				? bbt_filter_files(ctx, fp.data(), (int)fp.size(), prefix.c_str(), rs)
+				: bbt_filter_files_print(ctx, fp.data(), (int)fp.size(), prefix.c_str(),
+						out_type.c_str(), postfix.c_str(), rs);
 	}
 	if (rc != BBT_OK) {
 		cerr << "Error: " << bbt_last_error(ctx) << endl;

@@ -62,6 +62,8 @@ struct bbt_ctx {
 	uint32_t *d_tp_vmask = nullptr;
 	uint64_t tp_frames_cap = 0;
 	bool same_k = true;
+	/* -d / -n: print reads of the first filter (or all others) to stdout */
+	bool to_stdout = false, inverse = false;
 	/* long-first read order of the persistent kernel (0 = index order) */
 	uint64_t long_bases = 0;
 	uint64_t *d_order = nullptr;

@@ -136,12 +136,14 @@ long FastxReader::read(std::string &name, std::string &comment, std::vector<char
 	return slen;
 }
 
-/* One host batch: concatenated bases (pinned), offsets, read names. */
+/* One host batch: concatenated bases (pinned), offsets, read names (and,
+ * when records are printed, names, comments and qualities of both mates). */
 struct HostBatch {
 	char *seq[2] = {nullptr, nullptr};
 	size_t cap = 0;
 	std::vector<uint64_t> off[2];
 	std::vector<std::string> names;
+	std::vector<std::string> rname[2], rcomment[2], rqual[2];
 	std::vector<uint32_t> cat;
 	uint64_t n = 0;
 	bool last = false;
@@ -159,12 +161,17 @@ struct Pipe {
 
 /* Fill b from the reader(s); returns false at end of input. */
 bool fill_batch(HostBatch &b, FastxReader *r1, FastxReader *r2, uint64_t max_reads,
-		uint64_t max_bases, bool keep_names, std::vector<char> &s1, std::vector<char> &s2,
-		std::string &perr)
+		uint64_t max_bases, bool keep_names, bool keep_records, std::vector<char> &s1,
+		std::vector<char> &s2, std::string &perr)
 {
 	std::string name, comment, qual, name2, comment2, qual2;
 	b.n = 0;
 	b.names.clear();
+	for (int m = 0; m < 2; ++m) {
+		b.rname[m].clear();
+		b.rcomment[m].clear();
+		b.rqual[m].clear();
+	}
 	s1.clear();
 	s2.clear();
 	b.off[0].assign(1, 0);
@@ -189,15 +196,103 @@ bool fill_batch(HostBatch &b, FastxReader *r1, FastxReader *r2, uint64_t max_rea
 			b.off[1].push_back(s2.size());
 		if (keep_names)
 			b.names.push_back(name);
+		if (keep_records) {
+			b.rname[0].push_back(name);
+			b.rcomment[0].push_back(comment);
+			b.rqual[0].push_back(qual);
+			if (r2) {
+				b.rname[1].push_back(name2);
+				b.rcomment[1].push_back(comment2);
+				b.rqual[1].push_back(qual2);
+			}
+		}
 		++b.n;
 	}
 	return more;
 }
 
+/* A categorized-read output file: plain or gzip (".gz" postfix), as
+ * Dynamicofstream chooses by the name (Common/Dynamicofstream.cpp:14-24). */
+struct OutFile {
+	FILE *f = nullptr;
+	gzFile g = nullptr;
+	bool open(const std::string &path)
+	{
+		if (path.size() >= 3 && path.compare(path.size() - 3, 3, ".gz") == 0)
+			g = gzopen(path.c_str(), "wb");
+		else
+			f = fopen(path.c_str(), "wb");
+		return f || g;
+	}
+	bool write(const std::string &t)
+	{
+		if (t.empty())
+			return true;
+		if (g)
+			return gzwrite(g, t.data(), (unsigned)t.size()) == (int)t.size();
+		return fwrite(t.data(), 1, t.size(), f) == t.size();
+	}
+	bool close()
+	{
+		bool ok = true;
+		if (g)
+			ok = gzclose(g) == Z_OK;
+		if (f)
+			ok = fclose(f) == 0;
+		f = nullptr;
+		g = nullptr;
+		return ok;
+	}
+};
+
+/* ">name comment\nseq\n" or "@name comment\nseq\n+\nqual\n", with the space
+ * written even for an empty comment (BioBloomClassifier.h:144-209). */
+void append_record(std::string &out, bool fastq, const std::string &name,
+		const std::string &comment, const char *seq, size_t len, const std::string &qual)
+{
+	out += fastq ? '@' : '>';
+	out += name;
+	out += ' ';
+	out += comment;
+	out += '\n';
+	out.append(seq, len);
+	if (fastq) {
+		out += "\n+\n";
+		out += qual;
+	}
+	out += '\n';
+}
+
 int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std::string *file2,
-		const char *prefix, const char *read_status)
+		const char *prefix, const char *read_status, const char *out_type = nullptr,
+		const char *postfix = nullptr)
 {
 	const bool paired = file2 != nullptr;
+	const bool print = out_type && out_type[0];
+	const bool fastq_out = print && std::string(out_type) == "fq";
+	const bool keep_records = print || ctx->to_stdout;
+	/* output files: one per filter, then noMatch, then multiMatch
+	 * (BioBloomClassifier.cpp:116-127, 319-337) */
+	std::vector<OutFile> outs[2];
+	if (print) {
+		const std::string pre = prefix ? prefix : "", post = postfix ? postfix : "";
+		std::vector<std::string> labels(ctx->ids);
+		labels.push_back("noMatch");
+		labels.push_back("multiMatch");
+		for (int m = 0; m < (paired ? 2 : 1); ++m) {
+			outs[m].resize(labels.size());
+			for (size_t i = 0; i < labels.size(); ++i) {
+				const std::string path = pre + "_" + labels[i] +
+						(paired ? (m ? "_2." : "_1.") : ".") + out_type + post;
+				if (!outs[m][i].open(path)) {
+					for (int mm = 0; mm < 2; ++mm)
+						for (OutFile &o : outs[mm])
+							o.close();
+					return fail(ctx, BBT_ERR_IO, "cannot write " + path);
+				}
+			}
+		}
+	}
 	const uint64_t max_reads = std::min<uint64_t>(ctx->cap_reads, 1ull << 18);
 	const uint64_t max_bases = std::min<uint64_t>(ctx->cap_bases, 64ull << 20);
 	std::ofstream status;
@@ -266,7 +361,7 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 			if (have) {
 				std::string perr;
 				bool more = fill_batch(b, r1, r2, max_reads, max_bases, read_status != nullptr,
-						stage1[which], stage2[which], perr);
+						keep_records, stage1[which], stage2[which], perr);
 				if (!perr.empty())
 					std::cerr << "warning: " << perr << "; reading of this file stopped there"
 					          << std::endl;
@@ -329,11 +424,42 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 			bbt_result res;
 			res.hits = nullptr;
 			res.hits2 = nullptr;
-			res.category = read_status ? b.cat.data() : nullptr;
+			res.category = (read_status || keep_records) ? b.cat.data() : nullptr;
 			res.location = BBT_HOST;
 			rc = bbt_classify_batch(ctx, &bt, &res, nullptr);
 			if (rc)
 				break;
+			if (keep_records) {
+				/* categorized files, and stdout for the first filter's reads (-d)
+				 * or everything else (-n), BioBloomClassifier.h:115-142, 211-247 */
+				std::vector<std::string> text[2];
+				if (print) {
+					text[0].resize(ctx->nf + 2);
+					text[1].resize(ctx->nf + 2);
+				}
+				std::string so;
+				for (uint64_t i = 0; i < b.n; ++i) {
+					const uint32_t c = b.cat[i];
+					for (int m = 0; m < (paired ? 2 : 1); ++m) {
+						const uint64_t o = b.off[m][i], e = b.off[m][i + 1];
+						const char *sq = b.seq[m] + o;
+						if (print)
+							append_record(text[m][c], fastq_out, b.rname[m][i], b.rcomment[m][i],
+									sq, e - o, b.rqual[m][i]);
+						if (ctx->to_stdout && (ctx->inverse ? c != 0 : c == 0))
+							append_record(so, true, b.rname[m][i], b.rcomment[m][i], sq, e - o,
+									b.rqual[m][i]);
+					}
+				}
+				for (int m = 0; m < (paired ? 2 : 1) && print; ++m)
+					for (size_t c = 0; c < text[m].size(); ++c)
+						if (!outs[m][c].write(text[m][c]))
+							rc = fail(ctx, BBT_ERR_IO, "cannot write a categorized read file");
+				if (!so.empty() && fwrite(so.data(), 1, so.size(), stdout) != so.size())
+					rc = fail(ctx, BBT_ERR_IO, "cannot write to stdout");
+				if (rc)
+					break;
+			}
 			if (read_status) {
 				for (uint64_t i = 0; i < b.n; ++i) {
 					uint32_t c = b.cat[i];
@@ -363,8 +489,15 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 		cudaFreeHost(x.seq[0]);
 		cudaFreeHost(x.seq[1]);
 	}
+	bool closed = true;
+	for (int m = 0; m < 2; ++m)
+		for (OutFile &o : outs[m])
+			closed = o.close() && closed;
+	fflush(stdout);
 	if (rc)
 		return rc;
+	if (!closed)
+		return fail(ctx, BBT_ERR_IO, "cannot write a categorized read file");
 	if (!pipe.err.empty())
 		return fail(ctx, BBT_ERR_IO, pipe.err);
 	std::cerr << "Total Reads: " << total << "\n";
@@ -408,4 +541,31 @@ extern "C" int bbt_filter_pair_files(bbt_ctx *ctx, const char *file1, const char
 	std::string f2 = file2;
 	std::cerr << "Filtering Start" << std::endl;
 	return run_pipeline(ctx, f, &f2, prefix, read_status);
+}
+
+extern "C" int bbt_filter_files_print(bbt_ctx *ctx, const char *const *files, int n_files,
+		const char *prefix, const char *out_type, const char *postfix, const char *read_status)
+{
+	if (!ctx || !files || n_files <= 0)
+		return fail(ctx, BBT_ERR_ARG, "bbt_filter_files_print: need at least one input file");
+	if (!out_type || (std::string(out_type) != "fa" && std::string(out_type) != "fq"))
+		return fail(ctx, BBT_ERR_ARG, "bbt_filter_files_print: out_type is \"fa\" or \"fq\"");
+	std::vector<std::string> f;
+	for (int i = 0; i < n_files; ++i)
+		f.push_back(files[i]);
+	std::cerr << "Filtering Start" << std::endl;
+	return run_pipeline(ctx, f, nullptr, prefix, read_status, out_type, postfix);
+}
+
+extern "C" int bbt_filter_pair_files_print(bbt_ctx *ctx, const char *file1, const char *file2,
+		const char *prefix, const char *out_type, const char *postfix, const char *read_status)
+{
+	if (!ctx || !file1 || !file2)
+		return fail(ctx, BBT_ERR_ARG, "bbt_filter_pair_files_print: need two input files");
+	if (!out_type || (std::string(out_type) != "fa" && std::string(out_type) != "fq"))
+		return fail(ctx, BBT_ERR_ARG, "bbt_filter_pair_files_print: out_type is \"fa\" or \"fq\"");
+	std::vector<std::string> f(1, file1);
+	std::string f2 = file2;
+	std::cerr << "Filtering Start" << std::endl;
+	return run_pipeline(ctx, f, &f2, prefix, read_status, out_type, postfix);
 }

@@ -162,6 +162,26 @@ int bbt_filter_files(bbt_ctx *ctx, const char *const *files, int n_files,
 int bbt_filter_pair_files(bbt_ctx *ctx, const char *file1, const char *file2,
 		const char *prefix, const char *read_status);
 
+/*
+ * The same pipelines, also writing every read (pair) to a file of its category
+ * (--fa / --fq, with -g for gzip): "<prefix>_<filterID>.<out_type><postfix>"
+ * per filter, then "_noMatch" and "_multiMatch" (pairs: "_1" / "_2" before
+ * the extension); records are ">name comment\nseq\n" or
+ * "@name comment\nseq\n+\nqual\n" in input order.  out_type: "fa" or "fq";
+ * postfix: "" or ".gz".  Replaces BioBloomClassifier::filterPrint
+ * (BioBloomClassifier.cpp:108-203) and filterPairPrint (:311-450).
+ */
+int bbt_filter_files_print(bbt_ctx *ctx, const char *const *files, int n_files,
+		const char *prefix, const char *out_type, const char *postfix, const char *read_status);
+int bbt_filter_pair_files_print(bbt_ctx *ctx, const char *file1, const char *file2,
+		const char *prefix, const char *out_type, const char *postfix, const char *read_status);
+
+/* -d / -n: the file pipelines also print, as FASTQ on stdout, each read (both
+ * mates of a pair) whose category is the first filter (inverse: every other
+ * category).  Replaces BioBloomClassifier::setStdout and printSingle /
+ * printPair (BioBloomClassifier.h:81-83, 115-142, 211-247). */
+int bbt_set_stdout(bbt_ctx *ctx, int on, int inverse);
+
 /* Pairs count for a filter when either mate hits (-i; union of the mates' hit
  * lists) instead of both (intersection, the default).
  * Replaces BioBloomClassifier::setInclusive (BioBloomClassifier.h:77-79). */
