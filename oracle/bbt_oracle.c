@@ -436,6 +436,173 @@ int oracle_eval_simple(const char *seq, size_t len, const oracle_bf *bf,
 	return 0;
 }
 
+/* SeqEval::evalHarmonic (Common/SeqEval.h:116-193), without dust/subtract:
+ * evalSimple's walk, with a hit in a streak of s earlier hits adding
+ * 1 - 1/(1 + s) instead of 1. */
+int oracle_eval_harmonic(const char *seq, size_t len, const oracle_bf *bf,
+		double threshold, unsigned streak_threshold, uint64_t *probes)
+{
+	const size_t frames = len - bf->k + 1; /* size_t arithmetic, as upstream */
+	const double thres = threshold * (double)frames;
+	const double anti_thres = floor((1.0 - threshold) * (double)frames);
+	double score = 0;
+	unsigned anti = 0, streak = 0, prev = 0;
+	oracle_ntitr it;
+	oracle_ntitr_init(&it, seq, len, bf->k, bf->k);
+	if (!oracle_ntitr_end(&it)) {
+		if (oracle_bf_contains(bf, it.hv, probes)) {
+			score += 0.5;
+			if (thres <= score)
+				return 1;
+			++streak;
+		} else {
+			if (anti_thres <= ++anti)
+				return 0;
+		}
+		prev = (unsigned)it.pos;
+		oracle_ntitr_next(&it);
+	}
+	while (!oracle_ntitr_end(&it)) {
+		if (it.pos != (size_t)prev + 1) {
+			anti += (unsigned)(it.pos - prev - 1);
+			if (anti_thres <= anti)
+				return 0;
+			streak = 0;
+		}
+		if (oracle_bf_contains(bf, it.hv, probes)) {
+			if (streak == 0)
+				score += 0.5;
+			else
+				score += 1.0 - 1.0 / (1.0 + (double)streak);
+			if (thres <= score)
+				return 1;
+			prev = (unsigned)it.pos;
+			oracle_ntitr_next(&it);
+			++streak;
+		} else {
+			if (streak < streak_threshold) {
+				if (anti_thres <= ++anti)
+					return 0;
+				prev = (unsigned)it.pos;
+				oracle_ntitr_next(&it);
+			} else {
+				unsigned skip_end = (unsigned)it.pos + bf->k;
+				while (it.pos < skip_end) {
+					if (anti_thres <= ++anti)
+						return 0;
+					prev = (unsigned)it.pos;
+					oracle_ntitr_next(&it);
+				}
+			}
+			streak = 0;
+		}
+	}
+	return 0;
+}
+
+/* BloomFilter::getFPRPrecompute as restated: (set bits / m) ^ h. */
+double oracle_bf_fpr(const oracle_bf *bf)
+{
+	uint64_t pop = 0;
+	for (uint64_t i = 0; i < bf->m / 8; ++i)
+		pop += (uint64_t)__builtin_popcount(bf->bits[i]);
+	return pow((double)pop / (double)bf->m, (double)bf->h);
+}
+
+/* P(X > x) summed from the top of the tail down, and the smallest x with
+ * P(X > x) <= q. */
+static double binom_pmf(double n, double p, double i)
+{
+	if (p <= 0.0)
+		return i == 0 ? 1.0 : 0.0;
+	if (p >= 1.0)
+		return i == n ? 1.0 : 0.0;
+	return exp(lgamma(n + 1) - lgamma(i + 1) - lgamma(n - i + 1) + i * log(p) +
+			(n - i) * log1p(-p));
+}
+
+unsigned oracle_binom_upper_quantile(unsigned n, double p, double q)
+{
+	double x = n, tail = 0.0;
+	while (x > 0) {
+		double t = tail + binom_pmf(n, p, x);
+		if (t > q)
+			break;
+		tail = t;
+		x -= 1.0;
+	}
+	return (unsigned)x;
+}
+
+/* SeqEval::calcMinCount (Common/SeqEval.h:199-207). */
+unsigned oracle_calc_min_count(unsigned frame_len, double bf_fpr, double min_fpr)
+{
+	unsigned i = oracle_binom_upper_quantile(frame_len, bf_fpr, min_fpr);
+	return i > 1 ? i : 1;
+}
+
+/* SeqEval::evalBinomial (Common/SeqEval.h:218-290), without dust/subtract:
+ * every hit adds 1; accept at calcMinCount hits, reject at frameLen minus that
+ * many misses.  fpr = the filter's getFPRPrecompute(). */
+int oracle_eval_binomial(const char *seq, size_t len, const oracle_bf *bf,
+		double threshold, double fpr, unsigned streak_threshold, uint64_t *probes)
+{
+	if (len < bf->k)
+		return 0;
+	const unsigned frame_len = (unsigned)(len - bf->k + 1);
+	const unsigned thres = oracle_calc_min_count(frame_len, fpr, threshold);
+	const unsigned anti_thres = frame_len - thres;
+	unsigned score = 0, anti = 0, streak = 0, prev = 0;
+	oracle_ntitr it;
+	oracle_ntitr_init(&it, seq, len, bf->k, bf->k);
+	if (!oracle_ntitr_end(&it)) {
+		if (oracle_bf_contains(bf, it.hv, probes)) {
+			score++;
+			if (thres <= score)
+				return 1;
+			++streak;
+		} else {
+			if (anti_thres <= ++anti)
+				return 0;
+		}
+		prev = (unsigned)it.pos;
+		oracle_ntitr_next(&it);
+	}
+	while (!oracle_ntitr_end(&it)) {
+		if (it.pos != (size_t)prev + 1) {
+			anti += (unsigned)(it.pos - prev - 1);
+			if (anti_thres <= anti)
+				return 0;
+			streak = 0;
+		}
+		if (oracle_bf_contains(bf, it.hv, probes)) {
+			++score;
+			if (thres <= score)
+				return 1;
+			prev = (unsigned)it.pos;
+			oracle_ntitr_next(&it);
+			++streak;
+		} else {
+			if (streak < streak_threshold) {
+				if (anti_thres <= ++anti)
+					return 0;
+				prev = (unsigned)it.pos;
+				oracle_ntitr_next(&it);
+			} else {
+				unsigned skip_end = (unsigned)it.pos + bf->k;
+				while (it.pos < skip_end) {
+					if (anti_thres <= ++anti)
+						return 0;
+					prev = (unsigned)it.pos;
+					oracle_ntitr_next(&it);
+				}
+			}
+			streak = 0;
+		}
+	}
+	return 0;
+}
+
 /* SeqEval::evalMinMatchLen (Common/SeqEval.h:295-332), without
  * dust/subtract.  The iterator is built with getHashNum() hashes. */
 int oracle_eval_min_match_len(const char *seq, size_t len,
@@ -475,6 +642,10 @@ void oracle_classify(const char *seq, const uint64_t *off, size_t n,
 		uint64_t *probes)
 {
 	unsigned words = (nf + 63) / 64;
+	double fpr[1024];
+	if (scoring == ORACLE_BINOMIAL)
+		for (unsigned f = 0; f < nf && f < 1024; ++f)
+			fpr[f] = oracle_bf_fpr(filters[f]);
 	for (size_t r = 0; r < n; ++r) {
 		const char *s = seq + off[r];
 		size_t len = (size_t)(off[r + 1] - off[r]);
@@ -485,6 +656,12 @@ void oracle_classify(const char *seq, const uint64_t *off, size_t n,
 			if (scoring == ORACLE_LENGTH)
 				hit = oracle_eval_min_match_len(s, len, filters[f],
 						(unsigned)round(threshold), probes);
+			else if (scoring == ORACLE_HARMONIC)
+				hit = oracle_eval_harmonic(s, len, filters[f], threshold,
+						streak_threshold, probes);
+			else if (scoring == ORACLE_BINOMIAL)
+				hit = oracle_eval_binomial(s, len, filters[f], threshold, fpr[f],
+						streak_threshold, probes);
 			else
 				hit = oracle_eval_simple(s, len, filters[f], threshold,
 						streak_threshold, probes);

@@ -123,10 +123,23 @@ int oracle_eval_simple(const char *seq, size_t len, const oracle_bf *bf,
 int oracle_eval_min_match_len(const char *seq, size_t len,
 		const oracle_bf *bf, unsigned min_match_len, uint64_t *probes);
 
+/* SeqEval::evalHarmonic (HARMONIC scoring, -S harmonic). */
+int oracle_eval_harmonic(const char *seq, size_t len, const oracle_bf *bf,
+		double threshold, unsigned streak_threshold, uint64_t *probes);
+/* SeqEval::evalBinomial (BINOMIAL scoring, -S binomial): threshold is the
+ * minimum FPR of a match (10^(-s/10)), fpr the filter's (set bits / m)^h. */
+int oracle_eval_binomial(const char *seq, size_t len, const oracle_bf *bf,
+		double threshold, double fpr, unsigned streak_threshold, uint64_t *probes);
+double oracle_bf_fpr(const oracle_bf *bf);
+/* Binomial(n, p): smallest x with P(X > x) <= q, summed from the top of the
+ * tail (boost's quantile(complement(...)) under integer_round_up). */
+unsigned oracle_binom_upper_quantile(unsigned n, double p, double q);
+unsigned oracle_calc_min_count(unsigned frame_len, double bf_fpr, double min_fpr);
+
 /* ---------------- Batch driver + summary ---------------- */
 
-/* Scoring methods, in the order of opt::ScoringMethod (Common/Options.h:75). */
-enum { ORACLE_SIMPLE = 0, ORACLE_LENGTH = 1 };
+/* Scoring methods, in the order of opt::ScoringMethod (Common/Options.h:35). */
+enum { ORACLE_SIMPLE = 0, ORACLE_LENGTH = 1, ORACLE_HARMONIC = 2, ORACLE_BINOMIAL = 3 };
 
 /* Classify reads against nf filters (evaluateReadStd,
  * BioBloomClassifier.cpp:1182-1189).  Reads are seq[off[i] .. off[i+1]).

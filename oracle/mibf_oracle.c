@@ -439,28 +439,3 @@ unsigned oracle_mibf_query(const oracle_mibf *f, const char *seq, size_t len,
 	free(t);
 	return nout;
 }
-
-/* P(X > x) summed from the top of the tail down, and the smallest x with
- * P(X > x) <= q. */
-static double binom_pmf(double n, double p, double i)
-{
-	if (p <= 0.0)
-		return i == 0 ? 1.0 : 0.0;
-	if (p >= 1.0)
-		return i == n ? 1.0 : 0.0;
-	return exp(lgamma(n + 1) - lgamma(i + 1) - lgamma(n - i + 1) + i * log(p) +
-			(n - i) * log1p(-p));
-}
-
-unsigned oracle_binom_upper_quantile(unsigned n, double p, double q)
-{
-	double x = n, tail = 0.0;
-	while (x > 0) {
-		double t = tail + binom_pmf(n, p, x);
-		if (t > q)
-			break;
-		tail = t;
-		x -= 1.0;
-	}
-	return (unsigned)x;
-}

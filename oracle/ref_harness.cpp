@@ -22,6 +22,7 @@
 #include "Common/Options.h"
 #include "Common/SeqEval.h"
 #include <omp.h>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <sstream>
@@ -41,8 +42,20 @@ static vector<string> split_commas(const string &s)
 	return out;
 }
 
+/* -s as BioBloomCategorizer.cpp:414-441 reads it; the scoring method (-S)
+ * comes from the environment variable BBT_SCORING ("harmonic" or
+ * "binomial"; unset = simple). */
 static void set_score(double score)
 {
+	const char *m = getenv("BBT_SCORING");
+	std::string method = m ? m : "";
+	if (method == "binomial") {
+		opt::scoringMethod = opt::BINOMIAL;
+		opt::score = pow(10.0, -(score / 10.0));
+		return;
+	}
+	if (method == "harmonic")
+		opt::scoringMethod = opt::HARMONIC;
 	opt::score = score;
 	unsigned matchLen = (unsigned)score;
 	if (matchLen > 1) {

@@ -14,6 +14,8 @@ LIB_PATH = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
 
 SIMPLE = 0
 LENGTH = 1
+HARMONIC = 2
+BINOMIAL = 3
 
 
 class _BF(ctypes.Structure):

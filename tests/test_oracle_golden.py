@@ -122,3 +122,47 @@ def test_sizing_matches_reference_formulas():
     # Common/BloomFilterInfo.h:57-76 for the 5 Mbp, k=25, FPR 0.075 filter
     assert ol.lib().oracle_calc_optimal_hash_num(0.075) == 3
     assert ol.lib().oracle_calc_optimal_size(5000000 - 24, 0.075, 3) == 27387648
+
+
+# HARMONIC / BINOMIAL scoring (-S), golden files from tests/golden/make_golden_modes.py
+MODE_CASES = [("harmonic_s0.15_r3", "harmonic", 0.15, 3, False),
+              ("harmonic_s0.4_r1", "harmonic", 0.4, 1, False),
+              ("harmonic_pe_s0.15_r3", "harmonic", 0.15, 3, True),
+              ("binomial_s100_r3", "binomial", 100, 3, False),
+              ("binomial_s30_r2", "binomial", 30, 2, False),
+              ("binomial_pe_s100_r3", "binomial", 100, 3, True)]
+
+
+def mode_args(method, score):
+    """(threshold, scoring) as BioBloomCategorizer.cpp:414-441 derives them."""
+    if method == "binomial":
+        return 10.0 ** (-(score / 10.0)), ol.BINOMIAL
+    return score, ol.HARMONIC
+
+
+@pytest.mark.parametrize("name,method,score,streak,paired", MODE_CASES)
+def test_oracle_scoring_modes_match_reference(name, method, score, streak, paired):
+    filters = [ol.Filter.load(p) for p in filter_paths()]
+    thr, scoring = mode_args(method, score)
+    rows, summary = expected_hits(name)
+    if paired:
+        r1 = read_fastx(golden("reads_1.fq.gz"))
+        r2 = read_fastx(golden("reads_2.fq.gz"))
+        s1, o1 = ol.pack_reads([s for _, s in r1])
+        s2, o2 = ol.pack_reads([s for _, s in r2])
+        h1, _ = ol.classify(s1, o1, filters, thr, streak, scoring)
+        h2, _ = ol.classify(s2, o2, filters, thr, streak, scoring)
+        assert _hitsets(h1, 3) == [r[1] for r in rows]
+        assert _hitsets(h2, 3) == [r[2] for r in rows]
+        counts, _ = ol.summary_counts(h1, 3, h2)
+        n = len(r1)
+    else:
+        recs = read_fastx(golden("reads_se.fa.gz"))
+        seq, off = ol.pack_reads([s for _, s in recs])
+        hits, _ = ol.classify(seq, off, filters, thr, streak, scoring)
+        assert _hitsets(hits, 3) == [r[1] for r in rows]
+        counts, _ = ol.summary_counts(hits, 3)
+        n = len(recs)
+    assert ol.summary_tsv(counts, filter_ids(), n) == summary
+    with open(golden(f"expected_summary_{name}.tsv")) as f:
+        assert ol.summary_tsv(counts, filter_ids(), n) == f.read()
