@@ -16,7 +16,7 @@ BBT_ERR = {-1: "ARG", -2: "IO", -3: "FORMAT", -4: "CUDA", -5: "NOMEM", -6: "UNSU
 ERR_OVERFLOW = -9
 MIBF_OUT_TSV, MIBF_OUT_FASTA, MIBF_OUT_FASTQ = 0, 1, 2
 MIBF_LAYOUT_AUTO, MIBF_LAYOUT_RANK, MIBF_LAYOUT_DENSE = 0, 1, 2
-SCORE_SIMPLE, SCORE_LENGTH = 0, 1
+SCORE_SIMPLE, SCORE_LENGTH, SCORE_HARMONIC, SCORE_BINOMIAL = 0, 1, 2, 3
 HOST, DEVICE = 0, 1
 PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT, PATH_FILTER_MAJOR = 0, 1, 2, 3
 

@@ -29,12 +29,17 @@ def pack(seqs):
 
 
 class BioBloomClassifier:
-    def __init__(self, filter_paths, score_threshold=0.15, prefix="", postfix="", *,
+    def __init__(self, filter_paths, score_threshold=None, prefix="", postfix="", *,
                  streak_threshold=3, device=0, path=L.PATH_AUTO, warps_per_block=0,
-                 frames_per_lane=0, max_batch_reads=0, max_batch_bases=0, l2_fetch_bytes=0):
+                 frames_per_lane=0, max_batch_reads=0, max_batch_bases=0, l2_fetch_bytes=0,
+                 score_type="simple"):
+        """score_type: "simple", "harmonic" or "binomial" (-S); for binomial the
+        score is the -s value, the minimum -10*log10(FPR) of a match [100]."""
         lib = L.lib()
         p = L.Params()
         lib.bbt_default_params(ctypes.byref(p))
+        if score_threshold is None:
+            score_threshold = 100 if score_type == "binomial" else 0.15
         p.score = float(score_threshold)
         p.streak_threshold = int(streak_threshold)
         p.device = int(device)
@@ -44,11 +49,16 @@ class BioBloomClassifier:
         p.max_batch_reads = int(max_batch_reads)
         p.max_batch_bases = int(max_batch_bases)
         p.l2_fetch_bytes = int(l2_fetch_bytes)
-        # BioBloomCategorizer.cpp:423-430: an integer score > 1 is a minimum
-        # match length (LENGTH scoring)
-        if int(score_threshold) > 1:
+        # BioBloomCategorizer.cpp:414-441: binomial scores are -10*log10(FPR);
+        # otherwise an integer score > 1 is a minimum match length
+        if score_type == "binomial":
+            p.scoring = L.SCORE_BINOMIAL
+            p.score = 10.0 ** (-(float(score_threshold) / 10.0))
+        elif int(score_threshold) > 1:
             p.score = float(int(score_threshold))
             p.scoring = L.SCORE_LENGTH
+        elif score_type == "harmonic":
+            p.scoring = L.SCORE_HARMONIC
         paths = [str(x).encode() for x in filter_paths]
         arr = (ctypes.c_char_p * len(paths))(*paths)
         ctx = ctypes.c_void_p()

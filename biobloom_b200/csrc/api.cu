@@ -134,6 +134,8 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 	cudaFree(ctx->d_work);
 	cudaFree(ctx->d_order);
 	cudaFree(ctx->d_order_cnt);
+	cudaFree(ctx->d_bthres);
+	cudaFree(ctx->d_lenset);
 	cudaFree(ctx->d_stat);
 	cudaFree(ctx->d_tmp_hits[0]);
 	cudaFree(ctx->d_tmp_hits[1]);
@@ -170,8 +172,10 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 }
 
 /* Read one .bf payload and copy it to the device in pinned chunks. */
-static int upload_filter(bbt_ctx *ctx, const std::string &path, BfHeader &hd, uint32_t **d_out)
+static int upload_filter(bbt_ctx *ctx, const std::string &path, BfHeader &hd, uint32_t **d_out,
+		uint64_t *pop_out)
 {
+	uint64_t pop = 0;
 	FILE *f = fopen(path.c_str(), "rb");
 	if (!f)
 		return fail(ctx, BBT_ERR_IO, "file " + path + " cannot be opened");
@@ -211,6 +215,11 @@ static int upload_filter(bbt_ctx *ctx, const std::string &path, BfHeader &hd, ui
 			rc = fail(ctx, BBT_ERR_FORMAT, path + ": filter payload is shorter than its header says");
 			break;
 		}
+		for (size_t i = 0; i + 8 <= n; i += 8) {
+			uint64_t w;
+			memcpy(&w, buf + i, 8);
+			pop += (uint64_t)__builtin_popcountll(w);
+		}
 		e = cudaMemcpyAsync((char *)d + done, buf, n, cudaMemcpyHostToDevice, ctx->h2d);
 		if (e != cudaSuccess) {
 			rc = cuda_fail(ctx, e, "cudaMemcpyAsync(filter)");
@@ -231,6 +240,8 @@ static int upload_filter(bbt_ctx *ctx, const std::string &path, BfHeader &hd, ui
 		return rc;
 	}
 	*d_out = d;
+	if (pop_out)
+		*pop_out = pop;
 	return BBT_OK;
 }
 
@@ -251,7 +262,7 @@ static int alloc_slot(bbt_ctx *ctx, Slot &s, uint64_t bases, uint64_t reads)
  * persistent read-major kernel. */
 static int auto_path(const bbt_ctx *ctx)
 {
-	if (ctx->nf < 2 || !ctx->same_k)
+	if (ctx->nf < 2 || !ctx->same_k || ctx->p.scoring > BBT_SCORE_LENGTH)
 		return BBT_PATH_PERSISTENT;
 	int l2 = 0;
 	cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->dev);
@@ -283,8 +294,8 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 		ctx->p = *params;
 	else
 		bbt_default_params(&ctx->p);
-	if (ctx->p.score > 1 && ctx->p.scoring == BBT_SCORE_SIMPLE &&
-			(unsigned)ctx->p.score > 1) {
+	if (ctx->p.score > 1 && (ctx->p.scoring == BBT_SCORE_SIMPLE ||
+			ctx->p.scoring == BBT_SCORE_HARMONIC) && (unsigned)ctx->p.score > 1) {
 		/* BioBloomCategorizer.cpp:423-430: an integer score > 1 is a
 		 * minimum match length */
 		ctx->p.score = (double)(unsigned)ctx->p.score;
@@ -292,6 +303,14 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 	}
 	if (ctx->p.scoring == BBT_SCORE_SIMPLE && (ctx->p.score < 0 || ctx->p.score > 1)) {
 		std::string m = "score must be in [0, 1] or an integer > 1";
+		bbt_close(ctx);
+		return fail(nullptr, BBT_ERR_ARG, m);
+	}
+	if ((ctx->p.scoring == BBT_SCORE_HARMONIC && (ctx->p.score < 0 || ctx->p.score > 1)) ||
+			(ctx->p.scoring == BBT_SCORE_BINOMIAL && !(ctx->p.score > 0 && ctx->p.score <= 1)) ||
+			ctx->p.scoring < BBT_SCORE_SIMPLE || ctx->p.scoring > BBT_SCORE_BINOMIAL) {
+		std::string m = "harmonic scores are in [0, 1]; binomial scores are a minimum FPR in "
+				"(0, 1]; the scoring method is BBT_SCORE_*";
 		bbt_close(ctx);
 		return fail(nullptr, BBT_ERR_ARG, m);
 	}
@@ -355,11 +374,14 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 		ctx->ids.push_back(it->second);
 		BfHeader hd;
 		uint32_t *d = nullptr;
-		rc = upload_filter(ctx, path, hd, &d);
+		uint64_t pop = 0;
+		rc = upload_filter(ctx, path, hd, &d, &pop);
 		if (rc != BBT_OK)
 			goto fail_out;
 		ctx->d_words.push_back(d);
 		ctx->hf.push_back(make_filter_dev(d, hd.m, hd.h, hd.k));
+		/* BloomFilter::getFPRPrecompute as restated: (set bits / m) ^ h */
+		ctx->fpr.push_back(pow((double)pop / (double)hd.m, (double)hd.h));
 		ctx->kmax = std::max(ctx->kmax, hd.k);
 	}
 	ctx->nf = (uint32_t)n_filters;
@@ -405,6 +427,135 @@ extern "C" const char *bbt_filter_id(const bbt_ctx *ctx, int i)
 	return ctx->ids[i].c_str();
 }
 
+/* ---- BINOMIAL thresholds: calcMinCount(frames, fpr of filter, score) ---- */
+
+namespace bbt {
+unsigned binom_upper_quantile(unsigned n, double p, double q);
+}
+
+/* Rows for read lengths below `rows` (callers hold bt_mu). */
+static int bt_grow(bbt_ctx *ctx, uint64_t rows)
+{
+	if (rows <= ctx->bt_rows)
+		return BBT_OK;
+	rows = std::max<uint64_t>(rows, std::max<uint64_t>(2 * ctx->bt_rows, 1024));
+	std::vector<uint32_t> h((size_t)ctx->nf * rows, 0);
+	for (uint32_t f = 0; f < ctx->nf && ctx->bt_rows; ++f)
+		memcpy(&h[(size_t)f * rows], &ctx->h_bthres[(size_t)f * ctx->bt_rows], ctx->bt_rows * 4);
+	uint32_t *d = nullptr;
+	CUDA_TRY(ctx, cudaDeviceSynchronize()); /* no kernel may still read the old table */
+	CUDA_TRY(ctx, cudaMalloc(&d, h.size() * 4));
+	CUDA_TRY(ctx, cudaMemcpy(d, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
+	cudaFree(ctx->d_bthres);
+	ctx->d_bthres = d;
+	ctx->h_bthres.swap(h);
+	ctx->bt_have.resize(rows, 0);
+	ctx->bt_rows = rows;
+	return BBT_OK;
+}
+
+/* Make the rows of these read lengths present on the device. */
+static int ensure_bthres(bbt_ctx *ctx, const std::vector<uint64_t> &lens)
+{
+	if (ctx->p.scoring != BBT_SCORE_BINOMIAL || lens.empty())
+		return BBT_OK;
+	std::lock_guard<std::mutex> lk(ctx->bt_mu);
+	int rc = bt_grow(ctx, lens.back() + 1);
+	if (rc)
+		return rc;
+	std::vector<uint64_t> missing;
+	for (uint64_t L : lens)
+		if (!ctx->bt_have[L])
+			missing.push_back(L);
+	if (missing.empty())
+		return BBT_OK;
+	const long long nm = (long long)missing.size() * ctx->nf;
+#pragma omp parallel for schedule(dynamic, 8)
+	for (long long t = 0; t < nm; ++t) {
+		const uint64_t L = missing[t / ctx->nf];
+		const uint32_t f = (uint32_t)(t % ctx->nf);
+		const unsigned k = ctx->hf[f].k;
+		if (L < k)
+			continue;
+		const uint64_t fc = L - k + 1;
+		const unsigned i = binom_upper_quantile((unsigned)fc, ctx->fpr[f], ctx->p.score);
+		ctx->h_bthres[(size_t)f * ctx->bt_rows + fc] = i > 1 ? i : 1;
+	}
+	for (uint64_t L : missing)
+		ctx->bt_have[L] = 1;
+	/* rows L - k + 1 of each filter, for the lengths just computed */
+	for (uint32_t f = 0; f < ctx->nf; ++f) {
+		const unsigned k = ctx->hf[f].k;
+		for (uint64_t L : missing) {
+			if (L < k)
+				continue;
+			const size_t at = (size_t)f * ctx->bt_rows + (L - k + 1);
+			CUDA_TRY(ctx, cudaMemcpy(ctx->d_bthres + at, &ctx->h_bthres[at], 4,
+					cudaMemcpyHostToDevice));
+		}
+	}
+	return BBT_OK;
+}
+
+static std::vector<uint64_t> host_lengths(const uint64_t *off, const uint64_t *off2, uint64_t n)
+{
+	std::vector<uint64_t> lens;
+	std::vector<uint8_t> seen;
+	for (int m = 0; m < (off2 ? 2 : 1); ++m) {
+		const uint64_t *o = m ? off2 : off;
+		for (uint64_t i = 0; i < n; ++i) {
+			const uint64_t L = o[i + 1] - o[i];
+			if (L >= seen.size())
+				seen.resize(L + 1, 0);
+			if (!seen[L]) {
+				seen[L] = 1;
+				lens.push_back(L);
+			}
+		}
+	}
+	std::sort(lens.begin(), lens.end());
+	return lens;
+}
+
+static int device_lengths(bbt_ctx *ctx, const bbt_batch *b, cudaStream_t s,
+		std::vector<uint64_t> &lens)
+{
+	if (!ctx->d_lenset)
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_lenset, (1 + 2048) * 4));
+	CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_lenset, 0, (1 + 2048) * 4, s));
+	CUDA_TRY(ctx, launch_length_set(b->offsets, b->seq2 ? b->offsets2 : nullptr, b->n_reads,
+			b->seq2 ? 2 : 1, ctx->d_lenset, ctx->num_sms, s));
+	std::vector<unsigned int> h(1 + 2048);
+	CUDA_TRY(ctx, cudaMemcpyAsync(h.data(), ctx->d_lenset, h.size() * 4, cudaMemcpyDeviceToHost,
+			s));
+	CUDA_TRY(ctx, cudaStreamSynchronize(s));
+	for (uint64_t L = 0; L < 65536 && L <= h[0]; ++L)
+		if ((h[1 + (L >> 5)] >> (L & 31)) & 1u)
+			lens.push_back(L);
+	for (uint64_t L = 65536; L <= h[0]; ++L) /* rare: every longer length up to the maximum */
+		lens.push_back(L);
+	return BBT_OK;
+}
+
+int bbt::bf_reserve_rows(bbt_ctx *ctx, uint64_t max_len)
+{
+	if (ctx->p.scoring != BBT_SCORE_BINOMIAL)
+		return BBT_OK;
+	std::lock_guard<std::mutex> lk(ctx->bt_mu);
+	return bt_grow(ctx, max_len + 1);
+}
+
+int bbt::bf_rows_for(bbt_ctx *ctx, const uint64_t *off, const uint64_t *off2, uint64_t n)
+{
+	if (ctx->p.scoring != BBT_SCORE_BINOMIAL)
+		return BBT_OK;
+	std::vector<uint64_t> lens = host_lengths(off, off2, n);
+	if (!lens.empty() && lens.back() >= ctx->bt_rows)
+		return fail(ctx, BBT_ERR_ARG, "a read is longer than the binomial threshold rows "
+				"reserved for serving");
+	return ensure_bthres(ctx, lens);
+}
+
 static ClassifyArgs base_args(const bbt_ctx *ctx)
 {
 	ClassifyArgs a;
@@ -418,6 +569,8 @@ static ClassifyArgs base_args(const bbt_ctx *ctx)
 	a.scoring = ctx->p.scoring;
 	a.min_len = (unsigned)std::round(ctx->p.score);
 	a.kmax = ctx->kmax;
+	a.bthres = ctx->d_bthres;
+	a.bthres_rows = ctx->bt_rows;
 	a.work = ctx->d_work;
 	if (ctx->lc.count) {
 		a.probes = ctx->d_stat;
@@ -514,7 +667,8 @@ static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStream_t s)
 {
 	ctx->last.kernels = 2; /* classification (counted below for two-pass) + summary */
-	const bool two_pass = ctx->lc.path == BBT_PATH_FILTER_MAJOR && ctx->same_k;
+	const bool two_pass = ctx->lc.path == BBT_PATH_FILTER_MAJOR && ctx->same_k &&
+			ctx->p.scoring <= BBT_SCORE_LENGTH;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k0, s));
 	if (two_pass) {
 		/* accepted (filter, read) items OR their bit into zeroed words */
@@ -567,6 +721,15 @@ static int ensure_tmp_hits(bbt_ctx *ctx, uint64_t n)
 static int classify_device(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r, cudaStream_t s)
 {
 	const bool paired = b->seq2 != nullptr;
+	if (ctx->p.scoring == BBT_SCORE_BINOMIAL && !ctx->capturing) {
+		/* the thresholds of the batch's read lengths (a short host wait) */
+		std::vector<uint64_t> lens;
+		int rc = device_lengths(ctx, b, s, lens);
+		if (!rc)
+			rc = ensure_bthres(ctx, lens);
+		if (rc)
+			return rc;
+	}
 	ClassifyArgs a = base_args(ctx);
 	a.seq[0] = (const uint8_t *)b->seq;
 	a.off[0] = b->offsets;
@@ -598,6 +761,11 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r)
 {
 	const bool paired = b->seq2 != nullptr;
 	const uint64_t n = b->n_reads;
+	if (ctx->p.scoring == BBT_SCORE_BINOMIAL) {
+		int rc = ensure_bthres(ctx, host_lengths(b->offsets, paired ? b->offsets2 : nullptr, n));
+		if (rc)
+			return rc;
+	}
 	uint64_t i0 = 0;
 	int which = 0;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
@@ -1003,9 +1171,18 @@ extern "C" int bbt_graph_create(bbt_ctx *ctx, const bbt_batch *b, const bbt_resu
 		if (rc)
 			return rc;
 	}
+	if (ctx->p.scoring == BBT_SCORE_BINOMIAL) { /* thresholds before capture */
+		std::vector<uint64_t> lens;
+		int rc = device_lengths(ctx, b, ctx->stream, lens);
+		if (!rc)
+			rc = ensure_bthres(ctx, lens);
+		if (rc)
+			return rc;
+	}
 	bbt_graph *g = new bbt_graph();
 	g->ctx = ctx;
 	g->reads = n;
+	ctx->capturing = true;
 	cudaError_t e = cudaStreamCreateWithFlags(&g->capture, cudaStreamNonBlocking);
 	if (e == cudaSuccess)
 		e = cudaStreamBeginCapture(g->capture, cudaStreamCaptureModeThreadLocal);
@@ -1025,6 +1202,7 @@ extern "C" int bbt_graph_create(bbt_ctx *ctx, const bbt_batch *b, const bbt_resu
 	}
 	cudaGraph_t graph = nullptr;
 	e = cudaStreamEndCapture(g->capture, &graph);
+	ctx->capturing = false;
 	if (rc == BBT_OK && e != cudaSuccess)
 		rc = cuda_fail(ctx, e, "cudaStreamEndCapture");
 	g->graph = graph;

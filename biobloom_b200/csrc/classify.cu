@@ -41,7 +41,7 @@ namespace {
 /* Evaluate read r against filters [f0, f1).  Returns the hit bits of those
  * filters that fall in word f0 / 64 (bit f % 64); read-major launches call it
  * with the whole filter range and write every word themselves. */
-template <int SEG, bool COUNT, bool LENGTH_MODE>
+template <int SEG, bool COUNT, int MODE>
 __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, uint32_t f1,
 		const Window<SEG> &win, int lane, uint64_t &myword, unsigned long long &probe_acc,
 		unsigned long long &frame_acc, unsigned long long &alg_acc)
@@ -64,8 +64,14 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 		const uint64_t frames = len - k + 1;
 		SimpleState st;
 		LengthState ls;
-		constexpr bool length_mode = LENGTH_MODE;
-		if (length_mode)
+		SeqState qs;
+		constexpr bool length_mode = MODE == BBT_SCORE_LENGTH;
+		constexpr bool seq_mode = MODE == BBT_SCORE_HARMONIC || MODE == BBT_SCORE_BINOMIAL;
+		if (MODE == BBT_SCORE_HARMONIC)
+			harmonic_init(qs, a.score, a.one_minus, frames);
+		else if (MODE == BBT_SCORE_BINOMIAL)
+			binomial_init(qs, a.bthres[f * a.bthres_rows + frames], (uint32_t)frames);
+		else if (length_mode)
 			length_init(ls, a.min_len, len, (int)k);
 		else
 			simple_init(st, a.score, a.one_minus, frames);
@@ -83,8 +89,8 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 			}
 			for (int c = 0; c < wn;) {
 				/* frames [c, c + nfc) of the window this step */
-				const int nfc = min((length_mode || !a.tight_steps) ? 32 : simple_step_frames(st),
-						wn - c);
+				const int nfc = min((length_mode || seq_mode || !a.tight_steps) ? 32
+						: simple_step_frames(st), wn - c);
 				const int q = c + lane;
 				const int32_t p = (int32_t)w0 + q;
 				const int vi = c >> 5, vs = c & 31;
@@ -94,13 +100,17 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 				if (nfc < 32)
 					V &= (1u << nfc) - 1u;
 				const bool v = (V >> lane) & 1u;
-				const bool probe = v && (length_mode || p >= st.skip_until);
+				const bool probe = v && (length_mode ||
+						p >= (seq_mode ? (int32_t)seq_probe_from(qs) : st.skip_until));
 				const unsigned r0 = reads;
 				const bool hit = probe && contains(F, win.h0[q], reads);
 				const uint32_t H = __ballot_sync(kFull, hit);
 				uint32_t alg = 0;
 				decided = length_mode
 						? length_chunk(ls, V, H, (int64_t)w0 + c, nfc, COUNT ? &alg : nullptr)
+						: seq_mode
+						? seq_chunk(qs, V, H, (int64_t)w0 + c, nfc, (int)k, a.streak_thr,
+								COUNT ? &alg : nullptr)
 						: simple_chunk(st, V, H, (int32_t)w0 + c, nfc, (int)k, (int)a.streak_thr,
 								COUNT ? &alg : nullptr);
 				if (COUNT && ((alg >> lane) & 1u))
@@ -124,7 +134,7 @@ enum { ORDER_PLAIN = 0, ORDER_READS = 1 };
  * ORDER_READS:   persistent; warps take reads from a counter, all filters each.
  * (The filter-major order is the two-pass path in twopass.cu.)
  */
-template <int SEG, int ORDER, bool COUNT, bool LENGTH_MODE>
+template <int SEG, int ORDER, bool COUNT, int MODE>
 __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
@@ -144,7 +154,7 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 			if (a.order)
 				r = a.order[r];
 			uint64_t myword = 0;
-			classify_read<SEG, COUNT, LENGTH_MODE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
+			classify_read<SEG, COUNT, MODE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
 					frame_acc, alg_acc);
 			const uint32_t mate = r >= a.n ? 1u : 0u;
 			if (lane < (int)a.words)
@@ -154,7 +164,7 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 		const uint64_t r = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp;
 		if (r < total) {
 			uint64_t myword = 0;
-			classify_read<SEG, COUNT, LENGTH_MODE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
+			classify_read<SEG, COUNT, MODE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
 					frame_acc, alg_acc);
 			const uint32_t mate = r >= a.n ? 1u : 0u;
 			if (lane < (int)a.words)
@@ -258,8 +268,10 @@ cudaError_t launch_one(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream
 {
 	const int threads = lc.warps_per_block * 32;
 	const size_t smem = classify_smem_bytes(lc, a.kmax);
-	auto kern = a.scoring == BBT_SCORE_LENGTH ? classify_kernel<SEG, ORDER, C, true>
-	                                          : classify_kernel<SEG, ORDER, C, false>;
+	auto kern = a.scoring == BBT_SCORE_LENGTH ? classify_kernel<SEG, ORDER, C, BBT_SCORE_LENGTH>
+	          : a.scoring == BBT_SCORE_HARMONIC ? classify_kernel<SEG, ORDER, C, BBT_SCORE_HARMONIC>
+	          : a.scoring == BBT_SCORE_BINOMIAL ? classify_kernel<SEG, ORDER, C, BBT_SCORE_BINOMIAL>
+	                                            : classify_kernel<SEG, ORDER, C, BBT_SCORE_SIMPLE>;
 	cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			(int)smem);
 	if (e != cudaSuccess)
@@ -329,6 +341,35 @@ cudaError_t launch_long_first(const ClassifyArgs &a, uint64_t long_bases, uint64
 	const uint64_t cap = (uint64_t)num_sms * 8;
 	long_first_kernel<<<(unsigned)(need < cap ? need : cap), 256, 0, s>>>(a, long_bases, order,
 			counters);
+	return cudaGetLastError();
+}
+
+/* Read lengths of a batch: out[0] = the largest, out[1 + L / 32] bit L % 32
+ * for each length L below 65536. */
+__global__ void length_set_kernel(const uint64_t *off0, const uint64_t *off1, uint64_t n,
+		uint32_t mates, unsigned int *out)
+{
+	for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n * mates;
+			r += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t *off = r >= n ? off1 : off0;
+		const uint64_t i = r >= n ? r - n : r;
+		const uint64_t l = off[i + 1] - off[i];
+		const unsigned int L = l > 0xFFFFFFFFull ? 0xFFFFFFFFu : (unsigned int)l;
+		atomicMax(out, L);
+		if (L < 65536u)
+			atomicOr(out + 1 + (L >> 5), 1u << (L & 31));
+	}
+}
+
+cudaError_t launch_length_set(const uint64_t *off0, const uint64_t *off1, uint64_t n,
+		uint32_t mates, unsigned int *out, int num_sms, cudaStream_t s)
+{
+	if (n == 0)
+		return cudaSuccess;
+	const uint64_t need = (n * mates + 255) / 256;
+	const uint64_t cap = (uint64_t)num_sms * 4;
+	length_set_kernel<<<(unsigned)(need < cap ? need : cap), 256, 0, s>>>(off0, off1, n, mates,
+			out);
 	return cudaGetLastError();
 }
 

@@ -33,6 +33,9 @@ struct ClassifyArgs {
 	unsigned long long *work;  /* persistent: next read to take (zeroed) */
 	const uint64_t *order;     /* persistent: optional order of the reads (a permutation
 	                              of [0, n * mates)); NULL = index order */
+	const uint32_t *bthres;    /* BINOMIAL: accept threshold of filter f for a read of
+	                              n frames at bthres[f * bthres_rows + n] */
+	uint64_t bthres_rows;
 	int tight_steps;           /* SIMPLE scoring: size probe steps by the frames that could
 	                              still accept the read (seqeval_chunk.cuh,
 	                              simple_step_frames) instead of 32 frames per step */
@@ -58,6 +61,11 @@ cudaError_t launch_classify(const ClassifyArgs &a, const LaunchConfig &lc, cudaS
  * specified; results do not depend on it).  counters: two zeroed words. */
 cudaError_t launch_long_first(const ClassifyArgs &a, uint64_t long_bases, uint64_t *order,
 		unsigned long long *counters, int num_sms, cudaStream_t s);
+
+/* Read lengths of a batch (BINOMIAL thresholds): out has 1 + 2048 words,
+ * zeroed; out[0] = the largest length, bit L of out[1..] for L < 65536. */
+cudaError_t launch_length_set(const uint64_t *off0, const uint64_t *off1, uint64_t n,
+		uint32_t mates, unsigned int *out, int num_sms, cudaStream_t s);
 
 /* Categories and summary counters for n reads (or pairs when h2 != NULL):
  * counts = aboveThreshold[nf+2], unique[nf+2], multiMatch, noMatch. */

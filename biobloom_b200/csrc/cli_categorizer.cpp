@@ -81,6 +81,7 @@ int main(int argc, char **argv)
 	bbt_params p;
 	bbt_default_params(&p);
 	string filters, prefix, read_status, postfix;
+	double binomial_score = 100; /* -s for binomial scoring, BioBloomCategorizer.cpp:168 */
 	bool paired = false, die = false, to_stdout = false, inverse = false;
 	int fastq = 0, fasta = 0, verbose = 0;
 	int device = 0;
@@ -123,8 +124,20 @@ int main(int argc, char **argv)
 		case 's': {
 			stringstream conv(optarg);
 			conv >> p.score;
+			binomial_score = p.score;
 			break;
 		}
+		case 'S':
+			if (strcmp(optarg, "harmonic") == 0) {
+				p.scoring = BBT_SCORE_HARMONIC;
+			} else if (strcmp(optarg, "binomial") == 0) {
+				p.scoring = BBT_SCORE_BINOMIAL;
+			} else {
+				cerr << "scoring method not recognized. Valid strings: harmonic or binomial"
+				     << endl;
+				die = true;
+			}
+			break;
 		case 'f': filters = optarg; break;
 		case 'p': prefix = optarg; break;
 		case 'h': usage_exit(EXIT_SUCCESS); break;
@@ -145,7 +158,7 @@ int main(int argc, char **argv)
 		case 'g': postfix = ".gz"; break;
 		case 'd': to_stdout = true; break;
 		case 'n': inverse = true; break;
-		case 'l': case 'c': case 'b': case 'w': case 'S':
+		case 'l': case 'c': case 'b': case 'w':
 		case 'D': case 'T': case 'W': case 'o':
 			unsupported += string(" -") + (char)c;
 			break;
@@ -194,18 +207,24 @@ int main(int argc, char **argv)
 		cerr << "Error: option(s)" << unsupported << " are not supported by this build" << endl;
 		exit(EXIT_FAILURE);
 	}
-	if (p.score < 0) {
-		cerr << "Error - s must be a positive integer or a floating point between 0 and 1."
-		     << endl;
-		exit(EXIT_FAILURE);
-	}
-	unsigned match_len = (unsigned)p.score;
-	if (match_len > 1) {
-		p.score = match_len;
-		p.scoring = BBT_SCORE_LENGTH;
-		cerr << "Min match length threshold: " << match_len << " bp" << endl;
+	if (p.scoring == BBT_SCORE_BINOMIAL) {
+		/* BioBloomCategorizer.cpp:418-421 */
+		p.score = pow(10.0, -(binomial_score / 10.0));
+		cerr << "FPR of a match: " << p.score << endl;
 	} else {
-		cerr << "Min score threshold: " << p.score << endl;
+		if (p.score < 0) {
+			cerr << "Error - s must be a positive integer or a floating point between 0 and 1."
+			     << endl;
+			exit(EXIT_FAILURE);
+		}
+		unsigned match_len = (unsigned)p.score;
+		if (match_len > 1) {
+			p.score = match_len;
+			p.scoring = BBT_SCORE_LENGTH;
+			cerr << "Min match length threshold: " << match_len << " bp" << endl;
+		} else {
+			cerr << "Min score threshold: " << p.score << endl;
+		}
 	}
 	if (prefix.find('/') != string::npos) {
 		struct stat sb;

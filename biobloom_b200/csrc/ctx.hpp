@@ -6,6 +6,7 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -62,6 +63,16 @@ struct bbt_ctx {
 	uint32_t *d_tp_vmask = nullptr;
 	uint64_t tp_frames_cap = 0;
 	bool same_k = true;
+	/* BINOMIAL scoring: each filter's FPR and the accept thresholds
+	 * calcMinCount(frames, fpr, score) by filter and frame count */
+	std::vector<double> fpr;
+	std::mutex bt_mu;
+	std::vector<uint32_t> h_bthres;  /* nf x bt_rows */
+	std::vector<uint8_t> bt_have;    /* by read length */
+	uint32_t *d_bthres = nullptr;
+	uint64_t bt_rows = 0;
+	unsigned int *d_lenset = nullptr;
+	bool capturing = false;          /* a CUDA graph is being captured */
 	/* -d / -n: print reads of the first filter (or all others) to stdout */
 	bool to_stdout = false, inverse = false;
 	/* long-first read order of the persistent kernel (0 = index order) */
@@ -88,6 +99,11 @@ struct BfScratch {
 	uint64_t order_cap = 0;
 };
 int bf_scratch_init(bbt_ctx *ctx, BfScratch &sc, uint64_t max_reads);
+/* BINOMIAL: allocate threshold rows for reads up to max_len bases up front
+ * (the serving engine, so that the table never moves under running kernels),
+ * and fill the rows of these reads (host offsets). */
+int bf_reserve_rows(bbt_ctx *ctx, uint64_t max_len);
+int bf_rows_for(bbt_ctx *ctx, const uint64_t *off, const uint64_t *off2, uint64_t n);
 void bf_scratch_free(BfScratch &sc);
 /* Classify n reads (n pairs when seq2) resident on the device, offsets
  * relative to seq / seq2, into hits (hits2) and category on stream s, adding to

@@ -98,6 +98,10 @@ extern "C" int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filter
 	}
 	if (scoring == BBT_SCORE_SIMPLE && (score < 0 || score > 1))
 		return fail(nullptr, BBT_ERR_ARG, "bbt_classify_noalloc: score must be in [0, 1] or an integer > 1");
+	if (scoring != BBT_SCORE_SIMPLE && scoring != BBT_SCORE_LENGTH)
+		return fail(nullptr, BBT_ERR_UNSUPPORTED,
+				"bbt_classify_noalloc: simple or length scoring only (harmonic and binomial "
+				"thresholds live in context memory)");
 	FilterDev table[BBT_NOALLOC_MAX_FILTERS];
 	uint32_t kmax = 0;
 	for (int i = 0; i < n_filters; ++i) {

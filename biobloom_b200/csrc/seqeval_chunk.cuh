@@ -28,6 +28,7 @@
 #ifndef BBT_SEQEVAL_CHUNK_CUH
 #define BBT_SEQEVAL_CHUNK_CUH
 
+#include <math.h>
 #include <stdint.h>
 
 #if defined(__CUDACC__)
@@ -498,6 +499,154 @@ BBT_HD int length_chunk(LengthState &s, uint32_t V, uint32_t H, int64_t base,
 			return s.decided;
 		}
 		s.prev = pos;
+	}
+	return s.decided;
+}
+
+/*
+ * HARMONIC and BINOMIAL scoring (SeqEval.h:116-193, 218-290): the walk of
+ * evalSimple with a score kept in double (HARMONIC: a hit in a streak of s
+ * earlier hits adds 1 - 1/(1 + s), a streak's first hit 0.5; BINOMIAL: every
+ * hit adds 1 against an integer threshold).  The running score of HARMONIC is
+ * a sum of doubles whose rounding depends on the order of the additions, so a
+ * chunk is walked frame by frame, exactly as the reference iterates; every
+ * lane runs the same walk on the chunk's ballots.
+ */
+enum { SEQ_HARMONIC = 2, SEQ_BINOMIAL = 3 };
+
+struct SeqState {
+	double score;
+	double thres;        /* accept when thres <= score */
+	double anti_thres;   /* reject when anti_thres <= anti */
+	uint32_t anti;
+	uint32_t streak;
+	int64_t prev;        /* last iterated frame */
+	int64_t skip_end;    /* frames below this belong to an open skip window */
+	int32_t started;
+	int32_t in_skip;
+	int32_t mode;        /* SEQ_HARMONIC or SEQ_BINOMIAL */
+	int32_t decided;
+};
+
+/* thres / antiThres of HARMONIC (as evalSimple computes them). */
+BBT_HD void harmonic_init(SeqState &s, double threshold, double one_minus, uint64_t frames)
+{
+	double fr = (double)frames;
+	double thres = threshold * fr;
+	double anti = one_minus * fr;
+#if defined(__CUDA_ARCH__)
+	thres = __dmul_rn(threshold, fr);
+	anti = __dmul_rn(one_minus, fr);
+#endif
+	s.score = 0.0;
+	s.thres = thres;
+	s.anti_thres = floor(anti);
+	s.anti = 0;
+	s.streak = 0;
+	s.prev = 0;
+	s.skip_end = 0;
+	s.started = 0;
+	s.in_skip = 0;
+	s.mode = SEQ_HARMONIC;
+	s.decided = EVAL_OPEN;
+}
+
+/* BINOMIAL: thres = calcMinCount(frameLen, fpr, minFPR), computed on the host. */
+BBT_HD void binomial_init(SeqState &s, uint32_t thres, uint32_t frame_len)
+{
+	s.score = 0.0;
+	s.thres = (double)thres;
+	s.anti_thres = (double)(uint32_t)(frame_len - thres); /* unsigned, as upstream */
+	s.anti = 0;
+	s.streak = 0;
+	s.prev = 0;
+	s.skip_end = 0;
+	s.started = 0;
+	s.in_skip = 0;
+	s.mode = SEQ_BINOMIAL;
+	s.decided = EVAL_OPEN;
+}
+
+/* Frames below this are not probed (an open skip window). */
+BBT_HD int64_t seq_probe_from(const SeqState &s)
+{
+	return s.in_skip ? s.skip_end : 0;
+}
+
+BBT_HD double harmonic_add(double score, uint32_t streak)
+{
+#if defined(__CUDA_ARCH__)
+	if (streak == 0)
+		return __dadd_rn(score, 0.5);
+	return __dadd_rn(score, __dsub_rn(1.0, __ddiv_rn(1.0, __dadd_rn(1.0, (double)streak))));
+#else
+	if (streak == 0)
+		return score + 0.5;
+	return score + (1.0 - 1.0 / (1.0 + (double)streak));
+#endif
+}
+
+/* Walk the valid frames of one chunk (frame j = base + j, j < nf); H holds the
+ * hits of the frames probed (those at or after seq_probe_from when the chunk
+ * began).  alg receives the frames the reference probes. */
+BBT_HD int seq_chunk(SeqState &s, uint32_t V, uint32_t H, int64_t base, int nf, int k,
+		uint32_t streak_thr, uint32_t *alg = nullptr)
+{
+	if (s.decided)
+		return s.decided;
+	V &= low_mask(nf);
+	uint32_t x = V;
+	while (x) {
+		const int q = lowbit32(x);
+		x &= x - 1;
+		const int64_t p = base + q;
+		if (s.in_skip && p < s.skip_end) { /* iterated inside a skip window, not probed */
+			if (s.anti_thres <= (double)(++s.anti))
+				return s.decided = EVAL_REJECT;
+			s.prev = p;
+			continue;
+		}
+		s.in_skip = 0;
+		const bool hit = (H >> q) & 1u;
+		if (!s.started) { /* the first frame: no gap check, no skip window */
+			s.started = 1;
+			if (alg)
+				*alg |= 1u << q;
+			if (hit) {
+				s.score = s.mode == SEQ_BINOMIAL ? s.score + 1.0 : harmonic_add(s.score, 0);
+				if (s.thres <= s.score)
+					return s.decided = EVAL_ACCEPT;
+				++s.streak;
+			} else if (s.anti_thres <= (double)(++s.anti)) {
+				return s.decided = EVAL_REJECT;
+			}
+			s.prev = p;
+			continue;
+		}
+		if (p != s.prev + 1) {
+			s.anti += (uint32_t)(p - s.prev - 1);
+			if (s.anti_thres <= (double)s.anti)
+				return s.decided = EVAL_REJECT;
+			s.streak = 0;
+		}
+		if (alg) /* the reference probes the frame only after the gap check */
+			*alg |= 1u << q;
+		if (hit) {
+			s.score = s.mode == SEQ_BINOMIAL ? s.score + 1.0 : harmonic_add(s.score, s.streak);
+			if (s.thres <= s.score)
+				return s.decided = EVAL_ACCEPT;
+			s.prev = p;
+			++s.streak;
+		} else {
+			if (s.streak >= streak_thr) { /* the window starts at this frame */
+				s.in_skip = 1;
+				s.skip_end = (int64_t)(uint32_t)((uint32_t)p + (uint32_t)k);
+			}
+			if (s.anti_thres <= (double)(++s.anti))
+				return s.decided = EVAL_REJECT;
+			s.prev = p;
+			s.streak = 0;
+		}
 	}
 	return s.decided;
 }

@@ -221,6 +221,9 @@ int run_chunk(bbt_server *srv, ServeSlot &sl, Req &q, char *base, uint64_t i0, u
 		uint64_t *dh = (uint64_t *)(base + L.out[0]);
 		uint64_t *dh2 = paired ? (uint64_t *)(base + L.out[1]) : nullptr;
 		uint32_t *dc = (uint32_t *)(base + L.out[2]);
+		rc = bf_rows_for(srv->bf, sl.h_off, paired ? sl.h_off + srv->p.chunk_reads + 1 : nullptr, c);
+		if (rc)
+			return rc;
 		rc = bf_classify_slot(srv->bf, dseq[0], doff[0], dseq[1], doff[1], c, dh, dh2, dc, s,
 				sl.bf);
 		if (rc)
@@ -389,6 +392,8 @@ extern "C" int bbt_server_create(bbt_ctx *bloom, bbt_mibf *mibf, const bbt_serve
 	};
 	if (cudaSetDevice(srv->dev) != cudaSuccess)
 		return bail(BBT_ERR_CUDA, "cudaSetDevice failed");
+	if (bloom && bf_reserve_rows(bloom, (uint64_t)srv->p.max_frames + bloom->kmax))
+		return bail(BBT_ERR_NOMEM, "cannot reserve the binomial threshold rows: " + bloom->err);
 	if (mibf && mibf_reserve_rows(mibf, srv->p.max_frames + 1))
 		return bail(BBT_ERR_NOMEM, "cannot reserve the miBF minCount rows: " + mibf->err);
 	size_t free_b = 0, total_b = 0;

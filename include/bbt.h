@@ -42,6 +42,9 @@ extern "C" {
 /* ---- scoring methods (opt::ScoringMethod, Common/Options.h:75) ---- */
 #define BBT_SCORE_SIMPLE 0
 #define BBT_SCORE_LENGTH 1
+#define BBT_SCORE_HARMONIC 2   /* -S harmonic: score in [0, 1] */
+#define BBT_SCORE_BINOMIAL 3   /* -S binomial: score = minimum FPR of a match,
+                                  10^(-s/10) (BioBloomCategorizer.cpp:418-420) */
 
 /* ---- where batch buffers live ---- */
 #define BBT_HOST 0

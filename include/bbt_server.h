@@ -40,7 +40,7 @@ typedef struct {
 	uint64_t mem_budget;     /* device bytes for requests in flight; 0 = 40% of free HBM */
 	uint32_t slots;          /* requests in flight at once; 0 = 4 */
 	uint64_t chunk_reads;    /* reads per launch inside a request; 0 = 1M */
-	uint32_t max_frames;     /* longest read (frames) a miBF request may hold; 0 = 16384 */
+	uint32_t max_frames;     /* longest read (frames) a request may hold; 0 = 16384 */
 } bbt_server_params;
 
 /* One request: host reads (pairs when seq2 != NULL) and host result arrays,

@@ -45,6 +45,36 @@ static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
 		hit[it.pos] = (uint8_t)oracle_bf_contains(bf, it.hv, &c);
 		cost[it.pos] = (uint32_t)c;
 	}
+	if (scoring == ORACLE_HARMONIC || scoring == ORACLE_BINOMIAL) {
+		/* the kernel's 32-frame steps over the sequential walk */
+		bbt::SeqState qs;
+		if (scoring == ORACLE_HARMONIC)
+			bbt::harmonic_init(qs, threshold, 1.0 - threshold, frames);
+		else
+			bbt::binomial_init(qs, oracle_calc_min_count((unsigned)frames, oracle_bf_fpr(bf),
+					threshold), (uint32_t)frames);
+		for (uint64_t base = 0; base < frames; base += 32) {
+			const int nf = frames - base >= 32 ? 32 : (int)(frames - base);
+			const int64_t from = bbt::seq_probe_from(qs);
+			uint32_t V = 0, H = 0;
+			for (int j = 0; j < nf; ++j) {
+				const uint64_t p = base + j;
+				if (!valid[p])
+					continue;
+				V |= 1u << j;
+				if ((int64_t)p >= from && hit[p])
+					H |= 1u << j;
+			}
+			uint32_t alg = 0;
+			const int d = bbt::seq_chunk(qs, V, H, (int64_t)base, nf, (int)k, streak_thr, &alg);
+			for (int j = 0; j < nf; ++j)
+				if ((alg >> j) & 1u)
+					*alg_probes += cost[base + j];
+			if (d)
+				return d == bbt::EVAL_ACCEPT;
+		}
+		return 0;
+	}
 	bbt::SimpleState ss;
 	bbt::LengthState ls;
 	if (scoring == ORACLE_LENGTH)

@@ -66,6 +66,12 @@ def lib():
                                         ctypes.c_char_p, u64, u64, dbl, u64, dbl]
         L.oracle_eval_simple.argtypes = [ctypes.c_char_p, sz, P(_BF), dbl, u32, P(u64)]
         L.oracle_eval_min_match_len.argtypes = [ctypes.c_char_p, sz, P(_BF), u32, P(u64)]
+        L.oracle_eval_harmonic.argtypes = [ctypes.c_char_p, sz, P(_BF), dbl, u32, P(u64)]
+        L.oracle_eval_binomial.argtypes = [ctypes.c_char_p, sz, P(_BF), dbl, dbl, u32, P(u64)]
+        L.oracle_bf_fpr.restype = dbl
+        L.oracle_bf_fpr.argtypes = [P(_BF)]
+        L.oracle_calc_min_count.restype = u32
+        L.oracle_calc_min_count.argtypes = [u32, dbl, dbl]
         L.oracle_classify.argtypes = [ctypes.c_char_p, P(u64), sz, P(P(_BF)), u32, dbl, u32,
                                       ctypes.c_int, P(u64), P(u64)]
         L.oracle_update_summary.restype = u32

@@ -73,3 +73,52 @@ def test_chunk_model_matches_oracle(model, seed):
             if a != m_ or c1.value != c2.value:
                 mism += 1
     assert mism == 0
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_sequential_walk_matches_oracle_harmonic_binomial(model, seed):
+    """HARMONIC and BINOMIAL: the chunked sequential walk (seq_chunk) gives the
+    oracle's decision and algorithmic probe count."""
+    rng = np.random.default_rng(100 + seed)
+    L = ol.lib()
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    mism = 0
+    for trial in range(30):
+        h = int(rng.integers(1, 5))
+        k = max(h, int(rng.integers(3, 40)))
+        f = ol.Filter.create(64 * int(rng.integers(1, 60)), h, k)
+        g = rng.choice(acgt, 3000)
+        fill = rng.random()
+        for p, hv in ol.kmers(g.tobytes(), h, k):
+            if rng.random() < fill:
+                L.oracle_bf_insert(ctypes.byref(f.bf), (ctypes.c_uint64 * 64)(*hv))
+        fpr = L.oracle_bf_fpr(ctypes.byref(f.bf))
+        for r in range(50):
+            n = int(rng.integers(0, 500))
+            st = int(rng.integers(0, 2500))
+            s = g[st:st + n].copy() if rng.random() < 0.6 else rng.choice(acgt, n)
+            s = s[:n]
+            m = rng.random(len(s)) < rng.random() * 0.05
+            s[m] = rng.choice(acgt, m.sum())
+            if rng.random() < 0.3:
+                m = rng.random(len(s)) < rng.random() * 0.2
+                s[m] = ord("N")
+            b = s.tobytes()
+            streak = int(rng.integers(0, 6))
+            c1 = ctypes.c_uint64(0)
+            c2 = ctypes.c_uint64(0)
+            if rng.random() < 0.5:
+                thr = float(rng.random())
+                a = L.oracle_eval_harmonic(b, len(b), ctypes.byref(f.bf), thr, streak,
+                                           ctypes.byref(c1))
+                mode = ol.HARMONIC
+            else:
+                thr = 10.0 ** (-float(rng.uniform(1, 100)) / 10.0)
+                a = L.oracle_eval_binomial(b, len(b), ctypes.byref(f.bf), thr, fpr, streak,
+                                           ctypes.byref(c1))
+                mode = ol.BINOMIAL
+            m_ = model.model_eval(b, len(b), ctypes.byref(f.bf), thr, streak, mode,
+                                  ctypes.byref(c2))
+            if a != m_ or c1.value != c2.value:
+                mism += 1
+    assert mism == 0
