@@ -6,9 +6,10 @@ biobloommicategorizer CLIs over it; this package holds the Python mirrors of
 the reference's BioBloomClassifier and MIBFClassifier interfaces and the
 workload generators used by tests and the benchmark.
 """
-from ._lib import BBTError, LibraryMissing, lib  # noqa: F401
+from ._lib import (MODE_BESTHIT, MODE_ORDERED, MODE_SCORES, MODE_STD, BBTError,  # noqa: F401
+                   LibraryMissing, lib)
 from .classifier import BioBloomClassifier, pack  # noqa: F401
 from .mibf import MIBFClassifier, make_mibf  # noqa: F401
 
 __all__ = ["BioBloomClassifier", "MIBFClassifier", "BBTError", "LibraryMissing", "lib", "pack",
-           "make_mibf"]
+           "make_mibf", "MODE_STD", "MODE_ORDERED", "MODE_BESTHIT", "MODE_SCORES"]

@@ -19,6 +19,7 @@ MIBF_LAYOUT_AUTO, MIBF_LAYOUT_RANK, MIBF_LAYOUT_DENSE = 0, 1, 2
 SCORE_SIMPLE, SCORE_LENGTH, SCORE_HARMONIC, SCORE_BINOMIAL = 0, 1, 2, 3
 HOST, DEVICE = 0, 1
 PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT, PATH_FILTER_MAJOR = 0, 1, 2, 3
+MODE_STD, MODE_ORDERED, MODE_BESTHIT, MODE_SCORES = 0, 1, 2, 3
 
 
 class LibraryMissing(RuntimeError):
@@ -151,6 +152,14 @@ def lib():
         "bbt_summary_tsv": (i32, [vp, ctypes.c_char_p, ctypes.c_size_t, P(ctypes.c_size_t)]),
         "bbt_filter_files": (i32, [vp, P(cp), i32, cp, cp]),
         "bbt_filter_pair_files": (i32, [vp, cp, cp, cp, cp]),
+        "bbt_filter_files_print": (i32, [vp, P(cp), i32, cp, cp, cp, cp]),
+        "bbt_filter_pair_files_print": (i32, [vp, cp, cp, cp, cp, cp, cp]),
+        "bbt_filter_pair_file_lists": (i32, [vp, P(cp), P(cp), i32, cp, cp]),
+        "bbt_filter_smart_pairs": (i32, [vp, cp, cp, cp]),
+        "bbt_filter_smart_pairs_print": (i32, [vp, cp, cp, cp, cp, cp]),
+        "bbt_set_stdout": (i32, [vp, i32, i32]),
+        "bbt_set_mode": (i32, [vp, i32]),
+        "bbt_classify_batch_scores": (i32, [vp, P(Batch), P(Result), vp, vp, vp]),
         "bbt_last_stats": (i32, [vp, P(Stats)]),
         "bbt_set_counting": (i32, [vp, i32]),
         "bbt_set_launch": (i32, [vp, i32, i32, i32]),

@@ -4,7 +4,8 @@ over the C ABI of libbbt.so.
     bbc = BioBloomClassifier(["a.bf", "b.bf"], 0.15, "out")
     bbc.filter(["reads.fq"])                 # writes out_summary.tsv
     bbc.filterPair("r1.fq", "r2.fq")         # paired (intersection of mates)
-    hits, cats = bbc.classify([b"ACGT...", ...])  # in-memory batch
+    bbc.filterPrint(["reads.fq"], "fq")      # also out_<filter>.fq per category
+    hits, hits2, cats = bbc.classify([b"ACGT...", ...])  # in-memory batch
 
 Every call goes through the CUDA path; there is no CPU fallback.
 """
@@ -71,6 +72,7 @@ class BioBloomClassifier:
         self.words = (self.n_filters + 63) // 64
         self.filter_ids = [lib.bbt_filter_id(ctx, i).decode() for i in range(self.n_filters)]
         self._inclusive = False
+        self.mode = L.MODE_STD
 
     # -- reference-style configuration -------------------------------------
     def setInclusive(self):
@@ -80,7 +82,24 @@ class BioBloomClassifier:
         self._inclusive = True
 
     def setOrderedFilter(self):
-        raise L.BBTError(-6, "ordered filtering (-c) is not implemented on the GPU path")
+        """-c: only the first filter (in load order) that a read passes counts;
+        BioBloomClassifier::setOrderedFilter (BioBloomClassifier.h:67-75),
+        which refuses best-hit mode."""
+        if self.mode == L.MODE_BESTHIT:
+            raise L.BBTError(-1,
+                             "Best Hit mode and Ordered mode detected. Not yet supported.")
+        self.set_mode(L.MODE_ORDERED)
+
+    def setStdout(self, inverse=False):
+        """-d (-n): the file pipelines print the first filter's reads (all
+        others) to stdout; BioBloomClassifier::setStdout (BioBloomClassifier.h:81-83)."""
+        L.check(L.lib().bbt_set_stdout(self._ctx, 1, int(bool(inverse))), self._ctx)
+
+    def set_mode(self, mode):
+        """opt::mode: MODE_STD, MODE_ORDERED (-c), MODE_BESTHIT (-b) or
+        MODE_SCORES (-w)."""
+        L.check(L.lib().bbt_set_mode(self._ctx, int(mode)), self._ctx)
+        self.mode = int(mode)
 
     def set_launch(self, path=0, warps_per_block=0, frames_per_lane=0):
         L.check(L.lib().bbt_set_launch(self._ctx, path, warps_per_block, frames_per_lane),
@@ -128,11 +147,56 @@ class BioBloomClassifier:
                                               read_status.encode() if read_status else None),
                 self._ctx)
 
+    def filterPrint(self, input_files, output_type, read_status=None):
+        """Also write each read to "<prefix>_<category>.<output_type><postfix>"
+        (output_type "fa" or "fq"); BioBloomClassifier::filterPrint."""
+        files = [str(f).encode() for f in input_files]
+        arr = (ctypes.c_char_p * len(files))(*files)
+        L.check(L.lib().bbt_filter_files_print(self._ctx, arr, len(files), self.prefix.encode(),
+                                                output_type.encode(), self.postfix.encode(),
+                                                read_status.encode() if read_status else None),
+                self._ctx)
+
+    def filterPairPrint(self, file1, file2, output_type=None, read_status=None):
+        """filterPairPrint(file1, file2, type), or filterPairPrint(file, type)
+        for one file of name-matched mates when output_type is None."""
+        if output_type is None:
+            L.check(L.lib().bbt_filter_smart_pairs_print(
+                self._ctx, str(file1).encode(), self.prefix.encode(), str(file2).encode(),
+                self.postfix.encode(), read_status.encode() if read_status else None), self._ctx)
+            return
+        L.check(L.lib().bbt_filter_pair_files_print(
+            self._ctx, str(file1).encode(), str(file2).encode(), self.prefix.encode(),
+            output_type.encode(), self.postfix.encode(),
+            read_status.encode() if read_status else None), self._ctx)
+
+    def filterSmartPair(self, file, read_status=None):
+        """filterPair(file): mates matched by name in one file
+        (BioBloomClassifier.cpp:463-564)."""
+        L.check(L.lib().bbt_filter_smart_pairs(self._ctx, str(file).encode(),
+                                               self.prefix.encode(),
+                                               read_status.encode() if read_status else None),
+                self._ctx)
+
+    def filterPairList(self, files1, files2, read_status=None):
+        """filterPair(vector, vector): file i of files2 holds the mates of file
+        i of files1 (BioBloomClassifier.cpp:731-806)."""
+        if len(files1) != len(files2):
+            raise ValueError("file lists differ in length")
+        a = (ctypes.c_char_p * len(files1))(*[str(f).encode() for f in files1])
+        b = (ctypes.c_char_p * len(files2))(*[str(f).encode() for f in files2])
+        L.check(L.lib().bbt_filter_pair_file_lists(self._ctx, a, b, len(files1),
+                                                   self.prefix.encode(),
+                                                   read_status.encode() if read_status else None),
+                self._ctx)
+
     # -- in-memory batches ---------------------------------------------------
-    def classify(self, reads, reads2=None):
+    def classify(self, reads, reads2=None, scores=False):
         """Classify host reads (list of bytes or (uint8 array, uint64 offsets)).
         Returns (hits, hits2, category) as numpy arrays; hits2 is None for
-        single-end input."""
+        single-end input.  scores=True also returns SeqEval::evalScore of
+        every read against every filter: (hits, hits2, category, scores,
+        scores2), scores n x n_filters float64."""
         seq, off = pack(reads) if isinstance(reads, list) else reads
         seq = np.ascontiguousarray(seq, dtype=np.uint8)
         off = np.ascontiguousarray(off, dtype=np.uint64)
@@ -153,15 +217,23 @@ class BioBloomClassifier:
             b.seq2, b.offsets2 = _ptr(seq2), _ptr(off2)
             hits2 = np.zeros((n, self.words), dtype=np.uint64)
             r.hits2 = _ptr(hits2)
+        if scores:
+            sc = np.zeros((n, self.n_filters), dtype=np.float64)
+            sc2 = np.zeros((n, self.n_filters), dtype=np.float64) if reads2 is not None else None
+            L.check(L.lib().bbt_classify_batch_scores(
+                self._ctx, ctypes.byref(b), ctypes.byref(r), _ptr(sc),
+                _ptr(sc2) if sc2 is not None else None, None), self._ctx)
+            return hits, hits2, cat, sc, sc2
         L.check(L.lib().bbt_classify_batch(self._ctx, ctypes.byref(b), ctypes.byref(r), None),
                 self._ctx)
         return hits, hits2, cat
 
     def classify_device(self, seq, off, seq2=None, off2=None, hits=None, hits2=None,
-                        category=None, stream=None):
+                        category=None, stream=None, scores=None, scores2=None):
         """Classify reads resident on the GPU (torch uint8 / int64 tensors).
         Enqueued on `stream` (a torch.cuda.Stream, default: the current
-        stream); returns (hits, hits2, category) tensors."""
+        stream); returns (hits, hits2, category) tensors.  scores / scores2
+        (float64 tensors of n x n_filters, optional) receive evalScore."""
         import torch
         n = off.numel() - 1
         dev = seq.device
@@ -179,6 +251,12 @@ class BioBloomClassifier:
             b.seq2, b.offsets2 = seq2.data_ptr(), off2.data_ptr()
             r.hits2 = hits2.data_ptr()
         s = stream if stream is not None else torch.cuda.current_stream(dev)
+        if scores is not None:
+            L.check(L.lib().bbt_classify_batch_scores(
+                self._ctx, ctypes.byref(b), ctypes.byref(r), ctypes.c_void_p(scores.data_ptr()),
+                ctypes.c_void_p(scores2.data_ptr()) if scores2 is not None else None,
+                ctypes.c_void_p(s.cuda_stream)), self._ctx)
+            return hits, hits2, category
         L.check(L.lib().bbt_classify_batch(self._ctx, ctypes.byref(b), ctypes.byref(r),
                                            ctypes.c_void_p(s.cuda_stream)), self._ctx)
         return hits, hits2, category

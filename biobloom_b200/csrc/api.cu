@@ -108,10 +108,13 @@ static void free_slot(Slot &s)
 		cudaFree(s.d_seq[m]);
 		cudaFree(s.d_off[m]);
 		cudaFree(s.d_hits[m]);
+		cudaFree(s.d_scores[m]);
 		s.d_seq[m] = nullptr;
 		s.d_off[m] = nullptr;
 		s.d_hits[m] = nullptr;
+		s.d_scores[m] = nullptr;
 	}
+	s.scores_cap = 0;
 	cudaFree(s.d_cat);
 	s.d_cat = nullptr;
 }
@@ -130,6 +133,7 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 	for (uint32_t *w : ctx->d_words)
 		cudaFree(w);
 	cudaFree(ctx->d_filters);
+	cudaFree(ctx->d_fpr);
 	cudaFree(ctx->d_counts);
 	cudaFree(ctx->d_work);
 	cudaFree(ctx->d_order);
@@ -390,6 +394,9 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 	ctx->words = (ctx->nf + 63) / 64;
 	OPEN_TRY(cudaMalloc(&ctx->d_filters, sizeof(FilterDev) * ctx->nf));
 	OPEN_TRY(cudaMemcpy(ctx->d_filters, ctx->hf.data(), sizeof(FilterDev) * ctx->nf,
+			cudaMemcpyHostToDevice));
+	OPEN_TRY(cudaMalloc(&ctx->d_fpr, sizeof(double) * ctx->nf));
+	OPEN_TRY(cudaMemcpy(ctx->d_fpr, ctx->fpr.data(), sizeof(double) * ctx->nf,
 			cudaMemcpyHostToDevice));
 	OPEN_TRY(cudaMalloc(&ctx->d_counts, sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
 	OPEN_TRY(cudaMemset(ctx->d_counts, 0, sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
@@ -663,14 +670,26 @@ static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 	return BBT_OK;
 }
 
-/* classify + summarize one staged or device-resident batch on stream s */
-static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStream_t s)
+/* classify + summarize one staged or device-resident batch on stream s;
+ * scores (optional, per mate array): evalScore of every filter */
+static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStream_t s,
+		double *const *scores = nullptr)
 {
 	ctx->last.kernels = 2; /* classification (counted below for two-pass) + summary */
+	ScoreArgs sa;
+	sa.scores[0] = scores ? scores[0] : nullptr;
+	sa.scores[1] = scores && a.mates == 2 ? scores[1] : nullptr;
+	sa.fpr = ctx->d_fpr;
+	sa.besthit = 0;
+	const bool want_scores = sa.scores[0] || sa.scores[1];
 	const bool two_pass = ctx->lc.path == BBT_PATH_FILTER_MAJOR && ctx->same_k &&
 			ctx->p.scoring <= BBT_SCORE_LENGTH;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k0, s));
-	if (two_pass) {
+	if (ctx->mode == BBT_MODE_BESTHIT) {
+		/* the hit words are the filters of the largest score */
+		sa.besthit = 1;
+		CUDA_TRY(ctx, launch_scores(a, sa, ctx->lc, s));
+	} else if (two_pass) {
 		/* accepted (filter, read) items OR their bit into zeroed words */
 		const size_t hb = a.n * ctx->words * sizeof(uint64_t);
 		CUDA_TRY(ctx, cudaMemsetAsync(a.hits[0], 0, hb, s));
@@ -698,9 +717,14 @@ static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStrea
 		}
 		CUDA_TRY(ctx, launch_classify(a, lc, s));
 	}
+	if (want_scores && ctx->mode != BBT_MODE_BESTHIT) {
+		CUDA_TRY(ctx, launch_scores(a, sa, ctx->lc, s));
+		ctx->last.kernels += 1;
+	}
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k1, s));
 	CUDA_TRY(ctx, launch_summarize(a.hits[0], a.mates == 2 ? a.hits[1] : nullptr, a.n, ctx->nf,
-			ctx->words, ctx->p.inclusive, d_cat, ctx->d_counts, ctx->num_sms, s));
+			ctx->words, ctx->p.inclusive, ctx->mode == BBT_MODE_ORDERED, d_cat, ctx->d_counts,
+			ctx->num_sms, s));
 	return BBT_OK;
 }
 
@@ -718,10 +742,12 @@ static int ensure_tmp_hits(bbt_ctx *ctx, uint64_t n)
 	return BBT_OK;
 }
 
-static int classify_device(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r, cudaStream_t s)
+static int classify_device(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r, cudaStream_t s,
+		double *const *scores = nullptr)
 {
 	const bool paired = b->seq2 != nullptr;
-	if (ctx->p.scoring == BBT_SCORE_BINOMIAL && !ctx->capturing) {
+	if (ctx->p.scoring == BBT_SCORE_BINOMIAL && ctx->mode != BBT_MODE_BESTHIT &&
+			!ctx->capturing) {
 		/* the thresholds of the batch's read lengths (a short host wait) */
 		std::vector<uint64_t> lens;
 		int rc = device_lengths(ctx, b, s, lens);
@@ -745,7 +771,7 @@ static int classify_device(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r, cuda
 	a.hits[0] = r->hits ? r->hits : ctx->d_tmp_hits[0];
 	a.hits[1] = paired ? (r->hits2 ? r->hits2 : ctx->d_tmp_hits[1]) : nullptr;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, s));
-	int rc = run_kernels(ctx, a, r->category, s);
+	int rc = run_kernels(ctx, a, r->category, s, scores);
 	if (rc)
 		return rc;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, s));
@@ -757,11 +783,29 @@ static int classify_device(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r, cuda
 /* Host batches: split into sub-batches that fit the staging slots; copies in
  * (h2d stream), kernels (ctx->stream) and copies out (d2h stream) of
  * consecutive sub-batches overlap, two slots deep. */
-static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r)
+static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
+		double *const *scores = nullptr)
 {
 	const bool paired = b->seq2 != nullptr;
 	const uint64_t n = b->n_reads;
-	if (ctx->p.scoring == BBT_SCORE_BINOMIAL) {
+	const bool want_scores = scores && (scores[0] || (paired && scores[1]));
+	if (want_scores) {
+		/* per-slot score arrays of cap_reads reads */
+		for (Slot &sl : ctx->slot) {
+			if (sl.scores_cap >= ctx->cap_reads)
+				continue;
+			for (int m = 0; m < 2; ++m) {
+				cudaFree(sl.d_scores[m]);
+				sl.d_scores[m] = nullptr;
+			}
+			sl.scores_cap = 0;
+			for (int m = 0; m < 2; ++m)
+				CUDA_TRY(ctx, cudaMalloc(&sl.d_scores[m],
+						ctx->cap_reads * ctx->nf * sizeof(double)));
+			sl.scores_cap = ctx->cap_reads;
+		}
+	}
+	if (ctx->p.scoring == BBT_SCORE_BINOMIAL && ctx->mode != BBT_MODE_BESTHIT) {
 		int rc = ensure_bthres(ctx, host_lengths(b->offsets, paired ? b->offsets2 : nullptr, n));
 		if (rc)
 			return rc;
@@ -833,7 +877,12 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r)
 		}
 		CUDA_TRY(ctx, cudaEventRecord(s.copied, ctx->h2d));
 		CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->stream, s.copied, 0));
-		int rc = run_kernels(ctx, a, s.d_cat, ctx->stream);
+		double *slot_scores[2] = {nullptr, nullptr};
+		if (want_scores) {
+			slot_scores[0] = scores[0] ? s.d_scores[0] : nullptr;
+			slot_scores[1] = paired && scores[1] ? s.d_scores[1] : nullptr;
+		}
+		int rc = run_kernels(ctx, a, s.d_cat, ctx->stream, want_scores ? slot_scores : nullptr);
 		if (rc)
 			return rc;
 		CUDA_TRY(ctx, cudaEventRecord(s.computed, ctx->stream));
@@ -848,6 +897,10 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r)
 		if (r->category)
 			CUDA_TRY(ctx, cudaMemcpyAsync(r->category + i0, s.d_cat, cnt * sizeof(uint32_t),
 					cudaMemcpyDeviceToHost, ctx->d2h));
+		for (int m = 0; m < 2; ++m)
+			if (slot_scores[m])
+				CUDA_TRY(ctx, cudaMemcpyAsync(scores[m] + i0 * ctx->nf, slot_scores[m],
+						cnt * ctx->nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->d2h));
 		CUDA_TRY(ctx, cudaEventRecord(s.done, ctx->d2h));
 		s.used = true;
 		which ^= 1;
@@ -863,25 +916,51 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r)
 	return BBT_OK;
 }
 
-extern "C" int bbt_classify_batch(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *result,
-		void *stream)
+static int classify_batch(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *result,
+		void *stream, double *const *scores, const char *who)
 {
 	if (!ctx || !batch || !result)
-		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch: null argument");
+		return fail(ctx, BBT_ERR_ARG, std::string(who) + ": null argument");
 	if (batch->n_reads == 0)
 		return BBT_OK;
 	if (!batch->seq || !batch->offsets || (batch->seq2 && !batch->offsets2))
-		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch: missing sequence or offsets");
+		return fail(ctx, BBT_ERR_ARG, std::string(who) + ": missing sequence or offsets");
 	if (batch->location != result->location)
-		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch: batch and result must both be host or both device");
+		return fail(ctx, BBT_ERR_ARG,
+				std::string(who) + ": batch and result must both be host or both device");
 	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
 	if (batch->location == BBT_DEVICE) {
 		cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-		return classify_device(ctx, batch, result, s);
+		return classify_device(ctx, batch, result, s, scores);
 	}
 	if (batch->location != BBT_HOST)
-		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch: location must be BBT_HOST or BBT_DEVICE");
-	return classify_host(ctx, batch, result);
+		return fail(ctx, BBT_ERR_ARG, std::string(who) + ": location must be BBT_HOST or BBT_DEVICE");
+	return classify_host(ctx, batch, result, scores);
+}
+
+extern "C" int bbt_classify_batch(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *result,
+		void *stream)
+{
+	return classify_batch(ctx, batch, result, stream, nullptr, "bbt_classify_batch");
+}
+
+extern "C" int bbt_classify_batch_scores(bbt_ctx *ctx, const bbt_batch *batch,
+		bbt_result *result, double *scores, double *scores2, void *stream)
+{
+	if (ctx && batch && batch->seq2 && scores2 == nullptr && scores != nullptr)
+		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch_scores: pairs need scores2 too");
+	double *sc[2] = {scores, batch && batch->seq2 ? scores2 : nullptr};
+	return classify_batch(ctx, batch, result, stream, sc, "bbt_classify_batch_scores");
+}
+
+extern "C" int bbt_set_mode(bbt_ctx *ctx, int mode)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	if (mode < BBT_MODE_STD || mode > BBT_MODE_SCORES)
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_mode: unknown mode");
+	ctx->mode = mode;
+	return BBT_OK;
 }
 
 extern "C" int bbt_sync(bbt_ctx *ctx)
@@ -1295,7 +1374,13 @@ int bbt::bf_classify_slot(bbt_ctx *ctx, const uint8_t *seq, const uint64_t *off,
 	lc.count = 0;
 	if (lc.path == BBT_PATH_FILTER_MAJOR)
 		lc.path = BBT_PATH_PERSISTENT;
-	if (lc.path != BBT_PATH_PLAIN) {
+	if (ctx->mode == BBT_MODE_BESTHIT) {
+		ScoreArgs sa;
+		sa.scores[0] = sa.scores[1] = nullptr;
+		sa.fpr = ctx->d_fpr;
+		sa.besthit = 1;
+		CUDA_TRY(ctx, launch_scores(a, sa, lc, s));
+	} else if (lc.path != BBT_PATH_PLAIN) {
 		CUDA_TRY(ctx, cudaMemsetAsync(sc.work, 0, sizeof(unsigned long long), s));
 		if (ctx->long_bases && n * a.mates <= sc.order_cap) {
 			CUDA_TRY(ctx, cudaMemsetAsync(sc.order_cnt, 0, 2 * sizeof(unsigned long long), s));
@@ -1304,9 +1389,11 @@ int bbt::bf_classify_slot(bbt_ctx *ctx, const uint8_t *seq, const uint64_t *off,
 			a.order = sc.order;
 		}
 	}
-	CUDA_TRY(ctx, launch_classify(a, lc, s));
+	if (ctx->mode != BBT_MODE_BESTHIT)
+		CUDA_TRY(ctx, launch_classify(a, lc, s));
 	CUDA_TRY(ctx, launch_summarize(a.hits[0], paired ? a.hits[1] : nullptr, n, ctx->nf,
-			ctx->words, ctx->p.inclusive, category, ctx->d_counts, ctx->num_sms, s));
+			ctx->words, ctx->p.inclusive, ctx->mode == BBT_MODE_ORDERED, category,
+			ctx->d_counts, ctx->num_sms, s));
 	return BBT_OK;
 }
 

@@ -189,9 +189,14 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 }
 
 /* ResultsManager::updateSummaryData (ResultsManager.hpp:66-189) over a batch:
- * the category of each read (pair) and block-aggregated counter updates. */
-__global__ void summarize_kernel(const uint64_t *__restrict__ h1, const uint64_t *__restrict__ h2,
-		uint64_t n, uint32_t nf, uint32_t words, int inclusive, uint32_t *category,
+ * the category of each read (pair) and block-aggregated counter updates.
+ * ordered: evaluateReadOrdered / evaluateReadOrderedPair
+ * (BioBloomClassifier.cpp:1145-1180) stop at the first filter, in load order,
+ * that the read passes (pairs: that both mates pass, or either with -i) and
+ * report that filter alone for both mates: the lowest set bit of the same
+ * combined words, written back as the hit words. */
+__global__ void summarize_kernel(uint64_t *__restrict__ h1, uint64_t *__restrict__ h2,
+		uint64_t n, uint32_t nf, uint32_t words, int inclusive, int ordered, uint32_t *category,
 		unsigned long long *counts)
 {
 	extern __shared__ unsigned long long sc[];
@@ -206,6 +211,12 @@ __global__ void summarize_kernel(const uint64_t *__restrict__ h1, const uint64_t
 			uint64_t x = h1[i * words + w];
 			if (h2)
 				x = inclusive ? (x | h2[i * words + w]) : (x & h2[i * words + w]);
+			if (ordered) {
+				x = idx == nf ? (x & (0ull - x)) : 0ull; /* the first filter only */
+				h1[i * words + w] = x;
+				if (h2)
+					h2[i * words + w] = x;
+			}
 			while (x) {
 				uint32_t f = w * 64 + (uint32_t)(__ffsll((long long)x) - 1);
 				x &= x - 1;
@@ -373,9 +384,9 @@ cudaError_t launch_length_set(const uint64_t *off0, const uint64_t *off1, uint64
 	return cudaGetLastError();
 }
 
-cudaError_t launch_summarize(const uint64_t *h1, const uint64_t *h2, uint64_t n, uint32_t nf,
-		uint32_t words, int inclusive, uint32_t *category, unsigned long long *counts,
-		int num_sms, cudaStream_t s)
+cudaError_t launch_summarize(uint64_t *h1, uint64_t *h2, uint64_t n, uint32_t nf,
+		uint32_t words, int inclusive, int ordered, uint32_t *category,
+		unsigned long long *counts, int num_sms, cudaStream_t s)
 {
 	if (n == 0)
 		return cudaSuccess;
@@ -384,8 +395,8 @@ cudaError_t launch_summarize(const uint64_t *h1, const uint64_t *h2, uint64_t n,
 	uint64_t cap = (uint64_t)num_sms * 4;
 	unsigned blocks = (unsigned)(need < cap ? need : cap);
 	size_t smem = sizeof(unsigned long long) * (2 * (nf + 2) + 2);
-	summarize_kernel<<<blocks, threads, smem, s>>>(h1, h2, n, nf, words, inclusive, category,
-			counts);
+	summarize_kernel<<<blocks, threads, smem, s>>>(h1, h2, n, nf, words, inclusive, ordered,
+			category, counts);
 	return cudaGetLastError();
 }
 

@@ -68,10 +68,24 @@ cudaError_t launch_length_set(const uint64_t *off0, const uint64_t *off1, uint64
 		uint32_t mates, unsigned int *out, int num_sms, cudaStream_t s);
 
 /* Categories and summary counters for n reads (or pairs when h2 != NULL):
- * counts = aboveThreshold[nf+2], unique[nf+2], multiMatch, noMatch. */
-cudaError_t launch_summarize(const uint64_t *h1, const uint64_t *h2, uint64_t n, uint32_t nf,
-		uint32_t words, int inclusive, uint32_t *category, unsigned long long *counts,
-		int num_sms, cudaStream_t s);
+ * counts = aboveThreshold[nf+2], unique[nf+2], multiMatch, noMatch.
+ * ordered (-c): only the first filter of the read's hits (pairs: of the
+ * intersection, or of the union with inclusive) counts, and the hit words
+ * of both mates are rewritten to that one filter. */
+cudaError_t launch_summarize(uint64_t *h1, uint64_t *h2, uint64_t n, uint32_t nf,
+		uint32_t words, int inclusive, int ordered, uint32_t *category,
+		unsigned long long *counts, int num_sms, cudaStream_t s);
+
+/* Exhaustive per-filter scores (SeqEval::evalScore) of the reads of a
+ * ClassifyArgs batch (score.cu).  scores[m] (optional): n x nf doubles of mate
+ * array m.  besthit: also write, as a.hits, the filters of the largest score. */
+struct ScoreArgs {
+	double *scores[2];
+	const double *fpr;   /* BINOMIAL: each filter's FPR (getFPRPrecompute) */
+	int besthit;
+};
+cudaError_t launch_scores(const ClassifyArgs &a, const ScoreArgs &sa, const LaunchConfig &lc,
+		cudaStream_t s);
 
 } // namespace bbt
 

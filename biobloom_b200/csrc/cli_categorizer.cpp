@@ -2,15 +2,16 @@
  * cli_categorizer.cpp -- biobloomcategorizer on the B200 path.
  *
  * Same flags as the reference CLI (BioBloomCategorizer/BioBloomCategorizer.cpp:
- * 171-205); the score conversion (integer > 1 selects LENGTH scoring,
- * :416-441), the filter existence check (:444-452) and the mode dispatch
- * (:458-532) follow it.  Output: "<prefix>_summary.tsv" and, with
- * --read_status FILE, one "<read>\t<category>" line per read (pair).
- * --fa / --fq (with -g) write the reads of each category to their own files,
- * -d / -n print the first filter's reads (or all others) to stdout.  Options
- * whose outputs this build does not produce yet (-b, -w, -c, -S, -D, -l,
- * single-file paired input) are refused with a message instead of being
- * ignored.
+ * 171-205); the option checks (:355-385, 398-442), the score conversion
+ * (integer > 1 selects LENGTH scoring, binomial -s as a Phred-scaled FPR,
+ * :414-441), the filter existence check (:444-452) and the dispatch over
+ * paired / smart-paired / file-list / single-end inputs (:458-532) follow it.
+ * Output: "<prefix>_summary.tsv" and, with --read_status FILE, one
+ * "<read>\t<category>" line per read (pair).  --fa / --fq (with -g) write the
+ * reads of each category to their own files, -d / -n print the first filter's
+ * reads (or all others) to stdout; -c, -b and -w select the ordered, best-hit
+ * and with-scores modes.  DUST masking (-D, -T, -W) is refused with a message
+ * instead of being ignored.
  */
 #include <getopt.h>
 #include <sys/stat.h>
@@ -50,6 +51,13 @@ static void usage_exit(int code)
 	        "  -d, --stdout_filter    Outputs all matching reads to stdout for the first\n"
 	        "                         filter listed by -f.\n"
 	        "  -n, --inverse          Inverts the output of -d (everything but first filter).\n"
+	        "  -l, --file_list=N      A file of list of file pairs to run in parallel.\n"
+	        "  -c, --ordered          Use ordered filtering. Order of filters matters\n"
+	        "                         (filters listed first have higher priority).\n"
+	        "  -b, --best_hit         Places reads into the filter with the best score\n"
+	        "                         (no minimum threshold).\n"
+	        "  -w, --with_score       Output multimatches with scores in the order of filter.\n"
+	        "  -S, --score_type=N     harmonic or binomial scoring.\n"
 	        "  -r, --streak=N         Hits tiling in second pass needed to jump several tiles\n"
 	        "                         upon a miss. [3]\n"
 	        "  -I, --interval         Accepted for compatibility.\n"
@@ -82,7 +90,9 @@ int main(int argc, char **argv)
 	bbt_default_params(&p);
 	string filters, prefix, read_status, postfix;
 	double binomial_score = 100; /* -s for binomial scoring, BioBloomCategorizer.cpp:168 */
-	bool paired = false, die = false, to_stdout = false, inverse = false;
+	bool paired = false, die = false, to_stdout = false, inverse = false, collab = false;
+	int mode = BBT_MODE_STD;
+	string file_list;
 	int fastq = 0, fasta = 0, verbose = 0;
 	int device = 0;
 	string unsupported;
@@ -158,7 +168,31 @@ int main(int argc, char **argv)
 		case 'g': postfix = ".gz"; break;
 		case 'd': to_stdout = true; break;
 		case 'n': inverse = true; break;
-		case 'l': case 'c': case 'b': case 'w':
+		case 'l': {
+			stringstream conv(optarg);
+			if (!(conv >> file_list)) {
+				cerr << "Error - Invalid set of bloom filter parameters! l: " << optarg << endl;
+				return 0;
+			}
+			break;
+		}
+		case 'c': collab = true; break;
+		case 'w':
+			if (mode == BBT_MODE_STD) {
+				mode = BBT_MODE_SCORES;
+			} else {
+				cerr << "Filter scoring modes cannot be mixed with score mode" << endl;
+				die = true;
+			}
+			break;
+		case 'b':
+			if (mode == BBT_MODE_STD) {
+				mode = BBT_MODE_BESTHIT;
+			} else {
+				cerr << "Filter scoring modes cannot be mixed with best hit mode" << endl;
+				die = true;
+			}
+			break;
 		case 'D': case 'T': case 'W': case 'o':
 			unsupported += string(" -") + (char)c;
 			break;
@@ -181,17 +215,24 @@ int main(int argc, char **argv)
 	while (optind < argc)
 		files.push_back(argv[optind++]);
 	vector<string> paths = split_ws(filters);
-	if (paired && files.size() != 2) {
-		if (files.size() == 1)
-			unsupported += " (single-file paired input)";
-		else {
+	bool smart = false;
+	if (paired) {
+		if (files.size() == 1) {
+			smart = true;
+		} else if (files.size() != 2 && file_list.empty()) {
 			cerr << "Usage of paired end mode:\n"
 			        "biobloomcategorizer [OPTION]... -f \"[FILTER1]...\" [FILEPAIR1] [FILEPAIR2]\n"
+			        "or biobloomcategorizer [OPTION]... -f \"[FILTER1]...\" [SMARTPAIR]\n"
 			     << endl;
 			die = true;
 		}
 	}
-	if (files.empty()) {
+	if (!file_list.empty() && !files.empty()) {
+		cerr << "--file_list (-l) cannot be used with read files in specified in arguments"
+		     << endl;
+		die = true;
+	}
+	if (files.empty() && file_list.empty()) {
 		cerr << "Error: Need Input File" << endl;
 		die = true;
 	}
@@ -207,16 +248,22 @@ int main(int argc, char **argv)
 		cerr << "Error: option(s)" << unsupported << " are not supported by this build" << endl;
 		exit(EXIT_FAILURE);
 	}
-	if (p.scoring == BBT_SCORE_BINOMIAL) {
+	if (paired && !file_list.empty() && !out_type.empty()) {
+		/* the reference dereferences the empty input-file list here */
+		cerr << "Error: --file_list (-l) with paired-end mode does not write read files" << endl;
+		exit(EXIT_FAILURE);
+	}
+	if (mode == BBT_MODE_SCORES && out_type.empty()) {
+		cerr << "Error: -w option cannot be used without output method" << endl;
+		exit(EXIT_FAILURE);
+	}
+	if (mode == BBT_MODE_BESTHIT) {
+		cerr << "Best Hit mode (no minimum threshold)" << endl;
+	} else if (p.scoring == BBT_SCORE_BINOMIAL) {
 		/* BioBloomCategorizer.cpp:418-421 */
 		p.score = pow(10.0, -(binomial_score / 10.0));
 		cerr << "FPR of a match: " << p.score << endl;
 	} else {
-		if (p.score < 0) {
-			cerr << "Error - s must be a positive integer or a floating point between 0 and 1."
-			     << endl;
-			exit(EXIT_FAILURE);
-		}
 		unsigned match_len = (unsigned)p.score;
 		if (match_len > 1) {
 			p.score = match_len;
@@ -224,6 +271,11 @@ int main(int argc, char **argv)
 			cerr << "Min match length threshold: " << match_len << " bp" << endl;
 		} else {
 			cerr << "Min score threshold: " << p.score << endl;
+		}
+		if (p.score < 0) {
+			cerr << "Error - s must be a positive integer or a floating point between 0 and 1."
+			     << endl;
+			exit(EXIT_FAILURE);
 		}
 	}
 	if (prefix.find('/') != string::npos) {
@@ -253,23 +305,78 @@ int main(int argc, char **argv)
 	for (int i = 0; i < bbt_num_filters(ctx); ++i)
 		cerr << "Loaded Filter: " << bbt_filter_id(ctx, i) << endl;
 	cerr << "Filter Loading Complete." << endl;
-	int rc;
+	if (collab) {
+		/* BioBloomClassifier::setOrderedFilter (BioBloomClassifier.h:67-75) */
+		if (mode == BBT_MODE_BESTHIT) {
+			cerr << "Best Hit mode and Ordered mode detected. Not yet supported." << endl;
+			bbt_close(ctx);
+			exit(1);
+		}
+		mode = BBT_MODE_ORDERED;
+	}
+	bbt_set_mode(ctx, mode);
+	int rc = BBT_OK;
 	const char *rs = read_status.empty() ? nullptr : read_status.c_str();
 	if (to_stdout)
 		bbt_set_stdout(ctx, 1, inverse ? 1 : 0);
+	/* the list file: whitespace-separated first (and second) file per line */
+	vector<string> list1, list2;
+	if (!file_list.empty()) {
+		ifstream lf(file_list.c_str());
+		if (!lf.is_open() && paired) {
+			cout << "Unable to open file";
+			bbt_close(ctx);
+			return 0;
+		}
+		string line;
+		while (getline(lf, line)) {
+			stringstream ss(line);
+			string a, b;
+			ss >> a;
+			ss >> b;
+			list1.push_back(a);
+			list2.push_back(b);
+		}
+		cerr << "Using file list" << endl;
+	}
+	auto cstrs = [](const vector<string> &v) {
+		vector<const char *> out;
+		for (const string &f : v)
+			out.push_back(f.c_str());
+		return out;
+	};
 	if (paired) {
-		rc = out_type.empty()
-				? bbt_filter_pair_files(ctx, files[0].c_str(), files[1].c_str(), prefix.c_str(), rs)
-				: bbt_filter_pair_files_print(ctx, files[0].c_str(), files[1].c_str(),
+		if (!out_type.empty()) {
+			rc = smart ? bbt_filter_smart_pairs_print(ctx, files[0].c_str(), prefix.c_str(),
+						out_type.c_str(), postfix.c_str(), rs)
+			           : bbt_filter_pair_files_print(ctx, files[0].c_str(), files[1].c_str(),
 						prefix.c_str(), out_type.c_str(), postfix.c_str(), rs);
+		} else if (smart) {
+			rc = bbt_filter_smart_pairs(ctx, files[0].c_str(), prefix.c_str(), rs);
+		} else if (!file_list.empty()) {
+			vector<const char *> a = cstrs(list1), b = cstrs(list2);
+			if (a.empty()) {
+				cerr << "Error: the file list holds no files" << endl;
+				rc = BBT_ERR_ARG;
+			} else {
+				rc = bbt_filter_pair_file_lists(ctx, a.data(), b.data(), (int)a.size(),
+						prefix.c_str(), rs);
+			}
+		} else {
+			rc = bbt_filter_pair_files(ctx, files[0].c_str(), files[1].c_str(), prefix.c_str(), rs);
+		}
 	} else {
-		vector<const char *> fp;
-		for (const string &f : files)
-			fp.push_back(f.c_str());
-		rc = out_type.empty()
-				? bbt_filter_files(ctx, fp.data(), (int)fp.size(), prefix.c_str(), rs)
-				: bbt_filter_files_print(ctx, fp.data(), (int)fp.size(), prefix.c_str(),
-						out_type.c_str(), postfix.c_str(), rs);
+		const vector<string> &in = file_list.empty() ? files : list1;
+		vector<const char *> fp = cstrs(in);
+		if (fp.empty()) {
+			cerr << "Error: the file list holds no files" << endl;
+			rc = BBT_ERR_ARG;
+		} else {
+			rc = out_type.empty()
+					? bbt_filter_files(ctx, fp.data(), (int)fp.size(), prefix.c_str(), rs)
+					: bbt_filter_files_print(ctx, fp.data(), (int)fp.size(), prefix.c_str(),
+							out_type.c_str(), postfix.c_str(), rs);
+		}
 	}
 	if (rc != BBT_OK) {
 		cerr << "Error: " << bbt_last_error(ctx) << endl;

@@ -21,6 +21,8 @@ struct Slot {
 	uint64_t *d_off[2] = {nullptr, nullptr};
 	uint64_t *d_hits[2] = {nullptr, nullptr};
 	uint32_t *d_cat = nullptr;
+	double *d_scores[2] = {nullptr, nullptr}; /* BESTHIT / SCORES: reads x filters */
+	uint64_t scores_cap = 0;                  /* reads d_scores holds */
 	cudaEvent_t copied = nullptr;   /* inputs are on the device */
 	cudaEvent_t computed = nullptr; /* kernels done */
 	cudaEvent_t done = nullptr;     /* results are back on the host */
@@ -52,6 +54,9 @@ struct bbt_ctx {
 	uint64_t cap_bases = 0, cap_reads = 0;
 	uint64_t *d_tmp_hits[2] = {nullptr, nullptr};
 	uint64_t tmp_hits_cap = 0;
+	/* filtering mode (BBT_MODE_*): ORDERED, BESTHIT and SCORES */
+	int mode = BBT_MODE_STD;
+	double *d_fpr = nullptr;         /* each filter's FPR on the device (BINOMIAL scores) */
 	/* two-pass filter-major scratch: padded frame offsets, per-block sums,
 	 * per-frame canonical hashes and validity words of one sub-batch */
 	uint64_t *d_tp_local = nullptr;

@@ -21,6 +21,7 @@
 #include <mutex>
 #include <thread>
 #include <algorithm>
+#include <unordered_map>
 
 #include "bbt.h"
 #include "ctx.hpp"
@@ -211,6 +212,75 @@ bool fill_batch(HostBatch &b, FastxReader *r1, FastxReader *r2, uint64_t max_rea
 	return more;
 }
 
+/* A mate waiting for its partner in a single-file paired input. */
+struct PendingMate {
+	std::string comment, qual;
+	std::vector<char> seq;
+};
+
+/* BioBloomClassifier::filterPair(file) / filterPairPrint(file, type)
+ * (BioBloomClassifier.cpp:463-564, 571-729): the header is the read name
+ * without its last two characters when it ends in '1' or '2' ("x/1" -> "x");
+ * the first record of a header waits in `pending`, the next record with the
+ * same header completes the pair (the waiting record is mate 1) and the
+ * header is free again.  Records never paired are dropped.  Mates go to the
+ * batch in the order their pairs complete. */
+bool fill_batch_smart(HostBatch &b, FastxReader *r, uint64_t max_reads, uint64_t max_bases,
+		bool keep_names, bool keep_records, std::vector<char> &s1, std::vector<char> &s2,
+		std::unordered_map<std::string, PendingMate> &pending, std::string &perr)
+{
+	std::string name, comment, qual;
+	std::vector<char> seq;
+	b.n = 0;
+	b.names.clear();
+	for (int m = 0; m < 2; ++m) {
+		b.rname[m].clear();
+		b.rcomment[m].clear();
+		b.rqual[m].clear();
+	}
+	s1.clear();
+	s2.clear();
+	b.off[0].assign(1, 0);
+	b.off[1].assign(1, 0);
+	while (b.n < max_reads && s1.size() < max_bases && s2.size() < max_bases) {
+		seq.clear();
+		long l = r->read(name, comment, seq, qual);
+		if (l < 0) {
+			if (l < -1)
+				perr = l == -2 ? "truncated quality string" : "stream error";
+			return false;
+		}
+		if (!name.empty() && (name.back() == '1' || name.back() == '2'))
+			name.resize(name.size() >= 2 ? name.size() - 2 : 0);
+		auto it = pending.find(name);
+		if (it == pending.end()) {
+			PendingMate &pm = pending[name];
+			pm.comment = comment;
+			pm.qual = qual;
+			pm.seq = seq;
+			continue;
+		}
+		PendingMate &m1 = it->second;
+		s1.insert(s1.end(), m1.seq.begin(), m1.seq.end());
+		s2.insert(s2.end(), seq.begin(), seq.end());
+		b.off[0].push_back(s1.size());
+		b.off[1].push_back(s2.size());
+		if (keep_names)
+			b.names.push_back(name);
+		if (keep_records) {
+			b.rname[0].push_back(name);
+			b.rcomment[0].push_back(m1.comment);
+			b.rqual[0].push_back(m1.qual);
+			b.rname[1].push_back(name);
+			b.rcomment[1].push_back(comment);
+			b.rqual[1].push_back(qual);
+		}
+		pending.erase(it);
+		++b.n;
+	}
+	return true;
+}
+
 /* A categorized-read output file: plain or gzip (".gz" postfix), as
  * Dynamicofstream chooses by the name (Common/Dynamicofstream.cpp:14-24). */
 struct OutFile {
@@ -246,14 +316,17 @@ struct OutFile {
 };
 
 /* ">name comment\nseq\n" or "@name comment\nseq\n+\nqual\n", with the space
- * written even for an empty comment (BioBloomClassifier.h:144-209). */
+ * written even for an empty comment (BioBloomClassifier.h:144-209); extra
+ * (scores, each with its leading space) goes right after the comment. */
 void append_record(std::string &out, bool fastq, const std::string &name,
-		const std::string &comment, const char *seq, size_t len, const std::string &qual)
+		const std::string &comment, const char *seq, size_t len, const std::string &qual,
+		const std::string &extra = std::string())
 {
 	out += fastq ? '@' : '>';
 	out += name;
 	out += ' ';
 	out += comment;
+	out += extra;
 	out += '\n';
 	out.append(seq, len);
 	if (fastq) {
@@ -263,14 +336,76 @@ void append_record(std::string &out, bool fastq, const std::string &name,
 	out += '\n';
 }
 
-int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std::string *file2,
-		const char *prefix, const char *read_status, const char *out_type = nullptr,
-		const char *postfix = nullptr)
+/* A double as std::ostream prints it by default (precision 6, %g). */
+void append_double(std::string &out, double v)
 {
-	const bool paired = file2 != nullptr;
+	char buf[64];
+	snprintf(buf, sizeof buf, " %g", v);
+	out += buf;
+}
+
+/* BESTHIT: the largest score of one read (evaluateReadBestHit,
+ * BioBloomClassifier.cpp:1194-1218: maxScore starts at 0) and how many
+ * filters reach it (none unless it is above 0). */
+double best_of(const double *sc, uint32_t nf, uint32_t *count)
+{
+	double mx = 0;
+	for (uint32_t f = 0; f < nf; ++f)
+		if (mx < sc[f])
+			mx = sc[f];
+	uint32_t c = 0;
+	if (mx > 0)
+		for (uint32_t f = 0; f < nf; ++f)
+			c += sc[f] == mx;
+	*count = c;
+	return mx;
+}
+
+/* What a categorized file's record carries after the comment
+ * (printSingleToFile / printPairToFile, BioBloomClassifier.h:144-209,
+ * 291-411): SCORES puts every filter's score on multiMatch records; BESTHIT
+ * puts the read's best score on every record, except multiMatch records of
+ * FASTA files and of pairs, which carry the score once per best filter. */
+std::string file_extra(const bbt_ctx *ctx, uint32_t cat, bool fastq, bool paired,
+		const double *sc)
+{
+	std::string x;
+	const uint32_t multi = ctx->nf + 1;
+	if (ctx->mode == BBT_MODE_SCORES && cat == multi) {
+		for (uint32_t f = 0; f < ctx->nf; ++f)
+			append_double(x, sc[f]);
+	} else if (ctx->mode == BBT_MODE_BESTHIT) {
+		uint32_t cnt = 0;
+		const double mx = best_of(sc, ctx->nf, &cnt);
+		if (cat == multi && (!fastq || paired)) {
+			for (uint32_t i = 0; i < cnt; ++i)
+				append_double(x, mx);
+		} else {
+			append_double(x, mx);
+		}
+	}
+	return x;
+}
+
+/* The reads of one pipeline run: single-end files; pairs of files (files2[i]
+ * holds the mates of files1[i]); or one file whose mates are matched by name. */
+struct PipeInput {
+	std::vector<std::string> files1, files2;
+	bool smart = false;
+};
+
+int run_pipeline(bbt_ctx *ctx, const PipeInput &in, const char *prefix, const char *read_status,
+		const char *out_type = nullptr, const char *postfix = nullptr)
+{
+	const std::vector<std::string> &files1 = in.files1;
+	const bool paired = in.smart || !in.files2.empty();
 	const bool print = out_type && out_type[0];
 	const bool fastq_out = print && std::string(out_type) == "fq";
 	const bool keep_records = print || ctx->to_stdout;
+	/* BESTHIT and SCORES records carry evalScore values */
+	const bool want_scores = keep_records &&
+			(ctx->mode == BBT_MODE_BESTHIT || ctx->mode == BBT_MODE_SCORES);
+	std::vector<double> scores[2];
 	/* output files: one per filter, then noMatch, then multiMatch
 	 * (BioBloomClassifier.cpp:116-127, 319-337) */
 	std::vector<OutFile> outs[2];
@@ -326,6 +461,7 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 		size_t fi = 0;
 		FastxReader *r1 = nullptr;
 		FastxReader *r2 = nullptr;
+		std::unordered_map<std::string, PendingMate> pending;
 		auto open_next = [&]() -> bool {
 			delete r1;
 			delete r2;
@@ -337,10 +473,10 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 				pipe.err = "file " + files1[fi] + " cannot be opened";
 				return false;
 			}
-			if (paired) {
-				r2 = new FastxReader(*file2);
+			if (!in.files2.empty()) {
+				r2 = new FastxReader(in.files2[fi]);
 				if (!r2->ok()) {
-					pipe.err = "file " + *file2 + " cannot be opened";
+					pipe.err = "file " + in.files2[fi] + " cannot be opened";
 					return false;
 				}
 			}
@@ -360,8 +496,11 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 			b.n = 0;
 			if (have) {
 				std::string perr;
-				bool more = fill_batch(b, r1, r2, max_reads, max_bases, read_status != nullptr,
-						keep_records, stage1[which], stage2[which], perr);
+				bool more = in.smart
+						? fill_batch_smart(b, r1, max_reads, max_bases, read_status != nullptr,
+								keep_records, stage1[which], stage2[which], pending, perr)
+						: fill_batch(b, r1, r2, max_reads, max_bases, read_status != nullptr,
+								keep_records, stage1[which], stage2[which], perr);
 				if (!perr.empty())
 					std::cerr << "warning: " << perr << "; reading of this file stopped there"
 					          << std::endl;
@@ -388,7 +527,7 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 						memcpy(b.seq[1], stage2[which].data(), stage2[which].size());
 				}
 				if (have && !more)
-					have = paired ? false : open_next();
+					have = in.smart ? false : open_next();
 			}
 			b.last = !have;
 			{
@@ -426,7 +565,14 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 			res.hits2 = nullptr;
 			res.category = (read_status || keep_records) ? b.cat.data() : nullptr;
 			res.location = BBT_HOST;
-			rc = bbt_classify_batch(ctx, &bt, &res, nullptr);
+			if (want_scores) {
+				for (int m = 0; m < (paired ? 2 : 1); ++m)
+					scores[m].resize(b.n * ctx->nf);
+				rc = bbt_classify_batch_scores(ctx, &bt, &res, scores[0].data(),
+						paired ? scores[1].data() : nullptr, nullptr);
+			} else {
+				rc = bbt_classify_batch(ctx, &bt, &res, nullptr);
+			}
 			if (rc)
 				break;
 			if (keep_records) {
@@ -438,17 +584,27 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 					text[1].resize(ctx->nf + 2);
 				}
 				std::string so;
+				const std::string none;
 				for (uint64_t i = 0; i < b.n; ++i) {
 					const uint32_t c = b.cat[i];
 					for (int m = 0; m < (paired ? 2 : 1); ++m) {
 						const uint64_t o = b.off[m][i], e = b.off[m][i + 1];
 						const char *sq = b.seq[m] + o;
+						const double *sc = want_scores ? scores[m].data() + i * ctx->nf : nullptr;
 						if (print)
 							append_record(text[m][c], fastq_out, b.rname[m][i], b.rcomment[m][i],
-									sq, e - o, b.rqual[m][i]);
-						if (ctx->to_stdout && (ctx->inverse ? c != 0 : c == 0))
+									sq, e - o, b.rqual[m][i],
+									sc ? file_extra(ctx, c, fastq_out, paired, sc) : none);
+						if (ctx->to_stdout && (ctx->inverse ? c != 0 : c == 0)) {
+							/* printSingle / printPair: BESTHIT adds the read's score */
+							std::string x;
+							if (sc && !ctx->inverse && ctx->mode == BBT_MODE_BESTHIT) {
+								uint32_t cnt;
+								append_double(x, best_of(sc, ctx->nf, &cnt));
+							}
 							append_record(so, true, b.rname[m][i], b.rcomment[m][i], sq, e - o,
-									b.rqual[m][i]);
+									b.rqual[m][i], x);
+						}
 					}
 				}
 				for (int m = 0; m < (paired ? 2 : 1) && print; ++m)
@@ -520,16 +676,21 @@ int run_pipeline(bbt_ctx *ctx, const std::vector<std::string> &files1, const std
 
 using namespace bbt;
 
+static bool valid_out_type(const char *t)
+{
+	return t && (std::string(t) == "fa" || std::string(t) == "fq");
+}
+
 extern "C" int bbt_filter_files(bbt_ctx *ctx, const char *const *files, int n_files,
 		const char *prefix, const char *read_status)
 {
 	if (!ctx || !files || n_files <= 0)
 		return fail(ctx, BBT_ERR_ARG, "bbt_filter_files: need at least one input file");
-	std::vector<std::string> f;
+	PipeInput in;
 	for (int i = 0; i < n_files; ++i)
-		f.push_back(files[i]);
+		in.files1.push_back(files[i]);
 	std::cerr << "Filtering Start" << std::endl;
-	return run_pipeline(ctx, f, nullptr, prefix, read_status);
+	return run_pipeline(ctx, in, prefix, read_status);
 }
 
 extern "C" int bbt_filter_pair_files(bbt_ctx *ctx, const char *file1, const char *file2,
@@ -537,10 +698,11 @@ extern "C" int bbt_filter_pair_files(bbt_ctx *ctx, const char *file1, const char
 {
 	if (!ctx || !file1 || !file2)
 		return fail(ctx, BBT_ERR_ARG, "bbt_filter_pair_files: need two input files");
-	std::vector<std::string> f(1, file1);
-	std::string f2 = file2;
+	PipeInput in;
+	in.files1.push_back(file1);
+	in.files2.push_back(file2);
 	std::cerr << "Filtering Start" << std::endl;
-	return run_pipeline(ctx, f, &f2, prefix, read_status);
+	return run_pipeline(ctx, in, prefix, read_status);
 }
 
 extern "C" int bbt_filter_files_print(bbt_ctx *ctx, const char *const *files, int n_files,
@@ -548,13 +710,13 @@ extern "C" int bbt_filter_files_print(bbt_ctx *ctx, const char *const *files, in
 {
 	if (!ctx || !files || n_files <= 0)
 		return fail(ctx, BBT_ERR_ARG, "bbt_filter_files_print: need at least one input file");
-	if (!out_type || (std::string(out_type) != "fa" && std::string(out_type) != "fq"))
+	if (!valid_out_type(out_type))
 		return fail(ctx, BBT_ERR_ARG, "bbt_filter_files_print: out_type is \"fa\" or \"fq\"");
-	std::vector<std::string> f;
+	PipeInput in;
 	for (int i = 0; i < n_files; ++i)
-		f.push_back(files[i]);
+		in.files1.push_back(files[i]);
 	std::cerr << "Filtering Start" << std::endl;
-	return run_pipeline(ctx, f, nullptr, prefix, read_status, out_type, postfix);
+	return run_pipeline(ctx, in, prefix, read_status, out_type, postfix);
 }
 
 extern "C" int bbt_filter_pair_files_print(bbt_ctx *ctx, const char *file1, const char *file2,
@@ -562,10 +724,53 @@ extern "C" int bbt_filter_pair_files_print(bbt_ctx *ctx, const char *file1, cons
 {
 	if (!ctx || !file1 || !file2)
 		return fail(ctx, BBT_ERR_ARG, "bbt_filter_pair_files_print: need two input files");
-	if (!out_type || (std::string(out_type) != "fa" && std::string(out_type) != "fq"))
-		return fail(ctx, BBT_ERR_ARG, "bbt_filter_pair_files_print: out_type is \"fa\" or \"fq\"");
-	std::vector<std::string> f(1, file1);
-	std::string f2 = file2;
+	if (!valid_out_type(out_type))
+		return fail(ctx, BBT_ERR_ARG,
+				"bbt_filter_pair_files_print: out_type is \"fa\" or \"fq\"");
+	PipeInput in;
+	in.files1.push_back(file1);
+	in.files2.push_back(file2);
 	std::cerr << "Filtering Start" << std::endl;
-	return run_pipeline(ctx, f, &f2, prefix, read_status, out_type, postfix);
+	return run_pipeline(ctx, in, prefix, read_status, out_type, postfix);
+}
+
+extern "C" int bbt_filter_pair_file_lists(bbt_ctx *ctx, const char *const *files1,
+		const char *const *files2, int n_pairs, const char *prefix, const char *read_status)
+{
+	if (!ctx || !files1 || !files2 || n_pairs <= 0)
+		return fail(ctx, BBT_ERR_ARG, "bbt_filter_pair_file_lists: need at least one file pair");
+	PipeInput in;
+	for (int i = 0; i < n_pairs; ++i) {
+		in.files1.push_back(files1[i] ? files1[i] : "");
+		in.files2.push_back(files2[i] ? files2[i] : "");
+	}
+	std::cerr << "Filtering Start" << std::endl;
+	return run_pipeline(ctx, in, prefix, read_status);
+}
+
+extern "C" int bbt_filter_smart_pairs(bbt_ctx *ctx, const char *file, const char *prefix,
+		const char *read_status)
+{
+	if (!ctx || !file)
+		return fail(ctx, BBT_ERR_ARG, "bbt_filter_smart_pairs: need an input file");
+	PipeInput in;
+	in.files1.push_back(file);
+	in.smart = true;
+	std::cerr << "Filtering Start" << std::endl;
+	return run_pipeline(ctx, in, prefix, read_status);
+}
+
+extern "C" int bbt_filter_smart_pairs_print(bbt_ctx *ctx, const char *file, const char *prefix,
+		const char *out_type, const char *postfix, const char *read_status)
+{
+	if (!ctx || !file)
+		return fail(ctx, BBT_ERR_ARG, "bbt_filter_smart_pairs_print: need an input file");
+	if (!valid_out_type(out_type))
+		return fail(ctx, BBT_ERR_ARG,
+				"bbt_filter_smart_pairs_print: out_type is \"fa\" or \"fq\"");
+	PipeInput in;
+	in.files1.push_back(file);
+	in.smart = true;
+	std::cerr << "Filtering Start" << std::endl;
+	return run_pipeline(ctx, in, prefix, read_status, out_type, postfix);
 }

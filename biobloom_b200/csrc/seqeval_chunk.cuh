@@ -651,6 +651,117 @@ BBT_HD int seq_chunk(SeqState &s, uint32_t V, uint32_t H, int64_t base, int nf, 
 	return s.decided;
 }
 
+/*
+ * SeqEval::evalScore (Common/SeqEval.h:534-560): the exhaustive walks that
+ * score a read against one filter without stopping early (BESTHIT and SCORES
+ * modes).
+ *   SIMPLE   evalSimpleScore (:334-376): +0.5 for a hit that starts a streak,
+ *            +1 for a hit that continues one;
+ *   HARMONIC evalHarmonicScore (:378-419): +0.5, then +1 - 1/(1 + streak);
+ *   BINOMIAL evalBinomialScore (:450-491): +1 per hit (the count then goes
+ *            through the binomial upper tail);
+ * in all three a frame after an N gap (pos != prevPos + 1) starts a new streak,
+ * and a miss that ends a streak of at least streakThreshold hits leaves the
+ * frames below pos + k unprobed (they still move prevPos).  SIMPLE and
+ * HARMONIC divide the sum by len - k + 1 (normalizeScore, :33-35).
+ *   LENGTH   evalMinMatchLenScore (:421-448): every frame is probed; the value
+ *            is the length of the run of hits that reaches the last frame (k
+ *            for its first hit, +1 per further hit; a miss or a gap ends it).
+ * Unlike evalSimple there is no first-frame special case: prevPos starts at 0
+ * and the streak at 0, so the first frame's gap check changes nothing.
+ */
+enum { SCORE_SIMPLE = 0, SCORE_LENGTH = 1, SCORE_HARMONIC = 2, SCORE_BINOMIAL = 3 };
+
+struct ScoreState {
+	double score;        /* SIMPLE / HARMONIC sum; BINOMIAL hit count */
+	uint32_t streak;
+	uint32_t run;        /* LENGTH: the current match length */
+	int64_t prev;        /* last iterated frame */
+	int64_t skip_end;    /* frames below this are iterated without a probe */
+};
+
+BBT_HD void score_init(ScoreState &s)
+{
+	s.score = 0.0;
+	s.streak = 0;
+	s.run = 0;
+	s.prev = 0;
+	s.skip_end = 0;
+}
+
+/* Walk the valid frames of one chunk (frame j = base + j, j < nf); H holds the
+ * hits of the frames probed (every frame for LENGTH, otherwise those at or
+ * after skip_end when the chunk began). */
+BBT_HD void score_chunk(ScoreState &s, uint32_t V, uint32_t H, int64_t base, int nf, int k,
+		uint32_t streak_thr, int mode)
+{
+	uint32_t x = V & low_mask(nf);
+	while (x) {
+		const int q = lowbit32(x);
+		x &= x - 1;
+		const int64_t p = base + q;
+		const bool hit = (H >> q) & 1u;
+		if (mode == SCORE_LENGTH) {
+			if (p != s.prev + 1)
+				s.run = 0;
+			s.run = hit ? (s.run ? s.run + 1 : (uint32_t)k) : 0u;
+			s.prev = p;
+			continue;
+		}
+		if (p < s.skip_end) {
+			s.prev = p;
+			continue;
+		}
+		if (p != s.prev + 1)
+			s.streak = 0;
+		if (hit) {
+			if (mode == SCORE_HARMONIC)
+				s.score = harmonic_add(s.score, s.streak);
+			else if (mode == SCORE_BINOMIAL)
+				s.score = s.score + 1.0;
+			else
+				s.score = s.score + (s.streak ? 1.0 : 0.5);
+			++s.streak;
+		} else {
+			if (s.streak >= streak_thr)
+				s.skip_end = (int64_t)(uint32_t)((uint32_t)p + (uint32_t)k);
+			s.streak = 0;
+		}
+		s.prev = p;
+	}
+}
+
+/* The value of 0.0 / 0.0 on x86-64 (the negative default NaN), which is what
+ * normalizeScore returns for a read of k - 1 bases. */
+BBT_HD double x86_default_nan()
+{
+#if defined(__CUDA_ARCH__)
+	return __longlong_as_double((long long)0xFFF8000000000000ull);
+#else
+	union {
+		uint64_t u;
+		double d;
+	} v;
+	v.u = 0xFFF8000000000000ull;
+	return v.d;
+#endif
+}
+
+/* normalizeScore (Common/SeqEval.h:33-35): score / (len - k + 1), the divisor
+ * in size_t arithmetic (it wraps for len < k - 1; for len = k - 1 it is 0,
+ * and so is the score: 0 / 0). */
+BBT_HD double score_normalize(double score, uint64_t len, unsigned k)
+{
+	const uint64_t d = len - (uint64_t)k + 1u;
+	if (d == 0)
+		return x86_default_nan();
+#if defined(__CUDA_ARCH__)
+	return __ddiv_rn(score, __ull2double_rn(d));
+#else
+	return score / (double)d;
+#endif
+}
+
 } // namespace bbt
 
 #endif

@@ -171,17 +171,46 @@ int bbt_filter_pair_files(bbt_ctx *ctx, const char *file1, const char *file2,
  * per filter, then "_noMatch" and "_multiMatch" (pairs: "_1" / "_2" before
  * the extension); records are ">name comment\nseq\n" or
  * "@name comment\nseq\n+\nqual\n" in input order.  out_type: "fa" or "fq";
- * postfix: "" or ".gz".  Replaces BioBloomClassifier::filterPrint
- * (BioBloomClassifier.cpp:108-203) and filterPairPrint (:311-450).
+ * postfix: "" or ".gz".  In BESTHIT and SCORES modes (bbt_set_mode) records
+ * carry scores after the comment, each as " %g": SCORES on multiMatch records
+ * every filter's score; BESTHIT the read's best score, except on multiMatch
+ * records of FASTA files and of pairs, which repeat it once per best filter
+ * (BioBloomClassifier.h:144-209, 291-411).  Replaces
+ * BioBloomClassifier::filterPrint (BioBloomClassifier.cpp:108-203) and
+ * filterPairPrint (:311-450).
  */
 int bbt_filter_files_print(bbt_ctx *ctx, const char *const *files, int n_files,
 		const char *prefix, const char *out_type, const char *postfix, const char *read_status);
 int bbt_filter_pair_files_print(bbt_ctx *ctx, const char *file1, const char *file2,
 		const char *prefix, const char *out_type, const char *postfix, const char *read_status);
 
+/*
+ * Pairs from a list of file pairs (-e -l): files2[i] holds the mates of
+ * files1[i]; each pair of files is read until either ends, and one summary
+ * covers them all.  Replaces BioBloomClassifier::filterPair(vector, vector)
+ * (BioBloomClassifier.cpp:731-806; list parsing BioBloomCategorizer.cpp:
+ * 482-497).
+ */
+int bbt_filter_pair_file_lists(bbt_ctx *ctx, const char *const *files1,
+		const char *const *files2, int n_pairs, const char *prefix, const char *read_status);
+
+/*
+ * Pairs from one file (-e with a single input): a record's header is its name
+ * without the last two characters when the name ends in '1' or '2'; the first
+ * record of a header waits until the next record with that header arrives,
+ * which completes the pair (the waiting record is mate 1) and frees the
+ * header.  Records that never pair are not counted.  Records are written with
+ * the shortened header.  Replaces BioBloomClassifier::filterPair(file) and
+ * filterPairPrint(file, type) (BioBloomClassifier.cpp:463-564, 571-729).
+ */
+int bbt_filter_smart_pairs(bbt_ctx *ctx, const char *file, const char *prefix,
+		const char *read_status);
+int bbt_filter_smart_pairs_print(bbt_ctx *ctx, const char *file, const char *prefix,
+		const char *out_type, const char *postfix, const char *read_status);
+
 /* -d / -n: the file pipelines also print, as FASTQ on stdout, each read (both
  * mates of a pair) whose category is the first filter (inverse: every other
- * category).  Replaces BioBloomClassifier::setStdout and printSingle /
+ * category; BESTHIT adds the read's best score to the first filter's reads).  Replaces BioBloomClassifier::setStdout and printSingle /
  * printPair (BioBloomClassifier.h:81-83, 115-142, 211-247). */
 int bbt_set_stdout(bbt_ctx *ctx, int on, int inverse);
 
@@ -189,6 +218,42 @@ int bbt_set_stdout(bbt_ctx *ctx, int on, int inverse);
  * lists) instead of both (intersection, the default).
  * Replaces BioBloomClassifier::setInclusive (BioBloomClassifier.h:77-79). */
 int bbt_set_inclusive(bbt_ctx *ctx, int inclusive);
+
+/*
+ * Filtering mode (opt::mode, BioBloomCategorizer/Options.h:22-24), chosen in
+ * the reference by -c, -b and -w (BioBloomCategorizer.cpp:276-318, 460-464):
+ *   BBT_MODE_STD      every filter SeqEval::evalRead accepts
+ *                     (evaluateReadStd, BioBloomClassifier.cpp:1182-1189);
+ *   BBT_MODE_ORDERED  -c: only the first such filter in load order; pairs take
+ *                     the first filter both mates pass, or either mate with -i
+ *                     (evaluateReadOrdered / evaluateReadOrderedPair,
+ *                     BioBloomClassifier.cpp:1145-1180; setOrderedFilter,
+ *                     BioBloomClassifier.h:67-75);
+ *   BBT_MODE_BESTHIT  -b: no threshold; the filters whose SeqEval::evalScore is
+ *                     the largest, if that is above 0 (evaluateReadBestHit,
+ *                     BioBloomClassifier.cpp:1194-1218);
+ *   BBT_MODE_SCORES   -w: STD hits, and evalScore of every filter for the
+ *                     multiMatch output (evaluateReadScore, :1224-1237).
+ * Pairs outside ORDERED evaluate each mate alone, as in STD.  The hit words
+ * of bbt_result carry the mode's hits.  BESTHIT and ORDERED cannot be combined
+ * (the setting replaces the previous one).
+ */
+#define BBT_MODE_STD 0
+#define BBT_MODE_ORDERED 1
+#define BBT_MODE_BESTHIT 2
+#define BBT_MODE_SCORES 3
+int bbt_set_mode(bbt_ctx *ctx, int mode);
+
+/*
+ * bbt_classify_batch that also returns evalScore (Common/SeqEval.h:534-560)
+ * of every read against every filter: scores (scores2 for the mates) hold
+ * n_reads x n_filters doubles, read-major, in result->location memory.  The
+ * score of the scoring method in use: SIMPLE and HARMONIC sums divided by
+ * len - k + 1, the final match length for LENGTH, -10 log10 of the binomial
+ * tail for BINOMIAL.  Any mode; the hit words and summary follow the mode.
+ */
+int bbt_classify_batch_scores(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *result,
+		double *scores, double *scores2, void *stream);
 
 /* Kernel path and launch shape (BBT_PATH_*, warps per block 4 or 8, frames
  * per lane when hashing 4 or 8); 0 keeps the current value.  Used by the

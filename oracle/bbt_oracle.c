@@ -636,6 +636,149 @@ int oracle_eval_min_match_len(const char *seq, size_t len,
 /* ------------------------------------------------------------------------ */
 
 /* BioBloomClassifier::evaluateReadStd (BioBloomClassifier.cpp:1182-1189). */
+/* boost's cdf(complement(binomial(n, p), x)) = P(X > x), summed from the top
+ * of the tail down (SeqEval::calcProbMatches, Common/SeqEval.h:209-216). */
+double oracle_binom_sf(unsigned n, double p, unsigned x)
+{
+	double tail = 0.0;
+	for (double i = n; i > (double)x; i -= 1.0)
+		tail += binom_pmf(n, p, i);
+	return tail;
+}
+
+/* SeqEval::evalScore (Common/SeqEval.h:534-560), without dust/subtract:
+ * evalSimpleScore (:334-376), evalHarmonicScore (:378-419),
+ * evalMinMatchLenScore (:421-448) and evalBinomialScore (:450-491) followed by
+ * log10(...) * -10.  fpr is the filter's getFPRPrecompute (BINOMIAL only). */
+double oracle_eval_score(const char *seq, size_t len, const oracle_bf *bf, int scoring,
+		unsigned streak_threshold, double fpr)
+{
+	oracle_ntitr it;
+	if (scoring == ORACLE_LENGTH) {
+		unsigned match_len = 0, prev = 0;
+		oracle_ntitr_init(&it, seq, len, bf->h, bf->k);
+		while (!oracle_ntitr_end(&it)) {
+			if (it.pos != (size_t)prev + 1)
+				match_len = 0;
+			if (oracle_bf_contains(bf, it.hv, NULL))
+				match_len = match_len == 0 ? bf->k : match_len + 1;
+			else
+				match_len = 0;
+			prev = (unsigned)it.pos;
+			oracle_ntitr_next(&it);
+		}
+		return (double)match_len;
+	}
+	if (scoring == ORACLE_BINOMIAL && len < bf->k)
+		return log10(1.0) * -10;
+	double score = 0;
+	unsigned streak = 0, prev = 0;
+	oracle_ntitr_init(&it, seq, len, bf->k, bf->k);
+	while (!oracle_ntitr_end(&it)) {
+		if (it.pos != (size_t)prev + 1)
+			streak = 0;
+		if (oracle_bf_contains(bf, it.hv, NULL)) {
+			if (scoring == ORACLE_BINOMIAL)
+				score += 1;
+			else if (streak == 0)
+				score += 0.5;
+			else if (scoring == ORACLE_HARMONIC)
+				score += 1.0 - 1.0 / (1.0 + (double)streak);
+			else
+				score += 1;
+			prev = (unsigned)it.pos;
+			oracle_ntitr_next(&it);
+			++streak;
+		} else {
+			if (streak < streak_threshold) {
+				prev = (unsigned)it.pos;
+				oracle_ntitr_next(&it);
+			} else {
+				unsigned skip_end = (unsigned)it.pos + bf->k;
+				while (it.pos < skip_end) {
+					prev = (unsigned)it.pos;
+					oracle_ntitr_next(&it);
+				}
+			}
+			streak = 0;
+		}
+	}
+	if (scoring == ORACLE_BINOMIAL) {
+		const unsigned frame_len = (unsigned)(len - bf->k + 1);
+		return log10(oracle_binom_sf(frame_len, fpr, (unsigned)score)) * -10;
+	}
+	/* normalizeScore (:33-35): the divisor in size_t arithmetic */
+	return score / (double)(len - bf->k + 1);
+}
+
+void oracle_classify_scores(const char *seq, const uint64_t *off, size_t n,
+		const oracle_bf *const *filters, unsigned nf, int scoring,
+		unsigned streak_threshold, double *scores)
+{
+	for (size_t r = 0; r < n; ++r) {
+		const char *s = seq + off[r];
+		size_t len = (size_t)(off[r + 1] - off[r]);
+		for (unsigned f = 0; f < nf; ++f) {
+			double fpr = scoring == ORACLE_BINOMIAL ? oracle_bf_fpr(filters[f]) : 0.0;
+			scores[r * nf + f] = oracle_eval_score(s, len, filters[f], scoring,
+					streak_threshold, fpr);
+		}
+	}
+}
+
+/* BioBloomClassifier::evaluateReadBestHit (BioBloomClassifier.cpp:1194-1218)
+ * over one read's scores: the filters of the largest score (a larger score
+ * replaces the list, an equal one joins it), kept only when that score is
+ * above 0.  Returns the largest score (0 when none is above 0). */
+double oracle_best_hit(const double *scores, unsigned nf, uint64_t *hits)
+{
+	unsigned words = (nf + 63) / 64;
+	double max_score = 0;
+	memset(hits, 0, words * sizeof(uint64_t));
+	for (unsigned f = 0; f < nf; ++f) {
+		double sc = scores[f];
+		if (max_score < sc) {
+			max_score = sc;
+			memset(hits, 0, words * sizeof(uint64_t));
+			hits[f >> 6] |= 1ULL << (f & 63);
+		} else if (max_score == sc) {
+			hits[f >> 6] |= 1ULL << (f & 63);
+		}
+	}
+	if (!(max_score > 0))
+		memset(hits, 0, words * sizeof(uint64_t));
+	return max_score;
+}
+
+/* evaluateReadOrdered / evaluateReadOrderedPair (BioBloomClassifier.cpp:
+ * 1145-1180) from the STD hit words: the first filter the read passes (pairs:
+ * that both mates pass, or either with inclusive) is the only hit, of both
+ * mates.  hits2 may be NULL (single end). */
+void oracle_ordered(uint64_t *hits1, uint64_t *hits2, unsigned nf, int inclusive)
+{
+	unsigned words = (nf + 63) / 64, f = nf;
+	for (unsigned i = 0; i < nf; ++i) {
+		int a = (int)((hits1[i >> 6] >> (i & 63)) & 1);
+		int pass = a;
+		if (hits2) {
+			int b = (int)((hits2[i >> 6] >> (i & 63)) & 1);
+			pass = inclusive ? (a || b) : (a && b);
+		}
+		if (pass) {
+			f = i;
+			break;
+		}
+	}
+	memset(hits1, 0, words * sizeof(uint64_t));
+	if (hits2)
+		memset(hits2, 0, words * sizeof(uint64_t));
+	if (f < nf) {
+		hits1[f >> 6] |= 1ULL << (f & 63);
+		if (hits2)
+			hits2[f >> 6] |= 1ULL << (f & 63);
+	}
+}
+
 void oracle_classify(const char *seq, const uint64_t *off, size_t n,
 		const oracle_bf *const *filters, unsigned nf, double threshold,
 		unsigned streak_threshold, int scoring, uint64_t *hits,

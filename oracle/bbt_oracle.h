@@ -149,6 +149,17 @@ void oracle_classify(const char *seq, const uint64_t *off, size_t n,
 		unsigned streak_threshold, int scoring, uint64_t *hits,
 		uint64_t *probes);
 
+/* Exhaustive scores (SeqEval::evalScore, Common/SeqEval.h:534-560) and the
+ * modes built on them and on the STD hits: BESTHIT, ORDERED. */
+double oracle_binom_sf(unsigned n, double p, unsigned x);
+double oracle_eval_score(const char *seq, size_t len, const oracle_bf *bf, int scoring,
+		unsigned streak_threshold, double fpr);
+void oracle_classify_scores(const char *seq, const uint64_t *off, size_t n,
+		const oracle_bf *const *filters, unsigned nf, int scoring,
+		unsigned streak_threshold, double *scores);
+double oracle_best_hit(const double *scores, unsigned nf, uint64_t *hits);
+void oracle_ordered(uint64_t *hits1, uint64_t *hits2, unsigned nf, int inclusive);
+
 /* Summary accounting (ResultsManager.hpp:66-189).  counts has nf+2 entries
  * of aboveThreshold then nf+2 entries of unique, then multiMatch, noMatch.
  * Returns the category index (filter, nf = noMatch, nf+1 = multiMatch). */

@@ -10,6 +10,11 @@
  *       (for pairs: "<hits1>|<hits2>").  Then prints "#SUMMARY" and the
  *       ResultsManager summary text (ResultsManager.hpp:191-237), computed
  *       by the reference's own ResultsManager.
+ *   ref_harness scores METHOD STREAK FILTER.bf[,FILTER.bf...] READS
+ *       For every read, prints "<name>\t<s0>,<s1>,..." where s_f is
+ *       SeqEval::evalScore (Common/SeqEval.h:534-560) of the read against
+ *       filter f under METHOD (simple, length, harmonic or binomial), as the
+ *       16 hex digits of the double's bits.
  *   ref_harness time  SCORE STREAK THREADS INCLUSIVE PREFIX FILTERS READS [READS2]
  *       Builds a BioBloomClassifier (BioBloomClassifier.cpp:21-28; filter
  *       load not timed), then times filter()/filterPair() and prints one JSON
@@ -25,6 +30,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -135,6 +141,48 @@ static int mode_hits(int argc, char **argv)
 	return 0;
 }
 
+static int mode_scores(int argc, char **argv)
+{
+	if (argc < 6) {
+		fprintf(stderr, "usage: ref_harness scores METHOD STREAK FILTERS READS\n");
+		return 2;
+	}
+	string method = argv[2];
+	if (method == "length")
+		opt::scoringMethod = opt::LENGTH;
+	else if (method == "harmonic")
+		opt::scoringMethod = opt::HARMONIC;
+	else if (method == "binomial")
+		opt::scoringMethod = opt::BINOMIAL;
+	else
+		opt::scoringMethod = opt::SIMPLE;
+	opt::streakThreshold = (unsigned)atoi(argv[3]);
+	vector<string> paths = split_commas(argv[4]);
+	vector<BloomFilter *> filters;
+	for (size_t i = 0; i < paths.size(); ++i)
+		filters.push_back(new BloomFilter(paths[i]));
+	gzFile fp = gzopen(argv[5], "r");
+	if (fp == Z_NULL) {
+		fprintf(stderr, "cannot open reads\n");
+		return 1;
+	}
+	kseq_t *k = kseq_init(fp);
+	for (int l; (l = kseq_read(k)) >= 0;) {
+		string seq(k->seq.s, l);
+		printf("%s\t", k->name.s);
+		for (unsigned f = 0; f < filters.size(); ++f) {
+			double v = SeqEval::evalScore(seq, *filters[f]);
+			unsigned long long bits;
+			memcpy(&bits, &v, sizeof bits);
+			printf("%s%016llx", f ? "," : "", bits);
+		}
+		printf("\n");
+	}
+	kseq_destroy(k);
+	gzclose(fp);
+	return 0;
+}
+
 static size_t count_records(const char *path)
 {
 	gzFile fp = gzopen(path, "r");
@@ -191,6 +239,8 @@ int main(int argc, char **argv)
 		return mode_hits(argc, argv);
 	if (mode == "time")
 		return mode_time(argc, argv);
+	if (mode == "scores")
+		return mode_scores(argc, argv);
 	fprintf(stderr, "unknown mode %s\n", argv[1]);
 	return 2;
 }

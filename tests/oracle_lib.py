@@ -74,6 +74,15 @@ def lib():
         L.oracle_calc_min_count.argtypes = [u32, dbl, dbl]
         L.oracle_classify.argtypes = [ctypes.c_char_p, P(u64), sz, P(P(_BF)), u32, dbl, u32,
                                       ctypes.c_int, P(u64), P(u64)]
+        L.oracle_binom_sf.restype = dbl
+        L.oracle_binom_sf.argtypes = [u32, dbl, u32]
+        L.oracle_eval_score.restype = dbl
+        L.oracle_eval_score.argtypes = [ctypes.c_char_p, sz, P(_BF), ctypes.c_int, u32, dbl]
+        L.oracle_classify_scores.argtypes = [ctypes.c_char_p, P(u64), sz, P(P(_BF)), u32,
+                                             ctypes.c_int, u32, P(dbl)]
+        L.oracle_best_hit.restype = dbl
+        L.oracle_best_hit.argtypes = [P(dbl), u32, P(u64)]
+        L.oracle_ordered.argtypes = [P(u64), P(u64), u32, ctypes.c_int]
         L.oracle_update_summary.restype = u32
         L.oracle_update_summary.argtypes = [P(u64), u32, P(u64)]
         L.oracle_update_summary_pair.restype = u32
@@ -201,6 +210,48 @@ def classify(seq_bytes, offsets, filters, threshold=0.15, streak=3, scoring=SIMP
     lib().oracle_classify(seq_bytes, _u64p(off), n, arr, nf, threshold, streak, scoring,
                           _u64p(hits), ctypes.byref(probes) if count_probes else None)
     return hits, probes.value
+
+
+def classify_scores(seq_bytes, offsets, filters, scoring=SIMPLE, streak=3):
+    """SeqEval::evalScore of every read against every filter: (n, nf) float64."""
+    n = len(offsets) - 1
+    nf = len(filters)
+    out = np.zeros((n, nf), dtype=np.float64)
+    arr = (ctypes.POINTER(_BF) * nf)(*[ctypes.pointer(f.bf) for f in filters])
+    off = np.ascontiguousarray(offsets, dtype=np.uint64)
+    lib().oracle_classify_scores(seq_bytes, _u64p(off), n, arr, nf, scoring, streak,
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return out
+
+
+def best_hit(scores):
+    """evaluateReadBestHit over (n, nf) scores: hit words (n, words) and the
+    largest score per read."""
+    n, nf = scores.shape
+    words = (nf + 63) // 64
+    hits = np.zeros((n, words), dtype=np.uint64)
+    best = np.zeros(n, dtype=np.float64)
+    for i in range(n):
+        row = np.ascontiguousarray(scores[i])
+        h = np.zeros(words, dtype=np.uint64)
+        best[i] = lib().oracle_best_hit(row.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), nf,
+                                        _u64p(h))
+        hits[i] = h
+    return hits, best
+
+
+def ordered(hits, nf, hits2=None, inclusive=False):
+    """evaluateReadOrdered(Pair) from STD hit words; returns new arrays."""
+    h1 = np.array(hits, dtype=np.uint64, copy=True)
+    h2 = None if hits2 is None else np.array(hits2, dtype=np.uint64, copy=True)
+    for i in range(len(h1)):
+        r1 = np.ascontiguousarray(h1[i])
+        r2 = None if h2 is None else np.ascontiguousarray(h2[i])
+        lib().oracle_ordered(_u64p(r1), None if r2 is None else _u64p(r2), nf, int(inclusive))
+        h1[i] = r1
+        if h2 is not None:
+            h2[i] = r2
+    return h1, h2
 
 
 def summary_counts(hits, nf, hits2=None, inclusive=False):
