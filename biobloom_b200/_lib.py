@@ -159,6 +159,7 @@ def lib():
         "bbt_filter_smart_pairs_print": (i32, [vp, cp, cp, cp, cp, cp]),
         "bbt_set_stdout": (i32, [vp, i32, i32]),
         "bbt_set_mode": (i32, [vp, i32]),
+        "bbt_set_dust": (i32, [vp, i32, u32, u32]),
         "bbt_classify_batch_scores": (i32, [vp, P(Batch), P(Result), vp, vp, vp]),
         "bbt_last_stats": (i32, [vp, P(Stats)]),
         "bbt_set_counting": (i32, [vp, i32]),

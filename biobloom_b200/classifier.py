@@ -95,6 +95,11 @@ class BioBloomClassifier:
         others) to stdout; BioBloomClassifier::setStdout (BioBloomClassifier.h:81-83)."""
         L.check(L.lib().bbt_set_stdout(self._ctx, 1, int(bool(inverse))), self._ctx)
 
+    def set_dust(self, on=True, T=20, W=64):
+        """-D (-T, -W): SDUST masking of low-complexity frames before every
+        evaluation (opt::dust, Common/SDust.hpp)."""
+        L.check(L.lib().bbt_set_dust(self._ctx, int(bool(on)), int(T), int(W)), self._ctx)
+
     def set_mode(self, mode):
         """opt::mode: MODE_STD, MODE_ORDERED (-c), MODE_BESTHIT (-b) or
         MODE_SCORES (-w)."""

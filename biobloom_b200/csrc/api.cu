@@ -134,6 +134,11 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 		cudaFree(w);
 	cudaFree(ctx->d_filters);
 	cudaFree(ctx->d_fpr);
+	cudaFree(ctx->d_dust[0]);
+	cudaFree(ctx->d_dust[1]);
+	cudaFree(ctx->d_dust_redo);
+	cudaFree(ctx->d_dust_cnt);
+	cudaFree(ctx->d_dust_scratch);
 	cudaFree(ctx->d_counts);
 	cudaFree(ctx->d_work);
 	cudaFree(ctx->d_order);
@@ -670,12 +675,70 @@ static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 	return BBT_OK;
 }
 
+/* -D: the SDUST masks of a batch's reads (dust.cu) into ctx->d_dust, set in
+ * a.dust.  mate_bases: bases of each mate array counted from its off_base. */
+static int run_dust(bbt_ctx *ctx, ClassifyArgs &a, const uint64_t *mate_bases, cudaStream_t s)
+{
+	DustArgs d;
+	memset(&d, 0, sizeof d);
+	for (uint32_t m = 0; m < a.mates; ++m) {
+		const uint64_t words = mate_bases[m] / 32 + 2;
+		int rc = grow(ctx, &ctx->d_dust[m], ctx->dust_words_cap[m], words);
+		if (rc)
+			return rc;
+		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_dust[m], 0, words * sizeof(uint32_t), s));
+		d.seq[m] = a.seq[m];
+		d.off[m] = a.off[m];
+		d.off_base[m] = a.off_base[m];
+		d.mask[m] = ctx->d_dust[m];
+	}
+	int rc = grow(ctx, &ctx->d_dust_redo, ctx->dust_redo_cap, a.n * a.mates);
+	if (rc)
+		return rc;
+	CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_dust_cnt, 0, sizeof(unsigned long long), s));
+	d.n = a.n;
+	d.mates = a.mates;
+	d.T = ctx->dust_T;
+	d.W = ctx->dust_W;
+	d.redo = ctx->d_dust_redo;
+	d.redo_count = ctx->d_dust_cnt;
+	d.failed = ctx->d_dust_cnt + 1;
+	d.scratch = ctx->d_dust_scratch;
+	d.scratch_per_thread = ctx->dust_per_thread;
+	CUDA_TRY(ctx, launch_dust_pass1(d, ctx->num_sms, s));
+	CUDA_TRY(ctx, launch_dust_pass2(d, ctx->dust_threads2, s));
+	a.dust[0] = ctx->d_dust[0];
+	a.dust[1] = a.mates == 2 ? ctx->d_dust[1] : nullptr;
+	ctx->last.kernels += 2;
+	return BBT_OK;
+}
+
+/* -D: after the stream has finished a call's batches, fail the call if a
+ * read's masking did not fit pass 2's scratch. */
+static int dust_check(bbt_ctx *ctx)
+{
+	unsigned long long failed = 0;
+	CUDA_TRY(ctx, cudaMemcpy(&failed, ctx->d_dust_cnt + 1, sizeof failed, cudaMemcpyDeviceToHost));
+	if (failed)
+		return fail(ctx, BBT_ERR_UNSUPPORTED,
+				"DUST: " + std::to_string(failed) + " read(s) held more pending low-complexity "
+				"intervals than the masking kernel's scratch");
+	return BBT_OK;
+}
+
 /* classify + summarize one staged or device-resident batch on stream s;
  * scores (optional, per mate array): evalScore of every filter */
 static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStream_t s,
-		double *const *scores = nullptr)
+		double *const *scores = nullptr, const uint64_t *mate_bases = nullptr)
 {
 	ctx->last.kernels = 2; /* classification (counted below for two-pass) + summary */
+	if (ctx->dust) {
+		if (!mate_bases)
+			return fail(ctx, BBT_ERR_UNSUPPORTED, "DUST masking needs the batch's base counts");
+		int rc = run_dust(ctx, a, mate_bases, s);
+		if (rc)
+			return rc;
+	}
 	ScoreArgs sa;
 	sa.scores[0] = scores ? scores[0] : nullptr;
 	sa.scores[1] = scores && a.mates == 2 ? scores[1] : nullptr;
@@ -683,7 +746,7 @@ static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStrea
 	sa.besthit = 0;
 	const bool want_scores = sa.scores[0] || sa.scores[1];
 	const bool two_pass = ctx->lc.path == BBT_PATH_FILTER_MAJOR && ctx->same_k &&
-			ctx->p.scoring <= BBT_SCORE_LENGTH;
+			ctx->p.scoring <= BBT_SCORE_LENGTH && !ctx->dust;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k0, s));
 	if (ctx->mode == BBT_MODE_BESTHIT) {
 		/* the hit words are the filters of the largest score */
@@ -770,11 +833,35 @@ static int classify_device(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r, cuda
 	}
 	a.hits[0] = r->hits ? r->hits : ctx->d_tmp_hits[0];
 	a.hits[1] = paired ? (r->hits2 ? r->hits2 : ctx->d_tmp_hits[1]) : nullptr;
+	uint64_t mate_bases[2] = {0, 0};
+	if (ctx->dust) {
+		if (ctx->capturing)
+			return fail(ctx, BBT_ERR_UNSUPPORTED, "DUST masking cannot be captured in a graph");
+		/* the mask arrays are sized by the batch's bases (a short host wait) */
+		for (uint32_t m = 0; m < a.mates; ++m) {
+			uint64_t ends[2];
+			CUDA_TRY(ctx, cudaMemcpyAsync(&ends[0], a.off[m], sizeof(uint64_t),
+					cudaMemcpyDeviceToHost, s));
+			CUDA_TRY(ctx, cudaMemcpyAsync(&ends[1], a.off[m] + b->n_reads, sizeof(uint64_t),
+					cudaMemcpyDeviceToHost, s));
+			CUDA_TRY(ctx, cudaStreamSynchronize(s));
+			a.off_base[m] = ends[0];
+			mate_bases[m] = ends[1] - ends[0];
+			a.seq[m] += ends[0]; /* bases indexed from offsets[0] */
+		}
+		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_dust_cnt + 1, 0, sizeof(unsigned long long), s));
+	}
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, s));
-	int rc = run_kernels(ctx, a, r->category, s, scores);
+	int rc = run_kernels(ctx, a, r->category, s, scores, mate_bases);
 	if (rc)
 		return rc;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, s));
+	if (ctx->dust) {
+		CUDA_TRY(ctx, cudaStreamSynchronize(s));
+		rc = dust_check(ctx);
+		if (rc)
+			return rc;
+	}
 	ctx->reads_seen += b->n_reads;
 	ctx->last.reads = b->n_reads * a.mates;
 	return BBT_OK;
@@ -812,6 +899,9 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 	}
 	uint64_t i0 = 0;
 	int which = 0;
+	if (ctx->dust)
+		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_dust_cnt + 1, 0, sizeof(unsigned long long),
+				ctx->stream));
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
 	while (i0 < n) {
 		/* largest i1 with bases and reads inside the slot capacity */
@@ -855,10 +945,12 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 		ClassifyArgs a = base_args(ctx);
 		a.n = cnt;
 		a.mates = paired ? 2 : 1;
+		uint64_t mate_bases[2] = {0, 0};
 		for (int m = 0; m < (paired ? 2 : 1); ++m) {
 			const char *seq = m ? b->seq2 : b->seq;
 			const uint64_t *off = m ? b->offsets2 : b->offsets;
 			const uint64_t lo = off[i0], hi = off[i1];
+			mate_bases[m] = hi - lo;
 			if (hi > lo)
 				CUDA_TRY(ctx, cudaMemcpyAsync(s.d_seq[m], seq + lo, hi - lo,
 						cudaMemcpyHostToDevice, ctx->h2d));
@@ -882,7 +974,8 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 			slot_scores[0] = scores[0] ? s.d_scores[0] : nullptr;
 			slot_scores[1] = paired && scores[1] ? s.d_scores[1] : nullptr;
 		}
-		int rc = run_kernels(ctx, a, s.d_cat, ctx->stream, want_scores ? slot_scores : nullptr);
+		int rc = run_kernels(ctx, a, s.d_cat, ctx->stream, want_scores ? slot_scores : nullptr,
+				mate_bases);
 		if (rc)
 			return rc;
 		CUDA_TRY(ctx, cudaEventRecord(s.computed, ctx->stream));
@@ -911,6 +1004,11 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 	CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
 	for (Slot &s : ctx->slot)
 		s.used = false;
+	if (ctx->dust) {
+		int rc = dust_check(ctx);
+		if (rc)
+			return rc;
+	}
 	ctx->reads_seen += n;
 	ctx->last.reads = n * (paired ? 2 : 1);
 	return BBT_OK;
@@ -951,6 +1049,44 @@ extern "C" int bbt_classify_batch_scores(bbt_ctx *ctx, const bbt_batch *batch,
 		return fail(ctx, BBT_ERR_ARG, "bbt_classify_batch_scores: pairs need scores2 too");
 	double *sc[2] = {scores, batch && batch->seq2 ? scores2 : nullptr};
 	return classify_batch(ctx, batch, result, stream, sc, "bbt_classify_batch_scores");
+}
+
+extern "C" int bbt_set_dust(bbt_ctx *ctx, int on, unsigned T, unsigned W)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	if (!on) {
+		ctx->dust = false;
+		return BBT_OK;
+	}
+	if (W < 3 || W > (unsigned)kDustMaxWindow)
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_dust: the window W must be in [3, " +
+				std::to_string(kDustMaxWindow) + "]");
+	if (T > 100000)
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_dust: T must be at most 100000");
+	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
+	CUDA_TRY(ctx, cudaDeviceSynchronize());
+	/* pass-2 scratch: any read's perfect intervals fit in W^2 + 2W + 64 entries;
+	 * as many threads as fit in 256 MB (at least 32) */
+	const uint64_t per = (uint64_t)W * W + 2ull * W + 64;
+	const uint64_t bytes_per = per * dust_perfect_bytes();
+	uint64_t threads = (256ull << 20) / bytes_per;
+	threads = std::max<uint64_t>(32, std::min<uint64_t>(2048, threads / 32 * 32));
+	if (per != ctx->dust_per_thread || threads != ctx->dust_threads2) {
+		cudaFree(ctx->d_dust_scratch);
+		ctx->d_dust_scratch = nullptr;
+		ctx->dust_per_thread = 0;
+		ctx->dust_threads2 = 0;
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_dust_scratch, threads * bytes_per));
+		ctx->dust_per_thread = per;
+		ctx->dust_threads2 = (uint32_t)threads;
+	}
+	if (!ctx->d_dust_cnt)
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_dust_cnt, 2 * sizeof(unsigned long long)));
+	ctx->dust = true;
+	ctx->dust_T = (int)T;
+	ctx->dust_W = (int)W;
+	return BBT_OK;
 }
 
 extern "C" int bbt_set_mode(bbt_ctx *ctx, int mode)
@@ -1240,6 +1376,9 @@ extern "C" int bbt_graph_create(bbt_ctx *ctx, const bbt_batch *b, const bbt_resu
 	if (ctx->lc.path == BBT_PATH_FILTER_MAJOR)
 		return fail(ctx, BBT_ERR_UNSUPPORTED, "bbt_graph_create: the filter-major path reads "
 				"block sums on the host; use the plain or persistent path in a graph");
+	if (ctx->dust)
+		return fail(ctx, BBT_ERR_UNSUPPORTED, "bbt_graph_create: DUST masking sizes its "
+				"buffers on the host and cannot be captured");
 	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
 	const uint64_t n = b->n_reads;
 	const uint64_t chunk = reads_per_launch ? std::min(reads_per_launch, std::max<uint64_t>(n, 1))
@@ -1370,6 +1509,8 @@ int bbt::bf_classify_slot(bbt_ctx *ctx, const uint8_t *seq, const uint64_t *off,
 	a.hits[0] = hits;
 	a.hits[1] = paired ? hits2 : nullptr;
 	a.work = sc.work;
+	if (ctx->dust)
+		return fail(ctx, BBT_ERR_UNSUPPORTED, "the serving engine does not run DUST masking");
 	LaunchConfig lc = ctx->lc;
 	lc.count = 0;
 	if (lc.path == BBT_PATH_FILTER_MAJOR)

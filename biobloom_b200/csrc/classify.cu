@@ -101,7 +101,8 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 					V &= (1u << nfc) - 1u;
 				const bool v = (V >> lane) & 1u;
 				const bool probe = v && (length_mode ||
-						p >= (seq_mode ? (int32_t)seq_probe_from(qs) : st.skip_until));
+						p >= (seq_mode ? (int32_t)seq_probe_from(qs) : st.skip_until)) &&
+						!dust_low(a.dust[mate], start + (uint64_t)p);
 				const unsigned r0 = reads;
 				const bool hit = probe && contains(F, win.h0[q], reads);
 				const uint32_t H = __ballot_sync(kFull, hit);

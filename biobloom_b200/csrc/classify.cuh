@@ -36,6 +36,8 @@ struct ClassifyArgs {
 	const uint32_t *bthres;    /* BINOMIAL: accept threshold of filter f for a read of
 	                              n frames at bthres[f * bthres_rows + n] */
 	uint64_t bthres_rows;
+	const uint32_t *dust[2];   /* -D: bit g set when base g of the mate array lies in a
+	                              masked low-complexity interval (dust.cu); NULL = off */
 	int tight_steps;           /* SIMPLE scoring: size probe steps by the frames that could
 	                              still accept the read (seqeval_chunk.cuh,
 	                              simple_step_frames) instead of 32 frames per step */
@@ -43,6 +45,13 @@ struct ClassifyArgs {
 	unsigned long long *frames;/* optional: frames hashed */
 	unsigned long long *alg_probes; /* optional: words the sequential algorithm reads */
 };
+
+/* -D: the frame starting at base g of a mate array is masked (a miss that is
+ * not probed, SeqEval's sduster->isLowComp test). */
+__device__ __forceinline__ bool dust_low(const uint32_t *mask, uint64_t g)
+{
+	return mask && ((mask[g >> 5] >> (g & 31u)) & 1u);
+}
 
 struct LaunchConfig {
 	int path;             /* BBT_PATH_PLAIN or BBT_PATH_PERSISTENT */

@@ -10,8 +10,7 @@
  * "<read>\t<category>" line per read (pair).  --fa / --fq (with -g) write the
  * reads of each category to their own files, -d / -n print the first filter's
  * reads (or all others) to stdout; -c, -b and -w select the ordered, best-hit
- * and with-scores modes.  DUST masking (-D, -T, -W) is refused with a message
- * instead of being ignored.
+ * and with-scores modes, -D (with -T, -W) SDUST low-complexity masking.
  */
 #include <getopt.h>
 #include <sys/stat.h>
@@ -60,6 +59,9 @@ static void usage_exit(int code)
 	        "  -S, --score_type=N     harmonic or binomial scoring.\n"
 	        "  -r, --streak=N         Hits tiling in second pass needed to jump several tiles\n"
 	        "                         upon a miss. [3]\n"
+	        "  -D, --dust             Filter using dust.\n"
+	        "  -T, --T_dust           T parameter for dust. [20]\n"
+	        "  -W, --window_dust      Window size for dust. [64]\n"
 	        "  -I, --interval         Accepted for compatibility.\n"
 	        "      --read_status=F    Write one '<read>\\t<category>' line per read to F.\n"
 	        "      --device=N         CUDA device ordinal. [0]\n"
@@ -93,9 +95,10 @@ int main(int argc, char **argv)
 	bool paired = false, die = false, to_stdout = false, inverse = false, collab = false;
 	int mode = BBT_MODE_STD;
 	string file_list;
+	bool dust = false;
+	unsigned dust_T = 20, dust_W = 64; /* Common/Options.cpp:36-38 */
 	int fastq = 0, fasta = 0, verbose = 0;
 	int device = 0;
-	string unsupported;
 	enum { OPT_READ_STATUS = 1000, OPT_DEVICE };
 	static struct option long_options[] = {
 		{"prefix", required_argument, NULL, 'p'},
@@ -193,9 +196,18 @@ int main(int argc, char **argv)
 				die = true;
 			}
 			break;
-		case 'D': case 'T': case 'W': case 'o':
-			unsupported += string(" -") + (char)c;
+		case 'D': dust = true; break;
+		case 'T': {
+			stringstream conv(optarg);
+			conv >> dust_T;
 			break;
+		}
+		case 'W': {
+			stringstream conv(optarg);
+			conv >> dust_W;
+			break;
+		}
+		case 'o': break; /* --min_hit_only: accepted and ignored, as upstream */
 		case OPT_READ_STATUS: read_status = optarg; break;
 		case OPT_DEVICE: device = atoi(optarg); break;
 		case '?': die = true; break;
@@ -242,10 +254,6 @@ int main(int argc, char **argv)
 	}
 	if (die) {
 		cerr << "Try '--help' for more information.\n";
-		exit(EXIT_FAILURE);
-	}
-	if (!unsupported.empty()) {
-		cerr << "Error: option(s)" << unsupported << " are not supported by this build" << endl;
 		exit(EXIT_FAILURE);
 	}
 	if (paired && !file_list.empty() && !out_type.empty()) {
@@ -315,6 +323,11 @@ int main(int argc, char **argv)
 		mode = BBT_MODE_ORDERED;
 	}
 	bbt_set_mode(ctx, mode);
+	if (dust && bbt_set_dust(ctx, 1, dust_T, dust_W) != BBT_OK) {
+		cerr << "Error: " << bbt_last_error(ctx) << endl;
+		bbt_close(ctx);
+		exit(1);
+	}
 	int rc = BBT_OK;
 	const char *rs = read_status.empty() ? nullptr : read_status.c_str();
 	if (to_stdout)

@@ -12,6 +12,7 @@
 
 #include "bbt.h"
 #include "classify.cuh"
+#include "dust.cuh"
 
 namespace bbt {
 
@@ -57,6 +58,17 @@ struct bbt_ctx {
 	/* filtering mode (BBT_MODE_*): ORDERED, BESTHIT and SCORES */
 	int mode = BBT_MODE_STD;
 	double *d_fpr = nullptr;         /* each filter's FPR on the device (BINOMIAL scores) */
+	/* -D: SDUST masking before classification (dust.cu) */
+	bool dust = false;
+	int dust_T = 20, dust_W = 64;
+	uint32_t *d_dust[2] = {nullptr, nullptr};  /* per-mate masked-base bits */
+	uint64_t dust_words_cap[2] = {0, 0};
+	uint64_t *d_dust_redo = nullptr;
+	uint64_t dust_redo_cap = 0;
+	unsigned long long *d_dust_cnt = nullptr;  /* reads queued for pass 2, reads failed */
+	void *d_dust_scratch = nullptr;
+	uint64_t dust_per_thread = 0;
+	uint32_t dust_threads2 = 0;
 	/* two-pass filter-major scratch: padded frame offsets, per-block sums,
 	 * per-frame canonical hashes and validity words of one sub-batch */
 	uint64_t *d_tp_local = nullptr;

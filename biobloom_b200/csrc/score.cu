@@ -122,7 +122,8 @@ __device__ void score_read(const ClassifyArgs &a, const ScoreArgs &sa, uint64_t 
 					if (nfc < 32)
 						V &= (1u << nfc) - 1u;
 					const bool v = (V >> lane) & 1u;
-					const bool probe = v && (MODE == SCORE_LENGTH || p >= st.skip_end);
+					const bool probe = v && (MODE == SCORE_LENGTH || p >= st.skip_end) &&
+							!dust_low(a.dust[mate], start + (uint64_t)p);
 					const bool hit = probe && contains(F, win.h0[q], reads);
 					const uint32_t H = __ballot_sync(kFull, hit);
 					score_chunk(st, V, H, (int64_t)w0 + c, nfc, (int)k, a.streak_thr, MODE);

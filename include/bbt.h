@@ -245,6 +245,17 @@ int bbt_set_inclusive(bbt_ctx *ctx, int inclusive);
 int bbt_set_mode(bbt_ctx *ctx, int mode);
 
 /*
+ * -D / -T / -W: SDUST low-complexity masking (Common/sdust.c through
+ * Common/SDust.hpp; options BioBloomCategorizer.cpp:323-337, defaults T = 20,
+ * W = 64 in Common/Options.cpp:36-38).  Every evaluation then treats a frame
+ * whose first base lies in a masked interval of its read as a miss that is not
+ * probed, in all scoring methods and modes.  W must be in [3, 1024].  Calls
+ * with masking wait for their stream before returning; the serving engine and
+ * CUDA graphs refuse it.
+ */
+int bbt_set_dust(bbt_ctx *ctx, int on, unsigned T, unsigned W);
+
+/*
  * bbt_classify_batch that also returns evalScore (Common/SeqEval.h:534-560)
  * of every read against every filter: scores (scores2 for the mates) hold
  * n_reads x n_filters doubles, read-major, in result->location memory.  The

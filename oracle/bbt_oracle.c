@@ -373,8 +373,264 @@ int oracle_write_info(const char *path, const char *filter_id, unsigned k,
 /* SeqEval                                                                   */
 /* ------------------------------------------------------------------------ */
 
+/* ------------------------------------------------------------------------ */
+/* SDUST low-complexity masking (-D)                                         */
+/* ------------------------------------------------------------------------ */
+
+/*
+ * The symmetric DUST algorithm (Morgulis et al., "A fast and symmetric DUST
+ * implementation to mask low-complexity DNA sequences", J Comput Biol 2006)
+ * as the reference runs it: Common/sdust.c (sdust_core, shift_window,
+ * find_perfect, save_masked_regions), called once per evaluated read by
+ * Common/SDust.hpp with T = opt::dustT (20) and W = opt::dustWindow (64).
+ *
+ * Words are the triplets of consecutive A/C/G/T bases (any case).  The
+ * window holds the last W - 2 triplets; for a set of triplets the score is
+ * sum over triplet kinds of c(c-1)/2.  cw / rw count the whole window; cv /
+ * rv count its longest suffix of L triplets in which no triplet kind occurs
+ * more than 2T/10 times.  When 10 rw > L T the window may hold "perfect
+ * intervals": suffixes whose score r over length l has 10 r > T l and is at
+ * least that of every perfect interval starting inside them; those are kept,
+ * by descending start, in `perf`.  A perfect interval whose start falls out of
+ * the window is saved as masked, merged with the previous masked interval if
+ * they touch.  A non-ACGT base (and the end of the read) flushes all pending
+ * perfect intervals, but does not empty the window.
+ */
+typedef struct {
+	int start, finish, r, l;
+} dust_perfect;
+
+typedef struct {
+	int T, W;
+	int *ring;             /* window triplets, oldest first */
+	size_t head, size, cap;
+	int cw[64], cv[64];
+	int rw, rv, L;
+	dust_perfect *perf;    /* by descending start, then ascending finish */
+	size_t np, pcap;
+	uint64_t *res;         /* masked intervals: start << 32 | finish (exclusive) */
+	size_t nres, rcap;
+	size_t max_np;         /* largest perf size seen (capacity studies) */
+} dust_state;
+
+static int dust_code(unsigned char c)
+{
+	switch (c) {
+	case 'A': case 'a': return 0;
+	case 'C': case 'c': return 1;
+	case 'G': case 'g': return 2;
+	case 'T': case 't': return 3;
+	default: return 4;
+	}
+}
+
+static int dust_at(const dust_state *d, size_t i)
+{
+	return d->ring[(d->head + i) % d->cap];
+}
+
+static void dust_save(dust_state *d, int start)
+{
+	if (d->np == 0 || d->perf[d->np - 1].start >= start)
+		return;
+	const dust_perfect *p = &d->perf[d->np - 1];
+	int merged = 0;
+	if (d->nres) {
+		const int s = (int)(d->res[d->nres - 1] >> 32);
+		const int f = (int)(uint32_t)d->res[d->nres - 1];
+		if (p->start <= f) {
+			merged = 1;
+			d->res[d->nres - 1] = (uint64_t)s << 32 | (uint64_t)(f > p->finish ? f : p->finish);
+		}
+	}
+	if (!merged) {
+		if (d->nres == d->rcap) {
+			d->rcap = d->rcap ? 2 * d->rcap : 16;
+			d->res = (uint64_t *)realloc(d->res, d->rcap * sizeof(uint64_t));
+		}
+		d->res[d->nres++] = (uint64_t)p->start << 32 | (uint64_t)p->finish;
+	}
+	long i = (long)d->np - 1;
+	while (i >= 0 && d->perf[i].start < start)
+		--i;
+	d->np = (size_t)(i + 1);
+}
+
+static void dust_shift(dust_state *d, int t)
+{
+	if ((int)d->size >= d->W - 2) {
+		const int s = d->ring[d->head];
+		d->head = (d->head + 1) % d->cap;
+		--d->size;
+		d->rw -= --d->cw[s];
+		if (d->L > (int)d->size) {
+			--d->L;
+			d->rv -= --d->cv[s];
+		}
+	}
+	d->ring[(d->head + d->size) % d->cap] = t;
+	++d->size;
+	++d->L;
+	d->rw += d->cw[t]++;
+	d->rv += d->cv[t]++;
+	if (d->cv[t] * 10 > d->T * 2) {
+		int s;
+		do {
+			s = dust_at(d, d->size - (size_t)d->L);
+			d->rv -= --d->cv[s];
+			--d->L;
+		} while (s != t);
+	}
+}
+
+static void dust_find_perfect(dust_state *d, int start)
+{
+	int c[64];
+	memcpy(c, d->cv, sizeof c);
+	int r = d->rv, max_r = 0, max_l = 0;
+	for (long i = (long)d->size - d->L - 1; i >= 0; --i) {
+		const int t = dust_at(d, (size_t)i);
+		r += c[t]++;
+		const int new_r = r, new_l = (int)((long)d->size - i - 1);
+		if (new_r * 10 <= d->T * new_l)
+			continue;
+		size_t j = 0;
+		for (; j < d->np && d->perf[j].start >= (int)i + start; ++j) {
+			const dust_perfect *p = &d->perf[j];
+			if (max_r == 0 || p->r * max_l > max_r * p->l) {
+				max_r = p->r;
+				max_l = p->l;
+			}
+		}
+		if (max_r == 0 || new_r * max_l >= max_r * new_l) {
+			max_r = new_r;
+			max_l = new_l;
+			if (d->np == d->pcap) {
+				d->pcap = d->pcap ? 2 * d->pcap : 16;
+				d->perf = (dust_perfect *)realloc(d->perf, d->pcap * sizeof(dust_perfect));
+			}
+			memmove(d->perf + j + 1, d->perf + j, (d->np - j) * sizeof(dust_perfect));
+			++d->np;
+			d->perf[j].start = (int)i + start;
+			d->perf[j].finish = (int)d->size + 2 + start;
+			d->perf[j].r = new_r;
+			d->perf[j].l = new_l;
+			if (d->np > d->max_np)
+				d->max_np = d->np;
+		}
+	}
+}
+
+static void dust_run(dust_state *d, const char *seq, int len)
+{
+	int l = 0;
+	unsigned t = 0;
+	for (int i = 0; i <= len; ++i) {
+		const int b = i < len ? dust_code((unsigned char)seq[i]) : 4;
+		if (b < 4) {
+			++l;
+			t = (t << 2 | (unsigned)b) & 63u;
+			if (l >= 3) {
+				const int start = (l - d->W > 0 ? l - d->W : 0) + (i + 1 - l);
+				dust_save(d, start);
+				dust_shift(d, (int)t);
+				if (d->rw * 10 > d->L * d->T)
+					dust_find_perfect(d, start);
+			}
+		} else {
+			int start = (l - d->W + 1 > 0 ? l - d->W + 1 : 0) + (i + 1 - l);
+			while (d->np)
+				dust_save(d, start++);
+			l = 0;
+			t = 0;
+		}
+	}
+}
+
+static void dust_free(dust_state *d)
+{
+	free(d->ring);
+	free(d->perf);
+	free(d->res);
+}
+
+int oracle_sdust(const char *seq, size_t len, int T, int W, uint64_t *out, int cap,
+		int *max_perfect)
+{
+	dust_state d;
+	memset(&d, 0, sizeof d);
+	d.T = T;
+	d.W = W;
+	d.cap = W > 3 ? (size_t)W : 4;
+	d.ring = (int *)malloc(d.cap * sizeof(int));
+	dust_run(&d, seq, (int)len);
+	int n = (int)d.nres;
+	for (int i = 0; i < n && i < cap; ++i)
+		out[i] = d.res[i];
+	if (max_perfect)
+		*max_perfect = (int)d.max_np;
+	dust_free(&d);
+	return n;
+}
+
+/* -D: SeqEval's evaluation functions treat a frame whose start lies in a
+ * masked interval as a miss without probing the filter (the
+ * sduster->isLowComp(itr.pos()) test, Common/SeqEval.h:53,78,...). */
+static int g_dust = 0, g_dust_T = 20, g_dust_W = 64;
+
+void oracle_set_dust(int on, int T, int W)
+{
+	g_dust = on != 0;
+	g_dust_T = T;
+	g_dust_W = W;
+}
+
+/* SDust (Common/SDust.hpp): the masked intervals of one read and a cursor
+ * that only moves forward, as isLowComp assumes increasing positions. */
+typedef struct {
+	uint64_t *iv;
+	int n, cur;
+} dust_mask;
+
+static void dust_mask_init(dust_mask *m, const char *seq, size_t len)
+{
+	m->iv = NULL;
+	m->n = 0;
+	m->cur = 0;
+	if (!g_dust)
+		return;
+	dust_state d;
+	memset(&d, 0, sizeof d);
+	d.T = g_dust_T;
+	d.W = g_dust_W;
+	d.cap = g_dust_W > 3 ? (size_t)g_dust_W : 4;
+	d.ring = (int *)malloc(d.cap * sizeof(int));
+	dust_run(&d, seq, (int)len);
+	m->iv = d.res;
+	m->n = (int)d.nres;
+	d.res = NULL;
+	dust_free(&d);
+}
+
+static int dust_low(dust_mask *m, size_t pos)
+{
+	const unsigned p = (unsigned)pos;
+	while (m->cur < m->n && p >= (unsigned)m->iv[m->cur])
+		++m->cur;
+	return m->cur < m->n && p >= (unsigned)(m->iv[m->cur] >> 32) &&
+			p < (unsigned)m->iv[m->cur];
+}
+
+/* A frame's hit: not masked, and in the filter. */
+static int frame_hit(const oracle_bf *bf, const oracle_ntitr *it, dust_mask *m, uint64_t *probes)
+{
+	if (m->n && dust_low(m, it->pos))
+		return 0;
+	return oracle_bf_contains(bf, it->hv, probes);
+}
+
 /* SeqEval::evalSimple (Common/SeqEval.h:37-114), without dust/subtract. */
-int oracle_eval_simple(const char *seq, size_t len, const oracle_bf *bf,
+static int oracle_eval_simple_impl(dust_mask *dm, const char *seq, size_t len, const oracle_bf *bf,
 		double threshold, unsigned streak_threshold, uint64_t *probes)
 {
 	const size_t frames = len - bf->k + 1; /* size_t arithmetic, as upstream */
@@ -385,7 +641,7 @@ int oracle_eval_simple(const char *seq, size_t len, const oracle_bf *bf,
 	oracle_ntitr it;
 	oracle_ntitr_init(&it, seq, len, bf->k, bf->k);
 	if (!oracle_ntitr_end(&it)) {
-		if (oracle_bf_contains(bf, it.hv, probes)) {
+		if (frame_hit(bf, &it, dm, probes)) {
 			score += 0.5;
 			if (thres <= score)
 				return 1;
@@ -404,7 +660,7 @@ int oracle_eval_simple(const char *seq, size_t len, const oracle_bf *bf,
 				return 0;
 			streak = 0;
 		}
-		if (oracle_bf_contains(bf, it.hv, probes)) {
+		if (frame_hit(bf, &it, dm, probes)) {
 			if (streak == 0)
 				score += 0.5;
 			else
@@ -436,10 +692,20 @@ int oracle_eval_simple(const char *seq, size_t len, const oracle_bf *bf,
 	return 0;
 }
 
+int oracle_eval_simple(const char *seq, size_t len, const oracle_bf *bf,
+		double threshold, unsigned streak_threshold, uint64_t *probes)
+{
+	dust_mask dm;
+	dust_mask_init(&dm, seq, len);
+	int v = oracle_eval_simple_impl(&dm, seq, len, bf, threshold, streak_threshold, probes);
+	free(dm.iv);
+	return v;
+}
+
 /* SeqEval::evalHarmonic (Common/SeqEval.h:116-193), without dust/subtract:
  * evalSimple's walk, with a hit in a streak of s earlier hits adding
  * 1 - 1/(1 + s) instead of 1. */
-int oracle_eval_harmonic(const char *seq, size_t len, const oracle_bf *bf,
+static int oracle_eval_harmonic_impl(dust_mask *dm, const char *seq, size_t len, const oracle_bf *bf,
 		double threshold, unsigned streak_threshold, uint64_t *probes)
 {
 	const size_t frames = len - bf->k + 1; /* size_t arithmetic, as upstream */
@@ -450,7 +716,7 @@ int oracle_eval_harmonic(const char *seq, size_t len, const oracle_bf *bf,
 	oracle_ntitr it;
 	oracle_ntitr_init(&it, seq, len, bf->k, bf->k);
 	if (!oracle_ntitr_end(&it)) {
-		if (oracle_bf_contains(bf, it.hv, probes)) {
+		if (frame_hit(bf, &it, dm, probes)) {
 			score += 0.5;
 			if (thres <= score)
 				return 1;
@@ -469,7 +735,7 @@ int oracle_eval_harmonic(const char *seq, size_t len, const oracle_bf *bf,
 				return 0;
 			streak = 0;
 		}
-		if (oracle_bf_contains(bf, it.hv, probes)) {
+		if (frame_hit(bf, &it, dm, probes)) {
 			if (streak == 0)
 				score += 0.5;
 			else
@@ -498,6 +764,16 @@ int oracle_eval_harmonic(const char *seq, size_t len, const oracle_bf *bf,
 		}
 	}
 	return 0;
+}
+
+int oracle_eval_harmonic(const char *seq, size_t len, const oracle_bf *bf,
+		double threshold, unsigned streak_threshold, uint64_t *probes)
+{
+	dust_mask dm;
+	dust_mask_init(&dm, seq, len);
+	int v = oracle_eval_harmonic_impl(&dm, seq, len, bf, threshold, streak_threshold, probes);
+	free(dm.iv);
+	return v;
 }
 
 /* BloomFilter::getFPRPrecompute as restated: (set bits / m) ^ h. */
@@ -544,7 +820,7 @@ unsigned oracle_calc_min_count(unsigned frame_len, double bf_fpr, double min_fpr
 /* SeqEval::evalBinomial (Common/SeqEval.h:218-290), without dust/subtract:
  * every hit adds 1; accept at calcMinCount hits, reject at frameLen minus that
  * many misses.  fpr = the filter's getFPRPrecompute(). */
-int oracle_eval_binomial(const char *seq, size_t len, const oracle_bf *bf,
+static int oracle_eval_binomial_impl(dust_mask *dm, const char *seq, size_t len, const oracle_bf *bf,
 		double threshold, double fpr, unsigned streak_threshold, uint64_t *probes)
 {
 	if (len < bf->k)
@@ -556,7 +832,7 @@ int oracle_eval_binomial(const char *seq, size_t len, const oracle_bf *bf,
 	oracle_ntitr it;
 	oracle_ntitr_init(&it, seq, len, bf->k, bf->k);
 	if (!oracle_ntitr_end(&it)) {
-		if (oracle_bf_contains(bf, it.hv, probes)) {
+		if (frame_hit(bf, &it, dm, probes)) {
 			score++;
 			if (thres <= score)
 				return 1;
@@ -575,7 +851,7 @@ int oracle_eval_binomial(const char *seq, size_t len, const oracle_bf *bf,
 				return 0;
 			streak = 0;
 		}
-		if (oracle_bf_contains(bf, it.hv, probes)) {
+		if (frame_hit(bf, &it, dm, probes)) {
 			++score;
 			if (thres <= score)
 				return 1;
@@ -603,9 +879,19 @@ int oracle_eval_binomial(const char *seq, size_t len, const oracle_bf *bf,
 	return 0;
 }
 
+int oracle_eval_binomial(const char *seq, size_t len, const oracle_bf *bf,
+		double threshold, double fpr, unsigned streak_threshold, uint64_t *probes)
+{
+	dust_mask dm;
+	dust_mask_init(&dm, seq, len);
+	int v = oracle_eval_binomial_impl(&dm, seq, len, bf, threshold, fpr, streak_threshold, probes);
+	free(dm.iv);
+	return v;
+}
+
 /* SeqEval::evalMinMatchLen (Common/SeqEval.h:295-332), without
  * dust/subtract.  The iterator is built with getHashNum() hashes. */
-int oracle_eval_min_match_len(const char *seq, size_t len,
+static int oracle_eval_min_match_len_impl(dust_mask *dm, const char *seq, size_t len,
 		const oracle_bf *bf, unsigned min_match_len, uint64_t *probes)
 {
 	unsigned match = 0, prev = 0;
@@ -616,7 +902,7 @@ int oracle_eval_min_match_len(const char *seq, size_t len,
 			return 0;
 		if (it.pos != (size_t)prev + 1)
 			match = 0;
-		if (oracle_bf_contains(bf, it.hv, probes)) {
+		if (frame_hit(bf, &it, dm, probes)) {
 			if (match == 0)
 				match = bf->k;
 			else
@@ -629,6 +915,16 @@ int oracle_eval_min_match_len(const char *seq, size_t len,
 		prev = (unsigned)it.pos;
 	}
 	return 0;
+}
+
+int oracle_eval_min_match_len(const char *seq, size_t len,
+		const oracle_bf *bf, unsigned min_match_len, uint64_t *probes)
+{
+	dust_mask dm;
+	dust_mask_init(&dm, seq, len);
+	int v = oracle_eval_min_match_len_impl(&dm, seq, len, bf, min_match_len, probes);
+	free(dm.iv);
+	return v;
 }
 
 /* ------------------------------------------------------------------------ */
@@ -650,7 +946,7 @@ double oracle_binom_sf(unsigned n, double p, unsigned x)
  * evalSimpleScore (:334-376), evalHarmonicScore (:378-419),
  * evalMinMatchLenScore (:421-448) and evalBinomialScore (:450-491) followed by
  * log10(...) * -10.  fpr is the filter's getFPRPrecompute (BINOMIAL only). */
-double oracle_eval_score(const char *seq, size_t len, const oracle_bf *bf, int scoring,
+static double oracle_eval_score_impl(dust_mask *dm, const char *seq, size_t len, const oracle_bf *bf, int scoring,
 		unsigned streak_threshold, double fpr)
 {
 	oracle_ntitr it;
@@ -660,7 +956,7 @@ double oracle_eval_score(const char *seq, size_t len, const oracle_bf *bf, int s
 		while (!oracle_ntitr_end(&it)) {
 			if (it.pos != (size_t)prev + 1)
 				match_len = 0;
-			if (oracle_bf_contains(bf, it.hv, NULL))
+			if (frame_hit(bf, &it, dm, NULL))
 				match_len = match_len == 0 ? bf->k : match_len + 1;
 			else
 				match_len = 0;
@@ -677,7 +973,7 @@ double oracle_eval_score(const char *seq, size_t len, const oracle_bf *bf, int s
 	while (!oracle_ntitr_end(&it)) {
 		if (it.pos != (size_t)prev + 1)
 			streak = 0;
-		if (oracle_bf_contains(bf, it.hv, NULL)) {
+		if (frame_hit(bf, &it, dm, NULL)) {
 			if (scoring == ORACLE_BINOMIAL)
 				score += 1;
 			else if (streak == 0)
@@ -709,6 +1005,16 @@ double oracle_eval_score(const char *seq, size_t len, const oracle_bf *bf, int s
 	}
 	/* normalizeScore (:33-35): the divisor in size_t arithmetic */
 	return score / (double)(len - bf->k + 1);
+}
+
+double oracle_eval_score(const char *seq, size_t len, const oracle_bf *bf, int scoring,
+		unsigned streak_threshold, double fpr)
+{
+	dust_mask dm;
+	dust_mask_init(&dm, seq, len);
+	double v = oracle_eval_score_impl(&dm, seq, len, bf, scoring, streak_threshold, fpr);
+	free(dm.iv);
+	return v;
 }
 
 void oracle_classify_scores(const char *seq, const uint64_t *off, size_t n,

@@ -136,6 +136,16 @@ double oracle_bf_fpr(const oracle_bf *bf);
 unsigned oracle_binom_upper_quantile(unsigned n, double p, double q);
 unsigned oracle_calc_min_count(unsigned frame_len, double bf_fpr, double min_fpr);
 
+/* SDUST (Common/sdust.c, through Common/SDust.hpp): masked intervals of one
+ * read as start << 32 | finish (finish exclusive), at most cap written;
+ * returns how many there are.  max_perfect (optional): the largest number
+ * of pending perfect intervals held at once. */
+int oracle_sdust(const char *seq, size_t len, int T, int W, uint64_t *out, int cap,
+		int *max_perfect);
+/* -D: every oracle_eval_* and the batch drivers treat frames starting in a
+ * masked interval as misses without a probe (off by default). */
+void oracle_set_dust(int on, int T, int W);
+
 /* ---------------- Batch driver + summary ---------------- */
 
 /* Scoring methods, in the order of opt::ScoringMethod (Common/Options.h:35). */

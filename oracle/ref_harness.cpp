@@ -15,17 +15,23 @@
  *       SeqEval::evalScore (Common/SeqEval.h:534-560) of the read against
  *       filter f under METHOD (simple, length, harmonic or binomial), as the
  *       16 hex digits of the double's bits.
+ *   ref_harness dust T W READS
+ *       For every read, prints "<name>\t<start>-<finish>,..." with the
+ *       intervals the reference's sdust (Common/sdust.c) masks.
  *   ref_harness time  SCORE STREAK THREADS INCLUSIVE PREFIX FILTERS READS [READS2]
  *       Builds a BioBloomClassifier (BioBloomClassifier.cpp:21-28; filter
  *       load not timed), then times filter()/filterPair() and prints one JSON
  *       line with the wall time, reads and cores used.
  *
  * A score > 1 selects LENGTH scoring, as BioBloomCategorizer.cpp:423-430 does.
+ * The environment variable BBT_DUST="T,W" turns on DUST masking (-D -T T -W W,
+ * BioBloomCategorizer.cpp:323-337) for hits and scores.
  */
 #include "BioBloomClassifier.h"
 #include "ResultsManager.hpp"
 #include "Common/Options.h"
 #include "Common/SeqEval.h"
+#include "Common/sdust.h"
 #include <omp.h>
 #include <cmath>
 #include <cstdio>
@@ -70,6 +76,19 @@ static void set_score(double score)
 	}
 }
 
+static void set_dust()
+{
+	const char *d = getenv("BBT_DUST");
+	if (!d || !*d)
+		return;
+	opt::dust = true;
+	unsigned T = 20, W = 64;
+	if (sscanf(d, "%u,%u", &T, &W) >= 1) {
+		opt::dustT = T;
+		opt::dustWindow = W;
+	}
+}
+
 static string join(const vector<unsigned> &v)
 {
 	string s;
@@ -88,6 +107,7 @@ static int mode_hits(int argc, char **argv)
 		return 2;
 	}
 	set_score(atof(argv[2]));
+	set_dust();
 	opt::streakThreshold = (unsigned)atoi(argv[3]);
 	vector<string> paths = split_commas(argv[4]);
 	vector<BloomFilter *> filters;
@@ -156,6 +176,7 @@ static int mode_scores(int argc, char **argv)
 		opt::scoringMethod = opt::BINOMIAL;
 	else
 		opt::scoringMethod = opt::SIMPLE;
+	set_dust();
 	opt::streakThreshold = (unsigned)atoi(argv[3]);
 	vector<string> paths = split_commas(argv[4]);
 	vector<BloomFilter *> filters;
@@ -177,6 +198,33 @@ static int mode_scores(int argc, char **argv)
 			printf("%s%016llx", f ? "," : "", bits);
 		}
 		printf("\n");
+	}
+	kseq_destroy(k);
+	gzclose(fp);
+	return 0;
+}
+
+static int mode_dust(int argc, char **argv)
+{
+	if (argc < 5) {
+		fprintf(stderr, "usage: ref_harness dust T W READS\n");
+		return 2;
+	}
+	int T = atoi(argv[2]), W = atoi(argv[3]);
+	gzFile fp = gzopen(argv[4], "r");
+	if (fp == Z_NULL) {
+		fprintf(stderr, "cannot open reads\n");
+		return 1;
+	}
+	kseq_t *k = kseq_init(fp);
+	for (int l; (l = kseq_read(k)) >= 0;) {
+		int n = 0;
+		uint64_t *iv = sdust(0, (const uint8_t *)k->seq.s, l, T, W, &n);
+		printf("%s\t", k->name.s);
+		for (int i = 0; i < n; ++i)
+			printf("%s%u-%u", i ? "," : "", (unsigned)(iv[i] >> 32), (unsigned)iv[i]);
+		printf("\n");
+		free(iv);
 	}
 	kseq_destroy(k);
 	gzclose(fp);
@@ -241,6 +289,8 @@ int main(int argc, char **argv)
 		return mode_time(argc, argv);
 	if (mode == "scores")
 		return mode_scores(argc, argv);
+	if (mode == "dust")
+		return mode_dust(argc, argv);
 	fprintf(stderr, "unknown mode %s\n", argv[1]);
 	return 2;
 }

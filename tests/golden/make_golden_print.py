@@ -10,8 +10,9 @@ contents (stdout as "### stdout").
 MODE_CASES cover the filtering modes (-c ordered, -b best hit, -w with
 scores), single-file paired input (reads_smart.fq.gz, written here from the
 paired fixtures with "/1" and "/2" names, mates out of order and orphans) and
-file lists (-l, written into the run's directory); their golden files also
-hold "<prefix>_summary.tsv".
+file lists (-l, written into the run's directory) and DUST masking (-D, -T,
+-W, on the reads of make_golden_dust.py, which runs first); their golden files
+also hold "<prefix>_summary.tsv".
 
 Usage: python tests/golden/make_golden_print.py [--all]
 (--all also rewrites the CASES files, which the MODE_CASES run leaves as they are)
@@ -62,6 +63,12 @@ MODE_CASES = {
     "list_se": ([], "list_se"),
     "list_se_fa": (["--fa"], "list_se"),
     "list_pe": (["-e"], "list_pe"),
+    "dust_se_fa": (["-D", "--fa"], "dust_se"),
+    "dust_t30_w32_se": (["-D", "-T", "30", "-W", "32"], "dust_se"),
+    "dust_pe_fq": (["-D", "-e", "--fq"], "dust_pe"),
+    "dust_best_se_fa": (["-D", "-b", "--fa"], "dust_se"),
+    "dust_ord_pe_incl": (["-D", "-c", "-e", "-i"], "dust_pe"),
+    "dust_scores_length_se_fq": (["-D", "-w", "-s", "30", "--fq"], "dust_se"),
 }
 # Not a case: -e -d with -l.  That path prints kseq records
 # (BioBloomClassifier.h:249-287) and inserts comment.s into std::cout, a null
@@ -85,6 +92,10 @@ def mode_inputs(kind, tmp):
         return inputs(True)
     if kind == "smart":
         return [SMART]
+    if kind == "dust_se":
+        return [os.path.join(BBT, "reads_dust.fa.gz")]
+    if kind == "dust_pe":
+        return [os.path.join(BBT, "reads_dust.fa.gz"), os.path.join(BBT, "reads_dust_2.fa.gz")]
     lst = os.path.join(tmp, "list.txt")
     se = os.path.join(BBT, "reads_se.fa.gz")
     r1, r2 = inputs(True)
@@ -131,9 +142,9 @@ def write_smart_fixture():
         if i == 40:
             recs.append(("odd", m2[0][1], m2[0][2]))
     recs += held
-    with gzip.open(SMART, "wt", compresslevel=9) as f:
+    with gzip.GzipFile(SMART, "wb", compresslevel=9, mtime=0) as f:
         for name, seq, qual in recs:
-            f.write(f"@{name}\n{seq}\n+\n{qual}\n")
+            f.write(f"@{name}\n{seq}\n+\n{qual}\n".encode())
 
 
 def collect(tmp, stdout, summary=False):
@@ -169,7 +180,8 @@ def main():
             if p.returncode:
                 sys.stderr.write(p.stderr.decode(errors="replace"))
                 raise SystemExit(f"failed: {case}")
-            with gzip.open(os.path.join(BBT, f"print_{case}.txt.gz"), "wb", compresslevel=9) as f:
+            with gzip.GzipFile(os.path.join(BBT, f"print_{case}.txt.gz"), "wb", compresslevel=9,
+                               mtime=0) as f:
                 f.write(collect(tmp, p.stdout, summary=True))
     print("written", ", ".join(f"print_{c}.txt.gz" for c in list(CASES) + list(MODE_CASES)))
 

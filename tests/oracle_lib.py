@@ -74,6 +74,10 @@ def lib():
         L.oracle_calc_min_count.argtypes = [u32, dbl, dbl]
         L.oracle_classify.argtypes = [ctypes.c_char_p, P(u64), sz, P(P(_BF)), u32, dbl, u32,
                                       ctypes.c_int, P(u64), P(u64)]
+        L.oracle_sdust.restype = ctypes.c_int
+        L.oracle_sdust.argtypes = [ctypes.c_char_p, sz, ctypes.c_int, ctypes.c_int, P(u64),
+                                   ctypes.c_int, P(ctypes.c_int)]
+        L.oracle_set_dust.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.oracle_binom_sf.restype = dbl
         L.oracle_binom_sf.argtypes = [u32, dbl, u32]
         L.oracle_eval_score.restype = dbl
@@ -210,6 +214,31 @@ def classify(seq_bytes, offsets, filters, threshold=0.15, streak=3, scoring=SIMP
     lib().oracle_classify(seq_bytes, _u64p(off), n, arr, nf, threshold, streak, scoring,
                           _u64p(hits), ctypes.byref(probes) if count_probes else None)
     return hits, probes.value
+
+
+def sdust(seq, T=20, W=64):
+    """Masked intervals [(start, finish)] of one sequence (Common/sdust.c) and
+    the largest number of pending perfect intervals held at once."""
+    cap = len(seq) + 16
+    buf = np.zeros(cap, dtype=np.uint64)
+    mp = ctypes.c_int(0)
+    n = lib().oracle_sdust(seq, len(seq), T, W, _u64p(buf), cap, ctypes.byref(mp))
+    return [(int(v) >> 32, int(v) & 0xffffffff) for v in buf[:n]], mp.value
+
+
+class dust:
+    """Context manager: the oracle's evaluations mask low-complexity frames
+    (-D) inside the block."""
+
+    def __init__(self, T=20, W=64):
+        self.T, self.W = T, W
+
+    def __enter__(self):
+        lib().oracle_set_dust(1, self.T, self.W)
+        return self
+
+    def __exit__(self, *a):
+        lib().oracle_set_dust(0, 20, 64)
 
 
 def classify_scores(seq_bytes, offsets, filters, scoring=SIMPLE, streak=3):
