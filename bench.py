@@ -512,6 +512,129 @@ def check_sample(paths, s1, s2, off, hits1, hits2, n):
                                                         (g2 != w2).any(1).sum())}
 
 
+# ------------------------------------------------- filtering modes / scoring methods
+
+MODE_VARIANTS = [
+    # name, constructor keywords, mode, with scores, dust
+    ("std_simple", dict(score_threshold=SCORE), "std", False, False),
+    ("ordered", dict(score_threshold=SCORE), "ordered", False, False),
+    ("besthit", dict(score_threshold=SCORE), "besthit", False, False),
+    ("with_scores", dict(score_threshold=SCORE), "scores", True, False),
+    ("harmonic", dict(score_threshold=SCORE, score_type="harmonic"), "std", False, False),
+    ("binomial", dict(score_threshold=100, score_type="binomial"), "std", False, False),
+    ("length_40", dict(score_threshold=40), "std", False, False),
+    ("dust", dict(score_threshold=SCORE), "std", False, True),
+]
+
+
+def mode_oracle(ol, filters, name, kw, mode, dust, s, off):
+    """The oracle's hits of one variant for the reads s[off[i]:off[i+1]]."""
+    st = kw.get("score_type", "simple")
+    thr = kw["score_threshold"]
+    if st == "binomial":
+        thr, scoring = 10.0 ** (-(thr / 10.0)), ol.BINOMIAL
+    elif st == "harmonic":
+        scoring = ol.HARMONIC
+    elif thr > 1:
+        scoring = ol.LENGTH
+    else:
+        scoring = ol.SIMPLE
+    seq = s[:off[-1]].tobytes()
+    if dust:
+        with ol.dust():
+            return ol.classify(seq, off, filters, thr, STREAK, scoring)[0]
+    if mode == "besthit":
+        return ol.best_hit(ol.classify_scores(seq, off, filters, scoring, STREAK))[0]
+    return ol.classify(seq, off, filters, thr, STREAK, scoring)[0]
+
+
+def run_modes(args):
+    """Every filtering mode and scoring method on the 10-filter workload's
+    data (device-resident reads, CUDA-event timing per step), each checked
+    against the oracle on a sample of pairs."""
+    import torch
+
+    from biobloom_b200 import MODE_BESTHIT, MODE_SCORES, BioBloomClassifier
+    dev = torch.device("cuda", 0)
+    d = workdir()
+    paths, genomes = build_filters(d, 0)
+    n_pairs = args.pairs
+    s1, s2, off = make_reads(genomes, n_pairs, 5000)
+    bases = int(off[-1])
+    d1 = torch.from_numpy(s1[:bases]).to(dev)
+    d2 = torch.from_numpy(s2[:bases]).to(dev)
+    doff = torch.from_numpy(off.view(np.int64)).to(dev)
+    stream = torch.cuda.Stream(device=dev)
+    ol = None
+    filters = None
+    if not args.no_check:
+        try:
+            from tests import oracle_lib as ol
+            filters = [ol.Filter.load(p) for p in paths]
+        except Exception:
+            ol = None
+    n_check = 500
+    out = {}
+    for name, kw, mode, with_scores, dust in MODE_VARIANTS:
+        bbc = BioBloomClassifier(paths, streak_threshold=STREAK, device=0, **kw)
+        if mode == "ordered":
+            bbc.setOrderedFilter()
+        elif mode == "besthit":
+            bbc.set_mode(MODE_BESTHIT)
+        elif mode == "scores":
+            bbc.set_mode(MODE_SCORES)
+        if dust:
+            bbc.set_dust(True)
+        h1 = torch.empty((n_pairs, bbc.words), dtype=torch.int64, device=dev)
+        h2 = torch.empty((n_pairs, bbc.words), dtype=torch.int64, device=dev)
+        cat = torch.empty(n_pairs, dtype=torch.int32, device=dev)
+        sc1 = sc2 = None
+        if with_scores:
+            sc1 = torch.empty((n_pairs, bbc.n_filters), dtype=torch.float64, device=dev)
+            sc2 = torch.empty((n_pairs, bbc.n_filters), dtype=torch.float64, device=dev)
+
+        def step():
+            bbc.classify_device(d1, doff, d2, doff, h1, h2, cat, stream=stream, scores=sc1,
+                                scores2=sc2)
+
+        for _ in range(args.warmup):
+            step()
+        stream.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        res = {"reads_per_s": 2 * n_pairs / (ms * 1e-3), "ms_per_step": ms}
+        if ol is not None:
+            o = off[:n_check + 1]
+            w1 = mode_oracle(ol, filters, name, kw, mode, dust, s1, o)
+            w2 = mode_oracle(ol, filters, name, kw, mode, dust, s2, o)
+            g1 = h1[:n_check].cpu().numpy().view(np.uint64).copy()
+            g2 = h2[:n_check].cpu().numpy().view(np.uint64).copy()
+            if mode == "ordered":
+                w1, w2 = ol.ordered(w1, len(filters), w2, False)
+            res["checked_pairs"] = n_check
+            res["mismatched_reads"] = int((g1 != w1).any(1).sum() + (g2 != w2).any(1).sum())
+        out[name] = res
+        bbc.close()
+        log(name, json.dumps(res))
+    base = out["std_simple"]["reads_per_s"]
+    line = {
+        "metric": "reads/s per filtering mode and scoring method on 1 B200",
+        "value": base, "unit": "reads/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": WORKLOAD.replace("10M pairs", f"{n_pairs} pairs"),
+                   "pairs": n_pairs, "timed": "device-resident reads; every kernel of a call "
+                   "(DUST masking, classification, scores, summary)"},
+        "variants": {k: dict(v, relative_to_std=v["reads_per_s"] / base) for k, v in out.items()},
+    }
+    print(json.dumps(line), flush=True)
+
+
 # ------------------------------------------------- single-filter workloads
 
 SINGLE = {
@@ -1288,7 +1411,7 @@ def main():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity (bytes)")
     ap.add_argument("--workload", default="bf",
-                    choices=["bf", "mibf", "varlen", "small", "serve"])
+                    choices=["bf", "mibf", "varlen", "small", "serve", "modes"])
     ap.add_argument("--requests", type=int, default=200, help="requests (--workload serve)")
     ap.add_argument("--load", type=float, default=0.7,
                     help="offered load, fraction of offline capacity (--workload serve)")
@@ -1311,6 +1434,11 @@ def main():
             run_serve(args)
     elif args.workload == "mibf":
         (run_mibf_reference if args.impl == "reference" else run_mibf)(args)
+    elif args.workload == "modes":
+        if args.impl == "reference":
+            run_reference(args)
+        else:
+            run_modes(args)
     elif args.workload in SINGLE:
         (run_single_reference if args.impl == "reference" else run_single)(args)
     elif args.impl == "reference":
