@@ -271,7 +271,7 @@ static int alloc_slot(bbt_ctx *ctx, Slot &s, uint64_t bases, uint64_t reads)
  * persistent read-major kernel. */
 static int auto_path(const bbt_ctx *ctx)
 {
-	if (ctx->nf < 2 || !ctx->same_k || ctx->p.scoring > BBT_SCORE_LENGTH)
+	if (ctx->nf < 2 || !ctx->same_k)
 		return BBT_PATH_PERSISTENT;
 	int l2 = 0;
 	cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->dev);
@@ -745,8 +745,7 @@ static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStrea
 	sa.fpr = ctx->d_fpr;
 	sa.besthit = 0;
 	const bool want_scores = sa.scores[0] || sa.scores[1];
-	const bool two_pass = ctx->lc.path == BBT_PATH_FILTER_MAJOR && ctx->same_k &&
-			ctx->p.scoring <= BBT_SCORE_LENGTH && !ctx->dust;
+	const bool two_pass = ctx->lc.path == BBT_PATH_FILTER_MAJOR && ctx->same_k;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k0, s));
 	if (ctx->mode == BBT_MODE_BESTHIT) {
 		/* the hit words are the filters of the largest score */

@@ -66,11 +66,13 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 		LengthState ls;
 		SeqState qs;
 		constexpr bool length_mode = MODE == BBT_SCORE_LENGTH;
-		constexpr bool seq_mode = MODE == BBT_SCORE_HARMONIC || MODE == BBT_SCORE_BINOMIAL;
+		/* HARMONIC walks frame by frame (seq_chunk); BINOMIAL is SIMPLE's
+		 * machine with integer hits (binomial_simple_init) */
+		constexpr bool seq_mode = MODE == BBT_SCORE_HARMONIC;
 		if (MODE == BBT_SCORE_HARMONIC)
 			harmonic_init(qs, a.score, a.one_minus, frames);
 		else if (MODE == BBT_SCORE_BINOMIAL)
-			binomial_init(qs, a.bthres[f * a.bthres_rows + frames], (uint32_t)frames);
+			binomial_simple_init(st, a.bthres[f * a.bthres_rows + frames], frames);
 		else if (length_mode)
 			length_init(ls, a.min_len, len, (int)k);
 		else

@@ -68,6 +68,16 @@ BBT_HD int highbit32(uint32_t x)
 #endif
 }
 
+/* number of consecutive set bits from bit 31 down */
+BBT_HD int leading_ones32(uint32_t x)
+{
+#if defined(__CUDA_ARCH__)
+	return __clz(~x);
+#else
+	return ~x ? __builtin_clz(~x) : 32;
+#endif
+}
+
 /* bits [0, n) set, n in [0, 32] */
 BBT_HD uint32_t low_mask(int n)
 {
@@ -144,6 +154,7 @@ struct SimpleState {
 	int32_t in_window;    /* a skip window is open (frames < skip_until) */
 	int32_t pending;      /* invalid window frames after its last valid one */
 	int32_t decided;      /* EVAL_* */
+	int32_t flat;         /* BINOMIAL: every hit adds 1 (2 to score2) */
 };
 
 /* Reads are limited to this many frames so that every counter of the state
@@ -185,6 +196,29 @@ BBT_HD void simple_init(SimpleState &s, double threshold, double one_minus,
 	s.in_window = 0;
 	s.pending = 0;
 	s.decided = EVAL_OPEN;
+	s.flat = 0;
+}
+
+/*
+ * SeqEval::evalBinomial (Common/SeqEval.h:218-290) is evalSimple's walk with
+ * an integer score: every hit adds 1, "thres <= score" with thres =
+ * calcMinCount(frameLen, fpr, minFPR) (computed on the host), and
+ * "antiThres <= antiScore" with antiThres = frameLen - thres (unsigned; thres
+ * never exceeds frameLen).  In score2's half units: every hit adds 2.
+ */
+BBT_HD void binomial_simple_init(SimpleState &s, uint32_t thres, uint64_t frames)
+{
+	s.score2 = 0;
+	s.anti = 0;
+	s.thres2 = (int32_t)(2u * thres);
+	s.anti_thres = (int32_t)(uint32_t)((uint32_t)frames - thres);
+	s.streak = 0;
+	s.started = 0;
+	s.skip_until = 0;
+	s.in_window = 0;
+	s.pending = 0;
+	s.decided = EVAL_OPEN;
+	s.flat = 1;
 }
 
 /*
@@ -203,7 +237,7 @@ BBT_HD int simple_step_frames(const SimpleState &s)
 	const int32_t gap = s.thres2 - s.score2;
 	if (gap <= 0 || (s.started && s.streak == 0))
 		return 32;
-	const int32_t need = s.streak > 0 ? (gap + 1) / 2 : 1 + gap / 2;
+	const int32_t need = (s.streak > 0 || s.flat) ? (gap + 1) / 2 : 1 + gap / 2;
 	return need < 8 ? 8 : (need > 32 ? 32 : (int)need);
 }
 
@@ -242,7 +276,7 @@ BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int32_t base,
 		const uint32_t M = V & ~H;
 		const uint32_t trig = M & run;
 		const uint32_t pre = trig ? low_mask(lowbit32(trig)) : inread;
-		const uint32_t prevhit = H & ((H << 1) | (st > 0 ? 1u : 0u));
+		const uint32_t prevhit = s.flat ? H : (H & ((H << 1) | (st > 0 ? 1u : 0u)));
 		/* invalid frames count, except those before the first valid one */
 		const uint32_t C = s.started ? (~V & inread)
 		                             : (V ? (~V & inread & ~low_mask(lowbit32(V))) : 0u);
@@ -345,7 +379,7 @@ BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int32_t base,
 		const uint64_t ext = ((uint64_t)Hr << 32) | carry;
 		/* hits whose previous frame is a hit of the same streak: these add
 		 * 1.0 to the score, the others 0.5 */
-		const uint32_t prevhit = (uint32_t)((ext << 1) >> 32) & Hr;
+		const uint32_t prevhit = s.flat ? Hr : ((uint32_t)((ext << 1) >> 32) & Hr);
 		/* skip triggers: a miss after at least streak_thr consecutive hits */
 		uint32_t trig;
 		if (streak_thr <= 0) {
@@ -470,13 +504,55 @@ BBT_HD void length_init(LengthState &s, unsigned min_len, uint64_t len, int k)
 	s.decided = EVAL_OPEN;
 }
 
-/* Advance over one chunk; every valid frame must have been probed. */
+/* Advance over one chunk; every valid frame must have been probed.
+ *
+ * Without alg (no probe accounting) the chunk is settled by runs instead of
+ * frame by frame.  The match after a valid frame is k + (its run of
+ * consecutive hit frames - 1), or 0 after a miss; a run that touches bit 0
+ * continues the previous chunk's match when the last visited frame was the
+ * one just before.  The read is accepted iff some frame's match reaches
+ * min_len.  The reference's reject test (len - pos + match < min_len before
+ * a frame) only fires when no later frame can reach min_len, so the decision
+ * does not depend on where it fires: here a chunk rejects when the frames
+ * left cannot reach min_len even as one run continuing this chunk's last
+ * one. */
 BBT_HD int length_chunk(LengthState &s, uint32_t V, uint32_t H, int64_t base,
 		int nf, uint32_t *alg = nullptr)
 {
 	if (s.decided)
 		return s.decided;
 	V &= low_mask(nf);
+	if (!alg) {
+		H &= V;
+		const bool carry = s.match > 0 && s.prev == base - 1;
+		uint32_t x = H;
+		while (x) {
+			const int a = lowbit32(x);
+			const uint32_t rest = ~(H >> a); /* zero bits from a upwards */
+			const int run = rest ? lowbit32(rest) : 32 - a;
+			const int64_t m0 = (a == 0 && carry) ? s.match + 1 : (int64_t)s.k;
+			if (m0 + run - 1 >= s.min_len)
+				return s.decided = EVAL_ACCEPT;
+			x &= ~range_mask(a, a + run);
+		}
+		if (V) {
+			const int last = highbit32(V);
+			if ((H >> last) & 1u) {
+				const int run = leading_ones32(H << (31 - last));
+				const int a = last - run + 1;
+				s.match = (a == 0 && carry) ? s.match + run : (int64_t)s.k + run - 1;
+			} else {
+				s.match = 0;
+			}
+			s.prev = base + last;
+		}
+		const int64_t rem = s.len - s.k + 1 - (base + nf);
+		const bool cont = nf > 0 && ((H >> (nf - 1)) & 1u);
+		const int64_t best = cont ? s.match + rem : (rem > 0 ? s.k + rem - 1 : 0);
+		if (best < s.min_len)
+			return s.decided = EVAL_REJECT;
+		return EVAL_OPEN;
+	}
 	uint32_t x = V;
 	while (x) {
 		int q = lowbit32(x);

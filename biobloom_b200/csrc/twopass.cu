@@ -184,6 +184,7 @@ struct ItemMeta {
 	uint64_t len;
 	uint64_t base;
 	uint64_t i;
+	uint64_t start;   /* the read's first base in its mate array (DUST mask index) */
 	uint32_t mate;
 };
 
@@ -194,7 +195,9 @@ __device__ __forceinline__ ItemMeta item_meta(const ClassifyArgs &a, const TwoPa
 	const uint64_t r = p.r_first + t;
 	m.mate = r >= a.n ? 1u : 0u;
 	m.i = r - (m.mate ? a.n : 0);
-	m.len = a.off[m.mate][m.i + 1] - a.off[m.mate][m.i];
+	const uint64_t o = a.off[m.mate][m.i];
+	m.len = a.off[m.mate][m.i + 1] - o;
+	m.start = o - a.off_base[m.mate];
 	m.base = frame_base(p, t);
 	return m;
 }
@@ -202,10 +205,15 @@ __device__ __forceinline__ ItemMeta item_meta(const ClassifyArgs &a, const TwoPa
 /* Filter pass: (filter, read) items of reads [t0, t1) in filter-major order.
  * The next chunk's hashes and validity word, and the next item's metadata,
  * are loaded while the current ones are in use, to overlap their latency
- * with the probes. */
-template <bool COUNT, bool LENGTH_MODE>
+ * with the probes.  MODE is the scoring method: SIMPLE and BINOMIAL run the
+ * chunk machine of simple_chunk (BINOMIAL with integer hits), LENGTH
+ * length_chunk, HARMONIC the sequential walk seq_chunk.  With DUST masking a
+ * frame whose first base is masked is a miss that is not probed. */
+template <bool COUNT, int MODE>
 __global__ void __launch_bounds__(256, 6) filter_pass_kernel(ClassifyArgs a, TwoPassArgs p)
 {
+	constexpr bool LENGTH_MODE = MODE == BBT_SCORE_LENGTH;
+	constexpr bool SEQ_MODE = MODE == BBT_SCORE_HARMONIC;
 	const int lane = threadIdx.x & 31;
 	const uint64_t nreads = p.t1 - p.t0;
 	const uint64_t items = nreads * a.nf;
@@ -235,10 +243,16 @@ __global__ void __launch_bounds__(256, 6) filter_pass_kernel(ClassifyArgs a, Two
 				const uint64_t *hs = p.h0 + cur.base;
 				SimpleState st;
 				LengthState ls;
+				SeqState qs;
 				if (LENGTH_MODE)
 					length_init(ls, a.min_len, cur.len, (int)F.k);
+				else if (SEQ_MODE)
+					harmonic_init(qs, a.score, a.one_minus, frames);
+				else if (MODE == BBT_SCORE_BINOMIAL)
+					binomial_simple_init(st, a.bthres[f * a.bthres_rows + frames], frames);
 				else
 					simple_init(st, a.score, a.one_minus, frames);
+				const uint32_t *dm = a.dust[cur.mate];
 				int decided = EVAL_OPEN;
 				unsigned reads = 0;
 				/* two chunks (64 frames) per step; the second one's probes are
@@ -258,9 +272,12 @@ __global__ void __launch_bounds__(256, 6) filter_pass_kernel(ClassifyArgs a, Two
 						hn1 = ((Vn1 >> lane) & 1u) ? ld_stream_u64(hs + c + 96 + lane, pol) : 0;
 					}
 					const int32_t pf = (int32_t)c + lane;
-					const bool p0 = ((V0 >> lane) & 1u) && (LENGTH_MODE || pf >= st.skip_until);
-					const bool p1 = ((V1 >> lane) & 1u) &&
-							(LENGTH_MODE || pf + 32 >= st.skip_until);
+					const int32_t from = LENGTH_MODE ? 0 : SEQ_MODE ? (int32_t)seq_probe_from(qs)
+					                                                 : st.skip_until;
+					const bool p0 = ((V0 >> lane) & 1u) && pf >= from &&
+							!dust_low(dm, cur.start + (uint64_t)pf);
+					const bool p1 = ((V1 >> lane) & 1u) && pf + 32 >= from &&
+							!dust_low(dm, cur.start + (uint64_t)pf + 32);
 					bool hit0, hit1;
 					unsigned r0 = 0, r1 = 0;
 					contains2(F, h0v, p0, h1v, p1, hit0, hit1, r0, r1);
@@ -272,6 +289,9 @@ __global__ void __launch_bounds__(256, 6) filter_pass_kernel(ClassifyArgs a, Two
 					const int nf0 = (int)min((uint64_t)32, frames - c);
 					decided = LENGTH_MODE
 							? length_chunk(ls, V0, H0, (int64_t)c, nf0, COUNT ? &alg : nullptr)
+							: SEQ_MODE
+							? seq_chunk(qs, V0, H0, (int64_t)c, nf0, (int)F.k, a.streak_thr,
+									COUNT ? &alg : nullptr)
 							: simple_chunk(st, V0, H0, (int32_t)c, nf0, (int)F.k, (int)a.streak_thr,
 									COUNT ? &alg : nullptr);
 					if (COUNT && ((alg >> lane) & 1u))
@@ -282,6 +302,9 @@ __global__ void __launch_bounds__(256, 6) filter_pass_kernel(ClassifyArgs a, Two
 					const int nf1 = (int)min((uint64_t)32, frames - c - 32);
 					decided = LENGTH_MODE
 							? length_chunk(ls, V1, H1, (int64_t)c + 32, nf1, COUNT ? &alg : nullptr)
+							: SEQ_MODE
+							? seq_chunk(qs, V1, H1, (int64_t)c + 32, nf1, (int)F.k, a.streak_thr,
+									COUNT ? &alg : nullptr)
 							: simple_chunk(st, V1, H1, (int32_t)c + 32, nf1, (int)F.k,
 									(int)a.streak_thr, COUNT ? &alg : nullptr);
 					if (COUNT && ((alg >> lane) & 1u))
@@ -376,9 +399,17 @@ cudaError_t two_pass_sub_batch(const ClassifyArgs &a, const TwoPassArgs &p, cons
 	if ((e = cudaMemsetAsync(p.work, 0, sizeof(unsigned long long), s)) != cudaSuccess)
 		return e;
 	{
-		const bool L = a.scoring == BBT_SCORE_LENGTH;
-		auto kern = L ? (C ? filter_pass_kernel<true, true> : filter_pass_kernel<false, true>)
-		              : (C ? filter_pass_kernel<true, false> : filter_pass_kernel<false, false>);
+		auto kern = a.scoring == BBT_SCORE_LENGTH
+				? (C ? filter_pass_kernel<true, BBT_SCORE_LENGTH>
+				     : filter_pass_kernel<false, BBT_SCORE_LENGTH>)
+				: a.scoring == BBT_SCORE_HARMONIC
+				? (C ? filter_pass_kernel<true, BBT_SCORE_HARMONIC>
+				     : filter_pass_kernel<false, BBT_SCORE_HARMONIC>)
+				: a.scoring == BBT_SCORE_BINOMIAL
+				? (C ? filter_pass_kernel<true, BBT_SCORE_BINOMIAL>
+				     : filter_pass_kernel<false, BBT_SCORE_BINOMIAL>)
+				: (C ? filter_pass_kernel<true, BBT_SCORE_SIMPLE>
+				     : filter_pass_kernel<false, BBT_SCORE_SIMPLE>);
 		kern<<<persistent_blocks(kern, threads, 0, lc.num_sms, (nreads * a.nf + 31) / 32), threads,
 				0, s>>>(a, p);
 		if ((e = cudaGetLastError()) != cudaSuccess)

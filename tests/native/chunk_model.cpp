@@ -11,24 +11,28 @@
 #include <vector>
 
 static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
-		double threshold, unsigned streak_thr, int scoring, uint64_t *alg_probes, int tight);
+		double threshold, unsigned streak_thr, int scoring, uint64_t *alg_probes, int tight,
+		int count);
 
 extern "C" int model_eval(const char *seq, uint64_t len, const oracle_bf *bf,
 		double threshold, unsigned streak_thr, int scoring, uint64_t *alg_probes)
 {
 	/* both step policies of the kernel must give the oracle's decision and
-	 * algorithmic probe count */
-	uint64_t a1 = 0, a2 = 0;
-	const int d1 = model_eval_steps(seq, len, bf, threshold, streak_thr, scoring, &a1, 1);
-	const int d2 = model_eval_steps(seq, len, bf, threshold, streak_thr, scoring, &a2, 0);
-	if (d1 != d2 || a1 != a2)
+	 * algorithmic probe count, and the kernels' path without probe
+	 * accounting (alg == nullptr) the same decision */
+	uint64_t a1 = 0, a2 = 0, a3 = 0;
+	const int d1 = model_eval_steps(seq, len, bf, threshold, streak_thr, scoring, &a1, 1, 1);
+	const int d2 = model_eval_steps(seq, len, bf, threshold, streak_thr, scoring, &a2, 0, 1);
+	const int d3 = model_eval_steps(seq, len, bf, threshold, streak_thr, scoring, &a3, 0, 0);
+	if (d1 != d2 || a1 != a2 || d3 != d1)
 		return -1;
 	*alg_probes += a1;
 	return d1;
 }
 
 static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
-		double threshold, unsigned streak_thr, int scoring, uint64_t *alg_probes, int tight)
+		double threshold, unsigned streak_thr, int scoring, uint64_t *alg_probes, int tight,
+		int count)
 {
 	const unsigned k = bf->k;
 	if (len < k)
@@ -45,14 +49,10 @@ static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
 		hit[it.pos] = (uint8_t)oracle_bf_contains(bf, it.hv, &c);
 		cost[it.pos] = (uint32_t)c;
 	}
-	if (scoring == ORACLE_HARMONIC || scoring == ORACLE_BINOMIAL) {
+	if (scoring == ORACLE_HARMONIC) {
 		/* the kernel's 32-frame steps over the sequential walk */
 		bbt::SeqState qs;
-		if (scoring == ORACLE_HARMONIC)
-			bbt::harmonic_init(qs, threshold, 1.0 - threshold, frames);
-		else
-			bbt::binomial_init(qs, oracle_calc_min_count((unsigned)frames, oracle_bf_fpr(bf),
-					threshold), (uint32_t)frames);
+		bbt::harmonic_init(qs, threshold, 1.0 - threshold, frames);
 		for (uint64_t base = 0; base < frames; base += 32) {
 			const int nf = frames - base >= 32 ? 32 : (int)(frames - base);
 			const int64_t from = bbt::seq_probe_from(qs);
@@ -66,7 +66,8 @@ static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
 					H |= 1u << j;
 			}
 			uint32_t alg = 0;
-			const int d = bbt::seq_chunk(qs, V, H, (int64_t)base, nf, (int)k, streak_thr, &alg);
+			const int d = bbt::seq_chunk(qs, V, H, (int64_t)base, nf, (int)k, streak_thr,
+					count ? &alg : nullptr);
 			for (int j = 0; j < nf; ++j)
 				if ((alg >> j) & 1u)
 					*alg_probes += cost[base + j];
@@ -79,6 +80,9 @@ static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
 	bbt::LengthState ls;
 	if (scoring == ORACLE_LENGTH)
 		bbt::length_init(ls, (unsigned)(threshold + 0.5), len, (int)k);
+	else if (scoring == ORACLE_BINOMIAL) /* evalSimple's machine with integer hits */
+		bbt::binomial_simple_init(ss, oracle_calc_min_count((unsigned)frames,
+				oracle_bf_fpr(bf), threshold), frames);
 	else
 		bbt::simple_init(ss, threshold, 1.0 - threshold, frames);
 	for (uint64_t base = 0; base < frames;) {
@@ -96,9 +100,10 @@ static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
 				H |= 1u << j;
 		}
 		uint32_t alg = 0;
+		uint32_t *ap = count ? &alg : nullptr;
 		int d = scoring == ORACLE_LENGTH
-				? bbt::length_chunk(ls, V, H, (int64_t)base, nf, &alg)
-				: bbt::simple_chunk(ss, V, H, (int32_t)base, nf, (int)k, (int)streak_thr, &alg);
+				? bbt::length_chunk(ls, V, H, (int64_t)base, nf, ap)
+				: bbt::simple_chunk(ss, V, H, (int32_t)base, nf, (int)k, (int)streak_thr, ap);
 		for (int j = 0; j < nf; ++j)
 			if ((alg >> j) & 1u)
 				*alg_probes += cost[base + j];

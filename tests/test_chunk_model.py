@@ -77,7 +77,8 @@ def test_chunk_model_matches_oracle(model, seed):
 
 @pytest.mark.parametrize("seed", range(4))
 def test_sequential_walk_matches_oracle_harmonic_binomial(model, seed):
-    """HARMONIC and BINOMIAL: the chunked sequential walk (seq_chunk) gives the
+    """HARMONIC (the chunked sequential walk, seq_chunk) and BINOMIAL (the
+    SIMPLE chunk machine with integer hits, both step policies) give the
     oracle's decision and algorithmic probe count."""
     rng = np.random.default_rng(100 + seed)
     L = ol.lib()
