@@ -134,6 +134,8 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 		cudaFree(w);
 	cudaFree(ctx->d_filters);
 	cudaFree(ctx->d_fpr);
+	cudaFree(ctx->d_tmp_scores[0]);
+	cudaFree(ctx->d_tmp_scores[1]);
 	cudaFree(ctx->d_dust[0]);
 	cudaFree(ctx->d_dust[1]);
 	cudaFree(ctx->d_dust_redo);
@@ -610,7 +612,8 @@ static int grow(bbt_ctx *ctx, T **buf, uint64_t &cap, uint64_t n)
  * scan of padded frame counts, a host read of the per-block totals to cut the
  * batch into sub-batches whose frames fit the scratch, then hash pass and
  * filter pass per sub-batch. */
-static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
+static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s,
+		const ScoreArgs *sa = nullptr, bool classify = true)
 {
 	const uint64_t total = a.n * a.mates;
 	const uint64_t B = two_pass_block_reads();
@@ -657,7 +660,8 @@ static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_tp_vmask, (most / 32 + 1) * sizeof(uint32_t)));
 		ctx->tp_frames_cap = most;
 	}
-	ctx->last.kernels += 2 + 2 * (cuts.size() - 1); /* scans, then hash + filter passes */
+	/* scans, then per sub-batch the hash pass and the filter and / or score pass */
+	ctx->last.kernels += 2 + (cuts.size() - 1) * (1 + (classify ? 1 : 0) + (sa ? 1 : 0));
 	for (size_t c = 0; c + 1 < cuts.size(); ++c) {
 		TwoPassArgs p;
 		p.t0 = cuts[c] * B;
@@ -670,7 +674,7 @@ static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 		p.h0 = ctx->d_tp_h0;
 		p.vmask = ctx->d_tp_vmask;
 		p.work = ctx->d_work;
-		CUDA_TRY(ctx, two_pass_sub_batch(a, p, ctx->lc, s));
+		CUDA_TRY(ctx, two_pass_sub_batch(a, p, ctx->lc, s, sa, classify));
 	}
 	return BBT_OK;
 }
@@ -744,10 +748,44 @@ static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStrea
 	sa.scores[1] = scores && a.mates == 2 ? scores[1] : nullptr;
 	sa.fpr = ctx->d_fpr;
 	sa.besthit = 0;
-	const bool want_scores = sa.scores[0] || sa.scores[1];
+	bool want_scores = sa.scores[0] || sa.scores[1];
 	const bool two_pass = ctx->lc.path == BBT_PATH_FILTER_MAJOR && ctx->same_k;
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_k0, s));
-	if (ctx->mode == BBT_MODE_BESTHIT) {
+	if (two_pass && (ctx->mode == BBT_MODE_BESTHIT || want_scores)) {
+		/* filter-major score pass (and filter pass for the hits unless
+		 * BESTHIT, whose hits come from the scores) */
+		ScoreArgs ps = sa;
+		if (ctx->mode == BBT_MODE_BESTHIT && !want_scores) {
+			const uint64_t need = a.n * ctx->nf;
+			if (need > ctx->tmp_scores_cap) {
+				cudaFree(ctx->d_tmp_scores[0]);
+				cudaFree(ctx->d_tmp_scores[1]);
+				ctx->d_tmp_scores[0] = ctx->d_tmp_scores[1] = nullptr;
+				ctx->tmp_scores_cap = 0;
+				CUDA_TRY(ctx, cudaMalloc(&ctx->d_tmp_scores[0], need * sizeof(double)));
+				CUDA_TRY(ctx, cudaMalloc(&ctx->d_tmp_scores[1], need * sizeof(double)));
+				ctx->tmp_scores_cap = need;
+			}
+			ps.scores[0] = ctx->d_tmp_scores[0];
+			ps.scores[1] = a.mates == 2 ? ctx->d_tmp_scores[1] : nullptr;
+		}
+		const bool classify = ctx->mode != BBT_MODE_BESTHIT;
+		if (classify) {
+			const size_t hb = a.n * ctx->words * sizeof(uint64_t);
+			CUDA_TRY(ctx, cudaMemsetAsync(a.hits[0], 0, hb, s));
+			if (a.mates == 2)
+				CUDA_TRY(ctx, cudaMemsetAsync(a.hits[1], 0, hb, s));
+		}
+		ctx->last.kernels -= 1; /* the passes count themselves */
+		int rc = run_two_pass(ctx, a, s, &ps, classify);
+		if (rc)
+			return rc;
+		if (!classify) {
+			CUDA_TRY(ctx, launch_best_hits(a, ps.scores, ctx->num_sms, s));
+			ctx->last.kernels += 1;
+		}
+		want_scores = false; /* done */
+	} else if (ctx->mode == BBT_MODE_BESTHIT) {
 		/* the hit words are the filters of the largest score */
 		sa.besthit = 1;
 		CUDA_TRY(ctx, launch_scores(a, sa, ctx->lc, s));
@@ -757,7 +795,7 @@ static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStrea
 		CUDA_TRY(ctx, cudaMemsetAsync(a.hits[0], 0, hb, s));
 		if (a.mates == 2)
 			CUDA_TRY(ctx, cudaMemsetAsync(a.hits[1], 0, hb, s));
-		ctx->last.kernels = 1;
+		ctx->last.kernels -= 1; /* the passes count themselves */
 		int rc = run_two_pass(ctx, a, s);
 		if (rc)
 			return rc;

@@ -95,6 +95,9 @@ struct ScoreArgs {
 };
 cudaError_t launch_scores(const ClassifyArgs &a, const ScoreArgs &sa, const LaunchConfig &lc,
 		cudaStream_t s);
+/* BESTHIT hit words (a.hits) from stored scores (n x nf per mate array). */
+cudaError_t launch_best_hits(const ClassifyArgs &a, double *const *scores, int num_sms,
+		cudaStream_t s);
 
 } // namespace bbt
 

@@ -58,6 +58,8 @@ struct bbt_ctx {
 	/* filtering mode (BBT_MODE_*): ORDERED, BESTHIT and SCORES */
 	int mode = BBT_MODE_STD;
 	double *d_fpr = nullptr;         /* each filter's FPR on the device (BINOMIAL scores) */
+	double *d_tmp_scores[2] = {nullptr, nullptr}; /* BESTHIT scores nobody asked for */
+	uint64_t tmp_scores_cap = 0;                  /* elements per mate array */
 	/* -D: SDUST masking before classification (dust.cu) */
 	bool dust = false;
 	int dust_T = 20, dust_W = 64;

@@ -38,9 +38,9 @@ BBT_DHD int dust_code(uint8_t c)
 }
 
 /* sdust over one read; false when the perfect list would exceed pcap
- * entries.  ring: W bytes. */
-template <class MaskFn>
-BBT_DHD bool dust_scan(const uint8_t *seq, uint64_t len, int T, int W, DustPerfect *perf,
+ * entries.  seq(i) returns base i (i = 0, 1, ... in order); ring: W bytes. */
+template <class SeqFn, class MaskFn>
+BBT_DHD bool dust_scan(SeqFn &&seq, uint64_t len, int T, int W, DustPerfect *perf,
 		int pcap, uint8_t *ring, MaskFn &&mask)
 {
 	uint16_t cw[64], cv[64];
@@ -52,7 +52,12 @@ BBT_DHD bool dust_scan(const uint8_t *seq, uint64_t len, int T, int W, DustPerfe
 	int np = 0;
 	bool have_res = false;
 	int res_f = 0;  /* finish of the last masked interval */
-	auto at = [&](int i) -> int { return ring[(head + i) % rcap]; };
+	/* ring index of window entry i (head, i < rcap) */
+	auto slot = [&](int i) -> int {
+		const int x = head + i;
+		return x >= rcap ? x - rcap : x;
+	};
+	auto at = [&](int i) -> int { return ring[slot(i)]; };
 	/* save_masked_regions */
 	auto save = [&](int start) {
 		if (np == 0 || perf[np - 1].start >= start)
@@ -77,7 +82,7 @@ BBT_DHD bool dust_scan(const uint8_t *seq, uint64_t len, int T, int W, DustPerfe
 	unsigned t = 0;
 	const int n = (int)len;
 	for (int i = 0; i <= n; ++i) {
-		const int b = i < n ? dust_code(seq[i]) : 4;
+		const int b = i < n ? dust_code(seq(i)) : 4;
 		if (b < 4) {
 			++l;
 			t = (t << 2 | (unsigned)b) & 63u;
@@ -88,7 +93,7 @@ BBT_DHD bool dust_scan(const uint8_t *seq, uint64_t len, int T, int W, DustPerfe
 			/* shift_window */
 			if (size >= W - 2) {
 				const int s = ring[head];
-				head = (head + 1) % rcap;
+				head = head + 1 == rcap ? 0 : head + 1;
 				--size;
 				rw -= --cw[s];
 				if (L > size) {
@@ -96,7 +101,7 @@ BBT_DHD bool dust_scan(const uint8_t *seq, uint64_t len, int T, int W, DustPerfe
 					rv -= --cv[s];
 				}
 			}
-			ring[(head + size) % rcap] = (uint8_t)t;
+			ring[slot(size)] = (uint8_t)t;
 			++size;
 			++L;
 			rw += cw[t]++;

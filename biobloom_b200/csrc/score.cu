@@ -16,6 +16,7 @@
  * its hit bits come from the classification kernel.
  */
 #include "classify.cuh"
+#include "score_value.cuh"
 #include "seqeval_chunk.cuh"
 #include "window.cuh"
 
@@ -24,63 +25,6 @@
 namespace bbt {
 
 namespace {
-
-/* Sum over the warp in a fixed order, the same value in every lane (a
- * butterfly would give lanes differently rounded sums). */
-__device__ __forceinline__ double warp_sum_uniform(double v)
-{
-	for (int o = 16; o; o >>= 1)
-		v += __shfl_down_sync(kFull, v, o);
-	return __shfl_sync(kFull, v, 0);
-}
-
-/*
- * P(X > c) for X ~ Binomial(n, p): SeqEval::calcProbMatches
- * (Common/SeqEval.h:209-216), boost's cdf(complement(binomial(n, p), c)).
- * The probability masses C(n,i) p^i (1-p)^(n-i) are evaluated in log space
- * (lgamma, log, log1p, exp), 32 terms per step, from i = c + 1 upwards; past
- * the mode (n+1)p the terms only shrink, and the sum stops once a step adds
- * less than 2^-60 of it.  Within a few units in the last place of boost's
- * value (the terms are positive, so the sum has no cancellation).
- */
-__device__ double binom_sf_warp(uint32_t n, double p, uint32_t c, int lane)
-{
-	if (c >= n)
-		return 0.0;
-	if (p <= 0.0)
-		return 0.0;
-	if (p >= 1.0)
-		return 1.0;
-	const double dn = (double)n;
-	const double lp = log(p), lq = log1p(-p), lgn = lgamma(dn + 1.0);
-	const double mode = floor((dn + 1.0) * p);
-	double sum = 0.0;
-	for (uint32_t i0 = c + 1; i0 <= n; i0 += 32) {
-		const uint32_t i = i0 + (uint32_t)lane;
-		double t = 0.0;
-		if (i <= n && i >= i0) {
-			const double di = (double)i;
-			t = exp(lgn - lgamma(di + 1.0) - lgamma(dn - di + 1.0) + di * lp + (dn - di) * lq);
-		}
-		const double step = warp_sum_uniform(t);
-		sum += step;
-		if ((double)i0 > mode && step <= sum * 0x1p-60)
-			break;
-		if (i0 > n - 32u)
-			break;
-	}
-	return sum;
-}
-
-/* log10(calcProbMatches(...)) * -10, as evalScore returns it for BINOMIAL
- * (Common/SeqEval.h:545-555); a read shorter than k scores log10(1.0) * -10. */
-__device__ double binomial_score(uint64_t len, unsigned k, uint32_t count, double fpr, int lane)
-{
-	if (len < k)
-		return log10(1.0) * -10.0;
-	const uint32_t frame_len = (uint32_t)(len - k + 1);
-	return log10(binom_sf_warp(frame_len, fpr, count, lane)) * -10.0;
-}
 
 template <int SEG, int MODE>
 __device__ void score_read(const ClassifyArgs &a, const ScoreArgs &sa, uint64_t r,
@@ -130,13 +74,8 @@ __device__ void score_read(const ClassifyArgs &a, const ScoreArgs &sa, uint64_t 
 				}
 			}
 		}
-		double val;
-		if (MODE == SCORE_LENGTH)
-			val = (double)st.run;
-		else if (MODE == SCORE_BINOMIAL)
-			val = binomial_score(len, k, (uint32_t)st.score, sa.fpr[f], lane);
-		else
-			val = score_normalize(st.score, len, k);
+		const double val = score_value<MODE>(st, len, k, MODE == SCORE_BINOMIAL ? sa.fpr[f] : 0.0,
+				lane);
 		if (sa.scores[mate] && lane == 0)
 			sa.scores[mate][i * a.nf + f] = val;
 		if (sa.besthit) {
@@ -191,7 +130,47 @@ cudaError_t launch_score_seg(const ClassifyArgs &a, const ScoreArgs &sa, const L
 	return cudaGetLastError();
 }
 
+/* evaluateReadBestHit over stored scores: one thread per read (mate). */
+__global__ void best_hits_kernel(ClassifyArgs a, const double *s0, const double *s1)
+{
+	const uint64_t total = a.n * a.mates;
+	for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < total;
+			r += (uint64_t)gridDim.x * blockDim.x) {
+		const uint32_t mate = r >= a.n ? 1u : 0u;
+		const uint64_t i = r - (mate ? a.n : 0);
+		const double *sc = (mate ? s1 : s0) + i * a.nf;
+		uint64_t *h = a.hits[mate] + i * a.words;
+		double best = 0.0;
+		for (uint32_t f = 0; f < a.nf; ++f) {
+			const double v = sc[f];
+			if (best < v)
+				best = v;
+		}
+		/* the filters whose score equals the largest, when it is above 0 */
+		for (uint32_t w = 0; w < a.words; ++w) {
+			uint64_t word = 0;
+			if (best > 0.0)
+				for (uint32_t b = 0; b < 64 && w * 64 + b < a.nf; ++b)
+					word |= (uint64_t)(sc[w * 64 + b] == best) << b;
+			h[w] = word;
+		}
+	}
+}
+
 } // namespace
+
+cudaError_t launch_best_hits(const ClassifyArgs &a, double *const *scores, int num_sms,
+		cudaStream_t s)
+{
+	const uint64_t total = a.n * a.mates;
+	if (total == 0)
+		return cudaSuccess;
+	const uint64_t need = (total + 255) / 256;
+	const uint64_t cap = (uint64_t)num_sms * 8;
+	best_hits_kernel<<<(unsigned)(need < cap ? need : cap), 256, 0, s>>>(a, scores[0],
+			a.mates == 2 ? scores[1] : nullptr);
+	return cudaGetLastError();
+}
 
 cudaError_t launch_scores(const ClassifyArgs &a, const ScoreArgs &sa, const LaunchConfig &lc,
 		cudaStream_t s)

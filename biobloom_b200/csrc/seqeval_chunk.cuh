@@ -671,7 +671,48 @@ BBT_HD int seq_chunk(SeqState &s, uint32_t V, uint32_t H, int64_t base, int nf, 
 	if (s.decided)
 		return s.decided;
 	V &= low_mask(nf);
-	uint32_t x = V;
+	H &= V;
+	int from = 0;
+	/* Without probe accounting, runs of misses outside a skip window are
+	 * settled at once: each visited frame adds its gap and 1 to antiScore, so
+	 * a run adds (last frame - previous frame) and leaves the streak at 0,
+	 * and a rejection inside it is final before the next hit.  Only a miss
+	 * right after a streak of streak_thr hits (it opens a skip window) goes to
+	 * the frame-by-frame walk below. */
+	if (!alg && s.started && !s.in_skip && streak_thr >= 1) {
+		for (;;) {
+			const uint32_t hm = H & ~low_mask(from);
+			const int h = hm ? lowbit32(hm) : nf;
+			const uint32_t mm = V & ~H & range_mask(from, h);
+			if (mm) {
+				const int64_t p0 = base + lowbit32(mm);
+				if (p0 == s.prev + 1 && s.streak >= streak_thr)
+					break; /* opens a skip window */
+				const int64_t pl = base + highbit32(mm);
+				s.anti += (uint32_t)(pl - s.prev);
+				s.prev = pl;
+				s.streak = 0;
+				if (s.anti_thres <= (double)s.anti)
+					return s.decided = EVAL_REJECT;
+			}
+			if (h >= nf)
+				return EVAL_OPEN;
+			const int64_t p = base + h;
+			if (p != s.prev + 1) {
+				s.anti += (uint32_t)(p - s.prev - 1);
+				if (s.anti_thres <= (double)s.anti)
+					return s.decided = EVAL_REJECT;
+				s.streak = 0;
+			}
+			s.score = s.mode == SEQ_BINOMIAL ? s.score + 1.0 : harmonic_add(s.score, s.streak);
+			if (s.thres <= s.score)
+				return s.decided = EVAL_ACCEPT;
+			s.prev = p;
+			++s.streak;
+			from = h + 1;
+		}
+	}
+	uint32_t x = V & ~low_mask(from);
 	while (x) {
 		const int q = lowbit32(x);
 		x &= x - 1;

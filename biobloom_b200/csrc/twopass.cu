@@ -29,6 +29,7 @@
 #include "bbt.h"
 #include "classify.cuh"
 #include "ctx.hpp"
+#include "score_value.cuh"
 #include "seqeval_chunk.cuh"
 #include "twopass.cuh"
 #include "window.cuh"
@@ -341,6 +342,76 @@ __global__ void __launch_bounds__(256, 6) filter_pass_kernel(ClassifyArgs a, Two
 	}
 }
 
+/* Score pass: SeqEval::evalScore of (filter, read) items in filter-major
+ * order (BESTHIT / SCORES), the exhaustive walk of score_chunk over the
+ * stored hashes; lane 0 writes the item's score to sa.scores[mate]. */
+template <int MODE>
+__global__ void __launch_bounds__(256, 6) score_pass_kernel(ClassifyArgs a, TwoPassArgs p,
+		ScoreArgs sa)
+{
+	const int lane = threadIdx.x & 31;
+	const uint64_t nreads = p.t1 - p.t0;
+	const uint64_t items = nreads * a.nf;
+	const uint64_t pol = evict_first_policy();
+	for (;;) {
+		unsigned long long b = 0;
+		if (lane == 0)
+			b = atomicAdd(p.work, 32ull);
+		b = __shfl_sync(kFull, b, 0);
+		if (b >= items)
+			break;
+		uint32_t f = (uint32_t)(b / nreads);
+		uint64_t t = p.t0 + (b - (uint64_t)f * nreads);
+		const uint64_t e = b + 32 < items ? b + 32 : items;
+		FilterDev F = a.filters[f];
+		ItemMeta cur = item_meta(a, p, t);
+		for (uint64_t it = b; it < e; ++it) {
+			uint64_t tn = t + 1 == p.t1 ? p.t0 : t + 1;
+			ItemMeta nxt = cur;
+			if (it + 1 < e)
+				nxt = item_meta(a, p, tn);
+			ScoreState st;
+			score_init(st);
+			if (cur.len >= F.k) {
+				const uint64_t frames = cur.len - F.k + 1;
+				const uint32_t *vm = p.vmask + cur.base / 32;
+				const uint64_t *hs = p.h0 + cur.base;
+				const uint32_t *dm = a.dust[cur.mate];
+				unsigned reads = 0;
+				uint32_t Vn = ld_stream_u32(vm, pol);
+				uint64_t hn = ((Vn >> lane) & 1u) ? ld_stream_u64(hs + lane, pol) : 0;
+				for (uint64_t c = 0; c < frames; c += 32) {
+					const uint32_t V = Vn;
+					const uint64_t hv = hn;
+					if (c + 32 < frames) {
+						Vn = ld_stream_u32(vm + (c >> 5) + 1, pol);
+						hn = ((Vn >> lane) & 1u) ? ld_stream_u64(hs + c + 32 + lane, pol) : 0;
+					}
+					const int64_t pf = (int64_t)c + lane;
+					const bool probe = ((V >> lane) & 1u) &&
+							(MODE == SCORE_LENGTH || pf >= st.skip_end) &&
+							!dust_low(dm, cur.start + (uint64_t)pf);
+					const bool hit = probe && contains(F, hv, reads);
+					const uint32_t H = __ballot_sync(kFull, hit);
+					const int nfc = (int)min((uint64_t)32, frames - c);
+					score_chunk(st, V, H, (int64_t)c, nfc, (int)F.k, a.streak_thr, MODE);
+				}
+			}
+			const double val = score_value<MODE>(st, cur.len, F.k,
+					MODE == SCORE_BINOMIAL ? sa.fpr[f] : 0.0, lane);
+			if (lane == 0)
+				sa.scores[cur.mate][cur.i * a.nf + f] = val;
+			t = tn;
+			if (t == p.t0) {
+				++f;
+				if (f < a.nf)
+					F = a.filters[f];
+			}
+			cur = nxt;
+		}
+	}
+}
+
 template <typename K>
 unsigned persistent_blocks(K kern, int threads, size_t smem, int num_sms, uint64_t warps_needed)
 {
@@ -374,7 +445,7 @@ uint64_t two_pass_block_reads()
 }
 
 cudaError_t two_pass_sub_batch(const ClassifyArgs &a, const TwoPassArgs &p, const LaunchConfig &lc,
-		cudaStream_t s)
+		cudaStream_t s, const ScoreArgs *sa, bool classify)
 {
 	const uint64_t nreads = p.t1 - p.t0;
 	if (nreads == 0)
@@ -396,9 +467,9 @@ cudaError_t two_pass_sub_batch(const ClassifyArgs &a, const TwoPassArgs &p, cons
 		if ((e = cudaGetLastError()) != cudaSuccess)
 			return e;
 	}
-	if ((e = cudaMemsetAsync(p.work, 0, sizeof(unsigned long long), s)) != cudaSuccess)
-		return e;
-	{
+	if (classify) {
+		if ((e = cudaMemsetAsync(p.work, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+			return e;
 		auto kern = a.scoring == BBT_SCORE_LENGTH
 				? (C ? filter_pass_kernel<true, BBT_SCORE_LENGTH>
 				     : filter_pass_kernel<false, BBT_SCORE_LENGTH>)
@@ -412,6 +483,18 @@ cudaError_t two_pass_sub_batch(const ClassifyArgs &a, const TwoPassArgs &p, cons
 				     : filter_pass_kernel<false, BBT_SCORE_SIMPLE>);
 		kern<<<persistent_blocks(kern, threads, 0, lc.num_sms, (nreads * a.nf + 31) / 32), threads,
 				0, s>>>(a, p);
+		if ((e = cudaGetLastError()) != cudaSuccess)
+			return e;
+	}
+	if (sa) {
+		if ((e = cudaMemsetAsync(p.work, 0, sizeof(unsigned long long), s)) != cudaSuccess)
+			return e;
+		auto kern = a.scoring == BBT_SCORE_LENGTH ? score_pass_kernel<SCORE_LENGTH>
+		          : a.scoring == BBT_SCORE_HARMONIC ? score_pass_kernel<SCORE_HARMONIC>
+		          : a.scoring == BBT_SCORE_BINOMIAL ? score_pass_kernel<SCORE_BINOMIAL>
+		                                            : score_pass_kernel<SCORE_SIMPLE>;
+		kern<<<persistent_blocks(kern, threads, 0, lc.num_sms, (nreads * a.nf + 31) / 32), threads,
+				0, s>>>(a, p, *sa);
 		if ((e = cudaGetLastError()) != cudaSuccess)
 			return e;
 	}

@@ -34,10 +34,11 @@ struct TwoPassArgs {
 cudaError_t two_pass_scan(const ClassifyArgs &a, unsigned k, uint64_t *local,
 		unsigned long long *sums, cudaStream_t s);
 uint64_t two_pass_block_reads();
-/* Hash pass then filter pass for one sub-batch (hits must be zeroed once per
- * batch beforehand). */
+/* Hash pass, then the filter pass (classify: hits must be zeroed once per
+ * batch beforehand) and / or the score pass (sa: every item's evalScore into
+ * sa->scores), for one sub-batch. */
 cudaError_t two_pass_sub_batch(const ClassifyArgs &a, const TwoPassArgs &p, const LaunchConfig &lc,
-		cudaStream_t s);
+		cudaStream_t s, const ScoreArgs *sa = nullptr, bool classify = true);
 
 } // namespace bbt
 

@@ -15,7 +15,8 @@ extern "C" int model_sdust(const char *seq, uint64_t len, int T, int W, int pcap
 	std::vector<bbt::DustPerfect> perf((size_t)pcap);
 	std::vector<uint8_t> ring((size_t)W);
 	std::vector<uint64_t> iv;
-	const bool ok = bbt::dust_scan((const uint8_t *)seq, len, T, W, perf.data(), pcap,
+	const uint8_t *bases = (const uint8_t *)seq;
+	const bool ok = bbt::dust_scan([&](int i) { return bases[i]; }, len, T, W, perf.data(), pcap,
 			ring.data(), [&](int a, int b) {
 				/* an extension of the last interval starts at its finish */
 				if (!iv.empty() && (uint32_t)iv.back() == (uint32_t)a)
