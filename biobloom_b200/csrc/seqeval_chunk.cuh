@@ -808,43 +808,113 @@ BBT_HD void score_init(ScoreState &s)
 
 /* Walk the valid frames of one chunk (frame j = base + j, j < nf); H holds the
  * hits of the frames probed (every frame for LENGTH, otherwise those at or
- * after skip_end when the chunk began). */
+ * after skip_end when the chunk began).
+ *
+ * The walk goes by runs rather than frame by frame.  LENGTH only needs the
+ * run of hits that reaches the chunk's last valid frame.  Otherwise: frames
+ * inside an open skip window are passed over; a run of misses leaves the
+ * streak at 0, and only its first frame can open a window (right after a
+ * streak of streak_thr hits); a run of consecutive hits adds, for SIMPLE,
+ * 0.5 for a first hit and 1 for each other (all partial sums are multiples
+ * of 0.5, exact in a double, so one addition gives the sequential result),
+ * for BINOMIAL 1 per hit, and for HARMONIC its terms one at a time in the
+ * reference's order.  streak_thr = 0 (every miss opens a window) is walked
+ * frame by frame. */
 BBT_HD void score_chunk(ScoreState &s, uint32_t V, uint32_t H, int64_t base, int nf, int k,
 		uint32_t streak_thr, int mode)
 {
-	uint32_t x = V & low_mask(nf);
-	while (x) {
-		const int q = lowbit32(x);
-		x &= x - 1;
-		const int64_t p = base + q;
-		const bool hit = (H >> q) & 1u;
-		if (mode == SCORE_LENGTH) {
-			if (p != s.prev + 1)
-				s.run = 0;
-			s.run = hit ? (s.run ? s.run + 1 : (uint32_t)k) : 0u;
-			s.prev = p;
-			continue;
-		}
-		if (p < s.skip_end) {
-			s.prev = p;
-			continue;
-		}
-		if (p != s.prev + 1)
-			s.streak = 0;
-		if (hit) {
-			if (mode == SCORE_HARMONIC)
-				s.score = harmonic_add(s.score, s.streak);
-			else if (mode == SCORE_BINOMIAL)
-				s.score = s.score + 1.0;
-			else
-				s.score = s.score + (s.streak ? 1.0 : 0.5);
-			++s.streak;
+	V &= low_mask(nf);
+	if (!V)
+		return;
+	H &= V;
+	if (mode == SCORE_LENGTH) {
+		const int last = highbit32(V);
+		if ((H >> last) & 1u) {
+			const int run = leading_ones32(H << (31 - last));
+			const bool carry = last - run + 1 == 0 && s.run > 0 && s.prev == base - 1;
+			s.run = carry ? s.run + (uint32_t)run : (uint32_t)k + (uint32_t)run - 1u;
 		} else {
-			if (s.streak >= streak_thr)
-				s.skip_end = (int64_t)(uint32_t)((uint32_t)p + (uint32_t)k);
-			s.streak = 0;
+			s.run = 0;
 		}
-		s.prev = p;
+		s.prev = base + last;
+		return;
+	}
+	if (streak_thr == 0) {
+		uint32_t x = V;
+		while (x) {
+			const int q = lowbit32(x);
+			x &= x - 1;
+			const int64_t p = base + q;
+			if (p < s.skip_end) {
+				s.prev = p;
+				continue;
+			}
+			if (p != s.prev + 1)
+				s.streak = 0;
+			if ((H >> q) & 1u) {
+				s.score = mode == SCORE_HARMONIC ? harmonic_add(s.score, s.streak)
+				        : mode == SCORE_BINOMIAL ? s.score + 1.0
+				                                 : s.score + (s.streak ? 1.0 : 0.5);
+				++s.streak;
+			} else {
+				s.skip_end = (int64_t)(uint32_t)((uint32_t)p + (uint32_t)k);
+				s.streak = 0;
+			}
+			s.prev = p;
+		}
+		return;
+	}
+	int j = 0;
+	for (;;) {
+		/* frames inside an open skip window: iterated, not probed */
+		const int64_t se = s.skip_end - base;
+		if (se > j) {
+			const int e = se >= nf ? nf : (int)se;
+			const uint32_t w = V & range_mask(j, e);
+			if (w)
+				s.prev = base + highbit32(w);
+			j = e;
+			if (j >= nf)
+				return;
+		}
+		const uint32_t hm = H & ~low_mask(j);
+		const int h = hm ? lowbit32(hm) : nf;
+		const uint32_t mm = V & ~H & range_mask(j, h);
+		if (mm) {
+			const int m0 = lowbit32(mm);
+			const int64_t p0 = base + m0;
+			if (p0 == s.prev + 1 && s.streak >= streak_thr) {
+				/* the window starts at this miss */
+				s.skip_end = (int64_t)(uint32_t)((uint32_t)p0 + (uint32_t)k);
+				s.streak = 0;
+				s.prev = p0;
+				j = m0 + 1;
+				continue;
+			}
+			s.streak = 0;
+			s.prev = base + highbit32(mm);
+		}
+		if (h >= nf)
+			return;
+		if (base + h != s.prev + 1)
+			s.streak = 0;
+		if (mode == SCORE_HARMONIC) {
+			s.score = harmonic_add(s.score, s.streak);
+			++s.streak;
+			s.prev = base + h;
+			j = h + 1;
+		} else {
+			const uint32_t rest = ~(H >> h);
+			const int run = rest ? lowbit32(rest) : 32 - h;
+			const double add = mode == SCORE_BINOMIAL ? (double)run
+			                 : (s.streak ? (double)run : (double)run - 0.5);
+			s.score = s.score + add;
+			s.streak += (uint32_t)run;
+			s.prev = base + h + run - 1;
+			j = h + run;
+		}
+		if (j >= nf)
+			return;
 	}
 }
 

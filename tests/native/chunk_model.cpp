@@ -113,3 +113,48 @@ static int model_eval_steps(const char *seq, uint64_t len, const oracle_bf *bf,
 	}
 	return 0;
 }
+
+/* SeqEval::evalScore as the scoring kernels compute it: 32-frame chunks,
+ * frames probed from the skip window's end (every valid frame for LENGTH),
+ * score_chunk over the ballots, then the final value (the BINOMIAL tail from
+ * the oracle's own sum, which the tests compare against). */
+extern "C" double model_score(const char *seq, uint64_t len, const oracle_bf *bf, int scoring,
+		unsigned streak_thr, double fpr)
+{
+	const unsigned k = bf->k;
+	bbt::ScoreState st;
+	bbt::score_init(st);
+	const int mode = scoring; /* ORACLE_* and SCORE_* share values */
+	if (len >= k) {
+		const uint64_t frames = len - k + 1;
+		std::vector<uint8_t> valid(frames), hit(frames);
+		oracle_ntitr it;
+		for (oracle_ntitr_init(&it, seq, len, bf->h, k); !oracle_ntitr_end(&it);
+				oracle_ntitr_next(&it)) {
+			valid[it.pos] = 1;
+			hit[it.pos] = (uint8_t)oracle_bf_contains(bf, it.hv, nullptr);
+		}
+		for (uint64_t base = 0; base < frames; base += 32) {
+			const int nf = frames - base >= 32 ? 32 : (int)(frames - base);
+			const int64_t from = st.skip_end;
+			uint32_t V = 0, H = 0;
+			for (int j = 0; j < nf; ++j) {
+				const uint64_t p = base + j;
+				if (!valid[p])
+					continue;
+				V |= 1u << j;
+				if ((mode == bbt::SCORE_LENGTH || (int64_t)p >= from) && hit[p])
+					H |= 1u << j;
+			}
+			bbt::score_chunk(st, V, H, (int64_t)base, nf, (int)k, streak_thr, mode);
+		}
+	}
+	if (mode == bbt::SCORE_LENGTH)
+		return (double)st.run;
+	if (mode == bbt::SCORE_BINOMIAL) {
+		if (len < k)
+			return log10(1.0) * -10;
+		return log10(oracle_binom_sf((unsigned)(len - k + 1), fpr, (unsigned)st.score)) * -10;
+	}
+	return bbt::score_normalize(st.score, len, k);
+}

@@ -123,3 +123,44 @@ def test_sequential_walk_matches_oracle_harmonic_binomial(model, seed):
             if a != m_ or c1.value != c2.value:
                 mism += 1
     assert mism == 0
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_score_walk_matches_oracle(model, seed):
+    """The scoring kernels' chunked walk (score_chunk) against the oracle's
+    evalScore restatement, bit for bit, for all four scoring methods."""
+    model.model_score.restype = ctypes.c_double
+    model.model_score.argtypes = [ctypes.c_char_p, ctypes.c_uint64, ctypes.POINTER(ol._BF),
+                                  ctypes.c_int, ctypes.c_uint, ctypes.c_double]
+    rng = np.random.default_rng(200 + seed)
+    L = ol.lib()
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    bad = 0
+    for trial in range(25):
+        h = int(rng.integers(1, 5))
+        k = max(h, int(rng.integers(3, 40)))
+        f = ol.Filter.create(64 * int(rng.integers(1, 60)), h, k)
+        g = rng.choice(acgt, 3000)
+        fill = rng.random()
+        for p, hv in ol.kmers(g.tobytes(), h, k):
+            if rng.random() < fill:
+                L.oracle_bf_insert(ctypes.byref(f.bf), (ctypes.c_uint64 * 64)(*hv))
+        fpr = L.oracle_bf_fpr(ctypes.byref(f.bf))
+        for r in range(40):
+            n = int(rng.integers(0, 500))
+            st = int(rng.integers(0, 2500))
+            s = g[st:st + n].copy() if rng.random() < 0.6 else rng.choice(acgt, n)
+            s = s[:n]
+            m = rng.random(len(s)) < rng.random() * 0.05
+            s[m] = rng.choice(acgt, m.sum())
+            if rng.random() < 0.3:
+                m = rng.random(len(s)) < rng.random() * 0.2
+                s[m] = ord("N")
+            b = s.tobytes()
+            streak = int(rng.integers(0, 6))
+            for mode in (ol.SIMPLE, ol.LENGTH, ol.HARMONIC, ol.BINOMIAL):
+                want = L.oracle_eval_score(b, len(b), ctypes.byref(f.bf), mode, streak, fpr)
+                got = model.model_score(b, len(b), ctypes.byref(f.bf), mode, streak, fpr)
+                if np.float64(want).view(np.uint64) != np.float64(got).view(np.uint64):
+                    bad += 1
+    assert bad == 0
