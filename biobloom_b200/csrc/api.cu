@@ -117,6 +117,30 @@ static void free_slot(Slot &s)
 	s.scores_cap = 0;
 	cudaFree(s.d_cat);
 	s.d_cat = nullptr;
+	cudaFreeHost(s.h_stage);
+	s.h_stage = nullptr;
+	s.stage_cap = 0;
+	s.pending.clear();
+}
+
+/* Host memory that the GPU can copy into without staging (pinned or
+ * registered). */
+static bool host_pinned(const void *p)
+{
+	cudaPointerAttributes at;
+	if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+		cudaGetLastError();
+		return false;
+	}
+	return at.type == cudaMemoryTypeHost;
+}
+
+/* The staged results of a slot whose copies are done, to their destinations. */
+static void flush_slot(Slot &s)
+{
+	for (const Slot::HostCopy &c : s.pending)
+		memcpy(c.dst, s.h_stage + c.off, c.bytes);
+	s.pending.clear();
 }
 
 extern "C" int bbt_close(bbt_ctx *ctx)
@@ -934,8 +958,20 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 		if (rc)
 			return rc;
 	}
+	/* staged copies left by a call that failed part way belong to that call */
+	for (Slot &sl : ctx->slot) {
+		if (sl.used)
+			CUDA_TRY(ctx, cudaEventSynchronize(sl.done));
+		sl.pending.clear();
+		sl.used = false;
+	}
 	uint64_t i0 = 0;
 	int which = 0;
+	const bool out_pinned[5] = {r->hits && host_pinned(r->hits),
+			paired && r->hits2 && host_pinned(r->hits2),
+			r->category && host_pinned(r->category),
+			want_scores && scores[0] && host_pinned(scores[0]),
+			want_scores && paired && scores[1] && host_pinned(scores[1])};
 	if (ctx->dust)
 		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_dust_cnt + 1, 0, sizeof(unsigned long long),
 				ctx->stream));
@@ -964,6 +1000,7 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 				for (Slot &s : ctx->slot) {
 					if (s.used)
 						CUDA_TRY(ctx, cudaEventSynchronize(s.done));
+					flush_slot(s);
 					s.used = false;
 				}
 				uint64_t need = bases(i0, i1);
@@ -978,6 +1015,7 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 		Slot &s = ctx->slot[which];
 		if (s.used)
 			CUDA_TRY(ctx, cudaEventSynchronize(s.done));
+		flush_slot(s);
 		const uint64_t cnt = i1 - i0;
 		ClassifyArgs a = base_args(ctx);
 		a.n = cnt;
@@ -1017,20 +1055,49 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 			return rc;
 		CUDA_TRY(ctx, cudaEventRecord(s.computed, ctx->stream));
 		CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->d2h, s.computed, 0));
+		/* results: straight into pinned destinations, through the slot's
+		 * pinned staging buffer into pageable ones */
+		struct Out {
+			void *dst;
+			const void *src;
+			size_t bytes;
+			bool pinned;
+		} outs[5];
+		int no = 0;
 		const size_t hb = cnt * ctx->words * sizeof(uint64_t);
 		if (r->hits)
-			CUDA_TRY(ctx, cudaMemcpyAsync(r->hits + i0 * ctx->words, s.d_hits[0], hb,
-					cudaMemcpyDeviceToHost, ctx->d2h));
+			outs[no++] = {r->hits + i0 * ctx->words, s.d_hits[0], hb, out_pinned[0]};
 		if (paired && r->hits2)
-			CUDA_TRY(ctx, cudaMemcpyAsync(r->hits2 + i0 * ctx->words, s.d_hits[1], hb,
-					cudaMemcpyDeviceToHost, ctx->d2h));
+			outs[no++] = {r->hits2 + i0 * ctx->words, s.d_hits[1], hb, out_pinned[1]};
 		if (r->category)
-			CUDA_TRY(ctx, cudaMemcpyAsync(r->category + i0, s.d_cat, cnt * sizeof(uint32_t),
-					cudaMemcpyDeviceToHost, ctx->d2h));
+			outs[no++] = {r->category + i0, s.d_cat, cnt * sizeof(uint32_t), out_pinned[2]};
 		for (int m = 0; m < 2; ++m)
 			if (slot_scores[m])
-				CUDA_TRY(ctx, cudaMemcpyAsync(scores[m] + i0 * ctx->nf, slot_scores[m],
-						cnt * ctx->nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->d2h));
+				outs[no++] = {scores[m] + i0 * ctx->nf, slot_scores[m],
+						cnt * ctx->nf * sizeof(double), out_pinned[3 + m]};
+		size_t staged = 0;
+		for (int o = 0; o < no; ++o)
+			if (!outs[o].pinned)
+				staged += (outs[o].bytes + 255) & ~(size_t)255;
+		if (staged > s.stage_cap) {
+			cudaFreeHost(s.h_stage);
+			s.h_stage = nullptr;
+			s.stage_cap = 0;
+			CUDA_TRY(ctx, cudaMallocHost(&s.h_stage, staged));
+			s.stage_cap = staged;
+		}
+		size_t at = 0;
+		for (int o = 0; o < no; ++o) {
+			if (outs[o].pinned) {
+				CUDA_TRY(ctx, cudaMemcpyAsync(outs[o].dst, outs[o].src, outs[o].bytes,
+						cudaMemcpyDeviceToHost, ctx->d2h));
+			} else {
+				CUDA_TRY(ctx, cudaMemcpyAsync(s.h_stage + at, outs[o].src, outs[o].bytes,
+						cudaMemcpyDeviceToHost, ctx->d2h));
+				s.pending.push_back({outs[o].dst, at, outs[o].bytes});
+				at += (outs[o].bytes + 255) & ~(size_t)255;
+			}
+		}
 		CUDA_TRY(ctx, cudaEventRecord(s.done, ctx->d2h));
 		s.used = true;
 		which ^= 1;
@@ -1039,8 +1106,10 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_stop, ctx->stream));
 	CUDA_TRY(ctx, cudaStreamSynchronize(ctx->d2h));
 	CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-	for (Slot &s : ctx->slot)
+	for (Slot &s : ctx->slot) {
+		flush_slot(s);
 		s.used = false;
+	}
 	if (ctx->dust) {
 		int rc = dust_check(ctx);
 		if (rc)

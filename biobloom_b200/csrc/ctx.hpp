@@ -24,6 +24,19 @@ struct Slot {
 	uint32_t *d_cat = nullptr;
 	double *d_scores[2] = {nullptr, nullptr}; /* BESTHIT / SCORES: reads x filters */
 	uint64_t scores_cap = 0;                  /* reads d_scores holds */
+	/* Results bound for pageable host memory go through this pinned buffer
+	 * (a device-to-host copy into pageable memory would block the host until
+	 * the slot's kernels finish, and so stop the next slot's input copy from
+	 * overlapping them); `pending` lists the host copies to make once `done`
+	 * has been reached. */
+	struct HostCopy {
+		void *dst;
+		size_t off;
+		size_t bytes;
+	};
+	unsigned char *h_stage = nullptr;
+	size_t stage_cap = 0;
+	std::vector<HostCopy> pending;
 	cudaEvent_t copied = nullptr;   /* inputs are on the device */
 	cudaEvent_t computed = nullptr; /* kernels done */
 	cudaEvent_t done = nullptr;     /* results are back on the host */
