@@ -874,13 +874,24 @@ extern "C" int bbt_mibf_close(bbt_mibf *ctx)
 		cudaFree(ctx->d_stat);
 		cudaFree(ctx->d_minc);
 		cudaFree(ctx->d_fcmax);
-		for (int i = 0; i < 2; ++i) {
-			cudaFree(ctx->d_seq[i]);
-			cudaFree(ctx->d_off[i]);
-		}
 		cudaFree(ctx->d_hits);
 		cudaFree(ctx->d_nhits);
 		cudaFree(ctx->d_sat);
+		for (int c = 0; c < 2; ++c) {
+			for (int m = 0; m < 2; ++m) {
+				cudaFree(ctx->c_seq[c][m]);
+				cudaFree(ctx->c_off[c][m]);
+				cudaFreeHost(ctx->h_coff[c][m]);
+			}
+			if (ctx->c_copied[c])
+				cudaEventDestroy(ctx->c_copied[c]);
+			if (ctx->c_computed[c])
+				cudaEventDestroy(ctx->c_computed[c]);
+		}
+		if (ctx->h2d)
+			cudaStreamDestroy(ctx->h2d);
+		if (ctx->d2h)
+			cudaStreamDestroy(ctx->d2h);
 		if (ctx->ev0)
 			cudaEventDestroy(ctx->ev0);
 		if (ctx->ev1)
@@ -1095,10 +1106,18 @@ static int device_frame_counts(bbt_mibf *ctx, const bbt_batch *b, cudaStream_t s
 	return BBT_OK;
 }
 
+/* A batch may be classified in several launches (chunks of its reads, their
+ * results at their place in the batch's arrays): the first clears the batch's
+ * counters and overflow flag, the last commits the counters. */
+enum { kQueryBegin = 1, kQueryEnd = 2, kQueryWhole = 3 };
+
 static int run_query_sc(bbt_mibf *ctx, uint64_t n_reads, const uint8_t *seq, const uint64_t *off,
 		const uint8_t *seq2, const uint64_t *off2, bbt_mibf_hit *hits, uint32_t max_hits,
-		uint32_t *n_hits, uint32_t *sat, cudaStream_t s, const MibfScratch &sc, bool timed)
+		uint32_t *n_hits, uint32_t *sat, cudaStream_t s, const MibfScratch &sc, bool timed,
+		int phase = kQueryWhole, uint64_t total_reads = ~0ull)
 {
+	if (total_reads == ~0ull)
+		total_reads = n_reads;
 	const unsigned nids = (unsigned)ctx->names.size();
 	const size_t nc = counts_len(ctx);
 	unsigned long long *batch_counts = sc.counts;
@@ -1139,19 +1158,23 @@ static int run_query_sc(bbt_mibf *ctx, uint64_t n_reads, const uint8_t *seq, con
 	const size_t smem = mibf_smem_bytes(a.f.nse, a.T, kQueryThreads / 32);
 	const bool dense = ctx->d_dense != nullptr;
 	const int grid = ctx->num_sms * query_occupancy(dense, hsel, smem);
-	MIBF_TRY(ctx, cudaMemsetAsync(batch_counts, 0, nc * 8, s));
+	if (phase & kQueryBegin) {
+		MIBF_TRY(ctx, cudaMemsetAsync(batch_counts, 0, nc * 8, s));
+		MIBF_TRY(ctx, cudaMemsetAsync(sc.flags, 0, 4, s));
+		MIBF_TRY(ctx, cudaMemsetAsync(sc.stat, 0, 3 * 8, s));
+		if (timed)
+			MIBF_TRY(ctx, cudaEventRecord(ctx->ev0, s));
+	}
 	MIBF_TRY(ctx, cudaMemsetAsync(sc.work, 0, 8, s));
-	MIBF_TRY(ctx, cudaMemsetAsync(sc.flags, 0, 4, s));
-	MIBF_TRY(ctx, cudaMemsetAsync(sc.stat, 0, 3 * 8, s));
-	if (timed)
-		MIBF_TRY(ctx, cudaEventRecord(ctx->ev0, s));
 	if (n_reads)
 		MIBF_TRY(ctx, launch_query(a, dense, hsel, grid, smem, s));
-	if (timed)
-		MIBF_TRY(ctx, cudaEventRecord(ctx->ev1, s));
-	mibf_commit_kernel<<<1, 256, 0, s>>>(batch_counts, ctx->d_counts, (uint32_t)nc, sc.flags,
-			n_reads);
-	MIBF_TRY(ctx, cudaGetLastError());
+	if (phase & kQueryEnd) {
+		if (timed)
+			MIBF_TRY(ctx, cudaEventRecord(ctx->ev1, s));
+		mibf_commit_kernel<<<1, 256, 0, s>>>(batch_counts, ctx->d_counts, (uint32_t)nc, sc.flags,
+				total_reads);
+		MIBF_TRY(ctx, cudaGetLastError());
+	}
 	return BBT_OK;
 }
 
@@ -1200,31 +1223,102 @@ int bbt::mibf_classify_slot(bbt_mibf *ctx, uint64_t n, const uint8_t *seq, const
 	return run_query_sc(ctx, n, seq, off, seq2, off2, hits, max_hits, n_hits, sat, s, sc, false);
 }
 
-static int grow_staging(bbt_mibf *ctx, uint64_t bases, uint64_t reads, uint32_t max_hits)
+/* Chunk slots of the host-batch pipeline, for chunks of up to `reads` reads
+ * and `bases` bases per mate array. */
+static int grow_chunks(bbt_mibf *ctx, uint64_t bases, uint64_t reads)
 {
-	if (bases > ctx->cap_bases || reads > ctx->cap_reads) {
-		const uint64_t nb = std::max<uint64_t>(bases, ctx->cap_bases);
-		const uint64_t nr = std::max<uint64_t>(reads, ctx->cap_reads);
-		for (int i = 0; i < 2; ++i) {
-			cudaFree(ctx->d_seq[i]);
-			cudaFree(ctx->d_off[i]);
-			ctx->d_seq[i] = nullptr;
-			ctx->d_off[i] = nullptr;
-			MIBF_TRY(ctx, cudaMalloc(&ctx->d_seq[i], std::max<uint64_t>(nb, 16)));
-			MIBF_TRY(ctx, cudaMalloc(&ctx->d_off[i], (nr + 1) * 8));
+	if (!ctx->h2d) {
+		MIBF_TRY(ctx, cudaStreamCreateWithFlags(&ctx->h2d, cudaStreamNonBlocking));
+		MIBF_TRY(ctx, cudaStreamCreateWithFlags(&ctx->d2h, cudaStreamNonBlocking));
+		for (int c = 0; c < 2; ++c) {
+			MIBF_TRY(ctx, cudaEventCreateWithFlags(&ctx->c_copied[c], cudaEventDisableTiming));
+			MIBF_TRY(ctx, cudaEventCreateWithFlags(&ctx->c_computed[c], cudaEventDisableTiming));
 		}
-		ctx->cap_bases = nb;
-		ctx->cap_reads = nr;
 	}
-	if (reads > ctx->res_cap_reads || max_hits > ctx->res_cap_hits ||
-			(uint64_t)reads * max_hits > (uint64_t)ctx->res_cap_reads * ctx->res_cap_hits) {
-		const uint64_t nr = std::max<uint64_t>(reads, ctx->res_cap_reads);
-		const uint32_t nh = std::max<uint32_t>(max_hits, ctx->res_cap_hits);
+	if (bases <= ctx->c_bases_cap && reads <= ctx->c_reads_cap)
+		return BBT_OK;
+	const uint64_t nb = std::max(bases, ctx->c_bases_cap), nr = std::max(reads, ctx->c_reads_cap);
+	MIBF_TRY(ctx, cudaDeviceSynchronize());
+	ctx->c_bases_cap = ctx->c_reads_cap = 0;
+	for (int c = 0; c < 2; ++c)
+		for (int m = 0; m < 2; ++m) {
+			cudaFree(ctx->c_seq[c][m]);
+			cudaFree(ctx->c_off[c][m]);
+			cudaFreeHost(ctx->h_coff[c][m]);
+			ctx->c_seq[c][m] = nullptr;
+			ctx->c_off[c][m] = nullptr;
+			ctx->h_coff[c][m] = nullptr;
+			MIBF_TRY(ctx, cudaMalloc(&ctx->c_seq[c][m], std::max<uint64_t>(nb, 16)));
+			MIBF_TRY(ctx, cudaMalloc(&ctx->c_off[c][m], (nr + 1) * 8));
+			MIBF_TRY(ctx, cudaMallocHost(&ctx->h_coff[c][m], (nr + 1) * 8));
+		}
+	ctx->c_bases_cap = nb;
+	ctx->c_reads_cap = nr;
+	return BBT_OK;
+}
+
+/* Reads per chunk of the host-batch pipeline, and bases per mate array. */
+constexpr uint64_t kChunkReads = 1ull << 20;
+constexpr uint64_t kChunkBases = 256ull << 20;
+
+/*
+ * Host batch: the reads go in chunks through two slots.  Chunk c is
+ * classified on the context's stream while chunk c + 1's bases and offsets
+ * are copied in on a second stream and chunk c - 1's results go out on a
+ * third, so the copies overlap the classification.  The chunks' launches
+ * share the batch's counters, committed once after the last (none if a read
+ * overflowed max_hits), so results and summary equal one launch's.
+ */
+static int classify_host_chunks(bbt_mibf *ctx, const bbt_batch *b, bbt_mibf_result *res,
+		cudaStream_t s)
+{
+	const uint64_t n = b->n_reads;
+	if (n == 0) {
+		ctx->last_kernel_ms = 0;
+		return BBT_OK;
+	}
+	const bool paired = b->seq2 != nullptr;
+	auto bases = [&](uint64_t lo, uint64_t hi) {
+		uint64_t x = b->offsets[hi] - b->offsets[lo];
+		if (paired)
+			x = std::max(x, b->offsets2[hi] - b->offsets2[lo]);
+		return x;
+	};
+	std::vector<uint64_t> cuts(1, 0);
+	uint64_t most_reads = 1, most_bases = 16;
+	while (cuts.back() < n) {
+		const uint64_t r0 = cuts.back();
+		uint64_t r1 = std::min(n, r0 + kChunkReads);
+		if (r1 - r0 > 1 && bases(r0, r1) > kChunkBases) {
+			uint64_t lo = r0 + 1, hi = r1;
+			while (lo < hi) {
+				const uint64_t mid = (lo + hi + 1) / 2;
+				if (bases(r0, mid) <= kChunkBases)
+					lo = mid;
+				else
+					hi = mid - 1;
+			}
+			r1 = lo;
+		}
+		most_reads = std::max(most_reads, r1 - r0);
+		most_bases = std::max(most_bases, bases(r0, r1));
+		cuts.push_back(r1);
+	}
+	int rc = grow_chunks(ctx, most_bases, most_reads);
+	if (rc)
+		return rc;
+	/* device result arrays for the whole batch */
+	if (n > ctx->res_cap_reads || res->max_hits > ctx->res_cap_hits ||
+			n * res->max_hits > ctx->res_cap_reads * (uint64_t)ctx->res_cap_hits) {
+		const uint64_t nr = std::max<uint64_t>(n, ctx->res_cap_reads);
+		const uint32_t nh = std::max<uint32_t>(res->max_hits, ctx->res_cap_hits);
 		cudaFree(ctx->d_hits);
 		cudaFree(ctx->d_nhits);
 		cudaFree(ctx->d_sat);
 		ctx->d_hits = nullptr;
 		ctx->d_nhits = ctx->d_sat = nullptr;
+		ctx->res_cap_reads = 0;
+		ctx->res_cap_hits = 0;
 		MIBF_TRY(ctx, cudaMalloc(&ctx->d_hits, std::max<uint64_t>(nr * nh, 1) *
 				sizeof(bbt_mibf_hit)));
 		MIBF_TRY(ctx, cudaMalloc(&ctx->d_nhits, std::max<uint64_t>(nr, 1) * 4));
@@ -1232,6 +1326,71 @@ static int grow_staging(bbt_mibf *ctx, uint64_t bases, uint64_t reads, uint32_t 
 		ctx->res_cap_reads = nr;
 		ctx->res_cap_hits = nh;
 	}
+	const size_t nchunks = cuts.size() - 1;
+	/* input of chunk c into slot c % 2 (after the launch that last read it) */
+	auto copy_in = [&](size_t c) -> int {
+		const int sl = (int)(c & 1);
+		const uint64_t r0 = cuts[c], r1 = cuts[c + 1], cnt = r1 - r0;
+		if (c >= 2)
+			MIBF_TRY(ctx, cudaStreamWaitEvent(ctx->h2d, ctx->c_computed[sl], 0));
+		/* the pinned offsets of chunk c - 2 have been copied */
+		MIBF_TRY(ctx, cudaEventSynchronize(ctx->c_copied[sl]));
+		for (int m = 0; m < (paired ? 2 : 1); ++m) {
+			const char *seq = m ? b->seq2 : b->seq;
+			const uint64_t *off = m ? b->offsets2 : b->offsets;
+			uint64_t *ho = ctx->h_coff[sl][m];
+			const uint64_t o0 = off[r0];
+			for (uint64_t i = 0; i <= cnt; ++i)
+				ho[i] = off[r0 + i] - o0;
+			if (off[r1] > o0)
+				MIBF_TRY(ctx, cudaMemcpyAsync(ctx->c_seq[sl][m], seq + o0, off[r1] - o0,
+						cudaMemcpyHostToDevice, ctx->h2d));
+			MIBF_TRY(ctx, cudaMemcpyAsync(ctx->c_off[sl][m], ho, (cnt + 1) * 8,
+					cudaMemcpyHostToDevice, ctx->h2d));
+		}
+		MIBF_TRY(ctx, cudaEventRecord(ctx->c_copied[sl], ctx->h2d));
+		return BBT_OK;
+	};
+	for (int c = 0; c < 2; ++c) /* no copy is pending on either slot */
+		MIBF_TRY(ctx, cudaEventRecord(ctx->c_copied[c], ctx->h2d));
+	if (nchunks && (rc = copy_in(0)))
+		return rc;
+	const MibfScratch sc = ctx_scratch(ctx);
+	for (size_t c = 0; c < nchunks; ++c) {
+		const int sl = (int)(c & 1);
+		const uint64_t r0 = cuts[c], cnt = cuts[c + 1] - r0;
+		MIBF_TRY(ctx, cudaStreamWaitEvent(s, ctx->c_copied[sl], 0));
+		const int phase = (c == 0 ? kQueryBegin : 0) | (c + 1 == nchunks ? kQueryEnd : 0);
+		rc = run_query_sc(ctx, cnt, ctx->c_seq[sl][0], ctx->c_off[sl][0],
+				paired ? ctx->c_seq[sl][1] : nullptr, paired ? ctx->c_off[sl][1] : nullptr,
+				ctx->d_hits + r0 * res->max_hits, res->max_hits, ctx->d_nhits + r0,
+				ctx->d_sat + r0, s, sc, true, phase, n);
+		if (rc)
+			return rc;
+		MIBF_TRY(ctx, cudaEventRecord(ctx->c_computed[sl], s));
+		if (c + 1 < nchunks && (rc = copy_in(c + 1)))
+			return rc;
+		/* results of chunk c */
+		MIBF_TRY(ctx, cudaStreamWaitEvent(ctx->d2h, ctx->c_computed[sl], 0));
+		MIBF_TRY(ctx, cudaMemcpyAsync(res->n_hits + r0, ctx->d_nhits + r0, cnt * 4,
+				cudaMemcpyDeviceToHost, ctx->d2h));
+		MIBF_TRY(ctx, cudaMemcpyAsync(res->sat_count + r0, ctx->d_sat + r0, cnt * 4,
+				cudaMemcpyDeviceToHost, ctx->d2h));
+		if (res->max_hits)
+			MIBF_TRY(ctx, cudaMemcpyAsync(res->hits + r0 * res->max_hits,
+					ctx->d_hits + r0 * res->max_hits,
+					cnt * res->max_hits * sizeof(bbt_mibf_hit), cudaMemcpyDeviceToHost, ctx->d2h));
+	}
+	unsigned int flag = 0;
+	MIBF_TRY(ctx, cudaMemcpyAsync(&flag, ctx->d_flags, 4, cudaMemcpyDeviceToHost, s));
+	MIBF_TRY(ctx, cudaStreamSynchronize(s));
+	MIBF_TRY(ctx, cudaStreamSynchronize(ctx->d2h));
+	MIBF_TRY(ctx, cudaStreamSynchronize(ctx->h2d));
+	float ms = 0;
+	cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+	ctx->last_kernel_ms = ms;
+	if (flag)
+		return mibf_fail(ctx, BBT_ERR_OVERFLOW, "a read has more significant IDs than max_hits");
 	return BBT_OK;
 }
 
@@ -1262,66 +1421,11 @@ extern "C" int bbt_mibf_classify_batch(bbt_mibf *ctx, const bbt_batch *b, bbt_mi
 		return run_query(ctx, b, (const uint8_t *)b->seq, b->offsets, (const uint8_t *)b->seq2,
 				b->offsets2, res->hits, res->max_hits, res->n_hits, res->sat_count, s);
 	}
-	/* host batch: stage in, classify, copy out */
-	const uint64_t n = b->n_reads;
-	const uint64_t s1 = n ? b->offsets[0] : 0, e1 = n ? b->offsets[n] : 0;
-	const uint64_t s2 = (n && b->seq2) ? b->offsets2[0] : 0;
-	const uint64_t e2 = (n && b->seq2) ? b->offsets2[n] : 0;
-	rc = grow_staging(ctx, std::max(e1 - s1, e2 - s2), n, res->max_hits);
-	if (rc)
-		return rc;
+	/* host batch: chunks through two slots, copies overlapping the launches */
 	rc = ensure_min_count(ctx, host_frame_counts(b, ctx->hd.k), s);
 	if (rc)
 		return rc;
-	/* offsets are copied as they are when they start at 0, else rebased */
-	std::vector<uint64_t> o1, o2;
-	const uint64_t *h_o1 = b->offsets, *h_o2 = b->offsets2;
-	if (n && s1) {
-		o1.resize(n + 1);
-		for (uint64_t i = 0; i <= n; ++i)
-			o1[i] = b->offsets[i] - s1;
-		h_o1 = o1.data();
-	}
-	if (n && b->seq2 && s2) {
-		o2.resize(n + 1);
-		for (uint64_t i = 0; i <= n; ++i)
-			o2[i] = b->offsets2[i] - s2;
-		h_o2 = o2.data();
-	}
-	if (n) {
-		MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_seq[0], b->seq + s1, e1 - s1, cudaMemcpyHostToDevice,
-				s));
-		MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_off[0], h_o1, (n + 1) * 8, cudaMemcpyHostToDevice,
-				s));
-		if (b->seq2) {
-			MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_seq[1], b->seq2 + s2, e2 - s2,
-					cudaMemcpyHostToDevice, s));
-			MIBF_TRY(ctx, cudaMemcpyAsync(ctx->d_off[1], h_o2, (n + 1) * 8,
-					cudaMemcpyHostToDevice, s));
-		}
-	}
-	rc = run_query(ctx, b, ctx->d_seq[0], ctx->d_off[0], b->seq2 ? ctx->d_seq[1] : nullptr,
-			b->seq2 ? ctx->d_off[1] : nullptr, ctx->d_hits, res->max_hits, ctx->d_nhits,
-			ctx->d_sat, s);
-	if (rc)
-		return rc;
-	unsigned int flag = 0;
-	if (n) {
-		MIBF_TRY(ctx, cudaMemcpyAsync(res->n_hits, ctx->d_nhits, n * 4, cudaMemcpyDeviceToHost, s));
-		MIBF_TRY(ctx, cudaMemcpyAsync(res->sat_count, ctx->d_sat, n * 4, cudaMemcpyDeviceToHost,
-				s));
-		if (res->max_hits)
-			MIBF_TRY(ctx, cudaMemcpyAsync(res->hits, ctx->d_hits,
-					n * res->max_hits * sizeof(bbt_mibf_hit), cudaMemcpyDeviceToHost, s));
-	}
-	MIBF_TRY(ctx, cudaMemcpyAsync(&flag, ctx->d_flags, 4, cudaMemcpyDeviceToHost, s));
-	MIBF_TRY(ctx, cudaStreamSynchronize(s));
-	float ms = 0;
-	cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-	ctx->last_kernel_ms = ms;
-	if (flag)
-		return mibf_fail(ctx, BBT_ERR_OVERFLOW, "a read has more significant IDs than max_hits");
-	return BBT_OK;
+	return classify_host_chunks(ctx, b, res, s);
 }
 
 extern "C" int bbt_mibf_sync(bbt_mibf *ctx)

@@ -97,15 +97,19 @@ struct bbt_mibf {
 	std::vector<uint8_t> minc_have;
 	uint32_t *d_minc = nullptr;
 	uint32_t minc_rows = 0;               /* rows allocated on the device */
-	/* host-batch staging */
-	uint8_t *d_seq[2] = {nullptr, nullptr};
-	uint64_t *d_off[2] = {nullptr, nullptr};
-	uint64_t cap_bases = 0, cap_reads = 0;
+	/* host-batch results on the device */
 	bbt_mibf_hit *d_hits = nullptr;
 	uint32_t *d_nhits = nullptr, *d_sat = nullptr;
 	uint64_t res_cap_reads = 0;
 	uint32_t res_cap_hits = 0;
 	unsigned int *d_fcmax = nullptr;
+	/* host-batch pipeline: two chunk slots, each with its chunk's bases and
+	 * rebased offsets on the device and the offsets in pinned memory */
+	uint8_t *c_seq[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+	uint64_t *c_off[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+	uint64_t *h_coff[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+	uint64_t c_bases_cap = 0, c_reads_cap = 0;
+	cudaEvent_t c_copied[2] = {nullptr, nullptr}, c_computed[2] = {nullptr, nullptr};
 	uint64_t reads_seen = 0;
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	double last_kernel_ms = 0;

@@ -252,3 +252,83 @@ def test_gpu_maker_multi_contig_ids(tmp_path):
     for ext in (".bf", ".sdsl"):
         with open(str(tmp_path / "o") + ext, "rb") as a, open(str(tmp_path / "g") + ext, "rb") as b:
             assert a.read() == b.read(), ext
+
+
+def _many_reads(rng, targets, n, length):
+    """n reads of `length` bases: 80% substrings of the targets, 20% random."""
+    genome = np.frombuffer(b"".join(targets), dtype=np.uint8)
+    starts = rng.integers(0, len(genome) - length, n)
+    idx = starts[:, None] + np.arange(length)[None, :]
+    seq = genome[idx]
+    rand = rng.random(n) < 0.2
+    seq[rand] = np.frombuffer(b"ACGT", dtype=np.uint8)[rng.integers(0, 4, (int(rand.sum()),
+                                                                           length))]
+    off = np.arange(n + 1, dtype=np.uint64) * np.uint64(length)
+    return np.ascontiguousarray(seq.reshape(-1)), off
+
+
+def _abi_host(mc, seq, off, seq2, off2, max_hits):
+    import ctypes
+
+    from biobloom_b200 import _lib as L
+    n = len(off) - 1
+    b = L.Batch()
+    b.seq, b.offsets, b.n_reads, b.location = seq.ctypes.data, off.ctypes.data, n, L.HOST
+    if seq2 is not None:
+        b.seq2, b.offsets2 = seq2.ctypes.data, off2.ctypes.data
+    hits = np.zeros((n, max_hits, 7), dtype=np.uint32)
+    nh = np.zeros(n, dtype=np.uint32)
+    sat = np.zeros(n, dtype=np.uint32)
+    r = L.MibfResult()
+    r.hits, r.max_hits, r.n_hits, r.sat_count, r.location = (
+        hits.ctypes.data, max_hits, nh.ctypes.data, sat.ctypes.data, L.HOST)
+    rc = L.lib().bbt_mibf_classify_batch(mc._ctx, ctypes.byref(b), ctypes.byref(r), None)
+    return rc, hits, nh, sat
+
+
+@pytest.mark.parametrize("paired", [False, True])
+def test_host_batch_in_chunks_matches_one_device_launch(built, paired):
+    """A host batch of more than one pipeline chunk (1M reads) gives the
+    results and summary of the same reads classified in one device launch;
+    with too few result slots it reports the overflow, keeps n_hits exact and
+    adds nothing to the summary."""
+    import torch
+
+    from biobloom_b200 import _lib as L
+    from biobloom_b200.mibf import MIBFClassifier
+    targets, filters, _, names = built
+    path, _ = filters["ss"]
+    rng = np.random.default_rng(21)
+    n = 1_100_000
+    seq, off = _many_reads(rng, targets, n, 40)
+    seq2 = off2 = None
+    if paired:
+        seq2, off2 = _many_reads(rng, targets, n, 60)
+    mh = 8
+    a = MIBFClassifier(path)
+    rc, hits, nh, sat = _abi_host(a, seq, off, seq2, off2, mh)
+    assert rc == 0
+    counts_a, reads_a = a.summary()
+    d = MIBFClassifier(path)
+    t = lambda x: torch.from_numpy(x.astype(np.int64) if x.dtype == np.uint64 else x).cuda()
+    dh, dn, ds = d.classify_device(t(seq), t(off), t(seq2) if paired else None,
+                                   t(off2) if paired else None, max_hits=mh)
+    d.sync()
+    torch.cuda.synchronize()
+    dn = dn.cpu().numpy().view(np.uint32)
+    assert np.array_equal(nh, dn)
+    assert np.array_equal(sat, ds.cpu().numpy().view(np.uint32))
+    dh = dh.cpu().numpy().view(np.uint32).reshape(n, mh, 7)
+    keep = np.arange(mh)[None, :] < nh[:, None]
+    assert np.array_equal(hits[keep], dh[keep])
+    counts_d, reads_d = d.summary()
+    assert reads_a == reads_d == n and np.array_equal(counts_a, counts_d)
+    assert nh.max() > 1
+    # overflow: one result slot while some reads have more
+    rc, _, nh1, _ = _abi_host(a, seq, off, seq2, off2, 1)
+    assert rc == L.ERR_OVERFLOW
+    assert np.array_equal(nh1, nh)
+    counts_b, reads_b = a.summary()
+    assert reads_b == reads_a and np.array_equal(counts_b, counts_a)
+    a.close()
+    d.close()
