@@ -967,6 +967,11 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 	}
 	uint64_t i0 = 0;
 	int which = 0;
+	/* at least about eight slot loads per call (of 64k reads or more), so
+	 * that a batch that fits one slot still overlaps its copies with its
+	 * kernels */
+	const uint64_t step = std::min<uint64_t>(ctx->cap_reads,
+			std::max<uint64_t>(1ull << 16, (n + 7) / 8));
 	const bool out_pinned[5] = {r->hits && host_pinned(r->hits),
 			paired && r->hits2 && host_pinned(r->hits2),
 			r->category && host_pinned(r->category),
@@ -978,7 +983,7 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 	CUDA_TRY(ctx, cudaEventRecord(ctx->ev_start, ctx->stream));
 	while (i0 < n) {
 		/* largest i1 with bases and reads inside the slot capacity */
-		uint64_t i1 = std::min(n, i0 + ctx->cap_reads);
+		uint64_t i1 = std::min(n, i0 + step);
 		auto bases = [&](uint64_t lo, uint64_t hi) {
 			uint64_t x = b->offsets[hi] - b->offsets[lo];
 			if (paired)

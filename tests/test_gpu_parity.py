@@ -293,3 +293,42 @@ def test_gpu_maker_matches_oracle_maker(tmp_path):
     assert np.array_equal(mine.bits(), ref.bits())
     info = open(stem + ".txt").read()
     assert "filter_id=m\n" in info and "kmer_size=25\n" in info
+
+
+@pytest.mark.parametrize("paired", [False, True])
+def test_host_batch_in_slot_loads_matches_device_batch(tmp_path, paired):
+    """A host batch that fits one staging slot still goes through the slots in
+    about eight loads (copies overlapping kernels); results, categories and
+    summary equal one device-resident call's."""
+    import torch
+    rng, genomes, filters = _random_case(31)
+    paths = []
+    for i, f in enumerate(filters):
+        stem = str(tmp_path / f"s{i}")
+        f.store(stem + ".bf")
+        ol.write_info(stem + ".txt", f"s{i}", f.k, 0.075, f.h, 1, "x", f.m, 1, 0.1, 0, 0.1)
+        paths.append(stem + ".bf")
+    n = 600_000
+    g = np.concatenate(genomes)
+    st = rng.integers(0, len(g) - 80, n)
+    seq = g[st[:, None] + np.arange(80)[None, :]].reshape(-1).copy()
+    off = np.arange(n + 1, dtype=np.uint64) * np.uint64(80)
+    seq2 = None
+    if paired:
+        st2 = rng.integers(0, len(g) - 80, n)
+        seq2 = g[st2[:, None] + np.arange(80)[None, :]].reshape(-1).copy()
+    with _classifier(paths) as a:
+        h, h2, c = a.classify((seq, off), (seq2, off) if paired else None)
+        ca, na = a.summary()
+    with _classifier(paths) as d:
+        t = lambda x: torch.from_numpy(x.astype(np.int64) if x.dtype == np.uint64 else x).cuda()
+        dh, dh2, dc = d.classify_device(t(seq), t(off), t(seq2) if paired else None,
+                                        t(off) if paired else None)
+        torch.cuda.synchronize()
+        cd, nd = d.summary()
+    assert np.array_equal(h, dh.cpu().numpy().view(np.uint64))
+    if paired:
+        assert np.array_equal(h2, dh2.cpu().numpy().view(np.uint64))
+    assert np.array_equal(c, dc.cpu().numpy().view(np.uint32))
+    assert na == nd == n and np.array_equal(ca, cd)
+    assert h.any()
