@@ -392,6 +392,9 @@ extern "C" int bbt_server_create(bbt_ctx *bloom, bbt_mibf *mibf, const bbt_serve
 	};
 	if (cudaSetDevice(srv->dev) != cudaSuccess)
 		return bail(BBT_ERR_CUDA, "cudaSetDevice failed");
+	if (bloom && bloom->dust)
+		return bail(BBT_ERR_UNSUPPORTED, "bbt_server_create: the serving engine does not run "
+				"DUST masking (switch it off with bbt_set_dust)");
 	if (bloom && bf_reserve_rows(bloom, (uint64_t)srv->p.max_frames + bloom->kmax))
 		return bail(BBT_ERR_NOMEM, "cannot reserve the binomial threshold rows: " + bloom->err);
 	if (mibf && mibf_reserve_rows(mibf, srv->p.max_frames + 1))

@@ -75,7 +75,10 @@ typedef struct {
 } bbt_request_stats;
 
 /* Either context may be NULL (requests of that kind are then refused).  The
- * caller must not use the contexts while the server runs. */
+ * caller must not use the contexts while the server runs.  Bloom requests
+ * follow the context's filtering mode (bbt_set_mode): ORDERED and BESTHIT
+ * give their hit words and summary; SCORES gives the STD hits (requests carry
+ * no scores).  A context with DUST masking on is refused. */
 int bbt_server_create(bbt_ctx *bloom, bbt_mibf *mibf, const bbt_server_params *params,
 		bbt_server **out);
 /* Queue a request; *ticket identifies it. */

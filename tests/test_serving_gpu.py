@@ -152,3 +152,41 @@ def test_overflow_is_reported_per_request(contexts):
         ok = srv.submit_mibf(reads, max_hits=mc.num_ids)
         srv.wait(ok)
         assert srv.mibf_results(ok) == want
+
+
+@pytest.mark.parametrize("mode", ["ordered", "besthit"])
+def test_bloom_requests_follow_the_filtering_mode(contexts, mode):
+    """ORDERED and BESTHIT requests give the hit words and categories of the
+    batch entry point in the same mode."""
+    from biobloom_b200 import MODE_BESTHIT, MODE_STD
+    from biobloom_b200.server import Server
+    bbc, mc, genomes = contexts
+    rng = np.random.default_rng(5 if mode == "ordered" else 6)
+    reqs = [(_reads(rng, genomes, n), _reads(rng, genomes, n)) for n in (3, 900, 60)]
+    if mode == "ordered":
+        bbc.setOrderedFilter()
+    else:
+        bbc.set_mode(MODE_BESTHIT)
+    try:
+        with Server(bbc, None, slots=2) as srv:
+            hs = [srv.submit_bloom(r1, None, r2, None) for r1, r2 in reqs]
+            for h in hs:
+                srv.wait(h)
+        for (r1, r2), h in zip(reqs, hs):
+            w1, w2, wc = bbc.classify(r1, r2)
+            assert np.array_equal(h.hits[:h.n], w1) and np.array_equal(h.hits2[:h.n], w2)
+            assert np.array_equal(h.category[:h.n], wc)
+    finally:
+        bbc.set_mode(MODE_STD)
+
+
+def test_server_refuses_a_dust_context(contexts):
+    from biobloom_b200 import BBTError
+    from biobloom_b200.server import Server
+    bbc, mc, genomes = contexts
+    bbc.set_dust(True)
+    try:
+        with pytest.raises(BBTError):
+            Server(bbc, None, slots=1)
+    finally:
+        bbc.set_dust(False)
