@@ -180,9 +180,11 @@ def write_fastq(path, seq, off, lo, hi):
         f.write(b"".join(buf))
 
 
-def cpu_reference_run(d, paths, s1, s2, off, n_pairs, threads):
+def cpu_reference_run(d, paths, s1, s2, off, n_pairs, threads, score=None, env=None):
     """Time the reference's own classifier (oracle/_ref/ref_harness, compiled
-    from the reference sources) on n_pairs pairs with `threads` threads."""
+    from the reference sources) on n_pairs pairs with `threads` threads; env
+    selects a scoring method (BBT_SCORING), filtering mode (BBT_MODE) or DUST
+    (BBT_DUST) for the harness."""
     harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
     if not os.path.exists(harness):
         return None, "oracle/_ref/ref_harness is not built"
@@ -191,9 +193,10 @@ def cpu_reference_run(d, paths, s1, s2, off, n_pairs, threads):
     if not os.path.exists(f2):
         write_fastq(f1, s1, off, 0, n_pairs)
         write_fastq(f2, s2, off, 0, n_pairs)
-    p = subprocess.run([harness, "time", str(SCORE), str(STREAK), str(threads), "0",
-                        os.path.join(d, "refcpu"), ",".join(paths), f1, f2],
-                       capture_output=True, text=True)
+    p = subprocess.run([harness, "time", str(SCORE if score is None else score), str(STREAK),
+                        str(threads), "0", os.path.join(d, "refcpu"), ",".join(paths), f1, f2],
+                       capture_output=True, text=True,
+                       env=dict(os.environ, **(env or {})))
     if p.returncode:
         return None, "ref_harness failed: " + p.stderr[-300:]
     line = [x for x in p.stdout.splitlines() if x.startswith("{")][-1]
@@ -548,6 +551,31 @@ def mode_oracle(ol, filters, name, kw, mode, dust, s, off):
     return ol.classify(seq, off, filters, thr, STREAK, scoring)[0]
 
 
+def mode_cpu(d, paths, s1, s2, off, kw, mode, dust, budget_s=8.0):
+    """The reference's BioBloomClassifier::filterPair in one variant's mode and
+    scoring method, on a bounded sample of the same pairs, all host threads."""
+    env = {}
+    st = kw.get("score_type", "simple")
+    if st != "simple":
+        env["BBT_SCORING"] = st
+    if mode in ("ordered", "besthit", "scores"):
+        env["BBT_MODE"] = mode
+    if dust:
+        env["BBT_DUST"] = "20,64"
+    threads = os.cpu_count() or 1
+    probe = 2000
+    r, err = cpu_reference_run(d, paths, s1, s2, off, probe, threads, kw["score_threshold"], env)
+    if r is None:
+        return {"unavailable": err}
+    rate = probe / max(r["seconds"], 1e-6)
+    n = max(probe, (int(min(len(off) - 1, rate * budget_s)) // 1000) * 1000)
+    r, err = cpu_reference_run(d, paths, s1, s2, off, n, threads, kw["score_threshold"], env)
+    if r is None:
+        return {"unavailable": err}
+    return {"reads_per_s": 2 * r["records"] / r["seconds"], "cores": r["threads"],
+            "sample_pairs": r["records"], "kind": "reference"}
+
+
 def run_modes(args):
     """Every filtering mode and scoring method on the 10-filter workload's
     data (device-resident reads, CUDA-event timing per step), each checked
@@ -619,6 +647,17 @@ def run_modes(args):
                 w1, w2 = ol.ordered(w1, len(filters), w2, False)
             res["checked_pairs"] = n_check
             res["mismatched_reads"] = int((g1 != w1).any(1).sum() + (g2 != w2).any(1).sum())
+        if not args.no_cpu and kw.get("score_type") == "binomial":
+            res["cpu_reference"] = {
+                "unavailable": "the reference's binomial scoring needs Boost, which is not "
+                               "installed here; the compiled reference runs on this build's "
+                               "stand-in for boost::math::binomial, whose quantile search is "
+                               "far slower than Boost's, so its time would not be the "
+                               "reference's"}
+        elif not args.no_cpu:
+            res["cpu_reference"] = mode_cpu(d, paths, s1, s2, off, kw, mode, dust)
+            if res["cpu_reference"].get("reads_per_s"):
+                res["vs_cpu_reference"] = res["reads_per_s"] / res["cpu_reference"]["reads_per_s"]
         out[name] = res
         bbc.close()
         log(name, json.dumps(res))

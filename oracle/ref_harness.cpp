@@ -19,6 +19,7 @@
  *       For every read, prints "<name>\t<start>-<finish>,..." with the
  *       intervals the reference's sdust (Common/sdust.c) masks.
  *   ref_harness time  SCORE STREAK THREADS INCLUSIVE PREFIX FILTERS READS [READS2]
+ *       (BBT_MODE = ordered / besthit / scores selects a filtering mode)
  *       Builds a BioBloomClassifier (BioBloomClassifier.cpp:21-28; filter
  *       load not timed), then times filter()/filterPair() and prints one JSON
  *       line with the wall time, reads and cores used.
@@ -252,6 +253,7 @@ static int mode_time(int argc, char **argv)
 		return 2;
 	}
 	set_score(atof(argv[2]));
+	set_dust();
 	opt::streakThreshold = (unsigned)atoi(argv[3]);
 	int threads = atoi(argv[4]);
 	if (threads > 0)
@@ -265,6 +267,16 @@ static int mode_time(int argc, char **argv)
 	BioBloomClassifier bbc(paths, opt::score, opt::outputPrefix, opt::filePostfix);
 	if (inclusive)
 		bbc.setInclusive();
+	/* BBT_MODE: the filtering mode (-c, -b, -w; BioBloomCategorizer.cpp:
+	 * 276-318, 460-464) */
+	const char *md = getenv("BBT_MODE");
+	const string mode = md ? md : "";
+	if (mode == "ordered")
+		bbc.setOrderedFilter();
+	else if (mode == "besthit")
+		opt::mode = opt::BESTHIT;
+	else if (mode == "scores")
+		opt::mode = opt::SCORES;
 	double t0 = omp_get_wtime();
 	if (paired)
 		bbc.filterPair(argv[8], argv[9]);
