@@ -31,6 +31,7 @@ public:
 			std::cerr << "BloomFilter: cannot load " << path << " (" << rc << ")" << std::endl;
 			exit(1);
 		}
+		m_fpr = getFPR();
 	}
 	~BloomFilter() { oracle_bf_free(&m_bf); }
 	BloomFilter(const BloomFilter &) = delete;
@@ -56,7 +57,10 @@ public:
 	double getFPR() const {
 		return std::pow(double(getPop()) / double(m_bf.m), double(m_bf.h));
 	}
-	double getFPRPrecompute() const { return getFPR(); }
+	/* the FPR of a filter loaded from a file, computed once at load (SeqEval
+	 * calls this for every read it evaluates under BINOMIAL scoring, from
+	 * several threads) */
+	double getFPRPrecompute() const { return m_fpr >= 0 ? m_fpr : getFPR(); }
 	void storeFilter(const std::string &path) const {
 		if (oracle_bf_store(&m_bf, path.c_str())) {
 			std::cerr << "BloomFilter: cannot write " << path << std::endl;
@@ -71,5 +75,6 @@ public:
 	const oracle_bf &raw() const { return m_bf; }
 private:
 	oracle_bf m_bf;
+	double m_fpr = -1.0; /* FPR computed at load (getFPRPrecompute) */
 };
 #endif
