@@ -1021,14 +1021,15 @@ void oracle_classify_scores(const char *seq, const uint64_t *off, size_t n,
 		const oracle_bf *const *filters, unsigned nf, int scoring,
 		unsigned streak_threshold, double *scores)
 {
+	double fpr[1024];
+	for (unsigned f = 0; f < nf && f < 1024; ++f)
+		fpr[f] = scoring == ORACLE_BINOMIAL ? oracle_bf_fpr(filters[f]) : 0.0;
 	for (size_t r = 0; r < n; ++r) {
 		const char *s = seq + off[r];
 		size_t len = (size_t)(off[r + 1] - off[r]);
-		for (unsigned f = 0; f < nf; ++f) {
-			double fpr = scoring == ORACLE_BINOMIAL ? oracle_bf_fpr(filters[f]) : 0.0;
+		for (unsigned f = 0; f < nf && f < 1024; ++f)
 			scores[r * nf + f] = oracle_eval_score(s, len, filters[f], scoring,
-					streak_threshold, fpr);
-		}
+					streak_threshold, fpr[f]);
 	}
 }
 
