@@ -141,8 +141,11 @@ typedef struct {
  * Classify a batch (bbt_batch of bbt.h; pairs when seq2 != NULL) and add it to
  * the summary counters.  Replaces MIBFClassifier::classify (single,
  * MIBFClassifier.hpp:772-796; paired, :801-834) over every read of the batch.
- * Host buffers: returns when the results are in place.  Device buffers: runs
- * on `stream` (NULL = the context's stream) and returns when enqueued, except
+ * Host buffers: returns when the results are in place; the reads go through
+ * the device in chunks of up to 1M reads, each chunk's copies overlapping the
+ * classification of the one before (pinned host arrays overlap best), with
+ * the results and summary of a single launch.  Device buffers: runs on
+ * `stream` (NULL = the context's stream) and returns when enqueued, except
  * that the first batch with a new read length waits for the minCount table.
  */
 int bbt_mibf_classify_batch(bbt_mibf *ctx, const bbt_batch *batch, bbt_mibf_result *result,
