@@ -132,9 +132,12 @@ typedef struct {
  * Classify one batch and add it to the context's summary counters.
  * Replaces the per-read loop of BioBloomClassifier::filter / filterPair
  * (BioBloomClassifier.cpp:33-100, 217-303).  With BBT_HOST buffers the call
- * copies inputs in and results out and returns when they are in place; with
- * BBT_DEVICE buffers it enqueues on `stream` and returns (results are ready
- * when the stream reaches that point).
+ * copies inputs in and results out and returns when they are in place (the
+ * reads go through two device staging slots in about eight loads, each load's
+ * copies overlapping the kernels of the one before; pinned host arrays
+ * overlap best, results bound for pageable memory are staged through pinned
+ * buffers); with BBT_DEVICE buffers it enqueues on `stream` and returns
+ * (results are ready when the stream reaches that point).
  */
 int bbt_classify_batch(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *result,
 		void *stream);
