@@ -1,20 +1,30 @@
 #!/usr/bin/env python3
 """Benchmark of the read-classification path on B200.
 
-Workload (default): 10 Bloom filters (k=25, FPR 0.075, hash count auto = 3),
-each built from an independent seeded 100 Mbp reference (41% GC, 5% of each
-reference in 300 bp repeat copies); 10M read pairs 2x150 bp, 10% drawn from
-each reference with 0.5% substitutions and 0.01% N (the 10 x 10% leave no
-uniform-random remainder at these settings).  Synthetic data: no dataset is
-available on the box.
+Workload (default, --workload varlen): one Bloom filter (k=25, FPR 0.075,
+hash count auto = 3, 2.12 GB by the reference's sizing formula) from a seeded
+3.1 Gbp reference (41% GC, 45% of bases in repeat families of 300 bp - 6 kb at
+10-20% divergence); 50M single-end reads, 95% of lengths log-uniform over
+50-300 bp and 5% log-uniform over 300 bp - 10 kb, 70% drawn from the
+reference with 1% substitutions and 30% uniform random; score 0.15.
+Synthetic data: no dataset is available on the box.
 
-A step classifies all pairs once (persistent work-stealing kernel, reads
-resident in HBM, 3 GB of bases and 685 MB of filters: far above the 126 MB L2,
-so no L2 flush is needed between steps).  `value` is reads/s over the timed
-steps (device time, CUDA events); `e2e` is the same metric through the C ABI
-with pinned host buffers (host->device copies of the reads and device->host
-copies of the per-read results inside the timed region); `plain` is the
-one-warp-per-read, one-launch-per-batch kernel on the same data.
+A step classifies all reads once (13.5 G bases and the 2.12 GB filter resident
+in HBM, far above the 126 MB L2, so no L2 flush is needed between steps).
+`value` is reads/s of the batched path (autotuned, launches captured in one
+CUDA graph) over the timed steps (device time, CUDA events); `plain` is the
+one-warp-per-read, one-launch-per-batch kernel on the same data; `e2e` is the
+same metric through the C ABI with pinned host buffers (host->device copies of
+the reads and device->host copies of the per-read results inside the timed
+region).  `--impl reference` times the reference's own classifier
+(BioBloomClassifier::filter compiled from the reference sources,
+oracle/_ref/ref_harness) on the box's host cores, on inputs made by the CPU
+oracle's copy of the generator and filter build (no product library loaded).
+
+With --workload bf: 10 Bloom filters (k=25, FPR 0.075, h=3), each built from
+an independent seeded 100 Mbp reference (41% GC, 5% of each reference in
+300 bp repeat copies); 10M read pairs 2x150 bp, 10% drawn from each reference
+with 0.5% substitutions and 0.01% N.  3 GB of bases and 685 MB of filters.
 
 With --workload mibf: the multi-index workload -- a miBF over 500 targets,
 each a seeded 2 Mbp reference at 35-65% GC (uniform per target) with 20% of
@@ -23,13 +33,6 @@ weight 19 drawn from the seed; 20M single-end 150 bp reads, 90% from the
 targets with 1% substitutions, 10% uniform random.  A step classifies all
 reads once (reads and the 5 GB filter resident in HBM, far above L2).
 
-With --workload varlen: one filter (k=25, FPR 0.075, 2.12 GB) from a seeded
-3.1 Gbp reference (41% GC, 45% of bases in repeat families of 300 bp - 6 kb at
-10-20% divergence); 50M single-end reads, 95% log-uniform over 50-300 bp and
-5% log-uniform over 300 bp - 10 kb, 70% from the reference with 1%
-substitutions, 30% random.  The batched path (autotuned persistent kernel,
-long reads first, launches captured in one CUDA graph) is timed against the
-plain path (one warp per read, one launch per batch of 256k reads).
 With --workload small: one filter from a seeded 5 Mbp uniform reference,
 1M single-end 150 bp reads, 50% from the reference with 1% substitutions
 (the filter, 3.4 MB, is L2-resident).
@@ -42,7 +45,7 @@ substitutions, arrive as a seeded Poisson process at a fixed offered load
 once, the offline batched run); reports p50/p99 request latency and reads/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                  [--workload bf|mibf|varlen|small|serve]
+                  [--workload varlen|bf|mibf|small|serve|modes]
 """
 import argparse
 import json
@@ -240,25 +243,89 @@ def dist_setup(args):
     return world, rank, local, pg
 
 
+def native_libs():
+    """Shared libraries of this repository mapped into this process."""
+    out = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 6 and parts[-1].startswith(ROOT + os.sep) and ".so" in parts[-1]:
+                    out.add(os.path.relpath(parts[-1], ROOT))
+    except OSError:
+        pass
+    return sorted(out)
+
+
+def ref_rank_zero():
+    """The reference arm runs on rank 0 only; the other ranks exit without work."""
+    return int(os.environ.get("RANK", "0")) == 0
+
+
+def ref_store_filter(f, path, fid, source):
+    """Write an oracle-built filter as <stem>.bf + <stem>.txt."""
+    from tests import oracle_lib as ol
+    f.store(path)
+    n = f.bf.n_entry
+    approx = (1.0 - np.exp(-float(f.h) * n / float(f.m))) ** f.h
+    ol.write_info(path[:-2] + "txt", fid, f.k, FPR, f.h, f.expected_entries, source, f.m, n,
+                  approx, f.redundant, approx)
+
+
+def ref_step_budget(args):
+    """Seconds of CPU classification per reference step: the whole run stays
+    within about three minutes."""
+    return max(3.0, min(10.0, 150.0 / max(1, args.warmup + args.steps)))
+
+
+def ref_line(args, metric, value, sec, workload, sample, threads, extra=None):
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": "reads/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": workload},
+            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "inputs": "made by the CPU oracle's generator and threaded filter build "
+                      "(oracle/synth_oracle.c), the same bytes as the GPU arm's",
+            "native_so_loaded": native_libs()}
+    line.update(extra or {})
+    return line
+
+
 def run_reference(args):
-    world, rank, local, pg = dist_setup(args)
-    if rank != 0:
-        if pg:
-            pg.barrier()
-            pg.destroy_process_group()
+    """The 10-filter workload's CPU arm: the reference's own
+    BioBloomClassifier::filterPair on a bounded sample of the same pairs."""
+    if not ref_rank_zero():
         return
-    d = workdir()
-    paths, genomes = build_filters(d, local)
-    n_sample = 200_000
-    s1, s2, off = make_reads(genomes, n_sample, 7000)
+    from tests import oracle_lib as ol
+    d = os.path.join(tempfile.gettempdir(), "bbt_ref_c2")
+    os.makedirs(d, exist_ok=True)
+    t0 = time.time()
+    paths, genomes = [], []
+    for j in range(N_FILTERS):
+        g = ol.synth_genome(1002 * 1000 + j, REF_LEN, gc=0.41, repeat_frac=0.05, rep_min=300,
+                            rep_max=300)
+        genomes.append(g)
+        p = os.path.join(d, f"ref{j}.bf")
+        if not (os.path.exists(p) and os.path.exists(p[:-2] + "txt")):
+            ref_store_filter(ol.make_filter_par([g], k=K, fpr=FPR), p, f"ref{j}", f"ref{j}.fa")
+        paths.append(p)
+    log(f"reference arm: references + filters {time.time() - t0:.1f} s")
+    n_sample = 400_000
+    rp = ol.read_params(READ_LEN, READ_LEN, sub_rate=SUB, n_rate=NRATE, frag_min=300,
+                        frag_max=500)
+    s1, off, s2, _ = ol.synth_reads(5000, genomes, [1.0 / N_FILTERS] * N_FILTERS, n_sample, rp,
+                                    paired=True)
     threads = os.cpu_count() or 1
-    # calibrate the per-step sample to ~10 s of CPU work
     r, err = cpu_reference_run(d, paths, s1, s2, off, 2000, threads)
     if r is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
         return
     rate = 2000 / max(r["seconds"], 1e-6)
-    n = int(min(n_sample, max(2000, rate * 10.0)))
+    n = int(min(n_sample, max(2000, rate * ref_step_budget(args))))
     n = (n // 1000) * 1000
     times = []
     for i in range(args.warmup + args.steps):
@@ -270,21 +337,12 @@ def run_reference(args):
             times.append(r["seconds"])
     sec = sum(times) / len(times)
     value = 2 * n / sec
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "reads/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "pairs_per_step": n, "filters": N_FILTERS},
-            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads,
-                             "kind": "reference",
-                             "sample": f"{n} pairs per step, BioBloomClassifier::filterPair "
-                                       "compiled from the reference sources"},
-            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    print(json.dumps(ref_line(args, METRIC, value, sec, WORKLOAD,
+                              f"first {n} pairs of the workload per step, "
+                              "BioBloomClassifier::filterPair compiled from the reference "
+                              f"sources, {threads} OpenMP threads, filter load excluded",
+                              threads, {"config": {"workload": WORKLOAD, "pairs_per_step": n,
+                                                   "filters": N_FILTERS}})), flush=True)
 
 
 def traffic_per_read():
@@ -388,10 +446,8 @@ def run_gpu(args):
     del keep1, keep2
     bbc.set_launch(path=best)
 
-    # correctness of the timed configuration: a sample of pairs against the oracle
-    parity = None
-    if rank == 0 and not args.no_check:
-        parity = check_sample(paths, s1, s2, off, hits1, hits2, 2000)
+    g1_np = hits1.cpu().numpy().view(np.uint64)
+    g2_np = hits2.cpu().numpy().view(np.uint64)
 
     # e2e through the C ABI with pinned host buffers
     hb1 = np.empty((n_pairs, words), dtype=np.uint64)
@@ -435,8 +491,11 @@ def run_gpu(args):
 
     cpu = None
     cpu_err = None
+    parity = None
     if world == 1 and not args.no_cpu:
         cpu, cpu_err = cpu_baseline(d, paths, s1, s2, off)
+    if world == 1 and not args.no_check:
+        parity = pair_parity(d, paths, s1, s2, off, g1_np, g2_np, min(n_pairs, PARITY_READS))
 
     peak, peak_kind = measured_peaks()
     read_bytes = bases * 2 / 4.0  # 2-bit packed read bytes (both mates)
@@ -499,20 +558,29 @@ def run_gpu(args):
         pg.destroy_process_group()
 
 
-def check_sample(paths, s1, s2, off, hits1, hits2, n):
-    """Compare the first n pairs' hits with the CPU oracle."""
+def pair_parity(d, paths, s1, s2, off, g1, g2, m):
+    """The first m pairs' hits of the timed path against the reference's own
+    classifier code on the same pairs (outside the timed region)."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return {"checked_pairs": 0, "error": "oracle/_ref/ref_harness is not built"}
+    f1 = os.path.join(d, f"sample_{m}_1.fq")
+    f2 = os.path.join(d, f"sample_{m}_2.fq")
+    if not os.path.exists(f2):
+        write_fastq(f1, s1, off, 0, m)
+        write_fastq(f2, s2, off, 0, m)
+    t0 = time.time()
     try:
-        from tests import oracle_lib as ol
-    except Exception as e:  # the oracle is test infrastructure; report, do not fail
-        return {"checked": 0, "error": str(e)}
-    filters = [ol.Filter.load(p) for p in paths]
-    o = off[:n + 1]
-    w1, _ = ol.classify(s1[:o[-1]].tobytes(), o, filters, SCORE, STREAK)
-    w2, _ = ol.classify(s2[:o[-1]].tobytes(), o, filters, SCORE, STREAK)
-    g1 = hits1[:n].cpu().numpy().view(np.uint64)
-    g2 = hits2[:n].cpu().numpy().view(np.uint64)
-    return {"checked_pairs": n, "mismatched_reads": int((g1 != w1).any(1).sum() +
-                                                        (g2 != w2).any(1).sum())}
+        rows = harness_hits(harness, paths, f1, f2)
+    except RuntimeError as e:
+        return {"checked_pairs": 0, "error": str(e)}
+    w1 = np.array([r[0] for r in rows], dtype=np.uint64)
+    w2 = np.array([r[1] for r in rows], dtype=np.uint64)
+    n = len(rows)
+    bad = int((w1 != g1[:n, 0]).sum() + (w2 != g2[:n, 0]).sum())
+    return {"checked_pairs": n, "mismatched_reads": bad,
+            "against": "SeqEval::evalRead of the reference sources (ref_harness hits)",
+            "kind": "sample: the first pairs of the step", "seconds": time.time() - t0}
 
 
 # ------------------------------------------------- filtering modes / scoring methods
@@ -725,10 +793,7 @@ def single_cpu(d, path, s1, off, budget_s=15.0):
     def run(n):
         fq = os.path.join(d, f"sample_{n}.fq")
         if not os.path.exists(fq):
-            with open(fq, "wb") as f:
-                f.write(b"".join(b"@r%d\n%s\n+\n%s\n" % (i, s1[off[i]:off[i + 1]].tobytes(),
-                                                        b"I" * int(off[i + 1] - off[i]))
-                                 for i in range(n)))
+            write_single_fastq(fq, s1, off, n)
         pr = subprocess.run([harness, "time", str(SCORE), str(STREAK), str(threads), "0",
                              os.path.join(d, "refcpu"), path, fq], capture_output=True, text=True)
         if pr.returncode:
@@ -749,6 +814,53 @@ def single_cpu(d, path, s1, off, budget_s=15.0):
             "sample": f"first {r['records']} reads of the workload, BioBloomClassifier::filter "
                       f"from the reference sources, {r['threads']} OpenMP threads, filter load "
                       f"excluded", "seconds": r["seconds"]}, None
+
+
+PARITY_READS = 200_000
+
+
+def harness_hits(harness, paths, fq1, fq2=None):
+    """Per-read hit lists from the reference's own SeqEval::evalRead
+    (ref_harness hits), in file order: one list (or pair of lists) per read."""
+    cmd = [harness, "hits", str(SCORE), str(STREAK), ",".join(paths), fq1] + ([fq2] if fq2 else [])
+    pr = subprocess.run(cmd, capture_output=True, text=True)
+    if pr.returncode:
+        raise RuntimeError("ref_harness hits failed: " + pr.stderr[-300:])
+    rows = []
+    for line in pr.stdout.splitlines():
+        if line.startswith("#SUMMARY"):
+            break
+        ids = line.split("\t", 1)[1]
+
+        def bits(x):
+            w = 0
+            for t in x.split(","):
+                if t:
+                    w |= 1 << int(t)
+            return w
+        rows.append(tuple(bits(x) for x in ids.split("|")))
+    return rows
+
+
+def harness_parity(d, path, s1, off, gpu_hits, m):
+    """The first m reads' hits of the timed path against the reference's own
+    classifier code on the same reads (outside the timed region)."""
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return {"checked_reads": 0, "error": "oracle/_ref/ref_harness is not built"}
+    fq = os.path.join(d, f"sample_{m}.fq")
+    if not os.path.exists(fq):
+        write_single_fastq(fq, s1, off, m)
+    t0 = time.time()
+    try:
+        rows = harness_hits(harness, [path], fq)
+    except RuntimeError as e:
+        return {"checked_reads": 0, "error": str(e)}
+    want = np.array([r[0] for r in rows], dtype=np.uint64)
+    got = gpu_hits[:len(want), 0]
+    return {"checked_reads": len(want), "mismatched_reads": int((want != got).sum()),
+            "against": "SeqEval::evalRead of the reference sources (ref_harness hits)",
+            "kind": "sample: the first reads of the step", "seconds": time.time() - t0}
 
 
 def run_single(args):
@@ -843,18 +955,7 @@ def run_single(args):
     stream.synchronize()
     k_ms = bbc.last_stats()["classify_ms"]
 
-    parity = None
-    if rank == 0 and not args.no_check:
-        try:
-            from tests import oracle_lib as ol
-            f = ol.Filter.load(path)
-            m = 2000
-            o = off[:m + 1]
-            w, _ = ol.classify(s1[:o[-1]].tobytes(), o, [f], SCORE, STREAK)
-            g = hits[:m].cpu().numpy().view(np.uint64)
-            parity = {"checked_reads": m, "mismatched_reads": int((g != w).any(1).sum())}
-        except Exception as e:  # the oracle is test infrastructure: report, do not fail
-            parity = {"checked_reads": 0, "error": str(e)}
+    gpu_np = hits.cpu().numpy().view(np.uint64)
 
     # e2e: the C ABI with pinned host buffers (staged, pipelined copies)
     hh = torch.empty((n, 1), dtype=torch.int64).pin_memory()
@@ -887,8 +988,11 @@ def run_single(args):
             pg.destroy_process_group()
         return
     cpu, cpu_err = (None, "skipped (--no-cpu)")
+    parity = None
     if world == 1 and not args.no_cpu:
         cpu, cpu_err = single_cpu(d, path, s1, off)
+    if world == 1 and not args.no_check:
+        parity = harness_parity(d, path, s1, off, gpu_np, min(n, PARITY_READS))
     peak, peak_kind = measured_peaks()
     alg_bytes = 32.0 * alg_probes + bases / 4.0 + n * (8 + 4)
     achieved = alg_bytes / (k_ms * 1e-3) / 1e9
@@ -924,6 +1028,7 @@ def run_single(args):
         "graph_launches_per_step": 1,
         "clocks": clk,
         "parity_sample": parity,
+        "batched_equals_reference_sample": (parity or {}).get("mismatched_reads") == 0,
     }
     print(json.dumps(line), flush=True)
     graph.close()
@@ -933,37 +1038,85 @@ def run_single(args):
         pg.destroy_process_group()
 
 
+def ref_single_setup(cfg, n_reads):
+    """The single-filter workload built by the CPU oracle (generator restated
+    in oracle/synth_oracle.c, threaded filter build): the same reference, bit
+    array and first n_reads reads as single_setup, without the product
+    library."""
+    from tests import oracle_lib as ol
+    d = os.path.join(tempfile.gettempdir(), f"bbt_ref_{cfg['seed']}")
+    os.makedirs(d, exist_ok=True)
+    t0 = time.time()
+    g = ol.synth_genome(cfg["seed"], cfg["glen"], gc=cfg["gc"], repeat_frac=cfg["repeat_frac"],
+                        rep_min=cfg["rep_min"], rep_max=cfg["rep_max"], div_min=cfg["div_min"],
+                        div_max=cfg["div_max"])
+    path = os.path.join(d, "genome.bf")
+    if not (os.path.exists(path) and os.path.exists(path[:-2] + "txt")):
+        ref_store_filter(ol.make_filter_par([g], k=K, fpr=FPR), path, "genome", "genome.fa")
+    log(f"reference arm: reference + filter {time.time() - t0:.1f} s")
+    p = ol.read_params(cfg["len_min"], cfg["len_max"], long_frac=cfg["long_frac"],
+                       long_min=cfg["long_min"], long_max=cfg["long_max"], sub_rate=cfg["sub"])
+    s1, off, _, _ = ol.synth_reads(cfg["seed"] + 17, [g], [cfg["ref_frac"]], n_reads, p)
+    del g
+    return d, path, s1, off
+
+
 def run_single_reference(args):
-    world, rank, local, pg = dist_setup(args)
-    if rank != 0:
-        if pg:
-            pg.barrier()
-            pg.destroy_process_group()
+    """CPU arm of a single-filter workload: the reference's own
+    BioBloomClassifier::filter on a bounded sample of the workload's reads,
+    each step one run on the same sample, all host threads."""
+    if not ref_rank_zero():
         return
     cfg = SINGLE[args.workload]
-    d, path, s1, off = single_setup(cfg, local, min(cfg["reads"], 2_000_000))
-    times, n = [], None
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/ref_harness is not built"}))
+        return
+    d, path, s1, off = ref_single_setup(cfg, min(cfg["reads"], 4_000_000))
+    threads = os.cpu_count() or 1
+
+    def run(n):
+        fq = os.path.join(d, f"sample_{n}.fq")
+        if not os.path.exists(fq):
+            write_single_fastq(fq, s1, off, n)
+        pr = subprocess.run([harness, "time", str(SCORE), str(STREAK), str(threads), "0",
+                             os.path.join(d, "refcpu"), path, fq], capture_output=True, text=True)
+        if pr.returncode:
+            return None, "ref_harness failed: " + pr.stderr[-300:]
+        return json.loads([x for x in pr.stdout.splitlines() if x.startswith("{")][-1]), None
+
+    probe = 20000
+    r, err = run(probe)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    n = int(min(len(off) - 1, max(probe, probe / max(r["seconds"], 1e-6) * ref_step_budget(args))))
+    n = max(probe, (n // 10000) * 10000)
+    times = []
     for i in range(args.warmup + args.steps):
-        r, err = single_cpu(d, path, s1, off, budget_s=8.0)
+        r, err = run(n)
         if r is None:
             print(json.dumps({"impl": "reference", "unavailable": err}))
             return
         if i >= args.warmup:
-            times.append(r["value"])
-            n = r["sample"]
-    value = sum(times) / len(times)
-    line = {"impl": "reference", "metric": SINGLE_METRIC, "value": value, "unit": "reads/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
-            "data": "synthetic", "config": {"workload": cfg["workload"]},
-            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": os.cpu_count() or 1,
-                             "kind": "reference", "sample": n},
-            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+            times.append(r["seconds"])
+    sec = sum(times) / len(times)
+    value = n / sec
+    print(json.dumps(ref_line(
+        args, SINGLE_METRIC, value, sec, cfg["workload"],
+        f"first {n} reads of the workload per step ({int(off[n])} bases), "
+        f"BioBloomClassifier::filter compiled from the reference sources, {threads} OpenMP "
+        "threads, filter load excluded", threads,
+        {"config": {"workload": cfg["workload"], "reads_per_step": n,
+                    "bases_per_step": int(off[n])}})), flush=True)
+
+
+def write_single_fastq(path, s1, off, n):
+    with open(path, "wb") as f:
+        f.write(b"".join(b"@r%d\n%s\n+\n%s\n" % (i, s1[off[i]:off[i + 1]].tobytes(),
+                                                b"I" * int(off[i + 1] - off[i]))
+                         for i in range(n)))
 
 
 # ---------------------------------------------------------------- serving workload
@@ -1446,8 +1599,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity (bytes)")
-    ap.add_argument("--workload", default="bf",
-                    choices=["bf", "mibf", "varlen", "small", "serve", "modes"])
+    ap.add_argument("--workload", default="varlen",
+                    choices=["varlen", "bf", "mibf", "small", "serve", "modes"])
     ap.add_argument("--requests", type=int, default=200, help="requests (--workload serve)")
     ap.add_argument("--load", type=float, default=0.7,
                     help="offered load, fraction of offline capacity (--workload serve)")

@@ -329,6 +329,10 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 		ctx->p = *params;
 	else
 		bbt_default_params(&ctx->p);
+	if (!(ctx->p.score < 4294967296.0) && ctx->p.scoring != BBT_SCORE_BINOMIAL) {
+		bbt_close(ctx);
+		return fail(nullptr, BBT_ERR_ARG, "score must be below 2^32");
+	}
 	if (ctx->p.score > 1 && (ctx->p.scoring == BBT_SCORE_SIMPLE ||
 			ctx->p.scoring == BBT_SCORE_HARMONIC) && (unsigned)ctx->p.score > 1) {
 		/* BioBloomCategorizer.cpp:423-430: an integer score > 1 is a

@@ -49,6 +49,8 @@ static void usage_exit()
 	        "                         Ignored if k-mers used when indexing.\n"
 	        "  -m, --multi=N          Multi Match threshold. [1.0]\n"
 	        "  -r, --streak=N         Number of additional hits needed to skip classification. [3]\n"
+	        "                         Checked against -c but has no effect on the results here:\n"
+	        "                         every frame of a read is evaluated.\n"
 	        "  -c, --minNoSat=N       Minimum count of non saturated matches. Increasing this value\n"
 	        "                         will filter out repetitive or low quality sequences.[0]\n"
 	        "  -b, --bestHitAgree     Filters out all matches where best hit is ambiguous because\n"
@@ -123,7 +125,14 @@ int main(int argc, char **argv)
 		case 'a': parse_or_die(optarg, p.frame_matches, 'a'); break;
 		case 'b': p.best_hit_agree = 1; break;
 		case 'v': ++verbose; break;
-		case 'r': parse_or_die(optarg, p.streak, 'r'); break;
+		case 'r':
+			parse_or_die(optarg, p.streak, 'r');
+			/* The reference hands -r to MIBFQuerySupport
+			 * (MIBFClassifier.hpp:222-225), whose early-exit rule lives
+			 * in the btl_bloomfilter submodule, absent from the
+			 * reference tree; this build evaluates every frame. */
+			cerr << "Warning: -r has no effect: every frame of a read is evaluated" << endl;
+			break;
 		case 'c': parse_or_die(optarg, p.min_nonsat, 'c'); break;
 		case 'm': parse_or_die(optarg, p.multi_thresh, 'm'); break;
 		case 'd': refused += " -d"; break;

@@ -18,16 +18,17 @@
  * such calls one after another.
  *
  * In host code the array's name is only a host-side stand-in, not a device
- * address.  The device address is obtained once per GPU, with that GPU
- * current, by cudaGetSymbolAddress in noalloc_scratch() below; the first call
- * of bbt_classify_noalloc on a GPU does this set-up, so that first call should
+ * address.  Each call obtains the device address with cudaGetSymbolAddress,
+ * with the call's GPU current, in noalloc_scratch() below.  The address is not
+ * cached: after a cudaDeviceReset in the caller's process the GPU has a new
+ * context, in which the array may sit at another address.  The first call on a
+ * GPU also loads the library's device code there, so that first call should
  * come before any stream capture.
  */
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include <string>
 
 #include "bbt.h"
@@ -47,25 +48,15 @@ static_assert(sizeof(NoAllocLayout) <= kScratchBytes, "no-alloc scratch too smal
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-void *g_scratch_ptr[kMaxDevices] = {nullptr};
-
-/* Device address of the scratch array on `dev` (which is current). */
-int noalloc_scratch(int dev, NoAllocLayout **out)
+/* Device address of the scratch array on the current device. */
+int noalloc_scratch(NoAllocLayout **out)
 {
-	if (dev < 0 || dev >= kMaxDevices)
-		return fail(nullptr, BBT_ERR_ARG, "bbt_classify_noalloc: device ordinal out of range");
-	std::lock_guard<std::mutex> lk(g_mu);
-	if (!g_scratch_ptr[dev]) {
-		void *p = nullptr;
-		cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-		if (e != cudaSuccess || !p)
-			return cuda_fail(nullptr, e == cudaSuccess ? cudaErrorInvalidSymbol : e,
-					"cudaGetSymbolAddress(no-alloc scratch)");
-		g_scratch_ptr[dev] = p;
-	}
-	*out = reinterpret_cast<NoAllocLayout *>(g_scratch_ptr[dev]);
+	void *p = nullptr;
+	cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+	if (e != cudaSuccess || !p)
+		return cuda_fail(nullptr, e == cudaSuccess ? cudaErrorInvalidSymbol : e,
+				"cudaGetSymbolAddress(no-alloc scratch)");
+	*out = reinterpret_cast<NoAllocLayout *>(p);
 	return BBT_OK;
 }
 
@@ -92,8 +83,12 @@ extern "C" int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filter
 		return fail(nullptr, BBT_ERR_ARG, "bbt_classify_noalloc: missing reads, offsets or hits");
 	double score = params->score;
 	int scoring = params->scoring;
-	if (scoring == BBT_SCORE_SIMPLE && score > 1 && (unsigned)score > 1) {
-		score = (double)(unsigned)score; /* integer > 1: minimum match length */
+	if (!(score < 4294967296.0))
+		return fail(nullptr, BBT_ERR_ARG, "bbt_classify_noalloc: score must be below 2^32");
+	if ((scoring == BBT_SCORE_SIMPLE || scoring == BBT_SCORE_HARMONIC) && score > 1 &&
+			(unsigned)score > 1) {
+		/* as bbt_open: an integer score > 1 is a minimum match length */
+		score = (double)(unsigned)score;
 		scoring = BBT_SCORE_LENGTH;
 	}
 	if (scoring == BBT_SCORE_SIMPLE && (score < 0 || score > 1))
@@ -112,6 +107,8 @@ extern "C" int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filter
 		table[i] = make_filter_dev(v.words, v.m, v.h, v.k);
 		kmax = v.k > kmax ? v.k : kmax;
 	}
+	if (params->device < 0)
+		return fail(nullptr, BBT_ERR_ARG, "bbt_classify_noalloc: negative device ordinal");
 	if (batch->n_reads == 0)
 		return BBT_OK;
 	int prev = 0;
@@ -125,7 +122,7 @@ extern "C" int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filter
 	NoAllocLayout *scratch = nullptr;
 	cudaStream_t s = (cudaStream_t)stream;
 	int sms = 0;
-	if ((rc = noalloc_scratch(dev, &scratch)) != BBT_OK)
+	if ((rc = noalloc_scratch(&scratch)) != BBT_OK)
 		goto out;
 	if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) {
 		rc = cuda_fail(nullptr, e, "cudaDeviceGetAttribute");

@@ -128,28 +128,38 @@ static int mode_hits(int argc, char **argv)
 	}
 	kseq_t *k1 = kseq_init(fp1);
 	kseq_t *k2 = paired ? kseq_init(fp2) : NULL;
-	size_t total = 0;
+	/* records first, then SeqEval::evalRead over them on all threads (each
+	 * call reads only its filter and its sequence), output in file order */
+	vector<string> names, seqs1, seqs2;
 	for (;;) {
 		int l1 = kseq_read(k1);
 		int l2 = paired ? kseq_read(k2) : 0;
 		if (l1 < 0 || l2 < 0)
 			break;
-		string s1(k1->seq.s, l1);
-		vector<unsigned> h1, h2;
-		for (unsigned f = 0; f < filters.size(); ++f)
-			if (SeqEval::evalRead(s1, *filters[f], opt::score))
-				h1.push_back(f);
-		++total;
+		names.push_back(k1->name.s);
+		seqs1.push_back(string(k1->seq.s, l1));
+		if (paired)
+			seqs2.push_back(string(k2->seq.s, l2));
+	}
+	const size_t total = names.size();
+	vector<vector<unsigned> > hits1(total), hits2(paired ? total : 0);
+#pragma omp parallel for schedule(dynamic, 256)
+	for (long i = 0; i < (long)total; ++i) {
+		for (unsigned f = 0; f < filters.size(); ++f) {
+			if (SeqEval::evalRead(seqs1[i], *filters[f], opt::score))
+				hits1[i].push_back(f);
+			if (paired && SeqEval::evalRead(seqs2[i], *filters[f], opt::score))
+				hits2[i].push_back(f);
+		}
+	}
+	for (size_t i = 0; i < total; ++i) {
 		if (paired) {
-			string s2(k2->seq.s, l2);
-			for (unsigned f = 0; f < filters.size(); ++f)
-				if (SeqEval::evalRead(s2, *filters[f], opt::score))
-					h2.push_back(f);
-			res.updateSummaryData(h1, h2);
-			printf("%s\t%s|%s\n", k1->name.s, join(h1).c_str(), join(h2).c_str());
+			res.updateSummaryData(hits1[i], hits2[i]);
+			printf("%s\t%s|%s\n", names[i].c_str(), join(hits1[i]).c_str(),
+					join(hits2[i]).c_str());
 		} else {
-			res.updateSummaryData(h1);
-			printf("%s\t%s\n", k1->name.s, join(h1).c_str());
+			res.updateSummaryData(hits1[i]);
+			printf("%s\t%s\n", names[i].c_str(), join(hits1[i]).c_str());
 		}
 	}
 	printf("#SUMMARY\n%s", res.getResultsSummary(total).c_str());

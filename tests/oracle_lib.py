@@ -430,3 +430,96 @@ class MIBF:
 
 def binom_upper_quantile(n, p, q):
     return _mibf_lib().oracle_binom_upper_quantile(n, p, q)
+
+
+# ------------------------------------------------- workload generator (CPU arm)
+
+class ReadParams(ctypes.Structure):
+    """oracle_read_params: the field layout of the product's bbt_synth_read_params."""
+    _fields_ = [("len_min", ctypes.c_uint32), ("len_max", ctypes.c_uint32),
+                ("long_frac", ctypes.c_double), ("long_min", ctypes.c_uint32),
+                ("long_max", ctypes.c_uint32), ("sub_rate", ctypes.c_double),
+                ("n_rate", ctypes.c_double), ("frag_min", ctypes.c_uint32),
+                ("frag_max", ctypes.c_uint32)]
+
+
+_synth_sig_done = False
+
+
+def _synth_lib():
+    global _synth_sig_done
+    L = lib()
+    if not _synth_sig_done:
+        P = ctypes.POINTER
+        u64, u32, dbl, vp = ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double, ctypes.c_void_p
+        L.oracle_synth_genome.argtypes = [u64, u64, dbl, dbl, u32, u32, dbl, dbl, vp]
+        L.oracle_synth_read_lengths.argtypes = [u64, P(ReadParams), u64, vp]
+        L.oracle_synth_reads.argtypes = [u64, vp, vp, u32, vp, P(ReadParams), u64, vp, vp, vp,
+                                         vp]
+        L.oracle_make_filter_par.argtypes = [P(_BF), P(ctypes.c_char_p), P(u64), ctypes.c_size_t,
+                                             u32, dbl, u32, P(u64), P(u64)]
+        _synth_sig_done = True
+    return L
+
+
+def _vp(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def synth_genome(seed, length, gc=0.5, repeat_frac=0.0, rep_min=0, rep_max=0, div_min=0.0,
+                 div_max=0.0):
+    out = np.empty(int(length), dtype=np.uint8)
+    if _synth_lib().oracle_synth_genome(seed, int(length), gc, repeat_frac, rep_min, rep_max,
+                                        div_min, div_max, _vp(out)):
+        raise ValueError("oracle_synth_genome: bad arguments")
+    return out
+
+
+def read_params(len_min=150, len_max=None, long_frac=0.0, long_min=0, long_max=0, sub_rate=0.0,
+                n_rate=0.0, frag_min=0, frag_max=0):
+    return ReadParams(len_min, len_max if len_max is not None else len_min, long_frac, long_min,
+                      long_max, sub_rate, n_rate, frag_min, frag_max)
+
+
+def synth_reads(seed, refs, ref_frac, n_reads, params, paired=False):
+    """(seq1, off, seq2 or None, src), as the product's synth.reads."""
+    L = _synth_lib()
+    off = np.empty(n_reads + 1, dtype=np.uint64)
+    if L.oracle_synth_read_lengths(seed, ctypes.byref(params), n_reads, _vp(off)):
+        raise ValueError("oracle_synth_read_lengths: bad arguments")
+    total = int(off[-1])
+    s1 = np.empty(max(total, 1), dtype=np.uint8)
+    s2 = np.empty(max(total, 1), dtype=np.uint8) if paired else None
+    src = np.empty(n_reads, dtype=np.uint32)
+    if refs:
+        cat = np.concatenate(refs) if len(refs) > 1 else np.ascontiguousarray(refs[0])
+        roff = np.zeros(len(refs) + 1, dtype=np.uint64)
+        roff[1:] = np.cumsum([len(r) for r in refs])
+    else:
+        cat = np.zeros(1, dtype=np.uint8)
+        roff = np.zeros(1, dtype=np.uint64)
+    frac = np.asarray(ref_frac, dtype=np.float64)
+    if L.oracle_synth_reads(seed, _vp(cat), _vp(roff), len(refs), _vp(frac),
+                            ctypes.byref(params), n_reads, _vp(off), _vp(s1), _vp(s2),
+                            _vp(src)):
+        raise ValueError("oracle_synth_reads: a reference is shorter than a fragment")
+    return s1, off, s2, src
+
+
+def make_filter_par(seqs, k=25, fpr=0.075, h=0):
+    """Filter from uint8 arrays, built by the oracle's OpenMP threads (same bit
+    array as Filter.make)."""
+    L = _synth_lib()
+    f = Filter()
+    ptrs = (ctypes.c_char_p * len(seqs))(*[ctypes.cast(s.ctypes.data, ctypes.c_char_p)
+                                           for s in seqs])
+    lens = np.array([len(s) for s in seqs], dtype=np.uint64)
+    exp = ctypes.c_uint64()
+    red = ctypes.c_uint64()
+    if L.oracle_make_filter_par(ctypes.byref(f.bf), ptrs, _u64p(lens), len(seqs), k, fpr, h,
+                                ctypes.byref(exp), ctypes.byref(red)):
+        raise MemoryError
+    f._owned = True
+    f.expected_entries = exp.value
+    f.redundant = red.value
+    return f

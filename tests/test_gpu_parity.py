@@ -332,3 +332,42 @@ def test_host_batch_in_slot_loads_matches_device_batch(tmp_path, paired):
     assert np.array_equal(c, dc.cpu().numpy().view(np.uint32))
     assert na == nd == n and np.array_equal(ca, cd)
     assert h.any()
+
+
+def test_filter_above_2_pow_32_bits(tmp_path):
+    """A filter of m > 2^32 bits (600 MB; 89% of bit positions lie above 2^32):
+    the hash reduction and the word index use 64-bit arithmetic on every path,
+    including the filter-major two-pass path."""
+    import torch
+    rng = np.random.default_rng(4242)
+    m = 4_800_000_064
+    genome = bytes(rng.choice(np.frombuffer(b"ACGT", dtype=np.uint8), 30000))
+    f = ol.Filter.create(m, 3, 25)
+    f.insert_sequence(genome)
+    bits = f.bits()
+    high = np.flatnonzero(bits[(1 << 32) // 8:]).size
+    assert high > 0, "no set bit above 2^32"
+    stem = str(tmp_path / "big")
+    f.store(stem + ".bf")
+    ol.write_info(stem + ".txt", "big", 25, 0.075, 3, 30000, "x", m, 30000, 0.0, 0, 0.0)
+    reads = []
+    for i in range(2000):
+        L = int(rng.integers(60, 400))
+        if i % 2:
+            s = int(rng.integers(0, len(genome) - L))
+            r = bytearray(genome[s:s + L])
+            for j in np.flatnonzero(rng.random(L) < 0.02):
+                r[j] = ord("ACGT"[int(rng.integers(0, 4))])
+            reads.append(bytes(r))
+        else:
+            reads.append(bytes(rng.choice(np.frombuffer(b"ACGT", dtype=np.uint8), L)))
+    seq, off = ol.pack_reads(reads)
+    want, _ = ol.classify(seq, off, [f], 0.15, 3)
+    assert 0 < int((want[:, 0] != 0).sum()) < len(reads)
+    dseq = torch.tensor(np.frombuffer(seq, dtype=np.uint8), device="cuda")
+    doff = torch.tensor(off.astype(np.int64), device="cuda")
+    for launch in (PATHS[0], PATHS[1], PATHS[4]):
+        with _classifier([stem + ".bf"], **launch) as bbc:
+            hits, _, _ = bbc.classify_device(dseq, doff)
+            torch.cuda.synchronize()
+            assert np.array_equal(hits.cpu().numpy().view(np.uint64), want), launch

@@ -46,7 +46,7 @@ def _to_device(torch, reads):
             torch.tensor(off.astype(np.int64), device="cuda"))
 
 
-def _noalloc(L, torch, views, nf, seq, off, seq2=None, off2=None, score=0.15):
+def _noalloc(L, torch, views, nf, seq, off, seq2=None, off2=None, score=0.15, scoring=0):
     n = off.numel() - 1
     words = (nf + 63) // 64
     hits = torch.full((n, words), -1, dtype=torch.int64, device="cuda")
@@ -55,6 +55,7 @@ def _noalloc(L, torch, views, nf, seq, off, seq2=None, off2=None, score=0.15):
     p = L.Params()
     L.lib().bbt_default_params(ctypes.byref(p))
     p.score = score
+    p.scoring = scoring
     b = L.Batch()
     b.seq, b.offsets, b.n_reads, b.location = seq.data_ptr(), off.data_ptr(), n, L.DEVICE
     if seq2 is not None:
@@ -102,3 +103,21 @@ def test_noalloc_rejects_too_many_filters(setup):
     assert rc == -1
     assert b"at most" in L.lib().bbt_last_error(None) or b"between 1 and 64" in \
         L.lib().bbt_last_error(None)
+
+
+def test_noalloc_integer_harmonic_score_is_a_match_length(setup):
+    """As the ordinary entry point does (BioBloomCategorizer.cpp:423-430 reads
+    an integer score > 1 as a minimum match length, whatever -S says), a
+    harmonic score of 40 classifies by LENGTH; scores of 2^32 and more are
+    refused before any conversion."""
+    L, torch, filters, dev_words, views, r1, r2 = setup
+    from biobloom_b200 import BioBloomClassifier
+    s1, o1 = _to_device(torch, r1)
+    with BioBloomClassifier(filter_paths(), 40, score_type="harmonic") as bbc:
+        want, _, _ = bbc.classify_device(s1, o1)
+        torch.cuda.synchronize()
+    for _ in range(2):
+        got, _ = _noalloc(L, torch, views, len(filters), s1, o1, score=40, scoring=2)
+        assert torch.equal(got, want)
+    with pytest.raises(Exception):
+        _noalloc(L, torch, views, len(filters), s1, o1, score=2.0 ** 32, scoring=2)
