@@ -1589,6 +1589,30 @@ def run_mibf_reference(args):
         pg.destroy_process_group()
 
 
+# ---------------------------------------------------------------- gather ceilings
+
+def run_gather(args):
+    """Random 4-byte gather rates of this GPU (bbt_measure_gather): positions
+    streamed from HBM into tables that fit L2, and positions generated in the
+    kernel into tables from L2 size to several GB.  Prints one JSON line."""
+    import ctypes
+
+    from biobloom_b200 import _lib as L
+    lib = L.lib()
+    out = {"workload": "random 4-byte gathers (bbt_measure_gather)", "unit": "gathers/s",
+           "n_gathers": 1 << 29, "reps": 5, "streamed": {}, "generated": {}}
+    rate = ctypes.c_double()
+    for mb in (4, 8, 16, 24, 32, 48, 64, 80, 96, 128, 192, 256, 512):
+        L.check(lib.bbt_measure_gather(0, mb << 20, 1 << 29, 1, 5, ctypes.byref(rate)))
+        out["streamed"][f"{mb}MB"] = rate.value
+        log(f"streamed {mb} MB: {rate.value / 1e9:.1f} G/s")
+    for mb in (16, 32, 64, 96, 128, 1024, 2048, 4096, 8192):
+        L.check(lib.bbt_measure_gather(0, mb << 20, 1 << 29, 0, 5, ctypes.byref(rate)))
+        out["generated"][f"{mb}MB"] = rate.value
+        log(f"generated {mb} MB: {rate.value / 1e9:.1f} G/s")
+    print(json.dumps(out), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1600,7 +1624,7 @@ def main():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--l2-fetch", type=int, default=0, help="L2 fetch granularity (bytes)")
     ap.add_argument("--workload", default="varlen",
-                    choices=["varlen", "bf", "mibf", "small", "serve", "modes"])
+                    choices=["varlen", "bf", "mibf", "small", "serve", "modes", "gather"])
     ap.add_argument("--requests", type=int, default=200, help="requests (--workload serve)")
     ap.add_argument("--load", type=float, default=0.7,
                     help="offered load, fraction of offline capacity (--workload serve)")
@@ -1615,7 +1639,13 @@ def main():
         args.reads = 20_000_000
     if args.warmup < 3:
         log("warning: fewer than 3 warm-up steps")
-    if args.workload == "serve":
+    if args.workload == "gather":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable":
+                              "a property of the GPU; the reference has no GPU path"}))
+        else:
+            run_gather(args)
+    elif args.workload == "serve":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable":
                               "the serving engine has no counterpart in the reference"}))

@@ -18,6 +18,7 @@ MIBF_OUT_TSV, MIBF_OUT_FASTA, MIBF_OUT_FASTQ = 0, 1, 2
 MIBF_LAYOUT_AUTO, MIBF_LAYOUT_RANK, MIBF_LAYOUT_DENSE = 0, 1, 2
 SCORE_SIMPLE, SCORE_LENGTH, SCORE_HARMONIC, SCORE_BINOMIAL = 0, 1, 2, 3
 HOST, DEVICE = 0, 1
+BASES_ASCII, BASES_2BIT = 0, 1
 PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT, PATH_FILTER_MAJOR = 0, 1, 2, 3
 MODE_STD, MODE_ORDERED, MODE_BESTHIT, MODE_SCORES = 0, 1, 2, 3
 
@@ -43,7 +44,8 @@ class Params(ctypes.Structure):
 class Batch(ctypes.Structure):
     _fields_ = [("seq", ctypes.c_void_p), ("offsets", ctypes.c_void_p), ("seq2", ctypes.c_void_p),
                 ("offsets2", ctypes.c_void_p), ("n_reads", ctypes.c_uint64),
-                ("location", ctypes.c_int)]
+                ("location", ctypes.c_int), ("encoding", ctypes.c_int),
+                ("valid", ctypes.c_void_p), ("valid2", ctypes.c_void_p)]
 
 
 class Result(ctypes.Structure):
@@ -173,6 +175,8 @@ def lib():
         "bbt_graph_destroy": (i32, [vp]),
         "bbt_classify_noalloc": (i32, [P(FilterView), i32, P(Params), P(Batch), vp, vp, vp]),
         "bbt_make_filter": (i32, [vp, P(u64), u64, u32, dbl, u32, u64, cp, cp, cp, i32]),
+        "bbt_measure_gather": (i32, [i32, u64, u64, i32, i32, P(dbl)]),
+        "bbt_pack_bases": (i32, [vp, u64, vp, vp, P(u64)]),
         "bbt_synth_genome": (i32, [u64, u64, dbl, dbl, ctypes.c_uint32, ctypes.c_uint32, dbl, dbl,
                                    vp]),
         "bbt_synth_read_lengths": (i32, [u64, P(SynthReadParams), u64, vp]),

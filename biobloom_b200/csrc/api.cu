@@ -106,6 +106,8 @@ static void free_slot(Slot &s)
 {
 	for (int m = 0; m < 2; ++m) {
 		cudaFree(s.d_seq[m]);
+		cudaFree(s.d_valid[m]);
+		s.d_valid[m] = nullptr;
 		cudaFree(s.d_off[m]);
 		cudaFree(s.d_hits[m]);
 		cudaFree(s.d_scores[m]);
@@ -285,6 +287,8 @@ static int alloc_slot(bbt_ctx *ctx, Slot &s, uint64_t bases, uint64_t reads)
 	free_slot(s);
 	for (int m = 0; m < 2; ++m) {
 		CUDA_TRY(ctx, cudaMalloc(&s.d_seq[m], std::max<uint64_t>(bases, 16)));
+		/* a 2-bit batch's validity bits: one bit per base plus alignment */
+		CUDA_TRY(ctx, cudaMalloc(&s.d_valid[m], bases / 8 + 16));
 		CUDA_TRY(ctx, cudaMalloc(&s.d_off[m], (reads + 1) * sizeof(uint64_t)));
 		CUDA_TRY(ctx, cudaMalloc(&s.d_hits[m], reads * ctx->words * sizeof(uint64_t)));
 	}
@@ -889,6 +893,12 @@ static int classify_device(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r, cuda
 	a.off[0] = b->offsets;
 	a.seq[1] = (const uint8_t *)(paired ? b->seq2 : b->seq);
 	a.off[1] = paired ? b->offsets2 : b->offsets;
+	a.packed = b->encoding == BBT_BASES_2BIT;
+	if (a.packed && ctx->dust)
+		return fail(ctx, BBT_ERR_UNSUPPORTED, "DUST masking reads ASCII bases; pass the batch "
+				"as BBT_BASES_ASCII");
+	a.valid[0] = a.packed ? b->valid : nullptr;
+	a.valid[1] = a.packed ? (paired ? b->valid2 : b->valid) : nullptr;
 	a.n = b->n_reads;
 	a.mates = paired ? 2 : 1;
 	if (!r->hits || (paired && !r->hits2)) {
@@ -940,6 +950,7 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 {
 	const bool paired = b->seq2 != nullptr;
 	const uint64_t n = b->n_reads;
+	const bool packed = b->encoding == BBT_BASES_2BIT;
 	const bool want_scores = scores && (scores[0] || (paired && scores[1]));
 	if (want_scores) {
 		/* per-slot score arrays of cap_reads reads */
@@ -1030,23 +1041,45 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 		a.n = cnt;
 		a.mates = paired ? 2 : 1;
 		uint64_t mate_bases[2] = {0, 0};
+		a.packed = packed;
 		for (int m = 0; m < (paired ? 2 : 1); ++m) {
 			const char *seq = m ? b->seq2 : b->seq;
 			const uint64_t *off = m ? b->offsets2 : b->offsets;
 			const uint64_t lo = off[i0], hi = off[i1];
 			mate_bases[m] = hi - lo;
-			if (hi > lo)
-				CUDA_TRY(ctx, cudaMemcpyAsync(s.d_seq[m], seq + lo, hi - lo,
-						cudaMemcpyHostToDevice, ctx->h2d));
+			if (packed) {
+				/* whole words from a 32-base boundary, so that code words and
+				 * validity words share the slot's base index */
+				const uint64_t lo_a = lo & ~31ull;
+				const uint32_t *valid = m ? b->valid2 : b->valid;
+				if (hi > lo) {
+					const uint64_t w0 = lo_a / 16, w1 = (hi + 15) / 16;
+					CUDA_TRY(ctx, cudaMemcpyAsync(s.d_seq[m],
+							reinterpret_cast<const uint32_t *>(seq) + w0, (w1 - w0) * 4,
+							cudaMemcpyHostToDevice, ctx->h2d));
+					if (valid) {
+						const uint64_t v0 = lo_a / 32, v1 = (hi + 31) / 32;
+						CUDA_TRY(ctx, cudaMemcpyAsync(s.d_valid[m], valid + v0, (v1 - v0) * 4,
+								cudaMemcpyHostToDevice, ctx->h2d));
+					}
+				}
+				a.valid[m] = valid ? s.d_valid[m] : nullptr;
+				a.off_base[m] = lo_a;
+			} else {
+				if (hi > lo)
+					CUDA_TRY(ctx, cudaMemcpyAsync(s.d_seq[m], seq + lo, hi - lo,
+							cudaMemcpyHostToDevice, ctx->h2d));
+				a.off_base[m] = lo;
+			}
 			CUDA_TRY(ctx, cudaMemcpyAsync(s.d_off[m], off + i0, (cnt + 1) * sizeof(uint64_t),
 					cudaMemcpyHostToDevice, ctx->h2d));
 			a.seq[m] = s.d_seq[m];
 			a.off[m] = s.d_off[m];
-			a.off_base[m] = lo;
 			a.hits[m] = s.d_hits[m];
 		}
 		if (!paired) {
 			a.seq[1] = a.seq[0];
+			a.valid[1] = a.valid[0];
 			a.off[1] = a.off[0];
 			a.off_base[1] = a.off_base[0];
 			a.hits[1] = nullptr;
@@ -1141,6 +1174,17 @@ static int classify_batch(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *resu
 	if (batch->location != result->location)
 		return fail(ctx, BBT_ERR_ARG,
 				std::string(who) + ": batch and result must both be host or both device");
+	if (batch->encoding != BBT_BASES_ASCII && batch->encoding != BBT_BASES_2BIT)
+		return fail(ctx, BBT_ERR_ARG, std::string(who) + ": unknown base encoding");
+	if (batch->encoding == BBT_BASES_2BIT) {
+		if ((reinterpret_cast<uintptr_t>(batch->seq) & 3u) ||
+				(batch->seq2 && (reinterpret_cast<uintptr_t>(batch->seq2) & 3u)))
+			return fail(ctx, BBT_ERR_ARG, std::string(who) + ": 2-bit code words must be "
+					"4-byte aligned");
+		if (ctx->dust)
+			return fail(ctx, BBT_ERR_UNSUPPORTED, std::string(who) + ": DUST masking reads "
+					"ASCII bases; pass the batch as BBT_BASES_ASCII");
+	}
 	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
 	if (batch->location == BBT_DEVICE) {
 		cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;

@@ -52,7 +52,7 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 	const uint64_t *off = a.off[mate];
 	const uint64_t start = off[i] - a.off_base[mate];
 	const uint64_t len = off[i + 1] - off[i];
-	const uint8_t *s = a.seq[mate] + start;
+	const Bases s = read_bases(a, mate, start);
 	unsigned cached_k = 0;
 	int64_t cached_w0 = -1;
 	unsigned reads = 0;

@@ -9,13 +9,18 @@
 #include <stdint.h>
 
 #include "bbt_device.cuh"
+#if defined(__CUDACC__)
+#include "window.cuh"
+#endif
 
 namespace bbt {
 
 /* Everything one classify launch needs.  Reads r in [0, n * mates): r < n is
  * read r of mate array 0, otherwise read r - n of mate array 1. */
 struct ClassifyArgs {
-	const uint8_t *seq[2];
+	const uint8_t *seq[2];     /* ASCII bases, or 2-bit code words when packed */
+	const uint32_t *valid[2];  /* packed: validity bits (NULL = all bases ACGT) */
+	int packed;                /* bases are BBT_BASES_2BIT */
 	const uint64_t *off[2];
 	uint64_t off_base[2];      /* subtracted from offsets (staged batches) */
 	uint64_t n;                /* reads per mate array */
@@ -52,6 +57,25 @@ __device__ __forceinline__ bool dust_low(const uint32_t *mask, uint64_t g)
 {
 	return mask && ((mask[g >> 5] >> (g & 31u)) & 1u);
 }
+
+#if defined(__CUDACC__)
+/* The bases of the read starting at base `start` of mate array `mate`. */
+__device__ __forceinline__ Bases read_bases(const ClassifyArgs &a, uint32_t mate, uint64_t start)
+{
+	Bases b;
+	b.g0 = start;
+	if (a.packed) {
+		b.ascii = nullptr;
+		b.words = reinterpret_cast<const uint32_t *>(a.seq[mate]);
+		b.valid = a.valid[mate];
+	} else {
+		b.ascii = a.seq[mate];
+		b.words = nullptr;
+		b.valid = nullptr;
+	}
+	return b;
+}
+#endif
 
 struct LaunchConfig {
 	int path;             /* BBT_PATH_PLAIN or BBT_PATH_PERSISTENT */

@@ -18,7 +18,8 @@ namespace bbt {
 
 /* One staging slot for host batches (inputs in, results out). */
 struct Slot {
-	uint8_t *d_seq[2] = {nullptr, nullptr};
+	uint8_t *d_seq[2] = {nullptr, nullptr};   /* ASCII bytes or 2-bit code words */
+	uint32_t *d_valid[2] = {nullptr, nullptr}; /* 2-bit batches: validity bits */
 	uint64_t *d_off[2] = {nullptr, nullptr};
 	uint64_t *d_hits[2] = {nullptr, nullptr};
 	uint32_t *d_cat = nullptr;

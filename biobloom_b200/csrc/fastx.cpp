@@ -553,7 +553,7 @@ int run_pipeline(bbt_ctx *ctx, const PipeInput &in, const char *prefix, const ch
 		const bool last = b.last;
 		if (b.n) {
 			b.cat.resize(b.n);
-			bbt_batch bt;
+			bbt_batch bt = {};
 			bt.seq = b.seq[0];
 			bt.offsets = b.off[0].data();
 			bt.seq2 = paired ? b.seq[1] : nullptr;

@@ -172,7 +172,7 @@ int run(bbt_mibf *ctx, const std::vector<std::string> &files, const std::string 
 		MiBatch &b = hb[which];
 		const bool last = b.last;
 		if (b.n) {
-			bbt_batch bt;
+			bbt_batch bt = {};
 			bt.seq = b.seq[0].data();
 			bt.offsets = b.off[0].data();
 			bt.seq2 = paired ? b.seq[1].data() : nullptr;

@@ -81,6 +81,8 @@ extern "C" int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filter
 	const bool paired = batch->seq2 != nullptr;
 	if (!batch->seq || !batch->offsets || (paired && (!batch->offsets2 || !hits2)))
 		return fail(nullptr, BBT_ERR_ARG, "bbt_classify_noalloc: missing reads, offsets or hits");
+	if (batch->encoding != BBT_BASES_ASCII && batch->encoding != BBT_BASES_2BIT)
+		return fail(nullptr, BBT_ERR_ARG, "bbt_classify_noalloc: unknown base encoding");
 	double score = params->score;
 	int scoring = params->scoring;
 	if (!(score < 4294967296.0))
@@ -143,6 +145,9 @@ extern "C" int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filter
 		a.off[0] = batch->offsets;
 		a.seq[1] = (const uint8_t *)(paired ? batch->seq2 : batch->seq);
 		a.off[1] = paired ? batch->offsets2 : batch->offsets;
+		a.packed = batch->encoding == BBT_BASES_2BIT;
+		a.valid[0] = a.packed ? batch->valid : nullptr;
+		a.valid[1] = a.packed ? (paired ? batch->valid2 : batch->valid) : nullptr;
 		a.n = batch->n_reads;
 		a.mates = paired ? 2 : 1;
 		a.filters = scratch->filters;

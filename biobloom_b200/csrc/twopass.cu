@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256) hash_pass_kernel(ClassifyArgs a, TwoPassA
 		const uint64_t len = a.off[mate][i + 1] - a.off[mate][i];
 		if (len < p.k)
 			continue;
-		const uint8_t *s = a.seq[mate] + (a.off[mate][i] - a.off_base[mate]);
+		const Bases s = read_bases(a, mate, a.off[mate][i] - a.off_base[mate]);
 		const uint64_t frames = len - p.k + 1;
 		const uint64_t base = frame_base(p, t);
 		for (uint64_t w0 = 0; w0 < frames; w0 += W) {

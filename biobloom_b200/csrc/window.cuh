@@ -76,17 +76,39 @@ __device__ __forceinline__ uint64_t seed_of(const uint64_t *tab, int which, uint
 	return tab[code < 4 ? which * 4 + code : 16];
 }
 
-/* Hash frames [w0, w0 + wn) of the read at s into the window: base codes are
- * staged with coalesced loads, then each lane hashes S consecutive frames
- * (Horner over its first k-mer, rolling after), and the validity of the frames
- * is balloted into one mask word per 32 frames. */
+/* Where a read's bases are: base j of the read is element g0 + j of either an
+ * ASCII byte array, or of 2-bit code words (base g at bits 2 (g % 16) of
+ * words[g / 16]) with validity bits (bit g % 32 of valid[g / 32]; NULL = every
+ * base is ACGT). */
+struct Bases {
+	const uint8_t *ascii;
+	const uint32_t *words;
+	const uint32_t *valid;
+	uint64_t g0;
+};
+
+/* Code 0..3 of base j, 4 when it is not ACGT. */
+__device__ __forceinline__ uint8_t base_code_at(const Bases &b, uint64_t j)
+{
+	const uint64_t g = b.g0 + j;
+	if (b.ascii)
+		return base_code(b.ascii[g]);
+	if (b.valid && !((__ldg(b.valid + (g >> 5)) >> (g & 31u)) & 1u))
+		return 4;
+	return (uint8_t)((__ldg(b.words + (g >> 4)) >> (2u * (uint32_t)(g & 15u))) & 3u);
+}
+
+/* Hash frames [w0, w0 + wn) of the read whose bases src describes into the
+ * window: base codes are staged with coalesced loads, then each lane hashes S
+ * consecutive frames (Horner over its first k-mer, rolling after), and the
+ * validity of the frames is balloted into one mask word per 32 frames. */
 template <int SEG>
-__device__ void hash_window(const uint8_t *__restrict__ s, uint64_t w0, int wn, unsigned k,
+__device__ void hash_window(const Bases &src, uint64_t w0, int wn, unsigned k,
 		const Window<SEG> &win, int lane)
 {
 	const int nb = wn + (int)k - 1;
 	for (int b = lane; b < nb; b += 32)
-		win.code[b] = base_code(s[w0 + b]);
+		win.code[b] = base_code_at(src, w0 + b);
 	__syncwarp();
 	const int S = (wn + 31) >> 5; /* frames per lane in this window */
 	const int q0 = lane * S;

@@ -99,10 +99,24 @@ int bbt_num_filters(const bbt_ctx *ctx);
 /* Filter id of filter i (BloomFilterInfo::getFilterID, BloomFilterInfo.cpp:141). */
 const char *bbt_filter_id(const bbt_ctx *ctx, int i);
 
+/* Base encodings of a batch (bbt_batch.encoding). */
+#define BBT_BASES_ASCII 0      /* one byte per base, as in FASTA / FASTQ */
+#define BBT_BASES_2BIT 1       /* 2-bit codes + validity bits (below) */
+
 /*
  * A batch of reads.  Single-end: seq/offsets hold n_reads reads
- * (read i = seq[offsets[i] .. offsets[i+1])).  Paired: seq2/offsets2 hold the
- * mates, read i of seq pairs with read i of seq2, and n_reads counts pairs.
+ * (read i = bases offsets[i] .. offsets[i+1] of seq).  Paired: seq2/offsets2
+ * hold the mates, read i of seq pairs with read i of seq2, and n_reads counts
+ * pairs.
+ *
+ * encoding BBT_BASES_ASCII (0, the default of a zeroed struct): seq holds one
+ * byte per base.  BBT_BASES_2BIT: seq points to uint32 words with base g at
+ * bits 2 (g % 16) .. 2 (g % 16) + 1 of word g / 16 (A/a = 0, C/c = 1, G/g = 2,
+ * T/t = 3), 4 times fewer bytes to copy; valid (valid2 for seq2) holds bit
+ * g % 32 of word g / 32 = 1 when base g is one of ACGTacgt (any other base is
+ * skipped by the k-mer iterator, as an N is), or is NULL when every base is.
+ * The word arrays must be 4-byte aligned; bbt_pack_bases fills them.
+ * Offsets count bases in either encoding.
  */
 typedef struct {
 	const char *seq;
@@ -110,8 +124,21 @@ typedef struct {
 	const char *seq2;          /* NULL for single-end */
 	const uint64_t *offsets2;
 	uint64_t n_reads;
-	int location;              /* BBT_HOST or BBT_DEVICE for all four arrays */
+	int location;              /* BBT_HOST or BBT_DEVICE for all the arrays */
+	int encoding;              /* BBT_BASES_ASCII or BBT_BASES_2BIT */
+	const uint32_t *valid;     /* BBT_BASES_2BIT: validity bits of seq, or NULL */
+	const uint32_t *valid2;    /* BBT_BASES_2BIT: validity bits of seq2, or NULL */
 } bbt_batch;
+
+/*
+ * Pack n ASCII bases into the BBT_BASES_2BIT form: words (n + 15) / 16 uint32,
+ * valid (n + 31) / 32 uint32 (may be NULL when the caller knows every base is
+ * ACGTacgt).  *n_invalid (optional) receives the number of other bases; when
+ * it is 0 the batch may pass valid = NULL.  Host memory, all host threads.
+ * No counterpart in the reference, which keeps reads as strings.
+ */
+int bbt_pack_bases(const char *ascii, uint64_t n, uint32_t *words, uint32_t *valid,
+		uint64_t *n_invalid);
 
 /*
  * Per-read results.  hits/hits2 (optional): words = (n_filters + 63) / 64
@@ -381,6 +408,17 @@ typedef struct {
 int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filters,
 		const bbt_params *params, const bbt_batch *batch, uint64_t *hits,
 		uint64_t *hits2, void *stream);
+
+/* ---- machine ceilings ---- */
+
+/* Random 4-byte gathers per second into a table of table_bytes (allocated by
+ * the call) on `device`: n_gathers per launch, median of reps launches after
+ * one warm-up launch.  position_stream = 1 reads the 32-bit bit positions from
+ * device memory (4 bytes per gather, evict-first; table of at most 512 MB),
+ * 0 generates them in the kernel.  No counterpart in the reference: it states
+ * the ceilings Bloom probes run against (a table inside L2 or in HBM). */
+int bbt_measure_gather(int device, uint64_t table_bytes, uint64_t n_gathers,
+		int position_stream, int reps, double *gathers_per_s);
 
 /* ---- synthetic workloads (host only; no GPU needed) ---- */
 
