@@ -282,6 +282,37 @@ static int upload_filter(bbt_ctx *ctx, const std::string &path, BfHeader &hd, ui
 	return BBT_OK;
 }
 
+/* Host-only checks of one filter's files before any device work: the .txt
+ * sidecar opens and names the filter, the .bf header parses and the payload
+ * holds the m / 8 bytes the header promises.  The reference exits on the same
+ * conditions (BloomFilterInfo / BloomFilter constructors). */
+static int check_filter_files(const std::string &path)
+{
+	std::map<std::string, std::string> kv;
+	const std::string info = info_path_for(path);
+	if (!read_ini(info, kv))
+		return fail(nullptr, BBT_ERR_IO, "file " + info + " cannot be opened");
+	if (kv.find("user_input_options.filter_id") == kv.end())
+		return fail(nullptr, BBT_ERR_FORMAT, info + ": no user_input_options.filter_id");
+	FILE *f = fopen(path.c_str(), "rb");
+	if (!f)
+		return fail(nullptr, BBT_ERR_IO, "file " + path + " cannot be opened");
+	BfHeader hd;
+	const char *msg = read_bf_header(f, hd);
+	if (msg) {
+		fclose(f);
+		return fail(nullptr, BBT_ERR_FORMAT, path + ": " + msg);
+	}
+	const long at = ftell(f);
+	const bool sized = at >= 0 && fseek(f, 0, SEEK_END) == 0;
+	const long end = sized ? ftell(f) : -1;
+	fclose(f);
+	if (!sized || end < at || (uint64_t)(end - at) < hd.m / 8)
+		return fail(nullptr, BBT_ERR_FORMAT, path + ": filter payload is shorter than its "
+				"header says (" + std::to_string(hd.m / 8) + " bytes)");
+	return BBT_OK;
+}
+
 static int alloc_slot(bbt_ctx *ctx, Slot &s, uint64_t bases, uint64_t reads)
 {
 	free_slot(s);
@@ -356,6 +387,18 @@ extern "C" int bbt_open(const char *const *bf_paths, int n_filters, const bbt_pa
 				"(0, 1]; the scoring method is BBT_SCORE_*";
 		bbt_close(ctx);
 		return fail(nullptr, BBT_ERR_ARG, m);
+	}
+	for (int i = 0; i < n_filters; ++i) {
+		if (!bf_paths[i]) {
+			bbt_close(ctx);
+			return fail(nullptr, BBT_ERR_ARG, "null filter path");
+		}
+		int rc0 = check_filter_files(bf_paths[i]);
+		if (rc0 != BBT_OK) {
+			std::string m = bbt_last_error(nullptr);
+			bbt_close(ctx);
+			return fail(nullptr, rc0, m);
+		}
 	}
 	int ndev = 0;
 	cudaError_t e = cudaGetDeviceCount(&ndev);
