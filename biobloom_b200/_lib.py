@@ -19,7 +19,7 @@ MIBF_LAYOUT_AUTO, MIBF_LAYOUT_RANK, MIBF_LAYOUT_DENSE = 0, 1, 2
 SCORE_SIMPLE, SCORE_LENGTH, SCORE_HARMONIC, SCORE_BINOMIAL = 0, 1, 2, 3
 HOST, DEVICE = 0, 1
 BASES_ASCII, BASES_2BIT = 0, 1
-PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT, PATH_FILTER_MAJOR = 0, 1, 2, 3
+PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT, PATH_FILTER_MAJOR, PATH_BUCKETED = 0, 1, 2, 3, 4
 MODE_STD, MODE_ORDERED, MODE_BESTHIT, MODE_SCORES = 0, 1, 2, 3
 
 
@@ -177,6 +177,7 @@ def lib():
         "bbt_make_filter": (i32, [vp, P(u64), u64, u32, dbl, u32, u64, cp, cp, cp, i32]),
         "bbt_measure_gather": (i32, [i32, u64, u64, i32, i32, P(dbl)]),
         "bbt_pack_bases": (i32, [vp, u64, vp, vp, P(u64)]),
+        "bbt_set_bucketing": (i32, [vp, u32, u32, u32, u64]),
         "bbt_synth_genome": (i32, [u64, u64, dbl, dbl, ctypes.c_uint32, ctypes.c_uint32, dbl, dbl,
                                    vp]),
         "bbt_synth_read_lengths": (i32, [u64, P(SynthReadParams), u64, vp]),

@@ -22,7 +22,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC,
           "-Xcompiler", "-fPIC,-fopenmp,-O3,-Wall", "-ccbin", "/usr/bin/g++"]
-LIB_SOURCES = ["classify.cu", "score.cu", "dust.cu", "twopass.cu", "api.cu", "noalloc.cu", "gather_rate.cu", "maker.cu", "mibf.cu",
+LIB_SOURCES = ["classify.cu", "score.cu", "dust.cu", "twopass.cu", "bucketed.cu", "api.cu", "noalloc.cu", "gather_rate.cu", "maker.cu", "mibf.cu",
                "mibf_make.cu", "formats.cpp", "pack.cpp", "fastx.cpp", "synth.cpp", "mibf_host.cpp",
                "mibf_pipeline.cpp", "server.cpp"]
 CLIS = [("biobloomcategorizer", "cli_categorizer.cpp"),

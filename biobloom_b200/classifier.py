@@ -110,6 +110,11 @@ class BioBloomClassifier:
         L.check(L.lib().bbt_set_launch(self._ctx, path, warps_per_block, frames_per_lane),
                 self._ctx)
 
+    def set_bucketing(self, bucket_shift=0, phase_split=0, phase_min=0, max_frames=0):
+        """Settings of the bucketed path (bbt_set_bucketing; 0 keeps one)."""
+        L.check(L.lib().bbt_set_bucketing(self._ctx, bucket_shift, phase_split, phase_min,
+                                          max_frames), self._ctx)
+
     def set_schedule(self, long_bases=0):
         """Persistent kernel read order: reads of at least long_bases bases
         first (0 = index order)."""

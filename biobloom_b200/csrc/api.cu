@@ -4,6 +4,8 @@
  */
 #include <cuda_runtime.h>
 
+#include <cub/device/device_scan.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -15,6 +17,7 @@
 #include <vector>
 
 #include "bbt.h"
+#include "bucketed.cuh"
 #include "classify.cuh"
 #include "ctx.hpp"
 #include "formats.hpp"
@@ -179,6 +182,19 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 	cudaFree(ctx->d_tp_local);
 	cudaFree(ctx->d_tp_sums);
 	cudaFreeHost(ctx->h_tp_sums);
+	cudaFree(ctx->d_bk_fo);
+	cudaFree(ctx->d_bk_state);
+	cudaFreeHost(ctx->h_bk_samples);
+	cudaFree(ctx->d_bk_vbits);
+	cudaFree(ctx->d_bk_hbits);
+	cudaFree(ctx->d_bk_off);
+	cudaFree(ctx->d_bk_fid);
+	cudaFree(ctx->d_bk_res);
+	for (int i = 0; i < 2; ++i) {
+		cudaFree(ctx->d_bk_cnt[i]);
+		cudaFree(ctx->d_bk_seg[i]);
+	}
+	cudaFree(ctx->d_bk_tmp);
 	cudaFree(ctx->d_tp_h0);
 	cudaFree(ctx->d_tp_vmask);
 	for (Slot &s : ctx->slot) {
@@ -325,6 +341,16 @@ static int alloc_slot(bbt_ctx *ctx, Slot &s, uint64_t bases, uint64_t reads)
 	}
 	CUDA_TRY(ctx, cudaMalloc(&s.d_cat, reads * sizeof(uint32_t)));
 	return BBT_OK;
+}
+
+/* Filters far above L2, where sorting probes by address pays for its passes:
+ * the largest above 256 MB. */
+static bool bucketing_pays(const bbt_ctx *ctx)
+{
+	for (const FilterDev &f : ctx->hf)
+		if (f.m / 8 > (256ull << 20))
+			return true;
+	return false;
 }
 
 /* The tuned path: with two or more filters of one k that each fit in L2,
@@ -754,6 +780,272 @@ static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s,
 	return BBT_OK;
 }
 
+/* Scratch of the bucketed path for sub-batches of up to `frames` frames and
+ * nbkt buckets x nblk blocks of counts. */
+static int bk_reserve(bbt_ctx *ctx, uint64_t frames, uint64_t cnt_entries)
+{
+	if (frames > ctx->bk_frames_cap) {
+		cudaFree(ctx->d_bk_vbits);
+		cudaFree(ctx->d_bk_hbits);
+		cudaFree(ctx->d_bk_off);
+		cudaFree(ctx->d_bk_fid);
+		cudaFree(ctx->d_bk_res);
+		ctx->d_bk_vbits = ctx->d_bk_hbits = ctx->d_bk_off = ctx->d_bk_res = nullptr;
+		ctx->d_bk_fid = nullptr;
+		ctx->bk_frames_cap = 0;
+		/* whole window blocks, plus spare words for reads across the end */
+		const uint64_t f = (frames + kBkWinFrames - 1) / kBkWinFrames * kBkWinFrames;
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_vbits, (f / 32 + 2) * sizeof(uint32_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_hbits, (f / 32 + 2) * sizeof(uint32_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_off, f * sizeof(uint32_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_fid, f * sizeof(uint16_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_res, (f / 32 + 2) * sizeof(uint32_t)));
+		ctx->bk_frames_cap = f;
+	}
+	if (cnt_entries > ctx->bk_cnt_cap) {
+		for (int i = 0; i < 2; ++i) {
+			cudaFree(ctx->d_bk_cnt[i]);
+			cudaFree(ctx->d_bk_seg[i]);
+			ctx->d_bk_cnt[i] = ctx->d_bk_seg[i] = nullptr;
+		}
+		ctx->bk_cnt_cap = 0;
+		for (int i = 0; i < 2; ++i) {
+			CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_cnt[i], cnt_entries * sizeof(unsigned long long)));
+			CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_seg[i], cnt_entries * sizeof(unsigned long long)));
+		}
+		ctx->bk_cnt_cap = cnt_entries;
+	}
+	return BBT_OK;
+}
+
+static int bk_tmp(bbt_ctx *ctx, size_t bytes)
+{
+	if (bytes <= ctx->bk_tmp_cap)
+		return BBT_OK;
+	cudaFree(ctx->d_bk_tmp);
+	ctx->d_bk_tmp = nullptr;
+	ctx->bk_tmp_cap = 0;
+	CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_tmp, bytes));
+	ctx->bk_tmp_cap = bytes;
+	return BBT_OK;
+}
+
+struct BkCut {
+	uint64_t r0, r1;  /* reads of the sub-batch */
+	uint64_t f0, f1;  /* their frames */
+};
+
+/* Sub-batches of consecutive reads with at most `most` frames each, from the
+ * frame offsets fo (device) of `total` reads: samples of fo every 4096 reads
+ * come to the host (one short wait), and a sample interval above the limit is
+ * read in full.  Reads with more than `most` frames on their own go to
+ * `oversize`. */
+static int bk_plan(bbt_ctx *ctx, const uint64_t *fo, uint64_t total, uint64_t most,
+		cudaStream_t s, std::vector<BkCut> &cuts, std::vector<uint64_t> &oversize)
+{
+	const uint64_t S = 4096;
+	const uint64_t ns = total / S + 1;
+	if (ns + 1 > ctx->bk_samples_cap) {
+		cudaFreeHost(ctx->h_bk_samples);
+		ctx->h_bk_samples = nullptr;
+		ctx->bk_samples_cap = 0;
+		CUDA_TRY(ctx, cudaMallocHost(&ctx->h_bk_samples, (ns + 1) * sizeof(uint64_t)));
+		ctx->bk_samples_cap = ns + 1;
+	}
+	uint64_t *h = ctx->h_bk_samples;
+	CUDA_TRY(ctx, cudaMemcpy2DAsync(h, sizeof(uint64_t), fo, S * sizeof(uint64_t),
+			sizeof(uint64_t), ns, cudaMemcpyDeviceToHost, s));
+	CUDA_TRY(ctx, cudaMemcpyAsync(h + ns, fo + total, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+	CUDA_TRY(ctx, cudaStreamSynchronize(s));
+	std::vector<uint64_t> pt(ns + 1), fv(ns + 1);
+	for (uint64_t j = 0; j < ns; ++j) {
+		pt[j] = j * S;
+		fv[j] = h[j];
+	}
+	pt[ns] = total;
+	fv[ns] = h[ns];
+	cuts.clear();
+	oversize.clear();
+	uint64_t j = 0;
+	std::vector<uint64_t> fine;
+	while (pt[j] < total) {
+		uint64_t jj = j;
+		while (jj + 1 <= ns && fv[jj + 1] - fv[j] <= most)
+			++jj;
+		if (jj > j) {
+			if (fv[jj] > fv[j])
+				cuts.push_back({pt[j], pt[jj], fv[j], fv[jj]});
+			j = jj;
+			continue;
+		}
+		/* the next sample interval alone is above the limit: cut it per read */
+		const uint64_t a0 = pt[j], a1 = pt[j + 1];
+		fine.resize(a1 - a0 + 1);
+		CUDA_TRY(ctx, cudaMemcpy(fine.data(), fo + a0, fine.size() * sizeof(uint64_t),
+				cudaMemcpyDeviceToHost));
+		uint64_t r = a0;
+		while (r < a1) {
+			uint64_t e = r;
+			while (e + 1 <= a1 && fine[e + 1 - a0] - fine[r - a0] <= most)
+				++e;
+			if (e == r) {
+				oversize.push_back(r);
+				e = r + 1;
+			} else if (fine[e - a0] > fine[r - a0]) {
+				cuts.push_back({r, e, fine[r - a0], fine[e - a0]});
+			}
+			r = e;
+		}
+		j = j + 1;
+	}
+	return BBT_OK;
+}
+
+/* The bucketed probe path over one batch (STD / ORDERED modes, every scoring
+ * method): per filter, sub-batches of reads, each resolved in phases and
+ * rounds (bucketed.cu).  Hit words are built bit by bit: zeroed first. */
+static int run_bucketed(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
+{
+	const uint64_t total = a.n * a.mates;
+	const size_t hb = a.n * ctx->words * sizeof(uint64_t);
+	CUDA_TRY(ctx, cudaMemsetAsync(a.hits[0], 0, hb, s));
+	if (a.mates == 2)
+		CUDA_TRY(ctx, cudaMemsetAsync(a.hits[1], 0, hb, s));
+	if (total == 0)
+		return BBT_OK;
+	if (total + 1 > ctx->bk_reads_cap) {
+		cudaFree(ctx->d_bk_fo);
+		cudaFree(ctx->d_bk_state);
+		ctx->d_bk_fo = nullptr;
+		ctx->d_bk_state = nullptr;
+		ctx->bk_reads_cap = 0;
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_fo, (total + 1) * sizeof(uint64_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_state, total + 1));
+		ctx->bk_reads_cap = total + 1;
+	}
+	const uint64_t most = std::max<uint64_t>(ctx->bk_max_frames, kBkWinFrames);
+	size_t scan_bytes = 0;
+	CUDA_TRY(ctx, cub::DeviceScan::InclusiveSum(nullptr, scan_bytes, ctx->d_bk_fo + 1,
+			ctx->d_bk_fo + 1, total, s));
+	int rc = bk_tmp(ctx, scan_bytes);
+	if (rc)
+		return rc;
+	std::vector<BkCut> cuts;
+	std::vector<uint64_t> oversize;
+	unsigned cur_k = 0;
+	for (uint32_t f = 0; f < ctx->nf; ++f) {
+		const FilterDev &F = ctx->hf[f];
+		if (F.k != cur_k) {
+			cur_k = F.k;
+			CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_fo, 0, sizeof(uint64_t), s));
+			CUDA_TRY(ctx, launch_bk_frame_counts(a, cur_k, ctx->d_bk_fo + 1, ctx->num_sms, s));
+			CUDA_TRY(ctx, cub::DeviceScan::InclusiveSum(ctx->d_bk_tmp, scan_bytes,
+					ctx->d_bk_fo + 1, ctx->d_bk_fo + 1, total, s));
+			rc = bk_plan(ctx, ctx->d_bk_fo, total, most, s, cuts, oversize);
+			if (rc)
+				return rc;
+			ctx->last.kernels += 2;
+		}
+		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_state, 0, total, s));
+		for (uint64_t r : oversize) /* the direct kernel's, below */
+			CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_state + r, 1, 1, s));
+		unsigned bshift = std::max<unsigned>(ctx->bk_bshift, 12);
+		while (((F.m + (1ull << bshift) - 1) >> bshift) > 2048)
+			++bshift;
+		const uint32_t nbkt = (uint32_t)((F.m + (1ull << bshift) - 1) >> bshift);
+		const uint32_t split = std::min<uint32_t>(ctx->bk_phase_split, kBkPhaseDen);
+		std::vector<std::pair<uint32_t, uint32_t> > phases;
+		if (split > 0 && split < kBkPhaseDen)
+			phases = {{0, split}, {split, kBkPhaseDen}};
+		else
+			phases = {{0, kBkPhaseDen}};
+		for (const BkCut &c : cuts) {
+			const uint64_t T = c.f1 - c.f0;
+			const uint32_t nblk = (uint32_t)((T + kBkWinFrames - 1) / kBkWinFrames);
+			const uint64_t ncnt = (uint64_t)nbkt * nblk + 1;
+			rc = bk_reserve(ctx, T, ncnt);
+			if (rc)
+				return rc;
+			size_t cnt_bytes = 0;
+			CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(nullptr, cnt_bytes, ctx->d_bk_cnt[0],
+					ctx->d_bk_seg[0], ncnt, s));
+			rc = bk_tmp(ctx, std::max(cnt_bytes, scan_bytes));
+			if (rc)
+				return rc;
+			const uint64_t words = (T + 31) / 32 + 2;
+			CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_vbits, 0, words * sizeof(uint32_t), s));
+			CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_hbits, 0, words * sizeof(uint32_t), s));
+			for (int i = 0; i < 2; ++i)
+				CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_cnt[i] + ncnt - 1, 0,
+						sizeof(unsigned long long), s));
+			BucketArgs b;
+			memset(&b, 0, sizeof b);
+			b.a = a;
+			b.f = F;
+			b.fbit = f;
+			b.r0 = c.r0;
+			b.nr = c.r1 - c.r0;
+			b.fo = ctx->d_bk_fo;
+			b.fo0 = c.f0;
+			b.T = T;
+			b.nblk = nblk;
+			b.vbits = ctx->d_bk_vbits;
+			b.hbits = ctx->d_bk_hbits;
+			b.state = ctx->d_bk_state;
+			b.ph_min = ctx->bk_phase_min;
+			b.nbkt = nbkt;
+			b.bshift = bshift;
+			b.req_off = ctx->d_bk_off;
+			b.req_fid = ctx->d_bk_fid;
+			b.res = ctx->d_bk_res;
+			b.issued = a.probes;
+			for (const auto &ph : phases) {
+				b.ph_lo = ph.first;
+				b.ph_hi = ph.second;
+				for (uint32_t l = 0; l < F.h; ++l) {
+					b.level = l;
+					b.cnt = ctx->d_bk_cnt[l & 1];
+					b.seg = ctx->d_bk_seg[l & 1];
+					b.pcnt = l ? ctx->d_bk_cnt[(l - 1) & 1] : nullptr;
+					b.pseg = l ? ctx->d_bk_seg[(l - 1) & 1] : nullptr;
+					CUDA_TRY(ctx, launch_bk_count(b, s));
+					CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_bk_tmp, cnt_bytes, b.cnt,
+							b.seg, ncnt, s));
+					CUDA_TRY(ctx, launch_bk_write(b, s));
+					CUDA_TRY(ctx, launch_bk_resolve(b, ctx->num_sms, s));
+				}
+				b.pcnt = ctx->d_bk_cnt[(F.h - 1) & 1];
+				b.pseg = ctx->d_bk_seg[(F.h - 1) & 1];
+				CUDA_TRY(ctx, launch_bk_apply(b, s));
+				CUDA_TRY(ctx, launch_bk_walk(b, ctx->num_sms, s));
+				ctx->last.kernels += 4 * F.h + 2;
+			}
+		}
+	}
+	/* reads too long for any sub-batch: the persistent kernel, every filter */
+	for (uint64_t r : oversize) {
+		const uint32_t mate = r >= a.n ? 1u : 0u;
+		const uint64_t i = r - (mate ? a.n : 0);
+		ClassifyArgs one = a;
+		one.seq[0] = one.seq[1] = a.seq[mate];
+		one.valid[0] = one.valid[1] = a.valid[mate];
+		one.off[0] = one.off[1] = a.off[mate] + i;
+		one.off_base[0] = one.off_base[1] = a.off_base[mate];
+		one.dust[0] = one.dust[1] = a.dust[mate];
+		one.hits[0] = a.hits[mate] + i * ctx->words;
+		one.hits[1] = nullptr;
+		one.n = 1;
+		one.mates = 1;
+		one.order = nullptr;
+		LaunchConfig lc = ctx->lc;
+		lc.path = BBT_PATH_PERSISTENT;
+		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_work, 0, sizeof(unsigned long long), s));
+		CUDA_TRY(ctx, launch_classify(one, lc, s));
+		ctx->last.kernels += 1;
+	}
+	return BBT_OK;
+}
+
 /* -D: the SDUST masks of a batch's reads (dust.cu) into ctx->d_dust, set in
  * a.dust.  mate_bases: bases of each mate array counted from its off_base. */
 static int run_dust(bbt_ctx *ctx, ClassifyArgs &a, const uint64_t *mate_bases, cudaStream_t s)
@@ -864,6 +1156,11 @@ static int run_kernels(bbt_ctx *ctx, ClassifyArgs &a, uint32_t *d_cat, cudaStrea
 		/* the hit words are the filters of the largest score */
 		sa.besthit = 1;
 		CUDA_TRY(ctx, launch_scores(a, sa, ctx->lc, s));
+	} else if (ctx->lc.path == BBT_PATH_BUCKETED && !want_scores) {
+		ctx->last.kernels -= 1; /* the passes count themselves */
+		int rc = run_bucketed(ctx, a, s);
+		if (rc)
+			return rc;
 	} else if (two_pass) {
 		/* accepted (filter, read) items OR their bit into zeroed words */
 		const size_t hb = a.n * ctx->words * sizeof(uint64_t);
@@ -1414,6 +1711,26 @@ extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int s
 	return BBT_OK;
 }
 
+extern "C" int bbt_set_bucketing(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
+		unsigned phase_min, uint64_t max_frames)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	if (bucket_shift && (bucket_shift < 12 || bucket_shift > 34))
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_bucketing: bucket_shift must be in [12, 34]");
+	if (phase_split > kBkPhaseDen)
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_bucketing: phase_split must be at most 16");
+	if (bucket_shift)
+		ctx->bk_bshift = bucket_shift;
+	if (phase_split)
+		ctx->bk_phase_split = phase_split;
+	if (phase_min)
+		ctx->bk_phase_min = phase_min;
+	if (max_frames)
+		ctx->bk_max_frames = std::max<uint64_t>(max_frames, kBkWinFrames);
+	return BBT_OK;
+}
+
 extern "C" int bbt_set_schedule(bbt_ctx *ctx, uint64_t long_bases)
 {
 	if (!ctx)
@@ -1492,6 +1809,8 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 			if (auto_path(ctx) == BBT_PATH_FILTER_MAJOR)
 				cands.push_back({BBT_PATH_FILTER_MAJOR, w, sg, 0});
 		}
+	if (bucketing_pays(ctx))
+		cands.push_back({BBT_PATH_BUCKETED, 8, 4, 0});
 	const int cnt = ctx->lc.count;
 	for (const Cand &c : cands) {
 		if (rc)
@@ -1575,9 +1894,10 @@ extern "C" int bbt_graph_create(bbt_ctx *ctx, const bbt_batch *b, const bbt_resu
 		return fail(ctx, BBT_ERR_ARG, "bbt_graph_create: needs device batch and results");
 	if (!r->hits || (b->seq2 && !r->hits2))
 		return fail(ctx, BBT_ERR_ARG, "bbt_graph_create: result hit arrays are required");
-	if (ctx->lc.path == BBT_PATH_FILTER_MAJOR)
-		return fail(ctx, BBT_ERR_UNSUPPORTED, "bbt_graph_create: the filter-major path reads "
-				"block sums on the host; use the plain or persistent path in a graph");
+	if (ctx->lc.path == BBT_PATH_FILTER_MAJOR || ctx->lc.path == BBT_PATH_BUCKETED)
+		return fail(ctx, BBT_ERR_UNSUPPORTED, "bbt_graph_create: the filter-major and bucketed "
+				"paths plan their sub-batches on the host; use the plain or persistent path "
+				"in a graph");
 	if (ctx->dust)
 		return fail(ctx, BBT_ERR_UNSUPPORTED, "bbt_graph_create: DUST masking sizes its "
 				"buffers on the host and cannot be captured");

@@ -113,6 +113,28 @@ struct bbt_ctx {
 	uint64_t *d_order = nullptr;
 	uint64_t order_cap = 0;
 	unsigned long long *d_order_cnt = nullptr;
+	/* bucketed probe path (bucketed.cu): frame offsets of a batch's reads and
+	 * their host samples, per-read state, validity and hit bits of a
+	 * sub-batch, the request pool, per-(bucket, block) counts and their
+	 * scans, scan scratch; and the path's settings */
+	uint64_t *d_bk_fo = nullptr;
+	uint8_t *d_bk_state = nullptr;
+	uint64_t bk_reads_cap = 0;
+	uint64_t *h_bk_samples = nullptr;      /* pinned */
+	uint64_t bk_samples_cap = 0;
+	uint32_t *d_bk_vbits = nullptr, *d_bk_hbits = nullptr;
+	uint32_t *d_bk_off = nullptr, *d_bk_res = nullptr;
+	uint16_t *d_bk_fid = nullptr;
+	uint64_t bk_frames_cap = 0;
+	unsigned long long *d_bk_cnt[2] = {nullptr, nullptr};
+	unsigned long long *d_bk_seg[2] = {nullptr, nullptr};
+	uint64_t bk_cnt_cap = 0;
+	void *d_bk_tmp = nullptr;
+	size_t bk_tmp_cap = 0;
+	uint64_t bk_max_frames = 1ull << 31; /* frames per sub-batch */
+	uint32_t bk_bshift = 28;             /* bucket of 2^28 bits (32 MB) */
+	uint32_t bk_phase_split = 8;         /* phase boundary in sixteenths (16: one phase) */
+	uint32_t bk_phase_min = 64;          /* the first phase covers min(F, 64) frames or more */
 	cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 	cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr; /* around the last classify kernel */
 	bbt::LaunchConfig lc;

@@ -105,10 +105,12 @@ enum { EVAL_OPEN = 0, EVAL_ACCEPT = 1, EVAL_REJECT = 2 };
  * (restricted to `pre`) accepts when it is a hit and
  *   score2 + popc(H & frames<=j) + popc(P2 & frames<=j) >= thres2,
  * and rejects when it adds to antiScore and anti + popc(A & frames<=j) >=
- * anti_thres.  On the device every lane evaluates its own frame and two
- * ballots collect the answers (all 32 lanes of the warp must be here); on the
- * host the lanes are looped over.
+ * anti_thres.  On the device with WARP every lane evaluates its own frame and
+ * two ballots collect the answers (all 32 lanes of the warp must be here);
+ * otherwise (the host, or one thread walking a read on its own) the frames are
+ * looped over with running sums.
  */
+template <bool WARP = true>
 BBT_HD void crossing_masks(uint32_t H, uint32_t P2, uint32_t A, uint32_t pre, int32_t score2,
 		int32_t anti, int32_t thres2, int32_t anti_thres, uint32_t &acc, uint32_t &rej)
 {
@@ -116,25 +118,29 @@ BBT_HD void crossing_masks(uint32_t H, uint32_t P2, uint32_t A, uint32_t pre, in
 	P2 &= pre;
 	A &= pre;
 #if defined(__CUDA_ARCH__)
-	unsigned lane;
-	asm("mov.u32 %0, %%laneid;" : "=r"(lane));
-	const uint32_t le = 0xffffffffu >> (31 - lane);
-	const int32_t sc = score2 + __popc(H & le) + __popc(P2 & le);
-	const int32_t an = anti + __popc(A & le);
-	acc = __ballot_sync(0xffffffffu, ((H >> lane) & 1u) && sc >= thres2);
-	rej = __ballot_sync(0xffffffffu, ((A >> lane) & 1u) && an >= anti_thres);
-#else
-	acc = rej = 0;
-	for (unsigned lane = 0; lane < 32; ++lane) {
+	if (WARP) {
+		unsigned lane;
+		asm("mov.u32 %0, %%laneid;" : "=r"(lane));
 		const uint32_t le = 0xffffffffu >> (31 - lane);
-		const int32_t sc = score2 + popc32(H & le) + popc32(P2 & le);
-		const int32_t an = anti + popc32(A & le);
-		if (((H >> lane) & 1u) && sc >= thres2)
-			acc |= 1u << lane;
-		if (((A >> lane) & 1u) && an >= anti_thres)
-			rej |= 1u << lane;
+		const int32_t sc = score2 + __popc(H & le) + __popc(P2 & le);
+		const int32_t an = anti + __popc(A & le);
+		acc = __ballot_sync(0xffffffffu, ((H >> lane) & 1u) && sc >= thres2);
+		rej = __ballot_sync(0xffffffffu, ((A >> lane) & 1u) && an >= anti_thres);
+		return;
 	}
 #endif
+	/* one thread: running sums over the 32 frames */
+	acc = rej = 0;
+	int32_t sc = score2, an = anti;
+	for (unsigned j = 0; j < 32; ++j) {
+		const uint32_t h = (H >> j) & 1u, a = (A >> j) & 1u;
+		sc += (int32_t)(h + ((P2 >> j) & 1u));
+		an += (int32_t)a;
+		if (h && sc >= thres2)
+			acc |= 1u << j;
+		if (a && an >= anti_thres)
+			rej |= 1u << j;
+	}
 }
 
 /*
@@ -253,6 +259,7 @@ BBT_HD int simple_step_frames(const SimpleState &s)
  * algorithm probes (the ordinary frames up to the decision or the frame that
  * opens a skip window), for counting algorithmic probes.
  */
+template <bool WARP = true>
 BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int32_t base,
 		int nf, int k, int streak_thr, uint32_t *alg = nullptr)
 {
@@ -285,7 +292,8 @@ BBT_HD int simple_chunk(SimpleState &s, uint32_t V, uint32_t H, int32_t base,
 		const int32_t dA = popc32(A & pre);
 		if (s.score2 + dS >= s.thres2 || s.anti + dA >= s.anti_thres) {
 			uint32_t acc, rej;
-			crossing_masks(H, prevhit, A, pre, s.score2, s.anti, s.thres2, s.anti_thres, acc, rej);
+			crossing_masks<WARP>(H, prevhit, A, pre, s.score2, s.anti, s.thres2, s.anti_thres, acc,
+					rej);
 			const int ap = acc ? lowbit32(acc) : 32;
 			const int rp = rej ? lowbit32(rej) : 32;
 			if (ap < rp) {

@@ -55,6 +55,7 @@ extern "C" {
 #define BBT_PATH_PLAIN 1       /* one warp per read, one launch per batch */
 #define BBT_PATH_PERSISTENT 2  /* persistent work-stealing kernel, read-major */
 #define BBT_PATH_FILTER_MAJOR 3 /* persistent, (filter, read) items in filter order */
+#define BBT_PATH_BUCKETED 4    /* probes sorted by filter address (filters far above L2) */
 
 typedef struct bbt_ctx bbt_ctx;
 
@@ -307,6 +308,16 @@ int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int frames_per_l
  * not start last and hold the end of the launch); 0 = index order.  Results do
  * not depend on it.  No reference counterpart. */
 int bbt_set_schedule(bbt_ctx *ctx, uint64_t long_bases);
+
+/* Settings of the bucketed path (BBT_PATH_BUCKETED): each round's requests
+ * are resolved one bucket of 2^bucket_shift filter bits at a time (a bucket
+ * should fit L2: 28 = 32 MB); a read's frames are resolved in two phases split
+ * at phase_split / 16 of its frames (16 = one phase), the first covering at
+ * least min(frames, phase_min) frames; at most max_frames frames per
+ * sub-batch (scratch: about 6.3 bytes per frame).  0 keeps a setting.  Results
+ * do not depend on them.  No reference counterpart. */
+int bbt_set_bucketing(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
+		unsigned phase_min, uint64_t max_frames);
 
 /*
  * Autotuner: time every kernel configuration on a device-resident sample
