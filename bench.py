@@ -932,23 +932,39 @@ def run_single(args):
     plain_launches = 2 * ((n + PLAIN_BATCH - 1) // PLAIN_BATCH)
     plain_ok = bool(torch.equal(hits, want_hits))
 
-    # batched: autotuned configuration, launches captured in one CUDA graph
+    # batched: autotuned configuration; the plain and persistent paths run
+    # as one CUDA graph, the bucketed path (which plans its sub-batches on the
+    # host) as direct launches
     sample = min(n, 2_000_000)
     tune = bbc.autotune(d1, doff[:sample + 1])
     log(f"autotune: {tune}")
-    if tune["path"] == L.PATH_FILTER_MAJOR:  # not capturable; one filter never picks it
+    if tune["path"] == L.PATH_FILTER_MAJOR:  # one filter never picks it
         bbc.set_launch(path=L.PATH_PERSISTENT)
     bbc.classify_device(d1, doff, hits=hits, category=cat, stream=stream)  # warm-up, same sizes
     stream.synchronize()
     hits.zero_()
-    graph = bbc.graph(d1, doff, hits, category=cat, reads_per_launch=tune["reads_per_launch"])
+    graph = None
+    if tune["path"] == L.PATH_BUCKETED:
+        def batched_step():
+            bbc.classify_device(d1, doff, hits=hits, category=cat, stream=stream)
+    else:
+        graph = bbc.graph(d1, doff, hits, category=cat,
+                          reads_per_launch=tune["reads_per_launch"])
+
+        def batched_step():
+            graph.launch(stream)
     clocks = ClockSampler(local)
     clocks.start()
-    ms_batched = timed(lambda: graph.launch(stream))
+    ms_batched = timed(batched_step)
     clk = clocks.stop()
     batched_ok = bool(torch.equal(hits, want_hits))
-    kernels_per_launch = 3 if (tune["long_bases"] and tune["path"] != L.PATH_PLAIN) else 2
-    batched_launches = graph.launches * kernels_per_launch
+    if graph is not None:
+        kernels_per_launch = 3 if (tune["long_bases"] and tune["path"] != L.PATH_PLAIN) else 2
+        batched_launches = graph.launches * kernels_per_launch
+    else:
+        batched_step()
+        stream.synchronize()
+        batched_launches = bbc.last_stats()["kernels"]
 
     # kernel time of one launch of the whole batch in the tuned configuration
     bbc.classify_device(d1, doff, hits=hits, category=cat, stream=stream)
@@ -981,7 +997,8 @@ def run_single(args):
         e2e_s = float(t.item())
     e2e_ok = bool(torch.equal(hh, want_hits.cpu()))
     if rank != 0:
-        graph.close()
+        if graph is not None:
+            graph.close()
         bbc.close()
         if pg:
             pg.barrier()
@@ -1025,13 +1042,16 @@ def run_single(args):
                 "h2d_bytes_per_step": int(bases + (n + 1) * 8),
                 "d2h_bytes_per_step": int(n * (8 + 4)), "matches_device_results": e2e_ok},
         "gpu_launches": batched_launches * args.steps,
-        "graph_launches_per_step": 1,
+        "graph_launches_per_step": 1 if graph is not None else 0,
+        "batched_path": {L.PATH_PLAIN: "plain", L.PATH_PERSISTENT: "persistent",
+                         L.PATH_BUCKETED: "bucketed"}.get(tune["path"], str(tune["path"])),
         "clocks": clk,
         "parity_sample": parity,
         "batched_equals_reference_sample": (parity or {}).get("mismatched_reads") == 0,
     }
     print(json.dumps(line), flush=True)
-    graph.close()
+    if graph is not None:
+        graph.close()
     bbc.close()
     if pg:
         pg.barrier()

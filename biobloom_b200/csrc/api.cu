@@ -830,6 +830,10 @@ static int bk_tmp(bbt_ctx *ctx, size_t bytes)
 	return BBT_OK;
 }
 
+/* Staging slots of host batches on the bucketed path. */
+constexpr uint64_t kBkSlotBases = 2ull << 30;
+constexpr uint64_t kBkSlotReads = 8ull << 20;
+
 struct BkCut {
 	uint64_t r0, r1;  /* reads of the sub-batch */
 	uint64_t f0, f1;  /* their frames */
@@ -1292,6 +1296,24 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 	const uint64_t n = b->n_reads;
 	const bool packed = b->encoding == BBT_BASES_2BIT;
 	const bool want_scores = scores && (scores[0] || (paired && scores[1]));
+	if (ctx->lc.path == BBT_PATH_BUCKETED && !ctx->p.max_batch_bases &&
+			!ctx->p.max_batch_reads && ctx->cap_bases < kBkSlotBases && n > ctx->cap_reads) {
+		/* the bucketed path sweeps the filter once per round of a slot load:
+		 * large loads keep those sweeps few */
+		for (Slot &sl : ctx->slot)
+			if (sl.used)
+				CUDA_TRY(ctx, cudaEventSynchronize(sl.done));
+		CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+		ctx->cap_bases = kBkSlotBases;
+		ctx->cap_reads = kBkSlotReads;
+		for (Slot &sl : ctx->slot) {
+			flush_slot(sl);
+			sl.used = false;
+			int rc = alloc_slot(ctx, sl, ctx->cap_bases, ctx->cap_reads);
+			if (rc)
+				return rc;
+		}
+	}
 	if (want_scores) {
 		/* per-slot score arrays of cap_reads reads */
 		for (Slot &sl : ctx->slot) {

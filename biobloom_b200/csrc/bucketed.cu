@@ -113,12 +113,18 @@ __device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *
 		return;
 	const uint64_t x1 = min(x0 + kRun, b.T);
 	const unsigned k = b.f.k;
-	uint32_t vacc[kRun / 32], hacc[kRun / 32], touched[kRun / 32];
-	if (FIRST) {
-#pragma unroll
-		for (uint32_t w = 0; w < kRun / 32; ++w)
-			vacc[w] = hacc[w] = touched[w] = 0;
-	}
+	/* FIRST: the run's validity / hit bits, one word at a time (word cw of
+	 * the sub-batch), merged into the arrays when the run moves past it; the
+	 * run's words belong to this thread */
+	uint64_t cw = x0 >> 5;
+	uint32_t vacc = 0, hacc = 0, touched = 0;
+	auto flush = [&]() {
+		if (touched) {
+			b.vbits[cw] = (b.vbits[cw] & ~touched) | vacc;
+			b.hbits[cw] = (b.hbits[cw] & ~touched) | hacc;
+		}
+		vacc = hacc = touched = 0;
+	};
 	uint64_t r = bk_find_read(b, x0);
 	for (uint64_t x = x0; x < x1;) {
 		while (b.fo[r + 1] - b.fo0 <= x)
@@ -137,12 +143,15 @@ __device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *
 		const uint64_t i = r - (mate ? b.a.n : 0);
 		const uint64_t start = b.a.off[mate][i] - b.a.off_base[mate];
 		const Bases src = read_bases(b.a, mate, start);
+		BaseStream sin, sout; /* the base entering and the base leaving the k-mer */
+		sin.init(src);
+		sout.init(src);
 		/* ntHash of frame qa: forward and reverse-complement hashes over its k
 		 * bases, then rolled one base at a time (bbt_device.cuh) */
 		uint64_t fh = 0, rh = 0;
 		int64_t lb = -1; /* last base that is not ACGT, read coordinates */
 		for (unsigned j = 0; j < k; ++j) {
-			const uint8_t c = base_code_at(src, qa + j);
+			const uint8_t c = sin.code(qa + j);
 			fh = rol1(fh) ^ seed_fw_code(c);
 			rh ^= rolk(seed_rc_code(c), j);
 			if (c == 4)
@@ -150,8 +159,8 @@ __device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *
 		}
 		for (uint64_t q = qa; q < qb; ++q) {
 			if (q > qa) {
-				const uint8_t out = base_code_at(src, q - 1);
-				const uint8_t in = base_code_at(src, q + k - 1);
+				const uint8_t out = sout.code(q - 1);
+				const uint8_t in = sin.code(q + k - 1);
 				fh = rol1(fh) ^ rolk(seed_fw_code(out), k) ^ seed_fw_code(in);
 				rh = ror1(rh) ^ ror1(seed_rc_code(out)) ^ rolk(seed_rc_code(in), k - 1);
 				if (in == 4)
@@ -163,13 +172,16 @@ __device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *
 			if (FIRST) {
 				const bool valid = lb < (int64_t)q;
 				active = valid && !dust_low(b.a.dust[mate], start + q);
-				const uint32_t rel = (uint32_t)(xf - x0);
-				const uint32_t bit = 1u << (rel & 31u);
-				touched[rel >> 5] |= bit;
+				if ((xf >> 5) != cw) {
+					flush();
+					cw = xf >> 5;
+				}
+				const uint32_t bit = 1u << (uint32_t)(xf & 31u);
+				touched |= bit;
 				if (valid)
-					vacc[rel >> 5] |= bit;
+					vacc |= bit;
 				if (active)
-					hacc[rel >> 5] |= bit;
+					hacc |= bit;
 			} else {
 				active = (shb[fid >> 5] >> (fid & 31u)) & 1u;
 			}
@@ -180,17 +192,8 @@ __device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *
 			}
 		}
 	}
-	if (FIRST) {
-		/* the run's words belong to this thread: merge the phase's frames in */
-#pragma unroll
-		for (uint32_t w = 0; w < kRun / 32; ++w) {
-			if (!touched[w])
-				continue;
-			const uint64_t wi = (x0 >> 5) + w;
-			b.vbits[wi] = (b.vbits[wi] & ~touched[w]) | vacc[w];
-			b.hbits[wi] = (b.hbits[wi] & ~touched[w]) | hacc[w];
-		}
-	}
+	if (FIRST)
+		flush();
 }
 
 /* Load the hit bits of window block blk into shb. */
