@@ -143,6 +143,7 @@ def lib():
     sig = {
         "bbt_default_params": (None, [P(Params)]),
         "bbt_open": (i32, [P(cp), i32, P(Params), P(vp)]),
+        "bbt_open_devices": (i32, [P(cp), i32, P(Params), P(ctypes.c_int), i32, P(vp)]),
         "bbt_close": (i32, [vp]),
         "bbt_last_error": (cp, [vp]),
         "bbt_num_filters": (i32, [vp]),

@@ -33,9 +33,11 @@ class BioBloomClassifier:
     def __init__(self, filter_paths, score_threshold=None, prefix="", postfix="", *,
                  streak_threshold=3, device=0, path=L.PATH_AUTO, warps_per_block=0,
                  frames_per_lane=0, max_batch_reads=0, max_batch_bases=0, l2_fetch_bytes=0,
-                 score_type="simple"):
+                 score_type="simple", devices=None):
         """score_type: "simple", "harmonic" or "binomial" (-S); for binomial the
-        score is the -s value, the minimum -10*log10(FPR) of a match [100]."""
+        score is the -s value, the minimum -10*log10(FPR) of a match [100].
+        devices: a list of GPU ordinals to load the filters on (bbt_open_devices;
+        host batches and files are split across them); default: `device` alone."""
         lib = L.lib()
         p = L.Params()
         lib.bbt_default_params(ctypes.byref(p))
@@ -63,7 +65,12 @@ class BioBloomClassifier:
         paths = [str(x).encode() for x in filter_paths]
         arr = (ctypes.c_char_p * len(paths))(*paths)
         ctx = ctypes.c_void_p()
-        L.check(lib.bbt_open(arr, len(paths), ctypes.byref(p), ctypes.byref(ctx)))
+        if devices:
+            devs = (ctypes.c_int * len(devices))(*[int(d) for d in devices])
+            L.check(lib.bbt_open_devices(arr, len(paths), ctypes.byref(p), devs, len(devices),
+                                         ctypes.byref(ctx)))
+        else:
+            L.check(lib.bbt_open(arr, len(paths), ctypes.byref(p), ctypes.byref(ctx)))
         self._ctx = ctx
         self.params = p
         self.prefix = prefix

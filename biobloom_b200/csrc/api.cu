@@ -14,6 +14,7 @@
 #include <mutex>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "bbt.h"
@@ -152,6 +153,9 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 {
 	if (!ctx)
 		return BBT_OK;
+	for (bbt_ctx *peer : ctx->peers)
+		bbt_close(peer);
+	ctx->peers.clear();
 	cudaSetDevice(ctx->dev);
 	if (ctx->stream)
 		cudaStreamSynchronize(ctx->stream);
@@ -528,6 +532,38 @@ fail_out : {
 	return fail(nullptr, rc, m);
 }
 #undef OPEN_TRY
+}
+
+extern "C" int bbt_open_devices(const char *const *bf_paths, int n_filters,
+		const bbt_params *params, const int *devices, int n_devices, bbt_ctx **out)
+{
+	if (!out || !devices || n_devices < 1)
+		return fail(nullptr, BBT_ERR_ARG, "bbt_open_devices: need at least one device and an "
+				"out pointer");
+	*out = nullptr;
+	bbt_params p;
+	if (params)
+		p = *params;
+	else
+		bbt_default_params(&p);
+	bbt_ctx *first = nullptr;
+	p.device = devices[0];
+	int rc = bbt_open(bf_paths, n_filters, &p, &first);
+	if (rc)
+		return rc;
+	for (int i = 1; i < n_devices; ++i) {
+		bbt_ctx *peer = nullptr;
+		p.device = devices[i];
+		rc = bbt_open(bf_paths, n_filters, &p, &peer);
+		if (rc) {
+			std::string m = bbt_last_error(nullptr);
+			bbt_close(first);
+			return fail(nullptr, rc, "device " + std::to_string(devices[i]) + ": " + m);
+		}
+		first->peers.push_back(peer);
+	}
+	*out = first;
+	return BBT_OK;
 }
 
 extern "C" int bbt_num_filters(const bbt_ctx *ctx)
@@ -1524,6 +1560,56 @@ static int classify_host(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
 	return BBT_OK;
 }
 
+/* A host batch over this context's devices: contiguous shards of reads in
+ * proportion to the devices, classified concurrently (one host thread per
+ * replica), results written in place; each context adds its shard to its own
+ * summary counters, which bbt_summary adds up. */
+static int classify_host_devices(bbt_ctx *ctx, const bbt_batch *b, bbt_result *r,
+		double *const *scores)
+{
+	const size_t nd = ctx->peers.size() + 1;
+	const uint64_t n = b->n_reads;
+	std::vector<bbt_ctx *> c(nd);
+	c[0] = ctx;
+	for (size_t i = 1; i < nd; ++i)
+		c[i] = ctx->peers[i - 1];
+	std::vector<int> rcs(nd, BBT_OK);
+	auto shard = [&](size_t d) {
+		const uint64_t i0 = n * d / nd, i1 = n * (d + 1) / nd;
+		bbt_batch sb = *b;
+		sb.offsets = b->offsets + i0;
+		if (b->offsets2)
+			sb.offsets2 = b->offsets2 + i0;
+		sb.n_reads = i1 - i0;
+		bbt_result sr = *r;
+		if (r->hits)
+			sr.hits = r->hits + i0 * ctx->words;
+		if (r->hits2)
+			sr.hits2 = r->hits2 + i0 * ctx->words;
+		if (r->category)
+			sr.category = r->category + i0;
+		double *sc[2] = {nullptr, nullptr};
+		if (scores) {
+			sc[0] = scores[0] ? scores[0] + i0 * ctx->nf : nullptr;
+			sc[1] = scores[1] ? scores[1] + i0 * ctx->nf : nullptr;
+		}
+		cudaError_t e = cudaSetDevice(c[d]->dev);
+		rcs[d] = e != cudaSuccess ? cuda_fail(c[d], e, "cudaSetDevice")
+		                          : classify_host(c[d], &sb, &sr, scores ? sc : nullptr);
+	};
+	std::vector<std::thread> th;
+	for (size_t d = 1; d < nd; ++d)
+		th.emplace_back(shard, d);
+	shard(0);
+	for (std::thread &t : th)
+		t.join();
+	cudaSetDevice(ctx->dev);
+	for (size_t d = 0; d < nd; ++d)
+		if (rcs[d])
+			return d ? fail(ctx, rcs[d], c[d]->err) : rcs[d];
+	return BBT_OK;
+}
+
 static int classify_batch(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *result,
 		void *stream, double *const *scores, const char *who)
 {
@@ -1554,6 +1640,8 @@ static int classify_batch(bbt_ctx *ctx, const bbt_batch *batch, bbt_result *resu
 	}
 	if (batch->location != BBT_HOST)
 		return fail(ctx, BBT_ERR_ARG, std::string(who) + ": location must be BBT_HOST or BBT_DEVICE");
+	if (!ctx->peers.empty() && batch->n_reads >= 2 * (ctx->peers.size() + 1))
+		return classify_host_devices(ctx, batch, result, scores);
 	return classify_host(ctx, batch, result, scores);
 }
 
@@ -1572,7 +1660,7 @@ extern "C" int bbt_classify_batch_scores(bbt_ctx *ctx, const bbt_batch *batch,
 	return classify_batch(ctx, batch, result, stream, sc, "bbt_classify_batch_scores");
 }
 
-extern "C" int bbt_set_dust(bbt_ctx *ctx, int on, unsigned T, unsigned W)
+static int set_dust_one(bbt_ctx *ctx, int on, unsigned T, unsigned W)
 {
 	if (!ctx)
 		return BBT_ERR_ARG;
@@ -1610,7 +1698,16 @@ extern "C" int bbt_set_dust(bbt_ctx *ctx, int on, unsigned T, unsigned W)
 	return BBT_OK;
 }
 
-extern "C" int bbt_set_mode(bbt_ctx *ctx, int mode)
+extern "C" int bbt_set_dust(bbt_ctx *ctx, int on, unsigned T, unsigned W)
+{
+	int rc = set_dust_one(ctx, on, T, W);
+	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
+		if ((rc = set_dust_one(ctx->peers[i], on, T, W)) != BBT_OK)
+			fail(ctx, rc, ctx->peers[i]->err);
+	return rc;
+}
+
+static int set_mode_one(bbt_ctx *ctx, int mode)
 {
 	if (!ctx)
 		return BBT_ERR_ARG;
@@ -1620,10 +1717,24 @@ extern "C" int bbt_set_mode(bbt_ctx *ctx, int mode)
 	return BBT_OK;
 }
 
+extern "C" int bbt_set_mode(bbt_ctx *ctx, int mode)
+{
+	int rc = set_mode_one(ctx, mode);
+	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
+		if ((rc = set_mode_one(ctx->peers[i], mode)) != BBT_OK)
+			fail(ctx, rc, ctx->peers[i]->err);
+	return rc;
+}
+
 extern "C" int bbt_sync(bbt_ctx *ctx)
 {
 	if (!ctx)
 		return BBT_ERR_ARG;
+	for (bbt_ctx *peer : ctx->peers) {
+		int rc = bbt_sync(peer);
+		if (rc)
+			return fail(ctx, rc, peer->err);
+	}
 	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
 	CUDA_TRY(ctx, cudaDeviceSynchronize());
 	return BBT_OK;
@@ -1635,11 +1746,26 @@ extern "C" int bbt_summary(bbt_ctx *ctx, uint64_t *counts, uint64_t *reads)
 		return BBT_ERR_ARG;
 	CUDA_TRY(ctx, cudaSetDevice(ctx->dev));
 	CUDA_TRY(ctx, cudaDeviceSynchronize());
+	const size_t nc = 2 * (ctx->nf + 2) + 2;
 	if (counts)
-		CUDA_TRY(ctx, cudaMemcpy(counts, ctx->d_counts,
-				sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2), cudaMemcpyDeviceToHost));
+		CUDA_TRY(ctx, cudaMemcpy(counts, ctx->d_counts, sizeof(unsigned long long) * nc,
+				cudaMemcpyDeviceToHost));
 	if (reads)
 		*reads = ctx->reads_seen;
+	/* replicas on other devices: their counters add up (one host-side sum of
+	 * the (F + 2)-entry summaries) */
+	for (bbt_ctx *peer : ctx->peers) {
+		std::vector<uint64_t> pc(nc);
+		uint64_t pr = 0;
+		int rc = bbt_summary(peer, pc.data(), &pr);
+		if (rc)
+			return fail(ctx, rc, peer->err);
+		if (counts)
+			for (size_t i = 0; i < nc; ++i)
+				counts[i] += pc[i];
+		if (reads)
+			*reads += pr;
+	}
 	return BBT_OK;
 }
 
@@ -1652,6 +1778,11 @@ extern "C" int bbt_reset_summary(bbt_ctx *ctx)
 	CUDA_TRY(ctx, cudaMemset(ctx->d_counts, 0,
 			sizeof(unsigned long long) * (2 * (ctx->nf + 2) + 2)));
 	ctx->reads_seen = 0;
+	for (bbt_ctx *peer : ctx->peers) {
+		int rc = bbt_reset_summary(peer);
+		if (rc)
+			return fail(ctx, rc, peer->err);
+	}
 	return BBT_OK;
 }
 
@@ -1697,7 +1828,7 @@ extern "C" int bbt_last_stats(bbt_ctx *ctx, bbt_stats *out)
 	return BBT_OK;
 }
 
-extern "C" int bbt_set_inclusive(bbt_ctx *ctx, int inclusive)
+static int set_inclusive_one(bbt_ctx *ctx, int inclusive)
 {
 	if (!ctx)
 		return BBT_ERR_ARG;
@@ -1705,8 +1836,17 @@ extern "C" int bbt_set_inclusive(bbt_ctx *ctx, int inclusive)
 	return BBT_OK;
 }
 
+extern "C" int bbt_set_inclusive(bbt_ctx *ctx, int inclusive)
+{
+	int rc = set_inclusive_one(ctx, inclusive);
+	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
+		if ((rc = set_inclusive_one(ctx->peers[i], inclusive)) != BBT_OK)
+			fail(ctx, rc, ctx->peers[i]->err);
+	return rc;
+}
+
 /* Turn on probe/frame counting (diagnostics; adds atomics). */
-extern "C" int bbt_set_counting(bbt_ctx *ctx, int on)
+static int set_counting_one(bbt_ctx *ctx, int on)
 {
 	if (!ctx)
 		return BBT_ERR_ARG;
@@ -1716,8 +1856,17 @@ extern "C" int bbt_set_counting(bbt_ctx *ctx, int on)
 	return BBT_OK;
 }
 
+extern "C" int bbt_set_counting(bbt_ctx *ctx, int on)
+{
+	int rc = set_counting_one(ctx, on);
+	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
+		if ((rc = set_counting_one(ctx->peers[i], on)) != BBT_OK)
+			fail(ctx, rc, ctx->peers[i]->err);
+	return rc;
+}
+
 /* Change kernel path / launch shape after open (autotuner, bench). */
-extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int seg)
+static int set_launch_one(bbt_ctx *ctx, int path, int warps_per_block, int seg)
 {
 	if (!ctx)
 		return BBT_ERR_ARG;
@@ -1733,7 +1882,16 @@ extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int s
 	return BBT_OK;
 }
 
-extern "C" int bbt_set_bucketing(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
+extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int seg)
+{
+	int rc = set_launch_one(ctx, path, warps_per_block, seg);
+	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
+		if ((rc = set_launch_one(ctx->peers[i], path, warps_per_block, seg)) != BBT_OK)
+			fail(ctx, rc, ctx->peers[i]->err);
+	return rc;
+}
+
+static int set_bucketing_one(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
 		unsigned phase_min, uint64_t max_frames)
 {
 	if (!ctx)
@@ -1753,12 +1911,31 @@ extern "C" int bbt_set_bucketing(bbt_ctx *ctx, unsigned bucket_shift, unsigned p
 	return BBT_OK;
 }
 
-extern "C" int bbt_set_schedule(bbt_ctx *ctx, uint64_t long_bases)
+extern "C" int bbt_set_bucketing(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
+		unsigned phase_min, uint64_t max_frames)
+{
+	int rc = set_bucketing_one(ctx, bucket_shift, phase_split, phase_min, max_frames);
+	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
+		if ((rc = set_bucketing_one(ctx->peers[i], bucket_shift, phase_split, phase_min, max_frames)) != BBT_OK)
+			fail(ctx, rc, ctx->peers[i]->err);
+	return rc;
+}
+
+static int set_schedule_one(bbt_ctx *ctx, uint64_t long_bases)
 {
 	if (!ctx)
 		return BBT_ERR_ARG;
 	ctx->long_bases = long_bases;
 	return BBT_OK;
+}
+
+extern "C" int bbt_set_schedule(bbt_ctx *ctx, uint64_t long_bases)
+{
+	int rc = set_schedule_one(ctx, long_bases);
+	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
+		if ((rc = set_schedule_one(ctx->peers[i], long_bases)) != BBT_OK)
+			fail(ctx, rc, ctx->peers[i]->err);
+	return rc;
 }
 
 /* ---- autotuner ---- */

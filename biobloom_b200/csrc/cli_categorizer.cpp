@@ -65,6 +65,8 @@ static void usage_exit(int code)
 	        "  -I, --interval         Accepted for compatibility.\n"
 	        "      --read_status=F    Write one '<read>\\t<category>' line per read to F.\n"
 	        "      --device=N         CUDA device ordinal. [0]\n"
+	        "      --devices=LIST     Comma-separated CUDA device ordinals: the filters are\n"
+	        "                         loaded on each and the reads split across them.\n"
 	        "  -v, --version          Display version information.\n"
 	        "  -h, --help             Display this dialog.\n";
 	exit(code);
@@ -99,7 +101,8 @@ int main(int argc, char **argv)
 	unsigned dust_T = 20, dust_W = 64; /* Common/Options.cpp:36-38 */
 	int fastq = 0, fasta = 0, verbose = 0;
 	int device = 0;
-	enum { OPT_READ_STATUS = 1000, OPT_DEVICE };
+	vector<int> devices;
+	enum { OPT_READ_STATUS = 1000, OPT_DEVICE, OPT_DEVICES };
 	static struct option long_options[] = {
 		{"prefix", required_argument, NULL, 'p'},
 		{"filter_files", required_argument, NULL, 'f'},
@@ -129,6 +132,7 @@ int main(int argc, char **argv)
 		{"window_dust", required_argument, NULL, 'W'},
 		{"read_status", required_argument, NULL, OPT_READ_STATUS},
 		{"device", required_argument, NULL, OPT_DEVICE},
+		{"devices", required_argument, NULL, OPT_DEVICES},
 		{NULL, 0, NULL, 0}};
 	int c, idx = 0;
 	while ((c = getopt_long(argc, argv, "f:p:hegl:vs:r:t:cdiwI:nm:S:bDT:W:", long_options,
@@ -210,6 +214,14 @@ int main(int argc, char **argv)
 		case 'o': break; /* --min_hit_only: accepted and ignored, as upstream */
 		case OPT_READ_STATUS: read_status = optarg; break;
 		case OPT_DEVICE: device = atoi(optarg); break;
+		case OPT_DEVICES: {
+			stringstream ss(optarg);
+			string tok;
+			while (getline(ss, tok, ','))
+				if (!tok.empty())
+					devices.push_back(atoi(tok.c_str()));
+			break;
+		}
 		case '?': die = true; break;
 		default: break;
 		}
@@ -306,7 +318,11 @@ int main(int argc, char **argv)
 		cp.push_back(f.c_str());
 	cerr << "Starting to Load Filters." << endl;
 	bbt_ctx *ctx = nullptr;
-	if (bbt_open(cp.data(), (int)cp.size(), &p, &ctx) != BBT_OK) {
+	const int orc = devices.empty()
+			? bbt_open(cp.data(), (int)cp.size(), &p, &ctx)
+			: bbt_open_devices(cp.data(), (int)cp.size(), &p, devices.data(),
+					(int)devices.size(), &ctx);
+	if (orc != BBT_OK) {
 		cerr << "Error: " << bbt_last_error(nullptr) << endl;
 		exit(1);
 	}

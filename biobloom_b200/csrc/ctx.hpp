@@ -135,6 +135,9 @@ struct bbt_ctx {
 	uint32_t bk_bshift = 28;             /* bucket of 2^28 bits (32 MB) */
 	uint32_t bk_phase_split = 8;         /* phase boundary in sixteenths (16: one phase) */
 	uint32_t bk_phase_min = 64;          /* the first phase covers min(F, 64) frames or more */
+	/* bbt_open_devices: the same filters opened on the other devices; host
+	 * batches are split across this context and these */
+	std::vector<bbt_ctx *> peers;
 	cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
 	cudaEvent_t ev_k0 = nullptr, ev_k1 = nullptr; /* around the last classify kernel */
 	bbt::LaunchConfig lc;

@@ -96,6 +96,20 @@ int bbt_open(const char *const *bf_paths, int n_filters, const bbt_params *param
 int bbt_close(bbt_ctx *ctx);
 const char *bbt_last_error(const bbt_ctx *ctx);
 
+/*
+ * bbt_open on several GPUs: the filters are loaded on every device in
+ * `devices` (replicas; params->device is ignored).  Host batches
+ * (bbt_classify_batch with BBT_HOST buffers, and so the bbt_filter_* file
+ * pipeline and the CLI) are split into contiguous shards of reads, one per
+ * device, classified concurrently and written back in batch order; the
+ * summary counters of the devices are added up by bbt_summary.  Device
+ * batches run on the first device.  Setters apply to every device.  A device
+ * may be listed twice (two contexts on one GPU).  The reference's only
+ * parallelism is OpenMP threads (-t); this replaces it across GPUs.
+ */
+int bbt_open_devices(const char *const *bf_paths, int n_filters, const bbt_params *params,
+		const int *devices, int n_devices, bbt_ctx **out);
+
 int bbt_num_filters(const bbt_ctx *ctx);
 /* Filter id of filter i (BloomFilterInfo::getFilterID, BloomFilterInfo.cpp:141). */
 const char *bbt_filter_id(const bbt_ctx *ctx, int i);

@@ -139,3 +139,15 @@ def test_mibf_short_id_array(L, tmp_path):
 def test_mibf_missing_filter(L, tmp_path):
     rc, msg = _mibf_open(L, str(tmp_path / "none.bf"))
     assert rc == -2 and "cannot be opened" in msg
+
+
+def test_open_devices_arguments(L, tmp_path):
+    """bbt_open_devices checks its filters on the host first, like bbt_open,
+    and refuses an empty device list."""
+    p = _copy_filter(tmp_path)
+    arr = (ctypes.c_char_p * 1)(p.encode())
+    ctx = ctypes.c_void_p()
+    devs = (ctypes.c_int * 2)(0, 0)
+    assert L.lib().bbt_open_devices(arr, 1, None, devs, 0, ctypes.byref(ctx)) == -1
+    os.unlink(tmp_path / "x.txt")
+    assert L.lib().bbt_open_devices(arr, 1, None, devs, 2, ctypes.byref(ctx)) == -2
