@@ -28,6 +28,14 @@ public:
 			s.push_back(m_f.seeds[i]);
 		m_seedValues = parseSeedString(s);
 	}
+	/* an empty filter over a finished bit vector (MIBFConstructSupport::
+	 * getEmptyMIBF): takes the arrays, IDs all EMPTY */
+	MIBloomFilter(const oracle_mibf &f) : m_f(f) {
+		std::vector<std::string> s;
+		for (unsigned i = 0; i < m_f.nseeds; ++i)
+			s.push_back(m_f.seeds[i]);
+		m_seedValues = parseSeedString(s);
+	}
 	~MIBloomFilter() { oracle_mibf_free(&m_f); }
 	MIBloomFilter(const MIBloomFilter &) = delete;
 	MIBloomFilter &operator=(const MIBloomFilter &) = delete;
@@ -54,6 +62,31 @@ public:
 		return out;
 	}
 	size_t getPop() const { return m_f.pop; }
+	size_t getPopSaturated() const {
+		size_t n = 0;
+		for (uint64_t i = 0; i < m_f.pop; ++i)
+			n += (m_f.ids[i] & ORACLE_MIBF_SAT) ? 1 : 0;
+		return n;
+	}
+	/* slots owned per ID (saturated or not) */
+	void getIDCounts(std::vector<size_t> &counts) const {
+		for (uint64_t i = 0; i < m_f.pop; ++i) {
+			const unsigned id = m_f.ids[i] & 0x7FFFu;
+			if (id < counts.size())
+				++counts[id];
+		}
+	}
+	/* <prefix>.bf + <prefix>.sdsl from the path of the .bf */
+	void store(const std::string &bf_path) const {
+		std::string prefix = bf_path;
+		if (prefix.size() >= 3 && prefix.compare(prefix.size() - 3, 3, ".bf") == 0)
+			prefix.resize(prefix.size() - 3);
+		if (oracle_mibf_store(&m_f, prefix.c_str())) {
+			std::cerr << "MIBloomFilter: cannot store " << bf_path << std::endl;
+			exit(1);
+		}
+	}
+	oracle_mibf &rawMutable() { return m_f; }
 	size_t size() const { return m_f.m; }
 	const oracle_mibf &raw() const { return m_f; }
 private:

@@ -129,7 +129,7 @@ def test_scoring_methods(tmp_path, score_type, score, scoring):
         hits, _, _ = bbc.classify(reads)
     assert np.array_equal(hits, want)
     if scoring == ol.LENGTH:
-        w, _ = ol.classify(seq, off, filters, 40, 3)
+        w, _ = ol.classify(seq, off, filters, 40, 3, scoring=ol.LENGTH)
         assert np.array_equal(hits, w)
 
 
