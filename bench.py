@@ -936,7 +936,15 @@ def run_single(args):
     # as one CUDA graph, the bucketed path (which plans its sub-batches on the
     # host) as direct launches
     sample = min(n, 2_000_000)
-    tune = bbc.autotune(d1, doff[:sample + 1])
+    if args.path == "auto":
+        tune = bbc.autotune(d1, doff[:sample + 1])
+    else:  # a pinned path (the tuner's other choices at their defaults)
+        pinned = {"persistent": L.PATH_PERSISTENT, "bucketed": L.PATH_BUCKETED}[args.path]
+        bbc.set_launch(path=pinned, warps_per_block=8, frames_per_lane=4)
+        bbc.set_schedule(1024 if pinned == L.PATH_PERSISTENT else 0)
+        tune = {"path": pinned, "warps_per_block": 8, "frames_per_lane": 4,
+                "long_bases": 1024 if pinned == L.PATH_PERSISTENT else 0,
+                "reads_per_launch": 0, "reads_per_s": None, "pinned": True}
     log(f"autotune: {tune}")
     if tune["path"] == L.PATH_FILTER_MAJOR:  # one filter never picks it
         bbc.set_launch(path=L.PATH_PERSISTENT)
@@ -1653,6 +1661,8 @@ def main():
     ap.add_argument("--reads", type=int, default=None,
                     help="reads (--workload mibf / varlen / small; default: the workload's)")
     ap.add_argument("--layout", type=int, default=0, help="miBF layout: 0 auto, 1 rank, 2 dense")
+    ap.add_argument("--path", default="auto", choices=["auto", "persistent", "bucketed"],
+                    help="batched path of the single-filter workloads (default: autotuned)")
     args = ap.parse_args()
     args.reads_set = args.reads is not None
     if args.reads is None:

@@ -81,7 +81,13 @@ struct MibfArgs {
 	unsigned int *flags;
 	unsigned long long *stat;   /* frames visited, values probed, probes that hit */
 	uint32_t T;                 /* tally slots per warp, a multiple of 32 */
+	unsigned long long *gtally; /* more than kMibfSmemIds IDs: per-warp tally tables in
+	                               global memory (3 x T words each), zero between reads */
 };
+
+/* IDs a read may touch before a warp with global tally tables clears and scans
+ * every slot instead of its list. */
+constexpr uint32_t kTouchCap = 1024;
 
 struct LaneCounts {
 	unsigned long long frames = 0, probes = 0, hits = 0;
@@ -90,6 +96,13 @@ struct LaneCounts {
 __host__ __device__ inline size_t mibf_warp_bytes(uint32_t T)
 {
 	return 17 * 8 + 18 * 4 + (size_t)3 * T * 8; /* codes, invalid words, tally */
+}
+
+/* With the tally in global memory: codes, invalid words, the touched count and
+ * list. */
+__host__ __device__ inline size_t mibf_warp_bytes_big()
+{
+	return 17 * 8 + 18 * 4 + 4 + (size_t)kTouchCap * 4;
 }
 
 /* Seed tables: with BBT_MIBF_PAIR_TABLES (the default) one entry per pair of
@@ -102,9 +115,10 @@ constexpr int kTabEntries = BBT_MIBF_PAIR_TABLES ? 256 : 128; /* ulonglong2 per 
 constexpr int kQueryThreads = BBT_MIBF_PAIR_TABLES ? 256 : 128;
 constexpr int kQueryMinBlocks = BBT_MIBF_PAIR_TABLES ? 2 : 4;
 
-__host__ inline size_t mibf_smem_bytes(uint32_t nse, uint32_t T, int warps)
+__host__ inline size_t mibf_smem_bytes(uint32_t nse, uint32_t T, int warps, bool big)
 {
-	return (size_t)nse * kTabEntries * 16 + (size_t)warps * mibf_warp_bytes(T);
+	return (size_t)nse * kTabEntries * 16 +
+			(size_t)warps * (big ? mibf_warp_bytes_big() : mibf_warp_bytes(T));
 }
 
 __device__ __forceinline__ uint64_t spread_bits(uint32_t v)
@@ -282,7 +296,7 @@ __device__ __forceinline__ void probe_rank(const MibfArgs &a, bool ok, const uin
 template <int H>
 __device__ __forceinline__ void frame_tally(const MibfArgs &a, bool ok, const uint32_t *e,
 		const bool *hit, unsigned long long *TA, unsigned long long *TB, unsigned long long *TC,
-		uint32_t &satc, LaneCounts &lc, int lane)
+		uint32_t &satc, LaneCounts &lc, int lane, uint32_t *tlist)
 {
 	const uint32_t h = a.f.h, nids = a.f.nids, need = a.need;
 	bool anysat = false;
@@ -324,7 +338,14 @@ __device__ __forceinline__ void frame_tally(const MibfArgs &a, bool ok, const ui
 			const unsigned long long ic = nsh | ((unsigned long long)nsf << 32);
 			if (ia)
 				atomicAdd(TA + id, n * ia);
-			atomicAdd(TB + id, n * ib);
+			/* ib is never 0 (hits >= 1): the old value says whether this read
+			 * touched the ID before */
+			const unsigned long long old = atomicAdd(TB + id, n * ib);
+			if (tlist && old == 0) {
+				const uint32_t at = atomicAdd(tlist, 1u);
+				if (at < kTouchCap)
+					tlist[1 + at] = id;
+			}
 			if (ic)
 				atomicAdd(TC + id, n * ic);
 		}
@@ -337,7 +358,7 @@ template <int H, bool DENSE, int FPL>
 __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglong2 *tab,
 		uint64_t *cw, uint32_t *iw, unsigned long long *TA, unsigned long long *TB,
 		unsigned long long *TC, const uint8_t *__restrict__ s, uint64_t len, uint32_t &satc,
-		LaneCounts &lc, int lane)
+		LaneCounts &lc, int lane, uint32_t *tlist)
 {
 	const uint32_t k = a.f.k;
 	const uint64_t kmask = (k >= 64) ? ~0ull : ((1ull << k) - 1);
@@ -391,13 +412,19 @@ __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglon
 			}
 #pragma unroll
 			for (int f = 0; f < FPL; ++f)
-				frame_tally<H>(a, ok[f], e[f], hit[f], TA, TB, TC, satc, lc, lane);
+				frame_tally<H>(a, ok[f], e[f], hit[f], TA, TB, TC, satc, lc, lane, tlist);
 		}
 	}
 	__syncwarp();
 }
 
-template <int H, bool DENSE, int FPL>
+/*
+ * BIG (more than kMibfSmemIds IDs): each warp's tally table lives in global
+ * memory (a.gtally, zero between reads) and the warp lists the IDs the read
+ * touches (tlist in shared memory); candidates are looked for, and the table
+ * is cleared, over that list (over every slot when the list overflowed).
+ */
+template <int H, bool DENSE, int FPL, bool BIG>
 __global__ void __launch_bounds__(kQueryThreads, kQueryMinBlocks) mibf_query_kernel(MibfArgs a)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
@@ -406,13 +433,25 @@ __global__ void __launch_bounds__(kQueryThreads, kQueryMinBlocks) mibf_query_ker
 	unsigned long long *tabw = reinterpret_cast<unsigned long long *>(smem);
 	for (uint32_t i = threadIdx.x; i < nse * kTabEntries * 2; i += blockDim.x)
 		tabw[i] = a.tables[i];
-	unsigned char *wb = smem + (size_t)nse * kTabEntries * 16 + (size_t)wib * mibf_warp_bytes(T);
+	unsigned char *wb = smem + (size_t)nse * kTabEntries * 16 +
+			(size_t)wib * (BIG ? mibf_warp_bytes_big() : mibf_warp_bytes(T));
 	uint64_t *cw = reinterpret_cast<uint64_t *>(wb);
 	uint32_t *iw = reinterpret_cast<uint32_t *>(wb + 17 * 8);
-	unsigned long long *TA = reinterpret_cast<unsigned long long *>(wb + 17 * 8 + 18 * 4);
-	unsigned long long *TB = TA + T, *TC = TB + T;
-	for (uint32_t i = lane; i < 3 * T; i += 32)
-		TA[i] = 0;
+	unsigned long long *TA, *TB, *TC;
+	uint32_t *tlist = nullptr;
+	if (BIG) {
+		const uint64_t gw = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+		TA = a.gtally + gw * 3ull * T;
+		tlist = reinterpret_cast<uint32_t *>(wb + 17 * 8 + 18 * 4);
+		if (lane == 0)
+			tlist[0] = 0;
+	} else {
+		TA = reinterpret_cast<unsigned long long *>(wb + 17 * 8 + 18 * 4);
+		for (uint32_t i = lane; i < 3 * T; i += 32)
+			TA[i] = 0;
+	}
+	TB = TA + T;
+	TC = TB + T;
 	__syncthreads();
 	const ulonglong2 *tab = reinterpret_cast<const ulonglong2 *>(smem);
 	const uint32_t k = a.f.k;
@@ -439,26 +478,41 @@ __global__ void __launch_bounds__(kQueryThreads, kQueryMinBlocks) mibf_query_ker
 			uint32_t satc = 0;
 			if (fc) {
 				mibf_scan_mate<H, DENSE, FPL>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1,
-						satc, lc, lane);
+						satc, lc, lane, tlist);
 				if (a.seq2)
 					mibf_scan_mate<H, DENSE, FPL>(a, tab, cw, iw, TA, TB, TC, a.seq2 + b2,
-							len2, satc, lc, lane);
+							len2, satc, lc, lane, tlist);
 			}
+			__syncwarp();
+			/* the slots to look at: every slot, or the IDs the read touched */
+			const uint32_t touched = BIG ? tlist[0] : 0u;
+			const bool listed = BIG && touched <= kTouchCap;
+			const uint32_t nslots = listed ? touched : T;
+			auto slot_id = [&](uint32_t j) -> uint32_t { return listed ? tlist[1 + j] : j; };
+			const uint32_t *mrow = a.minc + (size_t)fc * nids;
+			auto significant = [&](uint32_t s) -> bool {
+				const unsigned long long A = TA[s];
+				const uint32_t cnt = (uint32_t)A, ns = (uint32_t)(A >> 32);
+				return s >= 1 && s < nids && cnt > 0 && cnt >= __ldg(mrow + s) &&
+						(a.min_nonsat == 0 || ns >= a.min_nonsat);
+			};
 			/* significant IDs */
 			uint32_t cmask = 0, maxns = 0;
 			Cand best = {0ull, 0ull};
 			if (fc) {
-				const uint32_t *mrow = a.minc + (size_t)fc * nids;
-				for (uint32_t j = 0; j < T / 32; ++j) {
-					const uint32_t s = lane + 32 * j;
-					const unsigned long long A = TA[s];
-					const uint32_t cnt = (uint32_t)A, ns = (uint32_t)(A >> 32);
-					if (s >= 1 && s < nids && cnt > 0 && cnt >= __ldg(mrow + s) &&
-							(a.min_nonsat == 0 || ns >= a.min_nonsat)) {
-						cmask |= 1u << j;
+				for (uint32_t j0 = 0; j0 < nslots; j0 += 32) {
+					const uint32_t j = j0 + lane;
+					if (j >= nslots)
+						continue;
+					const uint32_t s = slot_id(j);
+					if (significant(s)) {
+						if (!BIG)
+							cmask |= 1u << (j0 >> 5);
+						const unsigned long long A = TA[s];
 						Cand c = {cand_k1(A), ((TB[s] >> 32) << 32) | (0xFFFFFFFFull - s)};
 						if (cand_less(best, c))
 							best = c;
+						const uint32_t ns = (uint32_t)(A >> 32);
 						maxns = ns > maxns ? ns : maxns;
 					}
 				}
@@ -489,10 +543,15 @@ __global__ void __launch_bounds__(kQueryThreads, kQueryMinBlocks) mibf_query_ker
 					++n_out;
 					/* next: the best candidate below cur that passes the threshold */
 					Cand nx = {0ull, 0ull};
-					for (uint32_t j = 0; j < T / 32; ++j) {
-						if (!((cmask >> j) & 1u))
+					for (uint32_t j0 = 0; j0 < nslots; j0 += 32) {
+						if (!BIG && !((cmask >> (j0 >> 5)) & 1u))
 							continue;
-						const uint32_t s = lane + 32 * j;
+						const uint32_t j = j0 + lane;
+						if (j >= nslots)
+							continue;
+						const uint32_t s = slot_id(j);
+						if (BIG && !significant(s))
+							continue;
 						const unsigned long long A = TA[s];
 						Cand c = {cand_k1(A), ((TB[s] >> 32) << 32) | (0xFFFFFFFFull - s)};
 						if (cand_less(c, cur) && (double)(uint32_t)A > thr && cand_less(nx, c))
@@ -519,12 +578,15 @@ __global__ void __launch_bounds__(kQueryThreads, kQueryMinBlocks) mibf_query_ker
 				}
 			}
 			__syncwarp();
-			for (uint32_t j = 0; j < T / 32; ++j) {
-				const uint32_t s = lane + 32 * j;
+			for (uint32_t j = lane; j < nslots; j += 32) {
+				const uint32_t s = slot_id(j);
 				TA[s] = 0;
 				TB[s] = 0;
 				TC[s] = 0;
 			}
+			__syncwarp();
+			if (BIG && lane == 0)
+				tlist[0] = 0;
 			__syncwarp();
 		}
 	}
@@ -671,64 +733,71 @@ struct Fpl {
 	static constexpr int value = (D && H <= 4) ? BBT_MIBF_FPL : 1;
 };
 
-template <int H, bool D>
+template <int H, bool D, bool B>
 static cudaError_t launch_h(const MibfArgs &a, int grid, size_t smem, cudaStream_t s)
 {
-	mibf_query_kernel<H, D, Fpl<H, D>::value><<<grid, kQueryThreads, smem, s>>>(a);
+	mibf_query_kernel<H, D, Fpl<H, D>::value, B><<<grid, kQueryThreads, smem, s>>>(a);
 	return cudaGetLastError();
 }
 
 /* Blocks per SM of a variant with smem bytes of shared memory (also sets the
  * variant's shared-memory limit, which must precede its launch). */
-template <int H, bool D>
+template <int H, bool D, bool B>
 static int occupancy_h(size_t smem)
 {
-	auto kern = mibf_query_kernel<H, D, Fpl<H, D>::value>;
+	auto kern = mibf_query_kernel<H, D, Fpl<H, D>::value, B>;
 	cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 	int nb = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kQueryThreads, smem);
 	return nb > 0 ? nb : 1;
 }
 
-template <bool D>
-static cudaError_t launch_query_d(const MibfArgs &a, int hsel, int grid, size_t smem,
+template <bool D, bool B>
+static cudaError_t launch_query_db(const MibfArgs &a, int hsel, int grid, size_t smem,
 		cudaStream_t s)
 {
 	switch (hsel) {
-	case 1: return launch_h<1, D>(a, grid, smem, s);
-	case 2: return launch_h<2, D>(a, grid, smem, s);
-	case 3: return launch_h<3, D>(a, grid, smem, s);
-	case 4: return launch_h<4, D>(a, grid, smem, s);
-	case 6: return launch_h<6, D>(a, grid, smem, s);
-	case 8: return launch_h<8, D>(a, grid, smem, s);
-	default: return launch_h<16, D>(a, grid, smem, s);
+	case 1: return launch_h<1, D, B>(a, grid, smem, s);
+	case 2: return launch_h<2, D, B>(a, grid, smem, s);
+	case 3: return launch_h<3, D, B>(a, grid, smem, s);
+	case 4: return launch_h<4, D, B>(a, grid, smem, s);
+	case 6: return launch_h<6, D, B>(a, grid, smem, s);
+	case 8: return launch_h<8, D, B>(a, grid, smem, s);
+	default: return launch_h<16, D, B>(a, grid, smem, s);
 	}
 }
 
-template <bool D>
-static int query_occupancy_d(int hsel, size_t smem)
+template <bool D, bool B>
+static int query_occupancy_db(int hsel, size_t smem)
 {
 	switch (hsel) {
-	case 1: return occupancy_h<1, D>(smem);
-	case 2: return occupancy_h<2, D>(smem);
-	case 3: return occupancy_h<3, D>(smem);
-	case 4: return occupancy_h<4, D>(smem);
-	case 6: return occupancy_h<6, D>(smem);
-	case 8: return occupancy_h<8, D>(smem);
-	default: return occupancy_h<16, D>(smem);
+	case 1: return occupancy_h<1, D, B>(smem);
+	case 2: return occupancy_h<2, D, B>(smem);
+	case 3: return occupancy_h<3, D, B>(smem);
+	case 4: return occupancy_h<4, D, B>(smem);
+	case 6: return occupancy_h<6, D, B>(smem);
+	case 8: return occupancy_h<8, D, B>(smem);
+	default: return occupancy_h<16, D, B>(smem);
 	}
 }
 
-static cudaError_t launch_query(const MibfArgs &a, bool dense, int hsel, int grid, size_t smem,
-		cudaStream_t s)
+static cudaError_t launch_query(const MibfArgs &a, bool dense, bool big, int hsel, int grid,
+		size_t smem, cudaStream_t s)
 {
-	return dense ? launch_query_d<true>(a, hsel, grid, smem, s)
-	             : launch_query_d<false>(a, hsel, grid, smem, s);
+	if (big)
+		return dense ? launch_query_db<true, true>(a, hsel, grid, smem, s)
+		             : launch_query_db<false, true>(a, hsel, grid, smem, s);
+	return dense ? launch_query_db<true, false>(a, hsel, grid, smem, s)
+	             : launch_query_db<false, false>(a, hsel, grid, smem, s);
 }
 
-static int query_occupancy(bool dense, int hsel, size_t smem)
+static int query_occupancy(bool dense, bool big, int hsel, size_t smem)
 {
-	return dense ? query_occupancy_d<true>(hsel, smem) : query_occupancy_d<false>(hsel, smem);
+	if (big)
+		return dense ? query_occupancy_db<true, true>(hsel, smem)
+		             : query_occupancy_db<false, true>(hsel, smem);
+	return dense ? query_occupancy_db<true, false>(hsel, smem)
+	             : query_occupancy_db<false, false>(hsel, smem);
 }
 
 /* Exclusive scan of n 64-bit counts into out (cub). */
@@ -857,6 +926,29 @@ static int load_device(bbt_mibf *ctx, const std::string &sdsl, const std::vector
 	return rc;
 }
 
+/* Zeroed per-warp tally tables for a query grid of num_sms x
+ * kMibfBigBlocksPerSm blocks (contexts with more than kMibfSmemIds IDs). */
+static int alloc_gtally(bbt_mibf *ctx, unsigned long long **p, uint64_t *warps)
+{
+	const uint64_t T = tally_slots((uint32_t)ctx->names.size());
+	const uint64_t w = (uint64_t)ctx->num_sms * kMibfBigBlocksPerSm * (kQueryThreads / 32);
+	const size_t bytes = w * 3 * T * sizeof(unsigned long long);
+	if (cudaMalloc(p, bytes) != cudaSuccess) {
+		*p = nullptr;
+		return mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(per-warp tally tables, " +
+				std::to_string(bytes >> 20) + " MB)");
+	}
+	if (cudaMemset(*p, 0, bytes) != cudaSuccess)
+		return mibf_fail(ctx, BBT_ERR_CUDA, "cudaMemset(per-warp tally tables)");
+	*warps = w;
+	return BBT_OK;
+}
+
+static bool big_ids(const bbt_mibf *ctx)
+{
+	return ctx->names.size() > kMibfSmemIds;
+}
+
 extern "C" int bbt_mibf_close(bbt_mibf *ctx)
 {
 	if (!ctx)
@@ -872,6 +964,7 @@ extern "C" int bbt_mibf_close(bbt_mibf *ctx)
 		cudaFree(ctx->d_work);
 		cudaFree(ctx->d_flags);
 		cudaFree(ctx->d_stat);
+		cudaFree(ctx->d_gtally);
 		cudaFree(ctx->d_minc);
 		cudaFree(ctx->d_fcmax);
 		cudaFree(ctx->d_hits);
@@ -970,6 +1063,8 @@ extern "C" int bbt_mibf_open(const char *bf_path, const bbt_mibf_params *params,
 		return bail(mibf_fail(ctx, BBT_ERR_NOMEM, "cudaMalloc(context)"));
 	cudaMemcpy(ctx->d_tables, tabs.data(), tabs.size() * 8, cudaMemcpyHostToDevice);
 	cudaMemset(ctx->d_counts, 0, 2 * nc * 8);
+	if (big_ids(ctx) && (rc = alloc_gtally(ctx, &ctx->d_gtally, &ctx->gtally_warps)) != BBT_OK)
+		return bail(rc);
 	if (cudaDeviceSynchronize() != cudaSuccess)
 		return bail(mibf_fail(ctx, BBT_ERR_CUDA, "loading the miBF failed"));
 	*out = ctx;
@@ -1154,10 +1249,17 @@ static int run_query_sc(bbt_mibf *ctx, uint64_t n_reads, const uint8_t *seq, con
 	a.flags = sc.flags;
 	a.stat = sc.stat;
 	a.T = tally_slots(nids);
+	const bool big = big_ids(ctx);
+	a.gtally = big ? sc.gtally : nullptr;
 	const int hsel = pick_h(ctx->hd.h);
-	const size_t smem = mibf_smem_bytes(a.f.nse, a.T, kQueryThreads / 32);
+	const size_t smem = mibf_smem_bytes(a.f.nse, a.T, kQueryThreads / 32, big);
 	const bool dense = ctx->d_dense != nullptr;
-	const int grid = ctx->num_sms * query_occupancy(dense, hsel, smem);
+	int per_sm = query_occupancy(dense, big, hsel, smem);
+	if (big)
+		per_sm = std::min(per_sm, kMibfBigBlocksPerSm);
+	const int grid = ctx->num_sms * per_sm;
+	if (big && (!sc.gtally || (uint64_t)grid * (kQueryThreads / 32) > sc.gtally_warps))
+		return mibf_fail(ctx, BBT_ERR_ARG, "the per-warp tally tables are missing or too small");
 	if (phase & kQueryBegin) {
 		MIBF_TRY(ctx, cudaMemsetAsync(batch_counts, 0, nc * 8, s));
 		MIBF_TRY(ctx, cudaMemsetAsync(sc.flags, 0, 4, s));
@@ -1167,7 +1269,7 @@ static int run_query_sc(bbt_mibf *ctx, uint64_t n_reads, const uint8_t *seq, con
 	}
 	MIBF_TRY(ctx, cudaMemsetAsync(sc.work, 0, 8, s));
 	if (n_reads)
-		MIBF_TRY(ctx, launch_query(a, dense, hsel, grid, smem, s));
+		MIBF_TRY(ctx, launch_query(a, dense, big, hsel, grid, smem, s));
 	if (phase & kQueryEnd) {
 		if (timed)
 			MIBF_TRY(ctx, cudaEventRecord(ctx->ev1, s));
@@ -1186,6 +1288,8 @@ static MibfScratch ctx_scratch(bbt_mibf *ctx)
 	sc.counts = ctx->d_counts + counts_len(ctx) + 1;
 	sc.stat = ctx->d_stat;
 	sc.flags = ctx->d_flags;
+	sc.gtally = ctx->d_gtally;
+	sc.gtally_warps = ctx->gtally_warps;
 	return sc;
 }
 
@@ -1204,6 +1308,8 @@ int bbt::mibf_scratch_init(bbt_mibf *ctx, MibfScratch &sc)
 	MIBF_TRY(ctx, cudaMalloc(&sc.counts, counts_len(ctx) * 8));
 	MIBF_TRY(ctx, cudaMalloc(&sc.stat, 3 * 8));
 	MIBF_TRY(ctx, cudaMalloc(&sc.flags, 4));
+	if (big_ids(ctx))
+		return alloc_gtally(ctx, &sc.gtally, &sc.gtally_warps);
 	return BBT_OK;
 }
 
@@ -1213,6 +1319,9 @@ void bbt::mibf_scratch_free(MibfScratch &sc)
 	cudaFree(sc.counts);
 	cudaFree(sc.stat);
 	cudaFree(sc.flags);
+	cudaFree(sc.gtally);
+	sc.gtally = nullptr;
+	sc.gtally_warps = 0;
 	sc = MibfScratch();
 }
 

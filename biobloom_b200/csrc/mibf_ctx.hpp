@@ -19,7 +19,15 @@ namespace bbt {
 
 constexpr unsigned kMibfMaxSeeds = 16;
 constexpr unsigned kMibfMaxK = 32;
-constexpr unsigned kMibfMaxIds = 1024;   /* per-read tally table of the query kernel */
+/* IDs (target names + the empty ID 0): up to kMibfSmemIds the query kernel
+ * tallies a read in shared memory, above it in per-warp tables in global
+ * memory; IDs are 15-bit (the top bit of a slot is the saturation flag), as
+ * in the reference (BioBloomMaker/MIBFGen.hpp:112-118). */
+constexpr unsigned kMibfSmemIds = 1024;
+constexpr unsigned kMibfMaxIds = 32768;
+/* resident blocks per SM of the query kernel with global tally tables (each
+ * warp owns a 24 * num_ids byte table) */
+constexpr int kMibfBigBlocksPerSm = 2;
 constexpr uint16_t kMibfSat = 0x8000u;
 
 /* Header of a "<p>.bf" miBF file. */
@@ -91,6 +99,8 @@ struct bbt_mibf {
 	unsigned long long *d_work = nullptr;
 	unsigned int *d_flags = nullptr;       /* [0] result overflow */
 	unsigned long long *d_stat = nullptr;  /* frames, probes, hits of the last batch */
+	unsigned long long *d_gtally = nullptr; /* more than kMibfSmemIds IDs: per-warp tallies */
+	uint64_t gtally_warps = 0;
 	/* minCount rows, frame count -> num_ids entries; host copy and device copy */
 	std::mutex mc_mu;
 	std::vector<uint32_t> h_minc;
@@ -124,6 +134,8 @@ struct MibfScratch {
 	unsigned long long *counts = nullptr; /* a batch's summary counters */
 	unsigned long long *stat = nullptr;
 	unsigned int *flags = nullptr;
+	unsigned long long *gtally = nullptr;  /* per-warp tally tables (many IDs) */
+	uint64_t gtally_warps = 0;
 };
 int mibf_scratch_init(bbt_mibf *ctx, MibfScratch &sc);
 void mibf_scratch_free(MibfScratch &sc);

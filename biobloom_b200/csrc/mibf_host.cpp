@@ -348,7 +348,8 @@ int bbt::mibf_load_host(bbt_mibf *ctx, const char *bf_path, std::vector<uint16_t
 	}
 	if (ctx->names.size() > kMibfMaxIds) {
 		fclose(f);
-		return mibf_fail(ctx, BBT_ERR_UNSUPPORTED, "more than 1023 targets in " + idp);
+		return mibf_fail(ctx, BBT_ERR_UNSUPPORTED, "more than " + std::to_string(kMibfMaxIds - 1) +
+				" targets in " + idp + " (IDs are 15-bit)");
 	}
 	const unsigned nids = (unsigned)ctx->names.size();
 	std::vector<uint64_t> owned(nids, 0);

@@ -332,3 +332,60 @@ def test_host_batch_in_chunks_matches_one_device_launch(built, paired):
     assert reads_b == reads_a and np.array_equal(counts_b, counts_a)
     a.close()
     d.close()
+
+
+@pytest.fixture(scope="module")
+def many_targets(tmp_path_factory):
+    """A 5000-target miBF (IDs up to 5000, above the shared-memory tally's
+    1023): 5000 seeded 400 bp targets, every fourth sharing a block with the
+    one before, built by the oracle."""
+    rng = np.random.default_rng(77)
+    targets = [_genome(rng, 400, float(rng.uniform(0.35, 0.65))) for _ in range(5000)]
+    for i in range(1, 5000, 4):
+        targets[i][100:220] = targets[i - 1][50:170]
+    targets = [t.tobytes() for t in targets]
+    d = tmp_path_factory.mktemp("mibf5k")
+    names = [f"t{i + 1}" for i in range(len(targets))]
+    seeds = ["1111011101110010111011111", "1101111101001011111011011",
+             "1111101011100111010111111"]
+    f = oracle_lib.MIBF.build(targets, list(range(1, len(targets) + 1)), seeds=seeds, k=25,
+                              h=3, occupancy=0.5)
+    f.store(str(d / "big"))
+    with open(d / "big_ids.txt", "w") as fh:
+        for i, n in enumerate(names):
+            fh.write(f"{i + 1}\t{n}\n")
+    return targets, str(d / "big.bf"), f, names
+
+
+@pytest.mark.parametrize("layout", [1, 2])
+@pytest.mark.parametrize("oi", [0, 1, 2])
+def test_five_thousand_targets_match_oracle(many_targets, layout, oi):
+    """More IDs than the shared-memory tally holds: per-warp tally tables in
+    global memory, cleared over the IDs a read touched (or all of them after
+    a long read touched more than the list holds)."""
+    from biobloom_b200.mibf import MIBFClassifier
+    targets, path, f, names = many_targets
+    o = _opts(OPTS[oi])
+    rng = np.random.default_rng(300 + oi)
+    reads = []
+    for _ in range(1500):  # 150 bp: one minCount row for all of them
+        t = int(rng.integers(0, len(targets)))
+        st = int(rng.integers(0, 250))
+        a = np.frombuffer(targets[t][st:st + 150], dtype=np.uint8).copy()
+        m = rng.random(150) < 0.01
+        a[m] = BASES[rng.integers(0, 4, int(m.sum()))]
+        reads.append(a.tobytes() if rng.random() < 0.9 else BASES[rng.integers(0, 4, 150)].tobytes())
+    reads += [BASES[rng.integers(0, 4, 9000)].tobytes()]          # touches thousands of IDs
+    reads += [b"".join(targets[i] for i in range(40, 70))]      # 30 targets in one read
+    want = _oracle_query(f, names, reads, None, o)
+    mc = MIBFClassifier(path, score=o["score"], frame_matches=o["frame_matches"],
+                        multi=o["multi"], min_nonsat=o["min_nonsat"], best_hit_agree=o["best"],
+                        layout=layout)
+    assert mc.num_ids == 5001
+    got, sat = mc.classify(reads, None, max_hits=4)
+    for i, (res, s) in enumerate(want):
+        assert (got[i], int(sat[i])) == (res, s), i
+    assert any(len(r) for r, _ in want[:1500])
+    counts, n = mc.summary()
+    assert n == len(reads)
+    mc.close()
