@@ -189,6 +189,7 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 	cudaFree(ctx->d_bk_fo);
 	cudaFree(ctx->d_bk_state);
 	cudaFreeHost(ctx->h_bk_samples);
+	cudaFree(ctx->d_bk_samples);
 	cudaFree(ctx->d_bk_vbits);
 	cudaFree(ctx->d_bk_hbits);
 	cudaFree(ctx->d_bk_off);
@@ -887,15 +888,21 @@ static int bk_plan(bbt_ctx *ctx, const uint64_t *fo, uint64_t total, uint64_t mo
 	const uint64_t ns = total / S + 1;
 	if (ns + 1 > ctx->bk_samples_cap) {
 		cudaFreeHost(ctx->h_bk_samples);
+		cudaFree(ctx->d_bk_samples);
 		ctx->h_bk_samples = nullptr;
+		ctx->d_bk_samples = nullptr;
 		ctx->bk_samples_cap = 0;
 		CUDA_TRY(ctx, cudaMallocHost(&ctx->h_bk_samples, (ns + 1) * sizeof(uint64_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_samples, (ns + 1) * sizeof(uint64_t)));
 		ctx->bk_samples_cap = ns + 1;
 	}
 	uint64_t *h = ctx->h_bk_samples;
-	CUDA_TRY(ctx, cudaMemcpy2DAsync(h, sizeof(uint64_t), fo, S * sizeof(uint64_t),
-			sizeof(uint64_t), ns, cudaMemcpyDeviceToHost, s));
-	CUDA_TRY(ctx, cudaMemcpyAsync(h + ns, fo + total, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+	/* fo[0], fo[S], fo[2S], ..., then fo[total]: gathered on the device, one copy */
+	CUDA_TRY(ctx, launch_bk_samples(fo, total, S, ctx->d_bk_samples, ns, ctx->num_sms, s));
+	CUDA_TRY(ctx, launch_bk_samples(fo + total, 0, 0, ctx->d_bk_samples + ns, 1, ctx->num_sms,
+			s));
+	CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->d_bk_samples, (ns + 1) * sizeof(uint64_t),
+			cudaMemcpyDeviceToHost, s));
 	CUDA_TRY(ctx, cudaStreamSynchronize(s));
 	std::vector<uint64_t> pt(ns + 1), fv(ns + 1);
 	for (uint64_t j = 0; j < ns; ++j) {

@@ -96,6 +96,94 @@ __device__ __forceinline__ uint32_t bits_at(const uint32_t *w, uint64_t x)
 	return s ? (lo >> s) | (w[i + 1] << (32u - s)) : lo;
 }
 
+/* ntHash rolling tables of one k, indexed by (code of the base leaving the
+ * k-mer) << 3 | (code of the base entering it), codes 0..3 for ACGT and 4 for
+ * any other base (whose seed is 0):
+ *   tf[o, i] = rol(seed_fw(o), k) ^ seed_fw(i)
+ *   tr[o, i] = ror(seed_rc(o), 1) ^ rol(seed_rc(i), k - 1)
+ * so that a step is fh = rol(fh, 1) ^ tf, rh = ror(rh, 1) ^ tr; rc[c] is the
+ * plain reverse-complement seed (the first k-mer of a piece). */
+struct RollTables {
+	uint64_t tf[64];
+	uint64_t tr[64];
+	uint64_t rc[8];
+};
+
+__device__ void bk_set_tables(RollTables &t, unsigned k)
+{
+	for (int e = threadIdx.x; e < 64; e += blockDim.x) {
+		const uint8_t o = (uint8_t)(e >> 3), i = (uint8_t)(e & 7);
+		t.tf[e] = rolk(seed_fw_code(o), k) ^ seed_fw_code(i);
+		t.tr[e] = ror1(seed_rc_code(o)) ^ rolk(seed_rc_code(i), k - 1);
+		if (e < 8)
+			t.rc[e] = seed_rc_code((uint8_t)e);
+	}
+}
+
+/* Sequential 3-bit base codes (0..3 ACGT, 4 other) of one read for one
+ * thread, fetched 16 bases per load: the aligned 16-byte block of ASCII bases
+ * holding the base (bytes turned into codes and validity bits four at a time),
+ * or the 2-bit code word and its validity bits.  Calls ask for non-decreasing
+ * j.  (An aligned 16-byte block never crosses a page, so reading all of the
+ * block that holds a valid base stays inside mapped memory.) */
+struct CodeStream {
+	Bases src;
+	uint64_t blk;
+	uint32_t codes; /* 2 bits per base of the block */
+	uint32_t bad;   /* 1 bit per base of the block: not ACGT */
+
+	__device__ __forceinline__ void init(const Bases &s)
+	{
+		src = s;
+		blk = ~0ull;
+	}
+
+	/* four ASCII bytes: their 2-bit codes (A0 C1 G2 T3 by bits 1-2 of the
+	 * byte) in bits 0-7 and a validity nibble */
+	__device__ __forceinline__ static void ascii4(uint32_t w, uint32_t &c8, uint32_t &ok4)
+	{
+		const uint32_t t = ((w >> 1) & 0x03030303u) ^ ((w >> 2) & 0x01010101u);
+		c8 = (t & 3u) | ((t >> 6) & 0xCu) | ((t >> 12) & 0x30u) | ((t >> 18) & 0xC0u);
+		const uint32_t u = w & 0xDFDFDFDFu;
+		const uint32_t v = __vcmpeq4(u, 0x41414141u) | __vcmpeq4(u, 0x43434343u) |
+				__vcmpeq4(u, 0x47474747u) | __vcmpeq4(u, 0x54545454u);
+		ok4 = ((v >> 7) & 1u) | ((v >> 14) & 2u) | ((v >> 21) & 4u) | ((v >> 28) & 8u);
+	}
+
+	__device__ __forceinline__ uint32_t code(uint64_t j)
+	{
+		const uint64_t g = src.g0 + j;
+		uint32_t o;
+		if (src.ascii) {
+			const uintptr_t p = reinterpret_cast<uintptr_t>(src.ascii + g);
+			const uint64_t bk = p >> 4;
+			if (bk != blk) {
+				blk = bk;
+				const uint4 q = __ldg(reinterpret_cast<const uint4 *>(bk << 4));
+				uint32_t c0, c1, c2, c3, k0, k1, k2, k3;
+				ascii4(q.x, c0, k0);
+				ascii4(q.y, c1, k1);
+				ascii4(q.z, c2, k2);
+				ascii4(q.w, c3, k3);
+				codes = c0 | (c1 << 8) | (c2 << 16) | (c3 << 24);
+				bad = ~(k0 | (k1 << 4) | (k2 << 8) | (k3 << 12)) & 0xFFFFu;
+			}
+			o = (uint32_t)(p & 15u);
+		} else {
+			const uint64_t bk = g >> 4;
+			if (bk != blk) {
+				blk = bk;
+				codes = __ldg(src.words + bk);
+				bad = src.valid ? (~(__ldg(src.valid + (g >> 5)) >> (16u * (uint32_t)(bk & 1u))) &
+				                   0xFFFFu)
+				                : 0u;
+			}
+			o = (uint32_t)(g & 15u);
+		}
+		return ((bad >> o) & 1u) ? 4u : ((codes >> (2u * o)) & 3u);
+	}
+};
+
 /*
  * One thread's run of frames [x0, x0 + kRun) of window block blk: for every
  * frame of an open read inside the current phase, FIRST computes its validity
@@ -105,7 +193,8 @@ __device__ __forceinline__ uint32_t bits_at(const uint32_t *w, uint64_t x)
  * round's level selects and the frame's id in the block.
  */
 template <bool FIRST, class Op>
-__device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *shb, Op op)
+__device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *shb,
+		const RollTables &tab, Op op)
 {
 	const uint64_t w0 = (uint64_t)blk * kBkWinFrames;
 	const uint64_t x0 = w0 + (uint64_t)threadIdx.x * kRun;
@@ -143,26 +232,26 @@ __device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *
 		const uint64_t i = r - (mate ? b.a.n : 0);
 		const uint64_t start = b.a.off[mate][i] - b.a.off_base[mate];
 		const Bases src = read_bases(b.a, mate, start);
-		BaseStream sin, sout; /* the base entering and the base leaving the k-mer */
+		CodeStream sin, sout; /* the base entering and the base leaving the k-mer */
 		sin.init(src);
 		sout.init(src);
-		/* ntHash of frame qa: forward and reverse-complement hashes over its k
-		 * bases, then rolled one base at a time (bbt_device.cuh) */
+		/* ntHash of frame qa over its k bases, then rolled one base at a time */
 		uint64_t fh = 0, rh = 0;
 		int64_t lb = -1; /* last base that is not ACGT, read coordinates */
 		for (unsigned j = 0; j < k; ++j) {
-			const uint8_t c = sin.code(qa + j);
-			fh = rol1(fh) ^ seed_fw_code(c);
-			rh ^= rolk(seed_rc_code(c), j);
+			const uint32_t c = sin.code(qa + j);
+			fh = rol1(fh) ^ tab.tf[(4u << 3) | c];
+			rh ^= rolk(tab.rc[c], j);
 			if (c == 4)
 				lb = (int64_t)(qa + j);
 		}
 		for (uint64_t q = qa; q < qb; ++q) {
 			if (q > qa) {
-				const uint8_t out = sout.code(q - 1);
-				const uint8_t in = sin.code(q + k - 1);
-				fh = rol1(fh) ^ rolk(seed_fw_code(out), k) ^ seed_fw_code(in);
-				rh = ror1(rh) ^ ror1(seed_rc_code(out)) ^ rolk(seed_rc_code(in), k - 1);
+				const uint32_t out = sout.code(q - 1);
+				const uint32_t in = sin.code(q + k - 1);
+				const uint32_t e = (out << 3) | in;
+				fh = rol1(fh) ^ tab.tf[e];
+				rh = ror1(rh) ^ tab.tr[e];
 				if (in == 4)
 					lb = (int64_t)(q + k - 1);
 			}
@@ -237,6 +326,8 @@ __global__ void __launch_bounds__(kBkWinThreads) bk_count_kernel(BucketArgs b)
 	uint32_t *shb = bk_sm;
 	uint32_t *hist = bk_sm + kWinWords;
 	const uint32_t blk = blockIdx.x;
+	__shared__ RollTables tab;
+	bk_set_tables(tab, b.f.k);
 	for (uint32_t q = threadIdx.x; q < b.nbkt; q += blockDim.x)
 		hist[q] = 0;
 	if (!FIRST) {
@@ -246,7 +337,7 @@ __global__ void __launch_bounds__(kBkWinThreads) bk_count_kernel(BucketArgs b)
 	}
 	__syncthreads();
 	const unsigned sh = b.bshift;
-	bk_sweep_run<FIRST>(b, blk, shb, [&](uint64_t pos, uint32_t) {
+	bk_sweep_run<FIRST>(b, blk, shb, tab, [&](uint64_t pos, uint32_t) {
 		atomicAdd(&hist[pos >> sh], 1u);
 	});
 	__syncthreads();
@@ -260,13 +351,15 @@ __global__ void __launch_bounds__(kBkWinThreads) bk_write_kernel(BucketArgs b)
 	uint32_t *shb = bk_sm;
 	uint32_t *cur = bk_sm + kWinWords;
 	const uint32_t blk = blockIdx.x;
+	__shared__ RollTables tab;
+	bk_set_tables(tab, b.f.k);
 	for (uint32_t q = threadIdx.x; q < b.nbkt; q += blockDim.x)
 		cur[q] = 0;
 	bk_load_window(b, blk, shb);
 	__syncthreads();
 	const unsigned sh = b.bshift;
 	const uint64_t mask = (1ull << sh) - 1ull;
-	bk_sweep_run<false>(b, blk, shb, [&](uint64_t pos, uint32_t fid) {
+	bk_sweep_run<false>(b, blk, shb, tab, [&](uint64_t pos, uint32_t fid) {
 		const uint32_t q = (uint32_t)(pos >> sh);
 		const uint64_t i = b.seg[(uint64_t)q * b.nblk + blk] + atomicAdd(&cur[q], 1u);
 		b.req_off[i] = (uint32_t)(pos & mask);
@@ -384,6 +477,18 @@ __global__ void __launch_bounds__(256) bk_walk_kernel(BucketArgs b)
 	}
 }
 
+/* out[j] = fo[min(j * stride, total)] for j < n (frame offsets sampled for the
+ * host's sub-batch plan). */
+__global__ void bk_samples_kernel(const uint64_t *fo, uint64_t total, uint64_t stride,
+		uint64_t *out, uint64_t n)
+{
+	for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n;
+			j += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t r = j * stride;
+		out[j] = fo[r < total ? r : total];
+	}
+}
+
 __global__ void bk_frame_counts_kernel(ClassifyArgs a, unsigned k, uint64_t *fo_plus1)
 {
 	const uint64_t total = a.n * a.mates;
@@ -411,6 +516,15 @@ cudaError_t launch_bk_frame_counts(const ClassifyArgs &a, unsigned k, uint64_t *
 		return cudaSuccess;
 	const uint64_t need = (total + 255) / 256, cap = (uint64_t)num_sms * 8;
 	bk_frame_counts_kernel<<<(unsigned)(need < cap ? need : cap), 256, 0, s>>>(a, k, fo_plus1);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_bk_samples(const uint64_t *fo, uint64_t total, uint64_t stride, uint64_t *out,
+		uint64_t n, int num_sms, cudaStream_t s)
+{
+	const uint64_t need = (n + 255) / 256, cap = (uint64_t)num_sms * 4;
+	bk_samples_kernel<<<(unsigned)(need < cap ? need : cap), 256, 0, s>>>(fo, total, stride, out,
+			n);
 	return cudaGetLastError();
 }
 

@@ -48,6 +48,9 @@ struct BucketArgs {
 /* fo[i + 1] = frames of read i (n * mates reads); the caller scans it. */
 cudaError_t launch_bk_frame_counts(const ClassifyArgs &a, unsigned k, uint64_t *fo_plus1,
 		int num_sms, cudaStream_t s);
+/* out[j] = fo[min(j * stride, total)], j < n. */
+cudaError_t launch_bk_samples(const uint64_t *fo, uint64_t total, uint64_t stride, uint64_t *out,
+		uint64_t n, int num_sms, cudaStream_t s);
 /* A round's counting sweep (applying the previous round's results first). */
 cudaError_t launch_bk_count(const BucketArgs &b, cudaStream_t s);
 /* A round's writing sweep: requests in bucket-major order. */

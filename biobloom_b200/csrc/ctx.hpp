@@ -121,6 +121,7 @@ struct bbt_ctx {
 	uint8_t *d_bk_state = nullptr;
 	uint64_t bk_reads_cap = 0;
 	uint64_t *h_bk_samples = nullptr;      /* pinned */
+	uint64_t *d_bk_samples = nullptr;
 	uint64_t bk_samples_cap = 0;
 	uint32_t *d_bk_vbits = nullptr, *d_bk_hbits = nullptr;
 	uint32_t *d_bk_off = nullptr, *d_bk_res = nullptr;

@@ -99,11 +99,13 @@ __host__ __device__ inline size_t mibf_warp_bytes(uint32_t T)
 }
 
 /* With the tally in global memory: codes, invalid words, the touched count and
- * list. */
+ * list; rounded up to 16 bytes so that every warp's code words stay 8-byte
+ * aligned. */
 __host__ __device__ inline size_t mibf_warp_bytes_big()
 {
-	return 17 * 8 + 18 * 4 + 4 + (size_t)kTouchCap * 4;
+	return (17 * 8 + 18 * 4 + 4 + (size_t)kTouchCap * 4 + 15) & ~(size_t)15;
 }
+static_assert((17 * 8 + 18 * 4) % 8 == 0, "the tally words follow 8-byte aligned");
 
 /* Seed tables: with BBT_MIBF_PAIR_TABLES (the default) one entry per pair of
  * positions and pair of base codes (16 x 16 per seed: a value costs 13 table
