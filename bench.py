@@ -502,7 +502,29 @@ def run_gpu(args):
     result_bytes = n_pairs * (2 * words * 8 + 4)
     alg_bytes = 32.0 * alg_probes + read_bytes + result_bytes
     achieved = alg_bytes / (k_persistent * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "kernel": "classify path (scan + hash pass + filter pass)",
+                "classify_ms": k_persistent, "algorithmic_bytes_per_launch": alg_bytes}
+    if best == L.PATH_FILTER_MAJOR:
+        # each 68.5 MB filter is probed out of L2: the ceiling is the random
+        # 4-byte gather rate into a table of that size, measured here
+        import ctypes
+        fbytes = max(os.path.getsize(p) for p in paths)
+        rate = ctypes.c_double()
+        L.check(L.lib().bbt_measure_gather(local, (fbytes + 4095) // 4096 * 4096, 1 << 29, 0, 5,
+                                           ctypes.byref(rate)))
+        l2_peak = rate.value * 32.0 / 1e9
+        roofline.update({"bound": "l2", "peak": l2_peak, "frac": achieved / l2_peak,
+                         "peak_kind": f"measured in this run: {rate.value / 1e9:.1f} G random "
+                                      f"4-byte gathers/s into a {fbytes >> 20} MB table "
+                                      "(bbt_measure_gather) x 32 B per probe",
+                         "hbm_peak": peak, "hbm_frac": achieved / peak,
+                         "hbm_peak_kind": peak_kind})
     tpr = traffic_per_read()
+    roofline.update({"traffic": (tpr * n_reads if tpr else None),
+                     "traffic_note": "filter pass DRAM read+write per read from the committed "
+                                     "ncu capture, scaled to the step's reads"})
     value = world * n_reads / (ms_persistent * 1e-3)
     line = {
         "metric": METRIC,
@@ -534,14 +556,7 @@ def run_gpu(args):
                   "ms_per_step": ms_plain, "classify_ms": k_plain},
         "batched_over_plain": ms_plain / ms_persistent,
         "plain_equals_batched": plain_same,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": (tpr * n_reads if tpr else None),
-                     "traffic_note": "filter pass DRAM read+write per read from the committed ncu "
-                                     "capture, scaled to the step's reads",
-                     "kernel": "classify path (scan + hash pass + filter pass)",
-                     "classify_ms": k_persistent,
-                     "algorithmic_bytes_per_launch": alg_bytes},
+        "roofline": roofline,
         "cpu_baseline": cpu if cpu else {"value": None, "unavailable": cpu_err},
         "e2e": {"value": world * n_reads / e2e_s, "unit": "reads/s",
                 "h2d_bytes_per_step": int(2 * bases + 2 * (n_pairs + 1) * 8),
@@ -1023,6 +1038,24 @@ def run_single(args):
     achieved = alg_bytes / (k_ms * 1e-3) / 1e9
     fbytes = os.path.getsize(path)
     l2_resident = fbytes < 96 << 20
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                "kernel": {L.PATH_BUCKETED: "bucketed path (sweeps, resolve, walk)"}.get(
+                    tune["path"], "classify_kernel (tuned configuration)"),
+                "classify_ms": k_ms, "algorithmic_bytes_per_launch": alg_bytes}
+    if l2_resident:
+        # the filter is probed out of L2: the ceiling is the random 4-byte
+        # gather rate into a table of its size, measured here
+        rate = ctypes.c_double()
+        L.check(L.lib().bbt_measure_gather(local, max(fbytes, 1 << 20) // 4096 * 4096, 1 << 29, 0,
+                                           5, ctypes.byref(rate)))
+        l2_peak = rate.value * 32.0 / 1e9
+        roofline.update({"bound": "l2", "peak": l2_peak, "frac": achieved / l2_peak,
+                         "peak_kind": f"measured in this run: {rate.value / 1e9:.1f} G random "
+                                      f"4-byte gathers/s into a table of the filter's size "
+                                      "(bbt_measure_gather) x 32 B per probe",
+                         "hbm_peak": peak, "hbm_frac": achieved / peak,
+                         "hbm_peak_kind": peak_kind})
     line = {
         "metric": SINGLE_METRIC, "value": world * n / (ms_batched * 1e-3), "unit": "reads/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batched,
@@ -1041,10 +1074,7 @@ def run_single(args):
                   "reads_per_launch": PLAIN_BATCH, "equals_batched": plain_ok},
         "batched_over_plain": ms_plain / ms_batched,
         "batched_equals_counting_pass": batched_ok,
-        "roofline": {"bound": "l2" if l2_resident else "hbm", "achieved": achieved, "peak": peak,
-                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                     "traffic": None, "kernel": "classify_kernel (tuned configuration)",
-                     "classify_ms": k_ms, "algorithmic_bytes_per_launch": alg_bytes},
+        "roofline": roofline,
         "cpu_baseline": cpu if cpu else {"value": None, "unavailable": cpu_err},
         "e2e": {"value": world * n / e2e_s, "unit": "reads/s",
                 "h2d_bytes_per_step": int(bases + (n + 1) * 8),

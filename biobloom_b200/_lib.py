@@ -178,7 +178,7 @@ def lib():
         "bbt_make_filter": (i32, [vp, P(u64), u64, u32, dbl, u32, u64, cp, cp, cp, i32]),
         "bbt_measure_gather": (i32, [i32, u64, u64, i32, i32, P(dbl)]),
         "bbt_pack_bases": (i32, [vp, u64, vp, vp, P(u64)]),
-        "bbt_set_bucketing": (i32, [vp, u32, u32, u32, u64]),
+        "bbt_set_bucketing": (i32, [vp, u32, u32, u32, u64, u32]),
         "bbt_synth_genome": (i32, [u64, u64, dbl, dbl, ctypes.c_uint32, ctypes.c_uint32, dbl, dbl,
                                    vp]),
         "bbt_synth_read_lengths": (i32, [u64, P(SynthReadParams), u64, vp]),

@@ -117,10 +117,11 @@ class BioBloomClassifier:
         L.check(L.lib().bbt_set_launch(self._ctx, path, warps_per_block, frames_per_lane),
                 self._ctx)
 
-    def set_bucketing(self, bucket_shift=0, phase_split=0, phase_min=0, max_frames=0):
+    def set_bucketing(self, bucket_shift=0, phase_split=0, phase_min=0, max_frames=0,
+                      levels_per_round=0):
         """Settings of the bucketed path (bbt_set_bucketing; 0 keeps one)."""
         L.check(L.lib().bbt_set_bucketing(self._ctx, bucket_shift, phase_split, phase_min,
-                                          max_frames), self._ctx)
+                                          max_frames, levels_per_round), self._ctx)
 
     def set_schedule(self, long_bases=0):
         """Persistent kernel read order: reads of at least long_bases bases

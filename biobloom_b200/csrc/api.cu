@@ -821,7 +821,7 @@ static int run_two_pass(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s,
  * nbkt buckets x nblk blocks of counts. */
 static int bk_reserve(bbt_ctx *ctx, uint64_t frames, uint64_t cnt_entries)
 {
-	if (frames > ctx->bk_frames_cap) {
+	if (frames > ctx->bk_frames_cap || ctx->bk_levels > ctx->bk_pool_levels) {
 		cudaFree(ctx->d_bk_vbits);
 		cudaFree(ctx->d_bk_hbits);
 		cudaFree(ctx->d_bk_off);
@@ -834,10 +834,13 @@ static int bk_reserve(bbt_ctx *ctx, uint64_t frames, uint64_t cnt_entries)
 		const uint64_t f = (frames + kBkWinFrames - 1) / kBkWinFrames * kBkWinFrames;
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_vbits, (f / 32 + 2) * sizeof(uint32_t)));
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_hbits, (f / 32 + 2) * sizeof(uint32_t)));
-		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_off, f * sizeof(uint32_t)));
-		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_fid, f * sizeof(uint16_t)));
-		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_res, (f / 32 + 2) * sizeof(uint32_t)));
+		/* a round requests up to bk_levels tests per frame */
+		const uint64_t pool = f * ctx->bk_levels;
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_off, pool * sizeof(uint32_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_fid, pool * sizeof(uint16_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_res, (pool / 32 + 2) * sizeof(uint32_t)));
 		ctx->bk_frames_cap = f;
+		ctx->bk_pool_levels = ctx->bk_levels;
 	}
 	if (cnt_entries > ctx->bk_cnt_cap) {
 		for (int i = 0; i < 2; ++i) {
@@ -1046,26 +1049,35 @@ static int run_bucketed(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 			b.req_fid = ctx->d_bk_fid;
 			b.res = ctx->d_bk_res;
 			b.issued = a.probes;
+			/* rounds: level 0 alone, then up to bk_levels levels at a time */
+			std::vector<std::pair<uint32_t, uint32_t> > rounds;
+			for (uint32_t l = 0; l < F.h;) {
+				const uint32_t nl = l == 0 ? 1u : std::min<uint32_t>(ctx->bk_levels, F.h - l);
+				rounds.push_back({l, nl});
+				l += nl;
+			}
 			for (const auto &ph : phases) {
 				b.ph_lo = ph.first;
 				b.ph_hi = ph.second;
-				for (uint32_t l = 0; l < F.h; ++l) {
-					b.level = l;
-					b.cnt = ctx->d_bk_cnt[l & 1];
-					b.seg = ctx->d_bk_seg[l & 1];
-					b.pcnt = l ? ctx->d_bk_cnt[(l - 1) & 1] : nullptr;
-					b.pseg = l ? ctx->d_bk_seg[(l - 1) & 1] : nullptr;
+				for (size_t ri = 0; ri < rounds.size(); ++ri) {
+					b.level = rounds[ri].first;
+					b.nlevels = rounds[ri].second;
+					b.cnt = ctx->d_bk_cnt[ri & 1];
+					b.seg = ctx->d_bk_seg[ri & 1];
+					b.pcnt = ri ? ctx->d_bk_cnt[(ri - 1) & 1] : nullptr;
+					b.pseg = ri ? ctx->d_bk_seg[(ri - 1) & 1] : nullptr;
 					CUDA_TRY(ctx, launch_bk_count(b, s));
 					CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_bk_tmp, cnt_bytes, b.cnt,
 							b.seg, ncnt, s));
 					CUDA_TRY(ctx, launch_bk_write(b, s));
 					CUDA_TRY(ctx, launch_bk_resolve(b, ctx->num_sms, s));
 				}
-				b.pcnt = ctx->d_bk_cnt[(F.h - 1) & 1];
-				b.pseg = ctx->d_bk_seg[(F.h - 1) & 1];
+				const size_t last = rounds.size() - 1;
+				b.pcnt = ctx->d_bk_cnt[last & 1];
+				b.pseg = ctx->d_bk_seg[last & 1];
 				CUDA_TRY(ctx, launch_bk_apply(b, s));
 				CUDA_TRY(ctx, launch_bk_walk(b, ctx->num_sms, s));
-				ctx->last.kernels += 4 * F.h + 2;
+				ctx->last.kernels += 4 * (uint32_t)rounds.size() + 2;
 			}
 		}
 	}
@@ -1899,8 +1911,12 @@ extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int s
 }
 
 static int set_bucketing_one(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
-		unsigned phase_min, uint64_t max_frames)
+		unsigned phase_min, uint64_t max_frames, unsigned levels_per_round)
 {
+	if (levels_per_round > 2)
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_bucketing: levels_per_round must be 1 or 2");
+	if (levels_per_round)
+		ctx->bk_levels = levels_per_round;
 	if (!ctx)
 		return BBT_ERR_ARG;
 	if (bucket_shift && (bucket_shift < 12 || bucket_shift > 34))
@@ -1919,11 +1935,13 @@ static int set_bucketing_one(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase
 }
 
 extern "C" int bbt_set_bucketing(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
-		unsigned phase_min, uint64_t max_frames)
+		unsigned phase_min, uint64_t max_frames, unsigned levels_per_round)
 {
-	int rc = set_bucketing_one(ctx, bucket_shift, phase_split, phase_min, max_frames);
+	int rc = set_bucketing_one(ctx, bucket_shift, phase_split, phase_min, max_frames,
+			levels_per_round);
 	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
-		if ((rc = set_bucketing_one(ctx->peers[i], bucket_shift, phase_split, phase_min, max_frames)) != BBT_OK)
+		if ((rc = set_bucketing_one(ctx->peers[i], bucket_shift, phase_split, phase_min,
+				max_frames, levels_per_round)) != BBT_OK)
 			fail(ctx, rc, ctx->peers[i]->err);
 	return rc;
 }

@@ -21,11 +21,13 @@
  * To keep those extra tests few, a read's frames are resolved in phases: the
  * first phase covers a prefix of every read (most reads that match are
  * accepted early), the next the rest of the reads still undecided.  Per phase
- * and level, one round:
+ * and round (one hash level, or two: a frame that passed the levels before
+ * requests both, and stays a hit when both pass):
  *   count  -- per window block (kBkWinFrames frames of the sub-batch), apply
- *             the previous round's results to the block's hit bits, then hash
- *             the active frames (one thread per run of 128 consecutive frames,
- *             rolling ntHash) and count their requests per bucket;
+ *             the previous round's results to the block's hit bits (a frame
+ *             with any failed test is no longer a hit), then hash the active
+ *             frames (one thread per run of 128 consecutive frames, rolling
+ *             ntHash) and count their requests per bucket;
  *   scan   -- the counts in bucket-major order give every (bucket, block) its
  *             place in the request pool;
  *   write  -- hash again and write each request (bit offset in its bucket,
@@ -276,8 +278,10 @@ __device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *
 			}
 			if (active) {
 				const uint64_t canon = fh < rh ? fh : rh;
-				const uint64_t v = b.level ? extra_hash(canon, k, b.level) : canon;
-				op(reduce(v, b.f.m, b.f.minv), fid);
+				for (uint32_t l = b.level; l < b.level + b.nlevels; ++l) {
+					const uint64_t v = l ? extra_hash(canon, k, l) : canon;
+					op(reduce(v, b.f.m, b.f.minv), fid);
+				}
 			}
 		}
 	}

@@ -32,7 +32,8 @@ struct BucketArgs {
 	uint8_t *state;            /* per read of the batch: 0 open, 1 decided */
 	uint32_t ph_lo, ph_hi;     /* this phase: frames [bound(F, ph_lo), bound(F, ph_hi)) */
 	uint32_t ph_min;           /* bound(F, q) >= min(F, ph_min) for q > 0 */
-	uint32_t level;            /* hash function of this round (0 = the canonical hash) */
+	uint32_t level, nlevels;   /* hash functions of this round: [level, level + nlevels)
+	                              (0 = the canonical hash); a frame requests them all */
 	uint32_t nbkt, bshift;     /* bucket of bit p: p >> bshift */
 	unsigned long long *cnt;   /* this round's requests per (bucket, window): [nbkt][nblk],
 	                              one more entry (0) at the end for the scan's total */

@@ -127,6 +127,7 @@ struct bbt_ctx {
 	uint32_t *d_bk_off = nullptr, *d_bk_res = nullptr;
 	uint16_t *d_bk_fid = nullptr;
 	uint64_t bk_frames_cap = 0;
+	uint32_t bk_pool_levels = 0;          /* tests per frame the pool holds */
 	unsigned long long *d_bk_cnt[2] = {nullptr, nullptr};
 	unsigned long long *d_bk_seg[2] = {nullptr, nullptr};
 	uint64_t bk_cnt_cap = 0;
@@ -136,6 +137,7 @@ struct bbt_ctx {
 	uint32_t bk_bshift = 28;             /* bucket of 2^28 bits (32 MB) */
 	uint32_t bk_phase_split = 8;         /* phase boundary in sixteenths (16: one phase) */
 	uint32_t bk_phase_min = 64;          /* the first phase covers min(F, 64) frames or more */
+	uint32_t bk_levels = 2;              /* hash levels per round after the first (1 or 2) */
 	/* bbt_open_devices: the same filters opened on the other devices; host
 	 * batches are split across this context and these */
 	std::vector<bbt_ctx *> peers;
