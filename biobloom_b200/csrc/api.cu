@@ -190,15 +190,18 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 	cudaFree(ctx->d_bk_state);
 	cudaFreeHost(ctx->h_bk_samples);
 	cudaFree(ctx->d_bk_samples);
+	for (int i = 0; i < 2; ++i) {
+		cudaFree(ctx->d_bk_codes[i]);
+		cudaFree(ctx->d_bk_cvalid[i]);
+	}
 	cudaFree(ctx->d_bk_vbits);
 	cudaFree(ctx->d_bk_hbits);
+	cudaFree(ctx->d_bk_abits);
+	cudaFree(ctx->d_bk_canon);
 	cudaFree(ctx->d_bk_off);
 	cudaFree(ctx->d_bk_fid);
-	cudaFree(ctx->d_bk_res);
-	for (int i = 0; i < 2; ++i) {
-		cudaFree(ctx->d_bk_cnt[i]);
-		cudaFree(ctx->d_bk_seg[i]);
-	}
+	cudaFree(ctx->d_bk_cnt);
+	cudaFree(ctx->d_bk_loc);
 	cudaFree(ctx->d_bk_tmp);
 	cudaFree(ctx->d_tp_h0);
 	cudaFree(ctx->d_tp_vmask);
@@ -824,35 +827,34 @@ static int bk_reserve(bbt_ctx *ctx, uint64_t frames, uint64_t cnt_entries)
 	if (frames > ctx->bk_frames_cap || ctx->bk_levels > ctx->bk_pool_levels) {
 		cudaFree(ctx->d_bk_vbits);
 		cudaFree(ctx->d_bk_hbits);
+		cudaFree(ctx->d_bk_abits);
+		cudaFree(ctx->d_bk_canon);
 		cudaFree(ctx->d_bk_off);
 		cudaFree(ctx->d_bk_fid);
-		cudaFree(ctx->d_bk_res);
-		ctx->d_bk_vbits = ctx->d_bk_hbits = ctx->d_bk_off = ctx->d_bk_res = nullptr;
+		ctx->d_bk_vbits = ctx->d_bk_hbits = ctx->d_bk_abits = ctx->d_bk_off = nullptr;
+		ctx->d_bk_canon = nullptr;
 		ctx->d_bk_fid = nullptr;
 		ctx->bk_frames_cap = 0;
 		/* whole window blocks, plus spare words for reads across the end */
 		const uint64_t f = (frames + kBkWinFrames - 1) / kBkWinFrames * kBkWinFrames;
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_vbits, (f / 32 + 2) * sizeof(uint32_t)));
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_hbits, (f / 32 + 2) * sizeof(uint32_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_abits, (f / 32 + 2) * sizeof(uint32_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_canon, f * sizeof(uint64_t)));
 		/* a round requests up to bk_levels tests per frame */
-		const uint64_t pool = f * ctx->bk_levels;
+		const uint64_t pool = f * std::max<uint32_t>(ctx->bk_levels, 1);
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_off, pool * sizeof(uint32_t)));
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_fid, pool * sizeof(uint16_t)));
-		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_res, (pool / 32 + 2) * sizeof(uint32_t)));
 		ctx->bk_frames_cap = f;
-		ctx->bk_pool_levels = ctx->bk_levels;
+		ctx->bk_pool_levels = std::max<uint32_t>(ctx->bk_levels, 1);
 	}
 	if (cnt_entries > ctx->bk_cnt_cap) {
-		for (int i = 0; i < 2; ++i) {
-			cudaFree(ctx->d_bk_cnt[i]);
-			cudaFree(ctx->d_bk_seg[i]);
-			ctx->d_bk_cnt[i] = ctx->d_bk_seg[i] = nullptr;
-		}
+		cudaFree(ctx->d_bk_cnt);
+		cudaFree(ctx->d_bk_loc);
+		ctx->d_bk_cnt = ctx->d_bk_loc = nullptr;
 		ctx->bk_cnt_cap = 0;
-		for (int i = 0; i < 2; ++i) {
-			CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_cnt[i], cnt_entries * sizeof(unsigned long long)));
-			CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_seg[i], cnt_entries * sizeof(unsigned long long)));
-		}
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_cnt, cnt_entries * sizeof(uint32_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_loc, cnt_entries * sizeof(uint32_t)));
 		ctx->bk_cnt_cap = cnt_entries;
 	}
 	return BBT_OK;
@@ -884,29 +886,36 @@ struct BkCut {
  * come to the host (one short wait), and a sample interval above the limit is
  * read in full.  Reads with more than `most` frames on their own go to
  * `oversize`. */
-static int bk_plan(bbt_ctx *ctx, const uint64_t *fo, uint64_t total, uint64_t most,
-		cudaStream_t s, std::vector<BkCut> &cuts, std::vector<uint64_t> &oversize)
+static int bk_plan(bbt_ctx *ctx, const ClassifyArgs &a, const uint64_t *fo, uint64_t total,
+		uint64_t most, cudaStream_t s, std::vector<BkCut> &cuts, std::vector<uint64_t> &oversize,
+		uint64_t mate_end[2])
 {
 	const uint64_t S = 4096;
 	const uint64_t ns = total / S + 1;
-	if (ns + 1 > ctx->bk_samples_cap) {
+	if (ns + 3 > ctx->bk_samples_cap) {
 		cudaFreeHost(ctx->h_bk_samples);
 		cudaFree(ctx->d_bk_samples);
 		ctx->h_bk_samples = nullptr;
 		ctx->d_bk_samples = nullptr;
 		ctx->bk_samples_cap = 0;
-		CUDA_TRY(ctx, cudaMallocHost(&ctx->h_bk_samples, (ns + 1) * sizeof(uint64_t)));
-		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_samples, (ns + 1) * sizeof(uint64_t)));
-		ctx->bk_samples_cap = ns + 1;
+		CUDA_TRY(ctx, cudaMallocHost(&ctx->h_bk_samples, (ns + 3) * sizeof(uint64_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_samples, (ns + 3) * sizeof(uint64_t)));
+		ctx->bk_samples_cap = ns + 3;
 	}
 	uint64_t *h = ctx->h_bk_samples;
-	/* fo[0], fo[S], fo[2S], ..., then fo[total]: gathered on the device, one copy */
+	/* fo[0], fo[S], fo[2S], ..., then fo[total], then the end offset of each
+	 * mate array: gathered on the device, one copy */
 	CUDA_TRY(ctx, launch_bk_samples(fo, total, S, ctx->d_bk_samples, ns, ctx->num_sms, s));
 	CUDA_TRY(ctx, launch_bk_samples(fo + total, 0, 0, ctx->d_bk_samples + ns, 1, ctx->num_sms,
 			s));
-	CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->d_bk_samples, (ns + 1) * sizeof(uint64_t),
+	for (uint32_t m = 0; m < a.mates; ++m)
+		CUDA_TRY(ctx, launch_bk_samples(a.off[m] + a.n, 0, 0, ctx->d_bk_samples + ns + 1 + m, 1,
+				ctx->num_sms, s));
+	CUDA_TRY(ctx, cudaMemcpyAsync(h, ctx->d_bk_samples, (ns + 1 + a.mates) * sizeof(uint64_t),
 			cudaMemcpyDeviceToHost, s));
 	CUDA_TRY(ctx, cudaStreamSynchronize(s));
+	for (uint32_t m = 0; m < 2; ++m)
+		mate_end[m] = m < a.mates ? h[ns + 1 + m] : 0;
 	std::vector<uint64_t> pt(ns + 1), fv(ns + 1);
 	for (uint64_t j = 0; j < ns; ++j) {
 		pt[j] = j * S;
@@ -980,8 +989,12 @@ static int run_bucketed(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 	int rc = bk_tmp(ctx, scan_bytes);
 	if (rc)
 		return rc;
+	const uint32_t levels = std::max<uint32_t>(ctx->bk_levels, 1);
 	std::vector<BkCut> cuts;
 	std::vector<uint64_t> oversize;
+	PackedBases pk[2];
+	memset(pk, 0, sizeof pk);
+	bool have_pk = false;
 	unsigned cur_k = 0;
 	for (uint32_t f = 0; f < ctx->nf; ++f) {
 		const FilterDev &F = ctx->hf[f];
@@ -991,10 +1004,36 @@ static int run_bucketed(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 			CUDA_TRY(ctx, launch_bk_frame_counts(a, cur_k, ctx->d_bk_fo + 1, ctx->num_sms, s));
 			CUDA_TRY(ctx, cub::DeviceScan::InclusiveSum(ctx->d_bk_tmp, scan_bytes,
 					ctx->d_bk_fo + 1, ctx->d_bk_fo + 1, total, s));
-			rc = bk_plan(ctx, ctx->d_bk_fo, total, most, s, cuts, oversize);
+			uint64_t mate_end[2];
+			rc = bk_plan(ctx, a, ctx->d_bk_fo, total, most, s, cuts, oversize, mate_end);
 			if (rc)
 				return rc;
-			ctx->last.kernels += 2;
+			ctx->last.kernels += 2 + a.mates;
+			/* the bases as 2-bit codes: packed batches as they are, ASCII
+			 * batches packed once per call */
+			for (uint32_t m = 0; !have_pk && m < a.mates; ++m) {
+				const uint64_t len = mate_end[m] - a.off_base[m];
+				if (a.packed) {
+					pk[m].words = reinterpret_cast<const uint32_t *>(a.seq[m]);
+					pk[m].nwords = (len + 15) / 16;
+					pk[m].valid = a.valid[m];
+					pk[m].nvalid = a.valid[m] ? (len + 31) / 32 : 0;
+					continue;
+				}
+				rc = grow(ctx, &ctx->d_bk_codes[m], ctx->bk_codes_cap[m], 2 * (len / 32 + 2));
+				if (!rc)
+					rc = grow(ctx, &ctx->d_bk_cvalid[m], ctx->bk_cvalid_cap[m], len / 32 + 2);
+				if (rc)
+					return rc;
+				CUDA_TRY(ctx, launch_bk_pack(a.seq[m], len, ctx->d_bk_codes[m],
+						ctx->d_bk_cvalid[m], ctx->num_sms, s));
+				pk[m].words = ctx->d_bk_codes[m];
+				pk[m].nwords = 2 * (len / 32 + 2);
+				pk[m].valid = ctx->d_bk_cvalid[m];
+				pk[m].nvalid = len / 32 + 2;
+				ctx->last.kernels += 1;
+			}
+			have_pk = true;
 		}
 		CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_state, 0, total, s));
 		for (uint64_t r : oversize) /* the direct kernel's, below */
@@ -1009,28 +1048,27 @@ static int run_bucketed(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 			phases = {{0, split}, {split, kBkPhaseDen}};
 		else
 			phases = {{0, kBkPhaseDen}};
+		/* rounds of up to `levels` hash levels each */
+		std::vector<std::pair<uint32_t, uint32_t> > rounds;
+		for (uint32_t l = 0; l < F.h;) {
+			const uint32_t nl = std::min<uint32_t>(levels, F.h - l);
+			rounds.push_back({l, nl});
+			l += nl;
+		}
 		for (const BkCut &c : cuts) {
 			const uint64_t T = c.f1 - c.f0;
 			const uint32_t nblk = (uint32_t)((T + kBkWinFrames - 1) / kBkWinFrames);
-			const uint64_t ncnt = (uint64_t)nbkt * nblk + 1;
-			rc = bk_reserve(ctx, T, ncnt);
-			if (rc)
-				return rc;
-			size_t cnt_bytes = 0;
-			CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(nullptr, cnt_bytes, ctx->d_bk_cnt[0],
-					ctx->d_bk_seg[0], ncnt, s));
-			rc = bk_tmp(ctx, std::max(cnt_bytes, scan_bytes));
+			rc = bk_reserve(ctx, T, (uint64_t)nbkt * nblk);
 			if (rc)
 				return rc;
 			const uint64_t words = (T + 31) / 32 + 2;
 			CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_vbits, 0, words * sizeof(uint32_t), s));
 			CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_hbits, 0, words * sizeof(uint32_t), s));
-			for (int i = 0; i < 2; ++i)
-				CUDA_TRY(ctx, cudaMemsetAsync(ctx->d_bk_cnt[i] + ncnt - 1, 0,
-						sizeof(unsigned long long), s));
 			BucketArgs b;
 			memset(&b, 0, sizeof b);
 			b.a = a;
+			b.pk[0] = pk[0];
+			b.pk[1] = pk[1];
 			b.f = F;
 			b.fbit = f;
 			b.r0 = c.r0;
@@ -1041,43 +1079,32 @@ static int run_bucketed(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 			b.nblk = nblk;
 			b.vbits = ctx->d_bk_vbits;
 			b.hbits = ctx->d_bk_hbits;
+			b.abits = ctx->d_bk_abits;
+			b.canon = ctx->d_bk_canon;
 			b.state = ctx->d_bk_state;
 			b.ph_min = ctx->bk_phase_min;
 			b.nbkt = nbkt;
 			b.bshift = bshift;
+			b.cnt = ctx->d_bk_cnt;
+			b.loc = ctx->d_bk_loc;
+			b.cap = (uint64_t)kBkWinFrames * ctx->bk_pool_levels;
 			b.req_off = ctx->d_bk_off;
 			b.req_fid = ctx->d_bk_fid;
-			b.res = ctx->d_bk_res;
 			b.issued = a.probes;
-			/* rounds: level 0 alone, then up to bk_levels levels at a time */
-			std::vector<std::pair<uint32_t, uint32_t> > rounds;
-			for (uint32_t l = 0; l < F.h;) {
-				const uint32_t nl = l == 0 ? 1u : std::min<uint32_t>(ctx->bk_levels, F.h - l);
-				rounds.push_back({l, nl});
-				l += nl;
-			}
 			for (const auto &ph : phases) {
 				b.ph_lo = ph.first;
 				b.ph_hi = ph.second;
 				for (size_t ri = 0; ri < rounds.size(); ++ri) {
 					b.level = rounds[ri].first;
 					b.nlevels = rounds[ri].second;
-					b.cnt = ctx->d_bk_cnt[ri & 1];
-					b.seg = ctx->d_bk_seg[ri & 1];
-					b.pcnt = ri ? ctx->d_bk_cnt[(ri - 1) & 1] : nullptr;
-					b.pseg = ri ? ctx->d_bk_seg[(ri - 1) & 1] : nullptr;
-					CUDA_TRY(ctx, launch_bk_count(b, s));
-					CUDA_TRY(ctx, cub::DeviceScan::ExclusiveSum(ctx->d_bk_tmp, cnt_bytes, b.cnt,
-							b.seg, ncnt, s));
-					CUDA_TRY(ctx, launch_bk_write(b, s));
+					if (ri == 0)
+						CUDA_TRY(ctx, launch_bk_hash(b, s));
+					else
+						CUDA_TRY(ctx, launch_bk_emit(b, s));
 					CUDA_TRY(ctx, launch_bk_resolve(b, ctx->num_sms, s));
 				}
-				const size_t last = rounds.size() - 1;
-				b.pcnt = ctx->d_bk_cnt[last & 1];
-				b.pseg = ctx->d_bk_seg[last & 1];
-				CUDA_TRY(ctx, launch_bk_apply(b, s));
 				CUDA_TRY(ctx, launch_bk_walk(b, ctx->num_sms, s));
-				ctx->last.kernels += 4 * (uint32_t)rounds.size() + 2;
+				ctx->last.kernels += 2 * (uint32_t)rounds.size() + 1;
 			}
 		}
 	}
@@ -1913,8 +1940,8 @@ extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int s
 static int set_bucketing_one(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
 		unsigned phase_min, uint64_t max_frames, unsigned levels_per_round)
 {
-	if (levels_per_round > 2)
-		return fail(ctx, BBT_ERR_ARG, "bbt_set_bucketing: levels_per_round must be 1 or 2");
+	if (levels_per_round > 64)
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_bucketing: levels_per_round must be at most 64");
 	if (levels_per_round)
 		ctx->bk_levels = levels_per_round;
 	if (!ctx)

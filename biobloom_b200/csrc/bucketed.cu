@@ -13,29 +13,30 @@
  * The decisions are SeqEval's (Common/SeqEval.h:37-114 and the other scoring
  * methods) exactly: BloomFilter::contains is the AND of h bit tests, made
  * level by level (level l only for frames whose tests 0..l-1 all passed, as
- * contains() short-circuits), and the state machine of seqeval_chunk.cuh then
- * walks each read over the resolved hit bits.  The walk consumes only
- * contains() results, so making more tests than the sequential loop would (the
- * frames after a decision, frames in skip windows) changes no result.
+ * contains() short-circuits; or several levels per round when so set, a frame
+ * staying a hit only when all pass), and the state machine of
+ * seqeval_chunk.cuh then walks each read over the resolved hit bits.  The walk
+ * consumes only contains() results, so making more tests than the sequential
+ * loop would (frames after a decision, frames in skip windows, a second level
+ * after a failed first) changes no result.
  *
  * To keep those extra tests few, a read's frames are resolved in phases: the
  * first phase covers a prefix of every read (most reads that match are
- * accepted early), the next the rest of the reads still undecided.  Per phase
- * and round (one hash level, or two: a frame that passed the levels before
- * requests both, and stays a hit when both pass):
- *   count  -- per window block (kBkWinFrames frames of the sub-batch), apply
- *             the previous round's results to the block's hit bits (a frame
- *             with any failed test is no longer a hit), then hash the active
- *             frames (one thread per run of 128 consecutive frames, rolling
- *             ntHash) and count their requests per bucket;
- *   scan   -- the counts in bucket-major order give every (bucket, block) its
- *             place in the request pool;
- *   write  -- hash again and write each request (bit offset in its bucket,
- *             frame id in its block) to its place;
- *   resolve-- a resident grid tests the pool's requests in order, bucket by
- *             bucket, one result bit per request.
- * After the phase's last round the results are applied and one thread per
- * undecided read walks SeqEval over [0, phase end) of its frames.
+ * accepted early), the next the rest of the reads still undecided.  Per phase:
+ *   hash   -- per window block (kBkWinFrames frames of the sub-batch): the
+ *             phase's frames of the open reads are shared out evenly among
+ *             the block's threads, each rolling ntHash over its share (2-bit
+ *             codes, 16 bases per load); a frame's validity, hit and
+ *             requesting bits are set, its canonical hash kept, and its
+ *             requests of the round's levels counted per bucket, then written
+ *             to the block's region of the request pool in bucket order;
+ *   resolve-- the (bucket, block) segments in bucket-major order, one warp per
+ *             segment: each request's bit is tested out of the bucket held in
+ *             L2, and a failed test clears its frame's hit bit;
+ *   emit   -- (the later rounds) the block's frames still hits request their
+ *             next levels from their kept hashes, as above, then resolve;
+ * and after the last round one thread per undecided read walks SeqEval over
+ * [0, phase end) of its frames.
  */
 #include "bucketed.cuh"
 
@@ -47,10 +48,11 @@ namespace bbt {
 
 namespace {
 
-constexpr uint32_t kRun = kBkWinFrames / kBkWinThreads;  /* frames per thread: 128 */
+constexpr uint32_t kNT = kBkWinThreads;
+constexpr uint32_t kRun = kBkWinFrames / kNT;  /* frames per counting run: 128 */
 constexpr uint32_t kWinWords = kBkWinFrames / 32;
 constexpr uint32_t kMaxBuckets = 2048;
-static_assert(kRun % 32 == 0, "runs are whole hit-bit words");
+static_assert(kBkWinFrames % kNT == 0 && kNT % 32 == 0, "whole runs and warps");
 
 /* First frame of phase boundary q (sixteenths) of a read of F frames. */
 __device__ __forceinline__ uint64_t bk_bound(uint64_t F, uint32_t q, uint32_t pmin)
@@ -79,6 +81,18 @@ __device__ __forceinline__ uint64_t bk_find_read(const BucketArgs &b, uint64_t x
 	return lo;
 }
 
+/* The phase's frames of read r, clipped to [lo, hi) (sub-batch frames):
+ * [pa, pb), empty (pa >= pb) when the read is decided. */
+__device__ __forceinline__ void bk_piece(const BucketArgs &b, uint64_t r, uint64_t lo, uint64_t hi,
+		uint64_t &pa, uint64_t &pb)
+{
+	const uint64_t fr0 = b.fo[r] - b.fo0, F = b.fo[r + 1] - b.fo[r];
+	pa = max(lo, fr0 + bk_bound(F, b.ph_lo, b.ph_min));
+	pb = min(hi, fr0 + bk_bound(F, b.ph_hi, b.ph_min));
+	if (b.state[r])
+		pb = pa;
+}
+
 __device__ __forceinline__ uint64_t seed_fw_code(uint8_t c)
 {
 	return c == 0 ? kSeedA : c == 1 ? kSeedC : c == 2 ? kSeedG : c == 3 ? kSeedT : 0ull;
@@ -100,15 +114,15 @@ __device__ __forceinline__ uint32_t bits_at(const uint32_t *w, uint64_t x)
 
 /* ntHash rolling tables of one k, indexed by (code of the base leaving the
  * k-mer) << 3 | (code of the base entering it), codes 0..3 for ACGT and 4 for
- * any other base (whose seed is 0):
+ * any other base or for no base (seed 0):
  *   tf[o, i] = rol(seed_fw(o), k) ^ seed_fw(i)
  *   tr[o, i] = ror(seed_rc(o), 1) ^ rol(seed_rc(i), k - 1)
- * so that a step is fh = rol(fh, 1) ^ tf, rh = ror(rh, 1) ^ tr; rc[c] is the
- * plain reverse-complement seed (the first k-mer of a piece). */
+ * so that a step is fh = rol(fh, 1) ^ tf, rh = ror(rh, 1) ^ tr.  From
+ * fh = rh = 0, k steps with no base leaving give the hashes of the first
+ * k-mer: fh = XOR_j rol(seed_fw(s_j), k-1-j), rh = XOR_j rol(seed_rc(s_j), j). */
 struct RollTables {
 	uint64_t tf[64];
 	uint64_t tr[64];
-	uint64_t rc[8];
 };
 
 __device__ void bk_set_tables(RollTables &t, unsigned k)
@@ -117,316 +131,459 @@ __device__ void bk_set_tables(RollTables &t, unsigned k)
 		const uint8_t o = (uint8_t)(e >> 3), i = (uint8_t)(e & 7);
 		t.tf[e] = rolk(seed_fw_code(o), k) ^ seed_fw_code(i);
 		t.tr[e] = ror1(seed_rc_code(o)) ^ rolk(seed_rc_code(i), k - 1);
-		if (e < 8)
-			t.rc[e] = seed_rc_code((uint8_t)e);
 	}
 }
 
-/* Sequential 3-bit base codes (0..3 ACGT, 4 other) of one read for one
- * thread, fetched 16 bases per load: the aligned 16-byte block of ASCII bases
- * holding the base (bytes turned into codes and validity bits four at a time),
- * or the 2-bit code word and its validity bits.  Calls ask for non-decreasing
- * j.  (An aligned 16-byte block never crosses a page, so reading all of the
- * block that holds a valid base stays inside mapped memory.) */
-struct CodeStream {
-	Bases src;
-	uint64_t blk;
-	uint32_t codes; /* 2 bits per base of the block */
-	uint32_t bad;   /* 1 bit per base of the block: not ACGT */
-
-	__device__ __forceinline__ void init(const Bases &s)
-	{
-		src = s;
-		blk = ~0ull;
+/* Codes (2 bits per base) and non-ACGT flags (1 bit per base) of 16 bases
+ * from base g >= 0 of a packed mate array. */
+__device__ __forceinline__ void codes16_at(const PackedBases &p, uint64_t g, uint32_t &c,
+		uint32_t &bad)
+{
+	const uint64_t w = g >> 4;
+	const uint32_t lo = w < p.nwords ? __ldg(p.words + w) : 0u;
+	const uint32_t hi = w + 1 < p.nwords ? __ldg(p.words + w + 1) : 0u;
+	c = __funnelshift_r(lo, hi, (uint32_t)(g & 15u) * 2u);
+	if (p.valid) {
+		const uint64_t v = g >> 5;
+		const uint32_t vlo = v < p.nvalid ? __ldg(p.valid + v) : 0u;
+		const uint32_t vhi = v + 1 < p.nvalid ? __ldg(p.valid + v + 1) : 0u;
+		bad = ~__funnelshift_r(vlo, vhi, (uint32_t)(g & 31u)) & 0xFFFFu;
+	} else {
+		bad = 0;
 	}
+}
 
-	/* four ASCII bytes: their 2-bit codes (A0 C1 G2 T3 by bits 1-2 of the
-	 * byte) in bits 0-7 and a validity nibble */
-	__device__ __forceinline__ static void ascii4(uint32_t w, uint32_t &c8, uint32_t &ok4)
-	{
-		const uint32_t t = ((w >> 1) & 0x03030303u) ^ ((w >> 2) & 0x01010101u);
-		c8 = (t & 3u) | ((t >> 6) & 0xCu) | ((t >> 12) & 0x30u) | ((t >> 18) & 0xC0u);
-		const uint32_t u = w & 0xDFDFDFDFu;
-		const uint32_t v = __vcmpeq4(u, 0x41414141u) | __vcmpeq4(u, 0x43434343u) |
-				__vcmpeq4(u, 0x47474747u) | __vcmpeq4(u, 0x54545454u);
-		ok4 = ((v >> 7) & 1u) | ((v >> 14) & 2u) | ((v >> 21) & 4u) | ((v >> 28) & 8u);
+/* The same from base g, which may lie before the array (those bases flagged). */
+__device__ __forceinline__ void codes16(const PackedBases &p, int64_t g, uint32_t &c, uint32_t &bad)
+{
+	if (g >= 0) {
+		codes16_at(p, (uint64_t)g, c, bad);
+		return;
 	}
+	const int64_t d = -g;
+	if (d >= 16) {
+		c = 0;
+		bad = 0xFFFFu;
+		return;
+	}
+	uint32_t c0, b0;
+	codes16_at(p, 0, c0, b0);
+	c = c0 << (2u * (uint32_t)d);
+	bad = ((b0 << (uint32_t)d) | ((1u << (uint32_t)d) - 1u)) & 0xFFFFu;
+}
 
-	__device__ __forceinline__ uint32_t code(uint64_t j)
-	{
-		const uint64_t g = src.g0 + j;
-		uint32_t o;
-		if (src.ascii) {
-			const uintptr_t p = reinterpret_cast<uintptr_t>(src.ascii + g);
-			const uint64_t bk = p >> 4;
-			if (bk != blk) {
-				blk = bk;
-				const uint4 q = __ldg(reinterpret_cast<const uint4 *>(bk << 4));
-				uint32_t c0, c1, c2, c3, k0, k1, k2, k3;
-				ascii4(q.x, c0, k0);
-				ascii4(q.y, c1, k1);
-				ascii4(q.z, c2, k2);
-				ascii4(q.w, c3, k3);
-				codes = c0 | (c1 << 8) | (c2 << 16) | (c3 << 24);
-				bad = ~(k0 | (k1 << 4) | (k2 << 8) | (k3 << 12)) & 0xFFFFu;
+/* Four ASCII bytes: their 2-bit codes (A0 C1 G2 T3, by bits 1-2 of the byte)
+ * in bits 0-7 and a nibble of ACGT flags. */
+__device__ __forceinline__ void ascii4(uint32_t w, uint32_t &c8, uint32_t &ok4)
+{
+	const uint32_t t = ((w >> 1) & 0x03030303u) ^ ((w >> 2) & 0x01010101u);
+	c8 = (t & 3u) | ((t >> 6) & 0xCu) | ((t >> 12) & 0x30u) | ((t >> 18) & 0xC0u);
+	const uint32_t u = w & 0xDFDFDFDFu;
+	const uint32_t v = __vcmpeq4(u, 0x41414141u) | __vcmpeq4(u, 0x43434343u) |
+			__vcmpeq4(u, 0x47474747u) | __vcmpeq4(u, 0x54545454u);
+	ok4 = ((v >> 7) & 1u) | ((v >> 14) & 2u) | ((v >> 21) & 4u) | ((v >> 28) & 8u);
+}
+
+/* One thread per 32 bases: code words 2j, 2j + 1 and validity word j.  Bases
+ * at or past len are flagged and coded 0. */
+__global__ void bk_pack_kernel(const uint8_t *ascii, uint64_t len, uint32_t *words,
+		uint32_t *valid, uint64_t nvalid)
+{
+	const bool vec = (reinterpret_cast<uintptr_t>(ascii) & 15u) == 0;
+	for (uint64_t j = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nvalid;
+			j += (uint64_t)gridDim.x * blockDim.x) {
+		uint32_t ok = 0;
+		for (uint32_t h = 0; h < 2; ++h) {
+			const uint64_t g = j * 32 + h * 16;
+			uint32_t q[4] = {0, 0, 0, 0};
+			if (vec && g + 16 <= len) {
+				const uint4 v = __ldg(reinterpret_cast<const uint4 *>(ascii + g));
+				q[0] = v.x;
+				q[1] = v.y;
+				q[2] = v.z;
+				q[3] = v.w;
+			} else {
+				for (uint32_t i = 0; i < 16 && g + i < len; ++i)
+					q[i >> 2] |= (uint32_t)ascii[g + i] << (8u * (i & 3u));
 			}
-			o = (uint32_t)(p & 15u);
-		} else {
-			const uint64_t bk = g >> 4;
-			if (bk != blk) {
-				blk = bk;
-				codes = __ldg(src.words + bk);
-				bad = src.valid ? (~(__ldg(src.valid + (g >> 5)) >> (16u * (uint32_t)(bk & 1u))) &
-				                   0xFFFFu)
-				                : 0u;
+			uint32_t code = 0, ok16 = 0;
+			for (uint32_t i = 0; i < 4; ++i) {
+				uint32_t c8, k4;
+				ascii4(q[i], c8, k4);
+				code |= c8 << (8u * i);
+				ok16 |= k4 << (4u * i);
 			}
-			o = (uint32_t)(g & 15u);
+			if (g + 16 > len) { /* past the end: flagged, code 0 */
+				const uint32_t keep = g >= len ? 0u : (1u << (uint32_t)(len - g)) - 1u;
+				ok16 &= keep;
+				code &= g >= len ? 0u : (uint32_t)((1ull << (2u * (uint32_t)(len - g))) - 1u);
+			}
+			words[2 * j + h] = code;
+			ok |= ok16 << (16u * h);
 		}
-		return ((bad >> o) & 1u) ? 4u : ((codes >> (2u * o)) & 3u);
+		valid[j] = ok;
+	}
+}
+
+/* In-place exclusive scan of v[0, n) in shared memory by the whole block
+ * (blockDim.x == kNT); returns the total.  tmp: 33 words of shared memory. */
+__device__ uint32_t block_exscan(uint32_t *v, uint32_t n, uint32_t *tmp)
+{
+	const uint32_t t = threadIdx.x;
+	const uint32_t per = (n + kNT - 1) / kNT;
+	const uint32_t a = min(n, t * per), z = min(n, a + per);
+	uint32_t sum = 0;
+	for (uint32_t i = a; i < z; ++i)
+		sum += v[i];
+	const uint32_t lane = t & 31u, wid = t >> 5;
+	uint32_t inc = sum;
+#pragma unroll
+	for (uint32_t d = 1; d < 32; d <<= 1) {
+		const uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+		if (lane >= d)
+			inc += y;
+	}
+	if (lane == 31)
+		tmp[wid] = inc;
+	__syncthreads();
+	if (wid == 0) {
+		const uint32_t wv = lane < kNT / 32 ? tmp[lane] : 0u;
+		uint32_t wi = wv;
+#pragma unroll
+		for (uint32_t d = 1; d < 32; d <<= 1) {
+			const uint32_t y = __shfl_up_sync(0xffffffffu, wi, d);
+			if (lane >= d)
+				wi += y;
+		}
+		__syncwarp();
+		tmp[lane] = wi - wv;
+		if (lane == 31)
+			tmp[32] = wi;
+	}
+	__syncthreads();
+	uint32_t run = tmp[wid] + inc - sum;
+	for (uint32_t i = a; i < z; ++i) {
+		const uint32_t x = v[i];
+		v[i] = run;
+		run += x;
+	}
+	const uint32_t total = tmp[32];
+	__syncthreads();
+	return total;
+}
+
+/* Shared memory of the hash / emit kernels: the block's validity and
+ * requesting bits, counts and first slots of nbkt buckets. */
+struct SweepSmem {
+	uint32_t *sv, *sa, *hist, *loc;
+	__device__ __forceinline__ SweepSmem(uint32_t *base, uint32_t nbkt)
+	{
+		sv = base;
+		sa = base + kWinWords;
+		hist = sa + kWinWords;
+		loc = hist + nbkt;
 	}
 };
 
-/*
- * One thread's run of frames [x0, x0 + kRun) of window block blk: for every
- * frame of an open read inside the current phase, FIRST computes its validity
- * (ACGT only, not DUST-masked) into vbits / hbits; otherwise a frame is active
- * when its hit bit (shb, the block's words in shared memory) is still set.
- * op(pos, fid) is called for each active frame with the bit its hash of this
- * round's level selects and the frame's id in the block.
- */
-template <bool FIRST, class Op>
-__device__ void bk_sweep_run(const BucketArgs &b, uint32_t blk, const uint32_t *shb,
-		const RollTables &tab, Op op)
+/* After the block's requests are counted into sm.hist: their first slots per
+ * bucket (into sm.loc and the global cnt / loc tables), then each requesting
+ * frame of the block writes its requests of levels [level, level + nlevels) to
+ * its bucket's slots.  The canonical hashes are read back from b.canon. */
+__device__ void bk_scatter(const BucketArgs &b, const SweepSmem &sm, uint32_t *tmp)
 {
+	const uint32_t blk = blockIdx.x, t = threadIdx.x;
+	for (uint32_t q = t; q < b.nbkt; q += kNT)
+		sm.loc[q] = sm.hist[q];
+	__syncthreads();
+	block_exscan(sm.loc, b.nbkt, tmp);
+	for (uint32_t q = t; q < b.nbkt; q += kNT) {
+		b.cnt[(uint64_t)q * b.nblk + blk] = sm.hist[q];
+		b.loc[(uint64_t)q * b.nblk + blk] = sm.loc[q];
+		sm.hist[q] = 0;
+	}
+	__syncthreads();
 	const uint64_t w0 = (uint64_t)blk * kBkWinFrames;
-	const uint64_t x0 = w0 + (uint64_t)threadIdx.x * kRun;
-	if (x0 >= b.T)
-		return;
-	const uint64_t x1 = min(x0 + kRun, b.T);
-	const unsigned k = b.f.k;
-	/* FIRST: the run's validity / hit bits, one word at a time (word cw of
-	 * the sub-batch), merged into the arrays when the run moves past it; the
-	 * run's words belong to this thread */
-	uint64_t cw = x0 >> 5;
-	uint32_t vacc = 0, hacc = 0, touched = 0;
-	auto flush = [&]() {
-		if (touched) {
-			b.vbits[cw] = (b.vbits[cw] & ~touched) | vacc;
-			b.hbits[cw] = (b.hbits[cw] & ~touched) | hacc;
-		}
-		vacc = hacc = touched = 0;
-	};
-	uint64_t r = bk_find_read(b, x0);
-	for (uint64_t x = x0; x < x1;) {
-		while (b.fo[r + 1] - b.fo0 <= x)
-			++r;
-		const uint64_t fr0 = b.fo[r] - b.fo0, fr1 = b.fo[r + 1] - b.fo0;
-		const uint64_t F = fr1 - fr0;
-		const uint64_t q0 = x - fr0, q1 = min(x1, fr1) - fr0;
-		x = fr0 + q1;
-		if (b.state[r])
-			continue;
-		const uint64_t qa = max(q0, bk_bound(F, b.ph_lo, b.ph_min));
-		const uint64_t qb = min(q1, bk_bound(F, b.ph_hi, b.ph_min));
-		if (qa >= qb)
-			continue;
-		const uint32_t mate = r >= b.a.n ? 1u : 0u;
-		const uint64_t i = r - (mate ? b.a.n : 0);
-		const uint64_t start = b.a.off[mate][i] - b.a.off_base[mate];
-		const Bases src = read_bases(b.a, mate, start);
-		CodeStream sin, sout; /* the base entering and the base leaving the k-mer */
-		sin.init(src);
-		sout.init(src);
-		/* ntHash of frame qa over its k bases, then rolled one base at a time */
-		uint64_t fh = 0, rh = 0;
-		int64_t lb = -1; /* last base that is not ACGT, read coordinates */
-		for (unsigned j = 0; j < k; ++j) {
-			const uint32_t c = sin.code(qa + j);
-			fh = rol1(fh) ^ tab.tf[(4u << 3) | c];
-			rh ^= rolk(tab.rc[c], j);
-			if (c == 4)
-				lb = (int64_t)(qa + j);
-		}
-		for (uint64_t q = qa; q < qb; ++q) {
-			if (q > qa) {
-				const uint32_t out = sout.code(q - 1);
-				const uint32_t in = sin.code(q + k - 1);
-				const uint32_t e = (out << 3) | in;
-				fh = rol1(fh) ^ tab.tf[e];
-				rh = ror1(rh) ^ tab.tr[e];
-				if (in == 4)
-					lb = (int64_t)(q + k - 1);
-			}
-			const uint64_t xf = fr0 + q;
-			const uint32_t fid = (uint32_t)(xf - w0);
-			bool active;
-			if (FIRST) {
-				const bool valid = lb < (int64_t)q;
-				active = valid && !dust_low(b.a.dust[mate], start + q);
-				if ((xf >> 5) != cw) {
-					flush();
-					cw = xf >> 5;
-				}
-				const uint32_t bit = 1u << (uint32_t)(xf & 31u);
-				touched |= bit;
-				if (valid)
-					vacc |= bit;
-				if (active)
-					hacc |= bit;
-			} else {
-				active = (shb[fid >> 5] >> (fid & 31u)) & 1u;
-			}
-			if (active) {
-				const uint64_t canon = fh < rh ? fh : rh;
-				for (uint32_t l = b.level; l < b.level + b.nlevels; ++l) {
-					const uint64_t v = l ? extra_hash(canon, k, l) : canon;
-					op(reduce(v, b.f.m, b.f.minv), fid);
-				}
-			}
-		}
-	}
-	if (FIRST)
-		flush();
-}
-
-/* Load the hit bits of window block blk into shb. */
-__device__ __forceinline__ void bk_load_window(const BucketArgs &b, uint32_t blk, uint32_t *shb)
-{
-	const uint64_t wbase = (uint64_t)blk * kWinWords;
-	const uint64_t words = (b.T + 31) / 32;
-	for (uint32_t w = threadIdx.x; w < kWinWords; w += blockDim.x)
-		shb[w] = wbase + w < words ? b.hbits[wbase + w] : 0u;
-}
-
-/* Clear the hit bits of the block's frames whose previous-round test missed,
- * and store the block's words back. */
-__device__ void bk_apply_window(const BucketArgs &b, uint32_t blk, uint32_t *shb)
-{
-	for (uint32_t q = 0; q < b.nbkt; ++q) {
-		const uint64_t at = (uint64_t)q * b.nblk + blk;
-		const uint64_t s0 = b.pseg[at];
-		const uint32_t n = (uint32_t)b.pcnt[at];
-		for (uint32_t j = threadIdx.x; j < n; j += blockDim.x) {
-			const uint64_t i = s0 + j;
-			if (!((b.res[i >> 5] >> (i & 31u)) & 1u)) {
-				const uint32_t fid = b.req_fid[i];
-				atomicAnd(&shb[fid >> 5], ~(1u << (fid & 31u)));
-			}
-		}
-	}
-	__syncthreads();
-	const uint64_t wbase = (uint64_t)blk * kWinWords;
-	const uint64_t words = (b.T + 31) / 32;
-	for (uint32_t w = threadIdx.x; w < kWinWords; w += blockDim.x)
-		if (wbase + w < words)
-			b.hbits[wbase + w] = shb[w];
-	__syncthreads();
-}
-
-template <bool FIRST>
-__global__ void __launch_bounds__(kBkWinThreads) bk_count_kernel(BucketArgs b)
-{
-	extern __shared__ uint32_t bk_sm[];
-	uint32_t *shb = bk_sm;
-	uint32_t *hist = bk_sm + kWinWords;
-	const uint32_t blk = blockIdx.x;
-	__shared__ RollTables tab;
-	bk_set_tables(tab, b.f.k);
-	for (uint32_t q = threadIdx.x; q < b.nbkt; q += blockDim.x)
-		hist[q] = 0;
-	if (!FIRST) {
-		bk_load_window(b, blk, shb);
-		__syncthreads();
-		bk_apply_window(b, blk, shb);
-	}
-	__syncthreads();
-	const unsigned sh = b.bshift;
-	bk_sweep_run<FIRST>(b, blk, shb, tab, [&](uint64_t pos, uint32_t) {
-		atomicAdd(&hist[pos >> sh], 1u);
-	});
-	__syncthreads();
-	for (uint32_t q = threadIdx.x; q < b.nbkt; q += blockDim.x)
-		b.cnt[(uint64_t)q * b.nblk + blk] = hist[q];
-}
-
-__global__ void __launch_bounds__(kBkWinThreads) bk_write_kernel(BucketArgs b)
-{
-	extern __shared__ uint32_t bk_sm[];
-	uint32_t *shb = bk_sm;
-	uint32_t *cur = bk_sm + kWinWords;
-	const uint32_t blk = blockIdx.x;
-	__shared__ RollTables tab;
-	bk_set_tables(tab, b.f.k);
-	for (uint32_t q = threadIdx.x; q < b.nbkt; q += blockDim.x)
-		cur[q] = 0;
-	bk_load_window(b, blk, shb);
-	__syncthreads();
-	const unsigned sh = b.bshift;
+	const uint64_t base = (uint64_t)blk * b.cap;
+	const unsigned sh = b.bshift, k = b.f.k;
 	const uint64_t mask = (1ull << sh) - 1ull;
-	bk_sweep_run<false>(b, blk, shb, tab, [&](uint64_t pos, uint32_t fid) {
-		const uint32_t q = (uint32_t)(pos >> sh);
-		const uint64_t i = b.seg[(uint64_t)q * b.nblk + blk] + atomicAdd(&cur[q], 1u);
-		b.req_off[i] = (uint32_t)(pos & mask);
-		b.req_fid[i] = (uint16_t)fid;
-	});
+	const uint32_t lane = t & 31u;
+	for (uint32_t w = t >> 5; w < kWinWords; w += kNT / 32) {
+		const uint32_t am = sm.sa[w];
+		if (!((am >> lane) & 1u))
+			continue;
+		const uint32_t fid = w * 32 + lane;
+		const uint64_t canon = b.canon[w0 + fid];
+		for (uint32_t l = b.level; l < b.level + b.nlevels; ++l) {
+			const uint64_t pos = reduce(l ? extra_hash(canon, k, l) : canon, b.f.m, b.f.minv);
+			const uint32_t q = (uint32_t)(pos >> sh);
+			const uint64_t i = base + sm.loc[q] + atomicAdd(&sm.hist[q], 1u);
+			b.req_off[i] = (uint32_t)(pos & mask);
+			b.req_fid[i] = (uint16_t)fid;
+		}
+	}
 }
 
-__global__ void __launch_bounds__(kBkWinThreads) bk_apply_kernel(BucketArgs b)
+/*
+ * A phase's first round, per window block [w0, w1) of the sub-batch:
+ *  1. each thread counts the phase's frames of open reads in its run of kRun
+ *     frames, and a block scan numbers them 0..A-1 in frame order;
+ *  2. thread t takes frames [A t / kNT, A (t + 1) / kNT) of that numbering,
+ *     finds the first (its run by binary search over the scan, then the read
+ *     by walking the run) and rolls ntHash through them read piece by read
+ *     piece (k steps with no base leaving start each piece), setting the
+ *     frames' validity and requesting bits, keeping the canonical hash of each
+ *     requesting frame (valid, not DUST-masked) and counting its requests of
+ *     levels [0, nlevels) per bucket;
+ *  3. the bits go to the sub-batch arrays (this phase's frames are new there,
+ *     so hit bits start equal to the requesting bits), then bk_scatter.
+ */
+__global__ void __launch_bounds__(kNT) bk_hash_kernel(BucketArgs b)
 {
-	__shared__ uint32_t shb[kWinWords];
-	bk_load_window(b, blockIdx.x, shb);
+	extern __shared__ uint32_t bk_sm[];
+	const SweepSmem sm(bk_sm, b.nbkt);
+	__shared__ uint32_t pre[kNT + 1];
+	__shared__ uint32_t tmp[33];
+	__shared__ RollTables tab;
+	const uint32_t blk = blockIdx.x, t = threadIdx.x;
+	const uint64_t w0 = (uint64_t)blk * kBkWinFrames;
+	const uint64_t w1 = min(w0 + kBkWinFrames, b.T);
+	bk_set_tables(tab, b.f.k);
+	for (uint32_t w = t; w < kWinWords; w += kNT)
+		sm.sv[w] = sm.sa[w] = 0;
+	for (uint32_t q = t; q < b.nbkt; q += kNT)
+		sm.hist[q] = 0;
+
+	/* 1 */
+	const uint64_t end_r = b.r0 + b.nr;
+	uint32_t c = 0;
+	{
+		const uint64_t x0 = w0 + (uint64_t)t * kRun;
+		if (x0 < w1) {
+			const uint64_t x1 = min(x0 + kRun, w1);
+			for (uint64_t r = bk_find_read(b, x0); r < end_r && b.fo[r] - b.fo0 < x1; ++r) {
+				uint64_t pa, pb;
+				bk_piece(b, r, x0, x1, pa, pb);
+				if (pa < pb)
+					c += (uint32_t)(pb - pa);
+			}
+		}
+	}
+	pre[t] = c;
 	__syncthreads();
-	bk_apply_window(b, blockIdx.x, shb);
+	const uint32_t A = block_exscan(pre, kNT, tmp);
+	if (t == 0)
+		pre[kNT] = A;
+	__syncthreads();
+
+	/* 2 */
+	const uint32_t s0 = (uint32_t)((uint64_t)A * t / kNT);
+	const uint32_t s1 = (uint32_t)((uint64_t)A * (t + 1) / kNT);
+	const unsigned k = b.f.k;
+	uint32_t cw = 0xffffffffu, vacc = 0, aacc = 0;
+	if (s0 < s1) {
+		uint32_t lo = 0, hi = kNT; /* pre[lo] <= s0 < pre[lo + 1] */
+		while (hi - lo > 1) {
+			const uint32_t mid = (lo + hi) >> 1;
+			if (pre[mid] <= s0)
+				lo = mid;
+			else
+				hi = mid;
+		}
+		uint32_t o = s0 - pre[lo];
+		const uint64_t x0 = w0 + (uint64_t)lo * kRun, x1 = min(x0 + kRun, w1);
+		uint64_t r = bk_find_read(b, x0), xs = x1;
+		for (; r < end_r && b.fo[r] - b.fo0 < x1; ++r) {
+			uint64_t pa, pb;
+			bk_piece(b, r, x0, x1, pa, pb);
+			if (pa < pb) {
+				if (o < pb - pa) {
+					xs = pa + o;
+					break;
+				}
+				o -= (uint32_t)(pb - pa);
+			}
+		}
+		uint32_t left = s1 - s0;
+		while (left > 0 && r < end_r && xs < w1) {
+			const uint64_t fr0 = b.fo[r] - b.fo0;
+			uint64_t pa, pb;
+			bk_piece(b, r, xs, w1, pa, pb);
+			const uint32_t n = (uint32_t)min((uint64_t)left, pb > pa ? pb - pa : (uint64_t)0);
+			if (n > 0) {
+				const uint32_t mate = r >= b.a.n ? 1u : 0u;
+				const uint64_t i = r - (mate ? b.a.n : 0);
+				const uint64_t start = b.a.off[mate][i] - b.a.off_base[mate];
+				const PackedBases &P = b.pk[mate];
+				const uint32_t *dust = b.a.dust[mate];
+				const uint64_t qa = pa - fr0;           /* first frame, read coordinates */
+				const uint64_t steps = (uint64_t)n + k - 1;
+				uint64_t fh = 0, rh = 0;
+				int64_t lb = -1; /* last base that is not ACGT, read coordinates */
+				for (uint64_t j = qa; j < qa + steps; j += 16) {
+					const uint32_t gn = (uint32_t)min((uint64_t)16, qa + steps - j);
+					uint32_t cin, bin, cout, bout;
+					codes16(P, (int64_t)(start + j), cin, bin);
+					codes16(P, (int64_t)(start + j) - (int64_t)k, cout, bout);
+					if (j < qa + k) { /* the first k steps: no base leaves */
+						const uint64_t wu = qa + k - j;
+						bout |= wu >= 16 ? 0xFFFFu : (1u << (uint32_t)wu) - 1u;
+					}
+#pragma unroll
+					for (uint32_t u = 0; u < 16; ++u) {
+						if (u < gn) {
+							const uint32_t ci = ((bin >> u) & 1u) ? 4u : ((cin >> (2u * u)) & 3u);
+							const uint32_t co = ((bout >> u) & 1u) ? 4u : ((cout >> (2u * u)) & 3u);
+							const uint32_t e = (co << 3) | ci;
+							fh = rol1(fh) ^ tab.tf[e];
+							rh = ror1(rh) ^ tab.tr[e];
+							const uint64_t jj = j + u;
+							if (ci == 4u)
+								lb = (int64_t)jj;
+							if (jj + 1 >= qa + k) {
+								const uint64_t q = jj + 1 - k;
+								const uint32_t fid = (uint32_t)(fr0 + q - w0);
+								const uint32_t wi = fid >> 5, bit = 1u << (fid & 31u);
+								if (wi != cw) {
+									if (vacc)
+										atomicOr(&sm.sv[cw], vacc);
+									if (aacc)
+										atomicOr(&sm.sa[cw], aacc);
+									vacc = aacc = 0;
+									cw = wi;
+								}
+								if (lb < (int64_t)q) {
+									vacc |= bit;
+									if (!dust_low(dust, start + q)) {
+										aacc |= bit;
+										const uint64_t canon = fh < rh ? fh : rh;
+										b.canon[w0 + fid] = canon;
+										for (uint32_t l = 0; l < b.nlevels; ++l) {
+											const uint64_t pos = reduce(
+													l ? extra_hash(canon, k, l) : canon,
+													b.f.m, b.f.minv);
+											atomicAdd(&sm.hist[pos >> b.bshift], 1u);
+										}
+									}
+								}
+							}
+						}
+					}
+				}
+				left -= n;
+			}
+			/* the next read with frames in the phase */
+			++r;
+			xs = r < end_r ? max(xs, b.fo[r] - b.fo0) : w1;
+		}
+	}
+	if (vacc)
+		atomicOr(&sm.sv[cw], vacc);
+	if (aacc)
+		atomicOr(&sm.sa[cw], aacc);
+	__syncthreads();
+
+	/* 3 */
+	const uint64_t wbase = (uint64_t)blk * kWinWords;
+	const uint64_t words = (b.T + 31) / 32;
+	for (uint32_t w = t; w < kWinWords; w += kNT)
+		if (wbase + w < words) {
+			b.vbits[wbase + w] |= sm.sv[w];
+			b.hbits[wbase + w] |= sm.sa[w];
+			b.abits[wbase + w] = sm.sa[w];
+		}
+	bk_scatter(b, sm, tmp);
 }
 
-/* The pool's requests in index order (bucket-major), eight per lane in flight;
- * the bucket being tested is held in L2, the pool is read once (evict-first). */
+/* A later round, per window block: the frames requesting in this phase that
+ * are still hits count their requests of levels [level, level + nlevels) per
+ * bucket, then bk_scatter. */
+__global__ void __launch_bounds__(kNT) bk_emit_kernel(BucketArgs b)
+{
+	extern __shared__ uint32_t bk_sm[];
+	const SweepSmem sm(bk_sm, b.nbkt);
+	__shared__ uint32_t tmp[33];
+	const uint32_t blk = blockIdx.x, t = threadIdx.x;
+	const uint64_t w0 = (uint64_t)blk * kBkWinFrames;
+	const uint64_t wbase = (uint64_t)blk * kWinWords;
+	const uint64_t words = (b.T + 31) / 32;
+	for (uint32_t w = t; w < kWinWords; w += kNT)
+		sm.sa[w] = wbase + w < words ? b.abits[wbase + w] & b.hbits[wbase + w] : 0u;
+	for (uint32_t q = t; q < b.nbkt; q += kNT)
+		sm.hist[q] = 0;
+	__syncthreads();
+	const unsigned sh = b.bshift, k = b.f.k;
+	const uint32_t lane = t & 31u;
+	for (uint32_t w = t >> 5; w < kWinWords; w += kNT / 32) {
+		const uint32_t am = sm.sa[w];
+		if (!((am >> lane) & 1u))
+			continue;
+		const uint64_t canon = b.canon[w0 + w * 32 + lane];
+		for (uint32_t l = b.level; l < b.level + b.nlevels; ++l) {
+			const uint64_t pos = reduce(l ? extra_hash(canon, k, l) : canon, b.f.m, b.f.minv);
+			atomicAdd(&sm.hist[pos >> sh], 1u);
+		}
+	}
+	__syncthreads();
+	bk_scatter(b, sm, tmp);
+}
+
+/* The round's (bucket, block) segments in bucket-major order, one warp per
+ * segment and eight requests per lane in flight; the bucket being tested is
+ * held in L2, the pool is read once (streaming).  A failed test clears the
+ * frame's hit bit. */
 __global__ void __launch_bounds__(256) bk_resolve_kernel(BucketArgs b)
 {
-	__shared__ unsigned long long bs[kMaxBuckets + 1];
-	for (uint32_t q = threadIdx.x; q <= b.nbkt; q += blockDim.x)
-		bs[q] = b.seg[(uint64_t)q * b.nblk];
-	__syncthreads();
-	const uint64_t R = bs[b.nbkt];
-	if (b.issued && blockIdx.x == 0 && threadIdx.x == 0)
-		atomicAdd(b.issued, (unsigned long long)R);
-	const uint64_t pol = evict_first_policy();
-	const int lane = threadIdx.x & 31;
+	const uint32_t lane = threadIdx.x & 31u;
+	const uint64_t nseg = (uint64_t)b.nbkt * b.nblk;
 	const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
 	const uint32_t *words = b.f.words;
 	const unsigned sh = b.bshift;
-	for (uint64_t c = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c * 256 < R;
-			c += warps) {
-		uint64_t pos[8];
-		uint32_t w[8];
-#pragma unroll
-		for (int j = 0; j < 8; ++j) {
-			const uint64_t i = c * 256 + (uint64_t)j * 32 + lane;
-			pos[j] = ~0ull;
-			if (i < R) {
-				uint32_t lo = 0, hi = b.nbkt; /* bs[lo] <= i < bs[hi] */
-				while (hi - lo > 1) {
-					const uint32_t mid = (lo + hi) >> 1;
-					if (bs[mid] <= i)
-						lo = mid;
-					else
-						hi = mid;
-				}
-				pos[j] = ((uint64_t)lo << sh) | ld_stream_u32(b.req_off + i, pol);
-			}
+	unsigned long long issued = 0;
+	/* the next segment's count and first slot are loaded while this one is
+	 * tested */
+	uint64_t sg = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+	uint32_t n_next = sg < nseg ? b.cnt[sg] : 0u, loc_next = sg < nseg ? b.loc[sg] : 0u;
+	while (sg < nseg) {
+		const uint64_t cur = sg;
+		const uint32_t n = n_next, lc = loc_next;
+		sg += warps;
+		if (sg < nseg) {
+			n_next = b.cnt[sg];
+			loc_next = b.loc[sg];
 		}
+		if (n == 0)
+			continue;
+		const uint32_t q = (uint32_t)(cur / b.nblk);
+		const uint32_t blk = (uint32_t)(cur - (uint64_t)q * b.nblk);
+		const uint64_t base = (uint64_t)blk * b.cap + lc;
+		const uint64_t fbase = (uint64_t)blk * kBkWinFrames;
+		const uint64_t qbase = (uint64_t)q << sh;
+		issued += n;
+		for (uint32_t c = 0; c < n; c += 256) {
+			uint32_t off[8], fid[8], w[8];
 #pragma unroll
-		for (int j = 0; j < 8; ++j)
-			w[j] = pos[j] != ~0ull ? __ldg(words + (pos[j] >> 5)) : 0u;
+			for (int j = 0; j < 8; ++j) {
+				const uint32_t i = c + (uint32_t)j * 32 + lane;
+				off[j] = 0;
+				fid[j] = 0xffffffffu;
+				if (i < n) {
+					off[j] = __ldcs(b.req_off + base + i);
+					fid[j] = __ldcs(b.req_fid + base + i);
+				}
+			}
 #pragma unroll
-		for (int j = 0; j < 8; ++j) {
-			const uint32_t hit = __ballot_sync(0xffffffffu,
-					pos[j] != ~0ull && ((w[j] >> (pos[j] & 31u)) & 1u));
-			const uint64_t i0 = c * 256 + (uint64_t)j * 32;
-			if (lane == 0 && i0 < R)
-				b.res[i0 >> 5] = hit;
+			for (int j = 0; j < 8; ++j)
+				w[j] = fid[j] != 0xffffffffu ? __ldg(words + ((qbase + off[j]) >> 5)) : ~0u;
+#pragma unroll
+			for (int j = 0; j < 8; ++j)
+				if (!((w[j] >> (off[j] & 31u)) & 1u)) {
+					const uint64_t x = fbase + fid[j];
+					atomicAnd(&b.hbits[x >> 5], ~(1u << (uint32_t)(x & 31u)));
+				}
 		}
 	}
+	if (b.issued && lane == 0 && issued)
+		atomicAdd(b.issued, issued);
 }
 
 /* One thread per read of the sub-batch walks the exact state machine over
@@ -509,7 +666,7 @@ __global__ void bk_frame_counts_kernel(ClassifyArgs a, unsigned k, uint64_t *fo_
 
 size_t bk_sweep_smem(uint32_t nbkt)
 {
-	return (kWinWords + (size_t)nbkt) * sizeof(uint32_t);
+	return (2 * (size_t)kWinWords + 2 * (size_t)nbkt) * sizeof(uint32_t);
 }
 
 cudaError_t launch_bk_frame_counts(const ClassifyArgs &a, unsigned k, uint64_t *fo_plus1,
@@ -532,39 +689,33 @@ cudaError_t launch_bk_samples(const uint64_t *fo, uint64_t total, uint64_t strid
 	return cudaGetLastError();
 }
 
-cudaError_t launch_bk_count(const BucketArgs &b, cudaStream_t s)
+cudaError_t launch_bk_pack(const uint8_t *ascii, uint64_t len, uint32_t *words, uint32_t *valid,
+		int num_sms, cudaStream_t s)
 {
-	if (b.nblk == 0)
-		return cudaSuccess;
-	if (b.nbkt > kMaxBuckets)
-		return cudaErrorInvalidValue;
-	const size_t smem = bk_sweep_smem(b.nbkt);
-	if (b.pcnt) {
-		cudaError_t e = cudaFuncSetAttribute(bk_count_kernel<false>,
-				cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-		if (e != cudaSuccess)
-			return e;
-		bk_count_kernel<false><<<b.nblk, kBkWinThreads, smem, s>>>(b);
-	} else {
-		cudaError_t e = cudaFuncSetAttribute(bk_count_kernel<true>,
-				cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-		if (e != cudaSuccess)
-			return e;
-		bk_count_kernel<true><<<b.nblk, kBkWinThreads, smem, s>>>(b);
-	}
+	const uint64_t nvalid = len / 32 + 2;
+	const uint64_t need = (nvalid + 255) / 256, cap = (uint64_t)num_sms * 16;
+	bk_pack_kernel<<<(unsigned)(need < cap ? need : cap), 256, 0, s>>>(ascii, len, words, valid,
+			nvalid);
 	return cudaGetLastError();
 }
 
-cudaError_t launch_bk_write(const BucketArgs &b, cudaStream_t s)
+cudaError_t launch_bk_hash(const BucketArgs &b, cudaStream_t s)
 {
 	if (b.nblk == 0)
 		return cudaSuccess;
-	const size_t smem = bk_sweep_smem(b.nbkt);
-	cudaError_t e = cudaFuncSetAttribute(bk_write_kernel,
-			cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-	if (e != cudaSuccess)
-		return e;
-	bk_write_kernel<<<b.nblk, kBkWinThreads, smem, s>>>(b);
+	if (b.nbkt > kMaxBuckets || b.level != 0 || b.cap < (uint64_t)kBkWinFrames * b.nlevels)
+		return cudaErrorInvalidValue;
+	bk_hash_kernel<<<b.nblk, kNT, bk_sweep_smem(b.nbkt), s>>>(b);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_bk_emit(const BucketArgs &b, cudaStream_t s)
+{
+	if (b.nblk == 0)
+		return cudaSuccess;
+	if (b.nbkt > kMaxBuckets || b.cap < (uint64_t)kBkWinFrames * b.nlevels)
+		return cudaErrorInvalidValue;
+	bk_emit_kernel<<<b.nblk, kNT, bk_sweep_smem(b.nbkt), s>>>(b);
 	return cudaGetLastError();
 }
 
@@ -572,17 +723,13 @@ cudaError_t launch_bk_resolve(const BucketArgs &b, int num_sms, cudaStream_t s)
 {
 	if (b.nblk == 0)
 		return cudaSuccess;
-	if (b.nbkt > kMaxBuckets)
-		return cudaErrorInvalidValue;
-	bk_resolve_kernel<<<num_sms * 8, 256, 0, s>>>(b);
-	return cudaGetLastError();
-}
-
-cudaError_t launch_bk_apply(const BucketArgs &b, cudaStream_t s)
-{
-	if (b.nblk == 0)
-		return cudaSuccess;
-	bk_apply_kernel<<<b.nblk, kBkWinThreads, 0, s>>>(b);
+	/* one resident wave */
+	int per_sm = 0;
+	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk_resolve_kernel,
+			256, 0);
+	if (e != cudaSuccess)
+		return e;
+	bk_resolve_kernel<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, 0, s>>>(b);
 	return cudaGetLastError();
 }
 

@@ -18,8 +18,19 @@ constexpr int kBkWinThreads = 256;
 /* Phase boundaries are given in sixteenths of a read's frames. */
 constexpr uint32_t kBkPhaseDen = 16;
 
+/* A mate array's bases as 2-bit codes (16 per word, base g at bits 2 (g % 16)
+ * of word g / 16) and validity bits (base g at bit g % 32 of word g / 32; NULL
+ * when every base is ACGT); words past the ends read as 0. */
+struct PackedBases {
+	const uint32_t *words;
+	uint64_t nwords;
+	const uint32_t *valid;
+	uint64_t nvalid;
+};
+
 struct BucketArgs {
-	ClassifyArgs a;            /* the batch: bases, offsets, scoring, hit words */
+	ClassifyArgs a;            /* the batch: offsets, scoring, DUST masks, hit words */
+	PackedBases pk[2];         /* its bases, per mate array */
 	FilterDev f;               /* the filter of this pass */
 	uint32_t fbit;             /* its index: hit word fbit / 64, bit fbit % 64 */
 	uint64_t r0, nr;           /* reads [r0, r0 + nr) of the batch's read space */
@@ -29,20 +40,20 @@ struct BucketArgs {
 	uint32_t nblk;             /* window blocks: ceil(T / kBkWinFrames) */
 	uint32_t *vbits;           /* bit t: frame t of the sub-batch holds only ACGT */
 	uint32_t *hbits;           /* bit t: frame t is still a hit (all levels so far) */
+	uint32_t *abits;           /* bit t: frame t requests tests in this phase */
+	uint64_t *canon;           /* canonical ntHash of every requesting frame */
 	uint8_t *state;            /* per read of the batch: 0 open, 1 decided */
 	uint32_t ph_lo, ph_hi;     /* this phase: frames [bound(F, ph_lo), bound(F, ph_hi)) */
 	uint32_t ph_min;           /* bound(F, q) >= min(F, ph_min) for q > 0 */
 	uint32_t level, nlevels;   /* hash functions of this round: [level, level + nlevels)
 	                              (0 = the canonical hash); a frame requests them all */
 	uint32_t nbkt, bshift;     /* bucket of bit p: p >> bshift */
-	unsigned long long *cnt;   /* this round's requests per (bucket, window): [nbkt][nblk],
-	                              one more entry (0) at the end for the scan's total */
-	unsigned long long *seg;   /* their exclusive scan, total at [nbkt * nblk] */
-	const unsigned long long *pcnt; /* the previous round's (NULL in a phase's first round) */
-	const unsigned long long *pseg;
+	uint32_t *cnt;             /* this round's requests per (bucket, window block):
+	                              [nbkt][nblk] */
+	uint32_t *loc;             /* their first slot in the block's region of the pool */
+	uint64_t cap;              /* pool slots per window block */
 	uint32_t *req_off;         /* request pool: bit offset inside the bucket */
 	uint16_t *req_fid;         /*   frame id inside the window block */
-	uint32_t *res;             /* result bit per request */
 	unsigned long long *issued;/* optional: requests resolved (bit tests issued) */
 };
 
@@ -52,19 +63,25 @@ cudaError_t launch_bk_frame_counts(const ClassifyArgs &a, unsigned k, uint64_t *
 /* out[j] = fo[min(j * stride, total)], j < n. */
 cudaError_t launch_bk_samples(const uint64_t *fo, uint64_t total, uint64_t stride, uint64_t *out,
 		uint64_t n, int num_sms, cudaStream_t s);
-/* A round's counting sweep (applying the previous round's results first). */
-cudaError_t launch_bk_count(const BucketArgs &b, cudaStream_t s);
-/* A round's writing sweep: requests in bucket-major order. */
-cudaError_t launch_bk_write(const BucketArgs &b, cudaStream_t s);
-/* A round's bit tests, out of the bucket held in L2. */
+/* ASCII bases [0, len) into 2-bit codes (len / 16 + 2 words) and validity
+ * bits (len / 32 + 2 words). */
+cudaError_t launch_bk_pack(const uint8_t *ascii, uint64_t len, uint32_t *words, uint32_t *valid,
+		int num_sms, cudaStream_t s);
+/* A phase's first round: hash the phase's frames of the open reads, set their
+ * validity / hit / requesting bits, keep their canonical hashes and write
+ * their level-0 requests, sorted by bucket in each block's region. */
+cudaError_t launch_bk_hash(const BucketArgs &b, cudaStream_t s);
+/* A later round: requests of the frames still hits, levels
+ * [level, level + nlevels). */
+cudaError_t launch_bk_emit(const BucketArgs &b, cudaStream_t s);
+/* A round's bit tests, bucket by bucket (the bucket held in L2); a failed
+ * test clears its frame's hit bit. */
 cudaError_t launch_bk_resolve(const BucketArgs &b, int num_sms, cudaStream_t s);
-/* The last round's results into hbits (b.pcnt / b.pseg = that round's). */
-cudaError_t launch_bk_apply(const BucketArgs &b, cudaStream_t s);
 /* SeqEval over [0, bound(F, ph_hi)) of every open read; accepted reads set
  * their hit bit; reads decided or fully walked are closed. */
 cudaError_t launch_bk_walk(const BucketArgs &b, int num_sms, cudaStream_t s);
 
-/* Shared memory of the counting / writing kernels for nbkt buckets. */
+/* Dynamic shared memory of the hashing / emitting kernels for nbkt buckets. */
 size_t bk_sweep_smem(uint32_t nbkt);
 
 } // namespace bbt

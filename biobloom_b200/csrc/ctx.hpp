@@ -114,30 +114,34 @@ struct bbt_ctx {
 	uint64_t order_cap = 0;
 	unsigned long long *d_order_cnt = nullptr;
 	/* bucketed probe path (bucketed.cu): frame offsets of a batch's reads and
-	 * their host samples, per-read state, validity and hit bits of a
-	 * sub-batch, the request pool, per-(bucket, block) counts and their
-	 * scans, scan scratch; and the path's settings */
+	 * their host samples, per-read state, the batch's bases as 2-bit codes
+	 * (ASCII batches), validity / hit / requesting bits and canonical hashes
+	 * of a sub-batch's frames, the request pool, per-(bucket, block) counts
+	 * and first slots, scan scratch; and the path's settings */
 	uint64_t *d_bk_fo = nullptr;
 	uint8_t *d_bk_state = nullptr;
 	uint64_t bk_reads_cap = 0;
 	uint64_t *h_bk_samples = nullptr;      /* pinned */
 	uint64_t *d_bk_samples = nullptr;
 	uint64_t bk_samples_cap = 0;
-	uint32_t *d_bk_vbits = nullptr, *d_bk_hbits = nullptr;
-	uint32_t *d_bk_off = nullptr, *d_bk_res = nullptr;
+	uint32_t *d_bk_codes[2] = {nullptr, nullptr};
+	uint32_t *d_bk_cvalid[2] = {nullptr, nullptr};
+	uint64_t bk_codes_cap[2] = {0, 0}, bk_cvalid_cap[2] = {0, 0};
+	uint32_t *d_bk_vbits = nullptr, *d_bk_hbits = nullptr, *d_bk_abits = nullptr;
+	uint64_t *d_bk_canon = nullptr;
+	uint32_t *d_bk_off = nullptr;
 	uint16_t *d_bk_fid = nullptr;
 	uint64_t bk_frames_cap = 0;
 	uint32_t bk_pool_levels = 0;          /* tests per frame the pool holds */
-	unsigned long long *d_bk_cnt[2] = {nullptr, nullptr};
-	unsigned long long *d_bk_seg[2] = {nullptr, nullptr};
+	uint32_t *d_bk_cnt = nullptr, *d_bk_loc = nullptr;
 	uint64_t bk_cnt_cap = 0;
 	void *d_bk_tmp = nullptr;
 	size_t bk_tmp_cap = 0;
-	uint64_t bk_max_frames = 1ull << 31; /* frames per sub-batch */
+	uint64_t bk_max_frames = 1ull << 30; /* frames per sub-batch */
 	uint32_t bk_bshift = 28;             /* bucket of 2^28 bits (32 MB) */
 	uint32_t bk_phase_split = 8;         /* phase boundary in sixteenths (16: one phase) */
 	uint32_t bk_phase_min = 64;          /* the first phase covers min(F, 64) frames or more */
-	uint32_t bk_levels = 2;              /* hash levels per round after the first (1 or 2) */
+	uint32_t bk_levels = 1;              /* hash levels per round */
 	/* bbt_open_devices: the same filters opened on the other devices; host
 	 * batches are split across this context and these */
 	std::vector<bbt_ctx *> peers;

@@ -142,6 +142,12 @@ long FastxReader::read(std::string &name, std::string &comment, std::vector<char
 struct HostBatch {
 	char *seq[2] = {nullptr, nullptr};
 	size_t cap = 0;
+	/* the bases 2-bit packed with validity bits (pinned), as the batch goes
+	 * to the device when DUST masking is off; pk_bad: a mate has bases that
+	 * are not ACGT (else its validity bits are not sent) */
+	uint32_t *pkw[2] = {nullptr, nullptr}, *pkv[2] = {nullptr, nullptr};
+	size_t pk_cap = 0;
+	bool pk_bad[2] = {false, false};
 	std::vector<uint64_t> off[2];
 	std::vector<std::string> names;
 	std::vector<std::string> rname[2], rcomment[2], rqual[2];
@@ -438,6 +444,10 @@ int run_pipeline(bbt_ctx *ctx, const PipeInput &in, const char *prefix, const ch
 	}
 	HostBatch hb[2];
 	std::vector<char> stage1[2], stage2[2];
+	/* batches cross to the device 2-bit packed (a quarter of the bytes)
+	 * unless DUST masking needs the ASCII bases there; the ASCII copy stays
+	 * on the host for printing records */
+	const bool pack = !ctx->dust;
 	for (int i = 0; i < 2; ++i) {
 		size_t cap = max_bases + (1 << 20);
 		cudaError_t e = cudaMallocHost(&hb[i].seq[0], cap);
@@ -521,7 +531,37 @@ int run_pipeline(bbt_ctx *ctx, const PipeInput &in, const char *prefix, const ch
 						b.cap = need;
 					}
 				}
-				if (b.n) {
+				if (b.n && pack && need > b.pk_cap) {
+					for (int m = 0; m < 2; ++m) {
+						cudaFreeHost(b.pkw[m]);
+						cudaFreeHost(b.pkv[m]);
+						b.pkw[m] = b.pkv[m] = nullptr;
+					}
+					b.pk_cap = 0;
+					const size_t cap = std::max(need, b.cap);
+					bool okp = true;
+					for (int m = 0; okp && m < (paired ? 2 : 1); ++m)
+						okp = cudaMallocHost(&b.pkw[m], (cap / 16 + 2) * sizeof(uint32_t)) ==
+										cudaSuccess &&
+								cudaMallocHost(&b.pkv[m], (cap / 32 + 2) * sizeof(uint32_t)) ==
+										cudaSuccess;
+					if (!okp) {
+						pipe.err = "cannot allocate pinned memory for packed bases";
+						b.n = 0;
+						have = false;
+					} else {
+						b.pk_cap = cap;
+					}
+				}
+				if (b.n && pack) {
+					for (int m = 0; m < (paired ? 2 : 1); ++m) {
+						const std::vector<char> &st = m ? stage2[which] : stage1[which];
+						uint64_t bad = 0;
+						bbt_pack_bases(st.data(), st.size(), b.pkw[m], b.pkv[m], &bad);
+						b.pk_bad[m] = bad != 0;
+					}
+				}
+				if (b.n && (!pack || keep_records)) {
 					memcpy(b.seq[0], stage1[which].data(), stage1[which].size());
 					if (paired)
 						memcpy(b.seq[1], stage2[which].data(), stage2[which].size());
@@ -560,6 +600,15 @@ int run_pipeline(bbt_ctx *ctx, const PipeInput &in, const char *prefix, const ch
 			bt.offsets2 = paired ? b.off[1].data() : nullptr;
 			bt.n_reads = b.n;
 			bt.location = BBT_HOST;
+			if (pack) {
+				bt.encoding = BBT_BASES_2BIT;
+				bt.seq = (const char *)b.pkw[0];
+				bt.valid = b.pk_bad[0] ? b.pkv[0] : nullptr;
+				if (paired) {
+					bt.seq2 = (const char *)b.pkw[1];
+					bt.valid2 = b.pk_bad[1] ? b.pkv[1] : nullptr;
+				}
+			}
 			bbt_result res;
 			res.hits = nullptr;
 			res.hits2 = nullptr;
@@ -644,6 +693,10 @@ int run_pipeline(bbt_ctx *ctx, const PipeInput &in, const char *prefix, const ch
 	for (HostBatch &x : hb) {
 		cudaFreeHost(x.seq[0]);
 		cudaFreeHost(x.seq[1]);
+		for (int m = 0; m < 2; ++m) {
+			cudaFreeHost(x.pkw[m]);
+			cudaFreeHost(x.pkv[m]);
+		}
 	}
 	bool closed = true;
 	for (int m = 0; m < 2; ++m)

@@ -7,8 +7,17 @@
  *
  * Every valid k-mer of every sequence sets its h bits with atomicOr.  The bit
  * array does not depend on insertion order, so it equals the sequential
- * maker's.  As in the reference (whose OpenMP threads also race), the count of
- * "new" k-mers (num_entries) depends on the order insertions land in.
+ * maker's.  The counts of the .txt file do: BloomFilter::insertAndCheck
+ * (loadFilter, BloomFilterGenerator.h:170-174) counts a k-mer as redundant
+ * when all its bits were already set, which in a sequential insertion is when
+ * every bit it maps to was first set by an earlier k-mer.  So with k-mers
+ * numbered in insertion order (records in file order, k-mers left to right),
+ * first[b] = the lowest number mapping to bit b is taken with atomicMin, and
+ * k-mer i is new exactly when first[b] == i for one of its bits.  Those counts
+ * are the reference's for a one-threaded run (and for any run whose records
+ * each fit one thread, as a single-record genome does); its multi-threaded
+ * runs race between records.  first[] covers the filter in slices of at most
+ * 2^31 bits, each slice a pass over all k-mers.
  */
 #include <cuda_runtime.h>
 
@@ -28,14 +37,23 @@ namespace {
 
 constexpr int kMakerSeg = 64; /* frames per thread */
 
-/* Insert the frames [0, nframes) of chunk s (whose bases [0, nframes + k - 1)
- * are resident).  counts[0] += new k-mers, counts[1] += already-present ones. */
-__global__ void insert_kernel(const uint8_t *__restrict__ s, uint64_t nframes, unsigned k,
-		unsigned h, uint32_t *words, uint64_t m, uint64_t minv, unsigned long long *counts)
+enum MakerPass { kInsert, kFirst, kFresh };
+
+/* One pass over the frames [0, nframes) of chunk s (bases [0, nframes + k - 1)
+ * resident), numbered idx0 + q:
+ *   kInsert: set the h bits; counts[0] += valid k-mers;
+ *   kFirst:  first[b - lo] = min(first[b - lo], number) for bits b in
+ *            [lo, lo + span);
+ *   kFresh:  mark the k-mer new (bit `number` of fresh) when some bit b in
+ *            the slice has first[b - lo] == number. */
+template <int PASS, class IdxT>
+__global__ void maker_kernel(const uint8_t *__restrict__ s, uint64_t nframes, uint64_t idx0,
+		unsigned k, unsigned h, uint32_t *words, uint64_t m, uint64_t minv, IdxT *first,
+		uint64_t lo, uint64_t span, uint32_t *fresh, unsigned long long *counts)
 {
 	const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
 	const uint64_t q0 = t * kMakerSeg;
-	unsigned long long fresh = 0, seen = 0;
+	unsigned long long valid = 0;
 	if (q0 < nframes) {
 		const uint64_t qe = min(q0 + kMakerSeg, nframes);
 		uint64_t fh = 0, rh = 0;
@@ -51,17 +69,24 @@ __global__ void insert_kernel(const uint8_t *__restrict__ s, uint64_t nframes, u
 		const uint64_t fk[4] = {rolk(kSeedA, k), rolk(kSeedC, k), rolk(kSeedG, k), rolk(kSeedT, k)};
 		for (uint64_t q = q0;; ) {
 			if (lb < (int64_t)q) {
-				uint64_t canon = fh < rh ? fh : rh;
-				bool found = true;
+				const uint64_t canon = fh < rh ? fh : rh;
+				const uint64_t num = idx0 + q;
+				bool is_first = false;
 				for (unsigned i = 0; i < h; ++i) {
-					uint64_t v = i ? extra_hash(canon, k, i) : canon;
-					uint64_t b = reduce(v, m, minv);
-					uint32_t bit = 1u << (b & 31);
-					uint32_t old = atomicOr(words + (b >> 5), bit);
-					found = found && (old & bit);
+					const uint64_t v = i ? extra_hash(canon, k, i) : canon;
+					const uint64_t b = reduce(v, m, minv);
+					if (PASS == kInsert) {
+						atomicOr(words + (b >> 5), 1u << (b & 31));
+					} else if (b >= lo && b - lo < span) {
+						if (PASS == kFirst)
+							atomicMin(first + (b - lo), (IdxT)num);
+						else
+							is_first = is_first || first[b - lo] == (IdxT)num;
+					}
 				}
-				fresh += !found;
-				seen += found;
+				valid += 1;
+				if (PASS == kFresh && is_first)
+					atomicOr(fresh + (num >> 5), 1u << (num & 31));
 			}
 			if (++q >= qe)
 				break;
@@ -74,14 +99,25 @@ __global__ void insert_kernel(const uint8_t *__restrict__ s, uint64_t nframes, u
 				lb = (int64_t)(q + k - 1);
 		}
 	}
-	for (int o = 16; o; o >>= 1) {
-		fresh += __shfl_xor_sync(0xffffffffu, fresh, o);
-		seen += __shfl_xor_sync(0xffffffffu, seen, o);
+	if (PASS == kInsert) {
+		for (int o = 16; o; o >>= 1)
+			valid += __shfl_xor_sync(0xffffffffu, valid, o);
+		if ((threadIdx.x & 31) == 0 && valid)
+			atomicAdd(&counts[0], valid);
 	}
-	if ((threadIdx.x & 31) == 0 && (fresh || seen)) {
-		atomicAdd(&counts[0], fresh);
-		atomicAdd(&counts[1], seen);
-	}
+}
+
+/* counts[1] += set bits of w[0, n). */
+__global__ void popcount_kernel(const uint32_t *w, uint64_t n, unsigned long long *counts)
+{
+	unsigned long long c = 0;
+	for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+			i += (uint64_t)gridDim.x * blockDim.x)
+		c += __popc(w[i]);
+	for (int o = 16; o; o >>= 1)
+		c += __shfl_xor_sync(0xffffffffu, c, o);
+	if ((threadIdx.x & 31) == 0 && c)
+		atomicAdd(&counts[1], c);
 }
 
 /* BloomFilterInfo::calcRedunancyFPR (Common/BloomFilterInfo.cpp:289-297) is
@@ -137,8 +173,20 @@ extern "C" int bbt_make_filter(const char *seq, const uint64_t *offsets, uint64_
 	uint32_t *d_words = nullptr;
 	uint8_t *d_seq = nullptr;
 	unsigned long long *d_counts = nullptr;
+	void *d_first = nullptr;
+	uint32_t *d_fresh = nullptr;
 	const uint64_t chunk = 256ull << 20;
 	std::vector<uint8_t> host;
+	uint64_t nframes_total = 0;
+	for (uint64_t r = 0; r < n_seqs; ++r) {
+		const uint64_t len = offsets[r + 1] - offsets[r];
+		nframes_total += len >= k ? len - k + 1 : 0;
+	}
+	/* k-mer numbers fit 32 bits (all ones meaning "none") below 2^32 - 1 frames */
+	const bool narrow = nframes_total < 0xffffffffull;
+	const size_t isz = narrow ? sizeof(uint32_t) : sizeof(unsigned long long);
+	const uint64_t span = std::min<uint64_t>(m, 1ull << 31);
+	const int npass = 1 + 2 * (int)((m + span - 1) / span);
 	int rc = BBT_OK;
 #define MK_TRY(call)                                   \
 	do {                                               \
@@ -153,24 +201,64 @@ extern "C" int bbt_make_filter(const char *seq, const uint64_t *offsets, uint64_
 	MK_TRY(cudaMalloc(&d_seq, chunk + k));
 	MK_TRY(cudaMalloc(&d_counts, 2 * sizeof(unsigned long long)));
 	MK_TRY(cudaMemset(d_counts, 0, 2 * sizeof(unsigned long long)));
-	for (uint64_t r = 0; r < n_seqs; ++r) {
-		const uint64_t len = offsets[r + 1] - offsets[r];
-		if (len < k)
-			continue;
-		const uint64_t frames = len - k + 1;
-		for (uint64_t f0 = 0; f0 < frames; f0 += chunk) {
-			const uint64_t nfr = std::min(chunk, frames - f0);
-			MK_TRY(cudaMemcpy(d_seq, seq + offsets[r] + f0, nfr + k - 1, cudaMemcpyHostToDevice));
-			const uint64_t threads = (nfr + kMakerSeg - 1) / kMakerSeg;
-			const unsigned bs = 256;
-			insert_kernel<<<(unsigned)((threads + bs - 1) / bs), bs>>>(d_seq, nfr, k, h, d_words, m,
-					~0ull / m, d_counts);
-			MK_TRY(cudaGetLastError());
+	MK_TRY(cudaMalloc(&d_first, span * isz));
+	MK_TRY(cudaMalloc(&d_fresh, (nframes_total / 32 + 1) * sizeof(uint32_t)));
+	MK_TRY(cudaMemset(d_fresh, 0, (nframes_total / 32 + 1) * sizeof(uint32_t)));
+	/* the insertion pass, then per slice of bits the first-number pass and the
+	 * new-k-mer pass; each pass streams every sequence through d_seq */
+	for (int pass = 0; pass < npass; ++pass) {
+		const uint64_t lo = pass == 0 ? 0 : (uint64_t)((pass - 1) / 2) * span;
+		const uint64_t sp = pass == 0 ? 0 : std::min(span, m - lo);
+		if (pass & 1)
+			MK_TRY(cudaMemset(d_first, 0xff, sp * isz));
+		uint64_t idx0 = 0;
+		for (uint64_t r = 0; r < n_seqs; ++r) {
+			const uint64_t len = offsets[r + 1] - offsets[r];
+			if (len < k)
+				continue;
+			const uint64_t frames = len - k + 1;
+			for (uint64_t f0 = 0; f0 < frames; f0 += chunk) {
+				const uint64_t nfr = std::min(chunk, frames - f0);
+				MK_TRY(cudaMemcpy(d_seq, seq + offsets[r] + f0, nfr + k - 1,
+						cudaMemcpyHostToDevice));
+				const uint64_t threads = (nfr + kMakerSeg - 1) / kMakerSeg;
+				const unsigned bs = 256, grid = (unsigned)((threads + bs - 1) / bs);
+				const uint64_t i0 = idx0 + f0, minv = ~0ull / m;
+				if (pass == 0) {
+					maker_kernel<kInsert, uint32_t><<<grid, bs>>>(d_seq, nfr, i0, k, h, d_words,
+							m, minv, nullptr, 0, 0, nullptr, d_counts);
+				} else if (narrow) {
+					uint32_t *fi = (uint32_t *)d_first;
+					if (pass & 1)
+						maker_kernel<kFirst, uint32_t><<<grid, bs>>>(d_seq, nfr, i0, k, h,
+								nullptr, m, minv, fi, lo, sp, nullptr, nullptr);
+					else
+						maker_kernel<kFresh, uint32_t><<<grid, bs>>>(d_seq, nfr, i0, k, h,
+								nullptr, m, minv, fi, lo, sp, d_fresh, nullptr);
+				} else {
+					unsigned long long *fi = (unsigned long long *)d_first;
+					if (pass & 1)
+						maker_kernel<kFirst, unsigned long long><<<grid, bs>>>(d_seq, nfr, i0, k,
+								h, nullptr, m, minv, fi, lo, sp, nullptr, nullptr);
+					else
+						maker_kernel<kFresh, unsigned long long><<<grid, bs>>>(d_seq, nfr, i0, k,
+								h, nullptr, m, minv, fi, lo, sp, d_fresh, nullptr);
+				}
+				MK_TRY(cudaGetLastError());
+			}
+			idx0 += frames;
 		}
 	}
+	popcount_kernel<<<256, 256>>>(d_fresh, nframes_total / 32 + 1, d_counts);
+	MK_TRY(cudaGetLastError());
 	{
 		unsigned long long cnt[2];
 		MK_TRY(cudaMemcpy(cnt, d_counts, sizeof cnt, cudaMemcpyDeviceToHost));
+		/* counted: cnt[0] valid k-mers, cnt[1] new ones; below cnt[0] new and
+		 * cnt[1] redundant */
+		const unsigned long long fresh_n = cnt[1];
+		cnt[1] = cnt[0] - fresh_n;
+		cnt[0] = fresh_n;
 		host.resize(m / 8);
 		MK_TRY(cudaMemcpy(host.data(), d_words, m / 8, cudaMemcpyDeviceToHost));
 		BfHeader hd;
@@ -211,6 +299,8 @@ out:
 	cudaFree(d_words);
 	cudaFree(d_seq);
 	cudaFree(d_counts);
+	cudaFree(d_first);
+	cudaFree(d_fresh);
 	return rc;
 #undef MK_TRY
 }

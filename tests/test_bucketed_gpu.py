@@ -17,7 +17,8 @@ pytestmark = pytest.mark.gpu
 
 SETTINGS = [dict(bucket_shift=12, phase_split=8, phase_min=64, max_frames=40000),
             dict(bucket_shift=14, phase_split=16, phase_min=1, max_frames=1 << 20),
-            dict(bucket_shift=12, phase_split=3, phase_min=1, max_frames=33000),
+            dict(bucket_shift=12, phase_split=3, phase_min=1, max_frames=33000,
+                 levels_per_round=1),
             dict(bucket_shift=28, phase_split=8, phase_min=64, max_frames=0)]
 SET_IDS = ["b12-half", "b14-one-phase", "b12-3of16", "default"]
 

@@ -293,6 +293,31 @@ def test_gpu_maker_matches_oracle_maker(tmp_path):
     assert np.array_equal(mine.bits(), ref.bits())
     info = open(stem + ".txt").read()
     assert "filter_id=m\n" in info and "kmer_size=25\n" in info
+    # num_entries / redundant_sequences as a sequential insertion counts them
+    valid = sum(len(ol.kmers(s.tobytes(), 1, 25)) for s in (g, g2))
+    assert f"\nnum_entries={valid - ref.redundant}\n" in info
+    assert f"\nredundant_sequences={ref.redundant}\n" in info
+
+
+def test_gpu_maker_equals_reference_maker_files(tmp_path):
+    """The reference's biobloommaker output (tests/golden/bbt/f*.bf, f*.txt,
+    one single-record genome each) byte for byte: bit array, header and the
+    info file's counts and rates."""
+    import os
+    from biobloom_b200 import synth
+    from tests.golden import make_golden as mg
+    rng = np.random.default_rng(20240611)
+    genomes = [mg.genome(rng, 20000, gc) for gc in (0.5, 0.41, 0.6)]
+    genomes[2][5000:7000] = genomes[0][1000:3000]
+    gold = os.path.join(os.path.dirname(__file__), "golden", "bbt")
+    for i, g in enumerate(genomes):
+        want_txt = open(os.path.join(gold, f"f{i}.txt")).read()
+        src = [ln for ln in want_txt.splitlines() if ln.startswith("sequence_sources=")][0]
+        stem = str(tmp_path / f"f{i}")
+        synth.make_filter([g], stem, f"f{i}", k=25, fpr=0.075,
+                          sources=src[len("sequence_sources="):].rstrip(" "))
+        assert open(stem + ".txt").read() == want_txt
+        assert open(stem + ".bf", "rb").read() == open(os.path.join(gold, f"f{i}.bf"), "rb").read()
 
 
 @pytest.mark.parametrize("paired", [False, True])
