@@ -200,6 +200,8 @@ extern "C" int bbt_close(bbt_ctx *ctx)
 	cudaFree(ctx->d_bk_canon);
 	cudaFree(ctx->d_bk_off);
 	cudaFree(ctx->d_bk_fid);
+	cudaFree(ctx->d_bk_res);
+	cudaFree(ctx->d_bk_btot);
 	cudaFree(ctx->d_bk_cnt);
 	cudaFree(ctx->d_bk_loc);
 	cudaFree(ctx->d_bk_tmp);
@@ -831,9 +833,13 @@ static int bk_reserve(bbt_ctx *ctx, uint64_t frames, uint64_t cnt_entries)
 		cudaFree(ctx->d_bk_canon);
 		cudaFree(ctx->d_bk_off);
 		cudaFree(ctx->d_bk_fid);
+		cudaFree(ctx->d_bk_res);
+		cudaFree(ctx->d_bk_btot);
 		ctx->d_bk_vbits = ctx->d_bk_hbits = ctx->d_bk_abits = ctx->d_bk_off = nullptr;
+		ctx->d_bk_btot = nullptr;
 		ctx->d_bk_canon = nullptr;
 		ctx->d_bk_fid = nullptr;
+		ctx->d_bk_res = nullptr;
 		ctx->bk_frames_cap = 0;
 		/* whole window blocks, plus spare words for reads across the end */
 		const uint64_t f = (frames + kBkWinFrames - 1) / kBkWinFrames * kBkWinFrames;
@@ -845,6 +851,8 @@ static int bk_reserve(bbt_ctx *ctx, uint64_t frames, uint64_t cnt_entries)
 		const uint64_t pool = f * std::max<uint32_t>(ctx->bk_levels, 1);
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_off, pool * sizeof(uint32_t)));
 		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_fid, pool * sizeof(uint16_t)));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_res, pool));
+		CUDA_TRY(ctx, cudaMalloc(&ctx->d_bk_btot, (f / kBkWinFrames) * sizeof(uint32_t)));
 		ctx->bk_frames_cap = f;
 		ctx->bk_pool_levels = std::max<uint32_t>(ctx->bk_levels, 1);
 	}
@@ -1090,6 +1098,8 @@ static int run_bucketed(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 			b.cap = (uint64_t)kBkWinFrames * ctx->bk_pool_levels;
 			b.req_off = ctx->d_bk_off;
 			b.req_fid = ctx->d_bk_fid;
+			b.res = ctx->d_bk_res;
+			b.btot = ctx->d_bk_btot;
 			b.issued = a.probes;
 			for (const auto &ph : phases) {
 				b.ph_lo = ph.first;
@@ -1103,8 +1113,9 @@ static int run_bucketed(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 						CUDA_TRY(ctx, launch_bk_emit(b, s));
 					CUDA_TRY(ctx, launch_bk_resolve(b, ctx->num_sms, s));
 				}
+				CUDA_TRY(ctx, launch_bk_apply(b, s));
 				CUDA_TRY(ctx, launch_bk_walk(b, ctx->num_sms, s));
-				ctx->last.kernels += 2 * (uint32_t)rounds.size() + 1;
+				ctx->last.kernels += 2 * (uint32_t)rounds.size() + 2;
 			}
 		}
 	}

@@ -32,11 +32,15 @@
  *             to the block's region of the request pool in bucket order;
  *   resolve-- the (bucket, block) segments in bucket-major order, one warp per
  *             segment: each request's bit is tested out of the bucket held in
- *             L2, and a failed test clears its frame's hit bit;
- *   emit   -- (the later rounds) the block's frames still hits request their
- *             next levels from their kept hashes, as above, then resolve;
- * and after the last round one thread per undecided read walks SeqEval over
- * [0, phase end) of its frames.
+ *             L2, its result written as a byte beside it (the frames' hit
+ *             bits, spread over the whole sub-batch, are not touched here, so
+ *             that the bucket keeps L2 to itself);
+ *   emit   -- (the later rounds) per block, the previous round's results
+ *             clear the hit bits of the frames that failed, then the frames
+ *             still hits request their next levels from their kept hashes,
+ *             as above, then resolve;
+ * and after the last round (its results applied the same way) one thread per
+ * undecided read walks SeqEval over [0, phase end) of its frames.
  */
 #include "bucketed.cuh"
 
@@ -295,7 +299,9 @@ __device__ void bk_scatter(const BucketArgs &b, const SweepSmem &sm, uint32_t *t
 	for (uint32_t q = t; q < b.nbkt; q += kNT)
 		sm.loc[q] = sm.hist[q];
 	__syncthreads();
-	block_exscan(sm.loc, b.nbkt, tmp);
+	const uint32_t total = block_exscan(sm.loc, b.nbkt, tmp);
+	if (t == 0)
+		b.btot[blk] = total;
 	for (uint32_t q = t; q < b.nbkt; q += kNT) {
 		b.cnt[(uint64_t)q * b.nblk + blk] = sm.hist[q];
 		b.loc[(uint64_t)q * b.nblk + blk] = sm.loc[q];
@@ -494,9 +500,33 @@ __global__ void __launch_bounds__(kNT) bk_hash_kernel(BucketArgs b)
 	bk_scatter(b, sm, tmp);
 }
 
-/* A later round, per window block: the frames requesting in this phase that
- * are still hits count their requests of levels [level, level + nlevels) per
- * bucket, then bk_scatter. */
+/* The previous round's results of block blk applied to its hit bits: sh (the
+ * block's words, loaded) loses the bits of the frames with a failed test and
+ * goes back to b.hbits. */
+__device__ void bk_apply_block(const BucketArgs &b, uint32_t *sh)
+{
+	const uint32_t blk = blockIdx.x, t = threadIdx.x;
+	const uint64_t wbase = (uint64_t)blk * kWinWords;
+	const uint64_t words = (b.T + 31) / 32;
+	for (uint32_t w = t; w < kWinWords; w += kNT)
+		sh[w] = wbase + w < words ? b.hbits[wbase + w] : 0u;
+	__syncthreads();
+	const uint64_t base = (uint64_t)blk * b.cap;
+	const uint32_t n = b.btot[blk];
+	for (uint32_t i = t; i < n; i += kNT)
+		if (!__ldcs(b.res + base + i)) {
+			const uint32_t fid = __ldcs(b.req_fid + base + i);
+			atomicAnd(&sh[fid >> 5], ~(1u << (fid & 31u)));
+		}
+	__syncthreads();
+	for (uint32_t w = t; w < kWinWords; w += kNT)
+		if (wbase + w < words)
+			b.hbits[wbase + w] = sh[w];
+}
+
+/* A later round, per window block: the previous round's results applied,
+ * then the frames requesting in this phase that are still hits count their
+ * requests of levels [level, level + nlevels) per bucket, then bk_scatter. */
 __global__ void __launch_bounds__(kNT) bk_emit_kernel(BucketArgs b)
 {
 	extern __shared__ uint32_t bk_sm[];
@@ -506,8 +536,9 @@ __global__ void __launch_bounds__(kNT) bk_emit_kernel(BucketArgs b)
 	const uint64_t w0 = (uint64_t)blk * kBkWinFrames;
 	const uint64_t wbase = (uint64_t)blk * kWinWords;
 	const uint64_t words = (b.T + 31) / 32;
+	bk_apply_block(b, sm.sv);
 	for (uint32_t w = t; w < kWinWords; w += kNT)
-		sm.sa[w] = wbase + w < words ? b.abits[wbase + w] & b.hbits[wbase + w] : 0u;
+		sm.sa[w] = wbase + w < words ? b.abits[wbase + w] & sm.sv[w] : 0u;
 	for (uint32_t q = t; q < b.nbkt; q += kNT)
 		sm.hist[q] = 0;
 	__syncthreads();
@@ -527,10 +558,16 @@ __global__ void __launch_bounds__(kNT) bk_emit_kernel(BucketArgs b)
 	bk_scatter(b, sm, tmp);
 }
 
+__global__ void __launch_bounds__(kNT) bk_apply_kernel(BucketArgs b)
+{
+	__shared__ uint32_t sh[kWinWords];
+	bk_apply_block(b, sh);
+}
+
 /* The round's (bucket, block) segments in bucket-major order, one warp per
  * segment and eight requests per lane in flight; the bucket being tested is
- * held in L2, the pool is read once (streaming).  A failed test clears the
- * frame's hit bit. */
+ * held in L2, the pool is read once and the results written once
+ * (streaming). */
 __global__ void __launch_bounds__(256) bk_resolve_kernel(BucketArgs b)
 {
 	const uint32_t lane = threadIdx.x & 31u;
@@ -556,30 +593,26 @@ __global__ void __launch_bounds__(256) bk_resolve_kernel(BucketArgs b)
 		const uint32_t q = (uint32_t)(cur / b.nblk);
 		const uint32_t blk = (uint32_t)(cur - (uint64_t)q * b.nblk);
 		const uint64_t base = (uint64_t)blk * b.cap + lc;
-		const uint64_t fbase = (uint64_t)blk * kBkWinFrames;
 		const uint64_t qbase = (uint64_t)q << sh;
 		issued += n;
 		for (uint32_t c = 0; c < n; c += 256) {
-			uint32_t off[8], fid[8], w[8];
+			uint32_t off[8], w[8];
 #pragma unroll
 			for (int j = 0; j < 8; ++j) {
 				const uint32_t i = c + (uint32_t)j * 32 + lane;
-				off[j] = 0;
-				fid[j] = 0xffffffffu;
-				if (i < n) {
-					off[j] = __ldcs(b.req_off + base + i);
-					fid[j] = __ldcs(b.req_fid + base + i);
-				}
+				off[j] = i < n ? __ldcs(b.req_off + base + i) : 0u;
 			}
 #pragma unroll
-			for (int j = 0; j < 8; ++j)
-				w[j] = fid[j] != 0xffffffffu ? __ldg(words + ((qbase + off[j]) >> 5)) : ~0u;
+			for (int j = 0; j < 8; ++j) {
+				const uint32_t i = c + (uint32_t)j * 32 + lane;
+				w[j] = i < n ? __ldg(words + ((qbase + off[j]) >> 5)) : 0u;
+			}
 #pragma unroll
-			for (int j = 0; j < 8; ++j)
-				if (!((w[j] >> (off[j] & 31u)) & 1u)) {
-					const uint64_t x = fbase + fid[j];
-					atomicAnd(&b.hbits[x >> 5], ~(1u << (uint32_t)(x & 31u)));
-				}
+			for (int j = 0; j < 8; ++j) {
+				const uint32_t i = c + (uint32_t)j * 32 + lane;
+				if (i < n)
+					__stcs(b.res + base + i, (uint8_t)((w[j] >> (off[j] & 31u)) & 1u));
+			}
 		}
 	}
 	if (b.issued && lane == 0 && issued)
@@ -730,6 +763,14 @@ cudaError_t launch_bk_resolve(const BucketArgs &b, int num_sms, cudaStream_t s)
 	if (e != cudaSuccess)
 		return e;
 	bk_resolve_kernel<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, 0, s>>>(b);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_bk_apply(const BucketArgs &b, cudaStream_t s)
+{
+	if (b.nblk == 0)
+		return cudaSuccess;
+	bk_apply_kernel<<<b.nblk, kNT, 0, s>>>(b);
 	return cudaGetLastError();
 }
 

@@ -54,6 +54,8 @@ struct BucketArgs {
 	uint64_t cap;              /* pool slots per window block */
 	uint32_t *req_off;         /* request pool: bit offset inside the bucket */
 	uint16_t *req_fid;         /*   frame id inside the window block */
+	uint8_t *res;              /*   test result (1 = bit set) */
+	uint32_t *btot;            /* requests of this round per window block */
 	unsigned long long *issued;/* optional: requests resolved (bit tests issued) */
 };
 
@@ -71,12 +73,14 @@ cudaError_t launch_bk_pack(const uint8_t *ascii, uint64_t len, uint32_t *words, 
  * validity / hit / requesting bits, keep their canonical hashes and write
  * their level-0 requests, sorted by bucket in each block's region. */
 cudaError_t launch_bk_hash(const BucketArgs &b, cudaStream_t s);
-/* A later round: requests of the frames still hits, levels
- * [level, level + nlevels). */
+/* A later round: the previous round's results applied to the hit bits, then
+ * requests of the frames still hits, levels [level, level + nlevels). */
 cudaError_t launch_bk_emit(const BucketArgs &b, cudaStream_t s);
-/* A round's bit tests, bucket by bucket (the bucket held in L2); a failed
- * test clears its frame's hit bit. */
+/* A round's bit tests, bucket by bucket (the bucket held in L2), one result
+ * byte per request. */
 cudaError_t launch_bk_resolve(const BucketArgs &b, int num_sms, cudaStream_t s);
+/* The last round's results applied to the hit bits. */
+cudaError_t launch_bk_apply(const BucketArgs &b, cudaStream_t s);
 /* SeqEval over [0, bound(F, ph_hi)) of every open read; accepted reads set
  * their hit bit; reads decided or fully walked are closed. */
 cudaError_t launch_bk_walk(const BucketArgs &b, int num_sms, cudaStream_t s);

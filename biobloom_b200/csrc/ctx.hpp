@@ -131,6 +131,8 @@ struct bbt_ctx {
 	uint64_t *d_bk_canon = nullptr;
 	uint32_t *d_bk_off = nullptr;
 	uint16_t *d_bk_fid = nullptr;
+	uint8_t *d_bk_res = nullptr;
+	uint32_t *d_bk_btot = nullptr;
 	uint64_t bk_frames_cap = 0;
 	uint32_t bk_pool_levels = 0;          /* tests per frame the pool holds */
 	uint32_t *d_bk_cnt = nullptr, *d_bk_loc = nullptr;
@@ -138,8 +140,8 @@ struct bbt_ctx {
 	void *d_bk_tmp = nullptr;
 	size_t bk_tmp_cap = 0;
 	uint64_t bk_max_frames = 1ull << 30; /* frames per sub-batch */
-	uint32_t bk_bshift = 28;             /* bucket of 2^28 bits (32 MB) */
-	uint32_t bk_phase_split = 8;         /* phase boundary in sixteenths (16: one phase) */
+	uint32_t bk_bshift = 27;             /* bucket of 2^27 bits (16 MB) */
+	uint32_t bk_phase_split = 4;         /* phase boundary in sixteenths (16: one phase) */
 	uint32_t bk_phase_min = 64;          /* the first phase covers min(F, 64) frames or more */
 	uint32_t bk_levels = 1;              /* hash levels per round */
 	/* bbt_open_devices: the same filters opened on the other devices; host

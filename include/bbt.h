@@ -325,14 +325,15 @@ int bbt_set_schedule(bbt_ctx *ctx, uint64_t long_bases);
 
 /* Settings of the bucketed path (BBT_PATH_BUCKETED): each round's requests
  * are resolved one bucket of 2^bucket_shift filter bits at a time (a bucket
- * should fit L2: 28 = 32 MB); a read's frames are resolved in two phases split
- * at phase_split / 16 of its frames (16 = one phase), the first covering at
- * least min(frames, phase_min) frames; at most max_frames frames per
- * sub-batch (scratch: about 8.4 + 6 x levels_per_round bytes per frame);
- * each round tests levels_per_round hash levels (1 to 64: the first round
- * levels [0, L), the next [L, 2L), ...; a frame requests a round's levels
- * only when it passed all earlier ones).  0 keeps a setting.  Results do not
- * depend on them.  No reference counterpart. */
+ * should fit L2: the default 27 = 16 MB); a read's frames are resolved in two
+ * phases split at phase_split / 16 of its frames (default 4; 16 = one phase),
+ * the first covering at least min(frames, phase_min) frames (default 64); at
+ * most max_frames frames per sub-batch (default 2^30; scratch: about
+ * 8.4 + 7 x levels_per_round bytes per frame); each round tests
+ * levels_per_round hash levels (1 to 64, default 1: the first round levels
+ * [0, L), the next [L, 2L), ...; a frame requests a round's levels only when
+ * it passed all earlier ones).  0 keeps a setting.  Results do not depend on
+ * them.  No reference counterpart. */
 int bbt_set_bucketing(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
 		unsigned phase_min, uint64_t max_frames, unsigned levels_per_round);
 
