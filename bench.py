@@ -1011,6 +1011,10 @@ def run_single(args):
         tune = {"path": pinned, "warps_per_block": 8, "frames_per_lane": 4,
                 "long_bases": 1024 if pinned == L.PATH_PERSISTENT else 0,
                 "reads_per_launch": 0, "reads_per_s": None, "pinned": True}
+        if args.bucketing:
+            kv = {x.split("=")[0].strip(): int(x.split("=")[1]) for x in args.bucketing.split(",")}
+            bbc.set_bucketing(**kv)
+            tune["bucketing"] = kv
     log(f"autotune: {tune}")
     if tune["path"] == L.PATH_FILTER_MAJOR:  # one filter never picks it
         bbc.set_launch(path=L.PATH_PERSISTENT)
@@ -1785,6 +1789,9 @@ def main():
     ap.add_argument("--layout", type=int, default=0, help="miBF layout: 0 auto, 1 rank, 2 dense")
     ap.add_argument("--path", default="auto", choices=["auto", "persistent", "bucketed"],
                     help="batched path of the single-filter workloads (default: autotuned)")
+    ap.add_argument("--bucketing", default="",
+                    help="settings of the bucketed path, e.g. 'bucket_shift=27,phase_split=4,"
+                         "levels_per_round=1' (bbt_set_bucketing; --path bucketed)")
     args = ap.parse_args()
     args.reads_set = args.reads is not None
     if args.reads is None:

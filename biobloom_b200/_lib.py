@@ -202,6 +202,7 @@ def lib():
         "bbt_mibf_frame_probs": (i32, [vp, P(dbl), P(dbl)]),
         "bbt_mibf_classify_batch": (i32, [vp, P(Batch), P(MibfResult), vp]),
         "bbt_mibf_sync": (i32, [vp]),
+        "bbt_mibf_set_bucketing": (i32, [vp, i32, u32, u64]),
         "bbt_mibf_last_kernel_ms": (dbl, [vp]),
         "bbt_mibf_last_counts": (i32, [vp, P(u64)]),
         "bbt_mibf_summary": (i32, [vp, P(u64), P(u64)]),

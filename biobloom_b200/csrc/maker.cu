@@ -265,9 +265,12 @@ extern "C" int bbt_make_filter(const char *seq, const uint64_t *offsets, uint64_
 		hd.m = m;
 		hd.h = h;
 		hd.k = k;
-		hd.dfpr = fpr;
-		hd.n_entry = cnt[0];
-		hd.t_entry = cnt[0] + cnt[1];
+		/* the reference maker stores a BloomFilter built from (size, hash
+		 * count, k) (BloomFilterGenerator.cpp:63-71), whose FPR and entry
+		 * fields the header carries as 0; the counts go to the .txt file */
+		hd.dfpr = 0;
+		hd.n_entry = 0;
+		hd.t_entry = 0;
 		std::string bf = std::string(stem) + ".bf";
 		FILE *f = fopen(bf.c_str(), "wb");
 		if (!f) {

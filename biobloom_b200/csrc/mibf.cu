@@ -41,6 +41,7 @@
 #include <vector>
 
 #include "bbt_device.cuh"
+#include "bucketed.cuh"
 #include "mibf_ctx.hpp"
 #include "window.cuh"
 
@@ -83,6 +84,14 @@ struct MibfArgs {
 	uint32_t T;                 /* tally slots per warp, a multiple of 32 */
 	unsigned long long *gtally; /* more than kMibfSmemIds IDs: per-warp tally tables in
 	                               global memory (3 x T words each), zero between reads */
+	/* bucketed query (PRE kernels): the entries of every frame resolved
+	 * beforehand, frame order (h per frame), their validity bits, and the
+	 * frame offsets of these reads (pre_fo[r] - pre_fo0 = first frame of
+	 * read r) */
+	const uint16_t *pre_e;
+	const uint32_t *pre_valid;
+	const uint64_t *pre_fo;
+	uint64_t pre_fo0;
 };
 
 /* IDs a read may touch before a warp with global tally tables clears and scans
@@ -215,11 +224,11 @@ __device__ __forceinline__ bool frame_word(const uint64_t *cw, const uint32_t *i
 
 /* The h values of a frame (seed hashes, or ntHash and its extra hashes). */
 template <int H>
-__device__ __forceinline__ void frame_values(const MibfArgs &a, const ulonglong2 *tab, bool ok,
+__device__ __forceinline__ void frame_values(const MibfDev &f, const ulonglong2 *tab, bool ok,
 		uint64_t w, uint64_t *vals)
 {
-	const uint32_t k = a.f.k, h = a.f.h;
-	if (a.f.kmer_mode) {
+	const uint32_t k = f.k, h = f.h;
+	if (f.kmer_mode) {
 		const uint64_t c = ok ? (BBT_MIBF_PAIR_TABLES ? seed_value_pairs(tab, w, k)
 		                                              : seed_value(tab, w, k)) : 0;
 		vals[0] = c;
@@ -396,7 +405,7 @@ __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglon
 			for (int f = 0; f < FPL; ++f) {
 				uint64_t w;
 				ok[f] = frame_word(cw, iw, q0 + 32 * f + lane, nfr, kmask, w);
-				frame_values<H>(a, tab, ok[f], w, vals[f]);
+				frame_values<H>(a.f, tab, ok[f], w, vals[f]);
 			}
 			if (DENSE) {
 #pragma unroll
@@ -420,13 +429,40 @@ __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglon
 	__syncwarp();
 }
 
+/* The frames [x0, x0 + nfr) of one mate with their entries resolved
+ * beforehand (a.pre_e, dense-layout values: 0 for a clear bit), one frame per
+ * lane per step, tallied as mibf_scan_mate tallies them. */
+template <int H>
+__device__ __forceinline__ void mibf_scan_pre(const MibfArgs &a, uint64_t x0, uint32_t nfr,
+		unsigned long long *TA, unsigned long long *TB, unsigned long long *TC, uint32_t &satc,
+		LaneCounts &lc, int lane, uint32_t *tlist)
+{
+	const uint32_t h = a.f.h;
+	for (uint32_t q0 = 0; q0 < nfr; q0 += 32) {
+		const uint32_t q = q0 + lane;
+		bool ok = false;
+		uint32_t e[H];
+		bool hit[H];
+		const uint64_t x = x0 + q;
+		if (q < nfr)
+			ok = (__ldg(a.pre_valid + (x >> 5)) >> (x & 31u)) & 1u;
+#pragma unroll
+		for (int v = 0; v < H; ++v) {
+			e[v] = (ok && v < (int)h) ? __ldg(a.pre_e + x * h + v) : 0u;
+			hit[v] = e[v] != 0;
+		}
+		frame_tally<H>(a, ok, e, hit, TA, TB, TC, satc, lc, lane, tlist);
+	}
+}
+
 /*
  * BIG (more than kMibfSmemIds IDs): each warp's tally table lives in global
  * memory (a.gtally, zero between reads) and the warp lists the IDs the read
  * touches (tlist in shared memory); candidates are looked for, and the table
  * is cleared, over that list (over every slot when the list overflowed).
+ * PRE: the frames' entries come resolved (the bucketed query, dense layout).
  */
-template <int H, bool DENSE, int FPL, bool BIG>
+template <int H, bool DENSE, int FPL, bool BIG, bool PRE>
 __global__ void __launch_bounds__(kQueryThreads, kQueryMinBlocks) mibf_query_kernel(MibfArgs a)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
@@ -478,7 +514,14 @@ __global__ void __launch_bounds__(kQueryThreads, kQueryMinBlocks) mibf_query_ker
 			const uint32_t fc = len1 >= k ? (uint32_t)(len1 - k + 1)
 					: (len2 >= k ? (uint32_t)(len2 - k + 1) : 0u);
 			uint32_t satc = 0;
-			if (fc) {
+			if (fc && PRE) {
+				const uint64_t x = a.pre_fo[r] - a.pre_fo0;
+				const uint32_t f1 = len1 >= k ? (uint32_t)(len1 - k + 1) : 0u;
+				const uint32_t f2 = len2 >= k ? (uint32_t)(len2 - k + 1) : 0u;
+				mibf_scan_pre<H>(a, x, f1, TA, TB, TC, satc, lc, lane, tlist);
+				if (a.seq2)
+					mibf_scan_pre<H>(a, x + f1, f2, TA, TB, TC, satc, lc, lane, tlist);
+			} else if (fc) {
 				mibf_scan_mate<H, DENSE, FPL>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1,
 						satc, lc, lane, tlist);
 				if (a.seq2)
@@ -702,6 +745,341 @@ __global__ void mibf_dense_build_kernel(const uint64_t *raw, uint64_t m,
 	}
 }
 
+/* ---- bucketed query (dense layout) ----
+ *
+ * Every probe of the query is known once a read is hashed (MIBFQuerySupport
+ * visits every frame), so the probes of a sub-batch of reads can be sorted by
+ * address before any is made.  The dense ID map is cut into buckets of
+ * 2^bshift entries that fit L2:
+ *   hash     -- per window block of W frames (W * h <= kMbkRequests): every
+ *               frame's h values, from the packed bases and the seed tables;
+ *               its validity bit; its requests (entry offset in the bucket)
+ *               staged in shared memory, counted per bucket, then written to
+ *               the block's region of the pool in bucket order with their
+ *               slot (frame * h + value) in the block;
+ *   resolve  -- the (bucket, block) segments in bucket-major order, 32
+ *               segments per warp: each request reads its entry out of the
+ *               bucket held in L2 and writes it beside the request;
+ *   unscatter-- per block, the entries go to their slots in shared memory and
+ *               out to the sub-batch's entry array in frame order;
+ * then the query kernel (PRE) tallies every read from those entries exactly
+ * as it does from its own probes.
+ */
+constexpr uint32_t kMbkThreads = 256;
+constexpr uint32_t kMbkRequests = 12288;
+constexpr uint32_t kMbkMaxBuckets = 2048;
+
+struct MbkArgs {
+	MibfDev f;
+	const unsigned long long *tables;
+	PackedBases pk[2];
+	const uint64_t *off, *off2;  /* the batch's base offsets (off2 NULL: single-end) */
+	uint64_t r0, nr;             /* reads [r0, r0 + nr) */
+	const uint64_t *fo;          /* frame offsets of the batch's reads (both mates) */
+	uint64_t fo0, T;             /* fo[r0]; frames of the sub-batch */
+	uint32_t W, nblk, nbkt, bshift;
+	uint32_t *valid;             /* frame validity bits of the sub-batch */
+	uint16_t *e;                 /* entries of the sub-batch, T * h */
+	uint32_t *cnt, *loc, *btot;  /* per (bucket, block): requests, first slot; per block */
+	uint64_t cap;                /* pool slots per block: W * h */
+	uint32_t *req_off;           /* pool: entry offset inside the bucket */
+	uint16_t *req_slot;          /*   frame * h + value inside the block */
+	uint16_t *res;               /*   the entry read */
+};
+
+__device__ __forceinline__ uint64_t mbk_find_read(const MbkArgs &b, uint64_t x)
+{
+	uint64_t lo = b.r0, hi = b.r0 + b.nr; /* fo[lo] - fo0 <= x < fo[hi] - fo0 */
+	while (hi - lo > 1) {
+		const uint64_t mid = lo + (hi - lo) / 2;
+		if (b.fo[mid] - b.fo0 <= x)
+			lo = mid;
+		else
+			hi = mid;
+	}
+	return lo;
+}
+
+/* The 2-bit codes of 32 bases from base g (w, base j at bits 2j) and whether
+ * the k bases from g are all ACGT. */
+__device__ __forceinline__ bool mbk_frame(const PackedBases &p, uint64_t g, unsigned k,
+		uint64_t &w)
+{
+	const uint64_t i = g >> 4;
+	const uint32_t s = (uint32_t)(g & 15u) * 2u;
+	const uint32_t w0 = i < p.nwords ? __ldg(p.words + i) : 0u;
+	const uint32_t w1 = i + 1 < p.nwords ? __ldg(p.words + i + 1) : 0u;
+	const uint32_t w2 = i + 2 < p.nwords ? __ldg(p.words + i + 2) : 0u;
+	const uint64_t lo = (uint64_t)w0 | ((uint64_t)w1 << 32);
+	w = s ? (lo >> s) | ((uint64_t)w2 << (64u - s)) : lo;
+	if (!p.valid)
+		return true;
+	const uint64_t vi = g >> 5;
+	const uint32_t v0 = vi < p.nvalid ? __ldg(p.valid + vi) : 0u;
+	const uint32_t v1 = vi + 1 < p.nvalid ? __ldg(p.valid + vi + 1) : 0u;
+	const uint32_t v = __funnelshift_r(v0, v1, (uint32_t)(g & 31u));
+	const uint32_t km = k >= 32 ? 0xffffffffu : ((1u << k) - 1u);
+	return (~v & km) == 0;
+}
+
+/* In-place exclusive scan of v[0, n) in shared memory by the whole block
+ * (blockDim.x == kMbkThreads); returns the total.  tmp: 33 words. */
+__device__ uint32_t mbk_exscan(uint32_t *v, uint32_t n, uint32_t *tmp)
+{
+	const uint32_t t = threadIdx.x;
+	const uint32_t per = (n + kMbkThreads - 1) / kMbkThreads;
+	const uint32_t a0 = min(n, t * per), z = min(n, a0 + per);
+	uint32_t sum = 0;
+	for (uint32_t i = a0; i < z; ++i)
+		sum += v[i];
+	const uint32_t lane = t & 31u, wid = t >> 5;
+	uint32_t inc = sum;
+#pragma unroll
+	for (uint32_t d = 1; d < 32; d <<= 1) {
+		const uint32_t y = __shfl_up_sync(kFull, inc, d);
+		if (lane >= d)
+			inc += y;
+	}
+	if (lane == 31)
+		tmp[wid] = inc;
+	__syncthreads();
+	if (wid == 0) {
+		const uint32_t wv = lane < kMbkThreads / 32 ? tmp[lane] : 0u;
+		uint32_t wi = wv;
+#pragma unroll
+		for (uint32_t d = 1; d < 32; d <<= 1) {
+			const uint32_t y = __shfl_up_sync(kFull, wi, d);
+			if (lane >= d)
+				wi += y;
+		}
+		__syncwarp();
+		tmp[lane] = wi - wv;
+		if (lane == 31)
+			tmp[32] = wi;
+	}
+	__syncthreads();
+	uint32_t run = tmp[wid] + inc - sum;
+	for (uint32_t i = a0; i < z; ++i) {
+		const uint32_t x = v[i];
+		v[i] = run;
+		run += x;
+	}
+	const uint32_t total = tmp[32];
+	__syncthreads();
+	return total;
+}
+
+/* Shared memory of the hash kernel: seed tables, staged requests (offset,
+ * bucket), counts and first slots per bucket, validity words. */
+__host__ __device__ inline size_t mbk_hash_smem(uint32_t nse, uint32_t W, uint32_t h,
+		uint32_t nbkt)
+{
+	const size_t req = (size_t)W * h;
+	return (size_t)nse * kTabEntries * 16 + req * 4 + ((req * 2 + 15) & ~(size_t)15) +
+			(size_t)nbkt * 8 + (size_t)(W / 32) * 4;
+}
+
+template <int H>
+__global__ void __launch_bounds__(kMbkThreads) mbk_hash_kernel(MbkArgs b)
+{
+	extern __shared__ __align__(16) unsigned char smem[];
+	const uint32_t nse = b.f.nse, h = b.f.h, W = b.W, k = b.f.k, t = threadIdx.x;
+	const uint32_t blk = blockIdx.x, nreq = W * h;
+	unsigned long long *tabw = reinterpret_cast<unsigned long long *>(smem);
+	for (uint32_t i = t; i < nse * kTabEntries * 2; i += kMbkThreads)
+		tabw[i] = b.tables[i];
+	const ulonglong2 *tab = reinterpret_cast<const ulonglong2 *>(smem);
+	uint32_t *st_off = reinterpret_cast<uint32_t *>(smem + (size_t)nse * kTabEntries * 16);
+	uint16_t *st_bkt = reinterpret_cast<uint16_t *>(st_off + nreq);
+	uint32_t *hist = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(st_bkt) +
+			(((size_t)nreq * 2 + 15) & ~(size_t)15));
+	uint32_t *locs = hist + b.nbkt;
+	uint32_t *vw = locs + b.nbkt;
+	__shared__ uint32_t tmp[33];
+	for (uint32_t q = t; q < b.nbkt; q += kMbkThreads)
+		hist[q] = 0;
+	for (uint32_t i = t; i < W / 32; i += kMbkThreads)
+		vw[i] = 0;
+	const uint64_t w0 = (uint64_t)blk * W;
+	const uint64_t w1 = min(w0 + W, b.T);
+	/* slots of frames past the sub-batch's end request nothing */
+	for (uint32_t j = (uint32_t)(w1 - w0) * h + t; j < nreq; j += kMbkThreads)
+		st_bkt[j] = 0xffffu;
+	__syncthreads();
+	const uint32_t R = W / kMbkThreads;
+	const uint64_t x0 = w0 + (uint64_t)t * R;
+	const unsigned sh = b.bshift;
+	const uint64_t mask = (1ull << sh) - 1ull;
+	if (x0 < w1) {
+		const uint64_t x1 = min(x0 + R, w1);
+		uint64_t r = mbk_find_read(b, x0);
+		for (uint64_t x = x0; x < x1; ++x) {
+			while (b.fo[r + 1] - b.fo0 <= x)
+				++r;
+			const uint64_t q = x - (b.fo[r] - b.fo0);
+			const uint64_t len1 = b.off[r + 1] - b.off[r];
+			const uint64_t f1 = len1 >= k ? len1 - k + 1 : 0;
+			const uint32_t mate = q >= f1 ? 1u : 0u;
+			const uint64_t g = (mate ? b.off2[r] : b.off[r]) + (mate ? q - f1 : q);
+			uint64_t w;
+			const bool ok = mbk_frame(b.pk[mate], g, k, w);
+			uint64_t vals[H];
+			frame_values<H>(b.f, tab, ok, w, vals);
+			const uint32_t fid = (uint32_t)(x - w0);
+			if (ok)
+				atomicOr(&vw[fid >> 5], 1u << (fid & 31u));
+#pragma unroll
+			for (int v = 0; v < H; ++v) {
+				if (v < (int)h) {
+					const uint32_t j = fid * h + v;
+					if (ok) {
+						const uint64_t pos = reduce(vals[v], b.f.m, b.f.minv);
+						const uint32_t bk = (uint32_t)(pos >> sh);
+						st_off[j] = (uint32_t)(pos & mask);
+						st_bkt[j] = (uint16_t)bk;
+						atomicAdd(&hist[bk], 1u);
+					} else {
+						st_bkt[j] = 0xffffu;
+					}
+				}
+			}
+		}
+	}
+	__syncthreads();
+	const uint64_t vbase = w0 / 32, nv = (b.T + 31) / 32;
+	for (uint32_t i = t; i < W / 32; i += kMbkThreads)
+		if (vbase + i < nv)
+			b.valid[vbase + i] = vw[i];
+	for (uint32_t q = t; q < b.nbkt; q += kMbkThreads)
+		locs[q] = hist[q];
+	__syncthreads();
+	const uint32_t total = mbk_exscan(locs, b.nbkt, tmp);
+	if (t == 0)
+		b.btot[blk] = total;
+	for (uint32_t q = t; q < b.nbkt; q += kMbkThreads) {
+		b.cnt[(uint64_t)q * b.nblk + blk] = hist[q];
+		b.loc[(uint64_t)q * b.nblk + blk] = locs[q];
+		hist[q] = 0;
+	}
+	__syncthreads();
+	const uint64_t base = (uint64_t)blk * b.cap;
+	for (uint32_t j = t; j < nreq; j += kMbkThreads) {
+		const uint32_t bk = st_bkt[j];
+		if (bk == 0xffffu)
+			continue;
+		const uint64_t i = base + locs[bk] + atomicAdd(&hist[bk], 1u);
+		b.req_off[i] = st_off[j];
+		b.req_slot[i] = (uint16_t)j;
+	}
+}
+
+/* The round's (bucket, block) segments in bucket-major order, 32 consecutive
+ * segments per warp (their requests taken 256 at a time, eight per lane in
+ * flight); the bucket being read is held in L2, the pool streams through. */
+__global__ void __launch_bounds__(256) mbk_resolve_kernel(MbkArgs b, const uint16_t *dense)
+{
+	__shared__ uint32_t spre[8][33];
+	__shared__ unsigned long long sbase[8][32];
+	__shared__ uint32_t sq[8][32];
+	const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
+	const uint64_t nseg = (uint64_t)b.nbkt * b.nblk;
+	const uint64_t ngroups = (nseg + 31) / 32;
+	const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+	const unsigned sh = b.bshift;
+	for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib; g < ngroups; g += warps) {
+		const uint64_t sg = g * 32 + lane;
+		uint32_t n = 0, lc = 0, q = 0, blk = 0;
+		if (sg < nseg) {
+			n = b.cnt[sg];
+			lc = b.loc[sg];
+			q = (uint32_t)(sg / b.nblk);
+			blk = (uint32_t)(sg - (uint64_t)q * b.nblk);
+		}
+		uint32_t inc = n;
+#pragma unroll
+		for (uint32_t d = 1; d < 32; d <<= 1) {
+			const uint32_t y = __shfl_up_sync(kFull, inc, d);
+			if (lane >= d)
+				inc += y;
+		}
+		const uint32_t total = __shfl_sync(kFull, inc, 31);
+		spre[wib][lane] = inc - n;
+		if (lane == 31)
+			spre[wib][32] = inc;
+		sbase[wib][lane] = (uint64_t)blk * b.cap + lc;
+		sq[wib][lane] = q;
+		__syncwarp();
+		for (uint32_t c = 0; c < total; c += 256) {
+			uint32_t off[8], qq[8];
+			uint64_t idx[8];
+#pragma unroll
+			for (int j = 0; j < 8; ++j) {
+				const uint32_t i = c + (uint32_t)j * 32 + lane;
+				off[j] = 0;
+				qq[j] = 0;
+				idx[j] = ~0ull;
+				if (i < total) {
+					uint32_t lo = 0, hi = 32; /* spre[lo] <= i < spre[lo + 1] */
+					while (hi - lo > 1) {
+						const uint32_t mid = (lo + hi) >> 1;
+						if (spre[wib][mid] <= i)
+							lo = mid;
+						else
+							hi = mid;
+					}
+					idx[j] = sbase[wib][lo] + (i - spre[wib][lo]);
+					qq[j] = sq[wib][lo];
+					off[j] = __ldcs(b.req_off + idx[j]);
+				}
+			}
+			uint16_t e[8];
+#pragma unroll
+			for (int j = 0; j < 8; ++j)
+				e[j] = idx[j] != ~0ull ? __ldg(dense + (((uint64_t)qq[j] << sh) + off[j])) : 0;
+#pragma unroll
+			for (int j = 0; j < 8; ++j)
+				if (idx[j] != ~0ull)
+					__stcs(b.res + idx[j], e[j]);
+		}
+		__syncwarp();
+	}
+}
+
+/* Per block: the entries read go to their slots (shared memory), then out to
+ * the sub-batch's entry array in frame order; slots with no request (frames
+ * not valid) stay 0. */
+__global__ void __launch_bounds__(256) mbk_unscatter_kernel(MbkArgs b)
+{
+	extern __shared__ uint16_t se[];
+	const uint32_t h = b.f.h, blk = blockIdx.x, t = threadIdx.x;
+	const uint32_t nreq = b.W * h;
+	for (uint32_t j = t; j < nreq; j += blockDim.x)
+		se[j] = 0;
+	__syncthreads();
+	const uint64_t base = (uint64_t)blk * b.cap;
+	const uint32_t n = b.btot[blk];
+	for (uint32_t i = t; i < n; i += blockDim.x)
+		se[__ldcs(b.req_slot + base + i)] = __ldcs(b.res + base + i);
+	__syncthreads();
+	const uint64_t w0 = (uint64_t)blk * b.W;
+	const uint64_t w1 = min(w0 + b.W, b.T);
+	const uint32_t m = (uint32_t)(w1 - w0) * h;
+	for (uint32_t j = t; j < m; j += blockDim.x)
+		b.e[w0 * h + j] = se[j];
+}
+
+/* fo_plus1[r] = frames of read (pair) r: both mates. */
+__global__ void mbk_frames_kernel(const uint64_t *off, const uint64_t *off2, uint64_t n,
+		unsigned k, uint64_t *fo_plus1)
+{
+	for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n;
+			r += (uint64_t)gridDim.x * blockDim.x) {
+		const uint64_t l1 = off[r + 1] - off[r];
+		const uint64_t l2 = off2 ? off2[r + 1] - off2[r] : 0;
+		fo_plus1[r] = (l1 >= k ? l1 - k + 1 : 0) + (l2 >= k ? l2 - k + 1 : 0);
+	}
+}
+
 } // namespace bbt
 
 using namespace bbt;
@@ -735,57 +1113,61 @@ struct Fpl {
 	static constexpr int value = (D && H <= 4) ? BBT_MIBF_FPL : 1;
 };
 
-template <int H, bool D, bool B>
+template <int H, bool D, bool B, bool P = false>
 static cudaError_t launch_h(const MibfArgs &a, int grid, size_t smem, cudaStream_t s)
 {
-	mibf_query_kernel<H, D, Fpl<H, D>::value, B><<<grid, kQueryThreads, smem, s>>>(a);
+	mibf_query_kernel<H, D, Fpl<H, D>::value, B, P><<<grid, kQueryThreads, smem, s>>>(a);
 	return cudaGetLastError();
 }
 
 /* Blocks per SM of a variant with smem bytes of shared memory (also sets the
  * variant's shared-memory limit, which must precede its launch). */
-template <int H, bool D, bool B>
+template <int H, bool D, bool B, bool P = false>
 static int occupancy_h(size_t smem)
 {
-	auto kern = mibf_query_kernel<H, D, Fpl<H, D>::value, B>;
+	auto kern = mibf_query_kernel<H, D, Fpl<H, D>::value, B, P>;
 	cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 	int nb = 0;
 	cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, kQueryThreads, smem);
 	return nb > 0 ? nb : 1;
 }
 
-template <bool D, bool B>
+template <bool D, bool B, bool P = false>
 static cudaError_t launch_query_db(const MibfArgs &a, int hsel, int grid, size_t smem,
 		cudaStream_t s)
 {
 	switch (hsel) {
-	case 1: return launch_h<1, D, B>(a, grid, smem, s);
-	case 2: return launch_h<2, D, B>(a, grid, smem, s);
-	case 3: return launch_h<3, D, B>(a, grid, smem, s);
-	case 4: return launch_h<4, D, B>(a, grid, smem, s);
-	case 6: return launch_h<6, D, B>(a, grid, smem, s);
-	case 8: return launch_h<8, D, B>(a, grid, smem, s);
-	default: return launch_h<16, D, B>(a, grid, smem, s);
+	case 1: return launch_h<1, D, B, P>(a, grid, smem, s);
+	case 2: return launch_h<2, D, B, P>(a, grid, smem, s);
+	case 3: return launch_h<3, D, B, P>(a, grid, smem, s);
+	case 4: return launch_h<4, D, B, P>(a, grid, smem, s);
+	case 6: return launch_h<6, D, B, P>(a, grid, smem, s);
+	case 8: return launch_h<8, D, B, P>(a, grid, smem, s);
+	default: return launch_h<16, D, B, P>(a, grid, smem, s);
 	}
 }
 
-template <bool D, bool B>
+template <bool D, bool B, bool P = false>
 static int query_occupancy_db(int hsel, size_t smem)
 {
 	switch (hsel) {
-	case 1: return occupancy_h<1, D, B>(smem);
-	case 2: return occupancy_h<2, D, B>(smem);
-	case 3: return occupancy_h<3, D, B>(smem);
-	case 4: return occupancy_h<4, D, B>(smem);
-	case 6: return occupancy_h<6, D, B>(smem);
-	case 8: return occupancy_h<8, D, B>(smem);
-	default: return occupancy_h<16, D, B>(smem);
+	case 1: return occupancy_h<1, D, B, P>(smem);
+	case 2: return occupancy_h<2, D, B, P>(smem);
+	case 3: return occupancy_h<3, D, B, P>(smem);
+	case 4: return occupancy_h<4, D, B, P>(smem);
+	case 6: return occupancy_h<6, D, B, P>(smem);
+	case 8: return occupancy_h<8, D, B, P>(smem);
+	default: return occupancy_h<16, D, B, P>(smem);
 	}
 }
 
+/* pre: the bucketed query's tally kernel (dense layout only) */
 static cudaError_t launch_query(const MibfArgs &a, bool dense, bool big, int hsel, int grid,
-		size_t smem, cudaStream_t s)
+		size_t smem, cudaStream_t s, bool pre = false)
 {
+	if (pre)
+		return big ? launch_query_db<true, true, true>(a, hsel, grid, smem, s)
+		           : launch_query_db<true, false, true>(a, hsel, grid, smem, s);
 	if (big)
 		return dense ? launch_query_db<true, true>(a, hsel, grid, smem, s)
 		             : launch_query_db<false, true>(a, hsel, grid, smem, s);
@@ -793,8 +1175,11 @@ static cudaError_t launch_query(const MibfArgs &a, bool dense, bool big, int hse
 	             : launch_query_db<false, false>(a, hsel, grid, smem, s);
 }
 
-static int query_occupancy(bool dense, bool big, int hsel, size_t smem)
+static int query_occupancy(bool dense, bool big, int hsel, size_t smem, bool pre = false)
 {
+	if (pre)
+		return big ? query_occupancy_db<true, true, true>(hsel, smem)
+		           : query_occupancy_db<true, false, true>(hsel, smem);
 	if (big)
 		return dense ? query_occupancy_db<true, true>(hsel, smem)
 		             : query_occupancy_db<false, true>(hsel, smem);
@@ -972,6 +1357,22 @@ extern "C" int bbt_mibf_close(bbt_mibf *ctx)
 		cudaFree(ctx->d_hits);
 		cudaFree(ctx->d_nhits);
 		cudaFree(ctx->d_sat);
+		cudaFree(ctx->d_bk_fo);
+		cudaFreeHost(ctx->h_bk_samples);
+		cudaFree(ctx->d_bk_samples);
+		for (int m = 0; m < 2; ++m) {
+			cudaFree(ctx->d_bk_codes[m]);
+			cudaFree(ctx->d_bk_cvalid[m]);
+		}
+		cudaFree(ctx->d_bk_valid);
+		cudaFree(ctx->d_bk_e);
+		cudaFree(ctx->d_bk_off);
+		cudaFree(ctx->d_bk_slot);
+		cudaFree(ctx->d_bk_res);
+		cudaFree(ctx->d_bk_cnt);
+		cudaFree(ctx->d_bk_loc);
+		cudaFree(ctx->d_bk_btot);
+		cudaFree(ctx->d_bk_tmp);
 		for (int c = 0; c < 2; ++c) {
 			for (int m = 0; m < 2; ++m) {
 				cudaFree(ctx->c_seq[c][m]);
@@ -1203,6 +1604,213 @@ static int device_frame_counts(bbt_mibf *ctx, const bbt_batch *b, cudaStream_t s
 	return BBT_OK;
 }
 
+/* Device scratch of at least n elements (contents not kept). */
+template <class T>
+static int mbk_grow(bbt_mibf *ctx, T **p, uint64_t &cap, uint64_t n)
+{
+	if (n <= cap)
+		return BBT_OK;
+	cudaFree(*p);
+	*p = nullptr;
+	cap = 0;
+	MIBF_TRY(ctx, cudaMalloc(p, std::max<uint64_t>(n, 1) * sizeof(T)));
+	cap = n;
+	return BBT_OK;
+}
+
+template <int H>
+static cudaError_t mbk_launch_hash(const MbkArgs &b, size_t smem, cudaStream_t s)
+{
+	cudaError_t e = cudaFuncSetAttribute(mbk_hash_kernel<H>,
+			cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+	if (e != cudaSuccess)
+		return e;
+	mbk_hash_kernel<H><<<b.nblk, kMbkThreads, smem, s>>>(b);
+	return cudaGetLastError();
+}
+
+static cudaError_t mbk_hash(const MbkArgs &b, int hsel, size_t smem, cudaStream_t s)
+{
+	switch (hsel) {
+	case 1: return mbk_launch_hash<1>(b, smem, s);
+	case 2: return mbk_launch_hash<2>(b, smem, s);
+	case 3: return mbk_launch_hash<3>(b, smem, s);
+	case 4: return mbk_launch_hash<4>(b, smem, s);
+	case 6: return mbk_launch_hash<6>(b, smem, s);
+	case 8: return mbk_launch_hash<8>(b, smem, s);
+	default: return mbk_launch_hash<16>(b, smem, s);
+	}
+}
+
+/* Whether a call of n reads takes the bucketed query. */
+static bool mbk_wanted(const bbt_mibf *ctx, uint64_t n_reads)
+{
+	if (!ctx->d_dense || n_reads == 0 || ctx->bk_mode == 0)
+		return false;
+	return ctx->bk_mode == 1 || (2 * ctx->hd.m >= (256ull << 20) && n_reads >= (1ull << 20));
+}
+
+/*
+ * The bucketed query of n reads (the dense layout): frame offsets and a host
+ * plan of sub-batches (samples of the offsets, one short wait), the bases
+ * packed, then per sub-batch hash -> resolve -> unscatter -> the query kernel
+ * (PRE) over the sub-batch's reads, its results at their place in the call's
+ * arrays and its counters added to the batch's.  *done = false when the plan
+ * finds a read too long for any sub-batch (the caller then runs the direct
+ * kernel).
+ */
+static int run_query_bucketed(bbt_mibf *ctx, const MibfArgs &a, int hsel, bool big, int grid,
+		size_t smem, cudaStream_t s, bool *done)
+{
+	*done = false;
+	const uint64_t n = a.n_reads;
+	const unsigned k = a.f.k, h = a.f.h;
+	if (mbk_grow(ctx, &ctx->d_bk_fo, ctx->bk_fo_cap, n + 1))
+		return BBT_ERR_NOMEM;
+	MIBF_TRY(ctx, cudaMemsetAsync(ctx->d_bk_fo, 0, 8, s));
+	mbk_frames_kernel<<<ctx->num_sms * 8, 256, 0, s>>>(a.off, a.seq2 ? a.off2 : nullptr, n, k,
+			ctx->d_bk_fo + 1);
+	MIBF_TRY(ctx, cudaGetLastError());
+	size_t tb = 0;
+	MIBF_TRY(ctx, cub::DeviceScan::InclusiveSum(nullptr, tb, ctx->d_bk_fo + 1, ctx->d_bk_fo + 1,
+			(int64_t)n, s));
+	if (tb > ctx->bk_tmp_cap) {
+		cudaFree(ctx->d_bk_tmp);
+		ctx->d_bk_tmp = nullptr;
+		ctx->bk_tmp_cap = 0;
+		MIBF_TRY(ctx, cudaMalloc(&ctx->d_bk_tmp, tb));
+		ctx->bk_tmp_cap = tb;
+	}
+	MIBF_TRY(ctx, cub::DeviceScan::InclusiveSum(ctx->d_bk_tmp, tb, ctx->d_bk_fo + 1,
+			ctx->d_bk_fo + 1, (int64_t)n, s));
+	/* fo[0], fo[S], ..., fo[n], then the end offset of each mate array; S reads
+	 * per sample, fewer for small batches */
+	const uint64_t S = std::min<uint64_t>(4096, std::max<uint64_t>(1, n / 256)), ns = n / S + 1;
+	if (ns + 3 > ctx->bk_samples_cap) {
+		cudaFreeHost(ctx->h_bk_samples);
+		cudaFree(ctx->d_bk_samples);
+		ctx->h_bk_samples = ctx->d_bk_samples = nullptr;
+		ctx->bk_samples_cap = 0;
+		MIBF_TRY(ctx, cudaMallocHost(&ctx->h_bk_samples, (ns + 3) * 8));
+		MIBF_TRY(ctx, cudaMalloc(&ctx->d_bk_samples, (ns + 3) * 8));
+		ctx->bk_samples_cap = ns + 3;
+	}
+	MIBF_TRY(ctx, launch_bk_samples(ctx->d_bk_fo, n, S, ctx->d_bk_samples, ns, ctx->num_sms, s));
+	MIBF_TRY(ctx, launch_bk_samples(ctx->d_bk_fo + n, 0, 0, ctx->d_bk_samples + ns, 1,
+			ctx->num_sms, s));
+	const uint32_t mates = a.seq2 ? 2 : 1;
+	const uint64_t *offm[2] = {a.off, a.off2};
+	const uint8_t *seqm[2] = {a.seq, a.seq2};
+	for (uint32_t m = 0; m < mates; ++m)
+		MIBF_TRY(ctx, launch_bk_samples(offm[m] + n, 0, 0, ctx->d_bk_samples + ns + 1 + m, 1,
+				ctx->num_sms, s));
+	MIBF_TRY(ctx, cudaMemcpyAsync(ctx->h_bk_samples, ctx->d_bk_samples, (ns + 1 + mates) * 8,
+			cudaMemcpyDeviceToHost, s));
+	MIBF_TRY(ctx, cudaStreamSynchronize(s));
+	const uint64_t *hs = ctx->h_bk_samples;
+	struct Cut {
+		uint64_t r0, r1, f0, f1;
+	};
+	std::vector<Cut> cuts;
+	const uint64_t most = std::max<uint64_t>(ctx->bk_max_frames, 1ull << 16);
+	auto pt = [&](uint64_t j) { return j < ns ? j * S : n; };
+	for (uint64_t j = 0; pt(j) < n;) {
+		uint64_t jj = j;
+		while (jj + 1 <= ns && hs[jj + 1] - hs[j] <= most)
+			++jj;
+		if (jj == j)
+			return BBT_OK; /* S reads above a sub-batch: the direct kernel */
+		if (hs[jj] > hs[j])
+			cuts.push_back({pt(j), pt(jj), hs[j], hs[jj]});
+		j = jj;
+	}
+	/* the bases as 2-bit codes */
+	PackedBases pk[2];
+	memset(pk, 0, sizeof pk);
+	for (uint32_t m = 0; m < mates; ++m) {
+		const uint64_t len = hs[ns + 1 + m];
+		if (mbk_grow(ctx, &ctx->d_bk_codes[m], ctx->bk_codes_cap[m], 2 * (len / 32 + 2)) ||
+				mbk_grow(ctx, &ctx->d_bk_cvalid[m], ctx->bk_cvalid_cap[m], len / 32 + 2))
+			return BBT_ERR_NOMEM;
+		MIBF_TRY(ctx, launch_bk_pack(seqm[m], len, ctx->d_bk_codes[m], ctx->d_bk_cvalid[m],
+				ctx->num_sms, s));
+		pk[m].words = ctx->d_bk_codes[m];
+		pk[m].nwords = 2 * (len / 32 + 2);
+		pk[m].valid = ctx->d_bk_cvalid[m];
+		pk[m].nvalid = len / 32 + 2;
+	}
+	unsigned bshift = std::max<unsigned>(ctx->bk_bshift, 12);
+	while (((ctx->hd.m + (1ull << bshift) - 1) >> bshift) > kMbkMaxBuckets)
+		++bshift;
+	const uint32_t nbkt = (uint32_t)((ctx->hd.m + (1ull << bshift) - 1) >> bshift);
+	const uint32_t W = std::max<uint32_t>(kMbkThreads, kMbkRequests / h / kMbkThreads *
+			kMbkThreads);
+	const size_t hsmem = mbk_hash_smem(a.f.nse, W, h, nbkt);
+	int res_per_sm = 0;
+	MIBF_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res_per_sm, mbk_resolve_kernel,
+			256, 0));
+	for (const Cut &c : cuts) {
+		const uint64_t T = c.f1 - c.f0;
+		const uint32_t nblk = (uint32_t)((T + W - 1) / W);
+		const uint64_t cap = (uint64_t)W * h, pool = (uint64_t)nblk * cap;
+		if (mbk_grow(ctx, &ctx->d_bk_valid, ctx->bk_valid_cap, T / 32 + 2) ||
+				mbk_grow(ctx, &ctx->d_bk_e, ctx->bk_e_cap, T * h) ||
+				mbk_grow(ctx, &ctx->d_bk_off, ctx->bk_off_cap, pool) ||
+				mbk_grow(ctx, &ctx->d_bk_slot, ctx->bk_slot_cap, pool) ||
+				mbk_grow(ctx, &ctx->d_bk_res, ctx->bk_res_cap, pool) ||
+				mbk_grow(ctx, &ctx->d_bk_cnt, ctx->bk_cnt_cap, (uint64_t)nbkt * nblk) ||
+				mbk_grow(ctx, &ctx->d_bk_loc, ctx->bk_loc_cap, (uint64_t)nbkt * nblk) ||
+				mbk_grow(ctx, &ctx->d_bk_btot, ctx->bk_btot_cap, nblk))
+			return BBT_ERR_NOMEM;
+		MbkArgs b;
+		memset(&b, 0, sizeof b);
+		b.f = a.f;
+		b.tables = a.tables;
+		b.pk[0] = pk[0];
+		b.pk[1] = pk[1];
+		b.off = a.off;
+		b.off2 = a.seq2 ? a.off2 : nullptr;
+		b.r0 = c.r0;
+		b.nr = c.r1 - c.r0;
+		b.fo = ctx->d_bk_fo;
+		b.fo0 = c.f0;
+		b.T = T;
+		b.W = W;
+		b.nblk = nblk;
+		b.nbkt = nbkt;
+		b.bshift = bshift;
+		b.valid = ctx->d_bk_valid;
+		b.e = ctx->d_bk_e;
+		b.cnt = ctx->d_bk_cnt;
+		b.loc = ctx->d_bk_loc;
+		b.btot = ctx->d_bk_btot;
+		b.cap = cap;
+		b.req_off = ctx->d_bk_off;
+		b.req_slot = ctx->d_bk_slot;
+		b.res = ctx->d_bk_res;
+		MIBF_TRY(ctx, mbk_hash(b, hsel, hsmem, s));
+		mbk_resolve_kernel<<<ctx->num_sms * std::max(res_per_sm, 1), 256, 0, s>>>(b, a.f.dense);
+		MIBF_TRY(ctx, cudaGetLastError());
+		mbk_unscatter_kernel<<<nblk, 256, cap * sizeof(uint16_t), s>>>(b);
+		MIBF_TRY(ctx, cudaGetLastError());
+		MibfArgs q = a;
+		q.n_reads = c.r1 - c.r0;
+		q.off = a.off + c.r0;
+		q.off2 = a.seq2 ? a.off2 + c.r0 : a.off2;
+		q.hits = a.hits + c.r0 * a.max_hits;
+		q.n_hits = a.n_hits + c.r0;
+		q.sat = a.sat + c.r0;
+		q.pre_e = ctx->d_bk_e;
+		q.pre_valid = ctx->d_bk_valid;
+		q.pre_fo = ctx->d_bk_fo + c.r0;
+		q.pre_fo0 = c.f0;
+		MIBF_TRY(ctx, cudaMemsetAsync(a.work, 0, 8, s));
+		MIBF_TRY(ctx, launch_query(q, true, big, hsel, grid, smem, s, true));
+	}
+	*done = true;
+	return BBT_OK;
+}
+
 /* A batch may be classified in several launches (chunks of its reads, their
  * results at their place in the batch's arrays): the first clears the batch's
  * counters and overflow flag, the last commits the counters. */
@@ -1269,9 +1877,19 @@ static int run_query_sc(bbt_mibf *ctx, uint64_t n_reads, const uint8_t *seq, con
 		if (timed)
 			MIBF_TRY(ctx, cudaEventRecord(ctx->ev0, s));
 	}
-	MIBF_TRY(ctx, cudaMemsetAsync(sc.work, 0, 8, s));
-	if (n_reads)
-		MIBF_TRY(ctx, launch_query(a, dense, big, hsel, grid, smem, s));
+	bool bucketed = false;
+	if (sc.work == ctx->d_work && mbk_wanted(ctx, n_reads)) {
+		const int pre_sm = query_occupancy(true, big, hsel, smem, true);
+		const int pre_grid = ctx->num_sms * (big ? std::min(pre_sm, kMibfBigBlocksPerSm) : pre_sm);
+		int rc = run_query_bucketed(ctx, a, hsel, big, pre_grid, smem, s, &bucketed);
+		if (rc)
+			return rc;
+	}
+	if (!bucketed) {
+		MIBF_TRY(ctx, cudaMemsetAsync(sc.work, 0, 8, s));
+		if (n_reads)
+			MIBF_TRY(ctx, launch_query(a, dense, big, hsel, grid, smem, s));
+	}
 	if (phase & kQueryEnd) {
 		if (timed)
 			MIBF_TRY(ctx, cudaEventRecord(ctx->ev1, s));
@@ -1597,6 +2215,29 @@ extern "C" int bbt_mibf_summary_tsv(bbt_mibf *ctx, uint64_t read_count, char *bu
 		memcpy(buf, s.data(), n);
 		buf[n] = 0;
 	}
+	return BBT_OK;
+}
+
+extern "C" int bbt_mibf_set_bucketing(bbt_mibf *ctx, int mode, unsigned bucket_shift,
+		uint64_t max_frames)
+{
+	if (!ctx || ctx->host_only)
+		return BBT_ERR_ARG;
+	if (mode < 0 || mode > 2)
+		return mibf_fail(ctx, BBT_ERR_ARG, "bbt_mibf_set_bucketing: mode must be 0, 1 or 2");
+	if (bucket_shift && (bucket_shift < 12 || bucket_shift > 40))
+		return mibf_fail(ctx, BBT_ERR_ARG, "bbt_mibf_set_bucketing: bucket_shift must be in "
+				"[12, 40]");
+	if (mode == 1 && !ctx->d_dense)
+		return mibf_fail(ctx, BBT_ERR_UNSUPPORTED, "bbt_mibf_set_bucketing: the bucketed query "
+				"reads the dense layout");
+	MIBF_TRY(ctx, cudaSetDevice(ctx->dev));
+	MIBF_TRY(ctx, cudaDeviceSynchronize());
+	ctx->bk_mode = mode;
+	if (bucket_shift)
+		ctx->bk_bshift = bucket_shift;
+	if (max_frames)
+		ctx->bk_max_frames = max_frames;
 	return BBT_OK;
 }
 

@@ -123,6 +123,26 @@ struct bbt_mibf {
 	uint64_t reads_seen = 0;
 	cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 	double last_kernel_ms = 0;
+	/* bucketed query (dense layout, mibf.cu): settings, then the scratch of
+	 * one call (frame offsets, offset samples, packed bases, frame validity
+	 * bits, resolved entries, the request pool, per-(bucket, block) counts
+	 * and first slots, per-block totals, scan scratch) */
+	int bk_mode = 2;                      /* 0 off, 1 on, 2 large batches on large maps */
+	uint32_t bk_bshift = 23;              /* bucket of 2^23 entries (16 MB) */
+	uint64_t bk_max_frames = 1ull << 30;  /* frames per sub-batch */
+	uint64_t *d_bk_fo = nullptr, *h_bk_samples = nullptr, *d_bk_samples = nullptr;
+	uint64_t bk_fo_cap = 0, bk_samples_cap = 0;
+	uint32_t *d_bk_codes[2] = {nullptr, nullptr}, *d_bk_cvalid[2] = {nullptr, nullptr};
+	uint64_t bk_codes_cap[2] = {0, 0}, bk_cvalid_cap[2] = {0, 0};
+	uint32_t *d_bk_valid = nullptr;
+	uint16_t *d_bk_e = nullptr;
+	uint32_t *d_bk_off = nullptr;
+	uint16_t *d_bk_slot = nullptr, *d_bk_res = nullptr;
+	uint32_t *d_bk_cnt = nullptr, *d_bk_loc = nullptr, *d_bk_btot = nullptr;
+	uint64_t bk_valid_cap = 0, bk_e_cap = 0, bk_off_cap = 0, bk_slot_cap = 0, bk_res_cap = 0;
+	uint64_t bk_cnt_cap = 0, bk_loc_cap = 0, bk_btot_cap = 0;
+	void *d_bk_tmp = nullptr;
+	size_t bk_tmp_cap = 0;
 };
 
 namespace bbt {
