@@ -1569,6 +1569,8 @@ def run_mibf(args):
     d1, doff = h1.to(dev), hoff.to(dev)
     t0 = time.time()
     mc = MIBFClassifier(path, device=local, layout=args.layout)
+    if args.mibf_bucketing >= 0:
+        mc.set_bucketing(mode=args.mibf_bucketing)
     log(f"miBF load: {time.time() - t0:.1f} s")
     MH = 4
     hits = torch.empty((n, MH, 7), dtype=torch.int32, device=dev)
@@ -1667,6 +1669,8 @@ def run_mibf(args):
         "config": {"workload": mi_workload(args.targets, n), "reads_per_gpu": n,
                    "targets": args.targets,
                    "layout": "dense ID map" if dense else "rank blocks + ID array",
+                   "bucketed_query": {-1: "default (bbt_mibf_set_bucketing mode 2)", 0: "off",
+                                      1: "on", 2: "auto"}[args.mibf_bucketing],
                    "filter_bytes": int(os.path.getsize(path) + os.path.getsize(path[:-3] +
                                                                              ".sdsl")),
                    "l2": "inputs larger than L2 (3 GB reads + 5 GB miBF)",
@@ -1787,6 +1791,8 @@ def main():
     ap.add_argument("--reads", type=int, default=None,
                     help="reads (--workload mibf / varlen / small; default: the workload's)")
     ap.add_argument("--layout", type=int, default=0, help="miBF layout: 0 auto, 1 rank, 2 dense")
+    ap.add_argument("--mibf-bucketing", type=int, default=-1, choices=[-1, 0, 1, 2],
+                    help="miBF bucketed query (bbt_mibf_set_bucketing mode; -1: the default)")
     ap.add_argument("--path", default="auto", choices=["auto", "persistent", "bucketed"],
                     help="batched path of the single-filter workloads (default: autotuned)")
     ap.add_argument("--bucketing", default="",

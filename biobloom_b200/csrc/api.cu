@@ -1101,6 +1101,7 @@ static int run_bucketed(bbt_ctx *ctx, ClassifyArgs &a, cudaStream_t s)
 			b.res = ctx->d_bk_res;
 			b.btot = ctx->d_bk_btot;
 			b.issued = a.probes;
+			b.next = ctx->d_work;
 			for (const auto &ph : phases) {
 				b.ph_lo = ph.first;
 				b.ph_hi = ph.second;

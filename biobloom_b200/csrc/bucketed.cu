@@ -564,54 +564,56 @@ __global__ void __launch_bounds__(kNT) bk_apply_kernel(BucketArgs b)
 	bk_apply_block(b, sh);
 }
 
-/* The round's (bucket, block) segments in bucket-major order, one warp per
- * segment and eight requests per lane in flight; the bucket being tested is
- * held in L2, the pool is read once and the results written once
- * (streaming). */
+/* The round's (bucket, block) segments in bucket-major order, taken four at a
+ * time from a work counter (so that every warp works at the front and the
+ * buckets in flight stay few), one warp per segment and eight requests per
+ * lane in flight; the bucket being tested is held in L2, the pool is read once
+ * and the results written once (streaming). */
 __global__ void __launch_bounds__(256) bk_resolve_kernel(BucketArgs b)
 {
 	const uint32_t lane = threadIdx.x & 31u;
 	const uint64_t nseg = (uint64_t)b.nbkt * b.nblk;
-	const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
 	const uint32_t *words = b.f.words;
 	const unsigned sh = b.bshift;
 	unsigned long long issued = 0;
-	/* the next segment's count and first slot are loaded while this one is
-	 * tested */
-	uint64_t sg = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-	uint32_t n_next = sg < nseg ? b.cnt[sg] : 0u, loc_next = sg < nseg ? b.loc[sg] : 0u;
-	while (sg < nseg) {
-		const uint64_t cur = sg;
-		const uint32_t n = n_next, lc = loc_next;
-		sg += warps;
-		if (sg < nseg) {
-			n_next = b.cnt[sg];
-			loc_next = b.loc[sg];
-		}
-		if (n == 0)
-			continue;
-		const uint32_t q = (uint32_t)(cur / b.nblk);
-		const uint32_t blk = (uint32_t)(cur - (uint64_t)q * b.nblk);
-		const uint64_t base = (uint64_t)blk * b.cap + lc;
-		const uint64_t qbase = (uint64_t)q << sh;
-		issued += n;
-		for (uint32_t c = 0; c < n; c += 256) {
-			uint32_t off[8], w[8];
+	for (;;) {
+		unsigned long long g = 0;
+		if (lane == 0)
+			g = atomicAdd(b.next, 4ull);
+		g = __shfl_sync(0xffffffffu, g, 0);
+		if (g >= nseg)
+			break;
+		const uint32_t n4 = lane < 4 && g + lane < nseg ? b.cnt[g + lane] : 0u;
+		const uint32_t l4 = lane < 4 && g + lane < nseg ? b.loc[g + lane] : 0u;
+		for (uint32_t u = 0; u < 4 && g + u < nseg; ++u) {
+			const uint64_t cur = g + u;
+			const uint32_t n = __shfl_sync(0xffffffffu, n4, u);
+			const uint32_t lc = __shfl_sync(0xffffffffu, l4, u);
+			if (n == 0)
+				continue;
+			const uint32_t q = (uint32_t)(cur / b.nblk);
+			const uint32_t blk = (uint32_t)(cur - (uint64_t)q * b.nblk);
+			const uint64_t base = (uint64_t)blk * b.cap + lc;
+			const uint64_t qbase = (uint64_t)q << sh;
+			issued += n;
+			for (uint32_t c = 0; c < n; c += 256) {
+				uint32_t off[8], w[8];
 #pragma unroll
-			for (int j = 0; j < 8; ++j) {
-				const uint32_t i = c + (uint32_t)j * 32 + lane;
-				off[j] = i < n ? __ldcs(b.req_off + base + i) : 0u;
-			}
+				for (int j = 0; j < 8; ++j) {
+					const uint32_t i = c + (uint32_t)j * 32 + lane;
+					off[j] = i < n ? __ldcs(b.req_off + base + i) : 0u;
+				}
 #pragma unroll
-			for (int j = 0; j < 8; ++j) {
-				const uint32_t i = c + (uint32_t)j * 32 + lane;
-				w[j] = i < n ? __ldg(words + ((qbase + off[j]) >> 5)) : 0u;
-			}
+				for (int j = 0; j < 8; ++j) {
+					const uint32_t i = c + (uint32_t)j * 32 + lane;
+					w[j] = i < n ? __ldg(words + ((qbase + off[j]) >> 5)) : 0u;
+				}
 #pragma unroll
-			for (int j = 0; j < 8; ++j) {
-				const uint32_t i = c + (uint32_t)j * 32 + lane;
-				if (i < n)
-					__stcs(b.res + base + i, (uint8_t)((w[j] >> (off[j] & 31u)) & 1u));
+				for (int j = 0; j < 8; ++j) {
+					const uint32_t i = c + (uint32_t)j * 32 + lane;
+					if (i < n)
+						__stcs(b.res + base + i, (uint8_t)((w[j] >> (off[j] & 31u)) & 1u));
+				}
 			}
 		}
 	}
@@ -760,6 +762,9 @@ cudaError_t launch_bk_resolve(const BucketArgs &b, int num_sms, cudaStream_t s)
 	int per_sm = 0;
 	cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, bk_resolve_kernel,
 			256, 0);
+	if (e != cudaSuccess)
+		return e;
+	e = cudaMemsetAsync(b.next, 0, sizeof(unsigned long long), s);
 	if (e != cudaSuccess)
 		return e;
 	bk_resolve_kernel<<<num_sms * (per_sm > 0 ? per_sm : 1), 256, 0, s>>>(b);

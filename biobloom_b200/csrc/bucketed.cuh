@@ -57,6 +57,7 @@ struct BucketArgs {
 	uint8_t *res;              /*   test result (1 = bit set) */
 	uint32_t *btot;            /* requests of this round per window block */
 	unsigned long long *issued;/* optional: requests resolved (bit tests issued) */
+	unsigned long long *next;  /* resolve: next segment to take (zeroed before the launch) */
 };
 
 /* fo[i + 1] = frames of read i (n * mates reads); the caller scans it. */

@@ -766,7 +766,7 @@ __global__ void mibf_dense_build_kernel(const uint64_t *raw, uint64_t m,
  * as it does from its own probes.
  */
 constexpr uint32_t kMbkThreads = 256;
-constexpr uint32_t kMbkRequests = 12288;
+constexpr uint32_t kMbkRequests = 10752;
 constexpr uint32_t kMbkMaxBuckets = 2048;
 
 struct MbkArgs {
@@ -785,6 +785,7 @@ struct MbkArgs {
 	uint32_t *req_off;           /* pool: entry offset inside the bucket */
 	uint16_t *req_slot;          /*   frame * h + value inside the block */
 	uint16_t *res;               /*   the entry read */
+	unsigned long long *next;    /* resolve: next group of segments (zeroed before) */
 };
 
 __device__ __forceinline__ uint64_t mbk_find_read(const MbkArgs &b, uint64_t x)
@@ -798,28 +799,6 @@ __device__ __forceinline__ uint64_t mbk_find_read(const MbkArgs &b, uint64_t x)
 			hi = mid;
 	}
 	return lo;
-}
-
-/* The 2-bit codes of 32 bases from base g (w, base j at bits 2j) and whether
- * the k bases from g are all ACGT. */
-__device__ __forceinline__ bool mbk_frame(const PackedBases &p, uint64_t g, unsigned k,
-		uint64_t &w)
-{
-	const uint64_t i = g >> 4;
-	const uint32_t s = (uint32_t)(g & 15u) * 2u;
-	const uint32_t w0 = i < p.nwords ? __ldg(p.words + i) : 0u;
-	const uint32_t w1 = i + 1 < p.nwords ? __ldg(p.words + i + 1) : 0u;
-	const uint32_t w2 = i + 2 < p.nwords ? __ldg(p.words + i + 2) : 0u;
-	const uint64_t lo = (uint64_t)w0 | ((uint64_t)w1 << 32);
-	w = s ? (lo >> s) | ((uint64_t)w2 << (64u - s)) : lo;
-	if (!p.valid)
-		return true;
-	const uint64_t vi = g >> 5;
-	const uint32_t v0 = vi < p.nvalid ? __ldg(p.valid + vi) : 0u;
-	const uint32_t v1 = vi + 1 < p.nvalid ? __ldg(p.valid + vi + 1) : 0u;
-	const uint32_t v = __funnelshift_r(v0, v1, (uint32_t)(g & 31u));
-	const uint32_t km = k >= 32 ? 0xffffffffu : ((1u << k) - 1u);
-	return (~v & km) == 0;
 }
 
 /* In-place exclusive scan of v[0, n) in shared memory by the whole block
@@ -870,14 +849,52 @@ __device__ uint32_t mbk_exscan(uint32_t *v, uint32_t n, uint32_t *tmp)
 }
 
 /* Shared memory of the hash kernel: seed tables, staged requests (offset,
- * bucket), counts and first slots per bucket, validity words. */
+ * bucket), their order by bucket, counts and first slots per bucket, validity
+ * words. */
 __host__ __device__ inline size_t mbk_hash_smem(uint32_t nse, uint32_t W, uint32_t h,
 		uint32_t nbkt)
 {
 	const size_t req = (size_t)W * h;
-	return (size_t)nse * kTabEntries * 16 + req * 4 + ((req * 2 + 15) & ~(size_t)15) +
+	return (size_t)nse * kTabEntries * 16 + req * 4 + 2 * ((req * 2 + 15) & ~(size_t)15) +
 			(size_t)nbkt * 8 + (size_t)(W / 32) * 4;
 }
+
+/* A thread's view of the packed bases of one mate array: the code and
+ * validity words of the last frame fetched, reused while the next frame's
+ * bases start in the same 16-base word.  frame() gives the 2-bit codes of 32
+ * bases from base g (w, base j at bits 2j) and whether the k bases from g are
+ * all ACGT. */
+struct MbkCodes {
+	uint64_t ci = ~0ull;
+	uint32_t c0 = 0, c1 = 0, c2 = 0, v0 = 0, v1 = 0;
+
+	__device__ __forceinline__ bool frame(const PackedBases &p, uint64_t g, unsigned k,
+			uint64_t &w)
+	{
+		const uint64_t i = g >> 4;
+		if (i != ci) {
+			ci = i;
+			c0 = i < p.nwords ? __ldg(p.words + i) : 0u;
+			c1 = i + 1 < p.nwords ? __ldg(p.words + i + 1) : 0u;
+			c2 = i + 2 < p.nwords ? __ldg(p.words + i + 2) : 0u;
+			if (p.valid) {
+				const uint64_t vi = g >> 5;
+				v0 = vi < p.nvalid ? __ldg(p.valid + vi) : 0u;
+				v1 = vi + 1 < p.nvalid ? __ldg(p.valid + vi + 1) : 0u;
+			}
+		}
+		const uint32_t s = (uint32_t)(g & 15u) * 2u;
+		const uint64_t lo = (uint64_t)c0 | ((uint64_t)c1 << 32);
+		w = s ? (lo >> s) | ((uint64_t)c2 << (64u - s)) : lo;
+		if (!p.valid)
+			return true;
+		/* validity bits g .. g + 31 (words g / 32 and g / 32 + 1, the same for
+		 * every base of the 16-base word i) */
+		const uint32_t v = __funnelshift_r(v0, v1, (uint32_t)(g & 31u));
+		const uint32_t km = k >= 32 ? 0xffffffffu : ((1u << k) - 1u);
+		return (~v & km) == 0;
+	}
+};
 
 template <int H>
 __global__ void __launch_bounds__(kMbkThreads) mbk_hash_kernel(MbkArgs b)
@@ -892,7 +909,7 @@ __global__ void __launch_bounds__(kMbkThreads) mbk_hash_kernel(MbkArgs b)
 	uint32_t *st_off = reinterpret_cast<uint32_t *>(smem + (size_t)nse * kTabEntries * 16);
 	uint16_t *st_bkt = reinterpret_cast<uint16_t *>(st_off + nreq);
 	uint32_t *hist = reinterpret_cast<uint32_t *>(reinterpret_cast<unsigned char *>(st_bkt) +
-			(((size_t)nreq * 2 + 15) & ~(size_t)15));
+			2 * (((size_t)nreq * 2 + 15) & ~(size_t)15));
 	uint32_t *locs = hist + b.nbkt;
 	uint32_t *vw = locs + b.nbkt;
 	__shared__ uint32_t tmp[33];
@@ -913,16 +930,28 @@ __global__ void __launch_bounds__(kMbkThreads) mbk_hash_kernel(MbkArgs b)
 	if (x0 < w1) {
 		const uint64_t x1 = min(x0 + R, w1);
 		uint64_t r = mbk_find_read(b, x0);
+		/* the read's frame range, base offsets and mate-1 frames, reloaded
+		 * when the thread's frames move to the next read */
+		uint64_t rs = b.fo[r] - b.fo0, re = b.fo[r + 1] - b.fo0;
+		uint64_t o1 = b.off[r], o2 = b.off2 ? b.off2[r] : 0;
+		uint64_t f1 = b.off[r + 1] - o1;
+		f1 = f1 >= k ? f1 - k + 1 : 0;
+		MbkCodes cc[2];
 		for (uint64_t x = x0; x < x1; ++x) {
-			while (b.fo[r + 1] - b.fo0 <= x)
+			while (re <= x) {
 				++r;
-			const uint64_t q = x - (b.fo[r] - b.fo0);
-			const uint64_t len1 = b.off[r + 1] - b.off[r];
-			const uint64_t f1 = len1 >= k ? len1 - k + 1 : 0;
+				rs = re;
+				re = b.fo[r + 1] - b.fo0;
+				o1 = b.off[r];
+				o2 = b.off2 ? b.off2[r] : 0;
+				f1 = b.off[r + 1] - o1;
+				f1 = f1 >= k ? f1 - k + 1 : 0;
+			}
+			const uint64_t q = x - rs;
 			const uint32_t mate = q >= f1 ? 1u : 0u;
-			const uint64_t g = (mate ? b.off2[r] : b.off[r]) + (mate ? q - f1 : q);
+			const uint64_t g = mate ? o2 + (q - f1) : o1 + q;
 			uint64_t w;
-			const bool ok = mbk_frame(b.pk[mate], g, k, w);
+			const bool ok = cc[mate].frame(b.pk[mate], g, k, w);
 			uint64_t vals[H];
 			frame_values<H>(b.f, tab, ok, w, vals);
 			const uint32_t fid = (uint32_t)(x - w0);
@@ -962,20 +991,28 @@ __global__ void __launch_bounds__(kMbkThreads) mbk_hash_kernel(MbkArgs b)
 		hist[q] = 0;
 	}
 	__syncthreads();
-	const uint64_t base = (uint64_t)blk * b.cap;
+	/* each request's place in bucket order (inv: place -> request), then the
+	 * block's requests written out in that order, coalesced */
+	uint16_t *inv = reinterpret_cast<uint16_t *>(reinterpret_cast<unsigned char *>(st_bkt) +
+			(((size_t)nreq * 2 + 15) & ~(size_t)15));
 	for (uint32_t j = t; j < nreq; j += kMbkThreads) {
 		const uint32_t bk = st_bkt[j];
-		if (bk == 0xffffu)
-			continue;
-		const uint64_t i = base + locs[bk] + atomicAdd(&hist[bk], 1u);
-		b.req_off[i] = st_off[j];
-		b.req_slot[i] = (uint16_t)j;
+		if (bk != 0xffffu)
+			inv[locs[bk] + atomicAdd(&hist[bk], 1u)] = (uint16_t)j;
+	}
+	__syncthreads();
+	const uint64_t base = (uint64_t)blk * b.cap;
+	for (uint32_t i = t; i < total; i += kMbkThreads) {
+		const uint32_t j = inv[i];
+		b.req_off[base + i] = st_off[j];
+		b.req_slot[base + i] = (uint16_t)j;
 	}
 }
 
-/* The round's (bucket, block) segments in bucket-major order, 32 consecutive
- * segments per warp (their requests taken 256 at a time, eight per lane in
- * flight); the bucket being read is held in L2, the pool streams through. */
+/* The (bucket, block) segments in bucket-major order, 32 consecutive segments
+ * per warp taken from a work counter (every warp works at the front, so the
+ * buckets in flight stay few), their requests 256 at a time, eight per lane in
+ * flight; the bucket being read is held in L2, the pool streams through. */
 __global__ void __launch_bounds__(256) mbk_resolve_kernel(MbkArgs b, const uint16_t *dense)
 {
 	__shared__ uint32_t spre[8][33];
@@ -984,9 +1021,14 @@ __global__ void __launch_bounds__(256) mbk_resolve_kernel(MbkArgs b, const uint1
 	const uint32_t lane = threadIdx.x & 31u, wib = threadIdx.x >> 5;
 	const uint64_t nseg = (uint64_t)b.nbkt * b.nblk;
 	const uint64_t ngroups = (nseg + 31) / 32;
-	const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
 	const unsigned sh = b.bshift;
-	for (uint64_t g = (uint64_t)blockIdx.x * (blockDim.x >> 5) + wib; g < ngroups; g += warps) {
+	for (;;) {
+		unsigned long long g = 0;
+		if (lane == 0)
+			g = atomicAdd(b.next, 1ull);
+		g = __shfl_sync(kFull, g, 0);
+		if (g >= ngroups)
+			break;
 		const uint64_t sg = g * 32 + lane;
 		uint32_t n = 0, lc = 0, q = 0, blk = 0;
 		if (sg < nseg) {
@@ -1789,6 +1831,8 @@ static int run_query_bucketed(bbt_mibf *ctx, const MibfArgs &a, int hsel, bool b
 		b.req_slot = ctx->d_bk_slot;
 		b.res = ctx->d_bk_res;
 		MIBF_TRY(ctx, mbk_hash(b, hsel, hsmem, s));
+		b.next = a.work;
+		MIBF_TRY(ctx, cudaMemsetAsync(a.work, 0, 8, s));
 		mbk_resolve_kernel<<<ctx->num_sms * std::max(res_per_sm, 1), 256, 0, s>>>(b, a.f.dense);
 		MIBF_TRY(ctx, cudaGetLastError());
 		mbk_unscatter_kernel<<<nblk, 256, cap * sizeof(uint16_t), s>>>(b);
