@@ -1669,7 +1669,7 @@ def run_mibf(args):
         "config": {"workload": mi_workload(args.targets, n), "reads_per_gpu": n,
                    "targets": args.targets,
                    "layout": "dense ID map" if dense else "rank blocks + ID array",
-                   "bucketed_query": {-1: "default (bbt_mibf_set_bucketing mode 2)", 0: "off",
+                   "bucketed_query": {-1: "off (default)", 0: "off",
                                       1: "on", 2: "auto"}[args.mibf_bucketing],
                    "filter_bytes": int(os.path.getsize(path) + os.path.getsize(path[:-3] +
                                                                              ".sdsl")),

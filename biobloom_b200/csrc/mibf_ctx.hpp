@@ -127,7 +127,7 @@ struct bbt_mibf {
 	 * one call (frame offsets, offset samples, packed bases, frame validity
 	 * bits, resolved entries, the request pool, per-(bucket, block) counts
 	 * and first slots, per-block totals, scan scratch) */
-	int bk_mode = 2;                      /* 0 off, 1 on, 2 large batches on large maps */
+	int bk_mode = 0;                      /* 0 off, 1 on, 2 large batches on large maps */
 	uint32_t bk_bshift = 23;              /* bucket of 2^23 entries (16 MB) */
 	uint64_t bk_max_frames = 1ull << 30;  /* frames per sub-batch */
 	uint64_t *d_bk_fo = nullptr, *h_bk_samples = nullptr, *d_bk_samples = nullptr;

@@ -158,9 +158,7 @@ class MIBFClassifier:
     def set_bucketing(self, mode=None, bucket_shift=0, max_frames=0):
         """Bucketed query of the dense layout (bbt_mibf_set_bucketing): mode 0
         off, 1 on, 2 automatic (None keeps it); 0 keeps the other settings."""
-        m = -1 if mode is None else mode
-        if m < 0:
-            m = 2 if not hasattr(self, "_bk_mode") else self._bk_mode
+        m = getattr(self, "_bk_mode", 0) if mode is None else mode
         L.check_mibf(L.lib().bbt_mibf_set_bucketing(self._ctx, m, bucket_shift, max_frames),
                      self._ctx)
         self._bk_mode = m

@@ -153,9 +153,10 @@ int bbt_mibf_classify_batch(bbt_mibf *ctx, const bbt_batch *batch, bbt_mibf_resu
 int bbt_mibf_sync(bbt_mibf *ctx);
 /* The bucketed query of the dense layout: every probe of a sub-batch of reads
  * sorted by address and read out of L2 one bucket of 2^bucket_shift entries
- * at a time before the reads are tallied.  mode 0 off, 1 on (dense layout),
- * 2 (default) on for batches of 2^20 reads or more over an ID map of 256 MB
- * or more; bucket_shift default 23 (16 MB); at most max_frames frames per
+ * at a time before the reads are tallied.  mode 0 off (the default: on B200
+ * the direct kernel measured faster on the 500-target workload), 1 on (dense
+ * layout), 2 on for batches of 2^20 reads or more over an ID map of 256 MB or
+ * more; bucket_shift default 23 (16 MB); at most max_frames frames per
  * sub-batch (default 2^30; scratch about 8 h + 2 h + 1 bytes per frame);
  * 0 keeps a setting.  Results do not depend on them; the serving engine's
  * concurrent slots always take the direct kernel.  No reference counterpart. */
