@@ -1762,8 +1762,8 @@ static int run_query_bucketed(bbt_mibf *ctx, const MibfArgs &a, int hsel, bool b
 			++jj;
 		if (jj == j)
 			return BBT_OK; /* S reads above a sub-batch: the direct kernel */
-		if (hs[jj] > hs[j])
-			cuts.push_back({pt(j), pt(jj), hs[j], hs[jj]});
+		/* reads without frames still get their (empty) results and summary */
+		cuts.push_back({pt(j), pt(jj), hs[j], hs[jj]});
 		j = jj;
 	}
 	/* the bases as 2-bit codes */
@@ -1830,13 +1830,16 @@ static int run_query_bucketed(bbt_mibf *ctx, const MibfArgs &a, int hsel, bool b
 		b.req_off = ctx->d_bk_off;
 		b.req_slot = ctx->d_bk_slot;
 		b.res = ctx->d_bk_res;
-		MIBF_TRY(ctx, mbk_hash(b, hsel, hsmem, s));
-		b.next = a.work;
-		MIBF_TRY(ctx, cudaMemsetAsync(a.work, 0, 8, s));
-		mbk_resolve_kernel<<<ctx->num_sms * std::max(res_per_sm, 1), 256, 0, s>>>(b, a.f.dense);
-		MIBF_TRY(ctx, cudaGetLastError());
-		mbk_unscatter_kernel<<<nblk, 256, cap * sizeof(uint16_t), s>>>(b);
-		MIBF_TRY(ctx, cudaGetLastError());
+		if (T > 0) {
+			MIBF_TRY(ctx, mbk_hash(b, hsel, hsmem, s));
+			b.next = a.work;
+			MIBF_TRY(ctx, cudaMemsetAsync(a.work, 0, 8, s));
+			mbk_resolve_kernel<<<ctx->num_sms * std::max(res_per_sm, 1), 256, 0, s>>>(b,
+					a.f.dense);
+			MIBF_TRY(ctx, cudaGetLastError());
+			mbk_unscatter_kernel<<<nblk, 256, cap * sizeof(uint16_t), s>>>(b);
+			MIBF_TRY(ctx, cudaGetLastError());
+		}
 		MibfArgs q = a;
 		q.n_reads = c.r1 - c.r0;
 		q.off = a.off + c.r0;

@@ -113,6 +113,32 @@ def test_bucketed_five_thousand_targets(many_targets, oi):  # noqa: F811
     mc.close()
 
 
+@pytest.mark.parametrize("paired", [False, True])
+def test_bucketed_reads_without_frames(built, paired):  # noqa: F811
+    """Runs of reads shorter than k (whole sub-batch samples without a frame)
+    between ordinary reads: every read gets its result and the summary counts
+    them, as the direct kernel does."""
+    targets, filters, _, names = built
+    path, f = filters["ss"]
+    o = _opts({})
+    rng = np.random.default_rng(31 + paired)
+    reads, reads2 = _reads(rng, targets, 1200, paired=paired)
+    short = [BASES[rng.integers(0, 4, int(rng.integers(0, 20)))].tobytes() for _ in range(700)]
+    reads = reads[:300] + short + reads[300:]
+    if paired:
+        reads2 = reads2[:300] + [s[::-1] for s in short] + reads2[300:]
+    want = _oracle_query(f, names, reads, reads2, o)
+    mc = _open(path, o, SETTINGS[0])
+    got, sat = mc.classify(reads, reads2, max_hits=4)
+    for i, (res, s) in enumerate(want):
+        assert (got[i], int(sat[i])) == (res, s), i
+    counts, n = mc.summary()
+    assert n == len(reads)
+    nf = len(names) + 1
+    assert counts[2 * (nf + 2) + 1] == sum(1 for r, _ in want if not r)
+    mc.close()
+
+
 def test_bucketed_needs_the_dense_layout(built):  # noqa: F811
     from biobloom_b200 import _lib as L
     from biobloom_b200.mibf import MIBFClassifier
