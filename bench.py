@@ -1146,6 +1146,19 @@ def run_single(args):
                                       "(bbt_measure_gather) x 32 B per probe",
                          "hbm_peak": peak, "hbm_frac": achieved / peak,
                          "hbm_peak_kind": peak_kind})
+    else:
+        # beside the sector roofline: the rate this GPU serves isolated random
+        # 4-byte reads from a table of the filter's size (each a DRAM line
+        # fill), measured here, against the probes the batched path issues
+        rate = ctypes.c_double()
+        L.check(L.lib().bbt_measure_gather(local, fbytes // 4096 * 4096, 1 << 29, 0, 5,
+                                           ctypes.byref(rate)))
+        issued_rate = issued / (k_ms * 1e-3)
+        roofline["random_gather"] = {
+            "ceiling_per_s": rate.value, "issued_probes_per_s": issued_rate,
+            "frac": issued_rate / rate.value if rate.value else None,
+            "kind": "measured in this run: random 4-byte gathers/s into a table of the "
+                    "filter's size, positions generated in the kernel (bbt_measure_gather)"}
     line = {
         "metric": SINGLE_METRIC, "value": world * n / (ms_batched * 1e-3), "unit": "reads/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batched,
