@@ -238,13 +238,16 @@ BBT_HD void binomial_simple_init(SimpleState &s, uint32_t thres, uint64_t frames
  * keep several probes in flight per warp.  The decision itself does not
  * depend on the step sizes.
  */
+#ifndef BBT_TIGHT_MIN_STEP
+#define BBT_TIGHT_MIN_STEP 8
+#endif
 BBT_HD int simple_step_frames(const SimpleState &s)
 {
 	const int32_t gap = s.thres2 - s.score2;
 	if (gap <= 0 || (s.started && s.streak == 0))
 		return 32;
 	const int32_t need = (s.streak > 0 || s.flat) ? (gap + 1) / 2 : 1 + gap / 2;
-	return need < 8 ? 8 : (need > 32 ? 32 : (int)need);
+	return need < BBT_TIGHT_MIN_STEP ? BBT_TIGHT_MIN_STEP : (need > 32 ? 32 : (int)need);
 }
 
 /*
