@@ -241,11 +241,21 @@ BBT_HD void binomial_simple_init(SimpleState &s, uint32_t thres, uint64_t frames
 #ifndef BBT_TIGHT_MIN_STEP
 #define BBT_TIGHT_MIN_STEP 8
 #endif
+#ifndef BBT_TIGHT_REJECT
+#define BBT_TIGHT_REJECT 0
+#endif
 BBT_HD int simple_step_frames(const SimpleState &s)
 {
 	const int32_t gap = s.thres2 - s.score2;
-	if (gap <= 0 || (s.started && s.streak == 0))
+	if (gap <= 0)
 		return 32;
+	if (s.started && s.streak == 0) {
+		if (!BBT_TIGHT_REJECT)
+			return 32;
+		/* a missing read: no reject before anti_thres - anti more misses */
+		const int32_t agap = s.anti_thres - s.anti;
+		return agap < BBT_TIGHT_MIN_STEP ? BBT_TIGHT_MIN_STEP : (agap > 32 ? 32 : (int)agap);
+	}
 	const int32_t need = (s.streak > 0 || s.flat) ? (gap + 1) / 2 : 1 + gap / 2;
 	return need < BBT_TIGHT_MIN_STEP ? BBT_TIGHT_MIN_STEP : (need > 32 ? 32 : (int)need);
 }
