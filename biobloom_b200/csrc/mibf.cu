@@ -124,7 +124,10 @@ static_assert((17 * 8 + 18 * 4) % 8 == 0, "the tally words follow 8-byte aligned
 #endif
 constexpr int kTabEntries = BBT_MIBF_PAIR_TABLES ? 256 : 128; /* ulonglong2 per seed */
 constexpr int kQueryThreads = BBT_MIBF_PAIR_TABLES ? 256 : 128;
-constexpr int kQueryMinBlocks = BBT_MIBF_PAIR_TABLES ? 2 : 4;
+#ifndef BBT_MIBF_MIN_BLOCKS
+#define BBT_MIBF_MIN_BLOCKS (BBT_MIBF_PAIR_TABLES ? 2 : 4)
+#endif
+constexpr int kQueryMinBlocks = BBT_MIBF_MIN_BLOCKS;
 
 __host__ inline size_t mibf_smem_bytes(uint32_t nse, uint32_t T, int warps, bool big)
 {
