@@ -163,6 +163,26 @@ __device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t *p, uint64_t po
 	return v;
 }
 
+/* A probe's filter word.  With BBT_PROBE_EVICT_LAST the load carries an L2
+ * evict-last hint, so that a filter that fits L2 keeps its lines against the
+ * streamed data (a build setting, off by default). */
+#ifndef BBT_PROBE_EVICT_LAST
+#define BBT_PROBE_EVICT_LAST 0
+#endif
+__device__ __forceinline__ uint32_t ld_probe_u32(const uint32_t *p)
+{
+#if BBT_PROBE_EVICT_LAST
+	uint64_t pol;
+	asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+	uint32_t v;
+	asm("ld.global.nc.L1::no_allocate.L2::cache_hint.b32 %0, [%1], %2;"
+			: "=r"(v) : "l"(p), "l"(pol));
+	return v;
+#else
+	return __ldg(p);
+#endif
+}
+
 /* Two independent BloomFilter::contains chains per lane, their rounds
  * interleaved so that both probes of a round are in flight together.
  * pa / pb: whether frame a / b is probed at all.  Word reads are counted in
@@ -184,11 +204,11 @@ __device__ __forceinline__ void contains2(const FilterDev &f, uint64_t ca, bool 
 		uint64_t ba = 0, bb = 0;
 		if (la) {
 			ba = reduce(va, f.m, f.minv);
-			wa = __ldg(f.words + (ba >> 5));
+			wa = ld_probe_u32(f.words + (ba >> 5));
 		}
 		if (lb) {
 			bb = reduce(vb, f.m, f.minv);
-			wb = __ldg(f.words + (bb >> 5));
+			wb = ld_probe_u32(f.words + (bb >> 5));
 		}
 		ra += la;
 		rb += lb;
