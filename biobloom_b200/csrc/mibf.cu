@@ -64,10 +64,12 @@ struct MibfDev {
 
 struct MibfArgs {
 	MibfDev f;
-	const uint8_t *seq;
+	const uint8_t *seq;         /* ASCII bases, or 2-bit code words when packed */
 	const uint64_t *off;
 	const uint8_t *seq2;
 	const uint64_t *off2;
+	int packed;                 /* bases are BBT_BASES_2BIT */
+	const uint32_t *valid[2];   /* packed: validity bits per mate array (NULL = all ACGT) */
 	uint64_t n_reads;
 	const uint32_t *minc;
 	uint32_t need, min_nonsat;
@@ -366,12 +368,24 @@ __device__ __forceinline__ void frame_tally(const MibfArgs &a, bool ok, const ui
 	}
 }
 
+/* The bases of mate array m from base g0 on (ASCII or 2-bit codes). */
+__device__ __forceinline__ Bases mate_bases(const MibfArgs &a, uint32_t m, uint64_t g0)
+{
+	Bases b;
+	const uint8_t *sq = m ? a.seq2 : a.seq;
+	b.g0 = g0;
+	b.ascii = a.packed ? nullptr : sq;
+	b.words = a.packed ? reinterpret_cast<const uint32_t *>(sq) : nullptr;
+	b.valid = a.packed ? a.valid[m] : nullptr;
+	return b;
+}
+
 /* All frames of one mate: bases staged 512 at a time, then steps of 32 * FPL
  * frames, each lane holding FPL frames (FPL * h reads in flight per lane). */
 template <int H, bool DENSE, int FPL>
 __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglong2 *tab,
 		uint64_t *cw, uint32_t *iw, unsigned long long *TA, unsigned long long *TB,
-		unsigned long long *TC, const uint8_t *__restrict__ s, uint64_t len, uint32_t &satc,
+		unsigned long long *TC, const Bases &src, uint64_t len, uint32_t &satc,
 		LaneCounts &lc, int lane, uint32_t *tlist)
 {
 	const uint32_t k = a.f.k;
@@ -383,7 +397,7 @@ __device__ __forceinline__ void mibf_scan_mate(const MibfArgs &a, const ulonglon
 #pragma unroll 4
 		for (int it = 0; it < kStageBases / 32; ++it) {
 			const uint64_t pos = c0 + (uint64_t)it * 32 + lane;
-			const uint8_t c = base_code(pos < len ? s[pos] : (uint8_t)'N');
+			const uint8_t c = pos < len ? base_code_at(src, pos) : (uint8_t)4;
 			const uint32_t lo = __ballot_sync(kFull, c & 1u);
 			const uint32_t hi = __ballot_sync(kFull, (c >> 1) & 1u);
 			const uint32_t inv = __ballot_sync(kFull, c >> 2);
@@ -525,11 +539,11 @@ __global__ void __launch_bounds__(kQueryThreads, kQueryMinBlocks) mibf_query_ker
 				if (a.seq2)
 					mibf_scan_pre<H>(a, x + f1, f2, TA, TB, TC, satc, lc, lane, tlist);
 			} else if (fc) {
-				mibf_scan_mate<H, DENSE, FPL>(a, tab, cw, iw, TA, TB, TC, a.seq + b1, len1,
-						satc, lc, lane, tlist);
+				mibf_scan_mate<H, DENSE, FPL>(a, tab, cw, iw, TA, TB, TC,
+						mate_bases(a, 0, b1), len1, satc, lc, lane, tlist);
 				if (a.seq2)
-					mibf_scan_mate<H, DENSE, FPL>(a, tab, cw, iw, TA, TB, TC, a.seq2 + b2,
-							len2, satc, lc, lane, tlist);
+					mibf_scan_mate<H, DENSE, FPL>(a, tab, cw, iw, TA, TB, TC,
+							mate_bases(a, 1, b2), len2, satc, lc, lane, tlist);
 			}
 			__syncwarp();
 			/* the slots to look at: every slot, or the IDs the read touched */
@@ -1421,6 +1435,7 @@ extern "C" int bbt_mibf_close(bbt_mibf *ctx)
 		for (int c = 0; c < 2; ++c) {
 			for (int m = 0; m < 2; ++m) {
 				cudaFree(ctx->c_seq[c][m]);
+				cudaFree(ctx->c_valid[c][m]);
 				cudaFree(ctx->c_off[c][m]);
 				cudaFreeHost(ctx->h_coff[c][m]);
 			}
@@ -1774,6 +1789,13 @@ static int run_query_bucketed(bbt_mibf *ctx, const MibfArgs &a, int hsel, bool b
 	memset(pk, 0, sizeof pk);
 	for (uint32_t m = 0; m < mates; ++m) {
 		const uint64_t len = hs[ns + 1 + m];
+		if (a.packed) { /* the batch's own code words and validity bits */
+			pk[m].words = reinterpret_cast<const uint32_t *>(seqm[m]);
+			pk[m].nwords = (len + 15) / 16;
+			pk[m].valid = a.valid[m];
+			pk[m].nvalid = a.valid[m] ? (len + 31) / 32 : 0;
+			continue;
+		}
 		if (mbk_grow(ctx, &ctx->d_bk_codes[m], ctx->bk_codes_cap[m], 2 * (len / 32 + 2)) ||
 				mbk_grow(ctx, &ctx->d_bk_cvalid[m], ctx->bk_cvalid_cap[m], len / 32 + 2))
 			return BBT_ERR_NOMEM;
@@ -1866,10 +1888,17 @@ static int run_query_bucketed(bbt_mibf *ctx, const MibfArgs &a, int hsel, bool b
  * counters and overflow flag, the last commits the counters. */
 enum { kQueryBegin = 1, kQueryEnd = 2, kQueryWhole = 3 };
 
+/* The bases of a call: ASCII, or 2-bit code words (bbt_batch BBT_BASES_2BIT)
+ * with validity bits per mate array (NULL: every base is ACGT). */
+struct MibfEncoding {
+	bool packed = false;
+	const uint32_t *valid[2] = {nullptr, nullptr};
+};
+
 static int run_query_sc(bbt_mibf *ctx, uint64_t n_reads, const uint8_t *seq, const uint64_t *off,
 		const uint8_t *seq2, const uint64_t *off2, bbt_mibf_hit *hits, uint32_t max_hits,
 		uint32_t *n_hits, uint32_t *sat, cudaStream_t s, const MibfScratch &sc, bool timed,
-		int phase = kQueryWhole, uint64_t total_reads = ~0ull)
+		int phase = kQueryWhole, uint64_t total_reads = ~0ull, MibfEncoding enc = MibfEncoding())
 {
 	if (total_reads == ~0ull)
 		total_reads = n_reads;
@@ -1892,6 +1921,9 @@ static int run_query_sc(bbt_mibf *ctx, uint64_t n_reads, const uint8_t *seq, con
 	a.off = off;
 	a.seq2 = seq2;
 	a.off2 = off2;
+	a.packed = enc.packed ? 1 : 0;
+	a.valid[0] = enc.valid[0];
+	a.valid[1] = seq2 ? enc.valid[1] : enc.valid[0];
 	a.n_reads = n_reads;
 	a.minc = ctx->d_minc;
 	a.need = ctx->need;
@@ -1963,12 +1995,23 @@ static MibfScratch ctx_scratch(bbt_mibf *ctx)
 	return sc;
 }
 
+static MibfEncoding batch_encoding(const bbt_batch *b)
+{
+	MibfEncoding e;
+	e.packed = b->encoding == BBT_BASES_2BIT;
+	if (e.packed) {
+		e.valid[0] = b->valid;
+		e.valid[1] = b->valid2;
+	}
+	return e;
+}
+
 static int run_query(bbt_mibf *ctx, const bbt_batch *b, const uint8_t *seq, const uint64_t *off,
 		const uint8_t *seq2, const uint64_t *off2, bbt_mibf_hit *hits, uint32_t max_hits,
 		uint32_t *n_hits, uint32_t *sat, cudaStream_t s)
 {
 	return run_query_sc(ctx, b->n_reads, seq, off, seq2, off2, hits, max_hits, n_hits, sat, s,
-			ctx_scratch(ctx), true);
+			ctx_scratch(ctx), true, kQueryWhole, ~0ull, batch_encoding(b));
 }
 
 int bbt::mibf_scratch_init(bbt_mibf *ctx, MibfScratch &sc)
@@ -2022,12 +2065,16 @@ static int grow_chunks(bbt_mibf *ctx, uint64_t bases, uint64_t reads)
 	for (int c = 0; c < 2; ++c)
 		for (int m = 0; m < 2; ++m) {
 			cudaFree(ctx->c_seq[c][m]);
+			cudaFree(ctx->c_valid[c][m]);
 			cudaFree(ctx->c_off[c][m]);
 			cudaFreeHost(ctx->h_coff[c][m]);
 			ctx->c_seq[c][m] = nullptr;
+			ctx->c_valid[c][m] = nullptr;
 			ctx->c_off[c][m] = nullptr;
 			ctx->h_coff[c][m] = nullptr;
 			MIBF_TRY(ctx, cudaMalloc(&ctx->c_seq[c][m], std::max<uint64_t>(nb, 16)));
+			/* packed batches: the chunk's validity words, from a 32-base boundary */
+			MIBF_TRY(ctx, cudaMalloc(&ctx->c_valid[c][m], (nb / 32 + 4) * 4));
 			MIBF_TRY(ctx, cudaMalloc(&ctx->c_off[c][m], (nr + 1) * 8));
 			MIBF_TRY(ctx, cudaMallocHost(&ctx->h_coff[c][m], (nr + 1) * 8));
 		}
@@ -2057,6 +2104,7 @@ static int classify_host_chunks(bbt_mibf *ctx, const bbt_batch *b, bbt_mibf_resu
 		return BBT_OK;
 	}
 	const bool paired = b->seq2 != nullptr;
+	const bool packed = b->encoding == BBT_BASES_2BIT;
 	auto bases = [&](uint64_t lo, uint64_t hi) {
 		uint64_t x = b->offsets[hi] - b->offsets[lo];
 		if (paired)
@@ -2118,12 +2166,23 @@ static int classify_host_chunks(bbt_mibf *ctx, const bbt_batch *b, bbt_mibf_resu
 			const char *seq = m ? b->seq2 : b->seq;
 			const uint64_t *off = m ? b->offsets2 : b->offsets;
 			uint64_t *ho = ctx->h_coff[sl][m];
-			const uint64_t o0 = off[r0];
+			/* packed: the chunk's code and validity words from the 32-base
+			 * boundary at or before its first base */
+			const uint64_t o0 = packed ? off[r0] & ~31ull : off[r0];
 			for (uint64_t i = 0; i <= cnt; ++i)
 				ho[i] = off[r0 + i] - o0;
-			if (off[r1] > o0)
+			if (packed && off[r1] > o0) {
+				const uint32_t *w = reinterpret_cast<const uint32_t *>(seq);
+				const uint32_t *v = m ? b->valid2 : b->valid;
+				MIBF_TRY(ctx, cudaMemcpyAsync(ctx->c_seq[sl][m], w + o0 / 16,
+						(off[r1] - o0 + 15) / 16 * 4, cudaMemcpyHostToDevice, ctx->h2d));
+				if (v)
+					MIBF_TRY(ctx, cudaMemcpyAsync(ctx->c_valid[sl][m], v + o0 / 32,
+							(off[r1] - o0 + 31) / 32 * 4, cudaMemcpyHostToDevice, ctx->h2d));
+			} else if (off[r1] > o0) {
 				MIBF_TRY(ctx, cudaMemcpyAsync(ctx->c_seq[sl][m], seq + o0, off[r1] - o0,
 						cudaMemcpyHostToDevice, ctx->h2d));
+			}
 			MIBF_TRY(ctx, cudaMemcpyAsync(ctx->c_off[sl][m], ho, (cnt + 1) * 8,
 					cudaMemcpyHostToDevice, ctx->h2d));
 		}
@@ -2140,10 +2199,14 @@ static int classify_host_chunks(bbt_mibf *ctx, const bbt_batch *b, bbt_mibf_resu
 		const uint64_t r0 = cuts[c], cnt = cuts[c + 1] - r0;
 		MIBF_TRY(ctx, cudaStreamWaitEvent(s, ctx->c_copied[sl], 0));
 		const int phase = (c == 0 ? kQueryBegin : 0) | (c + 1 == nchunks ? kQueryEnd : 0);
+		MibfEncoding enc;
+		enc.packed = packed;
+		enc.valid[0] = packed && b->valid ? ctx->c_valid[sl][0] : nullptr;
+		enc.valid[1] = packed && paired && b->valid2 ? ctx->c_valid[sl][1] : nullptr;
 		rc = run_query_sc(ctx, cnt, ctx->c_seq[sl][0], ctx->c_off[sl][0],
 				paired ? ctx->c_seq[sl][1] : nullptr, paired ? ctx->c_off[sl][1] : nullptr,
 				ctx->d_hits + r0 * res->max_hits, res->max_hits, ctx->d_nhits + r0,
-				ctx->d_sat + r0, s, sc, true, phase, n);
+				ctx->d_sat + r0, s, sc, true, phase, n, enc);
 		if (rc)
 			return rc;
 		MIBF_TRY(ctx, cudaEventRecord(ctx->c_computed[sl], s));

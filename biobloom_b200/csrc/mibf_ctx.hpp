@@ -116,6 +116,7 @@ struct bbt_mibf {
 	/* host-batch pipeline: two chunk slots, each with its chunk's bases and
 	 * rebased offsets on the device and the offsets in pinned memory */
 	uint8_t *c_seq[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+	uint32_t *c_valid[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}}; /* packed batches */
 	uint64_t *c_off[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 	uint64_t *h_coff[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 	uint64_t c_bases_cap = 0, c_reads_cap = 0;
