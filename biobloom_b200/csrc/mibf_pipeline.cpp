@@ -26,6 +26,11 @@ namespace {
 
 struct MiBatch {
 	std::vector<char> seq[2];
+	/* the bases 2-bit packed with validity bits, as the batch goes to the
+	 * device (the ASCII bases stay for the output records); bad: a mate has
+	 * bases that are not ACGT (else its validity bits are not sent) */
+	std::vector<uint32_t> pw[2], pv[2];
+	bool bad[2] = {false, false};
 	std::vector<uint64_t> off[2];
 	std::vector<std::string> name[2], comment[2], qual[2];
 	uint64_t n = 0;
@@ -138,6 +143,14 @@ int run(bbt_mibf *ctx, const std::vector<std::string> &files, const std::string 
 			if (have) {
 				std::string perr;
 				bool more = fill(b, r1, r2, keep_qual, perr);
+				for (int m = 0; b.n && m < (paired ? 2 : 1); ++m) {
+					const uint64_t nb = b.seq[m].size();
+					b.pw[m].resize(nb / 16 + 2);
+					b.pv[m].resize(nb / 32 + 2);
+					uint64_t nbad = 0;
+					bbt_pack_bases(b.seq[m].data(), nb, b.pw[m].data(), b.pv[m].data(), &nbad);
+					b.bad[m] = nbad != 0;
+				}
 				if (!perr.empty())
 					std::cerr << "warning: " << perr << "; reading of this file stopped there"
 					          << std::endl;
@@ -173,12 +186,15 @@ int run(bbt_mibf *ctx, const std::vector<std::string> &files, const std::string 
 		const bool last = b.last;
 		if (b.n) {
 			bbt_batch bt = {};
-			bt.seq = b.seq[0].data();
+			bt.seq = (const char *)b.pw[0].data();
 			bt.offsets = b.off[0].data();
-			bt.seq2 = paired ? b.seq[1].data() : nullptr;
+			bt.seq2 = paired ? (const char *)b.pw[1].data() : nullptr;
 			bt.offsets2 = paired ? b.off[1].data() : nullptr;
 			bt.n_reads = b.n;
 			bt.location = BBT_HOST;
+			bt.encoding = BBT_BASES_2BIT;
+			bt.valid = b.bad[0] ? b.pv[0].data() : nullptr;
+			bt.valid2 = paired && b.bad[1] ? b.pv[1].data() : nullptr;
 			uint32_t mh = std::min<uint32_t>(8, nids);
 			for (;;) {
 				hits.resize(b.n * mh);
