@@ -98,51 +98,6 @@ __device__ __forceinline__ uint8_t base_code_at(const Bases &b, uint64_t j)
 	return (uint8_t)((__ldg(b.words + (g >> 4)) >> (2u * (uint32_t)(g & 15u))) & 3u);
 }
 
-/* Sequential reader of a read's base codes for one thread: bases are fetched
- * 16 at a time (the aligned 16-byte block of ASCII bases holding the base, or
- * the 2-bit code word and its validity bits), so that a thread walking a read
- * makes one load per 16 bases.  Calls must ask for non-decreasing j.  (An
- * aligned 16-byte block never crosses a page, so reading all of the block that
- * holds a valid base stays inside mapped memory.) */
-struct BaseStream {
-	Bases src;
-	uint64_t blk;
-	uint4 buf;
-
-	__device__ __forceinline__ void init(const Bases &s)
-	{
-		src = s;
-		blk = ~0ull;
-	}
-
-	__device__ __forceinline__ uint8_t code(uint64_t j)
-	{
-		const uint64_t g = src.g0 + j;
-		if (src.ascii) {
-			const uintptr_t p = reinterpret_cast<uintptr_t>(src.ascii + g);
-			const uint64_t b = p >> 4;
-			if (b != blk) {
-				blk = b;
-				buf = __ldg(reinterpret_cast<const uint4 *>(b << 4));
-			}
-			const uint32_t o = (uint32_t)(p & 15u);
-			const uint32_t w = o < 8 ? (o < 4 ? buf.x : buf.y) : (o < 12 ? buf.z : buf.w);
-			return base_code((uint8_t)(w >> (8u * (o & 3u))));
-		}
-		const uint64_t b = g >> 4;
-		if (b != blk) {
-			blk = b;
-			buf.x = __ldg(src.words + b);
-			buf.y = src.valid ? (__ldg(src.valid + (g >> 5)) >> (16u * (uint32_t)(b & 1u)))
-			                  : 0xffffu;
-		}
-		const uint32_t o = (uint32_t)(g & 15u);
-		if (!((buf.y >> o) & 1u))
-			return 4;
-		return (uint8_t)((buf.x >> (2u * o)) & 3u);
-	}
-};
-
 /* Hash frames [w0, w0 + wn) of the read whose bases src describes into the
  * window: base codes are staged with coalesced loads, then each lane hashes S
  * consecutive frames (Horner over its first k-mer, rolling after), and the
