@@ -1010,7 +1010,7 @@ def run_single(args):
         bbc.set_schedule(1024 if pinned == L.PATH_PERSISTENT else 0)
         tune = {"path": pinned, "warps_per_block": 8, "frames_per_lane": 4,
                 "long_bases": 1024 if pinned == L.PATH_PERSISTENT else 0,
-                "reads_per_launch": 0, "reads_per_s": None, "pinned": True}
+                "reads_per_launch": 0, "reads_per_s": None, "full_steps": 0, "pinned": True}
         if args.bucketing:
             kv = {x.split("=")[0].strip(): int(x.split("=")[1]) for x in args.bucketing.split(",")}
             bbc.set_bucketing(**kv)

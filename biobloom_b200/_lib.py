@@ -68,7 +68,8 @@ class FilterView(ctypes.Structure):
 class Tune(ctypes.Structure):
     _fields_ = [("path", ctypes.c_int), ("warps_per_block", ctypes.c_int),
                 ("frames_per_lane", ctypes.c_int), ("long_bases", ctypes.c_uint64),
-                ("reads_per_launch", ctypes.c_uint64), ("reads_per_s", ctypes.c_double)]
+                ("reads_per_launch", ctypes.c_uint64), ("reads_per_s", ctypes.c_double),
+                ("full_steps", ctypes.c_int)]
 
 
 class SynthReadParams(ctypes.Structure):
@@ -167,6 +168,7 @@ def lib():
         "bbt_last_stats": (i32, [vp, P(Stats)]),
         "bbt_set_counting": (i32, [vp, i32]),
         "bbt_set_launch": (i32, [vp, i32, i32, i32]),
+        "bbt_set_steps": (i32, [vp, i32]),
         "bbt_set_inclusive": (i32, [vp, i32]),
         "bbt_set_schedule": (i32, [vp, u64]),
         "bbt_autotune": (i32, [vp, P(Batch), P(Tune)]),

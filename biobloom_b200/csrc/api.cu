@@ -386,6 +386,7 @@ static LaunchConfig pick_config(const bbt_ctx *ctx)
 	lc.seg = ctx->p.frames_per_lane == 8 ? 8 : 4;
 	lc.num_sms = ctx->num_sms;
 	lc.count = 0;
+	lc.full_steps = ctx->full_steps;
 	return lc;
 }
 
@@ -1949,19 +1950,41 @@ extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int s
 	return rc;
 }
 
+static int set_steps_one(bbt_ctx *ctx, int full_steps)
+{
+	if (!ctx)
+		return BBT_ERR_ARG;
+	if (full_steps != 0 && full_steps != 1)
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_steps: full_steps must be 0 or 1");
+	ctx->full_steps = full_steps;
+	int cnt = ctx->lc.count;
+	ctx->lc = pick_config(ctx);
+	ctx->lc.count = cnt;
+	return BBT_OK;
+}
+
+extern "C" int bbt_set_steps(bbt_ctx *ctx, int full_steps)
+{
+	int rc = set_steps_one(ctx, full_steps);
+	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
+		if ((rc = set_steps_one(ctx->peers[i], full_steps)) != BBT_OK)
+			fail(ctx, rc, ctx->peers[i]->err);
+	return rc;
+}
+
 static int set_bucketing_one(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
 		unsigned phase_min, uint64_t max_frames, unsigned levels_per_round)
 {
-	if (levels_per_round > 64)
-		return fail(ctx, BBT_ERR_ARG, "bbt_set_bucketing: levels_per_round must be at most 64");
-	if (levels_per_round)
-		ctx->bk_levels = levels_per_round;
 	if (!ctx)
 		return BBT_ERR_ARG;
+	if (levels_per_round > 64)
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_bucketing: levels_per_round must be at most 64");
 	if (bucket_shift && (bucket_shift < 12 || bucket_shift > 34))
 		return fail(ctx, BBT_ERR_ARG, "bbt_set_bucketing: bucket_shift must be in [12, 34]");
 	if (phase_split > kBkPhaseDen)
 		return fail(ctx, BBT_ERR_ARG, "bbt_set_bucketing: phase_split must be at most 16");
+	if (levels_per_round)
+		ctx->bk_levels = levels_per_round;
 	if (bucket_shift)
 		ctx->bk_bshift = bucket_shift;
 	if (phase_split)
@@ -2059,21 +2082,28 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 	bbt_tune best;
 	memset(&best, 0, sizeof best);
 	float best_ms = 1e30f;
+	const int saved_full = ctx->full_steps;
 	struct Cand {
 		int path, warps, seg;
 		uint64_t long_bases;
+		int full;
 	};
 	std::vector<Cand> cands;
 	for (int w : {4, 8})
 		for (int sg : {4, 8}) {
-			cands.push_back({BBT_PATH_PLAIN, w, sg, 0});
-			cands.push_back({BBT_PATH_PERSISTENT, w, sg, 0});
-			cands.push_back({BBT_PATH_PERSISTENT, w, sg, 1024});
+			cands.push_back({BBT_PATH_PLAIN, w, sg, 0, 0});
+			/* the persistent kernel with steps sized to the read's decision
+			 * (fewer probes: filters in HBM) and with 32-frame steps (fewer
+			 * steps: filters held in L2) */
+			for (int full : {0, 1}) {
+				cands.push_back({BBT_PATH_PERSISTENT, w, sg, 0, full});
+				cands.push_back({BBT_PATH_PERSISTENT, w, sg, 1024, full});
+			}
 			if (auto_path(ctx) == BBT_PATH_FILTER_MAJOR)
-				cands.push_back({BBT_PATH_FILTER_MAJOR, w, sg, 0});
+				cands.push_back({BBT_PATH_FILTER_MAJOR, w, sg, 0, 0});
 		}
 	if (bucketing_pays(ctx))
-		cands.push_back({BBT_PATH_BUCKETED, 8, 4, 0});
+		cands.push_back({BBT_PATH_BUCKETED, 8, 4, 0, 0});
 	const int cnt = ctx->lc.count;
 	for (const Cand &c : cands) {
 		if (rc)
@@ -2081,6 +2111,7 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 		ctx->p.path = c.path;
 		ctx->p.warps_per_block = c.warps;
 		ctx->p.frames_per_lane = c.seg;
+		ctx->full_steps = c.full;
 		ctx->lc = pick_config(ctx);
 		ctx->lc.count = 0;
 		ctx->long_bases = c.long_bases;
@@ -2094,6 +2125,7 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 			best.warps_per_block = c.warps;
 			best.frames_per_lane = c.seg;
 			best.long_bases = c.long_bases;
+			best.full_steps = c.full;
 		}
 	}
 	/* reads per launch for the best kernel configuration */
@@ -2102,6 +2134,7 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 		ctx->p.path = best.path;
 		ctx->p.warps_per_block = best.warps_per_block;
 		ctx->p.frames_per_lane = best.frames_per_lane;
+		ctx->full_steps = best.full_steps;
 		ctx->lc = pick_config(ctx);
 		ctx->lc.count = 0;
 		ctx->long_bases = best.long_bases;
@@ -2130,6 +2163,7 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 	if (rc) {
 		ctx->p = saved_p;
 		ctx->long_bases = saved_long;
+		ctx->full_steps = saved_full;
 		ctx->lc = pick_config(ctx);
 		ctx->lc.count = cnt;
 		return rc;

@@ -336,12 +336,13 @@ size_t classify_smem_bytes(const LaunchConfig &lc, uint32_t kmax)
 
 cudaError_t launch_classify(const ClassifyArgs &a0, const LaunchConfig &lc, cudaStream_t s)
 {
-	/* The persistent kernel is bound by DRAM traffic: it takes steps sized to
-	 * the read's decision, which probe fewer frames.  The plain kernel is
-	 * bound by the latency of each warp's chain of steps: it keeps 32-frame
-	 * steps, which take fewer of them. */
+	/* The persistent kernel on a filter in HBM is bound by DRAM traffic: it
+	 * takes steps sized to the read's decision, which probe fewer frames.  The
+	 * plain kernel, and the persistent one on a filter held in L2 (full_steps,
+	 * chosen by the autotuner), are bound by the chain of steps and the
+	 * instructions per step: they keep 32-frame steps, fewer of them. */
 	ClassifyArgs a = a0;
-	a.tight_steps = lc.path != BBT_PATH_PLAIN;
+	a.tight_steps = lc.path != BBT_PATH_PLAIN && !lc.full_steps;
 	return lc.seg == 8 ? launch_seg<8>(a, lc, s) : launch_seg<4>(a, lc, s);
 }
 

@@ -340,7 +340,8 @@ int bbt_set_bucketing(bbt_ctx *ctx, unsigned bucket_shift, unsigned phase_split,
 /*
  * Autotuner: time every kernel configuration on a device-resident sample
  * (path plain / persistent / persistent long-first / filter-major when the
- * filters fit in L2; 4 or 8 warps per block; 4 or 8 frames per lane), keep
+ * filters fit in L2; 4 or 8 warps per block; 4 or 8 frames per lane; the
+ * persistent path with either step size of bbt_set_steps), keep
  * the fastest, then pick the reads per launch (64k, 256k, 1M or the whole
  * sample) for it, and leave the context set to the result.  The summary
  * counters are left as they were.  No reference counterpart (the reference's
@@ -353,8 +354,16 @@ typedef struct {
 	uint64_t long_bases;        /* bbt_set_schedule value */
 	uint64_t reads_per_launch;  /* 0 = whole batches (no split was faster) */
 	double reads_per_s;         /* on the sample */
+	int full_steps;             /* bbt_set_steps value */
 } bbt_tune;
 int bbt_autotune(bbt_ctx *ctx, const bbt_batch *sample, bbt_tune *out);
+
+/* Step sizes of the persistent path (SIMPLE and BINOMIAL scoring):
+ * full_steps 0 (the default) probes in steps sized to the frames that could
+ * still decide the read (fewer probes: filters in HBM); 1 keeps 32-frame steps
+ * (fewer steps and instructions: filters held in L2).  bbt_autotune tries
+ * both.  Results do not depend on it.  No reference counterpart. */
+int bbt_set_steps(bbt_ctx *ctx, int full_steps);
 
 /*
  * CUDA graph of the classification of one device batch in launches of

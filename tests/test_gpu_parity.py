@@ -36,9 +36,9 @@ def _classifier(paths, score=0.15, streak=3, **kw):
 
 PATHS = [dict(path=1), dict(path=2), dict(path=2, frames_per_lane=8),
          dict(path=1, warps_per_block=4, frames_per_lane=8), dict(path=3),
-         dict(path=3, frames_per_lane=8)]
+         dict(path=3, frames_per_lane=8), dict(path=2, full_steps=1)]
 PATH_IDS = ["plain", "persistent", "persistent-seg8", "plain-w4-seg8", "filter-major",
-            "filter-major-seg8"]
+            "filter-major-seg8", "persistent-full-steps"]
 
 
 @pytest.mark.parametrize("launch", PATHS, ids=PATH_IDS)
