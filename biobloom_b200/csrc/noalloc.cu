@@ -22,8 +22,7 @@
  * with the call's GPU current, in noalloc_scratch() below.  The address is not
  * cached: after a cudaDeviceReset in the caller's process the GPU has a new
  * context, in which the array may sit at another address.  The first call on a
- * GPU also loads the library's device code there, so that first call should
- * come before any stream capture.
+ * GPU also loads the library's device code there.
  */
 #include <cuda_runtime.h>
 

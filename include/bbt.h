@@ -432,9 +432,9 @@ int bbt_make_filter(const char *seq, const uint64_t *offsets, uint64_t n_seqs,
  * rejected with BBT_ERR_ARG).  The kernel's scratch (filter table and work
  * counter) is one small array of device memory per GPU that lives as long as
  * the library is loaded; every call on that GPU shares it, so calls that
- * overlap on the GPU race and must be issued one after another.  The first
- * call on each GPU looks up the array's device address, so make that first
- * call before any stream capture.
+ * overlap on the GPU race and must be issued one after another.  Each call
+ * looks up the array's device address (cudaGetSymbolAddress) and copies the
+ * filter table into it with cudaMemcpyAsync on `stream`.
  */
 #define BBT_NOALLOC_MAX_FILTERS 64
 typedef struct {
