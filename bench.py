@@ -76,6 +76,8 @@ WORKLOAD = ("10 filters x 100 Mbp (k=25, FPR 0.075, h=3), paired 2x150 bp reads,
             "0.5% substitutions, 0.01% N, score 0.15")
 
 
+STEP_FORMS = {"decision": 0, "full": 1, "wide": 2, "wide-full": 3}  # BBT_STEPS_*
+
 def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
@@ -1006,11 +1008,13 @@ def run_single(args):
         tune = bbc.autotune(d1, doff[:sample + 1])
     else:  # a pinned path (the tuner's other choices at their defaults)
         pinned = {"persistent": L.PATH_PERSISTENT, "bucketed": L.PATH_BUCKETED}[args.path]
+        form = STEP_FORMS[args.step_form]
         bbc.set_launch(path=pinned, warps_per_block=8, frames_per_lane=4)
         bbc.set_schedule(1024 if pinned == L.PATH_PERSISTENT else 0)
+        bbc.set_steps(form)
         tune = {"path": pinned, "warps_per_block": 8, "frames_per_lane": 4,
                 "long_bases": 1024 if pinned == L.PATH_PERSISTENT else 0,
-                "reads_per_launch": 0, "reads_per_s": None, "full_steps": 0, "pinned": True}
+                "reads_per_launch": 0, "reads_per_s": None, "steps": form, "pinned": True}
         if args.bucketing:
             kv = {x.split("=")[0].strip(): int(x.split("=")[1]) for x in args.bucketing.split(",")}
             bbc.set_bucketing(**kv)
@@ -1048,6 +1052,14 @@ def run_single(args):
     bbc.classify_device(d1, doff, hits=hits, category=cat, stream=stream)
     stream.synchronize()
     k_ms = bbc.last_stats()["classify_ms"]
+    if tune["path"] != L.PATH_BUCKETED:
+        # filter words the tuned configuration reads (its steps decide how
+        # many frames it probes past a read's decision): counting pass, untimed
+        bbc.set_counting(True)
+        bbc.classify_device(d1, doff, hits=hits, category=cat, stream=stream)
+        stream.synchronize()
+        issued = bbc.last_stats()["probes_issued"]
+        bbc.set_counting(False)
 
     gpu_np = hits.cpu().numpy().view(np.uint64)
 
@@ -1848,6 +1860,8 @@ def main():
     ap.add_argument("--layout", type=int, default=0, help="miBF layout: 0 auto, 1 rank, 2 dense")
     ap.add_argument("--mibf-bucketing", type=int, default=-1, choices=[-1, 0, 1, 2],
                     help="miBF bucketed query (bbt_mibf_set_bucketing mode; -1: the default)")
+    ap.add_argument("--step-form", default="decision", choices=sorted(STEP_FORMS),
+                    help="steps of a pinned persistent path (bbt_set_steps)")
     ap.add_argument("--path", default="auto", choices=["auto", "persistent", "bucketed"],
                     help="batched path of the single-filter workloads (default: autotuned)")
     ap.add_argument("--bucketing", default="",

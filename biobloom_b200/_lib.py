@@ -20,6 +20,7 @@ SCORE_SIMPLE, SCORE_LENGTH, SCORE_HARMONIC, SCORE_BINOMIAL = 0, 1, 2, 3
 HOST, DEVICE = 0, 1
 BASES_ASCII, BASES_2BIT = 0, 1
 PATH_AUTO, PATH_PLAIN, PATH_PERSISTENT, PATH_FILTER_MAJOR, PATH_BUCKETED = 0, 1, 2, 3, 4
+STEPS_DECISION, STEPS_FULL, STEPS_WIDE, STEPS_WIDE_FULL = 0, 1, 2, 3
 MODE_STD, MODE_ORDERED, MODE_BESTHIT, MODE_SCORES = 0, 1, 2, 3
 
 
@@ -69,7 +70,7 @@ class Tune(ctypes.Structure):
     _fields_ = [("path", ctypes.c_int), ("warps_per_block", ctypes.c_int),
                 ("frames_per_lane", ctypes.c_int), ("long_bases", ctypes.c_uint64),
                 ("reads_per_launch", ctypes.c_uint64), ("reads_per_s", ctypes.c_double),
-                ("full_steps", ctypes.c_int)]
+                ("steps", ctypes.c_int)]
 
 
 class SynthReadParams(ctypes.Structure):

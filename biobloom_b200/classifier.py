@@ -33,7 +33,7 @@ class BioBloomClassifier:
     def __init__(self, filter_paths, score_threshold=None, prefix="", postfix="", *,
                  streak_threshold=3, device=0, path=L.PATH_AUTO, warps_per_block=0,
                  frames_per_lane=0, max_batch_reads=0, max_batch_bases=0, l2_fetch_bytes=0,
-                 score_type="simple", devices=None, full_steps=0):
+                 score_type="simple", devices=None, steps=L.STEPS_DECISION):
         """score_type: "simple", "harmonic" or "binomial" (-S); for binomial the
         score is the -s value, the minimum -10*log10(FPR) of a match [100].
         devices: a list of GPU ordinals to load the filters on (bbt_open_devices;
@@ -80,8 +80,8 @@ class BioBloomClassifier:
         self.filter_ids = [lib.bbt_filter_id(ctx, i).decode() for i in range(self.n_filters)]
         self._inclusive = False
         self.mode = L.MODE_STD
-        if full_steps:
-            self.set_steps(full_steps)
+        if steps:
+            self.set_steps(steps)
 
     # -- reference-style configuration -------------------------------------
     def setInclusive(self):
@@ -143,12 +143,13 @@ class BioBloomClassifier:
         return {"path": t.path, "warps_per_block": t.warps_per_block,
                 "frames_per_lane": t.frames_per_lane, "long_bases": t.long_bases,
                 "reads_per_launch": t.reads_per_launch, "reads_per_s": t.reads_per_s,
-                "full_steps": t.full_steps}
+                "steps": t.steps}
 
-    def set_steps(self, full_steps):
-        """Step sizes of the persistent path (bbt_set_steps): 0 sized to the
-        read's decision, 1 32-frame steps."""
-        L.check(L.lib().bbt_set_steps(self._ctx, int(full_steps)), self._ctx)
+    def set_steps(self, steps):
+        """Steps of the persistent path (bbt_set_steps): STEPS_DECISION sized to
+        the read's decision, STEPS_FULL full 32-frame steps, STEPS_WIDE and
+        STEPS_WIDE_FULL the same with two frames per lane (up to 64 frames)."""
+        L.check(L.lib().bbt_set_steps(self._ctx, int(steps)), self._ctx)
 
     def graph(self, seq, off, hits, seq2=None, off2=None, hits2=None, category=None,
               reads_per_launch=0):

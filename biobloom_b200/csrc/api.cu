@@ -386,7 +386,7 @@ static LaunchConfig pick_config(const bbt_ctx *ctx)
 	lc.seg = ctx->p.frames_per_lane == 8 ? 8 : 4;
 	lc.num_sms = ctx->num_sms;
 	lc.count = 0;
-	lc.full_steps = ctx->full_steps;
+	lc.steps = ctx->steps;
 	return lc;
 }
 
@@ -1950,24 +1950,24 @@ extern "C" int bbt_set_launch(bbt_ctx *ctx, int path, int warps_per_block, int s
 	return rc;
 }
 
-static int set_steps_one(bbt_ctx *ctx, int full_steps)
+static int set_steps_one(bbt_ctx *ctx, int steps)
 {
 	if (!ctx)
 		return BBT_ERR_ARG;
-	if (full_steps != 0 && full_steps != 1)
-		return fail(ctx, BBT_ERR_ARG, "bbt_set_steps: full_steps must be 0 or 1");
-	ctx->full_steps = full_steps;
+	if (steps < BBT_STEPS_DECISION || steps > BBT_STEPS_WIDE_FULL)
+		return fail(ctx, BBT_ERR_ARG, "bbt_set_steps: steps must be one of BBT_STEPS_*");
+	ctx->steps = steps;
 	int cnt = ctx->lc.count;
 	ctx->lc = pick_config(ctx);
 	ctx->lc.count = cnt;
 	return BBT_OK;
 }
 
-extern "C" int bbt_set_steps(bbt_ctx *ctx, int full_steps)
+extern "C" int bbt_set_steps(bbt_ctx *ctx, int steps)
 {
-	int rc = set_steps_one(ctx, full_steps);
+	int rc = set_steps_one(ctx, steps);
 	for (size_t i = 0; ctx && !rc && i < ctx->peers.size(); ++i)
-		if ((rc = set_steps_one(ctx->peers[i], full_steps)) != BBT_OK)
+		if ((rc = set_steps_one(ctx->peers[i], steps)) != BBT_OK)
 			fail(ctx, rc, ctx->peers[i]->err);
 	return rc;
 }
@@ -2082,22 +2082,23 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 	bbt_tune best;
 	memset(&best, 0, sizeof best);
 	float best_ms = 1e30f;
-	const int saved_full = ctx->full_steps;
+	const int saved_steps = ctx->steps;
 	struct Cand {
 		int path, warps, seg;
 		uint64_t long_bases;
-		int full;
+		int steps;
 	};
 	std::vector<Cand> cands;
 	for (int w : {4, 8})
 		for (int sg : {4, 8}) {
 			cands.push_back({BBT_PATH_PLAIN, w, sg, 0, 0});
 			/* the persistent kernel with steps sized to the read's decision
-			 * (fewer probes: filters in HBM) and with 32-frame steps (fewer
-			 * steps: filters held in L2) */
-			for (int full : {0, 1}) {
-				cands.push_back({BBT_PATH_PERSISTENT, w, sg, 0, full});
-				cands.push_back({BBT_PATH_PERSISTENT, w, sg, 1024, full});
+			 * (fewer probes: filters in HBM) and with full steps (fewer steps:
+			 * filters held in L2), one or two frames per lane */
+			for (int st : {BBT_STEPS_DECISION, BBT_STEPS_FULL, BBT_STEPS_WIDE,
+					BBT_STEPS_WIDE_FULL}) {
+				cands.push_back({BBT_PATH_PERSISTENT, w, sg, 0, st});
+				cands.push_back({BBT_PATH_PERSISTENT, w, sg, 1024, st});
 			}
 			if (auto_path(ctx) == BBT_PATH_FILTER_MAJOR)
 				cands.push_back({BBT_PATH_FILTER_MAJOR, w, sg, 0, 0});
@@ -2111,7 +2112,7 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 		ctx->p.path = c.path;
 		ctx->p.warps_per_block = c.warps;
 		ctx->p.frames_per_lane = c.seg;
-		ctx->full_steps = c.full;
+		ctx->steps = c.steps;
 		ctx->lc = pick_config(ctx);
 		ctx->lc.count = 0;
 		ctx->long_bases = c.long_bases;
@@ -2125,7 +2126,7 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 			best.warps_per_block = c.warps;
 			best.frames_per_lane = c.seg;
 			best.long_bases = c.long_bases;
-			best.full_steps = c.full;
+			best.steps = c.steps;
 		}
 	}
 	/* reads per launch for the best kernel configuration */
@@ -2134,7 +2135,7 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 		ctx->p.path = best.path;
 		ctx->p.warps_per_block = best.warps_per_block;
 		ctx->p.frames_per_lane = best.frames_per_lane;
-		ctx->full_steps = best.full_steps;
+		ctx->steps = best.steps;
 		ctx->lc = pick_config(ctx);
 		ctx->lc.count = 0;
 		ctx->long_bases = best.long_bases;
@@ -2163,7 +2164,7 @@ extern "C" int bbt_autotune(bbt_ctx *ctx, const bbt_batch *b, bbt_tune *out)
 	if (rc) {
 		ctx->p = saved_p;
 		ctx->long_bases = saved_long;
-		ctx->full_steps = saved_full;
+		ctx->steps = saved_steps;
 		ctx->lc = pick_config(ctx);
 		ctx->lc.count = cnt;
 		return rc;

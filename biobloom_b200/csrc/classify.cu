@@ -38,10 +38,25 @@ namespace bbt {
 
 namespace {
 
+/* Valid-frame bits of frames [c, c + n) of the window (n <= 32). */
+template <int SEG>
+__device__ __forceinline__ uint32_t step_bits(const Window<SEG> &win, int c, int n)
+{
+	const int vi = c >> 5, vs = c & 31;
+	uint32_t V = win.vmask[vi] >> vs;
+	if (vs && vi + 1 < SEG)
+		V |= win.vmask[vi + 1] << (32 - vs);
+	if (n < 32)
+		V &= (1u << n) - 1u;
+	return V;
+}
+
 /* Evaluate read r against filters [f0, f1).  Returns the hit bits of those
  * filters that fall in word f0 / 64 (bit f % 64); read-major launches call it
- * with the whole filter range and write every word themselves. */
-template <int SEG, bool COUNT, int MODE>
+ * with the whole filter range and write every word themselves.  WIDE: every
+ * lane probes two frames per step (steps of up to 64 frames), twice the word
+ * reads in flight per warp. */
+template <int SEG, bool COUNT, int MODE, bool WIDE>
 __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, uint32_t f1,
 		const Window<SEG> &win, int lane, uint64_t &myword, unsigned long long &probe_acc,
 		unsigned long long &frame_acc, unsigned long long &alg_acc)
@@ -90,34 +105,59 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 					frame_acc += (lane == 0) ? (unsigned long long)wn : 0ull;
 			}
 			for (int c = 0; c < wn;) {
-				/* frames [c, c + nfc) of the window this step */
-				const int nfc = min((length_mode || seq_mode || !a.tight_steps) ? 32
-						: simple_step_frames(st), wn - c);
-				const int q = c + lane;
-				const int32_t p = (int32_t)w0 + q;
-				const int vi = c >> 5, vs = c & 31;
-				uint32_t V = win.vmask[vi] >> vs;
-				if (vs && vi + 1 < SEG)
-					V |= win.vmask[vi + 1] << (32 - vs);
-				if (nfc < 32)
-					V &= (1u << nfc) - 1u;
-				const bool v = (V >> lane) & 1u;
-				const bool probe = v && (length_mode ||
-						p >= (seq_mode ? (int32_t)seq_probe_from(qs) : st.skip_until)) &&
-						!dust_low(a.dust[mate], start + (uint64_t)p);
-				const unsigned r0 = reads;
-				const bool hit = probe && contains(F, win.h0[q], reads);
-				const uint32_t H = __ballot_sync(kFull, hit);
+				/* frames [c, c + nfc) of the window this step: lane l probes
+				 * frame c + l, and with WIDE also frame c + 32 + l; the
+				 * machine then takes them 32 at a time, in frame order */
+				constexpr int cap = WIDE ? 64 : 32;
+				const int nfc = min((length_mode || seq_mode || !a.tight_steps) ? cap
+						: simple_step_frames(st, cap), wn - c);
+				const int n0 = min(nfc, 32);
+				/* frames below this were in a skip window when the step began */
+				const int32_t pf = length_mode ? INT32_MIN
+						: seq_mode ? (int32_t)seq_probe_from(qs) : st.skip_until;
+				auto probe_at = [&](uint32_t V, int q) {
+					const int32_t p = (int32_t)w0 + q;
+					return ((V >> lane) & 1u) && p >= pf &&
+							!dust_low(a.dust[mate], start + (uint64_t)p);
+				};
+				auto advance = [&](uint32_t V, uint32_t H, int b, int n, uint32_t *alg) {
+					return length_mode ? length_chunk(ls, V, H, (int64_t)w0 + b, n, alg)
+							: seq_mode ? seq_chunk(qs, V, H, (int64_t)w0 + b, n, (int)k,
+									a.streak_thr, alg)
+							: simple_chunk(st, V, H, (int32_t)w0 + b, n, (int)k,
+									(int)a.streak_thr, alg);
+				};
+				const uint32_t V0 = step_bits<SEG>(win, c, n0);
+				const bool probe0 = probe_at(V0, c + lane);
 				uint32_t alg = 0;
-				decided = length_mode
-						? length_chunk(ls, V, H, (int64_t)w0 + c, nfc, COUNT ? &alg : nullptr)
-						: seq_mode
-						? seq_chunk(qs, V, H, (int64_t)w0 + c, nfc, (int)k, a.streak_thr,
-								COUNT ? &alg : nullptr)
-						: simple_chunk(st, V, H, (int32_t)w0 + c, nfc, (int)k, (int)a.streak_thr,
-								COUNT ? &alg : nullptr);
-				if (COUNT && ((alg >> lane) & 1u))
-					alg_acc += reads - r0;
+				if (WIDE) {
+					const int n1 = nfc - n0;
+					const uint32_t V1 = n1 > 0 ? step_bits<SEG>(win, c + 32, n1) : 0u;
+					const bool probe1 = probe_at(V1, c + 32 + lane);
+					bool hit0, hit1;
+					unsigned ra = 0, rb = 0;
+					contains2(F, probe0 ? win.h0[c + lane] : 0ull, probe0,
+							probe1 ? win.h0[c + 32 + lane] : 0ull, probe1, hit0, hit1, ra, rb);
+					reads += ra + rb;
+					const uint32_t H0 = __ballot_sync(kFull, hit0);
+					const uint32_t H1 = __ballot_sync(kFull, hit1);
+					decided = advance(V0, H0, c, n0, COUNT ? &alg : nullptr);
+					if (COUNT && ((alg >> lane) & 1u))
+						alg_acc += ra;
+					if (!decided && n1 > 0) {
+						alg = 0;
+						decided = advance(V1, H1, c + 32, n1, COUNT ? &alg : nullptr);
+						if (COUNT && ((alg >> lane) & 1u))
+							alg_acc += rb;
+					}
+				} else {
+					const unsigned r0 = reads;
+					const bool hit = probe0 && contains(F, win.h0[c + lane], reads);
+					const uint32_t H = __ballot_sync(kFull, hit);
+					decided = advance(V0, H, c, n0, COUNT ? &alg : nullptr);
+					if (COUNT && ((alg >> lane) & 1u))
+						alg_acc += reads - r0;
+				}
 				if (decided)
 					break;
 				c += nfc;
@@ -137,8 +177,13 @@ enum { ORDER_PLAIN = 0, ORDER_READS = 1 };
  * ORDER_READS:   persistent; warps take reads from a counter, all filters each.
  * (The filter-major order is the two-pass path in twopass.cu.)
  */
-template <int SEG, int ORDER, bool COUNT, int MODE>
-__global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
+/* Blocks of 256 threads the register budget leaves room for (a build
+ * setting: 4 gives each thread up to 64 registers, 32 warps per SM). */
+#ifndef BBT_CLASSIFY_MIN_BLOCKS
+#define BBT_CLASSIFY_MIN_BLOCKS 4
+#endif
+template <int SEG, int ORDER, bool COUNT, int MODE, bool WIDE>
+__global__ void __launch_bounds__(256, BBT_CLASSIFY_MIN_BLOCKS) classify_kernel(ClassifyArgs a)
 {
 	extern __shared__ __align__(16) unsigned char smem[];
 	const int lane = threadIdx.x & 31;
@@ -157,7 +202,7 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 			if (a.order)
 				r = a.order[r];
 			uint64_t myword = 0;
-			classify_read<SEG, COUNT, MODE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
+			classify_read<SEG, COUNT, MODE, WIDE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
 					frame_acc, alg_acc);
 			const uint32_t mate = r >= a.n ? 1u : 0u;
 			if (lane < (int)a.words)
@@ -167,7 +212,7 @@ __global__ void __launch_bounds__(256, 4) classify_kernel(ClassifyArgs a)
 		const uint64_t r = (uint64_t)blockIdx.x * (blockDim.x >> 5) + warp;
 		if (r < total) {
 			uint64_t myword = 0;
-			classify_read<SEG, COUNT, MODE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
+			classify_read<SEG, COUNT, MODE, WIDE>(a, r, 0, a.nf, win, lane, myword, probe_acc,
 					frame_acc, alg_acc);
 			const uint32_t mate = r >= a.n ? 1u : 0u;
 			if (lane < (int)a.words)
@@ -277,15 +322,15 @@ __global__ void long_first_kernel(ClassifyArgs a, uint64_t long_bases, uint64_t 
 	}
 }
 
-template <int SEG, int ORDER, bool C>
+template <int SEG, int ORDER, bool C, bool WIDE>
 cudaError_t launch_one(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
 {
 	const int threads = lc.warps_per_block * 32;
 	const size_t smem = classify_smem_bytes(lc, a.kmax);
-	auto kern = a.scoring == BBT_SCORE_LENGTH ? classify_kernel<SEG, ORDER, C, BBT_SCORE_LENGTH>
-	          : a.scoring == BBT_SCORE_HARMONIC ? classify_kernel<SEG, ORDER, C, BBT_SCORE_HARMONIC>
-	          : a.scoring == BBT_SCORE_BINOMIAL ? classify_kernel<SEG, ORDER, C, BBT_SCORE_BINOMIAL>
-	                                            : classify_kernel<SEG, ORDER, C, BBT_SCORE_SIMPLE>;
+	auto kern = a.scoring == BBT_SCORE_LENGTH ? classify_kernel<SEG, ORDER, C, BBT_SCORE_LENGTH, WIDE>
+	          : a.scoring == BBT_SCORE_HARMONIC ? classify_kernel<SEG, ORDER, C, BBT_SCORE_HARMONIC, WIDE>
+	          : a.scoring == BBT_SCORE_BINOMIAL ? classify_kernel<SEG, ORDER, C, BBT_SCORE_BINOMIAL, WIDE>
+	                                            : classify_kernel<SEG, ORDER, C, BBT_SCORE_SIMPLE, WIDE>;
 	cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			(int)smem);
 	if (e != cudaSuccess)
@@ -316,13 +361,17 @@ template <int SEG>
 cudaError_t launch_seg(const ClassifyArgs &a, const LaunchConfig &lc, cudaStream_t s)
 {
 	const bool C = lc.count != 0;
+	const bool W = lc.steps >= BBT_STEPS_WIDE;
 	switch (lc.path) {
 	case BBT_PATH_PLAIN:
-		return C ? launch_one<SEG, ORDER_PLAIN, true>(a, lc, s)
-		         : launch_one<SEG, ORDER_PLAIN, false>(a, lc, s);
+		return C ? launch_one<SEG, ORDER_PLAIN, true, false>(a, lc, s)
+		         : launch_one<SEG, ORDER_PLAIN, false, false>(a, lc, s);
 	default:
-		return C ? launch_one<SEG, ORDER_READS, true>(a, lc, s)
-		         : launch_one<SEG, ORDER_READS, false>(a, lc, s);
+		if (W)
+			return C ? launch_one<SEG, ORDER_READS, true, true>(a, lc, s)
+			         : launch_one<SEG, ORDER_READS, false, true>(a, lc, s);
+		return C ? launch_one<SEG, ORDER_READS, true, false>(a, lc, s)
+		         : launch_one<SEG, ORDER_READS, false, false>(a, lc, s);
 	}
 }
 
@@ -336,13 +385,16 @@ size_t classify_smem_bytes(const LaunchConfig &lc, uint32_t kmax)
 
 cudaError_t launch_classify(const ClassifyArgs &a0, const LaunchConfig &lc, cudaStream_t s)
 {
-	/* The persistent kernel on a filter in HBM is bound by DRAM traffic: it
-	 * takes steps sized to the read's decision, which probe fewer frames.  The
-	 * plain kernel, and the persistent one on a filter held in L2 (full_steps,
-	 * chosen by the autotuner), are bound by the chain of steps and the
-	 * instructions per step: they keep 32-frame steps, fewer of them. */
+	/* The persistent kernel on a filter in HBM is bound by DRAM traffic and
+	 * the latency of its dependent word reads: it takes steps sized to the
+	 * read's decision, which probe fewer frames, with two frames per lane
+	 * (BBT_STEPS_WIDE) for twice the reads in flight.  The plain kernel, and
+	 * the persistent one on a filter held in L2 (BBT_STEPS_FULL, chosen by the
+	 * autotuner), are bound by the chain of steps and the instructions per
+	 * step: they keep full steps, fewer of them. */
 	ClassifyArgs a = a0;
-	a.tight_steps = lc.path != BBT_PATH_PLAIN && !lc.full_steps;
+	a.tight_steps = lc.path != BBT_PATH_PLAIN &&
+			(lc.steps == BBT_STEPS_DECISION || lc.steps == BBT_STEPS_WIDE);
 	return lc.seg == 8 ? launch_seg<8>(a, lc, s) : launch_seg<4>(a, lc, s);
 }
 

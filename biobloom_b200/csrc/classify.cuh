@@ -83,8 +83,7 @@ struct LaunchConfig {
 	int seg;              /* frames per lane when hashing: 4 or 8 */
 	int num_sms;
 	int count;            /* gather probe / frame counters */
-	int full_steps;       /* persistent path: 32-frame steps instead of steps sized
-	                         to the read's decision */
+	int steps;            /* persistent path: BBT_STEPS_* (bbt_set_steps) */
 };
 
 /* Dynamic shared memory one block needs. */

@@ -144,7 +144,7 @@ struct bbt_ctx {
 	uint32_t bk_phase_split = 4;         /* phase boundary in sixteenths (16: one phase) */
 	uint32_t bk_phase_min = 64;          /* the first phase covers min(F, 64) frames or more */
 	uint32_t bk_levels = 1;              /* hash levels per round */
-	int full_steps = 0;                  /* bbt_set_steps */
+	int steps = BBT_STEPS_DECISION;      /* bbt_set_steps */
 	/* bbt_open_devices: the same filters opened on the other devices; host
 	 * batches are split across this context and these */
 	std::vector<bbt_ctx *> peers;

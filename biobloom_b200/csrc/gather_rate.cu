@@ -9,9 +9,16 @@
  * probe-resolving kernel: 4-byte positions streamed from device memory (read
  * once, marked evict-first so they do not push the table out of L2), eight
  * independent gathers in flight per thread, one bit kept per gather and the
- * bits of 32 gathers written as one word.  Used to choose how large a filter
- * range one probe pass may cover and to state the ceilings the kernels are
- * measured against.
+ * bits of 32 gathers written as one word.  Warps take their chunks of
+ * gathers from a counter, as the persistent classify kernel takes reads: on
+ * B200 a grid-stride loop over a grid of exactly one resident wave served
+ * random gathers into a 2 GB table at 39.7 G/s, the same grid taking chunks
+ * from a counter at 50.8 G/s (and a grid of two or more waves in a
+ * grid-stride loop at 48.8 G/s); each gather is a 128-byte DRAM line fill
+ * either way (122.6 bytes of DRAM reads per gather), so the counter-driven
+ * rate is ~6.2 TB/s of line fills.  Used to choose how large a filter range
+ * one probe pass may cover and to state the ceilings the kernels are measured
+ * against.
  */
 #include <cuda_runtime.h>
 
@@ -43,16 +50,28 @@ __global__ void positions_kernel(uint32_t *pos, uint64_t n, uint64_t bits, uint6
 		pos[i] = (uint32_t)(mix64d(seed ^ i) % bits);
 }
 
+/* A warp takes kTake consecutive chunks per visit to the counter (lane 0
+ * takes them): with one chunk per visit the counter itself limited tables
+ * held in L2 (~204 G gathers/s). */
+constexpr int kTake = 8;
+__device__ __forceinline__ uint64_t next_take(unsigned long long *next, int lane)
+{
+	unsigned long long w = 0;
+	if (lane == 0)
+		w = atomicAdd(next, 1ull);
+	return __shfl_sync(0xffffffffu, w, 0);
+}
+
 /* Resolve-shaped gathers: chunk c of 32 * kPerThread positions per warp. */
 __global__ void __launch_bounds__(256) gather_stream_kernel(const uint32_t *__restrict__ pos,
-		uint64_t n, const uint32_t *__restrict__ table, uint32_t *__restrict__ out)
+		uint64_t n, const uint32_t *__restrict__ table, uint32_t *__restrict__ out,
+		unsigned long long *next)
 {
 	const uint64_t pol = evict_first_policy();
 	const int lane = threadIdx.x & 31;
-	const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
 	const uint64_t chunk = 32ull * kPerThread;
-	for (uint64_t w = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-			w * chunk < n; w += warps) {
+	for (uint64_t t = next_take(next, lane); t * kTake * chunk < n; t = next_take(next, lane))
+	for (uint64_t w = t * kTake; w < (t + 1) * kTake && w * chunk < n; ++w) {
 		const uint64_t base = w * chunk;
 		uint32_t p[kPerThread], v[kPerThread];
 #pragma unroll
@@ -75,13 +94,13 @@ __global__ void __launch_bounds__(256) gather_stream_kernel(const uint32_t *__re
 
 /* Gathers at positions generated in the kernel (no position stream). */
 __global__ void __launch_bounds__(256) gather_hash_kernel(uint64_t n, uint64_t bits,
-		uint64_t seed, const uint32_t *__restrict__ table, uint32_t *__restrict__ out)
+		uint64_t seed, const uint32_t *__restrict__ table, uint32_t *__restrict__ out,
+		unsigned long long *next)
 {
 	const int lane = threadIdx.x & 31;
-	const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
 	const uint64_t chunk = 32ull * kPerThread;
-	for (uint64_t w = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-			w * chunk < n; w += warps) {
+	for (uint64_t t = next_take(next, lane); t * kTake * chunk < n; t = next_take(next, lane))
+	for (uint64_t w = t * kTake; w < (t + 1) * kTake && w * chunk < n; ++w) {
 		const uint64_t base = w * chunk;
 		uint64_t p[kPerThread];
 		uint32_t v[kPerThread];
@@ -122,6 +141,7 @@ extern "C" int bbt_measure_gather(int device, uint64_t table_bytes, uint64_t n_g
 	const uint64_t entries = table_bytes / 4;
 	const uint64_t bits = entries * 32;
 	uint32_t *table = nullptr, *pos = nullptr, *out = nullptr;
+	unsigned long long *next = nullptr;
 	cudaEvent_t e0 = nullptr, e1 = nullptr;
 	std::vector<float> ms;
 	int rc = BBT_OK;
@@ -129,6 +149,7 @@ extern "C" int bbt_measure_gather(int device, uint64_t table_bytes, uint64_t n_g
 	GR_TRY(cudaMalloc(&table, entries * 4));
 	GR_TRY(cudaMemset(table, 0x5a, entries * 4));
 	GR_TRY(cudaMalloc(&out, (n_gathers / 32 + 1) * 4));
+	GR_TRY(cudaMalloc(&next, sizeof(unsigned long long)));
 	if (position_stream) {
 		GR_TRY(cudaMalloc(&pos, n_gathers * 4));
 		positions_kernel<<<sms * 8, 256>>>(pos, n_gathers, bits, 12345);
@@ -137,11 +158,12 @@ extern "C" int bbt_measure_gather(int device, uint64_t table_bytes, uint64_t n_g
 	GR_TRY(cudaEventCreate(&e0));
 	GR_TRY(cudaEventCreate(&e1));
 	for (int r = 0; r < reps + 1; ++r) {
+		GR_TRY(cudaMemset(next, 0, sizeof(unsigned long long)));
 		GR_TRY(cudaEventRecord(e0));
 		if (position_stream)
-			gather_stream_kernel<<<sms * 8, 256>>>(pos, n_gathers, table, out);
+			gather_stream_kernel<<<sms * 8, 256>>>(pos, n_gathers, table, out, next);
 		else
-			gather_hash_kernel<<<sms * 8, 256>>>(n_gathers, bits, 777 + r, table, out);
+			gather_hash_kernel<<<sms * 8, 256>>>(n_gathers, bits, 777 + r, table, out, next);
 		GR_TRY(cudaGetLastError());
 		GR_TRY(cudaEventRecord(e1));
 		GR_TRY(cudaEventSynchronize(e1));
@@ -161,5 +183,6 @@ done:
 	cudaFree(table);
 	cudaFree(pos);
 	cudaFree(out);
+	cudaFree(next);
 	return rc;
 }

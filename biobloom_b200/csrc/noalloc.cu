@@ -167,7 +167,7 @@ extern "C" int bbt_classify_noalloc(const bbt_filter_view *filters, int n_filter
 		lc.seg = params->frames_per_lane == 8 ? 8 : 4;
 		lc.num_sms = sms;
 		lc.count = 0;
-		lc.full_steps = 0;
+		lc.steps = BBT_STEPS_DECISION;
 		if ((e = launch_classify(a, lc, s)) != cudaSuccess)
 			rc = cuda_fail(nullptr, e, "classify kernel launch");
 	}

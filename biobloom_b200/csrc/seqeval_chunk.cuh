@@ -228,15 +228,16 @@ BBT_HD void binomial_simple_init(SimpleState &s, uint32_t thres, uint64_t frames
 }
 
 /*
- * How many frames the next step should probe (8..32).  At the start of a read
- * and while it is on a run of hits, the step is the number of valid frames
- * that could still accept it if all of them hit (a hit that starts a streak
- * adds 1 to score2, any other hit 2), so a read that accepts wastes no probes
- * on frames after its decision; otherwise (a read that is missing, which
- * rarely accepts) the full 32 frames, which keeps the number of dependent
- * steps, and so the latency of a read, as low as before.  At least 8 frames
- * keep several probes in flight per warp.  The decision itself does not
- * depend on the step sizes.
+ * How many frames the next step should probe (8..cap; cap is 32, or 64 when
+ * every lane probes two frames per step).  At the start of a read and while
+ * it is on a run of hits, the step is the number of valid frames that could
+ * still accept it if all of them hit (a hit that starts a streak adds 1 to
+ * score2, any other hit 2), so a read that accepts wastes no probes on frames
+ * after its decision; otherwise (a read that is missing, which rarely
+ * accepts) the full cap, which keeps the number of dependent steps, and so
+ * the latency of a read, as low as before.  At least 8 frames keep several
+ * probes in flight per warp.  The decision itself does not depend on the step
+ * sizes.
  */
 #ifndef BBT_TIGHT_MIN_STEP
 #define BBT_TIGHT_MIN_STEP 8
@@ -244,20 +245,20 @@ BBT_HD void binomial_simple_init(SimpleState &s, uint32_t thres, uint64_t frames
 #ifndef BBT_TIGHT_REJECT
 #define BBT_TIGHT_REJECT 0
 #endif
-BBT_HD int simple_step_frames(const SimpleState &s)
+BBT_HD int simple_step_frames(const SimpleState &s, int cap = 32)
 {
 	const int32_t gap = s.thres2 - s.score2;
 	if (gap <= 0)
-		return 32;
+		return cap;
 	if (s.started && s.streak == 0) {
 		if (!BBT_TIGHT_REJECT)
-			return 32;
+			return cap;
 		/* a missing read: no reject before anti_thres - anti more misses */
 		const int32_t agap = s.anti_thres - s.anti;
-		return agap < BBT_TIGHT_MIN_STEP ? BBT_TIGHT_MIN_STEP : (agap > 32 ? 32 : (int)agap);
+		return agap < BBT_TIGHT_MIN_STEP ? BBT_TIGHT_MIN_STEP : (agap > cap ? cap : (int)agap);
 	}
 	const int32_t need = (s.streak > 0 || s.flat) ? (gap + 1) / 2 : 1 + gap / 2;
-	return need < BBT_TIGHT_MIN_STEP ? BBT_TIGHT_MIN_STEP : (need > 32 ? 32 : (int)need);
+	return need < BBT_TIGHT_MIN_STEP ? BBT_TIGHT_MIN_STEP : (need > cap ? cap : (int)need);
 }
 
 /*

@@ -354,16 +354,23 @@ typedef struct {
 	uint64_t long_bases;        /* bbt_set_schedule value */
 	uint64_t reads_per_launch;  /* 0 = whole batches (no split was faster) */
 	double reads_per_s;         /* on the sample */
-	int full_steps;             /* bbt_set_steps value */
+	int steps;                  /* bbt_set_steps value (BBT_STEPS_*) */
 } bbt_tune;
 int bbt_autotune(bbt_ctx *ctx, const bbt_batch *sample, bbt_tune *out);
 
-/* Step sizes of the persistent path (SIMPLE and BINOMIAL scoring):
- * full_steps 0 (the default) probes in steps sized to the frames that could
- * still decide the read (fewer probes: filters in HBM); 1 keeps 32-frame steps
- * (fewer steps and instructions: filters held in L2).  bbt_autotune tries
- * both.  Results do not depend on it.  No reference counterpart. */
-int bbt_set_steps(bbt_ctx *ctx, int full_steps);
+/* Steps of the persistent path.  Each step of a warp probes up to 32 frames
+ * of a read, one per lane, or up to 64 with two frames per lane (WIDE: twice
+ * the filter reads in flight, for filters in HBM where the kernel waits on
+ * them).  With SIMPLE and BINOMIAL scoring, DECISION steps are sized to the
+ * frames that could still decide the read (fewer probes: filters in HBM) and
+ * FULL steps are always full (fewer steps and instructions: filters held in
+ * L2).  BBT_STEPS_DECISION is the default; bbt_autotune tries all four.
+ * Results do not depend on it.  No reference counterpart. */
+#define BBT_STEPS_DECISION 0
+#define BBT_STEPS_FULL 1
+#define BBT_STEPS_WIDE 2
+#define BBT_STEPS_WIDE_FULL 3
+int bbt_set_steps(bbt_ctx *ctx, int steps);
 
 /*
  * CUDA graph of the classification of one device batch in launches of

@@ -36,9 +36,11 @@ def _classifier(paths, score=0.15, streak=3, **kw):
 
 PATHS = [dict(path=1), dict(path=2), dict(path=2, frames_per_lane=8),
          dict(path=1, warps_per_block=4, frames_per_lane=8), dict(path=3),
-         dict(path=3, frames_per_lane=8), dict(path=2, full_steps=1)]
+         dict(path=3, frames_per_lane=8), dict(path=2, steps=1), dict(path=2, steps=2),
+         dict(path=2, steps=3, frames_per_lane=8)]
 PATH_IDS = ["plain", "persistent", "persistent-seg8", "plain-w4-seg8", "filter-major",
-            "filter-major-seg8", "persistent-full-steps"]
+            "filter-major-seg8", "persistent-full-steps", "persistent-wide-steps",
+            "persistent-wide-full-steps-seg8"]
 
 
 @pytest.mark.parametrize("launch", PATHS, ids=PATH_IDS)
@@ -171,6 +173,32 @@ def test_random_parity_with_oracle(seed, k, h, score, streak, launch, tmp_path):
     assert np.array_equal(hits, want)
     counts, cats = ol.summary_counts(want, len(filters))
     assert np.array_equal(cat, cats)
+
+
+@pytest.mark.parametrize("score,streak", [(0.15, 3), (0.5, 1)])
+def test_algorithmic_probe_counts_on_every_step_form(score, streak, tmp_path):
+    """The counting pass (bbt_set_counting) reports the filter words the
+    sequential SeqEval::evalSimple reads, whatever the steps of the kernel:
+    plain, persistent with decision-sized, full and two-frames-per-lane steps
+    all count the oracle's number; the words issued are never fewer."""
+    import torch
+    rng, genomes, filters = _random_case(21, n_filters=2, glen=60000)
+    paths = _store(filters, tmp_path, "c")
+    reads = _random_reads(rng, genomes, 2500, lmin=20, lmax=600)
+    seq, off = ol.pack_reads(reads)
+    want, alg = ol.classify(seq, off, filters, score, streak, count_probes=True)
+    dseq = torch.tensor(np.frombuffer(seq, dtype=np.uint8), device="cuda")
+    doff = torch.tensor(off.astype(np.int64), device="cuda")
+    for launch in (dict(path=1), dict(path=2), dict(path=2, steps=1), dict(path=2, steps=2),
+                   dict(path=2, steps=3), dict(path=2, steps=2, frames_per_lane=8)):
+        with _classifier(paths, score, streak, **launch) as bbc:
+            bbc.set_counting(True)
+            hits, _, _ = bbc.classify_device(dseq, doff)
+            torch.cuda.synchronize()
+            st = bbc.last_stats()
+            assert np.array_equal(hits.cpu().numpy().view(np.uint64), want), launch
+            assert st["probes_algorithmic"] == alg, launch
+            assert st["probes_issued"] >= alg, launch
 
 
 def test_device_batches_and_long_reads(tmp_path):

@@ -84,8 +84,10 @@ def _case(seed, k, h, glen=40000, n_filters=2):
     (1, 25, 0, "harmonic", 0.15, 3), (2, 21, 2, "harmonic", 0.45, 1),
     (3, 17, 3, "harmonic", 0.05, 0), (4, 25, 0, "binomial", 100, 3),
     (5, 31, 2, "binomial", 20, 2), (6, 15, 4, "binomial", 60, 5)])
-@pytest.mark.parametrize("path", [1, 2])
-def test_random_modes_match_oracle(seed, k, h, method, score, streak, path, tmp_path):
+@pytest.mark.parametrize("launch", [dict(path=1), dict(path=2), dict(path=2, steps=2),
+                                    dict(path=2, steps=3)],
+                         ids=["plain", "persistent", "persistent-wide", "persistent-wide-full"])
+def test_random_modes_match_oracle(seed, k, h, method, score, streak, launch, tmp_path):
     import torch
     from biobloom_b200 import BioBloomClassifier
     rng, filters, reads = _case(seed, k, h)
@@ -99,7 +101,7 @@ def test_random_modes_match_oracle(seed, k, h, method, score, streak, path, tmp_
     seq, off = ol.pack_reads(reads)
     want, _ = ol.classify(seq, off, filters, thr, streak, scoring)
     with BioBloomClassifier(paths, score, streak_threshold=streak, score_type=method,
-                            path=path) as bbc:
+                            **launch) as bbc:
         hits, _, _ = bbc.classify(reads)
         assert np.array_equal(hits, want)
         dseq = torch.tensor(np.frombuffer(seq, dtype=np.uint8), device="cuda")
@@ -107,7 +109,7 @@ def test_random_modes_match_oracle(seed, k, h, method, score, streak, path, tmp_
         dh, _, _ = bbc.classify_device(dseq, doff)
         torch.cuda.synchronize()
         assert np.array_equal(dh.cpu().numpy().view(np.uint64), want)
-        if path == 2:
+        if launch["path"] == 2:
             gh = torch.zeros_like(dh)
             g = bbc.graph(dseq, doff, gh, reads_per_launch=300)
             s = torch.cuda.Stream()
