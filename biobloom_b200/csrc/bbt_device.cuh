@@ -137,6 +137,54 @@ __device__ __forceinline__ bool contains(const FilterDev &f, uint64_t canon, uns
 	return true;
 }
 
+/* BloomFilter::contains with the reads after the first issued together: the
+ * first bit is read alone (most frames of a read that is not in the filter
+ * stop there); when it is set, the other h - 1 bits (h <= 4) are read at once,
+ * two dependent DRAM round trips instead of h.  The result is contains()'s.
+ * *reads counts the words read; *seq the words the sequential contains()
+ * reads (up to and including the first clear bit). */
+__device__ __forceinline__ bool contains_split(const FilterDev &f, uint64_t canon,
+		unsigned &reads, unsigned &seq)
+{
+	const uint64_t b0 = reduce(canon, f.m, f.minv);
+	++reads;
+	++seq;
+	if (!test_bit(f.words, b0))
+		return false;
+	if (f.h > 4) {
+		for (unsigned i = 1; i < f.h; ++i) {
+			++reads;
+			++seq;
+			uint64_t t = canon * ((uint64_t)i ^ f.kmul);
+			t ^= t >> kMultiShift;
+			if (!test_bit(f.words, reduce(t, f.m, f.minv)))
+				return false;
+		}
+		return true;
+	}
+	uint32_t w[3] = {0u, 0u, 0u};
+	uint64_t b[3] = {0ull, 0ull, 0ull};
+#pragma unroll
+	for (unsigned i = 0; i < 3; ++i) {
+		if (i + 1 < f.h) {
+			uint64_t t = canon * ((uint64_t)(i + 1) ^ f.kmul);
+			t ^= t >> kMultiShift;
+			b[i] = reduce(t, f.m, f.minv);
+			w[i] = __ldg(f.words + (b[i] >> 5));
+		}
+	}
+	bool all = true;
+#pragma unroll
+	for (unsigned i = 0; i < 3; ++i) {
+		if (i + 1 < f.h) {
+			++reads;
+			seq += all ? 1u : 0u;
+			all = all && ((w[i] >> (b[i] & 31u)) & 1u);
+		}
+	}
+	return all;
+}
+
 /* Loads of data read once per pass (the two-pass path's stored hashes):
  * marked evict-first in L2 so that they do not push the filter being probed
  * out of L2, and not allocated in L1. */

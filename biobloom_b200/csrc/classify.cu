@@ -151,12 +151,17 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 							alg_acc += rb;
 					}
 				} else {
+					/* decision-sized steps (filters in HBM) read a frame's
+					 * bits after the first together */
 					const unsigned r0 = reads;
-					const bool hit = probe0 && contains(F, win.h0[c + lane], reads);
+					unsigned sq = 0;
+					const bool hit = probe0 && (a.tight_steps
+							? contains_split(F, win.h0[c + lane], reads, sq)
+							: contains(F, win.h0[c + lane], reads));
 					const uint32_t H = __ballot_sync(kFull, hit);
 					decided = advance(V0, H, c, n0, COUNT ? &alg : nullptr);
 					if (COUNT && ((alg >> lane) & 1u))
-						alg_acc += reads - r0;
+						alg_acc += a.tight_steps ? sq : reads - r0;
 				}
 				if (decided)
 					break;

@@ -155,7 +155,8 @@ def _random_reads(rng, genomes, n, lmin=20, lmax=400, nrate=0.02, sub=0.01):
 
 @pytest.mark.parametrize("seed,k,h,score,streak", [
     (1, 25, 0, 0.15, 3), (2, 21, 2, 0.3, 2), (3, 31, 4, 0.05, 1), (4, 17, 1, 0.9, 5),
-    (5, 25, 3, 0.0, 3), (6, 25, 3, 1.0, 3), (7, 12, 3, 0.4, 0), (8, 64, 3, 0.15, 3)])
+    (5, 25, 3, 0.0, 3), (6, 25, 3, 1.0, 3), (7, 12, 3, 0.4, 0), (8, 64, 3, 0.15, 3),
+    (9, 21, 6, 0.15, 3)])
 @pytest.mark.parametrize("launch", PATHS, ids=PATH_IDS)
 def test_random_parity_with_oracle(seed, k, h, score, streak, launch, tmp_path):
     rng, genomes, filters = _random_case(seed, k=k, h=h, fpr=0.2)
@@ -175,14 +176,15 @@ def test_random_parity_with_oracle(seed, k, h, score, streak, launch, tmp_path):
     assert np.array_equal(cat, cats)
 
 
-@pytest.mark.parametrize("score,streak", [(0.15, 3), (0.5, 1)])
-def test_algorithmic_probe_counts_on_every_step_form(score, streak, tmp_path):
+@pytest.mark.parametrize("score,streak,h", [(0.15, 3, 0), (0.5, 1, 0), (0.15, 3, 2), (0.15, 3, 4),
+                                            (0.3, 2, 7)])
+def test_algorithmic_probe_counts_on_every_step_form(score, streak, h, tmp_path):
     """The counting pass (bbt_set_counting) reports the filter words the
     sequential SeqEval::evalSimple reads, whatever the steps of the kernel:
     plain, persistent with decision-sized, full and two-frames-per-lane steps
     all count the oracle's number; the words issued are never fewer."""
     import torch
-    rng, genomes, filters = _random_case(21, n_filters=2, glen=60000)
+    rng, genomes, filters = _random_case(21, n_filters=2, glen=60000, h=h)
     paths = _store(filters, tmp_path, "c")
     reads = _random_reads(rng, genomes, 2500, lmin=20, lmax=600)
     seq, off = ol.pack_reads(reads)
