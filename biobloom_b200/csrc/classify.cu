@@ -93,6 +93,14 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 		else
 			simple_init(st, a.score, a.one_minus, frames);
 		int decided = EVAL_OPEN;
+		/* decision-sized steps read a frame's bits after the first together
+		 * while at least half of the read's frames probed in its last step
+		 * were hits (a read from the filter's reference: every bit gets read
+		 * anyway, in fewer round trips), one after another otherwise (a read
+		 * that is not in the filter: most frames stop at the first or second
+		 * clear bit, so fewer filter reads); warp-uniform, from the step's
+		 * ballots */
+		bool hitting = true;
 		for (uint64_t w0 = 0; w0 < frames && !decided; w0 += W) {
 			const int wn = (int)min((uint64_t)W, frames - w0);
 			if (cached_k != k || cached_w0 != (int64_t)w0) {
@@ -151,17 +159,21 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 							alg_acc += rb;
 					}
 				} else {
-					/* decision-sized steps (filters in HBM) read a frame's
-					 * bits after the first together */
 					const unsigned r0 = reads;
 					unsigned sq = 0;
-					const bool hit = probe0 && (a.tight_steps
+					const bool split = a.tight_steps && hitting;
+					const bool hit = probe0 && (split
 							? contains_split(F, win.h0[c + lane], reads, sq)
 							: contains(F, win.h0[c + lane], reads));
 					const uint32_t H = __ballot_sync(kFull, hit);
+					if (a.tight_steps) {
+						const uint32_t P = __ballot_sync(kFull, probe0);
+						if (P)
+							hitting = 2 * __popc(H) >= __popc(P);
+					}
 					decided = advance(V0, H, c, n0, COUNT ? &alg : nullptr);
 					if (COUNT && ((alg >> lane) & 1u))
-						alg_acc += a.tight_steps ? sq : reads - r0;
+						alg_acc += split ? sq : reads - r0;
 				}
 				if (decided)
 					break;
