@@ -20,8 +20,11 @@ BIN = os.path.join(PKG, "bin")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Build settings of the kernels (for example "-DBBT_HIT_READS_ALL=1"), space
+# separated; objects are rebuilt by date only, so clear _build/ after a change.
+DEFINES = os.environ.get("BBT_BUILD_DEFINES", "").split()
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-I" + os.path.join(ROOT, "include"), "-I" + CSRC,
-          "-Xcompiler", "-fPIC,-fopenmp,-O3,-Wall", "-ccbin", "/usr/bin/g++"]
+          "-Xcompiler", "-fPIC,-fopenmp,-O3,-Wall", "-ccbin", "/usr/bin/g++"] + DEFINES
 LIB_SOURCES = ["classify.cu", "score.cu", "dust.cu", "twopass.cu", "bucketed.cu", "api.cu", "noalloc.cu", "gather_rate.cu", "maker.cu", "mibf.cu",
                "mibf_make.cu", "formats.cpp", "pack.cpp", "fastx.cpp", "synth.cpp", "mibf_host.cpp",
                "mibf_pipeline.cpp", "server.cpp"]

@@ -185,6 +185,41 @@ __device__ __forceinline__ bool contains_split(const FilterDev &f, uint64_t cano
 	return all;
 }
 
+/* BloomFilter::contains with all h bits (h <= 4) read at once: one DRAM round
+ * trip, at the price of the words after a clear bit.  The result is
+ * contains()'s; *reads counts the words read, *seq the words the sequential
+ * contains() reads. */
+__device__ __forceinline__ bool contains_all(const FilterDev &f, uint64_t canon,
+		unsigned &reads, unsigned &seq)
+{
+	if (f.h > 4)
+		return contains_split(f, canon, reads, seq);
+	uint32_t w[4] = {0u, 0u, 0u, 0u};
+	uint64_t b[4] = {0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+	for (unsigned i = 0; i < 4; ++i) {
+		if (i < f.h) {
+			uint64_t t = canon;
+			if (i) {
+				t = canon * ((uint64_t)i ^ f.kmul);
+				t ^= t >> kMultiShift;
+			}
+			b[i] = reduce(t, f.m, f.minv);
+			w[i] = __ldg(f.words + (b[i] >> 5));
+		}
+	}
+	bool all = true;
+#pragma unroll
+	for (unsigned i = 0; i < 4; ++i) {
+		if (i < f.h) {
+			++reads;
+			seq += all ? 1u : 0u;
+			all = all && ((w[i] >> (b[i] & 31u)) & 1u);
+		}
+	}
+	return all;
+}
+
 /* Loads of data read once per pass (the two-pass path's stored hashes):
  * marked evict-first in L2 so that they do not push the filter being probed
  * out of L2, and not allocated in L1. */

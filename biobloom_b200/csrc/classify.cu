@@ -51,6 +51,12 @@ __device__ __forceinline__ uint32_t step_bits(const Window<SEG> &win, int c, int
 	return V;
 }
 
+/* Build setting: a read whose frames mostly hit reads all h bits of a frame
+ * at once (1) instead of the first, then the others together (0). */
+#ifndef BBT_HIT_READS_ALL
+#define BBT_HIT_READS_ALL 0
+#endif
+
 /* Evaluate read r against filters [f0, f1).  Returns the hit bits of those
  * filters that fall in word f0 / 64 (bit f % 64); read-major launches call it
  * with the whole filter range and write every word themselves.  WIDE: every
@@ -163,7 +169,9 @@ __device__ void classify_read(const ClassifyArgs &a, uint64_t r, uint32_t f0, ui
 					unsigned sq = 0;
 					const bool split = a.tight_steps && hitting;
 					const bool hit = probe0 && (split
-							? contains_split(F, win.h0[c + lane], reads, sq)
+							? (BBT_HIT_READS_ALL
+								? contains_all(F, win.h0[c + lane], reads, sq)
+								: contains_split(F, win.h0[c + lane], reads, sq))
 							: contains(F, win.h0[c + lane], reads));
 					const uint32_t H = __ballot_sync(kFull, hit);
 					if (a.tight_steps) {
