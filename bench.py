@@ -259,6 +259,15 @@ def native_libs():
     return sorted(out)
 
 
+def bf_config(args):
+    """The 10-filter workload's config, the same on the GPU arm and on the
+    reference arm (figures of the run sit beside it in the line)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"workload": WORKLOAD, "pairs_per_gpu": args.pairs, "reads_per_gpu": 2 * args.pairs,
+            "filters": N_FILTERS, "l2": "inputs larger than L2 (3 GB reads + 685 MB filters)",
+            "parallelism": f"replicas x{world} (reads sharded, filters replicated)"}
+
+
 def ref_rank_zero():
     """The reference arm runs on rank 0 only; the other ranks exit without work."""
     return int(os.environ.get("RANK", "0")) == 0
@@ -343,8 +352,8 @@ def run_reference(args):
                               f"first {n} pairs of the workload per step, "
                               "BioBloomClassifier::filterPair compiled from the reference "
                               f"sources, {threads} OpenMP threads, filter load excluded",
-                              threads, {"config": {"workload": WORKLOAD, "pairs_per_step": n,
-                                                   "filters": N_FILTERS}})), flush=True)
+                              threads, {"config": bf_config(args), "pairs_per_step": n})),
+          flush=True)
 
 
 def traffic_per_read():
@@ -586,15 +595,12 @@ def run_gpu(args):
         "vs_baseline": None,
         "dtype": "u8",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "pairs_per_gpu": n_pairs, "reads_per_gpu": n_reads,
-                   "filters": N_FILTERS,
-                   "filter_bytes_total": int(sum(os.path.getsize(p) for p in paths)),
-                   "path": {L.PATH_FILTER_MAJOR: "persistent, filter-major",
-                            L.PATH_PERSISTENT: "persistent, read-major"}[best],
-                   "batched_paths_ms": {"filter_major": paths_timed[L.PATH_FILTER_MAJOR][0],
-                                        "read_major": paths_timed[L.PATH_PERSISTENT][0]},
-                   "l2": "inputs larger than L2 (3 GB reads + 685 MB filters)",
-                   "parallelism": f"replicas x{world} (reads sharded, filters replicated)"},
+        "config": bf_config(args),
+        "filter_bytes_total": int(sum(os.path.getsize(p) for p in paths)),
+        "path": {L.PATH_FILTER_MAJOR: "persistent, filter-major",
+                 L.PATH_PERSISTENT: "persistent, read-major"}[best],
+        "batched_paths_ms": {"filter_major": paths_timed[L.PATH_FILTER_MAJOR][0],
+                             "read_major": paths_timed[L.PATH_PERSISTENT][0]},
         "probes_per_s": world * alg_probes / (ms_persistent * 1e-3),
         "probes_algorithmic_per_step": alg_probes,
         "probes_issued_per_step": issued,
@@ -813,7 +819,7 @@ SINGLE = {
     "varlen": dict(name="3.1 Gbp", glen=3_100_000_000, gc=0.41, repeat_frac=0.45, rep_min=300,
                    rep_max=6000, div_min=0.10, div_max=0.20, reads=50_000_000, len_min=50,
                    len_max=300, long_frac=0.05, long_min=300, long_max=10_000, ref_frac=0.7,
-                   sub=0.01, seed=3003,
+                   sub=0.01, seed=3003, l2_note="inputs larger than L2",
                    workload="1 filter from a 3.1 Gbp reference (41% GC, 45% repeats 300 bp-6 kb "
                             "at 10-20% divergence; k=25, FPR 0.075, 2.12 GB), 50M single-end "
                             "reads 50-300 bp log-uniform with 5% 300 bp-10 kb, 70% from the "
@@ -821,12 +827,24 @@ SINGLE = {
     "small": dict(name="5 Mbp", glen=5_000_000, gc=0.5, repeat_frac=0.0, rep_min=0, rep_max=0,
                   div_min=0.0, div_max=0.0, reads=1_000_000, len_min=150, len_max=150,
                   long_frac=0.0, long_min=0, long_max=0, ref_frac=0.5, sub=0.01, seed=1001,
+                  l2_note="filter L2-resident (3.4 MB); reads larger than L2",
                   workload="1 filter from a 5 Mbp uniform reference (k=25, FPR 0.075, 3.4 MB), "
                            "1M single-end 150 bp reads, 50% from the reference with 1% "
                            "substitutions, score 0.15"),
 }
 PLAIN_BATCH = 1 << 18   # reads per launch of the plain path (the CLI's batch)
 SINGLE_METRIC = "reads/s & Bloom probes/s on 1 B200: batched vs plain kernel, % HBM sector peak"
+
+
+def single_config(cfg, args):
+    """The line's config for a single-filter workload: what the workload is,
+    the same on the GPU arm and on the reference arm (figures of the run, such
+    as the tuned launch configuration, sit beside it in the line)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"workload": cfg["workload"],
+            "reads_per_gpu": args.reads if args.reads_set else cfg["reads"],
+            "l2": cfg["l2_note"],
+            "parallelism": f"replicas x{world} (reads sharded, filter replicated)"}
 
 
 def single_setup(cfg, device, n_reads, rank=0):
@@ -1176,11 +1194,8 @@ def run_single(args):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batched,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic",
-        "config": {"workload": cfg["workload"], "reads_per_gpu": n, "bases_per_gpu": bases,
-                   "filter_bytes": fbytes, "tuned": tune,
-                   "l2": ("filter L2-resident (3.4 MB); reads larger than L2" if l2_resident
-                          else "inputs larger than L2"),
-                   "parallelism": f"replicas x{world} (reads sharded, filter replicated)"},
+        "config": single_config(cfg, args),
+        "bases_per_gpu": bases, "filter_bytes": fbytes, "tuned": tune,
         "probes_per_s": world * alg_probes / (ms_batched * 1e-3),
         "probes_algorithmic_per_step": alg_probes, "probes_issued_per_step": issued,
         "frames_hashed_per_step": frames,
@@ -1287,8 +1302,8 @@ def run_single_reference(args):
         f"first {n} reads of the workload per step ({int(off[n])} bases), "
         f"BioBloomClassifier::filter compiled from the reference sources, {threads} OpenMP "
         "threads, filter load excluded", threads,
-        {"config": {"workload": cfg["workload"], "reads_per_step": n,
-                    "bases_per_step": int(off[n])}})), flush=True)
+        {"config": single_config(cfg, args), "reads_per_step": n,
+         "bases_per_step": int(off[n])})), flush=True)
 
 
 def write_single_fastq(path, s1, off, n):
