@@ -147,19 +147,33 @@ def workdir():
     return d
 
 
-def build_filters(d, device):
+def build_once(rank, pg, build):
+    """Input files cached on this host, which every rank reads, are written by
+    rank 0 alone while the other ranks wait at a barrier: ranks share the cache
+    directory, and a rank that rewrote a file another rank was already reading
+    would cut that read short."""
+    if rank == 0:
+        build()
+    if pg:
+        pg.barrier()
+
+
+def build_filters(d, device, rank=0, pg=None):
     """Generate the 10 references and build their filters (cached in d)."""
     from biobloom_b200 import synth
     paths = [os.path.join(d, f"ref{j}.bf") for j in range(N_FILTERS)]
     genomes = []
     t0 = time.time()
     for j in range(N_FILTERS):
-        g = synth.genome(1002 * 1000 + j, REF_LEN, gc=0.41, repeat_frac=0.05, rep_min=300,
-                         rep_max=300)
-        genomes.append(g)
-        if not (os.path.exists(paths[j]) and os.path.exists(paths[j][:-2] + "txt")):
-            synth.make_filter([g], paths[j][:-3], f"ref{j}", k=K, fpr=FPR, device=device,
-                              sources=f"ref{j}.fa")
+        genomes.append(synth.genome(1002 * 1000 + j, REF_LEN, gc=0.41, repeat_frac=0.05,
+                                    rep_min=300, rep_max=300))
+
+    def build():
+        for j, g in enumerate(genomes):
+            if not (os.path.exists(paths[j]) and os.path.exists(paths[j][:-2] + "txt")):
+                synth.make_filter([g], paths[j][:-3], f"ref{j}", k=K, fpr=FPR, device=device,
+                                  sources=f"ref{j}.fa")
+    build_once(rank, pg, build)
     log(f"references + filters: {time.time() - t0:.1f} s")
     return paths, genomes
 
@@ -376,7 +390,7 @@ def run_gpu(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     d = workdir()
-    paths, genomes = build_filters(d, local)
+    paths, genomes = build_filters(d, local, rank, pg)
     n_pairs = args.pairs
     s1, s2, off = make_reads(genomes, n_pairs, 5000 + rank)
     n_reads = 2 * n_pairs
@@ -847,7 +861,7 @@ def single_config(cfg, args):
             "parallelism": f"replicas x{world} (reads sharded, filter replicated)"}
 
 
-def single_setup(cfg, device, n_reads, rank=0):
+def single_setup(cfg, device, n_reads, rank=0, pg=None):
     from biobloom_b200 import synth
     d = os.path.join(tempfile.gettempdir(), f"bbt_bench_{cfg['seed']}")
     os.makedirs(d, exist_ok=True)
@@ -856,9 +870,12 @@ def single_setup(cfg, device, n_reads, rank=0):
                      rep_min=cfg["rep_min"], rep_max=cfg["rep_max"], div_min=cfg["div_min"],
                      div_max=cfg["div_max"])
     path = os.path.join(d, "genome.bf")
-    if not (os.path.exists(path) and os.path.exists(path[:-2] + "txt")):
-        synth.make_filter([g], path[:-3], "genome", k=K, fpr=FPR, device=device,
-                          sources="genome.fa")
+
+    def build():
+        if not (os.path.exists(path) and os.path.exists(path[:-2] + "txt")):
+            synth.make_filter([g], path[:-3], "genome", k=K, fpr=FPR, device=device,
+                              sources="genome.fa")
+    build_once(rank, pg, build)
     log(f"reference + filter: {time.time() - t0:.1f} s")
     t0 = time.time()
     p = synth.read_params(cfg["len_min"], cfg["len_max"], long_frac=cfg["long_frac"],
@@ -962,7 +979,7 @@ def run_single(args):
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n = args.reads if args.reads_set else cfg["reads"]
-    d, path, s1, off = single_setup(cfg, local, n, rank)
+    d, path, s1, off = single_setup(cfg, local, n, rank, pg)
     bases = int(off[-1])
     h1 = torch.from_numpy(s1[:max(bases, 1)]).pin_memory()
     hoff = torch.from_numpy(off.view(np.int64)).pin_memory()
@@ -1346,12 +1363,15 @@ def run_serve(args):
                      rep_min=cfg["rep_min"], rep_max=cfg["rep_max"], div_min=cfg["div_min"],
                      div_max=cfg["div_max"])
     bf_path = os.path.join(d, "genome.bf")
-    if not (os.path.exists(bf_path) and os.path.exists(bf_path[:-2] + "txt")):
-        synth.make_filter([g], bf_path[:-3], "genome", k=K, fpr=FPR, device=local,
-                          sources="genome.fa")
+
+    def build():
+        if not (os.path.exists(bf_path) and os.path.exists(bf_path[:-2] + "txt")):
+            synth.make_filter([g], bf_path[:-3], "genome", k=K, fpr=FPR, device=local,
+                              sources="genome.fa")
+    build_once(rank, pg, build)
     md = os.path.join(tempfile.gettempdir(), f"bbt_bench_mibf_{args.targets}")
     os.makedirs(md, exist_ok=True)
-    mi_path, targets, _ = mi_build(md, args.targets, local)
+    mi_path, targets, _ = mi_build(md, args.targets, local, rank, pg)
     pool_n = 2_000_000
     bs, boff = serve_pool([g], [0.8], pool_n, 5151 + rank)
     ms, moff = serve_pool(targets, [0.9 / len(targets)] * len(targets), pool_n, 5252 + rank)
@@ -1500,15 +1520,18 @@ def mi_targets(n_targets):
     return out, mi_seeds(rng)
 
 
-def mi_build(d, n_targets, device):
+def mi_build(d, n_targets, device, rank=0, pg=None):
     from biobloom_b200.mibf import make_mibf
     t0 = time.time()
     targets, seeds = mi_targets(n_targets)
     path = os.path.join(d, "targets.bf")
-    if not all(os.path.exists(path[:-3] + e) for e in (".bf", ".sdsl", "_ids.txt")):
-        make_mibf(path[:-3], [t.tobytes() for t in targets], list(range(1, n_targets + 1)),
-                  [f"target{i + 1}" for i in range(n_targets)], seeds=seeds, occupancy=0.5,
-                  device=device)
+
+    def build():
+        if not all(os.path.exists(path[:-3] + e) for e in (".bf", ".sdsl", "_ids.txt")):
+            make_mibf(path[:-3], [t.tobytes() for t in targets], list(range(1, n_targets + 1)),
+                      [f"target{i + 1}" for i in range(n_targets)], seeds=seeds, occupancy=0.5,
+                      device=device)
+    build_once(rank, pg, build)
     log(f"targets + miBF: {time.time() - t0:.1f} s")
     return path, targets, seeds
 
@@ -1599,7 +1622,7 @@ def run_mibf(args):
     dev = torch.device("cuda", local)
     d = os.path.join(tempfile.gettempdir(), f"bbt_bench_mibf_{args.targets}")
     os.makedirs(d, exist_ok=True)
-    path, targets, _ = mi_build(d, args.targets, local)
+    path, targets, _ = mi_build(d, args.targets, local, rank, pg)
     n = args.reads
     s1, off = mi_reads(targets, n, 6000 + rank)
     del targets
