@@ -1112,6 +1112,8 @@ def run_single(args):
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
+    if pg:
+        pg.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
@@ -1144,6 +1146,8 @@ def run_single(args):
 
     for _ in range(max(1, args.warmup)):
         e2e_packed_step()
+    if pg:
+        pg.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_packed_step()
