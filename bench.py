@@ -1499,6 +1499,15 @@ def mi_workload(n_targets, n_reads):
             f"reads (90% from targets with 1% substitutions, 10% random)")
 
 
+def mi_config(args):
+    """The miBF workload's config, the same on the GPU arm and on the reference
+    arm (figures of the run sit beside it in the line)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    return {"workload": mi_workload(args.targets, args.reads), "reads_per_gpu": args.reads,
+            "targets": args.targets, "l2": "inputs larger than L2 (3 GB reads + 5 GB miBF)",
+            "parallelism": f"replicas x{world} (reads sharded, miBF replicated)"}
+
+
 def mi_seeds(rng):
     out = []
     for _ in range(3):
@@ -1507,11 +1516,16 @@ def mi_seeds(rng):
     return out
 
 
-def mi_targets(n_targets):
-    from biobloom_b200 import synth
+def mi_targets(n_targets, genome=None):
+    """The targets and spaced seeds; genome makes one seeded sequence (default:
+    the product generator; the reference arm passes the oracle's copy, which
+    makes the same bytes)."""
+    if genome is None:
+        from biobloom_b200 import synth
+        genome = synth.genome
     rng = np.random.default_rng(4004)
     gcs = rng.uniform(0.35, 0.65, n_targets)
-    pristine = [synth.genome(4_000_000 + i, MI_TARGET_LEN, gc=float(gcs[i]))
+    pristine = [genome(4_000_000 + i, MI_TARGET_LEN, gc=float(gcs[i]))
                 for i in range(n_targets)]
     out = [g.copy() for g in pristine]
     blk = int(MI_SHARED * MI_TARGET_LEN)
@@ -1540,12 +1554,49 @@ def mi_build(d, n_targets, device, rank=0, pg=None):
     return path, targets, seeds
 
 
-def mi_reads(targets, n_reads, seed):
-    from biobloom_b200 import synth
-    p = synth.read_params(READ_LEN, READ_LEN, sub_rate=MI_SUB)
+def mi_reads(targets, n_reads, seed, oracle=False):
+    """Reads of the miBF workload, by the product generator or (oracle=True)
+    by the oracle's copy of it: the same bytes."""
+    if oracle:
+        from tests import oracle_lib as gen
+        params, reads = gen.read_params, gen.synth_reads
+    else:
+        from biobloom_b200 import synth as gen
+        params, reads = gen.read_params, gen.reads
+    p = params(READ_LEN, READ_LEN, sub_rate=MI_SUB)
     frac = [0.9 / len(targets)] * len(targets)
-    s1, off, _, _ = synth.reads(seed, targets, frac, n_reads, p)
+    s1, off, _, _ = reads(seed, targets, frac, n_reads, p)
     return s1, off
+
+
+def ref_mi_build(d, n_targets, threads):
+    """The miBF workload's filter made without the product library: targets
+    from the oracle's copy of the generator, written as one FASTA file (record
+    i + 1 named target<i+1>, so IDs follow the target order), and the miBF from
+    the reference's own maker (oracle/_ref/biobloommimaker, IDs by FASTA
+    header, occupancy 0.5, the workload's spaced seeds).  Returns (path,
+    targets, error)."""
+    from tests import oracle_lib as ol
+    t0 = time.time()
+    targets, seeds = mi_targets(n_targets, genome=ol.synth_genome)
+    path = os.path.join(d, "targets.bf")
+    if not all(os.path.exists(path[:-3] + e) for e in (".bf", ".sdsl", "_ids.txt")):
+        maker = os.path.join(ROOT, "oracle", "_ref", "biobloommimaker")
+        if not os.path.exists(maker):
+            return None, None, "oracle/_ref/biobloommimaker is not built"
+        fa = os.path.join(d, "targets.fa")
+        with open(fa, "wb") as f:
+            for i, t in enumerate(targets):
+                f.write(b">target%d\n" % (i + 1))
+                f.write(t.tobytes())
+                f.write(b"\n")
+        pr = subprocess.run([maker, "-t", str(threads), "-p", "targets", "-b", "0.5",
+                             "-S", " ".join(seeds), fa], cwd=d, capture_output=True, text=True)
+        os.unlink(fa)
+        if pr.returncode:
+            return None, None, "reference MI maker failed: " + pr.stderr[-300:]
+    log(f"reference arm: targets + miBF (reference maker) {time.time() - t0:.1f} s")
+    return path, targets, None
 
 
 def mi_cpu_run(d, path, s1, off, n, threads):
@@ -1769,15 +1820,10 @@ def run_mibf(args):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic",
-        "config": {"workload": mi_workload(args.targets, n), "reads_per_gpu": n,
-                   "targets": args.targets,
-                   "layout": "dense ID map" if dense else "rank blocks + ID array",
-                   "bucketed_query": {-1: "off (default)", 0: "off",
-                                      1: "on", 2: "auto"}[args.mibf_bucketing],
-                   "filter_bytes": int(os.path.getsize(path) + os.path.getsize(path[:-3] +
-                                                                             ".sdsl")),
-                   "l2": "inputs larger than L2 (3 GB reads + 5 GB miBF)",
-                   "parallelism": f"replicas x{world} (reads sharded, miBF replicated)"},
+        "config": mi_config(args),
+        "layout": "dense ID map" if dense else "rank blocks + ID array",
+        "bucketed_query": {-1: "off (default)", 0: "off", 1: "on", 2: "auto"}[args.mibf_bucketing],
+        "filter_bytes": int(os.path.getsize(path) + os.path.getsize(path[:-3] + ".sdsl")),
         "frames_per_step": frames, "probes_per_step": probes, "probe_hits_per_step": phits,
         "probes_per_s": world * probes / (ms * 1e-3),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -1812,17 +1858,19 @@ def run_mibf(args):
 
 
 def run_mibf_reference(args):
-    world, rank, local, pg = dist_setup(args)
-    if rank != 0:
-        if pg:
-            pg.barrier()
-            pg.destroy_process_group()
+    """The miBF workload's CPU arm: the reference's own MI categorizer on a
+    bounded sample of the workload's reads, all host threads, over inputs made
+    without the product library (ref_mi_build)."""
+    if not ref_rank_zero():
         return
-    d = os.path.join(tempfile.gettempdir(), f"bbt_bench_mibf_{args.targets}")
+    d = os.path.join(tempfile.gettempdir(), f"bbt_ref_mibf_{args.targets}")
     os.makedirs(d, exist_ok=True)
-    path, targets, _ = mi_build(d, args.targets, local)
-    s1, off = mi_reads(targets, 400_000, 6000)
     threads = os.cpu_count() or 1
+    path, targets, err = ref_mi_build(d, args.targets, threads)
+    if path is None:
+        print(json.dumps({"impl": "reference", "unavailable": err}))
+        return
+    s1, off = mi_reads(targets, 400_000, 6000, oracle=True)
     sec, err = mi_cpu_run(d, path, s1, off, 20000, threads)
     if sec is None:
         print(json.dumps({"impl": "reference", "unavailable": err}))
@@ -1839,21 +1887,15 @@ def run_mibf_reference(args):
             times.append(sec)
     sec = sum(times) / len(times)
     value = n / sec
-    line = {"impl": "reference", "metric": MI_METRIC, "value": value, "unit": "reads/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
-            "config": {"workload": mi_workload(args.targets, n), "reads_per_step": n},
-            "cpu_baseline": {"value": value, "unit": "reads/s", "cores": threads,
-                             "kind": "reference",
-                             "sample": f"{n} reads per step, MIBFClassifier::filter from the "
-                                       "reference sources over the oracle's miBF structures"},
-            "e2e": {"value": value, "unit": "reads/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-    if pg:
-        pg.barrier()
-        pg.destroy_process_group()
+    print(json.dumps(ref_line(
+        args, MI_METRIC, value, sec, mi_workload(args.targets, args.reads),
+        f"first {n} reads of the workload per step, MIBFClassifier::filter from the reference "
+        f"sources over the shim's miBF structures, {threads} OpenMP threads, filter load "
+        "excluded", threads,
+        {"config": mi_config(args), "reads_per_step": n,
+         "inputs": "targets and reads made by the CPU oracle's generator (oracle/synth_oracle.c, "
+                   "the same bytes as the GPU arm's), the miBF by the reference's own maker "
+                   "(oracle/_ref/biobloommimaker)"})), flush=True)
 
 
 # ---------------------------------------------------------------- gather ceilings
