@@ -370,10 +370,10 @@ def run_reference(args):
           flush=True)
 
 
-def traffic_per_read():
-    """DRAM bytes per read of the classify kernel from the committed ncu
-    summary (profiles/classify_c2_dram.json), or None."""
-    p = os.path.join(ROOT, "profiles", "classify_c2_dram.json")
+def traffic_per_read(name="classify_c2_dram.json"):
+    """DRAM bytes per read of a classify kernel from a committed ncu summary
+    (profiles/<name>), or None."""
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     with open(p) as f:
@@ -1205,6 +1205,12 @@ def run_single(args):
         L.check(L.lib().bbt_measure_gather(local, fbytes // 4096 * 4096, 1 << 29, 0, 5,
                                            ctypes.byref(rate)))
         issued_rate = issued / (k_ms * 1e-3)
+        tpr = traffic_per_read("classify_varlen_dram.json")
+        if tpr and tune["path"] != L.PATH_BUCKETED:
+            roofline["traffic"] = tpr * n
+            roofline["traffic_note"] = ("persistent kernel DRAM read+write per read from the "
+                                        "committed ncu capture of 400k reads of this workload, "
+                                        "scaled to the step's reads")
         roofline["random_gather"] = {
             "ceiling_per_s": rate.value, "issued_probes_per_s": issued_rate,
             "frac": issued_rate / rate.value if rate.value else None,
