@@ -226,15 +226,6 @@ int main(int argc, char **argv)
 		default: break;
 		}
 	}
-	string out_type;
-	if (fasta && fastq) {
-		cerr << "Error: fasta (--fa) and fastq (--fq) outputs types cannot be both set" << endl;
-		exit(1);
-	} else if (fastq) {
-		out_type = "fq";
-	} else if (fasta) {
-		out_type = "fa";
-	}
 	vector<string> files;
 	while (optind < argc)
 		files.push_back(argv[optind++]);
@@ -245,8 +236,8 @@ int main(int argc, char **argv)
 			smart = true;
 		} else if (files.size() != 2 && file_list.empty()) {
 			cerr << "Usage of paired end mode:\n"
-			        "biobloomcategorizer [OPTION]... -f \"[FILTER1]...\" [FILEPAIR1] [FILEPAIR2]\n"
-			        "or biobloomcategorizer [OPTION]... -f \"[FILTER1]...\" [SMARTPAIR]\n"
+			        "BioBloomCategorizer [OPTION]... -f \"[FILTER1]...\" [FILEPAIR1] [FILEPAIR2]\n"
+			        "or BioBloomCategorizer [OPTION]... -f \"[FILTER1]...\" [SMARTPAIR]\n"
 			     << endl;
 			die = true;
 		}
@@ -267,6 +258,30 @@ int main(int argc, char **argv)
 	if (die) {
 		cerr << "Try '--help' for more information.\n";
 		exit(EXIT_FAILURE);
+	}
+	/* the output folder, then the output type, in the reference's order
+	 * (BioBloomCategorizer.cpp:50-63,390-405) */
+	if (prefix.find('/') != string::npos) {
+		struct stat sb;
+		string dir = prefix.substr(0, prefix.find_last_of('/'));
+		if (stat(dir.c_str(), &sb) == 0) {
+			if (!S_ISDIR(sb.st_mode)) {
+				cerr << "Error: Output folder - file exists with this name. " << dir << endl;
+				exit(1);
+			}
+		} else {
+			cerr << "Error: Output folder does not exist. " << dir << endl;
+			exit(1);
+		}
+	}
+	string out_type;
+	if (fasta && fastq) {
+		cerr << "Error: fasta (--fa) and fastq (--fq) outputs types cannot be both set" << endl;
+		exit(1);
+	} else if (fastq) {
+		out_type = "fq";
+	} else if (fasta) {
+		out_type = "fa";
 	}
 	if (paired && !file_list.empty() && !out_type.empty()) {
 		/* the reference dereferences the empty input-file list here */
@@ -296,14 +311,6 @@ int main(int argc, char **argv)
 			cerr << "Error - s must be a positive integer or a floating point between 0 and 1."
 			     << endl;
 			exit(EXIT_FAILURE);
-		}
-	}
-	if (prefix.find('/') != string::npos) {
-		struct stat sb;
-		string dir = prefix.substr(0, prefix.find_last_of('/'));
-		if (stat(dir.c_str(), &sb) != 0 || !S_ISDIR(sb.st_mode)) {
-			cerr << "Error: Output folder does not exist. " << dir << endl;
-			exit(1);
 		}
 	}
 	for (const string &f : paths) {

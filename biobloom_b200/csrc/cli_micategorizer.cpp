@@ -120,7 +120,25 @@ int main(int argc, char **argv)
 		case 'f': filter = optarg; break;
 		case 'p': prefix = optarg; break;
 		case 'h': usage_exit(); break;
-		case 'I': case 't': break;
+		case 'I': {
+			/* the report interval has no use here, but is parsed as the
+			 * reference does, which returns 0 on a bad value
+			 * (BioBloomMICategorizer.cpp:187-194) */
+			unsigned interval = 0;
+			stringstream conv(optarg);
+			if (!(conv >> interval)) {
+				cerr << "Error - Invalid parameters! I: " << optarg << endl;
+				return 0;
+			}
+			break;
+		}
+		case 't': {
+			/* host threads: parsed and checked as the reference does; the
+			 * device does the classification */
+			unsigned threads = 0;
+			parse_or_die(optarg, threads, 't');
+			break;
+		}
 		case 'e': paired = true; break;
 		case 'a': parse_or_die(optarg, p.frame_matches, 'a'); break;
 		case 'b': p.best_hit_agree = 1; break;
@@ -181,7 +199,12 @@ int main(int argc, char **argv)
 	if (prefix.find('/') != string::npos) {
 		struct stat sb;
 		string dir = prefix.substr(0, prefix.find_last_of('/'));
-		if (stat(dir.c_str(), &sb) != 0 || !S_ISDIR(sb.st_mode)) {
+		if (stat(dir.c_str(), &sb) == 0) {
+			if (!S_ISDIR(sb.st_mode)) {
+				cerr << "Error: Output folder - file exists with this name. " << dir << endl;
+				exit(1);
+			}
+		} else {
 			cerr << "Error: Output folder does not exist. " << dir << endl;
 			exit(1);
 		}
