@@ -160,7 +160,30 @@ int main(int argc, char **argv)
 		case 'h': usage_exit(EXIT_SUCCESS); break;
 		case 'e': paired = true; break;
 		case 'i': p.inclusive = 1; break;
-		case 'I': case 't': case 'm': break;
+		case 'I': {
+			/* the report interval has no use here, but is parsed as the
+			 * reference does, which returns 0 on a bad value
+			 * (BioBloomCategorizer.cpp:227-234) */
+			unsigned interval = 0;
+			stringstream conv(optarg);
+			if (!(conv >> interval)) {
+				cerr << "Error - Invalid parameters! I: " << optarg << endl;
+				return 0;
+			}
+			break;
+		}
+		case 't': {
+			/* host threads: parsed and checked as the reference does
+			 * (BioBloomCategorizer.cpp:243-250); the device classifies */
+			unsigned threads = 0;
+			stringstream conv(optarg);
+			if (!(conv >> threads)) {
+				cerr << "Error - Invalid parameter! t: " << optarg << endl;
+				exit(EXIT_FAILURE);
+			}
+			break;
+		}
+		case 'm': break;
 		case 'r': {
 			stringstream conv(optarg);
 			if (!(conv >> p.streak_threshold)) {
