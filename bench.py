@@ -922,10 +922,10 @@ def single_cpu(d, path, s1, off, budget_s=15.0):
 PARITY_READS = 200_000
 
 
-def harness_hits(harness, paths, fq1, fq2=None):
+def harness_hits(harness, paths, fq1, fq2=None, score=SCORE, streak=STREAK):
     """Per-read hit lists from the reference's own SeqEval::evalRead
     (ref_harness hits), in file order: one list (or pair of lists) per read."""
-    cmd = [harness, "hits", str(SCORE), str(STREAK), ",".join(paths), fq1] + ([fq2] if fq2 else [])
+    cmd = [harness, "hits", str(score), str(streak), ",".join(paths), fq1] + ([fq2] if fq2 else [])
     pr = subprocess.run(cmd, capture_output=True, text=True)
     if pr.returncode:
         raise RuntimeError("ref_harness hits failed: " + pr.stderr[-300:])

@@ -1,0 +1,66 @@
+"""The CPU oracle against the reference's own SeqEval::evalRead, live, on seeded
+random cases (oracle/_ref/ref_harness, compiled from the reference sources):
+filters with k from 12 to 64 and 1 to 7 hash functions, reads of 10 bp to
+2 kb with N runs, lower-case bases and substitutions, scores from 0 to 1 and
+streak thresholds 0 to 5.  Per-read hit sets must be equal.  Host only; skipped
+where the reference has not been built (make -C oracle ref)."""
+import os
+
+import numpy as np
+import pytest
+
+from tests import oracle_lib as ol
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HARNESS = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+
+
+def _reads(rng, genomes, n):
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    out = []
+    for _ in range(n):
+        length = int(rng.integers(10, 2000))
+        src = int(rng.integers(-1, len(genomes)))
+        if src >= 0:
+            st = int(rng.integers(0, len(genomes[src]) - length))
+            r = genomes[src][st:st + length].copy()
+        else:
+            r = rng.choice(acgt, length)
+        m = rng.random(length) < 0.01
+        r[m] = rng.choice(acgt, int(m.sum()))
+        if rng.random() < 0.3:
+            a = int(rng.integers(0, length))
+            r[a:a + int(rng.integers(1, 30))] = ord("N")
+        if rng.random() < 0.2:
+            r = np.where(rng.random(length) < 0.5, r | 0x20, r).astype(np.uint8)
+        out.append(r.tobytes())
+    return out
+
+
+@pytest.mark.parametrize("seed,k,h,score,streak", [
+    (1, 25, 0, 0.15, 3), (2, 12, 2, 0.5, 1), (3, 31, 5, 0.05, 0), (4, 64, 1, 1.0, 5),
+    (5, 21, 7, 0.0, 2), (6, 17, 3, 0.3, 4)])
+def test_oracle_equals_reference_seqeval(seed, k, h, score, streak, tmp_path):
+    import bench
+    if not os.path.exists(HARNESS):
+        pytest.skip("oracle/_ref/ref_harness is not built (make -C oracle ref)")
+    rng = np.random.default_rng(seed)
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    genomes = [rng.choice(acgt, 40000) for _ in range(2)]
+    filters = [ol.Filter.make([g.tobytes()], k=k, fpr=0.2, h=h) for g in genomes]
+    paths = []
+    for i, f in enumerate(filters):
+        stem = str(tmp_path / f"o{i}")
+        f.store(stem + ".bf")
+        ol.write_info(stem + ".txt", f"o{i}", f.k, 0.2, f.h, 1, "x", f.m, 1, 0.1, 0, 0.1)
+        paths.append(stem + ".bf")
+    reads = _reads(rng, genomes, 1500)
+    seq, off = ol.pack_reads(reads)
+    want, _ = ol.classify(seq, off, filters, score, streak)
+    fq = str(tmp_path / "r.fq")
+    bench.write_single_fastq(fq, np.frombuffer(seq, dtype=np.uint8), off, len(reads))
+    rows = bench.harness_hits(HARNESS, paths, fq, score=score, streak=streak)
+    got = np.array([r[0] for r in rows], dtype=np.uint64)
+    assert len(got) == len(reads)
+    assert want[:, 0].any()          # the case exercises hits
+    assert np.array_equal(got, want[:, 0])
