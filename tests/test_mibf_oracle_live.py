@@ -1,6 +1,6 @@
 """The miBF oracle against the reference MI categorizer, live, on seeded random
 cases: a miBF made by the reference's own maker (oracle/_ref/biobloommimaker)
-from six targets that share segments, single-end reads classified by the
+from six targets that share segments, single-end reads and pairs classified by the
 reference CLI (oracle/_ref/biobloommicategorizer) and by the oracle's query,
 the latter formatted as the CLI's TSV records (MIBFClassifier.hpp:652-736):
 the texts must be equal.  Host only; skipped where the reference has not been
@@ -27,18 +27,10 @@ def _seeds(rng):
     return out
 
 
-def _case(rng, tmp_path):
+def _reads(rng, targets, n):
     acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
-    targets = [rng.choice(acgt, 30000) for _ in range(6)]
-    for i in range(6):                       # shared segments between targets
-        j = (i + 1 + int(rng.integers(0, 5))) % 6
-        a, b = int(rng.integers(0, 27000)), int(rng.integers(0, 27000))
-        targets[i][b:b + 3000] = targets[j][a:a + 3000]
-    with open(tmp_path / "targets.fa", "wb") as f:
-        for i, t in enumerate(targets):
-            f.write(b">t%d\n%s\n" % (i + 1, t.tobytes()))
     reads = []
-    for _ in range(400):
+    for _ in range(n):
         length = int(rng.integers(20, 300))
         if rng.random() < 0.8:
             t = targets[int(rng.integers(0, 6))]
@@ -51,24 +43,45 @@ def _case(rng, tmp_path):
         if rng.random() < 0.1:
             r[int(rng.integers(0, length))] = ord("N")
         reads.append(r.tobytes())
-    with open(tmp_path / "reads.fa", "wb") as f:
-        for i, r in enumerate(reads):
-            f.write(b">r%d\n%s\n" % (i, r))
     return reads
 
 
-@pytest.mark.parametrize("seed,args", [(1, []), (2, ["-s", "50"]), (3, ["-a", "2", "-c", "1"]),
-                                       (4, ["-b", "-m", "2"]), (5, ["-i"])])
-def test_oracle_records_equal_reference_cli(seed, args, tmp_path):
+def _write(path, reads):
+    with open(path, "wb") as f:
+        for i, r in enumerate(reads):
+            f.write(b">r%d\n%s\n" % (i, r))
+
+
+def _case(rng, tmp_path, paired):
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    targets = [rng.choice(acgt, 30000) for _ in range(6)]
+    for i in range(6):                       # shared segments between targets
+        j = (i + 1 + int(rng.integers(0, 5))) % 6
+        a, b = int(rng.integers(0, 27000)), int(rng.integers(0, 27000))
+        targets[i][b:b + 3000] = targets[j][a:a + 3000]
+    with open(tmp_path / "targets.fa", "wb") as f:
+        for i, t in enumerate(targets):
+            f.write(b">t%d\n%s\n" % (i + 1, t.tobytes()))
+    mates = [_reads(rng, targets, 400) for _ in range(2 if paired else 1)]
+    for m, reads in enumerate(mates):
+        _write(tmp_path / f"reads_{m + 1}.fa", reads)
+    return mates
+
+
+@pytest.mark.parametrize("seed,args,paired", [
+    (1, [], False), (2, ["-s", "50"], False), (3, ["-a", "2", "-c", "1"], False),
+    (4, ["-b", "-m", "2"], False), (5, ["-i"], False), (6, [], True), (7, ["-i", "-b"], True)])
+def test_oracle_records_equal_reference_cli(seed, args, paired, tmp_path):
     if not (os.path.exists(MAKER) and os.path.exists(CAT)):
         pytest.skip("the reference's miBF maker / categorizer are not built (make -C oracle ref)")
     rng = np.random.default_rng(seed)
     seeds = _seeds(rng)
-    reads = _case(rng, tmp_path)
+    mates = _case(rng, tmp_path, paired)
     subprocess.run([MAKER, "-t", "2", "-p", "x", "-S", " ".join(seeds), "targets.fa"],
                    cwd=tmp_path, check=True, capture_output=True)
     # one thread: the reference CLI then writes the records in input order
-    p = subprocess.run([CAT, "-t", "1", "-p", "out", "-f", "x.bf"] + args + ["reads.fa"],
+    files = ["-e", "reads_1.fa", "reads_2.fa"] if paired else ["reads_1.fa"]
+    p = subprocess.run([CAT, "-t", "1", "-p", "out", "-f", "x.bf"] + args + files,
                        cwd=tmp_path, check=True, capture_output=True)
     want = p.stdout.decode()
 
@@ -81,17 +94,20 @@ def test_oracle_records_equal_reference_cli(seed, args, tmp_path):
     allowed = 0 if (o["frame_matches"] > h or f.f.nseeds == 0) else h - o["frame_matches"]
     probs, _ = f.frame_probs(len(names), allowed)
     cache, text, hits = {}, [], 0
-    for i, s in enumerate(reads):
-        fc = mu.frame_count(len(s), 0, f.f.k, False)
+    for i, s in enumerate(mates[0]):
+        s2 = mates[1][i] if paired else None
+        fc = mu.frame_count(len(s), len(s2) if paired else 0, f.f.k, paired)
         res, sat = [], 0
         if fc:
             if fc not in cache:
                 cache[fc] = mu.min_counts(fc, probs, o["score"])
-            res, sat = f.query(s, cache[fc], multi=o["multi"], allowed_miss=allowed,
+            res, sat = f.query(s, cache[fc], seq2=s2, multi=o["multi"], allowed_miss=allowed,
                                min_nonsat=o["min_nonsat"], best_agree=o["best"])
         hits += bool(res)
         if o["hit_only"] and not res:
             continue
-        text.append(mu.format_record(names, o["out"], f"r{i}", "", s, b"", res, sat))
+        for m in range(len(mates)):
+            text.append(mu.format_record(names, o["out"], f"r{i}", "", mates[m][i], b"", res,
+                                         sat))
     assert hits > 0                          # the case exercises matches
     assert "".join(text) == want
