@@ -64,3 +64,34 @@ def test_oracle_equals_reference_seqeval(seed, k, h, score, streak, tmp_path):
     assert len(got) == len(reads)
     assert want[:, 0].any()          # the case exercises hits
     assert np.array_equal(got, want[:, 0])
+
+
+@pytest.mark.parametrize("seed,score,streak", [(11, 0.15, 3), (12, 0.4, 1)])
+def test_oracle_pairs_equal_reference_seqeval(seed, score, streak, tmp_path):
+    """Pairs: each mate is evaluated on its own (evaluateReadStd per mate)."""
+    import bench
+    if not os.path.exists(HARNESS):
+        pytest.skip("oracle/_ref/ref_harness is not built (make -C oracle ref)")
+    rng = np.random.default_rng(seed)
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    genomes = [rng.choice(acgt, 40000) for _ in range(3)]
+    filters = [ol.Filter.make([g.tobytes()], k=25, fpr=0.1) for g in genomes]
+    paths = []
+    for i, f in enumerate(filters):
+        stem = str(tmp_path / f"p{i}")
+        f.store(stem + ".bf")
+        ol.write_info(stem + ".txt", f"p{i}", f.k, 0.1, f.h, 1, "x", f.m, 1, 0.1, 0, 0.1)
+        paths.append(stem + ".bf")
+    m1, m2 = _reads(rng, genomes, 1000), _reads(rng, genomes, 1000)
+    s1, off1 = ol.pack_reads(m1)
+    s2, off2 = ol.pack_reads(m2)
+    w1, _ = ol.classify(s1, off1, filters, score, streak)
+    w2, _ = ol.classify(s2, off2, filters, score, streak)
+    fq1, fq2 = str(tmp_path / "r_1.fq"), str(tmp_path / "r_2.fq")
+    bench.write_single_fastq(fq1, np.frombuffer(s1, dtype=np.uint8), off1, len(m1))
+    bench.write_single_fastq(fq2, np.frombuffer(s2, dtype=np.uint8), off2, len(m2))
+    rows = bench.harness_hits(HARNESS, paths, fq1, fq2, score=score, streak=streak)
+    assert len(rows) == len(m1)
+    assert w1[:, 0].any() and w2[:, 0].any()
+    assert np.array_equal(np.array([r[0] for r in rows], dtype=np.uint64), w1[:, 0])
+    assert np.array_equal(np.array([r[1] for r in rows], dtype=np.uint64), w2[:, 0])
