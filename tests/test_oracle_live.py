@@ -1,9 +1,11 @@
-"""The CPU oracle against the reference's own SeqEval::evalRead, live, on seeded
-random cases (oracle/_ref/ref_harness, compiled from the reference sources):
-filters with k from 12 to 64 and 1 to 7 hash functions, reads of 10 bp to
-2 kb with N runs, lower-case bases and substitutions, scores from 0 to 0.8 and
-streak thresholds 0 to 5.  Per-read hit sets must be equal.  Host only; skipped
-where the reference has not been built (make -C oracle ref)."""
+"""The CPU oracle against the reference's own code, live, on seeded random
+cases (oracle/_ref/ref_harness, compiled from the reference sources):
+SeqEval::evalRead on filters with k from 12 to 64 and 1 to 7 hash functions,
+reads of 10 bp to 2 kb with N runs, lower-case bases and substitutions, scores
+from 0 to 0.8 and streak thresholds 0 to 5, single reads and pairs (per-read
+hit sets equal); SeqEval::evalScore under the four scoring methods (bit for
+bit); and sdust's masked intervals on reads with tandem repeats (equal).  Host
+only; skipped where the reference has not been built (make -C oracle ref)."""
 import os
 
 import numpy as np
@@ -95,3 +97,81 @@ def test_oracle_pairs_equal_reference_seqeval(seed, score, streak, tmp_path):
     assert w1[:, 0].any() and w2[:, 0].any()
     assert np.array_equal(np.array([r[0] for r in rows], dtype=np.uint64), w1[:, 0])
     assert np.array_equal(np.array([r[1] for r in rows], dtype=np.uint64), w2[:, 0])
+
+
+def _filters(rng, tmp_path, tag, n=2, k=25, fpr=0.1):
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    genomes = [rng.choice(acgt, 40000) for _ in range(n)]
+    filters = [ol.Filter.make([g.tobytes()], k=k, fpr=fpr) for g in genomes]
+    paths = []
+    for i, f in enumerate(filters):
+        stem = str(tmp_path / f"{tag}{i}")
+        f.store(stem + ".bf")
+        ol.write_info(stem + ".txt", f"{tag}{i}", f.k, fpr, f.h, 1, "x", f.m, 1, 0.1, 0, 0.1)
+        paths.append(stem + ".bf")
+    return genomes, filters, paths
+
+
+@pytest.mark.parametrize("method,scoring", [("simple", ol.SIMPLE), ("length", ol.LENGTH),
+                                            ("harmonic", ol.HARMONIC),
+                                            ("binomial", ol.BINOMIAL)])
+def test_oracle_scores_equal_reference_evalscore(method, scoring, tmp_path):
+    """SeqEval::evalScore of every read against every filter, bit for bit."""
+    import subprocess
+
+    import bench
+    if not os.path.exists(HARNESS):
+        pytest.skip("oracle/_ref/ref_harness is not built (make -C oracle ref)")
+    rng = np.random.default_rng(21)
+    genomes, filters, paths = _filters(rng, tmp_path, "s")
+    reads = _reads(rng, genomes, 800)
+    seq, off = ol.pack_reads(reads)
+    want = ol.classify_scores(seq, off, filters, scoring=scoring, streak=3)
+    fq = str(tmp_path / "r.fq")
+    bench.write_single_fastq(fq, np.frombuffer(seq, dtype=np.uint8), off, len(reads))
+    p = subprocess.run([HARNESS, "scores", method, "3", ",".join(paths), fq],
+                       capture_output=True, text=True, check=True)
+    got = np.array([[int(x, 16) for x in line.split("\t")[1].split(",")]
+                    for line in p.stdout.splitlines()], dtype=np.uint64)
+    assert got.shape == want.shape
+    assert (want > 0).any()
+    assert np.array_equal(got, want.view(np.uint64))
+
+
+@pytest.mark.parametrize("T,W", [(20, 64), (10, 32), (30, 64)])
+def test_oracle_sdust_equals_reference(T, W, tmp_path):
+    """The intervals the reference's sdust masks, on reads with tandem repeats
+    and homopolymers spliced into random sequence."""
+    import subprocess
+
+    import bench
+    if not os.path.exists(HARNESS):
+        pytest.skip("oracle/_ref/ref_harness is not built (make -C oracle ref)")
+    rng = np.random.default_rng(T * 100 + W)
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    reads = []
+    for _ in range(500):
+        r = rng.choice(acgt, int(rng.integers(30, 600)))
+        for _ in range(int(rng.integers(0, 4))):
+            unit = rng.choice(acgt, int(rng.integers(1, 7)))
+            rep = np.tile(unit, int(rng.integers(3, 40)))
+            a = int(rng.integers(0, len(r)))
+            r = np.concatenate([r[:a], rep, r[a:]])
+        if rng.random() < 0.2:
+            r[int(rng.integers(0, len(r)))] = ord("N")
+        reads.append(r.tobytes())
+    seq, off = ol.pack_reads(reads)
+    fq = str(tmp_path / "d.fq")
+    bench.write_single_fastq(fq, np.frombuffer(seq, dtype=np.uint8), off, len(reads))
+    p = subprocess.run([HARNESS, "dust", str(T), str(W), fq], capture_output=True, text=True,
+                       check=True)
+    lines = p.stdout.splitlines()
+    assert len(lines) == len(reads)
+    masked = 0
+    for r, line in zip(reads, lines):
+        field = line.split("\t")[1] if "\t" in line else ""
+        got = [tuple(int(v) for v in iv.split("-")) for iv in field.split(",") if iv]
+        want, _ = ol.sdust(r, T, W)
+        masked += bool(want)
+        assert got == want
+    assert masked > 0
