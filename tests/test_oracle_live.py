@@ -4,7 +4,8 @@ SeqEval::evalRead on filters with k from 12 to 64 and 1 to 7 hash functions,
 reads of 10 bp to 2 kb with N runs, lower-case bases and substitutions, scores
 from 0 to 0.8 and streak thresholds 0 to 5, single reads and pairs (per-read
 hit sets equal); SeqEval::evalScore under the four scoring methods (bit for
-bit); and sdust's masked intervals on reads with tandem repeats (equal).  Host
+bit); sdust's masked intervals on reads with tandem repeats (equal); and the
+reference biobloommaker's bit arrays for several k, FPR and hash counts.  Host
 only; skipped where the reference has not been built (make -C oracle ref)."""
 import os
 
@@ -175,3 +176,34 @@ def test_oracle_sdust_equals_reference(T, W, tmp_path):
         masked += bool(want)
         assert got == want
     assert masked > 0
+
+
+@pytest.mark.parametrize("k,fpr,g", [(25, 0.075, 0), (16, 0.01, 0), (31, 0.2, 5), (64, 0.05, 2)])
+def test_oracle_maker_equals_reference_maker(k, fpr, g, tmp_path):
+    """The reference biobloommaker (BloomFilterGenerator) on multi-record FASTA
+    with N runs and lower case: the oracle's maker gives the same m, h, k and
+    bit array."""
+    import subprocess
+    maker = os.path.join(ROOT, "oracle", "_ref", "biobloommaker")
+    if not os.path.exists(maker):
+        pytest.skip("oracle/_ref/biobloommaker is not built (make -C oracle ref)")
+    rng = np.random.default_rng(k * 1000 + g)
+    acgt = np.frombuffer(b"ACGT", dtype=np.uint8)
+    recs = []
+    for _ in range(4):
+        r = rng.choice(acgt, int(rng.integers(50, 30000)))
+        if rng.random() < 0.5:
+            a = int(rng.integers(0, len(r)))
+            r[a:a + int(rng.integers(1, 50))] = ord("N")
+        if rng.random() < 0.5:
+            r = np.where(rng.random(len(r)) < 0.3, r | 0x20, r).astype(np.uint8)
+        recs.append(r.tobytes())
+    with open(tmp_path / "in.fa", "wb") as f:
+        for i, r in enumerate(recs):
+            f.write(b">c%d\n%s\n" % (i, r))
+    cmd = [maker, "-p", "m", "-k", str(k), "-f", str(fpr)] + (["-g", str(g)] if g else [])
+    subprocess.run(cmd + ["in.fa"], cwd=tmp_path, check=True, capture_output=True)
+    ref = ol.Filter.load(str(tmp_path / "m.bf"))
+    mine = ol.Filter.make(recs, k=k, fpr=fpr, h=g)
+    assert (mine.m, mine.h, mine.k) == (ref.m, ref.h, ref.k)
+    assert np.array_equal(mine.bits(), ref.bits())
