@@ -3,7 +3,8 @@ cases: a miBF made by the reference's own maker (oracle/_ref/biobloommimaker)
 from six targets that share segments, single-end reads and pairs classified by the
 reference CLI (oracle/_ref/biobloommicategorizer) and by the oracle's query,
 the latter formatted as the CLI's TSV records (MIBFClassifier.hpp:652-736):
-the texts must be equal.  Host only; skipped where the reference has not been
+the texts must be equal; and the reference maker's files against the oracle's
+build, byte for byte.  Host only; skipped where the reference has not been
 built (make -C oracle ref)."""
 import os
 import subprocess
@@ -111,3 +112,30 @@ def test_oracle_records_equal_reference_cli(seed, args, paired, tmp_path):
                                          sat))
     assert hits > 0                          # the case exercises matches
     assert "".join(text) == want
+
+
+@pytest.mark.parametrize("seed,mode", [(21, "seeds"), (22, "kmers"), (23, "seeds")])
+def test_oracle_build_equals_reference_maker(seed, mode, tmp_path):
+    """The reference's own miBF maker (BioBloomMIMaker.cpp / MIBFGen.hpp over the
+    shim's MIBFConstructSupport) and the oracle's build write the same .bf and
+    .sdsl bytes, for spaced seeds and for k-mers with 3 hashes, IDs by FASTA
+    header."""
+    import filecmp
+    if not os.path.exists(MAKER):
+        pytest.skip("oracle/_ref/biobloommimaker is not built (make -C oracle ref)")
+    rng = np.random.default_rng(seed)
+    seeds = _seeds(rng)
+    _case(rng, tmp_path, False)
+    targets = []
+    with open(tmp_path / "targets.fa", "rb") as fh:
+        for line in fh.read().split(b"\n"):
+            if line and not line.startswith(b">"):
+                targets.append(line)
+    opts = ["-S", " ".join(seeds)] if mode == "seeds" else ["-k", "25", "-g", "3"]
+    subprocess.run([MAKER, "-t", "2", "-p", "x"] + opts + ["targets.fa"], cwd=tmp_path,
+                   check=True, capture_output=True)
+    m = ol.MIBF.build(targets, list(range(1, len(targets) + 1)),
+                      seeds=seeds if mode == "seeds" else None, k=25, h=3, occupancy=0.5)
+    m.store(str(tmp_path / "o"))
+    for ext in (".bf", ".sdsl"):
+        assert filecmp.cmp(tmp_path / ("o" + ext), tmp_path / ("x" + ext), shallow=False), ext
