@@ -5,7 +5,8 @@ reads of 10 bp to 2 kb with N runs, lower-case bases and substitutions, scores
 from 0 to 0.8 and streak thresholds 0 to 5, single reads and pairs (per-read
 hit sets equal); SeqEval::evalScore under the four scoring methods (bit for
 bit); sdust's masked intervals on reads with tandem repeats (equal); and the
-reference biobloommaker's bit arrays for several k, FPR and hash counts.  Host
+reference biobloommaker's bit arrays for several k, FPR and hash counts; and
+the reference CLI's summary.tsv (reads, pairs, -i, a match length).  Host
 only; skipped where the reference has not been built (make -C oracle ref)."""
 import os
 
@@ -207,3 +208,36 @@ def test_oracle_maker_equals_reference_maker(k, fpr, g, tmp_path):
     mine = ol.Filter.make(recs, k=k, fpr=fpr, h=g)
     assert (mine.m, mine.h, mine.k) == (ref.m, ref.h, ref.k)
     assert np.array_equal(mine.bits(), ref.bits())
+
+
+@pytest.mark.parametrize("paired,inclusive,score", [(False, False, 0.15), (True, False, 0.15),
+                                                    (True, True, 0.3), (False, False, 40)])
+def test_oracle_summary_equals_reference_cli(paired, inclusive, score, tmp_path):
+    """summary.tsv of the reference CLI (oracle/_ref/biobloomcategorizer, the
+    reference's ResultsManager) on random reads and pairs, with and without -i
+    and with a minimum match length: the oracle's counters and summary text
+    give the same file."""
+    import subprocess
+
+    import bench
+    cli = os.path.join(ROOT, "oracle", "_ref", "biobloomcategorizer")
+    if not os.path.exists(cli):
+        pytest.skip("oracle/_ref/biobloomcategorizer is not built (make -C oracle ref)")
+    rng = np.random.default_rng(31 + paired + 2 * inclusive)
+    genomes, filters, paths = _filters(rng, tmp_path, "c", n=3)
+    mates = [_reads(rng, genomes, 700) for _ in range(2 if paired else 1)]
+    scoring = ol.LENGTH if score > 1 else ol.SIMPLE
+    hits, files = [], []
+    for m, reads in enumerate(mates):
+        seq, off = ol.pack_reads(reads)
+        hits.append(ol.classify(seq, off, filters, score, 3, scoring)[0])
+        files.append(str(tmp_path / f"r_{m + 1}.fq"))
+        bench.write_single_fastq(files[-1], np.frombuffer(seq, dtype=np.uint8), off, len(reads))
+    counts, _ = ol.summary_counts(hits[0], 3, hits[1] if paired else None, inclusive=inclusive)
+    args = [cli, "-t", "1", "-p", "out", "-s", str(score), "-f", " ".join(paths)]
+    args += (["-e"] if paired else []) + (["-i"] if inclusive else []) + files
+    subprocess.run(args, cwd=tmp_path, check=True, capture_output=True)
+    with open(tmp_path / "out_summary.tsv") as f:
+        want = f.read()
+    ids = [f"c{i}" for i in range(3)]
+    assert ol.summary_tsv(counts, ids, len(mates[0])) == want
