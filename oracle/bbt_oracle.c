@@ -2,7 +2,8 @@
  * bbt_oracle.c -- CPU oracle (test infrastructure only; see bbt_oracle.h).
  *
  * Plain sequential C.  Every function follows one reference function; the
- * comment above each names it.  Nothing here is optimised: it is the checker.
+ * comment above each names it.  Nothing here is optimised: it is the oracle
+ * the GPU results are compared with.
  */
 #include "bbt_oracle.h"
 

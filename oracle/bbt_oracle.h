@@ -1,8 +1,8 @@
 /*
  * bbt_oracle.h -- CPU oracle for the BioBloom Tools read-classification path.
  *
- * TEST INFRASTRUCTURE ONLY.  This is the checker that the GPU path is compared
- * against.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
+ * TEST INFRASTRUCTURE ONLY.  The GPU path's results are compared with this
+ * oracle's.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline
  * leg may load it; the product library never links or calls it.
  *
  * What it restates (reference paths are relative to the biobloom project):

@@ -1,7 +1,8 @@
 """ctypes access to the CPU oracle (oracle/_build/liboracle.so).
 
 Test infrastructure only: tests/, __graft_entry__.smoke() and bench.py's
-CPU-baseline leg use this module as the checker; the product path never does.
+CPU-baseline leg use this module to compare results with; the product path
+never does.
 """
 import ctypes
 import os
