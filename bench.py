@@ -808,7 +808,7 @@ def run_modes(args):
             if kw.get("score_type") == "binomial":
                 res["cpu_reference"]["note"] = (
                     "Boost is not installed here: the reference's binomial quantile runs on "
-                    "this build's stand-in for boost::math::binomial (oracle/shim)")
+                    "the oracle shim's stand-in for boost::math::binomial (oracle/shim)")
             if res["cpu_reference"].get("reads_per_s"):
                 res["vs_cpu_reference"] = res["reads_per_s"] / res["cpu_reference"]["reads_per_s"]
         out[name] = res

@@ -148,7 +148,7 @@ int main(int argc, char **argv)
 			/* The reference hands -r to MIBFQuerySupport
 			 * (MIBFClassifier.hpp:222-225), whose early-exit rule lives
 			 * in the btl_bloomfilter submodule, absent from the
-			 * reference tree; this build evaluates every frame. */
+			 * reference tree; this implementation evaluates every frame. */
 			cerr << "Warning: -r has no effect: every frame of a read is evaluated" << endl;
 			break;
 		case 'c': parse_or_die(optarg, p.min_nonsat, 'c'); break;
@@ -193,7 +193,7 @@ int main(int argc, char **argv)
 	if (debug)
 		refused += " --debug";
 	if (!refused.empty()) {
-		cerr << "Error: option(s)" << refused << " are not supported by this build" << endl;
+		cerr << "Error: option(s)" << refused << " are not supported by this implementation" << endl;
 		exit(EXIT_FAILURE);
 	}
 	if (prefix.find('/') != string::npos) {

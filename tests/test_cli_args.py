@@ -43,7 +43,7 @@ CASES = {
     "ordered_and_besthit": ["-f", "x.bf", "-c", "-b", "r.fq"],
 }
 
-# -r is left out: this build warns that it has no effect (the rule it feeds
+# -r is left out: this implementation warns that it has no effect (the rule it feeds
 # lives in a submodule absent from the reference tree)
 MI_CASES = {
     "nothing": [],
