@@ -7,7 +7,7 @@ hash count auto = 3, 2.12 GB by the reference's sizing formula) from a seeded
 10-20% divergence); 50M single-end reads, 95% of lengths log-uniform over
 50-300 bp and 5% log-uniform over 300 bp - 10 kb, 70% drawn from the
 reference with 1% substitutions and 30% uniform random; score 0.15.
-Synthetic data: no dataset is available on the box.
+Synthetic data: the reads and references are generated from fixed seeds.
 
 A step classifies all reads once (13.5 G bases and the 2.12 GB filter resident
 in HBM, far above the 126 MB L2, so no L2 flush is needed between steps).
@@ -18,7 +18,7 @@ same metric through the C ABI with pinned host buffers (host->device copies of
 the reads and device->host copies of the per-read results inside the timed
 region).  `--impl reference` times the reference's own classifier
 (BioBloomClassifier::filter compiled from the reference sources,
-oracle/_ref/ref_harness) on the box's host cores, on inputs made by the CPU
+oracle/_ref/ref_harness) on the host's cores, on inputs made by the CPU
 oracle's copy of the generator and filter build (no product library loaded).
 
 With --workload bf: 10 Bloom filters (k=25, FPR 0.075, h=3), each built from
